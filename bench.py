@@ -1,0 +1,467 @@
+#!/usr/bin/env python
+"""Benchmark: GTEPS of BFS / SSSP / CC / PageRank on one B200 (per GPU).
+
+Workload (the reference's headline configuration at scale): RMAT scale 24,
+edge factor 16, a=.57 b=.19 c=.19, self-loops and duplicates removed,
+uint32 weights uniform in [1, 64], seeded; BFS and SSSP from seeded random
+non-isolated roots on the directed graph, CC on the symmetrised graph,
+PageRank (d = 0.85, 20 iterations, FP64) on the directed graph.
+
+One step = BFS(root) + SSSP(root) + CC + PageRank(20) with the step's root
+(roots cycle through 10 seeded roots).  GTEPS numerators: BFS/SSSP = sum of
+out-degrees of reached vertices; CC = edges of the symmetrised graph;
+PageRank = E x iterations.  `value` = all numerators of the K timed steps /
+their device time (CUDA events on the engine's stream, max over ranks).
+`e2e` = the same through the C ABI from pinned host buffers: every step
+uploads both CSRs (cgb_graph_create), runs the four algorithms and reads
+every result back into host memory.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "GTEPS (BFS/SSSP/WCC/PR) on 1 B200: learned vs heuristic schedule, % HBM peak"
+BFS, SSSP, CC, PR = 0, 1, 2, 3
+ALG_NAMES = ["bfs", "sssp", "cc", "pagerank"]
+N_ROOTS = 10
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["cgb200", "reference"], default="cgb200")
+    p.add_argument("--scale", type=int, default=24)
+    p.add_argument("--edge-factor", type=int, default=16)
+    p.add_argument("--seed", type=int, default=1)
+    p.add_argument("--pr-iters", type=int, default=20)
+    p.add_argument("--schedule", choices=["heuristic", "learned"], default="heuristic")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--e2e-steps", type=int, default=0, help="0 = same as --steps")
+    return p.parse_args()
+
+
+# ------------------------------------------------------------------ helpers
+class Clocks:
+    """Samples SM clocks and throttle reasons with nvidia-smi during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
+        mx = [num(r[2]) for r in rows if num(r[2]) is not None]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for i, n in enumerate(names):
+                if r[5 + i].lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def pick_roots(offsets: np.ndarray, seed: int, n: int) -> list:
+    deg = np.diff(offsets.astype(np.int64))
+    cand = np.nonzero(deg)[0]
+    rng = np.random.default_rng(seed + 1000)
+    return [int(x) for x in rng.choice(cand, size=min(n, cand.size), replace=False)]
+
+
+def load_peaks() -> dict:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return {"hbm_gbs": d["hbm_gbs"], "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+# ------------------------------------------------------------------ dist
+class Dist:
+    def __init__(self, want_gpus: int):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = False
+        if self.world > 1:
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device("cuda", self.local))
+            self.pg = True
+
+    def barrier(self):
+        if self.pg:
+            import torch.distributed as dist
+            dist.barrier(device_ids=[self.local])
+
+    def reduce(self, x: float, op: str) -> float:
+        if not self.pg:
+            return float(x)
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([float(x)], dtype=torch.float64, device=f"cuda:{self.local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------- our arm
+def run_step(gd, gs, root, opts, pr_iters):
+    """One step on resident graphs; returns per-algorithm (edges, ms, stats)."""
+    out = []
+    for g, alg, arg in ((gd, BFS, root), (gd, SSSP, root), (gs, CC, 0), (gd, PR, pr_iters)):
+        _, ms = g.run(alg, arg, opts, to_host=False)
+        out.append((alg, g.stats()))
+    return out
+
+
+def bench_cgb200(args, d: Dist):
+    import torch
+    import cggraph_b200 as cg
+    from cggraph_b200 import _lib as L
+
+    dev = d.local
+    torch.cuda.set_device(dev)
+    gd = cg.Graph.rmat(args.scale, args.edge_factor, args.seed, wmax=64, device=dev)
+    gs = cg.Graph.rmat(args.scale, args.edge_factor, args.seed, symmetrise=True, wmax=0, device=dev)
+    off_h, dst_h, w_h = gd.download()
+    roots_all = pick_roots(off_h, args.seed, N_ROOTS * d.world)
+    roots = roots_all[d.rank::d.world]
+    V, Ed, Es = gd.vertexNum, gd.edgeNum, gs.edgeNum
+
+    stream = torch.cuda.current_stream()
+    gd.set_stream(stream)
+    gs.set_stream(stream)
+    sched = L.SCHED_LEARNED if args.schedule == "learned" else L.SCHED_HEURISTIC
+    warm_opts = cg.make_options(schedule=sched)
+    timed_opts = cg.make_options(schedule=sched, flags=L.FLAG_KERNEL_TIMING)
+
+    for i in range(args.warmup):
+        run_step(gd, gs, roots[i % len(roots)], warm_opts, args.pr_iters)
+
+    clocks = Clocks(dev)
+    clocks.start()
+    per_alg_edges = [0] * 4
+    per_alg_ms = [0.0] * 4
+    kclass_ms = [0.0] * 8
+    kclass_launches = [0] * 8
+    launches = 0
+    pr_launch_ms = 0.0
+    pr_launches = 0
+    d.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for k in range(args.steps):
+        for alg, st in run_step(gd, gs, roots[k % len(roots)], timed_opts, args.pr_iters):
+            per_alg_edges[alg] += st.traversed_edges
+            per_alg_ms[alg] += st.ms
+            launches += st.launches
+            for c in range(8):
+                kclass_ms[c] += st.kernel_ms[c]
+                kclass_launches[c] += st.kernel_launches[c]
+            if alg == PR:
+                pr_launch_ms += st.kernel_ms[L.K_PR]
+                pr_launches += st.kernel_launches[L.K_PR]
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    d.barrier()
+    clk = clocks.stop()
+    ms_local = ev0.elapsed_time(ev1)
+    ms_max = d.reduce(ms_local, "max")
+    edges_total = d.reduce(sum(per_alg_edges), "sum")
+    value = edges_total / (ms_max / 1e3) / 1e9
+
+    # roofline of the dominant kernel class
+    peaks = load_peaks()
+    dom = int(np.argmax(kclass_ms))
+    roof = {"bound": "hbm", "unit": "GB/s", "peak": peaks["hbm_gbs"], "peak_source": peaks["source"]}
+    if pr_launches:
+        bytes_per_launch = 12 * Ed + 20 * V + 4
+        avg_s = pr_launch_ms / pr_launches / 1e3
+        achieved = bytes_per_launch / avg_s / 1e9
+        roof.update({"kernel": "k_pr_pull (+k_pr_huge_rows), one PageRank iteration",
+                     "alg_bytes_per_launch": bytes_per_launch, "avg_launch_ms": pr_launch_ms / pr_launches,
+                     "achieved": achieved, "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                     "dominant_class": L.KERNEL_CLASS_NAMES[dom],
+                     "class_share": {L.KERNEL_CLASS_NAMES[c]: round(kclass_ms[c] / max(1e-9, sum(kclass_ms)), 4)
+                                     for c in range(8) if kclass_ms[c] > 0}})
+
+    per_alg = {ALG_NAMES[a]: {"gteps": per_alg_edges[a] / (per_alg_ms[a] / 1e3) / 1e9 if per_alg_ms[a] else None,
+                              "ms_per_run": per_alg_ms[a] / args.steps} for a in range(4)}
+
+    # end to end through the C ABI with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        e2e = bench_e2e(args, d, cg, gd, gs, roots, off_h, dst_h, w_h, sched)
+
+    # CPU baseline: the reference's own engine on this host (rank 0, N = 1)
+    cpu = None
+    if d.world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline(args, gd, gs, off_h, dst_h, w_h, roots)
+        except Exception as e:  # reported, not fatal
+            cpu = {"value": None, "error": str(e)[-300:]}
+
+    gd.set_stream(None)
+    gs.set_stream(None)
+    gd.close()
+    gs.close()
+    result = {
+        "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": d.world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32 (BFS/SSSP/CC), f64 (PageRank)",
+        "data": "synthetic (seeded RMAT, generated on device)",
+        "config": {"workload": f"rmat{args.scale}_ef{args.edge_factor}_bfs_sssp_cc_pr{args.pr_iters}",
+                   "scale": args.scale, "edge_factor": args.edge_factor, "rmat_abc": [0.57, 0.19, 0.19],
+                   "vertices": V, "edges_directed": Ed, "edges_symmetrised": Es, "weights": "uniform [1,64]",
+                   "roots": roots, "schedule": args.schedule, "pr_iterations": args.pr_iters,
+                   "l2": "inputs larger than L2 (directed CSR %.2f GB, symmetrised %.2f GB)"
+                         % ((4 * (V + 1) + 8 * Ed) / 1e9, (4 * (V + 1) + 4 * Es) / 1e9),
+                   "parallelism": f"replicas x{d.world}"},
+        "per_algorithm": per_alg,
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": int(d.reduce(launches, "sum")),
+        "clocks": clk,
+    }
+    return result
+
+
+def bench_e2e(args, d, cg, gd, gs, roots, off_h, dst_h, w_h, sched):
+    import torch
+    V = gd.vertexNum
+    soff_h, sdst_h, _ = gs.download(with_weight=False)
+    pin = lambda a: torch.from_numpy(a.view(np.int32)).pin_memory()  # noqa: E731
+    t_off, t_dst, t_w = pin(off_h), pin(dst_h), pin(w_h)
+    t_soff, t_sdst = pin(soff_h), pin(sdst_h)
+    out_b = torch.empty(V, dtype=torch.int32).pin_memory()
+    out_s = torch.empty(V, dtype=torch.int32).pin_memory()
+    out_c = torch.empty(V, dtype=torch.int32).pin_memory()
+    out_p = torch.empty(V, dtype=torch.float64).pin_memory()
+    opts = cg.make_options(schedule=sched)
+    steps = args.e2e_steps or args.steps
+
+    def step(root):
+        edges = 0
+        g = cg.Graph.from_csr(t_off, t_dst, t_w, vertexNum=V, edgeNum=gd.edgeNum, device=d.local)
+        g.run(BFS, root, opts, out=out_b)
+        edges += g.stats().traversed_edges
+        g.run(SSSP, root, opts, out=out_s)
+        edges += g.stats().traversed_edges
+        g.run(PR, args.pr_iters, opts, out=out_p)
+        edges += g.stats().traversed_edges
+        g.close()
+        h = cg.Graph.from_csr(t_soff, t_sdst, None, vertexNum=V, edgeNum=gs.edgeNum, device=d.local)
+        h.run(CC, 0, opts, out=out_c)
+        edges += h.stats().traversed_edges
+        h.close()
+        return edges
+
+    step(roots[0])  # warm-up (allocator, first-touch of pinned pages)
+    torch.cuda.synchronize()
+    d.barrier()
+    t0 = time.perf_counter()
+    edges = 0
+    for k in range(steps):
+        edges += step(roots[k % len(roots)])
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    d.barrier()
+    s_max = d.reduce(t1 - t0, "max")
+    edges = d.reduce(edges, "sum")
+    h2d = 4 * (V + 1) + 8 * gd.edgeNum + 4 * (V + 1) + 4 * gs.edgeNum
+    d2h = 4 * V * 3 + 8 * V
+    return {"value": edges / s_max / 1e9, "unit": "GTEPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+            "ms_per_step": s_max * 1e3 / steps, "steps": steps,
+            "what": "cgb_graph_create(directed CSR, host pinned) + BFS + SSSP + PR(20) -> host, "
+                    "cgb_graph_create(symmetrised CSR) + CC -> host, destroy; wall clock"}
+
+
+def write_csr_files(dirpath, prefix, off, dst, w):
+    paths = [os.path.join(dirpath, f"{prefix}_{n}.bin") for n in ("off", "dst", "w")]
+    off.tofile(paths[0])
+    dst.tofile(paths[1])
+    if w is not None:
+        w.tofile(paths[2])
+    else:
+        paths[2] = None
+    return paths
+
+
+def cpu_baseline(args, gd, gs, off_h, dst_h, w_h, roots):
+    from oracle import oracle as O
+    if not O.ref_available():
+        return {"value": None, "unit": "GTEPS", "error": "reference harness oracle/_ref/cgref_oracle not built"}
+    threads = os.cpu_count() or 1
+    soff, sdst, _ = gs.download(with_weight=False)
+    tmp = "/dev/shm" if os.path.isdir("/dev/shm") else None
+    with tempfile.TemporaryDirectory(dir=tmp) as dd:
+        pd = write_csr_files(dd, "d", off_h, dst_h, w_h)
+        ps = write_csr_files(dd, "s", soff, sdst, None)
+        V, Ed, Es = gd.vertexNum, gd.edgeNum, gs.edgeNum
+        r3 = roots[:3]
+        ib = O.ref_run_files(pd, V, Ed, 0, r3, len(r3), threads)
+        isp = O.ref_run_files(pd, V, Ed, 1, r3, len(r3), threads)
+        ic = O.ref_run_files(ps, V, Es, 2, [0], 2, threads)
+    in_off, in_src = O.csc(off_h, dst_h)
+    t0 = time.perf_counter()
+    O.pagerank_pull_omp(off_h, in_off, in_src, 2, threads)
+    pr_s = time.perf_counter() - t0
+    edges = sum(ib["edges"]) + sum(isp["edges"]) + Es * len(ic["ms"]) + Ed * 2
+    secs = (sum(ib["ms"]) + sum(isp["ms"]) + sum(ic["ms"])) / 1e3 + pr_s
+    return {"value": edges / secs / 1e9, "unit": "GTEPS", "cores": int(ib["threads"]), "kind": "reference",
+            "sample": f"reference Graph_Numa (MULTI_CORE) on the same RMAT-{args.scale} CSR: BFS x3 roots, "
+                      f"SSSP x3 roots, CC x2 (symmetrised); PageRank by the FP64 OpenMP port (2 iterations, "
+                      f"the reference's own PageRank does not build); times from the reference's own timer",
+            "per_algorithm_gteps": {
+                "bfs": sum(ib["edges"]) / (sum(ib["ms"]) / 1e3) / 1e9,
+                "sssp": sum(isp["edges"]) / (sum(isp["ms"]) / 1e3) / 1e9,
+                "cc": Es * len(ic["ms"]) / (sum(ic["ms"]) / 1e3) / 1e9,
+                "pagerank_port": Ed * 2 / pr_s / 1e9}}
+
+
+# ------------------------------------------------------------ reference arm
+def bench_reference(args, d: Dist):
+    """The reference's own CPU implementation (Graph_Numa, built from the
+    reference sources into oracle/_ref) on this host's cores, same workload
+    and metric.  PageRank uses the FP64 OpenMP port because the reference's
+    PageRank does not build.  Input synthesis (the seeded RMAT CSR) is done
+    before any timing."""
+    if d.rank != 0:
+        return None
+    from oracle import oracle as O
+    if not O.ref_available():
+        return {"impl": "reference", "unavailable": "reference harness oracle/_ref/cgref_oracle was not built"}
+    import cggraph_b200 as cg
+    threads = os.cpu_count() or 1
+    gd = cg.Graph.rmat(args.scale, args.edge_factor, args.seed, wmax=64, device=d.local)
+    gs = cg.Graph.rmat(args.scale, args.edge_factor, args.seed, symmetrise=True, wmax=0, device=d.local)
+    off_h, dst_h, w_h = gd.download()
+    soff, sdst, _ = gs.download(with_weight=False)
+    V, Ed, Es = gd.vertexNum, gd.edgeNum, gs.edgeNum
+    gd.close()
+    gs.close()
+    roots = pick_roots(off_h, args.seed, N_ROOTS)
+    n = args.warmup + args.steps
+    seq = [roots[i % len(roots)] for i in range(n)]
+    tmp = "/dev/shm" if os.path.isdir("/dev/shm") else None
+    with tempfile.TemporaryDirectory(dir=tmp) as dd:
+        pd = write_csr_files(dd, "d", off_h, dst_h, w_h)
+        ps = write_csr_files(dd, "s", soff, sdst, None)
+        ib = O.ref_run_files(pd, V, Ed, 0, seq, n, threads)
+        isp = O.ref_run_files(pd, V, Ed, 1, seq, n, threads)
+        ic = O.ref_run_files(ps, V, Es, 2, [0], n, threads)
+    in_off, in_src = O.csc(off_h, dst_h)
+    pr_ms = []
+    for _ in range(n):
+        t0 = time.perf_counter()
+        O.pagerank_pull_omp(off_h, in_off, in_src, args.pr_iters, threads)
+        pr_ms.append((time.perf_counter() - t0) * 1e3)
+    w = args.warmup
+    edges = sum(ib["edges"][w:]) + sum(isp["edges"][w:]) + Es * args.steps + Ed * args.pr_iters * args.steps
+    ms = sum(ib["ms"][w:]) + sum(isp["ms"][w:]) + sum(ic["ms"][w:]) + sum(pr_ms[w:])
+    value = edges / (ms / 1e3) / 1e9
+    return {
+        "metric": METRIC, "value": value, "unit": "GTEPS", "impl": "reference", "n_gpus": d.world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32 (BFS/SSSP/CC), f64 (PageRank)",
+        "data": "synthetic (seeded RMAT)",
+        "config": {"workload": f"rmat{args.scale}_ef{args.edge_factor}_bfs_sssp_cc_pr{args.pr_iters}",
+                   "scale": args.scale, "edge_factor": args.edge_factor, "vertices": V, "edges_directed": Ed,
+                   "edges_symmetrised": Es, "roots": roots, "pr_iterations": args.pr_iters},
+        "per_algorithm": {
+            "bfs": sum(ib["edges"][w:]) / (sum(ib["ms"][w:]) / 1e3) / 1e9,
+            "sssp": sum(isp["edges"][w:]) / (sum(isp["ms"][w:]) / 1e3) / 1e9,
+            "cc": Es * args.steps / (sum(ic["ms"][w:]) / 1e3) / 1e9,
+            "pagerank_port": Ed * args.pr_iters * args.steps / (sum(pr_ms[w:]) / 1e3) / 1e9},
+        "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": int(ib["threads"]), "kind": "reference",
+                         "sample": "each step: reference Graph_Numa BFS + SSSP from the step's root and CC on the "
+                                   "symmetrised graph, plus the FP64 OpenMP PageRank port; reference's own timer"},
+        "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse_args()
+    d = Dist(args.gpus)
+    try:
+        if args.impl == "reference":
+            res = bench_reference(args, d)
+        else:
+            res = bench_cgb200(args, d)
+        if d.rank == 0 and res is not None:
+            print(json.dumps(res), flush=True)
+    finally:
+        d.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,290 @@
+// Direction-optimising BFS.
+//
+// Result semantics follow the reference's BFS: level[root] = 0, a vertex's
+// level is its parent's + 1, unreachable vertices keep 999999999
+// (my_project/CGgraph/GraphDevice.cuh:224-235, device_algorithm.cuh:85-119).
+// The reference pushes with atomicMin until no value changes; this engine
+// runs level-synchronously, which reaches the same fixpoint:
+//   top-down  -- push from a vertex queue with the degree-binned expansion of
+//                push.cuh; a visited bitmap (V/32 words, L2-resident) filters
+//                before one atomicOr claims a vertex, so each vertex is
+//                written and enqueued exactly once;
+//   bottom-up -- every unvisited vertex scans its in-edges (the CSC) until it
+//                finds a parent in the frontier bitmap; one warp owns 32
+//                consecutive vertices = one bitmap word, so visited and next-
+//                frontier words are written without atomics.
+// The direction switch is Beamer's (alpha = 15, beta = 18) unless the
+// schedule says otherwise.
+#include "engine.cuh"
+#include "policy.cuh"
+#include "push.cuh"
+
+namespace cgb {
+
+struct BfsTdOp {
+    const uint32_t* __restrict__ off;
+    const uint32_t* __restrict__ dst;
+    uint32_t* level;
+    uint32_t* visited;
+    uint32_t next_level;
+    uint32_t nz;
+    uint32_t* qout;
+    uint32_t* qlen;
+    uint32_t cap;
+    DevCounters* ctr;
+
+    __device__ __forceinline__ bool load(uint32_t v, uint32_t& s, uint32_t& d, uint32_t& m) const
+    {
+        s = off[v];
+        d = off[v + 1] - s;
+        m = 0;
+        return true;
+    }
+    __device__ __forceinline__ void edge(bool valid, uint32_t e, uint32_t) const
+    {
+        bool win = false;
+        uint32_t d = 0;
+        if (valid) {
+            d = dst[e];
+            const uint32_t bit = 1u << (d & 31u);
+            uint32_t* wp = visited + (d >> 5);
+            if (!(*wp & bit)) {
+                const uint32_t old = atomicOr(wp, bit);
+                if (!(old & bit)) {
+                    win = true;
+                    level[d] = next_level;
+                }
+            }
+        }
+        const bool enq = win && d < nz;
+        uint32_t deg = 0;
+        if (enq) deg = off[d + 1] - off[d];
+        warp_append(enq, d, qout, qlen, cap, &ctr->overflow);
+        if (__any_sync(0xffffffffu, enq)) {
+            const unsigned long long s = warp_sum((unsigned long long)deg);
+            const uint32_t mx = warp_max(deg);
+            if (lane_id() == 0) {
+                atomicAdd(&ctr->medges, s);
+                atomicMax(&ctr->max_deg, mx);
+            }
+        }
+    }
+};
+
+__global__ void k_bfs_init(uint32_t V, uint32_t* level, uint32_t* visited, uint32_t words)
+{
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < V; i += stride) level[i] = kValueMax;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < words; i += stride) visited[i] = 0;
+}
+
+__global__ void k_bfs_root(uint32_t* level, uint32_t* visited, uint32_t root, uint32_t* q0)
+{
+    level[root] = 0;
+    visited[root >> 5] = 1u << (root & 31u);
+    q0[0] = root;
+}
+
+// Queue -> frontier bitmap (bitmap cleared beforehand).
+__global__ void k_q2bm(const uint32_t* __restrict__ q, uint32_t n, uint32_t* bm)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t v = q[i];
+        atomicOr(bm + (v >> 5), 1u << (v & 31u));
+    }
+}
+
+// One bottom-up level.  Reads front (current frontier bitmap), writes
+// next (all words, so it needs no clearing) and the next queue.
+__global__ void __launch_bounds__(kBlock) k_bfs_bu(uint32_t V, const uint32_t* __restrict__ in_off,
+                                                   const uint32_t* __restrict__ in_src,
+                                                   const uint32_t* __restrict__ off, uint32_t* level,
+                                                   uint32_t* visited, const uint32_t* __restrict__ front,
+                                                   uint32_t* next, uint32_t next_level, uint32_t nz, uint32_t* qout,
+                                                   uint32_t* qlen, uint32_t cap, DevCounters* ctr)
+{
+    const uint32_t words = (V + 31) / 32;
+    const uint32_t warps = gridDim.x * (blockDim.x / 32);
+    unsigned long long medges = 0;
+    uint32_t found_cnt = 0, mx = 0;
+    for (uint32_t wi = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); wi < words; wi += warps) {
+        const uint32_t vis = visited[wi];
+        const uint32_t v = wi * 32 + lane_id();
+        bool found = false;
+        if (v < V && !((vis >> lane_id()) & 1u)) {
+            const uint32_t e1 = in_off[v + 1];
+            for (uint32_t e = in_off[v]; e < e1; e++) {
+                const uint32_t u = in_src[e];
+                if ((front[u >> 5] >> (u & 31u)) & 1u) {
+                    found = true;
+                    break;
+                }
+            }
+        }
+        const uint32_t fm = __ballot_sync(0xffffffffu, found);
+        if (found) level[v] = next_level;
+        if (lane_id() == 0) {
+            next[wi] = fm;
+            if (fm) visited[wi] = vis | fm;
+        }
+        const bool enq = found && v < nz;
+        uint32_t deg = 0;
+        if (enq) deg = off[v + 1] - off[v];
+        warp_append(enq, v, qout, qlen, cap, &ctr->overflow);
+        medges += deg;
+        found_cnt += enq;
+        mx = max(mx, deg);
+    }
+    medges = warp_sum(medges);
+    found_cnt = warp_sum(found_cnt);
+    mx = warp_max(mx);
+    if (lane_id() == 0 && found_cnt) {
+        atomicAdd(&ctr->medges, medges);
+        atomicAdd(&ctr->found, found_cnt);
+        atomicMax(&ctr->max_deg, mx);
+    }
+}
+
+static void reset_level_counters(cgb_graph* g, int out)
+{
+    // qlen[out], huge_len, medges, found, max_deg
+    CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->qlen[out], 0, sizeof(uint32_t), g->stream));
+    CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->huge_len, 0, sizeof(uint32_t), g->stream));
+    CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->medges, 0, sizeof(unsigned long long), g->stream));
+    CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->found, 0, sizeof(uint32_t), g->stream));
+    CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->max_deg, 0, sizeof(uint32_t), g->stream));
+}
+
+void run_bfs(cgb_graph* g, uint32_t root, const cgb_options& o)
+{
+    ensure_frontier(g);
+    const bool want_pull = !(o.schedule == CGB_SCHED_FIXED && o.variant != CGB_VAR_PULL && o.variant != CGB_VAR_AUTO);
+    const bool force_pull = (o.schedule == CGB_SCHED_FIXED && o.variant == CGB_VAR_PULL);
+    if (want_pull) ensure_csc(g);
+    const double alpha = o.bfs_alpha > 0 ? o.bfs_alpha : 15.0;
+    const double beta = o.bfs_beta > 0 ? o.bfs_beta : 18.0;
+    const uint32_t V = g->V;
+    const uint32_t words = g->words();
+    const bool timing = g->flags & CGB_FLAG_KERNEL_TIMING;
+    const bool tracing = g->flags & CGB_FLAG_TRACE;
+
+    uint32_t host_root_deg[2];
+    CGB_CUDA_TRY(cudaMemcpyAsync(host_root_deg, g->off + root, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                 g->stream));
+    CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    CGB_CUDA_TRY(cudaEventRecord(g->ev_start, g->stream));
+    if (timing) ktimer_begin(g, CGB_K_INIT);
+    ++g->stats.launches;
+    k_bfs_init<<<kNumSMs * 4, kBlock, 0, g->stream>>>(V, g->value, g->visited, words);
+    ++g->stats.launches;
+    k_bfs_root<<<1, 1, 0, g->stream>>>(g->value, g->visited, root, g->q[0]);
+    if (timing) ktimer_end(g);
+
+    uint32_t cur = 0;  // queue holding the current frontier
+    uint64_t nf = (root < g->nz) ? 1 : 0;
+    uint64_t scout = host_root_deg[1] - host_root_deg[0];
+    int64_t edges_to_check = (int64_t)g->E;
+    uint32_t maxdeg = (uint32_t)scout;
+    uint64_t visited_cnt = 1;
+    uint32_t level = 0;
+    bool bottom_up = false;
+    uint64_t awake = 0, old_awake = 0;
+    uint32_t* front = g->front_bm;
+    uint32_t* next = g->front_bm + words;
+    uint64_t iters = 0;
+    const uint64_t max_iters = o.max_iterations ? o.max_iterations : (uint64_t)V + 2;
+    Policy* pol = (o.schedule == CGB_SCHED_LEARNED) ? policy_get() : nullptr;
+
+    while (nf > 0) {
+        CGB_REQUIRE(iters < max_iters, CGB_ETIMEOUT, "BFS iteration budget exhausted");
+        // ----- direction decision
+        bool go_pull;
+        if (force_pull) go_pull = true;
+        else if (!want_pull) go_pull = false;
+        else if (pol) {
+            float feat[kPolicyFeatures];
+            policy_features(feat, CGB_BFS, g, nf, scout, (uint64_t)V - visited_cnt,
+                            (uint64_t)std::max<int64_t>(edges_to_check, 0), maxdeg, level, bottom_up ? 1 : 0, 0);
+            int choice = policy_choose_direction(pol, feat);
+            if (choice < 0) {  // fallback: heuristic
+                choice = bottom_up ? ((awake >= old_awake || awake > V / beta) ? 1 : 0)
+                                   : ((double)scout > (double)edges_to_check / alpha ? 1 : 0);
+            }
+            go_pull = choice == 1;
+        } else if (bottom_up) {
+            go_pull = (awake >= old_awake) || ((double)awake > (double)V / beta);
+        } else {
+            go_pull = (double)scout > (double)edges_to_check / alpha;
+        }
+
+        const int out = cur ^ 1;
+        reset_level_counters(g, out);
+        float it_ms = 0.f;
+        if (tracing) CGB_CUDA_TRY(cudaEventRecord(g->ev_iter[0], g->stream));
+        if (go_pull) {
+            if (!bottom_up) {
+                // entering bottom-up: frontier queue -> bitmap
+                if (timing) ktimer_begin(g, CGB_K_FRONTIER);
+                CGB_CUDA_TRY(cudaMemsetAsync(front, 0, words * sizeof(uint32_t), g->stream));
+                ++g->stats.launches;
+                k_q2bm<<<grid_for(nf, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(g->q[cur], (uint32_t)nf, front);
+                if (timing) ktimer_end(g);
+                awake = nf;
+                old_awake = 0;
+            }
+            if (timing) ktimer_begin(g, CGB_K_PULL);
+            const uint32_t grid = grid_for((uint64_t)words * 32, kBlock, kNumSMs * 16);
+            ++g->stats.launches;
+            k_bfs_bu<<<grid, kBlock, 0, g->stream>>>(V, g->in_off, g->in_src, g->off, g->value, g->visited, front,
+                                                     next, level + 1, g->nz, g->q[out], &g->ctr->qlen[out], V,
+                                                     g->ctr);
+            if (timing) ktimer_end(g);
+            std::swap(front, next);
+            g->stats.pulls_bu++;
+        } else {
+            if (timing) ktimer_begin(g, CGB_K_PUSH);
+            BfsTdOp op{g->off, g->dst, g->value, g->visited, level + 1, g->nz, g->q[out], &g->ctr->qlen[out], V, g->ctr};
+            launch_push_twc(g, g->q[cur], (uint32_t)nf, op, false);
+            if (timing) ktimer_end(g);
+            g->stats.pushes_td++;
+        }
+        if (tracing) CGB_CUDA_TRY(cudaEventRecord(g->ev_iter[1], g->stream));
+        sync_counters(g);
+        if (tracing) {
+            CGB_CUDA_TRY(cudaEventElapsedTime(&it_ms, g->ev_iter[0], g->ev_iter[1]));
+            cgb_iter_trace t{};
+            t.iteration = (uint32_t)iters;
+            t.algorithm = CGB_BFS;
+            t.frontier_vertices = nf;
+            t.frontier_edges = scout;
+            t.unvisited_vertices = (uint64_t)V - visited_cnt;
+            t.unvisited_edges = (uint64_t)std::max<int64_t>(edges_to_check, 0);
+            t.max_frontier_degree = maxdeg;
+            t.variant = go_pull ? CGB_VAR_PULL : CGB_VAR_TWC;
+            t.ms = it_ms;
+            g->trace.push_back(t);
+        }
+        CGB_REQUIRE(!g->h_ctr->overflow, CGB_EOVERFLOW, "BFS frontier queue overflow");
+        const uint64_t n_next = g->h_ctr->qlen[out];
+        const uint64_t m_next = g->h_ctr->medges;
+        if (go_pull) {
+            old_awake = awake;
+            awake = g->h_ctr->found;
+            visited_cnt += g->h_ctr->found;
+        } else {
+            visited_cnt += n_next;  // upper bound when nz < V; only steers the policy
+        }
+        bottom_up = go_pull;
+        edges_to_check -= (int64_t)scout;
+        scout = m_next;
+        maxdeg = g->h_ctr->max_deg;
+        nf = n_next;
+        cur = out;
+        level++;
+        iters++;
+    }
+    CGB_CUDA_TRY(cudaEventRecord(g->ev_stop, g->stream));
+    g->stats.iterations = iters;
+}
+
+}  // namespace cgb

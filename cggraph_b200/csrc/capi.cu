@@ -1,0 +1,332 @@
+// C ABI of the engine (include/cgb200.h, include/cgb200_gen.h).
+#include <sys/stat.h>
+
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/cgb200.h"
+#include "../../include/cgb200_gen.h"
+#include "engine.cuh"
+
+namespace cgb {
+cgb_graph* gen_rmat(uint32_t scale, uint32_t ef, uint64_t seed, double a, double b, double c, int scr, int sym,
+                    uint32_t wmax, int device);
+cgb_graph* gen_grid(uint32_t rows, uint32_t cols, uint64_t seed, uint32_t wmax, int device);
+}  // namespace cgb
+
+using namespace cgb;
+
+template <typename F>
+static cgb_status guarded(F&& f)
+{
+    try {
+        f();
+        return CGB_OK;
+    } catch (const Error& e) {
+        set_error(e.msg);
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        set_error("host allocation failed");
+        return CGB_ENOMEM;
+    } catch (const std::exception& e) {
+        set_error(e.what());
+        return CGB_ECUDA;
+    }
+}
+
+static cgb_options effective_options(const cgb_options* o)
+{
+    cgb_options r;
+    std::memset(&r, 0, sizeof(r));
+    r.struct_size = sizeof(r);
+    if (o && o->struct_size) std::memcpy(&r, o, std::min<size_t>(o->struct_size, sizeof(r)));
+    return r;
+}
+
+// Copies n elements from a host or device buffer (direction from the pointer).
+static void copy_any(void* dst, const void* src, size_t bytes, cudaStream_t s)
+{
+    if (!bytes) return;
+    CGB_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, s));
+}
+
+extern "C" {
+
+int cgb_abi_version(void) { return CGB_ABI_VERSION; }
+
+const char* cgb_last_error_string(void) { return last_error().c_str(); }
+
+const char* cgb_status_string(cgb_status s)
+{
+    switch (s) {
+    case CGB_OK: return "ok";
+    case CGB_EINVAL: return "invalid argument";
+    case CGB_EFORMAT: return "invalid CSR";
+    case CGB_EIO: return "I/O error";
+    case CGB_ENOMEM: return "out of memory";
+    case CGB_ECUDA: return "CUDA error";
+    case CGB_ETIMEOUT: return "timeout";
+    case CGB_EOVERFLOW: return "queue overflow";
+    case CGB_EUNSUPPORTED: return "unsupported";
+    }
+    return "unknown status";
+}
+
+cgb_status cgb_graph_create(const uint32_t* offsets, const uint32_t* dest, const uint32_t* weight, uint32_t V,
+                            uint32_t E, uint32_t nz, int device, cgb_graph** out)
+{
+    return guarded([&] {
+        CGB_REQUIRE(out != nullptr, CGB_EINVAL, "out is NULL");
+        *out = nullptr;
+        CGB_REQUIRE(offsets != nullptr, CGB_EINVAL, "offsets is NULL");
+        CGB_REQUIRE(E == 0 || dest != nullptr, CGB_EINVAL, "dest is NULL");
+        CGB_REQUIRE(V >= 1, CGB_EINVAL, "V must be >= 1");
+        CGB_REQUIRE(V < 0xFFFFFFFFu && E < 0xFFFFFFFFu, CGB_EUNSUPPORTED, "V and E must be < 2^32 - 1");
+        cgb_graph* g = graph_alloc(V, E, nz, device, weight != nullptr && E > 0);
+        try {
+            copy_any(g->off, offsets, ((size_t)V + 1) * 4, g->stream);
+            copy_any(g->dst, dest, (size_t)E * 4, g->stream);
+            if (g->w) copy_any(g->w, weight, (size_t)E * 4, g->stream);
+            CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+            validate_and_sort(g);
+            compute_weight_sum(g);
+        } catch (...) {
+            graph_free(g);
+            throw;
+        }
+        *out = g;
+    });
+}
+
+static std::vector<uint32_t> load_array(const char* path, uint64_t length)
+{
+    struct stat st;
+    CGB_REQUIRE(path != nullptr, CGB_EINVAL, "path is NULL");
+    if (stat(path, &st) != 0) throw Error{CGB_EIO, std::string("Bin File [") + path + "] Not Exist"};
+    if ((uint64_t)st.st_size != length * 4)
+        throw Error{CGB_EIO, std::string("(total_bytes / utilSize != length) for ") + path};
+    std::vector<uint32_t> a(length);
+    FILE* f = std::fopen(path, "rb");
+    if (!f) throw Error{CGB_EIO, std::string("cannot open ") + path};
+    size_t got = length ? std::fread(a.data(), 4, length, f) : 0;
+    std::fclose(f);
+    if (got != length) throw Error{CGB_EIO, std::string("short read on ") + path};
+    return a;
+}
+
+cgb_status cgb_graph_load_files(const char* off_path, const char* dst_path, const char* w_path, uint32_t V,
+                                uint32_t E, int device, cgb_graph** out)
+{
+    cgb_status st = CGB_OK;
+    std::vector<uint32_t> off, dst, w;
+    cgb_status ls = guarded([&] {
+        CGB_REQUIRE(out != nullptr, CGB_EINVAL, "out is NULL");
+        *out = nullptr;
+        off = load_array(off_path, (uint64_t)V + 1);
+        dst = load_array(dst_path, E);
+        if (w_path) w = load_array(w_path, E);
+    });
+    if (ls != CGB_OK) return ls;
+    st = cgb_graph_create(off.data(), dst.data(), w_path ? w.data() : nullptr, V, E, 0, device, out);
+    return st;
+}
+
+cgb_status cgb_graph_destroy(cgb_graph* g)
+{
+    return guarded([&] { graph_free(g); });
+}
+
+cgb_status cgb_graph_set_stream(cgb_graph* g, void* stream)
+{
+    return guarded([&] {
+        CGB_REQUIRE(g != nullptr, CGB_EINVAL, "graph is NULL");
+        std::lock_guard<std::mutex> lock(g->mu);
+        CGB_CUDA_TRY(cudaSetDevice(g->device));
+        CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        g->stream = stream ? (cudaStream_t)stream : g->own_stream;
+    });
+}
+
+cgb_status cgb_graph_info(const cgb_graph* g, uint32_t* V, uint32_t* E, int32_t* symmetric)
+{
+    return guarded([&] {
+        CGB_REQUIRE(g != nullptr, CGB_EINVAL, "graph is NULL");
+        if (V) *V = g->V;
+        if (E) *E = g->E;
+        if (symmetric) *symmetric = g->symmetric;
+    });
+}
+
+cgb_status cgb_graph_device_csr(const cgb_graph* g, const uint32_t** offsets, const uint32_t** dest,
+                                const uint32_t** weight)
+{
+    return guarded([&] {
+        CGB_REQUIRE(g != nullptr, CGB_EINVAL, "graph is NULL");
+        if (offsets) *offsets = g->off;
+        if (dest) *dest = g->dst;
+        if (weight) *weight = g->w;
+    });
+}
+
+cgb_status cgb_graph_result_device(const cgb_graph* g, const void** values)
+{
+    return guarded([&] {
+        CGB_REQUIRE(g != nullptr && values != nullptr, CGB_EINVAL, "NULL argument");
+        CGB_REQUIRE(g->result != nullptr, CGB_EINVAL, "no run has completed on this graph");
+        *values = g->result;
+    });
+}
+
+cgb_status cgb_graph_result_download(const cgb_graph* g, void* values)
+{
+    return guarded([&] {
+        CGB_REQUIRE(g != nullptr && values != nullptr, CGB_EINVAL, "NULL argument");
+        CGB_REQUIRE(g->result != nullptr, CGB_EINVAL, "no run has completed on this graph");
+        CGB_CUDA_TRY(cudaSetDevice(g->device));
+        const size_t bytes = (size_t)g->V * (g->result_alg == CGB_PR ? 8 : 4);
+        copy_any(values, g->result, bytes, g->stream);
+        CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    });
+}
+
+static void run_one(cgb_graph* g, int alg, uint32_t root_or_iters, const cgb_options& o)
+{
+    g->stats = cgb_run_stats{};
+    g->trace.clear();
+    g->flags = o.flags;
+    g->kev_class.clear();
+    g->kev_used = 0;
+    g->result = nullptr;
+    CGB_CUDA_TRY(cudaMemsetAsync(g->ctr, 0, sizeof(DevCounters), g->stream));
+    switch (alg) {
+    case CGB_BFS:
+        run_bfs(g, root_or_iters, o);
+        break;
+    case CGB_SSSP:
+        run_sssp(g, root_or_iters, o);
+        break;
+    case CGB_CC:
+        run_cc(g, o);
+        break;
+    case CGB_PR:
+        run_pr(g, root_or_iters, o);
+        break;
+    }
+    CGB_CUDA_TRY(cudaEventSynchronize(g->ev_stop));
+    CGB_CUDA_TRY(cudaGetLastError());
+    float ms = 0.f;
+    CGB_CUDA_TRY(cudaEventElapsedTime(&ms, g->ev_start, g->ev_stop));
+    g->stats.ms = ms;
+    if (o.flags & CGB_FLAG_KERNEL_TIMING) ktimer_collect(g);
+    const uint64_t V = g->V, E = g->E;
+    if (alg == CGB_BFS || alg == CGB_SSSP) {
+        count_reached(g);
+        const uint64_t per_edge = alg == CGB_BFS ? 8 : (g->w ? 12 : 8);
+        g->stats.alg_bytes = per_edge * g->stats.traversed_edges + 12 * V;
+    } else if (alg == CGB_CC) {
+        g->stats.traversed_edges = E;
+        g->stats.reached = V;
+        g->stats.alg_bytes = 8 * E + 20 * V;
+    } else {
+        g->stats.traversed_edges = E * g->stats.iterations;
+        g->stats.reached = V;
+        g->stats.alg_bytes = (12 * E + 20 * V + 4) * g->stats.iterations;
+    }
+    if (alg != CGB_PR) g->result = g->value;
+    g->result_alg = alg;
+}
+
+cgb_status cgb_run(cgb_graph* g, int algorithm, uint32_t root_or_iters, const cgb_options* opt, uint32_t* out_u32,
+                   double* out_f64, double* out_ms)
+{
+    return guarded([&] {
+        CGB_REQUIRE(g != nullptr, CGB_EINVAL, "graph is NULL");
+        CGB_REQUIRE(algorithm >= CGB_BFS && algorithm <= CGB_PR, CGB_EINVAL, "unknown Algorithm_type");
+        if (algorithm == CGB_BFS || algorithm == CGB_SSSP)
+            CGB_REQUIRE(root_or_iters < g->V, CGB_EINVAL, "root >= vertexNum");
+        const cgb_options o = effective_options(opt);
+        std::lock_guard<std::mutex> lock(g->mu);
+        CGB_CUDA_TRY(cudaSetDevice(g->device));
+        run_one(g, algorithm, root_or_iters, o);
+        if (algorithm == CGB_PR) {
+            if (out_f64) copy_any(out_f64, g->result, (size_t)g->V * 8, g->stream);
+        } else if (out_u32) {
+            copy_any(out_u32, g->result, (size_t)g->V * 4, g->stream);
+        }
+        CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        if (out_ms) *out_ms = g->stats.ms;
+    });
+}
+
+cgb_status cgb_run_batch(cgb_graph* g, int algorithm, const uint32_t* roots, uint32_t nroots, const cgb_options* opt,
+                         uint32_t* out_u32, double* out_ms)
+{
+    return guarded([&] {
+        CGB_REQUIRE(g != nullptr && roots != nullptr, CGB_EINVAL, "NULL argument");
+        CGB_REQUIRE(algorithm == CGB_BFS || algorithm == CGB_SSSP, CGB_EINVAL, "batch runs are BFS or SSSP");
+        for (uint32_t i = 0; i < nroots; i++) CGB_REQUIRE(roots[i] < g->V, CGB_EINVAL, "root >= vertexNum");
+        const cgb_options o = effective_options(opt);
+        std::lock_guard<std::mutex> lock(g->mu);
+        CGB_CUDA_TRY(cudaSetDevice(g->device));
+        double total = 0;
+        for (uint32_t i = 0; i < nroots; i++) {
+            run_one(g, algorithm, roots[i], o);
+            total += g->stats.ms;
+            if (out_u32) copy_any(out_u32 + (size_t)i * g->V, g->result, (size_t)g->V * 4, g->stream);
+        }
+        CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        if (out_ms) *out_ms = total;
+    });
+}
+
+cgb_status cgb_run_stats_get(const cgb_graph* g, cgb_run_stats* out)
+{
+    return guarded([&] {
+        CGB_REQUIRE(g != nullptr && out != nullptr, CGB_EINVAL, "NULL argument");
+        *out = g->stats;
+    });
+}
+
+cgb_status cgb_trace_get(const cgb_graph* g, cgb_iter_trace* out, uint32_t max_entries, uint32_t* count)
+{
+    return guarded([&] {
+        CGB_REQUIRE(g != nullptr, CGB_EINVAL, "graph is NULL");
+        if (count) *count = (uint32_t)g->trace.size();
+        if (out)
+            for (uint32_t i = 0; i < max_entries && i < g->trace.size(); i++) out[i] = g->trace[i];
+    });
+}
+
+cgb_status cgb_gen_rmat(uint32_t scale, uint32_t edge_factor, uint64_t seed, double a, double b, double c,
+                        int scramble, int symmetrise, uint32_t wmax, int device, cgb_graph** out)
+{
+    return guarded([&] {
+        CGB_REQUIRE(out != nullptr, CGB_EINVAL, "out is NULL");
+        *out = gen_rmat(scale, edge_factor, seed, a, b, c, scramble, symmetrise, wmax, device);
+    });
+}
+
+cgb_status cgb_gen_grid(uint32_t rows, uint32_t cols, uint64_t seed, uint32_t wmax, int device, cgb_graph** out)
+{
+    return guarded([&] {
+        CGB_REQUIRE(out != nullptr, CGB_EINVAL, "out is NULL");
+        *out = gen_grid(rows, cols, seed, wmax, device);
+    });
+}
+
+cgb_status cgb_graph_download(const cgb_graph* g, uint32_t* offsets, uint32_t* dest, uint32_t* weight)
+{
+    return guarded([&] {
+        CGB_REQUIRE(g != nullptr, CGB_EINVAL, "graph is NULL");
+        CGB_CUDA_TRY(cudaSetDevice(g->device));
+        if (offsets) copy_any(offsets, g->off, ((size_t)g->V + 1) * 4, g->stream);
+        if (dest) copy_any(dest, g->dst, (size_t)g->E * 4, g->stream);
+        if (weight && g->w) copy_any(weight, g->w, (size_t)g->E * 4, g->stream);
+        CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    });
+}
+
+}  // extern "C"

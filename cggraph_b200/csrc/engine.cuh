@@ -1,0 +1,117 @@
+// Internal state of a resident graph and the per-algorithm drivers.
+#pragma once
+
+#include <algorithm>
+#include <mutex>
+#include <vector>
+
+#include "common.cuh"
+
+// Device counters shared by the frontier kernels of one graph.
+struct DevCounters {
+    uint32_t qlen[2];         // lengths of the two alternating vertex queues
+    uint32_t huge_len;        // vertices deferred to the split-hub kernel
+    uint32_t far_len[2];      // SSSP far piles
+    uint32_t overflow;        // a queue ran out of capacity
+    uint32_t link_giveup;     // a CC link loop hit its retry bound
+    uint32_t found;           // BFS bottom-up: vertices found this level
+    unsigned long long medges;    // sum of out-degrees of the next frontier
+    unsigned long long reached_edges;
+    uint32_t reached;
+    uint32_t min_far;         // SSSP: smallest distance left in the far pile
+    uint32_t max_deg;         // max degree of the next frontier
+    uint32_t pad[3];
+};
+
+struct cgb_graph {
+    int device = 0;
+    uint32_t V = 0, E = 0, nz = 0;  // nz = noZeroOutDegreeNum
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    std::mutex mu;
+
+    // CSR (always resident)
+    uint32_t* off = nullptr;
+    uint32_t* dst = nullptr;
+    uint32_t* w = nullptr;  // may be null: unit weights
+    uint64_t sum_w = 0;     // sum of weights (delta heuristic)
+
+    // in-edge CSC (built on first need; aliases the CSR when symmetric)
+    uint32_t* in_off = nullptr;
+    uint32_t* in_src = nullptr;
+    bool csc_owned = false;
+    int symmetric = -1;
+
+    // PageRank: in-rows with in-degree >= kPrHuge
+    uint32_t* pr_huge_rows = nullptr;
+    uint32_t n_pr_huge = 0;
+    bool pr_ready = false;
+
+    // results / algorithm state
+    uint32_t* value = nullptr;  // uint32[V]
+    double* pr[2] = {nullptr, nullptr};
+    double* contrib[2] = {nullptr, nullptr};
+    const void* result = nullptr;
+    int result_alg = -1;
+
+    // frontier workspace
+    uint32_t* q[2] = {nullptr, nullptr};  // capacity V each
+    uint32_t* huge_q = nullptr;           // capacity V
+    uint32_t* visited = nullptr;          // bitmap, words = V/32 + 1
+    uint32_t* front_bm = nullptr;
+    uint32_t* stamp = nullptr;            // uint32[V]
+    uint2* far[2] = {nullptr, nullptr};
+    uint32_t far_cap = 0;
+    uint32_t* sample = nullptr;           // CC sampling buffer
+
+    DevCounters* ctr = nullptr;       // device
+    DevCounters* h_ctr = nullptr;     // pinned host mirror
+
+    cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+    cudaEvent_t ev_iter[2] = {nullptr, nullptr};
+    std::vector<cudaEvent_t> kev;     // per-launch timing events (pairs)
+    size_t kev_used = 0;
+    std::vector<int> kev_class;
+
+    cgb_run_stats stats{};
+    std::vector<cgb_iter_trace> trace;
+    uint32_t flags = 0;
+
+    uint32_t words() const { return V / 32 + 1; }
+};
+
+namespace cgb {
+
+constexpr uint32_t kPrHuge = 8192;   // PageRank rows handled by a whole CTA
+constexpr uint32_t kHugeDeg = 16384; // push: hubs split across CTAs
+constexpr uint32_t kCtaDeg = 1024;   // push: CTA-per-vertex tier
+constexpr uint32_t kHugeChunk = 4096;
+
+// graph lifetime and preparation (graph.cu)
+cgb_graph* graph_alloc(uint32_t V, uint32_t E, uint32_t nz, int device, bool with_weight);
+void graph_free(cgb_graph* g);
+void validate_and_sort(cgb_graph* g);
+void compute_weight_sum(cgb_graph* g);
+uint32_t sssp_default_delta(const cgb_graph* g);
+
+// workspace management (graph.cu)
+void ensure_frontier(cgb_graph* g);
+void ensure_sssp(cgb_graph* g);
+void ensure_csc(cgb_graph* g);
+void ensure_symmetry_known(cgb_graph* g);
+void ensure_pr(cgb_graph* g);
+void sync_counters(cgb_graph* g);
+
+// timing helpers (graph.cu)
+void ktimer_begin(cgb_graph* g, int cls);
+void ktimer_end(cgb_graph* g);
+void ktimer_collect(cgb_graph* g);
+
+// drivers
+void run_bfs(cgb_graph* g, uint32_t root, const cgb_options& o);
+void run_sssp(cgb_graph* g, uint32_t root, const cgb_options& o);
+void run_cc(cgb_graph* g, const cgb_options& o);
+void run_pr(cgb_graph* g, uint32_t iters, const cgb_options& o);
+void count_reached(cgb_graph* g);  // fills stats.reached / traversed_edges for BFS/SSSP
+
+}  // namespace cgb

@@ -1,0 +1,218 @@
+// Seeded synthetic graphs built directly in HBM (RMAT, 2-D grid).
+// The arithmetic mirrors the oracle's CPU twin exactly (integer quadrant
+// thresholds, splitmix64 counters), so both build the same CSR.
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+#include <cub/device/device_select.cuh>
+
+#include "../../include/cgb200_gen.h"
+#include "engine.cuh"
+
+namespace cgb {
+
+__device__ __forceinline__ uint32_t scramble_id(uint64_t x, uint32_t scale, uint64_t m1, uint64_t m2, uint64_t c)
+{
+    const uint64_t mask = (scale >= 64) ? ~0ull : ((1ull << scale) - 1);
+    const uint32_t sh = scale / 2 ? scale / 2 : 1;
+    x = (x * m1) & mask;
+    x ^= x >> sh;
+    x = (x * m2 + c) & mask;
+    return (uint32_t)x;
+}
+
+constexpr uint64_t kSentinel = ~0ull;
+
+__global__ void k_rmat_keys(uint32_t scale, uint64_t n, uint64_t s, uint64_t t1, uint64_t t2, uint64_t t3, int scr,
+                            uint64_t m1, uint64_t m2, uint64_t c, int sym, uint64_t* keys)
+{
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t u = 0, v = 0;
+        for (uint32_t l = 0; l < scale; l++) {
+            const uint64_t r = mix64(s ^ mix64(i * 64 + l)) >> 32;
+            const uint64_t bu = r >= t2;
+            const uint64_t bv = (r >= t1 && r < t2) || r >= t3;
+            u = (u << 1) | bu;
+            v = (v << 1) | bv;
+        }
+        if (scr) {
+            u = scramble_id(u, scale, m1, m2, c);
+            v = scramble_id(v, scale, m1, m2, c);
+        }
+        const bool loop = u == v;
+        keys[i] = loop ? kSentinel : ((u << 32) | v);
+        if (sym) keys[n + i] = loop ? kSentinel : ((v << 32) | u);
+    }
+}
+
+__global__ void k_keys_to_csr(uint32_t V, uint64_t m, const uint64_t* __restrict__ keys, uint32_t* off, uint32_t* dst)
+{
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e <= m; e += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t hi = e < m ? (keys[e] >> 32) : V;
+        const uint64_t lo = e == 0 ? 0 : (keys[e - 1] >> 32) + 1;
+        for (uint64_t v = lo; v <= hi; v++) off[v] = (uint32_t)e;
+        if (e < m) dst[e] = (uint32_t)keys[e];
+    }
+}
+
+__device__ __forceinline__ uint32_t src_of(const uint32_t* __restrict__ off, uint32_t V, uint32_t e)
+{
+    uint32_t lo = 0, hi = V;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (off[mid] <= e) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void k_edge_weights(uint32_t V, uint32_t E, const uint32_t* __restrict__ off,
+                               const uint32_t* __restrict__ dst, uint64_t s, uint32_t wmax, int sym_key, uint32_t* w)
+{
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x) {
+        uint32_t a = src_of(off, V, e), b = dst[e];
+        if (sym_key && b < a) {
+            const uint32_t t = a;
+            a = b;
+            b = t;
+        }
+        const uint64_t h = mix64(s ^ (((uint64_t)a << 32) | b));
+        w[e] = 1u + (uint32_t)(h % wmax);
+    }
+}
+
+__global__ void k_grid_deg(uint32_t rows, uint32_t cols, uint32_t* deg)
+{
+    const uint64_t V = (uint64_t)rows * cols;
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t r = (uint32_t)(v / cols), c = (uint32_t)(v % cols);
+        deg[v] = (r > 0) + (c > 0) + (c + 1 < cols) + (r + 1 < rows);
+    }
+}
+
+__global__ void k_grid_fill(uint32_t rows, uint32_t cols, const uint32_t* __restrict__ off, uint32_t* dst)
+{
+    const uint64_t V = (uint64_t)rows * cols;
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t r = (uint32_t)(v / cols), c = (uint32_t)(v % cols);
+        uint32_t e = off[v];
+        const uint32_t x = (uint32_t)v;
+        if (r > 0) dst[e++] = x - cols;
+        if (c > 0) dst[e++] = x - 1;
+        if (c + 1 < cols) dst[e++] = x + 1;
+        if (r + 1 < rows) dst[e++] = x + cols;
+    }
+}
+
+static void* galloc(size_t bytes)
+{
+    void* p = nullptr;
+    CGB_CUDA_TRY(cudaMalloc(&p, bytes ? bytes : 1));
+    return p;
+}
+
+cgb_graph* gen_rmat(uint32_t scale, uint32_t ef, uint64_t seed, double a, double b, double c, int scr, int sym,
+                    uint32_t wmax, int device)
+{
+    CGB_REQUIRE(scale >= 1 && scale <= 31, CGB_EINVAL, "RMAT scale must be in [1, 31]");
+    CGB_REQUIRE(a >= 0 && b >= 0 && c >= 0 && a + b + c <= 1.0, CGB_EINVAL, "bad RMAT probabilities");
+    CGB_CUDA_TRY(cudaSetDevice(device));
+    const uint32_t V = 1u << scale;
+    const uint64_t n = (uint64_t)ef << scale;
+    const uint64_t total = sym ? 2 * n : n;
+    const uint64_t t1 = (uint64_t)(a * 4294967296.0);
+    const uint64_t t2 = (uint64_t)((a + b) * 4294967296.0);
+    const uint64_t t3 = (uint64_t)((a + b + c) * 4294967296.0);
+    const uint64_t m1 = mix64(seed ^ 0x5C0A11ull) | 1ull;
+    const uint64_t m2 = mix64(seed ^ 0x5C0A12ull) | 1ull;
+    const uint64_t cc = mix64(seed ^ 0x5C0A13ull);
+    cudaStream_t st;
+    CGB_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    uint64_t* keys = (uint64_t*)galloc(total * 8);
+    uint64_t* alt = (uint64_t*)galloc(total * 8);
+    uint64_t* cnt = (uint64_t*)galloc(8);
+    void* temp = nullptr;
+    cgb_graph* g = nullptr;
+    try {
+        k_rmat_keys<<<kNumSMs * 16, kBlock, 0, st>>>(scale, n, mix64(seed), t1, t2, t3, scr, m1, m2, cc, sym, keys);
+        cub::DoubleBuffer<uint64_t> db(keys, alt);
+        size_t tb = 0, tb2 = 0;
+        CGB_CUDA_TRY(cub::DeviceRadixSort::SortKeys(nullptr, tb, db, total, 0, 32 + (int)scale, st));
+        uint64_t* in_unique = nullptr;
+        CGB_CUDA_TRY(cub::DeviceSelect::Unique(nullptr, tb2, keys, alt, cnt, total, st));
+        temp = galloc(std::max(tb, tb2));
+        CGB_CUDA_TRY(cub::DeviceRadixSort::SortKeys(temp, tb, db, total, 0, 32 + (int)scale, st));
+        in_unique = db.Current();
+        uint64_t* out_unique = db.Alternate();
+        CGB_CUDA_TRY(cub::DeviceSelect::Unique(temp, tb2, in_unique, out_unique, cnt, total, st));
+        uint64_t m = 0, last = 0;
+        CGB_CUDA_TRY(cudaMemcpyAsync(&m, cnt, 8, cudaMemcpyDeviceToHost, st));
+        CGB_CUDA_TRY(cudaStreamSynchronize(st));
+        if (m) {
+            CGB_CUDA_TRY(cudaMemcpyAsync(&last, out_unique + m - 1, 8, cudaMemcpyDeviceToHost, st));
+            CGB_CUDA_TRY(cudaStreamSynchronize(st));
+            if (last == kSentinel) m--;
+        }
+        CGB_REQUIRE(m < 0xFFFFFFFFull, CGB_EUNSUPPORTED, "RMAT graph has >= 2^32 edges");
+        g = graph_alloc(V, (uint32_t)m, V, device, wmax > 0);
+        k_keys_to_csr<<<kNumSMs * 16, kBlock, 0, st>>>(V, m, out_unique, g->off, g->dst);
+        if (wmax)
+            k_edge_weights<<<kNumSMs * 16, kBlock, 0, st>>>(V, (uint32_t)m, g->off, g->dst, mix64(seed ^ 0x77E16ull),
+                                                            wmax, sym, g->w);
+        CGB_CUDA_TRY(cudaStreamSynchronize(st));
+        if (sym) g->symmetric = 1;
+    } catch (...) {
+        cudaFree(keys);
+        cudaFree(alt);
+        cudaFree(cnt);
+        if (temp) cudaFree(temp);
+        cudaStreamDestroy(st);
+        if (g) graph_free(g);
+        throw;
+    }
+    cudaFree(keys);
+    cudaFree(alt);
+    cudaFree(cnt);
+    cudaFree(temp);
+    cudaStreamDestroy(st);
+    compute_weight_sum(g);
+    return g;
+}
+
+cgb_graph* gen_grid(uint32_t rows, uint32_t cols, uint64_t seed, uint32_t wmax, int device)
+{
+    const uint64_t V64 = (uint64_t)rows * cols;
+    CGB_REQUIRE(rows >= 1 && cols >= 1 && V64 < 0xFFFFFFFFull, CGB_EINVAL, "bad grid size");
+    const uint64_t E64 = 4 * V64 - 2ull * rows - 2ull * cols;
+    CGB_REQUIRE(E64 < 0xFFFFFFFFull, CGB_EUNSUPPORTED, "grid has >= 2^32 edges");
+    const uint32_t V = (uint32_t)V64, E = (uint32_t)E64;
+    CGB_CUDA_TRY(cudaSetDevice(device));
+    cgb_graph* g = graph_alloc(V, E, V, device, wmax > 0);
+    uint32_t* deg = nullptr;
+    void* temp = nullptr;
+    try {
+        deg = (uint32_t*)galloc(((size_t)V + 1) * 4);
+        k_grid_deg<<<kNumSMs * 8, kBlock, 0, g->stream>>>(rows, cols, deg);
+        CGB_CUDA_TRY(cudaMemsetAsync(deg + V, 0, 4, g->stream));
+        size_t tb = 0;
+        CGB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb, deg, g->off, (uint64_t)V + 1, g->stream));
+        temp = galloc(tb);
+        CGB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(temp, tb, deg, g->off, (uint64_t)V + 1, g->stream));
+        k_grid_fill<<<kNumSMs * 8, kBlock, 0, g->stream>>>(rows, cols, g->off, g->dst);
+        if (wmax)
+            k_edge_weights<<<kNumSMs * 16, kBlock, 0, g->stream>>>(V, E, g->off, g->dst, mix64(seed ^ 0x77E16ull), wmax,
+                                                                   1, g->w);
+        CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    } catch (...) {
+        if (deg) cudaFree(deg);
+        if (temp) cudaFree(temp);
+        graph_free(g);
+        throw;
+    }
+    cudaFree(deg);
+    cudaFree(temp);
+    g->symmetric = 1;
+    compute_weight_sum(g);
+    return g;
+}
+
+}  // namespace cgb

@@ -1,0 +1,493 @@
+// Resident graph: upload, validation, neighbour sort, in-edge CSC, symmetry
+// check, workspaces and kernel timers.
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
+#include <vector>
+
+#include "engine.cuh"
+
+namespace cgb {
+
+// ------------------------------------------------------------------ errors
+static thread_local std::string t_last_error;
+void set_error(const std::string& msg) { t_last_error = msg; }
+const std::string& last_error() { return t_last_error; }
+
+// --------------------------------------------------------------- allocation
+template <typename T>
+static T* dalloc(size_t n)
+{
+    void* p = nullptr;
+    if (n == 0) n = 1;
+    CGB_CUDA_TRY(cudaMalloc(&p, n * sizeof(T)));
+    return (T*)p;
+}
+
+static void dfree(void* p)
+{
+    if (p) cudaFree(p);
+}
+
+static uint32_t bits_for(uint64_t n)  // bits to represent values < n
+{
+    uint32_t b = 1;
+    while (b < 64 && (1ull << b) < n) b++;
+    return b;
+}
+
+// ------------------------------------------------------------- validation
+__global__ void k_check_offsets(uint32_t V, uint32_t E, const uint32_t* __restrict__ off, uint32_t* bad)
+{
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+        if (off[v] > off[v + 1]) atomicOr(bad, 1u);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (off[0] != 0) atomicOr(bad, 2u);
+        if (off[V] != E) atomicOr(bad, 4u);
+    }
+}
+
+// Marks the first edge of every non-empty neighbour list in a bitmap over
+// edge indices (E/32 + 1 words).
+__global__ void k_mark_heads(uint32_t V, const uint32_t* __restrict__ off, uint32_t* heads)
+{
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+        const uint32_t s = off[v];
+        if (off[v + 1] > s) atomicOr(heads + (s >> 5), 1u << (s & 31u));
+    }
+}
+
+// bad |= 8 for an id >= V; unsorted |= 1 where a list is not strictly
+// ascending; dup |= 1 where it has equal neighbours.
+__global__ void k_check_edges(uint32_t V, uint32_t E, const uint32_t* __restrict__ dst,
+                              const uint32_t* __restrict__ heads, uint32_t* flags)
+{
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x) {
+        const uint32_t d = dst[e];
+        if (d >= V) atomicOr(flags, 8u);
+        if (e + 1 < E && !((heads[(e + 1) >> 5] >> ((e + 1) & 31u)) & 1u)) {
+            const uint32_t d2 = dst[e + 1];
+            if (d > d2) atomicOr(flags + 1, 1u);
+            else if (d == d2) atomicOr(flags + 2, 1u);
+        }
+    }
+}
+
+// Source vertex of edge e: last v with off[v] <= e (skipping empty lists).
+__device__ __forceinline__ uint32_t edge_source(const uint32_t* __restrict__ off, uint32_t V, uint32_t e)
+{
+    uint32_t lo = 0, hi = V;  // invariant: off[lo] <= e < off[hi]
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (off[mid] <= e) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// key = src << b | dst (b = bits for V)
+__global__ void k_make_keys(uint32_t V, uint32_t E, const uint32_t* __restrict__ off,
+                            const uint32_t* __restrict__ dst, uint32_t b, uint64_t* keys, bool dst_major)
+{
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x) {
+        const uint64_t s = edge_source(off, V, e);
+        const uint64_t d = dst[e];
+        keys[e] = dst_major ? ((d << b) | s) : ((s << b) | d);
+    }
+}
+
+__global__ void k_split_keys(uint32_t E, const uint64_t* __restrict__ keys, uint32_t b, uint32_t* low)
+{
+    const uint64_t mask = (1ull << b) - 1;
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x)
+        low[e] = (uint32_t)(keys[e] & mask);
+}
+
+// Offsets from keys sorted by their high part h(e) = keys[e] >> b, with
+// h(n) = V as sentinel: off[v] = min{e : h(e) >= v}, i.e. edge e writes
+// off[v] for h(e-1) < v <= h(e).
+__global__ void k_offsets_from_keys(uint32_t V, uint64_t n, const uint64_t* __restrict__ keys, uint32_t b,
+                                    uint32_t* off)
+{
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e <= n; e += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t hi = e < n ? (keys[e] >> b) : V;
+        const uint64_t lo = e == 0 ? 0 : (keys[e - 1] >> b) + 1;
+        for (uint64_t v = lo; v <= hi; v++) off[v] = (uint32_t)e;
+    }
+}
+
+__global__ void k_widen(uint32_t n, const uint32_t* __restrict__ a, uint64_t* o)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) o[i] = a[i];
+}
+
+__global__ void k_narrow(uint32_t n, const uint64_t* __restrict__ a, uint32_t* o)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) o[i] = (uint32_t)a[i];
+}
+
+__global__ void k_sum_u32(uint32_t n, const uint32_t* __restrict__ a, unsigned long long* out)
+{
+    unsigned long long s = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += a[i];
+    s = warp_sum(s);
+    if (lane_id() == 0 && s) atomicAdd(out, s);
+}
+
+// For every edge u->v, is v->u present?  (binary search in v's sorted list)
+__global__ void k_check_symmetric(uint32_t V, uint32_t E, const uint32_t* __restrict__ off,
+                                  const uint32_t* __restrict__ dst, uint32_t* asym)
+{
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x) {
+        if ((e & 1023u) == 0 && *(volatile uint32_t*)asym) return;
+        const uint32_t u = edge_source(off, V, e);
+        const uint32_t v = dst[e];
+        uint32_t lo = off[v], hi = off[v + 1];
+        bool found = false;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            const uint32_t x = dst[mid];
+            if (x == u) {
+                found = true;
+                break;
+            }
+            if (x < u) lo = mid + 1;
+            else hi = mid;
+        }
+        if (!found) atomicOr(asym, 1u);
+    }
+}
+
+__global__ void k_collect_heavy_rows(uint32_t V, const uint32_t* __restrict__ in_off, uint32_t th, uint32_t* rows,
+                                     uint32_t* n)
+{
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+        if (in_off[v + 1] - in_off[v] >= th) rows[atomicAdd(n, 1u)] = v;
+    }
+}
+
+__global__ void k_count_reached(uint32_t V, const uint32_t* __restrict__ value, const uint32_t* __restrict__ off,
+                                DevCounters* ctr)
+{
+    unsigned long long edges = 0;
+    uint32_t cnt = 0;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+        if (value[v] != kValueMax) {
+            cnt++;
+            edges += off[v + 1] - off[v];
+        }
+    }
+    edges = warp_sum(edges);
+    cnt = warp_sum(cnt);
+    if (lane_id() == 0 && cnt) {
+        atomicAdd(&ctr->reached_edges, edges);
+        atomicAdd(&ctr->reached, cnt);
+    }
+}
+
+// -------------------------------------------------------------- graph ops
+void sync_counters(cgb_graph* g)
+{
+    CGB_CUDA_TRY(cudaMemcpyAsync(g->h_ctr, g->ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, g->stream));
+    CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+}
+
+static void radix_sort_u64(cgb_graph* g, uint64_t*& keys, uint64_t*& alt, uint64_t n, int end_bit)
+{
+    cub::DoubleBuffer<uint64_t> db(keys, alt);
+    size_t temp_bytes = 0;
+    CGB_CUDA_TRY(cub::DeviceRadixSort::SortKeys(nullptr, temp_bytes, db, n, 0, end_bit, g->stream));
+    void* temp = dalloc<char>(temp_bytes);
+    cudaError_t err = cub::DeviceRadixSort::SortKeys(temp, temp_bytes, db, n, 0, end_bit, g->stream);
+    CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    dfree(temp);
+    CGB_CUDA_TRY(err);
+    if (db.Current() != keys) std::swap(keys, alt);
+}
+
+// Sorts every neighbour list by destination, weights following
+// (nbrSort_taskSteal, my_project/CGgraph/sortNbr.hpp:8-99).
+static void sort_neighbours(cgb_graph* g)
+{
+    const uint32_t V = g->V, E = g->E;
+    const uint32_t b = bits_for(V);
+    uint64_t* keys = dalloc<uint64_t>(E);
+    uint64_t* alt = dalloc<uint64_t>(E);
+    const uint32_t grid = grid_for(E, kBlock, kNumSMs * 16);
+    if (g->w) {
+        uint64_t* vals = dalloc<uint64_t>(E);
+        uint64_t* valt = dalloc<uint64_t>(E);
+        k_make_keys<<<grid, kBlock, 0, g->stream>>>(V, E, g->off, g->dst, b, keys, false);
+        k_widen<<<grid, kBlock, 0, g->stream>>>(E, g->w, vals);
+        cub::DoubleBuffer<uint64_t> kb(keys, alt), vb(vals, valt);
+        size_t temp_bytes = 0;
+        CGB_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, kb, vb, (uint64_t)E, 0, 2 * b, g->stream));
+        void* temp = dalloc<char>(temp_bytes);
+        cudaError_t err = cub::DeviceRadixSort::SortPairs(temp, temp_bytes, kb, vb, (uint64_t)E, 0, 2 * b, g->stream);
+        CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        dfree(temp);
+        CGB_CUDA_TRY(err);
+        k_split_keys<<<grid, kBlock, 0, g->stream>>>(E, kb.Current(), b, g->dst);
+        k_narrow<<<grid, kBlock, 0, g->stream>>>(E, vb.Current(), g->w);
+        CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        dfree(vals);
+        dfree(valt);
+    } else {
+        k_make_keys<<<grid, kBlock, 0, g->stream>>>(V, E, g->off, g->dst, b, keys, false);
+        radix_sort_u64(g, keys, alt, E, 2 * b);
+        k_split_keys<<<grid, kBlock, 0, g->stream>>>(E, keys, b, g->dst);
+        CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    }
+    dfree(keys);
+    dfree(alt);
+}
+
+void validate_and_sort(cgb_graph* g)
+{
+    const uint32_t V = g->V, E = g->E;
+    uint32_t* flags = dalloc<uint32_t>(4);
+    CGB_CUDA_TRY(cudaMemsetAsync(flags, 0, 4 * sizeof(uint32_t), g->stream));
+    k_check_offsets<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, E, g->off, flags);
+    uint32_t h[4];
+    CGB_CUDA_TRY(cudaMemcpyAsync(h, flags, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
+    CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    if (h[0]) {
+        dfree(flags);
+        if (h[0] & 2u) throw Error{CGB_EFORMAT, "csr_offset[0] != 0"};
+        if (h[0] & 4u) throw Error{CGB_EFORMAT, "csr_offset[V] != E"};
+        throw Error{CGB_EFORMAT, "csr_offset is not non-decreasing"};
+    }
+    if (E == 0) {
+        dfree(flags);
+        return;
+    }
+    const uint32_t hw = E / 32 + 2;
+    uint32_t* heads = dalloc<uint32_t>(hw);
+    for (int pass = 0; pass < 2; pass++) {
+        CGB_CUDA_TRY(cudaMemsetAsync(heads, 0, hw * sizeof(uint32_t), g->stream));
+        CGB_CUDA_TRY(cudaMemsetAsync(flags, 0, 4 * sizeof(uint32_t), g->stream));
+        k_mark_heads<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, g->off, heads);
+        k_check_edges<<<grid_for(E, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(V, E, g->dst, heads, flags);
+        CGB_CUDA_TRY(cudaMemcpyAsync(h, flags, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
+        CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        if (h[0] & 8u) {
+            dfree(heads);
+            dfree(flags);
+            throw Error{CGB_EFORMAT, "csr_dest holds a vertex id >= V"};
+        }
+        if (pass == 0 && h[1]) {
+            sort_neighbours(g);
+            continue;
+        }
+        if (h[1] || h[2]) {
+            dfree(heads);
+            dfree(flags);
+            throw Error{CGB_EFORMAT, "neighbour list not strictly ascending after sorting (duplicate edge)"};
+        }
+        break;
+    }
+    dfree(heads);
+    dfree(flags);
+}
+
+void compute_weight_sum(cgb_graph* g)
+{
+    if (!g->w || g->E == 0) return;
+    unsigned long long* d = dalloc<unsigned long long>(1);
+    CGB_CUDA_TRY(cudaMemsetAsync(d, 0, sizeof(unsigned long long), g->stream));
+    k_sum_u32<<<grid_for(g->E, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(g->E, g->w, d);
+    unsigned long long h = 0;
+    CGB_CUDA_TRY(cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
+    CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    dfree(d);
+    g->sum_w = h;
+}
+
+void ensure_symmetry_known(cgb_graph* g)
+{
+    if (g->symmetric >= 0) return;
+    uint32_t* d = dalloc<uint32_t>(1);
+    CGB_CUDA_TRY(cudaMemsetAsync(d, 0, sizeof(uint32_t), g->stream));
+    if (g->E)
+        k_check_symmetric<<<grid_for(g->E, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(g->V, g->E, g->off, g->dst,
+                                                                                         d);
+    uint32_t h = 0;
+    CGB_CUDA_TRY(cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
+    CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    dfree(d);
+    g->symmetric = h ? 0 : 1;
+}
+
+void ensure_csc(cgb_graph* g)
+{
+    if (g->in_off) return;
+    ensure_symmetry_known(g);
+    if (g->symmetric == 1) {
+        g->in_off = g->off;
+        g->in_src = g->dst;
+        g->csc_owned = false;
+        return;
+    }
+    const uint32_t V = g->V, E = g->E;
+    const uint32_t b = bits_for(V);
+    g->in_off = dalloc<uint32_t>((size_t)V + 1);
+    g->in_src = dalloc<uint32_t>(E);
+    g->csc_owned = true;
+    if (E == 0) {
+        CGB_CUDA_TRY(cudaMemsetAsync(g->in_off, 0, ((size_t)V + 1) * sizeof(uint32_t), g->stream));
+        return;
+    }
+    uint64_t* keys = dalloc<uint64_t>(E);
+    uint64_t* alt = dalloc<uint64_t>(E);
+    const uint32_t grid = grid_for(E, kBlock, kNumSMs * 16);
+    k_make_keys<<<grid, kBlock, 0, g->stream>>>(V, E, g->off, g->dst, b, keys, true);
+    radix_sort_u64(g, keys, alt, E, 2 * b);
+    k_split_keys<<<grid, kBlock, 0, g->stream>>>(E, keys, b, g->in_src);
+    k_offsets_from_keys<<<grid_for((uint64_t)E + 1, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(V, E, keys, b,
+                                                                                                   g->in_off);
+    CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    dfree(keys);
+    dfree(alt);
+}
+
+void ensure_frontier(cgb_graph* g)
+{
+    if (g->q[0]) return;
+    const uint32_t V = g->V;
+    g->q[0] = dalloc<uint32_t>(V);
+    g->q[1] = dalloc<uint32_t>(V);
+    g->huge_q = dalloc<uint32_t>(V);
+    g->visited = dalloc<uint32_t>(g->words());
+    g->front_bm = dalloc<uint32_t>(2 * (size_t)g->words());
+    g->stamp = dalloc<uint32_t>(V);
+    g->sample = dalloc<uint32_t>(1024);
+}
+
+void ensure_sssp(cgb_graph* g)
+{
+    if (g->far[0]) return;
+    if (g->w && g->sum_w == 0) compute_weight_sum(g);
+    uint64_t cap = (uint64_t)g->E + g->V + 1024;
+    if (cap > 0xFFFFFFF0ull) cap = 0xFFFFFFF0ull;
+    g->far_cap = (uint32_t)cap;
+    g->far[0] = dalloc<uint2>(cap);
+    g->far[1] = dalloc<uint2>(cap);
+}
+
+void ensure_pr(cgb_graph* g)
+{
+    ensure_csc(g);
+    if (g->pr_ready) return;
+    const uint32_t V = g->V;
+    for (int i = 0; i < 2; i++) {
+        if (!g->pr[i]) g->pr[i] = dalloc<double>(V);
+        if (!g->contrib[i]) g->contrib[i] = dalloc<double>(V);
+    }
+    uint32_t* n = dalloc<uint32_t>(1);
+    CGB_CUDA_TRY(cudaMemsetAsync(n, 0, sizeof(uint32_t), g->stream));
+    uint32_t* rows = dalloc<uint32_t>(V);
+    k_collect_heavy_rows<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, g->in_off, kPrHuge, rows, n);
+    uint32_t h = 0;
+    CGB_CUDA_TRY(cudaMemcpyAsync(&h, n, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
+    CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    dfree(n);
+    g->n_pr_huge = h;
+    g->pr_huge_rows = rows;
+    g->pr_ready = true;
+}
+
+void count_reached(cgb_graph* g)
+{
+    CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->reached_edges, 0, sizeof(unsigned long long), g->stream));
+    CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->reached, 0, sizeof(uint32_t), g->stream));
+    k_count_reached<<<grid_for(g->V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(g->V, g->value, g->off, g->ctr);
+    sync_counters(g);
+    g->stats.reached = g->h_ctr->reached;
+    g->stats.traversed_edges = g->h_ctr->reached_edges;
+}
+
+// --------------------------------------------------------------- timers
+void ktimer_begin(cgb_graph* g, int cls)
+{
+    if (g->kev_used + 2 > g->kev.size()) {
+        for (int i = 0; i < 64; i++) {
+            cudaEvent_t e;
+            CGB_CUDA_TRY(cudaEventCreate(&e));
+            g->kev.push_back(e);
+        }
+    }
+    CGB_CUDA_TRY(cudaEventRecord(g->kev[g->kev_used], g->stream));
+    g->kev_class.push_back(cls);
+    g->kev_used += 2;
+}
+
+void ktimer_end(cgb_graph* g) { CGB_CUDA_TRY(cudaEventRecord(g->kev[g->kev_used - 1], g->stream)); }
+
+void ktimer_collect(cgb_graph* g)
+{
+    for (size_t i = 0; i < g->kev_class.size(); i++) {
+        float ms = 0.f;
+        CGB_CUDA_TRY(cudaEventElapsedTime(&ms, g->kev[2 * i], g->kev[2 * i + 1]));
+        const int c = g->kev_class[i];
+        g->stats.kernel_ms[c] += ms;
+        g->stats.kernel_launches[c] += 1;
+    }
+    g->kev_class.clear();
+    g->kev_used = 0;
+}
+
+// --------------------------------------------------------------- lifetime
+cgb_graph* graph_alloc(uint32_t V, uint32_t E, uint32_t nz, int device, bool with_weight)
+{
+    CGB_CUDA_TRY(cudaSetDevice(device));
+    cgb_graph* g = new cgb_graph();
+    g->device = device;
+    g->V = V;
+    g->E = E;
+    g->nz = (nz == 0 || nz > V) ? V : nz;
+    try {
+        CGB_CUDA_TRY(cudaStreamCreateWithFlags(&g->own_stream, cudaStreamNonBlocking));
+        g->stream = g->own_stream;
+        CGB_CUDA_TRY(cudaEventCreate(&g->ev_start));
+        CGB_CUDA_TRY(cudaEventCreate(&g->ev_stop));
+        CGB_CUDA_TRY(cudaEventCreate(&g->ev_iter[0]));
+        CGB_CUDA_TRY(cudaEventCreate(&g->ev_iter[1]));
+        g->ctr = dalloc<DevCounters>(1);
+        CGB_CUDA_TRY(cudaMallocHost((void**)&g->h_ctr, sizeof(DevCounters)));
+        CGB_CUDA_TRY(cudaMemsetAsync(g->ctr, 0, sizeof(DevCounters), g->stream));
+        g->off = dalloc<uint32_t>((size_t)V + 1);
+        g->dst = dalloc<uint32_t>(E);
+        if (with_weight) g->w = dalloc<uint32_t>(E);
+        g->value = dalloc<uint32_t>(V);
+    } catch (...) {
+        graph_free(g);
+        throw;
+    }
+    return g;
+}
+
+void graph_free(cgb_graph* g)
+{
+    if (!g) return;
+    cudaSetDevice(g->device);
+    if (g->stream) cudaStreamSynchronize(g->stream);
+    if (g->csc_owned) {
+        dfree(g->in_off);
+        dfree(g->in_src);
+    }
+    void* ptrs[] = {g->off, g->dst, g->w, g->pr_huge_rows, g->value, g->pr[0], g->pr[1], g->contrib[0],
+                    g->contrib[1], g->q[0], g->q[1], g->huge_q, g->visited, g->front_bm, g->stamp, g->far[0],
+                    g->far[1], g->sample, g->ctr};
+    for (void* p : ptrs) dfree(p);
+    if (g->h_ctr) cudaFreeHost(g->h_ctr);
+    for (cudaEvent_t e : g->kev) cudaEventDestroy(e);
+    cudaEvent_t evs[] = {g->ev_start, g->ev_stop, g->ev_iter[0], g->ev_iter[1]};
+    for (cudaEvent_t e : evs)
+        if (e) cudaEventDestroy(e);
+    if (g->own_stream) cudaStreamDestroy(g->own_stream);
+    delete g;
+}
+
+}  // namespace cgb

@@ -1,0 +1,131 @@
+// Degree-binned push expansion over a vertex frontier.
+//
+// Replaces the reference's per-thread load balancers WarpDonate::schedule
+// (my_project/CGgraph/device_warpDonate.cuh:42-388) and CTA::schedule
+// (my_project/CGgraph/device_CTA.cuh:28-112), which run one frontier vertex
+// per thread and hand large lists to the warp or CTA with __syncthreads
+// loops, serialising a hub's whole list on one CTA.  Here each frontier
+// vertex is binned by out-degree:
+//   deg >= kHugeDeg          deferred to k_push_huge, which splits the list
+//                            into kHugeChunk-edge chunks across every CTA;
+//   kCtaDeg <= deg < kHuge   the whole CTA walks the list (owner election);
+//   32 <= deg < kCtaDeg      one warp walks the list (ballot election);
+//   deg < 32                 fine-grained gather: a CTA-wide exclusive scan of
+//                            the remaining degrees packs the small lists
+//                            into shared memory, one edge per thread.
+// Every edge visit is warp-collective (Op::edge is called by all 32 lanes,
+// with `valid` false on idle lanes) so that the ops can aggregate their
+// queue appends with one ballot and one atomic per warp.
+#pragma once
+
+#include "common.cuh"
+#include "engine.cuh"
+
+namespace cgb {
+
+// Op interface:
+//   __device__ bool load(uint32_t v, uint32_t& start, uint32_t& deg, uint32_t& msg) const;
+//   __device__ void edge(bool valid, uint32_t e, uint32_t msg) const;   // warp-collective
+template <class Op, bool kIdentity>
+__global__ void __launch_bounds__(kBlock) k_push_twc(const uint32_t* __restrict__ qin, uint32_t nin, Op op,
+                                                     uint32_t* __restrict__ huge_q, uint32_t* huge_len)
+{
+    __shared__ uint32_t s_scan[kBlock / 32 + 1];
+    __shared__ uint32_t s_owner, s_start, s_deg, s_msg;
+    __shared__ uint32_t s_edge[kBlock];
+    __shared__ uint32_t s_emsg[kBlock];
+    const uint32_t tid = threadIdx.x;
+
+    for (uint32_t base = blockIdx.x * kBlock; base < nin; base += gridDim.x * kBlock) {
+        uint32_t i = base + tid;
+        uint32_t start = 0, deg = 0, msg = 0;
+        if (i < nin) {
+            uint32_t v = kIdentity ? i : qin[i];
+            if (!op.load(v, start, deg, msg)) deg = 0;
+            if (deg >= kHugeDeg) {
+                uint32_t slot = atomicAdd(huge_len, 1u);
+                huge_q[slot] = v;  // capacity V: each vertex appears once per frontier
+                deg = 0;
+            }
+        }
+        // CTA tier
+        while (__syncthreads_or(deg >= kCtaDeg)) {
+            if (deg >= kCtaDeg) s_owner = tid;
+            __syncthreads();
+            if (s_owner == tid) {
+                s_start = start;
+                s_deg = deg;
+                s_msg = msg;
+                deg = 0;
+            }
+            __syncthreads();
+            const uint32_t st = s_start, dg = s_deg, m = s_msg;
+            for (uint32_t k = 0; k < dg; k += kBlock) op.edge(k + tid < dg, st + k + tid, m);
+            __syncthreads();
+        }
+        // warp tier
+        uint32_t wmask;
+        while ((wmask = __ballot_sync(0xffffffffu, deg >= 32)) != 0) {
+            const uint32_t leader = __ffs(wmask) - 1;
+            const uint32_t st = __shfl_sync(0xffffffffu, start, leader);
+            const uint32_t dg = __shfl_sync(0xffffffffu, deg, leader);
+            const uint32_t m = __shfl_sync(0xffffffffu, msg, leader);
+            if (lane_id() == leader) deg = 0;
+            for (uint32_t k = 0; k < dg; k += 32) op.edge(k + lane_id() < dg, st + k + lane_id(), m);
+        }
+        // fine-grained tier
+        uint32_t total;
+        const uint32_t rank = block_excl_scan(deg, total, s_scan);
+        uint32_t consumed = 0;
+        for (uint32_t done = 0; done < total; done += kBlock) {
+            while (consumed < deg && rank + consumed < done + kBlock) {
+                s_edge[rank + consumed - done] = start + consumed;
+                s_emsg[rank + consumed - done] = msg;
+                consumed++;
+            }
+            __syncthreads();
+            const uint32_t n = min((uint32_t)kBlock, total - done);
+            const bool valid = tid < n;
+            op.edge(valid, valid ? s_edge[tid] : 0u, valid ? s_emsg[tid] : 0u);
+            __syncthreads();
+        }
+    }
+}
+
+// Hubs deferred by k_push_twc: the concatenated chunk list of all deferred
+// vertices is dealt round-robin to the CTAs of the grid.
+template <class Op>
+__global__ void __launch_bounds__(kBlock) k_push_huge(const uint32_t* __restrict__ huge_q, const uint32_t* huge_len,
+                                                      Op op)
+{
+    const uint32_t n = *huge_len;
+    uint64_t chunk_base = 0;
+    for (uint32_t h = 0; h < n; h++) {
+        const uint32_t v = huge_q[h];
+        uint32_t start, deg, msg;
+        if (!op.load(v, start, deg, msg)) continue;
+        const uint32_t nch = (deg + kHugeChunk - 1) / kHugeChunk;
+        const uint32_t first = (uint32_t)((blockIdx.x + gridDim.x - (chunk_base % gridDim.x)) % gridDim.x);
+        for (uint32_t c = first; c < nch; c += gridDim.x) {
+            const uint32_t cs = c * kHugeChunk;
+            const uint32_t ce = min(deg, cs + kHugeChunk);
+            for (uint32_t k = cs; k < ce; k += kBlock) op.edge(k + threadIdx.x < ce, start + k + threadIdx.x, msg);
+        }
+        chunk_base += nch;
+    }
+}
+
+// Launches the TWC expansion (plus the hub kernel) of a queue whose length
+// the host knows.
+template <class Op>
+inline void launch_push_twc(cgb_graph* g, const uint32_t* qin, uint32_t nin, const Op& op, bool identity)
+{
+    if (nin == 0) return;
+    const uint32_t grid = grid_for(nin, kBlock, kNumSMs * 8);
+    g->stats.launches += 2;
+    if (identity) k_push_twc<Op, true><<<grid, kBlock, 0, g->stream>>>(qin, nin, op, g->huge_q, &g->ctr->huge_len);
+    else k_push_twc<Op, false><<<grid, kBlock, 0, g->stream>>>(qin, nin, op, g->huge_q, &g->ctr->huge_len);
+    k_push_huge<Op><<<kNumSMs * 4, kBlock, 0, g->stream>>>(g->huge_q, &g->ctr->huge_len, op);
+}
+
+}  // namespace cgb

@@ -1,0 +1,383 @@
+"""Host-side mirror of the reference's interface for the SINGLE_GPU path.
+
+Reference (PengBo410/CGgraph, paths under CGgraph/):
+
+* enums ``Algorithm_type``, ``Engine_type``, ``OrderMethod`` and the
+  ``CSR_Result_type`` struct -- Basic/Graph/basic_struct.hpp:7-16,41-76,144-178;
+* ``load_binFile`` / ``save_binArray`` -- Basic/Other/IO.hpp:44-113;
+* ``GraphDeviceWorklist`` (constructor, ``graphProcess_device``,
+  ``result_D2H``, ``vertexValue``) -- my_project/CGgraph/GraphDevice.cuh:9-269;
+  its replacement here is ``GraphB200``, which runs the sm_100a engine of
+  libcgb200.so through the C ABI;
+* the SINGLE_GPU branch of ``main_partition()`` (root range check,
+  ``rootTranfer`` through ``old2new``, ``runs``, trimmed mean) --
+  my_project/CGgraph/main_partition.hpp:319-383,141-144;
+* ``checkBinResult`` (exact compare, ``old2new`` remap) -- Basic/Graph/util.cuh:59-118.
+
+Errors are raised as ``CgbError`` carrying the C status code where the
+reference aborts (``assert_msg``) or exits (``CUDA_CHECK``).
+"""
+from __future__ import annotations
+
+import ctypes
+import enum
+import os
+from dataclasses import dataclass
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib as L
+from ._lib import CgbError, check
+
+VertexValue_MAX = L.VALUE_MAX
+
+
+class Algorithm_type(enum.IntEnum):
+    """Basic/Graph/basic_struct.hpp:144-151."""
+    BFS = 0
+    SSSP = 1
+    CC = 2
+    PR = 3
+    UNDEFINE = 4
+
+
+class Engine_type(enum.IntEnum):
+    """Basic/Graph/basic_struct.hpp:165-178."""
+    COORDINATION = 0
+    COOPERATION = 1
+    SINGLE_CORE = 2
+    MULTI_CORE = 3
+    SINGLE_GPU = 4
+    BLOCK_2D = 5
+    COMPUTE_INDEGREE = 6
+    REORDER = 7
+    ACTIVEBLOCK = 8
+
+
+class OrderMethod(enum.IntEnum):
+    """Basic/Graph/basic_struct.hpp:41-76."""
+    NATIVE = 0
+    OUTDEGREE_NODE = 1
+    OUTDEGREE_SOCKET = 2
+    OUTDEGREE_THREAD = 3
+    GORDER = 4
+    RCM = 5
+    RCM_LAST_ZERO_OUTDEGREE = 6
+    RCM_LAST_ONE_ZERO_DEGREE = 7
+    OUTDEGREE_NODE_dec = 8
+    DEGREE_NODE = 9
+    RCM_INDEGREE = 10
+    RCM_OUTDEGREE = 11
+    NORMAL_OUTDEGREE_DEC = 12
+    UnDirected_NATIVE = 13
+    UnDirected_RCM = 14
+    UnDirected_RCM_LAST_ZERO_OUTDEGREE = 15
+    MY_BFS_OUT = 16
+    MY_BFS_IN = 17
+    MY_BFS_OUT_IN = 18
+    MY_IMAX_BFS_OUT = 19
+    MY_IMAX_BFS_IN = 20
+    IN_DEGREE_DEC = 21
+
+
+@dataclass
+class CSR_Result_type:
+    """Basic/Graph/basic_struct.hpp:7-16 (arrays are numpy uint32)."""
+    vertexNum: int
+    edgeNum: int
+    csr_offset: np.ndarray
+    csr_dest: np.ndarray
+    csr_weight: Optional[np.ndarray]
+    noZeroOutDegreeNum: int = 0
+
+
+def load_binFile(path: str, length: int, dtype=np.uint32) -> np.ndarray:
+    """Reads a raw little-endian array, requiring file bytes == length * itemsize
+    (Basic/Other/IO.hpp:44-92, which asserts the same)."""
+    if not os.path.exists(path):
+        raise CgbError(L.EIO, f"Bin File [{path}] Not Exist")
+    itemsize = np.dtype(dtype).itemsize
+    if os.path.getsize(path) // itemsize != length or os.path.getsize(path) % itemsize:
+        raise CgbError(L.EIO, f"(total_bytes / utilSize != length) In Function load_binFile({path})")
+    return np.fromfile(path, dtype=dtype, count=length)
+
+
+def save_binArray(path: str, array) -> None:
+    """Basic/Other/IO.hpp:97-113."""
+    np.ascontiguousarray(array).tofile(path)
+
+
+def _ptr(a) -> Optional[int]:
+    """Data pointer of a numpy array or a torch tensor (host, pinned or CUDA)."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        if not a.flags["C_CONTIGUOUS"]:
+            raise ValueError("array must be contiguous")
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        if not a.is_contiguous():
+            raise ValueError("tensor must be contiguous")
+        return a.data_ptr()
+    raise TypeError(f"unsupported buffer type {type(a)}")
+
+
+def _u32(a):
+    if a is None or not isinstance(a, np.ndarray):
+        return a
+    return np.ascontiguousarray(a, dtype=np.uint32)
+
+
+def make_options(schedule: int = L.SCHED_HEURISTIC, variant: int = L.VAR_AUTO, sssp_delta: int = 0,
+                 bfs_alpha: float = 0.0, bfs_beta: float = 0.0, max_iterations: int = 0, flags: int = 0) -> L.Options:
+    o = L.Options()
+    o.struct_size = ctypes.sizeof(L.Options)
+    o.schedule = schedule
+    o.variant = variant
+    o.sssp_delta = sssp_delta
+    o.bfs_alpha = bfs_alpha
+    o.bfs_beta = bfs_beta
+    o.max_iterations = max_iterations
+    o.flags = flags
+    return o
+
+
+class Graph:
+    """A graph resident in HBM (a ``cgb_graph`` handle)."""
+
+    def __init__(self, handle: int):
+        self._h = ctypes.c_void_p(handle)
+        V, E, sym = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_int32()
+        check(L.lib().cgb_graph_info(self._h, ctypes.byref(V), ctypes.byref(E), ctypes.byref(sym)))
+        self.vertexNum = V.value
+        self.edgeNum = E.value
+
+    # ---- constructors
+    @classmethod
+    def from_csr(cls, offsets, dest, weight=None, vertexNum: Optional[int] = None, edgeNum: Optional[int] = None,
+                 noZeroOutDegreeNum: int = 0, device: int = 0) -> "Graph":
+        offsets, dest, weight = _u32(offsets), _u32(dest), _u32(weight)
+        V = vertexNum if vertexNum is not None else len(offsets) - 1
+        E = edgeNum if edgeNum is not None else len(dest)
+        h = ctypes.c_void_p()
+        check(L.lib().cgb_graph_create(_ptr(offsets), _ptr(dest) if E else None, _ptr(weight) if E else None,
+                                       V, E, noZeroOutDegreeNum, device, ctypes.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def from_result(cls, csr: CSR_Result_type, device: int = 0) -> "Graph":
+        return cls.from_csr(csr.csr_offset, csr.csr_dest, csr.csr_weight, csr.vertexNum, csr.edgeNum,
+                            csr.noZeroOutDegreeNum, device)
+
+    @classmethod
+    def from_files(cls, offsets_path: str, dest_path: str, weight_path: Optional[str], vertexNum: int,
+                   edgeNum: int, device: int = 0) -> "Graph":
+        h = ctypes.c_void_p()
+        enc = lambda p: p.encode() if p is not None else None  # noqa: E731
+        check(L.lib().cgb_graph_load_files(enc(offsets_path), enc(dest_path), enc(weight_path), vertexNum, edgeNum,
+                                           device, ctypes.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def rmat(cls, scale: int, edge_factor: int = 16, seed: int = 1, a: float = 0.57, b: float = 0.19,
+             c: float = 0.19, scramble: bool = True, symmetrise: bool = False, wmax: int = 64,
+             device: int = 0) -> "Graph":
+        h = ctypes.c_void_p()
+        check(L.lib().cgb_gen_rmat(scale, edge_factor, seed, a, b, c, int(scramble), int(symmetrise), wmax, device,
+                                   ctypes.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def grid(cls, rows: int, cols: int, seed: int = 1, wmax: int = 1000, device: int = 0) -> "Graph":
+        h = ctypes.c_void_p()
+        check(L.lib().cgb_gen_grid(rows, cols, seed, wmax, device, ctypes.byref(h)))
+        return cls(h.value)
+
+    # ---- queries
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def symmetric(self) -> int:
+        sym = ctypes.c_int32()
+        check(L.lib().cgb_graph_info(self._h, None, None, ctypes.byref(sym)))
+        return sym.value
+
+    def set_stream(self, stream) -> None:
+        """Run this graph's work on `stream` (a torch.cuda.Stream, a raw
+        cudaStream_t as int, or None for the graph's own stream)."""
+        ptr = None
+        if stream is not None:
+            ptr = stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+        check(L.lib().cgb_graph_set_stream(self._h, ptr))
+
+    def download(self, with_weight: bool = True):
+        off = np.empty(self.vertexNum + 1, np.uint32)
+        dst = np.empty(max(1, self.edgeNum), np.uint32)
+        w = np.empty(max(1, self.edgeNum), np.uint32) if with_weight else None
+        check(L.lib().cgb_graph_download(self._h, _ptr(off), _ptr(dst), _ptr(w)))
+        return off, dst[: self.edgeNum], (w[: self.edgeNum] if w is not None else None)
+
+    def device_csr(self):
+        o, d, w = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+        check(L.lib().cgb_graph_device_csr(self._h, ctypes.byref(o), ctypes.byref(d), ctypes.byref(w)))
+        return o.value, d.value, w.value
+
+    def result_device_ptr(self) -> int:
+        p = ctypes.c_void_p()
+        check(L.lib().cgb_graph_result_device(self._h, ctypes.byref(p)))
+        return p.value
+
+    # ---- runs
+    def run(self, algorithm: int, root_or_iters: int = 0, options: Optional[L.Options] = None, out=None,
+            to_host: bool = True):
+        """One run.  Returns (values, ms).  ``out`` may be a numpy array or a
+        torch tensor (host, pinned or CUDA); with ``to_host=False`` and no
+        ``out`` the result stays on the device and values is None."""
+        alg = int(algorithm)
+        if out is None and to_host:
+            out = np.empty(self.vertexNum, np.float64 if alg == Algorithm_type.PR else np.uint32)
+        ms = ctypes.c_double()
+        p = _ptr(out)
+        check(L.lib().cgb_run(self._h, alg, int(root_or_iters), ctypes.byref(options) if options else None,
+                              p if alg != Algorithm_type.PR else None, p if alg == Algorithm_type.PR else None,
+                              ctypes.byref(ms)))
+        return out, ms.value
+
+    def run_batch(self, algorithm: int, roots: Sequence[int], options: Optional[L.Options] = None, out=None):
+        roots = np.ascontiguousarray(roots, dtype=np.uint32)
+        if out is None:
+            out = np.empty((len(roots), self.vertexNum), np.uint32)
+        ms = ctypes.c_double()
+        check(L.lib().cgb_run_batch(self._h, int(algorithm), _ptr(roots), len(roots),
+                                    ctypes.byref(options) if options else None, _ptr(out), ctypes.byref(ms)))
+        return out, ms.value
+
+    def stats(self) -> L.RunStats:
+        s = L.RunStats()
+        check(L.lib().cgb_run_stats_get(self._h, ctypes.byref(s)))
+        return s
+
+    def trace(self):
+        n = ctypes.c_uint32()
+        check(L.lib().cgb_trace_get(self._h, None, 0, ctypes.byref(n)))
+        arr = (L.IterTrace * max(1, n.value))()
+        check(L.lib().cgb_trace_get(self._h, arr, n.value, ctypes.byref(n)))
+        return [arr[i] for i in range(n.value)]
+
+    def close(self) -> None:
+        if self._h is not None and self._h.value:
+            check(L.lib().cgb_graph_destroy(self._h))
+        self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class GraphB200:
+    """Drop-in for ``GraphDeviceWorklist`` (my_project/CGgraph/GraphDevice.cuh:9-269).
+
+    ``GraphB200(csr_result, algorithm)`` uploads the CSR once (the reference's
+    constructor + ``csrToDevice``); ``graphProcess_device(algorithm, root)``
+    runs one traversal and returns its device time in ms (for PageRank
+    ``root`` is the iteration count, GraphDevice.cuh:159-162);
+    ``result_D2H()`` fills ``vertexValue`` (uint32[V], or float64[V] for
+    PageRank, which the reference computes in uint32 and so cannot produce).
+    """
+
+    def __init__(self, csr_result: CSR_Result_type, algorithm: Algorithm_type, device: int = 0,
+                 options: Optional[L.Options] = None):
+        self.vertexNum = csr_result.vertexNum
+        self.edgeNum = csr_result.edgeNum
+        self.noZeroOutDegreeNum = csr_result.noZeroOutDegreeNum or csr_result.vertexNum
+        self.zeroOutDegreeNum = self.vertexNum - self.noZeroOutDegreeNum
+        self.algorithm = Algorithm_type(algorithm)
+        self.options = options
+        self.graph = Graph.from_result(csr_result, device)
+        self.vertexValue = None
+        self._last_alg = None
+
+    def graphProcess_device(self, algorithm: Algorithm_type, root: int = 0) -> float:
+        _, ms = self.graph.run(int(algorithm), int(root), self.options, out=None, to_host=False)
+        self._last_alg = Algorithm_type(algorithm)
+        return ms
+
+    def result_D2H(self) -> None:
+        if self._last_alg is None:
+            raise CgbError(L.EINVAL, "result_D2H before any graphProcess_device")
+        is_pr = self._last_alg == Algorithm_type.PR
+        out = np.empty(self.vertexNum, np.float64 if is_pr else np.uint32)
+        check(L.lib().cgb_graph_result_download(self.graph.handle, _ptr(out)))
+        self.vertexValue = out
+
+    def close(self):
+        self.graph.close()
+
+
+def trimmed_mean_ms(times: Sequence[float]) -> float:
+    """main_partition.hpp:347-365: sort, drop min and max when runs > 2."""
+    t = sorted(times)
+    if len(t) > 2:
+        t = t[1:-1]
+    return sum(t) / len(t)
+
+
+def main_partition(csr_result: CSR_Result_type, algorithm: Algorithm_type, root: int = 0, runs: int = 1,
+                   engine_type: Engine_type = Engine_type.SINGLE_GPU, orderMethod: OrderMethod = OrderMethod.NATIVE,
+                   rootTranfer: bool = True, old2new: Optional[np.ndarray] = None, device: int = 0,
+                   options: Optional[L.Options] = None) -> dict:
+    """The SINGLE_GPU branch of main_partition() (main_partition.hpp:319-383).
+
+    Returns {"times": per-run ms, "total_run_time_ms": trimmed mean,
+    "vertexValue": result} -- the printed ``[Total Run Time]`` and the array
+    the reference then hands to checkBinResult.  A root outside [0, V)
+    returns without running, as the reference's ``do { if (root < 0 ||
+    root >= vertices) break; ... } while (0)`` does."""
+    if engine_type != Engine_type.SINGLE_GPU:
+        raise CgbError(L.EUNSUPPORTED, f"Engine_type {Engine_type(engine_type).name} is not provided by this engine "
+                                       "(only the SINGLE_GPU path is rebuilt)")
+    engine = GraphB200(csr_result, algorithm, device=device, options=options)
+    try:
+        times = []
+        if 0 <= root < csr_result.vertexNum:
+            switch_root = root
+            if orderMethod != OrderMethod.NATIVE and rootTranfer and algorithm != Algorithm_type.PR:
+                if old2new is None:
+                    raise CgbError(L.EINVAL, "rootTranfer needs old2new")
+                switch_root = int(old2new[root])
+            for _ in range(runs):
+                times.append(engine.graphProcess_device(algorithm, switch_root))
+            engine.result_D2H()
+        return {"times": times, "total_run_time_ms": trimmed_mean_ms(times) if times else None,
+                "vertexValue": engine.vertexValue}
+    finally:
+        engine.close()
+
+
+def checkBinResult(golden, current_array: np.ndarray, length: int, orderMethod: OrderMethod = OrderMethod.NATIVE,
+                   old2new: Optional[np.ndarray] = None) -> None:
+    """Exact element-wise compare (Basic/Graph/util.cuh:59-118); ``golden`` is
+    a result-file path or an array.  With a reordered graph the current array
+    is indexed through old2new.  Raises AssertionError naming the first
+    mismatch, as assert_msg does."""
+    ref = load_binFile(golden, length, current_array.dtype) if isinstance(golden, str) else np.asarray(golden)
+    cur = np.asarray(current_array)
+    if orderMethod == OrderMethod.NATIVE:
+        bad = np.nonzero(cur[:length] != ref[:length])[0]
+    else:
+        bad = np.nonzero(cur[np.asarray(old2new)[:length]] != ref[:length])[0]
+    if bad.size:
+        i = int(bad[0])
+        got = cur[i] if orderMethod == OrderMethod.NATIVE else cur[int(old2new[i])]
+        raise AssertionError(f"error: current_array[{i}] = {got}, resultArray[{i}] = {ref[i]}")

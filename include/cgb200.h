@@ -1,0 +1,199 @@
+/*
+ * cgb200 -- a B200 (sm_100a) graph engine for BFS, SSSP, CC and PageRank
+ * behind the selection interface of CGgraph (PengBo410/CGgraph).
+ *
+ * Plain C ABI: no C++ or framework types cross it.  Every call returns a
+ * cgb_status; cgb_last_error_string() describes the last failure on the
+ * calling thread.  Host and device pointers are both accepted wherever a
+ * buffer is passed (the copy direction is inferred from the pointer).
+ *
+ * Reference interfaces replaced (paths under CGgraph/ of the reference):
+ *   - CSR_Result_type {vertexNum, edgeNum, csr_offset, csr_dest, csr_weight,
+ *     noZeroOutDegreeNum}                    Basic/Graph/basic_struct.hpp:7-16
+ *   - load_binFile<T>(path, length)          Basic/Other/IO.hpp:44-92
+ *   - nbrSort_taskSteal(csr) (sort + strict-ascending check)
+ *                                            my_project/CGgraph/sortNbr.hpp:8-99
+ *   - GraphDeviceWorklist(csr, alg)          my_project/CGgraph/GraphDevice.cuh:48-71
+ *   - GraphDeviceWorklist::graphProcess_device(alg, root) -> ms
+ *                                            my_project/CGgraph/GraphDevice.cuh:92-176
+ *   - GraphDeviceWorklist::result_D2H() / vertexValue
+ *                                            my_project/CGgraph/GraphDevice.cuh:21,259-262
+ *   - Algorithm_type {BFS, SSSP, CC, PR}     Basic/Graph/basic_struct.hpp:144-151
+ *   - VertexValue_MAX = 999999999            Basic/Graph/basic_def.hpp:18
+ */
+#ifndef CGB200_H
+#define CGB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CGB_VALUE_MAX 999999999u /* VertexValue_MAX, Basic/Graph/basic_def.hpp:18 */
+#define CGB_ABI_VERSION 1
+
+typedef enum cgb_status {
+    CGB_OK = 0,
+    CGB_EINVAL = 1,    /* bad argument (null pointer, root >= V, unknown algorithm) */
+    CGB_EFORMAT = 2,   /* CSR violates the reference's invariants (offsets, ids, duplicates) */
+    CGB_EIO = 3,       /* file missing or of the wrong size (load_binFile's checks) */
+    CGB_ENOMEM = 4,    /* device or host allocation failed */
+    CGB_ECUDA = 5,     /* CUDA runtime error (replaces CUDA_CHECK's exit(1)) */
+    CGB_ETIMEOUT = 6,  /* a device-side wait or the iteration budget ran out */
+    CGB_EOVERFLOW = 7, /* a work queue overflowed its capacity */
+    CGB_EUNSUPPORTED = 8
+} cgb_status;
+
+/* Algorithm_type values, Basic/Graph/basic_struct.hpp:144-151. */
+typedef enum cgb_algorithm { CGB_BFS = 0, CGB_SSSP = 1, CGB_CC = 2, CGB_PR = 3 } cgb_algorithm;
+
+/* Per-iteration schedule choice.  Every schedule computes the same result. */
+typedef enum cgb_schedule {
+    CGB_SCHED_HEURISTIC = 0, /* Beamer direction switch, fixed SSSP delta */
+    CGB_SCHED_LEARNED = 1,   /* MLP policy (cgb_policy_*), heuristic fallback */
+    CGB_SCHED_FIXED = 2      /* the variant / direction given in cgb_options */
+} cgb_schedule;
+
+/* Push-expansion variants (cgb_options.variant for CGB_SCHED_FIXED). */
+typedef enum cgb_variant {
+    CGB_VAR_AUTO = 0,
+    CGB_VAR_TWC = 1,      /* degree-binned thread / warp / CTA expansion */
+    CGB_VAR_PULL = 2,     /* bottom-up pull over the in-edges (BFS only) */
+    CGB_VAR_PUSH = 3      /* top-down push (BFS: forbid the pull direction) */
+} cgb_variant;
+
+typedef struct cgb_options {
+    uint32_t struct_size;   /* sizeof(cgb_options); 0 = all defaults */
+    int32_t schedule;       /* cgb_schedule */
+    int32_t variant;        /* cgb_variant, for CGB_SCHED_FIXED */
+    uint32_t sssp_delta;    /* 0 = heuristic (mean weight * 32 / mean degree) */
+    double bfs_alpha;       /* Beamer alpha, 0 = 15 */
+    double bfs_beta;        /* Beamer beta, 0 = 18 */
+    uint64_t max_iterations;/* 0 = unlimited (V + 1 levels bound BFS anyway) */
+    uint32_t flags;         /* CGB_FLAG_* */
+    uint32_t reserved[7];
+} cgb_options;
+
+#define CGB_FLAG_KERNEL_TIMING 0x1u /* record per-kernel CUDA-event times (cgb_run_stats) */
+#define CGB_FLAG_TRACE 0x2u         /* log one cgb_iter_trace per iteration */
+
+typedef struct cgb_graph cgb_graph;
+
+/* Per-run statistics of the last cgb_run on a graph. */
+typedef struct cgb_run_stats {
+    double ms;                /* device time of the run (CUDA events around it) */
+    uint64_t iterations;      /* levels / relaxation rounds / PageRank iterations */
+    uint64_t traversed_edges; /* TEPS numerator: BFS/SSSP sum of outdeg of reached vertices,
+                                 CC edges of the graph, PR E * iterations */
+    uint64_t reached;         /* vertices with a value != CGB_VALUE_MAX */
+    uint64_t alg_bytes;       /* algorithmic HBM bytes of the run (lower bound) */
+    double kernel_ms[8];      /* per kernel class, with CGB_FLAG_KERNEL_TIMING */
+    uint64_t kernel_launches[8];
+    uint64_t pushes_td, pulls_bu; /* BFS: levels run top-down / bottom-up */
+    uint32_t sssp_delta;      /* delta used */
+    int32_t cc_path;          /* 0 = hook+compress (symmetric), 1 = label propagation */
+    uint64_t launches;        /* kernels launched by the run */
+} cgb_run_stats;
+
+/* Kernel classes indexing kernel_ms / kernel_launches. */
+#define CGB_K_PUSH 0   /* push expansion (BFS top-down, SSSP, CC label propagation) */
+#define CGB_K_PULL 1   /* BFS bottom-up */
+#define CGB_K_PR 2     /* PageRank pull iteration */
+#define CGB_K_HOOK 3   /* CC hooking */
+#define CGB_K_COMPRESS 4
+#define CGB_K_FRONTIER 5 /* frontier conversion / bucket split */
+#define CGB_K_INIT 6
+#define CGB_K_OTHER 7
+
+/* One entry per iteration when CGB_FLAG_TRACE is set (features the learned
+ * scheduler is trained on). */
+typedef struct cgb_iter_trace {
+    uint32_t iteration;
+    uint32_t algorithm;
+    uint64_t frontier_vertices;
+    uint64_t frontier_edges;
+    uint64_t unvisited_vertices;
+    uint64_t unvisited_edges;
+    uint32_t max_frontier_degree;
+    int32_t variant;       /* cgb_variant actually run */
+    uint32_t delta;        /* SSSP delta in force */
+    float ms;              /* measured device time of the iteration */
+} cgb_iter_trace;
+
+/* --------------------------------------------------------------- graph */
+
+/* Copies a CSR (host or device pointers) into HBM and checks the invariants
+ * the reference asserts: offsets[0] == 0, offsets non-decreasing,
+ * offsets[V] == E, dest[e] < V; neighbour lists are sorted by dest on the
+ * device (weights follow, as nbrSort_taskSteal does) and must then be
+ * strictly ascending (no duplicate edges).  weight may be NULL (SSSP then
+ * uses weight 1).  no_zero_out_degree_num = 0 means V.  The caller keeps
+ * ownership of its arrays.  Replaces GraphDeviceWorklist's constructor and
+ * csrToDevice() (GraphDevice.cuh:48-71,208-221). */
+cgb_status cgb_graph_create(const uint32_t* offsets, const uint32_t* dest, const uint32_t* weight,
+                            uint32_t V, uint32_t E, uint32_t no_zero_out_degree_num, int device,
+                            cgb_graph** out);
+
+/* Loads the three raw little-endian arrays with load_binFile's size check
+ * (file bytes == length * 4, Basic/Other/IO.hpp:50-52), then as
+ * cgb_graph_create.  weight_path may be NULL. */
+cgb_status cgb_graph_load_files(const char* offsets_path, const char* dest_path, const char* weight_path,
+                                uint32_t V, uint32_t E, int device, cgb_graph** out);
+
+cgb_status cgb_graph_destroy(cgb_graph* g);
+
+/* Runs all later work of this graph on `stream` (a cudaStream_t of the
+ * graph's device; NULL restores the graph's own stream).  Lets a caller
+ * order the engine's kernels with its own work and time them with events on
+ * its stream. */
+cgb_status cgb_graph_set_stream(cgb_graph* g, void* stream);
+
+/* V, E and whether the graph is symmetric (-1 = not yet known). */
+cgb_status cgb_graph_info(const cgb_graph* g, uint32_t* V, uint32_t* E, int32_t* symmetric);
+
+/* Device pointers of the resident CSR and of the last run's result
+ * (uint32[V] for BFS/SSSP/CC, double[V] for PR). */
+cgb_status cgb_graph_device_csr(const cgb_graph* g, const uint32_t** offsets, const uint32_t** dest,
+                                const uint32_t** weight);
+cgb_status cgb_graph_result_device(const cgb_graph* g, const void** values);
+
+/* Copies the last run's result (V uint32, or V double after PageRank) to a
+ * host or device buffer.  Replaces GraphDeviceWorklist::result_D2H()
+ * (GraphDevice.cuh:259-262). */
+cgb_status cgb_graph_result_download(const cgb_graph* g, void* values);
+
+/* ----------------------------------------------------------------- run */
+
+/* One run of `algorithm` (cgb_algorithm).  For BFS/SSSP root_or_iters is the
+ * root (< V); for CC it is ignored; for PR it is the iteration count, as in
+ * graphProcess_device (GraphDevice.cuh:159-162: at least one iteration).
+ * Results: out_u32 (V entries, BFS/SSSP/CC; CGB_VALUE_MAX = unreachable) or
+ * out_f64 (V entries, PR); either may be NULL to keep the result on the
+ * device only.  out_ms (may be NULL) receives the device time of the run,
+ * the quantity graphProcess_device returns.  Calls on one graph serialise. */
+cgb_status cgb_run(cgb_graph* g, int algorithm, uint32_t root_or_iters, const cgb_options* opt,
+                   uint32_t* out_u32, double* out_f64, double* out_ms);
+
+/* Several roots of BFS or SSSP in one call; out_u32 holds nroots * V values
+ * (root-major).  Results equal nroots separate cgb_run calls. */
+cgb_status cgb_run_batch(cgb_graph* g, int algorithm, const uint32_t* roots, uint32_t nroots,
+                         const cgb_options* opt, uint32_t* out_u32, double* out_ms);
+
+cgb_status cgb_run_stats_get(const cgb_graph* g, cgb_run_stats* out);
+
+/* Copies up to max_entries trace entries of the last traced run; *count
+ * receives the number available. */
+cgb_status cgb_trace_get(const cgb_graph* g, cgb_iter_trace* out, uint32_t max_entries, uint32_t* count);
+
+/* ---------------------------------------------------------------- misc */
+
+const char* cgb_last_error_string(void);
+const char* cgb_status_string(cgb_status s);
+int cgb_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CGB200_H */

@@ -1,0 +1,343 @@
+/*
+ * Oracle (TEST INFRASTRUCTURE ONLY).  A plain serial C restatement of what
+ * the reference computes for BFS, SSSP, WCC and PageRank, plus a CPU twin of
+ * the engine's synthetic-graph generators.  Only tests/, the smoke check and
+ * the CPU-baseline leg of the benchmark load this library; the engine never
+ * does.
+ *
+ * Conventions followed (reference = PengBo410/CGgraph, paths under CGgraph/):
+ *  - every id, offset, weight and result is uint32
+ *    (Basic/Type/data_type.hpp:6-15);
+ *  - "unreachable" is VertexValue_MAX = 999999999 (Basic/Graph/basic_def.hpp:18);
+ *  - BFS: root = 0, level = parent level + 1
+ *    (my_project/CGgraph/host_algorithm.hpp:169-177);
+ *  - SSSP: dist = min over in-edges of dist[u] + w, applied only when it is
+ *    below the current value (host_algorithm.hpp:277-300, device_algorithm.cuh:317-319),
+ *    so a vertex whose shortest path is >= 999999999 keeps 999999999;
+ *  - CC: label0 = vertex id, labels pushed along OUT-edges with min
+ *    (GraphNuma.cuh:539-544, host_algorithm.hpp:412-433).  On a directed
+ *    graph the fixpoint is label[v] = min{u : u reaches v}; on a symmetric
+ *    graph it is the minimum vertex id of v's weakly connected component;
+ *  - PageRank: pr0 = 1/N, pr' = 0.15/N + 0.85 * sum_{u->v} pr[u]/outdeg[u],
+ *    no dangling redistribution (GraphNuma.cuh:233-244,545-554,
+ *    device_algorithm.cuh:543), evaluated here in FP64 because the
+ *    reference's own PageRank is uint32 and does not build.
+ *
+ * Build: cc -O2 -fopenmp -shared -fPIC cgb_oracle.c -o liboracle.so
+ */
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define ORA_MAX 999999999u
+
+/* ------------------------------------------------------------------ BFS */
+/* Queue BFS; the level-synchronous fixpoint of the reference's write_min
+ * relaxation (host_algorithm.hpp:164-184). */
+int ora_bfs(uint32_t V, const uint32_t* off, const uint32_t* dst, uint32_t root, uint32_t* out)
+{
+    if (root >= V) return -1;
+    uint32_t* q = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)V);
+    if (!q) return -2;
+    for (uint32_t i = 0; i < V; i++) out[i] = ORA_MAX;
+    size_t head = 0, tail = 0;
+    out[root] = 0;
+    q[tail++] = root;
+    while (head < tail) {
+        uint32_t u = q[head++];
+        uint32_t l = out[u] + 1;
+        for (uint32_t e = off[u]; e < off[u + 1]; e++) {
+            uint32_t d = dst[e];
+            if (out[d] == ORA_MAX) { out[d] = l; q[tail++] = d; }
+        }
+    }
+    free(q);
+    return 0;
+}
+
+/* ----------------------------------------------------------------- SSSP */
+/* Dijkstra with a binary heap keyed by (dist << 32 | vertex). */
+typedef struct { uint64_t* a; size_t n, cap; } heap_t;
+static int heap_push(heap_t* h, uint64_t k)
+{
+    if (h->n == h->cap) {
+        size_t nc = h->cap ? h->cap * 2 : 1024;
+        uint64_t* na = (uint64_t*)realloc(h->a, nc * sizeof(uint64_t));
+        if (!na) return -1;
+        h->a = na; h->cap = nc;
+    }
+    size_t i = h->n++;
+    while (i > 0) {
+        size_t p = (i - 1) / 2;
+        if (h->a[p] <= k) break;
+        h->a[i] = h->a[p];
+        i = p;
+    }
+    h->a[i] = k;
+    return 0;
+}
+static uint64_t heap_pop(heap_t* h)
+{
+    uint64_t top = h->a[0];
+    uint64_t last = h->a[--h->n];
+    size_t i = 0;
+    for (;;) {
+        size_t c = 2 * i + 1;
+        if (c >= h->n) break;
+        if (c + 1 < h->n && h->a[c + 1] < h->a[c]) c++;
+        if (h->a[c] >= last) break;
+        h->a[i] = h->a[c];
+        i = c;
+    }
+    if (h->n) h->a[i] = last;
+    return top;
+}
+
+int ora_sssp(uint32_t V, const uint32_t* off, const uint32_t* dst, const uint32_t* w, uint32_t root, uint32_t* out)
+{
+    if (root >= V) return -1;
+    heap_t h = {0, 0, 0};
+    for (uint32_t i = 0; i < V; i++) out[i] = ORA_MAX;
+    out[root] = 0;
+    if (heap_push(&h, (uint64_t)root)) return -2;
+    while (h.n) {
+        uint64_t k = heap_pop(&h);
+        uint32_t u = (uint32_t)k;
+        uint32_t du = (uint32_t)(k >> 32);
+        if (du != out[u]) continue;
+        for (uint32_t e = off[u]; e < off[u + 1]; e++) {
+            uint64_t nd = (uint64_t)du + (uint64_t)w[e];
+            uint32_t d = dst[e];
+            if (nd < (uint64_t)out[d]) {
+                out[d] = (uint32_t)nd;
+                if (heap_push(&h, (nd << 32) | d)) { free(h.a); return -2; }
+            }
+        }
+    }
+    free(h.a);
+    return 0;
+}
+
+/* ------------------------------------------------------------------- CC */
+/* Reference CC semantics on any directed graph: label[v] = min{u : u ~> v}.
+ * Visiting sources in increasing id order, a BFS from u claims every vertex
+ * not yet claimed by a smaller source; each vertex is claimed once. */
+int ora_cc(uint32_t V, const uint32_t* off, const uint32_t* dst, uint32_t* out)
+{
+    uint32_t* q = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)(V ? V : 1));
+    if (!q) return -2;
+    for (uint32_t i = 0; i < V; i++) out[i] = ORA_MAX;
+    for (uint32_t s = 0; s < V; s++) {
+        if (out[s] != ORA_MAX) continue;
+        size_t head = 0, tail = 0;
+        out[s] = s;
+        q[tail++] = s;
+        while (head < tail) {
+            uint32_t u = q[head++];
+            for (uint32_t e = off[u]; e < off[u + 1]; e++) {
+                uint32_t d = dst[e];
+                if (out[d] == ORA_MAX) { out[d] = s; q[tail++] = d; }
+            }
+        }
+    }
+    free(q);
+    return 0;
+}
+
+/* Union-find restatement for symmetric graphs (min id of each component);
+ * an independent second check of ora_cc on symmetrised inputs. */
+static uint32_t uf_find(uint32_t* p, uint32_t x)
+{
+    while (p[x] != x) { p[x] = p[p[x]]; x = p[x]; }
+    return x;
+}
+int ora_wcc_unionfind(uint32_t V, const uint32_t* off, const uint32_t* dst, uint32_t* out)
+{
+    for (uint32_t i = 0; i < V; i++) out[i] = i;
+    for (uint32_t u = 0; u < V; u++)
+        for (uint32_t e = off[u]; e < off[u + 1]; e++) {
+            uint32_t a = uf_find(out, u), b = uf_find(out, dst[e]);
+            if (a < b) out[b] = a; else if (b < a) out[a] = b;
+        }
+    for (uint32_t i = 0; i < V; i++) out[i] = uf_find(out, i);
+    return 0;
+}
+
+/* ------------------------------------------------------------- PageRank */
+/* Serial FP64 push, in vertex order. */
+int ora_pagerank(uint32_t V, const uint32_t* off, const uint32_t* dst, uint32_t iters, double* out)
+{
+    if (V == 0) return 0;
+    double* acc = (double*)malloc(sizeof(double) * (size_t)V);
+    if (!acc) return -2;
+    const double N = (double)V;
+    for (uint32_t i = 0; i < V; i++) out[i] = 1.0 / N;
+    for (uint32_t it = 0; it < iters; it++) {
+        memset(acc, 0, sizeof(double) * (size_t)V);
+        for (uint32_t u = 0; u < V; u++) {
+            uint32_t deg = off[u + 1] - off[u];
+            if (!deg) continue;
+            double c = out[u] / (double)deg;
+            for (uint32_t e = off[u]; e < off[u + 1]; e++) acc[dst[e]] += c;
+        }
+        for (uint32_t v = 0; v < V; v++) out[v] = 0.15 / N + 0.85 * acc[v];
+    }
+    free(acc);
+    return 0;
+}
+
+/* OpenMP FP64 pull over a CSC (in_off/in_src), used as the timed CPU
+ * baseline for PageRank since the reference's own PageRank does not build. */
+int ora_pagerank_pull_omp(uint32_t V, const uint32_t* off, const uint32_t* in_off, const uint32_t* in_src,
+                          uint32_t iters, int threads, double* out)
+{
+    if (V == 0) return 0;
+    double* contrib = (double*)malloc(sizeof(double) * (size_t)V);
+    if (!contrib) return -2;
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#else
+    (void)threads;
+#endif
+    const double N = (double)V;
+    int64_t n = (int64_t)V;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; i++) out[i] = 1.0 / N;
+    for (uint32_t it = 0; it < iters; it++) {
+#pragma omp parallel for schedule(static)
+        for (int64_t u = 0; u < n; u++) {
+            uint32_t deg = off[u + 1] - off[u];
+            contrib[u] = deg ? out[u] / (double)deg : 0.0;
+        }
+#pragma omp parallel for schedule(dynamic, 4096)
+        for (int64_t v = 0; v < n; v++) {
+            double s = 0.0;
+            for (uint32_t e = in_off[v]; e < in_off[v + 1]; e++) s += contrib[in_src[e]];
+            out[v] = 0.15 / N + 0.85 * s;
+        }
+    }
+    free(contrib);
+    return 0;
+}
+
+int ora_num_threads(void)
+{
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+/* ----------------------------------------------- graph construction twin */
+/* CPU twin of the engine's generators, to check them on small sizes.
+ * splitmix64 finaliser (Steele, Lea, Flood 2014; public-domain constants). */
+static inline uint64_t mix64(uint64_t z)
+{
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+/* Bijective scramble of scale-bit vertex ids: odd multiply, xor-shift, odd
+ * multiply, add, all modulo 2^scale. */
+static inline uint32_t scramble(uint64_t x, uint32_t scale, uint64_t m1, uint64_t m2, uint64_t c)
+{
+    uint64_t mask = (scale >= 64) ? ~0ull : ((1ull << scale) - 1);
+    uint32_t sh = scale / 2 ? scale / 2 : 1;
+    x = (x * m1) & mask;
+    x ^= x >> sh;
+    x = (x * m2 + c) & mask;
+    return (uint32_t)x;
+}
+
+/* RMAT edge i of a (seed, scale) stream, quadrant thresholds t1<t2<t3 in
+ * units of 2^-32; optionally scrambled.  Mirrors the device generator. */
+void ora_rmat_edges(uint32_t scale, uint64_t nedges, uint64_t seed, uint64_t t1, uint64_t t2, uint64_t t3,
+                    int do_scramble, uint32_t* src, uint32_t* dst)
+{
+    uint64_t m1 = mix64(seed ^ 0x5C0A11ull) | 1ull;
+    uint64_t m2 = mix64(seed ^ 0x5C0A12ull) | 1ull;
+    uint64_t c = mix64(seed ^ 0x5C0A13ull);
+    uint64_t s = mix64(seed);
+    for (uint64_t i = 0; i < nedges; i++) {
+        uint64_t u = 0, v = 0;
+        for (uint32_t l = 0; l < scale; l++) {
+            uint64_t r = mix64(s ^ mix64(i * 64 + l)) >> 32;
+            uint64_t bu = r >= t2, bv = (r >= t1 && r < t2) || r >= t3;
+            u = (u << 1) | bu;
+            v = (v << 1) | bv;
+        }
+        if (do_scramble) { u = scramble(u, scale, m1, m2, c); v = scramble(v, scale, m1, m2, c); }
+        src[i] = (uint32_t)u;
+        dst[i] = (uint32_t)v;
+    }
+}
+
+static int cmp_u64(const void* a, const void* b)
+{
+    uint64_t x = *(const uint64_t*)a, y = *(const uint64_t*)b;
+    return (x > y) - (x < y);
+}
+
+/* Edge list -> CSR: drops self-loops, optionally adds reverse edges, sorts
+ * by (src, dst), removes duplicates.  Returns E, or -1 on allocation failure.
+ * off must hold V+1 entries; dst_out must hold (symmetrise ? 2 : 1) * n entries. */
+int64_t ora_build_csr(uint32_t V, uint64_t n, const uint32_t* src, const uint32_t* dst, int symmetrise,
+                      uint32_t* off, uint32_t* dst_out)
+{
+    uint64_t cap = symmetrise ? 2 * n : n;
+    uint64_t* k = (uint64_t*)malloc(sizeof(uint64_t) * (cap ? cap : 1));
+    if (!k) return -1;
+    uint64_t m = 0;
+    for (uint64_t i = 0; i < n; i++) {
+        if (src[i] == dst[i]) continue;
+        k[m++] = ((uint64_t)src[i] << 32) | dst[i];
+        if (symmetrise) k[m++] = ((uint64_t)dst[i] << 32) | src[i];
+    }
+    qsort(k, m, sizeof(uint64_t), cmp_u64);
+    uint64_t E = 0;
+    for (uint64_t i = 0; i < m; i++)
+        if (i == 0 || k[i] != k[i - 1]) k[E++] = k[i];
+    memset(off, 0, sizeof(uint32_t) * ((size_t)V + 1));
+    for (uint64_t i = 0; i < E; i++) { off[(k[i] >> 32) + 1]++; dst_out[i] = (uint32_t)k[i]; }
+    for (uint32_t v = 0; v < V; v++) off[v + 1] += off[v];
+    free(k);
+    return (int64_t)E;
+}
+
+/* Edge weight in [1, wmax] from a hash of (seed, edge); symmetric edges get
+ * the same weight in both directions when sym_key is set. */
+void ora_edge_weights(uint32_t V, const uint32_t* off, const uint32_t* dst, uint64_t seed, uint32_t wmax,
+                      int sym_key, uint32_t* w)
+{
+    uint64_t s = mix64(seed ^ 0x77E16ull);
+    for (uint32_t u = 0; u < V; u++)
+        for (uint32_t e = off[u]; e < off[u + 1]; e++) {
+            uint32_t a = u, b = dst[e];
+            if (sym_key && b < a) { uint32_t t = a; a = b; b = t; }
+            uint64_t h = mix64(s ^ (((uint64_t)a << 32) | b));
+            w[e] = 1u + (uint32_t)(h % wmax);
+        }
+}
+
+/* rows x cols 4-neighbour grid in CSR order (neighbours ascending). */
+int64_t ora_grid_csr(uint32_t rows, uint32_t cols, uint32_t* off, uint32_t* dst)
+{
+    uint64_t e = 0;
+    for (uint32_t r = 0; r < rows; r++)
+        for (uint32_t c = 0; c < cols; c++) {
+            uint32_t v = r * cols + c;
+            off[v] = (uint32_t)e;
+            if (r > 0) dst[e++] = v - cols;
+            if (c > 0) dst[e++] = v - 1;
+            if (c + 1 < cols) dst[e++] = v + 1;
+            if (r + 1 < rows) dst[e++] = v + cols;
+        }
+    off[(uint64_t)rows * cols] = (uint32_t)e;
+    return (int64_t)e;
+}

@@ -1,0 +1,259 @@
+"""Oracle bindings (TEST INFRASTRUCTURE ONLY).
+
+Two independent checkers for the engine's results, never used by the engine:
+
+* ``liboracle.so`` -- the serial C restatement in ``cgb_oracle.c`` (queue BFS,
+  Dijkstra, reference-semantics CC, union-find WCC, FP64 PageRank) plus the CPU
+  twin of the synthetic-graph generators;
+* ``_ref/cgref_oracle`` -- the reference's own MULTI_CORE engine
+  (Graph_Numa, my_project/CGgraph/GraphNuma.cuh:9-698) built from the reference
+  sources by ``build_ref.sh``; it reads the CSR as the three raw files of
+  load_binFile (Basic/Other/IO.hpp:44-92).
+
+Only tests/, the smoke check and the benchmark's CPU-baseline leg import this.
+"""
+from __future__ import annotations
+
+import ctypes
+import json
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+REF_BIN = os.path.join(HERE, "_ref", "cgref_oracle")
+VALUE_MAX = 999999999
+
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+_f64p = ctypes.POINTER(ctypes.c_double)
+
+
+def build(force: bool = False) -> str:
+    """Compile cgb_oracle.c into liboracle.so (gcc + OpenMP)."""
+    src = os.path.join(HERE, "cgb_oracle.c")
+    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
+        tmp = LIB_PATH + ".tmp"
+        subprocess.check_call(["gcc", "-O2", "-fopenmp", "-shared", "-fPIC", src, "-o", tmp])
+        os.replace(tmp, LIB_PATH)
+    return LIB_PATH
+
+
+def build_ref(reference_root: str = "/root/reference") -> str | None:
+    """Build the reference CPU engine harness when the reference is present."""
+    script = os.path.join(HERE, "build_ref.sh")
+    if os.path.isdir(os.path.join(reference_root, "CGgraph")):
+        subprocess.check_call(["bash", script, reference_root])
+    return REF_BIN if os.path.exists(REF_BIN) else None
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        L.ora_bfs.argtypes = [ctypes.c_uint32, _u32p, _u32p, ctypes.c_uint32, _u32p]
+        L.ora_sssp.argtypes = [ctypes.c_uint32, _u32p, _u32p, _u32p, ctypes.c_uint32, _u32p]
+        L.ora_cc.argtypes = [ctypes.c_uint32, _u32p, _u32p, _u32p]
+        L.ora_wcc_unionfind.argtypes = [ctypes.c_uint32, _u32p, _u32p, _u32p]
+        L.ora_pagerank.argtypes = [ctypes.c_uint32, _u32p, _u32p, ctypes.c_uint32, _f64p]
+        L.ora_pagerank_pull_omp.argtypes = [ctypes.c_uint32, _u32p, _u32p, _u32p, ctypes.c_uint32,
+                                            ctypes.c_int, _f64p]
+        L.ora_num_threads.restype = ctypes.c_int
+        L.ora_rmat_edges.argtypes = [ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64,
+                                     ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, _u32p, _u32p]
+        L.ora_build_csr.argtypes = [ctypes.c_uint32, ctypes.c_uint64, _u32p, _u32p, ctypes.c_int, _u32p, _u32p]
+        L.ora_build_csr.restype = ctypes.c_int64
+        L.ora_edge_weights.argtypes = [ctypes.c_uint32, _u32p, _u32p, ctypes.c_uint64, ctypes.c_uint32,
+                                       ctypes.c_int, _u32p]
+        L.ora_grid_csr.argtypes = [ctypes.c_uint32, ctypes.c_uint32, _u32p, _u32p]
+        L.ora_grid_csr.restype = ctypes.c_int64
+        for f in (L.ora_bfs, L.ora_sssp, L.ora_cc, L.ora_wcc_unionfind, L.ora_pagerank, L.ora_pagerank_pull_omp):
+            f.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def _p(a, t=_u32p):
+    return a.ctypes.data_as(t)
+
+
+def _u32(a):
+    return np.ascontiguousarray(a, dtype=np.uint32)
+
+
+def bfs(off, dst, root):
+    off, dst = _u32(off), _u32(dst)
+    V = off.size - 1
+    out = np.empty(V, np.uint32)
+    assert lib().ora_bfs(V, _p(off), _p(dst), root, _p(out)) == 0
+    return out
+
+
+def sssp(off, dst, w, root):
+    off, dst, w = _u32(off), _u32(dst), _u32(w)
+    V = off.size - 1
+    out = np.empty(V, np.uint32)
+    assert lib().ora_sssp(V, _p(off), _p(dst), _p(w), root, _p(out)) == 0
+    return out
+
+
+def cc(off, dst):
+    off, dst = _u32(off), _u32(dst)
+    V = off.size - 1
+    out = np.empty(V, np.uint32)
+    assert lib().ora_cc(V, _p(off), _p(dst), _p(out)) == 0
+    return out
+
+
+def wcc_unionfind(off, dst):
+    off, dst = _u32(off), _u32(dst)
+    V = off.size - 1
+    out = np.empty(V, np.uint32)
+    assert lib().ora_wcc_unionfind(V, _p(off), _p(dst), _p(out)) == 0
+    return out
+
+
+def pagerank(off, dst, iters=20):
+    off, dst = _u32(off), _u32(dst)
+    V = off.size - 1
+    out = np.empty(V, np.float64)
+    assert lib().ora_pagerank(V, _p(off), _p(dst), iters, _p(out, _f64p)) == 0
+    return out
+
+
+def csc(off, dst):
+    """In-edge CSC (in_off, in_src) with ascending sources, by counting sort."""
+    off, dst = _u32(off), _u32(dst)
+    V = off.size - 1
+    src = np.repeat(np.arange(V, dtype=np.uint32), np.diff(off.astype(np.int64)))
+    order = np.lexsort((src, dst))
+    in_src = src[order].astype(np.uint32)
+    in_off = np.zeros(V + 1, np.uint32)
+    np.cumsum(np.bincount(dst, minlength=V), out=in_off[1:])
+    return in_off, in_src
+
+
+def pagerank_pull_omp(off, in_off, in_src, iters=20, threads=0):
+    off, in_off, in_src = _u32(off), _u32(in_off), _u32(in_src)
+    V = off.size - 1
+    out = np.empty(V, np.float64)
+    assert lib().ora_pagerank_pull_omp(V, _p(off), _p(in_off), _p(in_src), iters, threads, _p(out, _f64p)) == 0
+    return out
+
+
+def num_threads() -> int:
+    return int(lib().ora_num_threads())
+
+
+# ------------------------------------------------------------ generator twin
+RMAT_ABC = (0.57, 0.19, 0.19)
+
+
+def rmat_thresholds(a=0.57, b=0.19, c=0.19):
+    """Quadrant thresholds in units of 2^-32 (floor), shared with the engine."""
+    t1 = int(a * 2**32)
+    t2 = int((a + b) * 2**32)
+    t3 = int((a + b + c) * 2**32)
+    return t1, t2, t3
+
+
+def rmat_edges(scale, edge_factor, seed, scramble=True, abc=RMAT_ABC):
+    n = edge_factor << scale
+    src = np.empty(n, np.uint32)
+    dst = np.empty(n, np.uint32)
+    t1, t2, t3 = rmat_thresholds(*abc)
+    lib().ora_rmat_edges(scale, n, seed, t1, t2, t3, int(scramble), _p(src), _p(dst))
+    return src, dst
+
+
+def build_csr(V, src, dst, symmetrise=False):
+    src, dst = _u32(src), _u32(dst)
+    off = np.empty(V + 1, np.uint32)
+    out = np.empty(max(1, (2 if symmetrise else 1) * src.size), np.uint32)
+    E = lib().ora_build_csr(V, src.size, _p(src), _p(dst), int(symmetrise), _p(off), _p(out))
+    assert E >= 0
+    return off, out[:E].copy()
+
+
+def edge_weights(off, dst, seed, wmax=64, sym_key=False):
+    off, dst = _u32(off), _u32(dst)
+    w = np.empty(dst.size, np.uint32)
+    lib().ora_edge_weights(off.size - 1, _p(off), _p(dst), seed, wmax, int(sym_key), _p(w))
+    return w
+
+
+def rmat_graph(scale, edge_factor=16, seed=1, symmetrise=False, wmax=64, scramble=True):
+    """(off, dst, w) of the seeded RMAT graph, exactly as the engine builds it."""
+    src, dst = rmat_edges(scale, edge_factor, seed, scramble)
+    off, d = build_csr(1 << scale, src, dst, symmetrise)
+    w = edge_weights(off, d, seed, wmax, sym_key=symmetrise)
+    return off, d, w
+
+
+def grid_graph(rows, cols, seed=1, wmax=1000):
+    V = rows * cols
+    off = np.empty(V + 1, np.uint32)
+    dst = np.empty(max(1, 4 * V), np.uint32)
+    E = lib().ora_grid_csr(rows, cols, _p(off), _p(dst))
+    dst = dst[:E].copy()
+    w = edge_weights(off, dst, seed, wmax, sym_key=True)
+    return off, dst, w
+
+
+# ------------------------------------------------- reference engine runner
+def ref_run_files(paths, V, E, alg, roots, runs, threads=0):
+    """Like ref_run on CSR files already written (offsets, dest, weight or
+    None); returns the harness's JSON (ms, edges, threads)."""
+    if not ref_available():
+        raise RuntimeError("reference oracle binary not built (oracle/build_ref.sh)")
+    with tempfile.TemporaryDirectory() as d:
+        out = os.path.join(d, "out.bin")
+        args = [REF_BIN, str(alg), str(V), str(E), paths[0], paths[1], paths[2] or "-",
+                ",".join(str(int(r)) for r in roots), out, str(runs), str(threads)]
+        r = subprocess.run(args, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"cgref_oracle failed ({r.returncode}): {r.stderr[-2000:]}")
+        line = [l for l in r.stdout.splitlines() if l.startswith("{")][-1]
+        return json.loads(line)
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_BIN)
+
+
+def ref_run(off, dst, w, alg, root=0, runs=1, threads=0, tmpdir=None, info_out=None):
+    """Run the reference's Graph_Numa (alg 0=BFS, 1=SSSP, 2=CC) on a CSR.
+
+    `root` may be a list (run i uses root i mod len).  Returns (values
+    uint32[V] of the last run, list of per-run ms as measured by the
+    reference's own timer, threads used); `info_out` (a dict) also receives
+    the per-run traversed-edge counts."""
+    if not ref_available():
+        raise RuntimeError("reference oracle binary not built (oracle/build_ref.sh)")
+    off, dst = _u32(off), _u32(dst)
+    V, E = off.size - 1, dst.size
+    with tempfile.TemporaryDirectory(dir=tmpdir) as d:
+        paths = [os.path.join(d, n) for n in ("off.bin", "dst.bin", "w.bin", "out.bin")]
+        off.tofile(paths[0])
+        dst.tofile(paths[1])
+        if w is not None:
+            _u32(w).tofile(paths[2])
+        roots = ",".join(str(int(r)) for r in (root if isinstance(root, (list, tuple)) else [root]))
+        args = [REF_BIN, str(alg), str(V), str(E), paths[0], paths[1], paths[2] if w is not None else "-",
+                roots, paths[3], str(runs), str(threads)]
+        r = subprocess.run(args, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"cgref_oracle failed ({r.returncode}): {r.stderr[-2000:]}")
+        line = [l for l in r.stdout.splitlines() if l.startswith("{")][-1]
+        info = json.loads(line)
+        vals = np.fromfile(paths[3], np.uint32)
+        if info_out is not None:
+            info_out.update(info)
+    return vals, info["ms"], info["threads"]

@@ -1,0 +1,115 @@
+// Oracle harness (test infrastructure only): drives the reference's own
+// MULTI_CORE CPU engine, Graph_Numa (my_project/CGgraph/GraphNuma.cuh:9-698),
+// on a CSR given as the three raw little-endian files the reference loads
+// with load_binFile (Basic/Other/IO.hpp:44-92).  It is compiled by
+// oracle/build_ref.sh from the reference sources and is only ever used to
+// check and to time the new engine, never as part of it.
+//
+// usage: cgref_oracle <alg> <V> <E> <offsets.bin> <dest.bin> <weight.bin|-> \
+//                     <root[,root...]> <out.bin|-> [runs] [threads]
+//   alg: 0 = BFS, 1 = SSSP, 2 = CC  (Algorithm_type, Basic/Graph/basic_struct.hpp:144-151)
+//   run i uses root i mod (number of roots).
+// Prints one line of JSON: {"alg":..,"runs":..,"ms":[..],"edges":[..],"threads":..},
+// where ms is the reference's own graphProcess time of each run and edges
+// the run's traversed-edge count (sum of out-degrees of reached vertices).
+// The values of the last run (uint32 per vertex, 999999999 = unreachable)
+// are written to out.bin.
+
+#include "Basic/basic_include.cuh"
+#include "my_project/CGgraph/host_algorithm.hpp"
+
+// The reference names these PageRank symbols in Graph_Numa::graphProcess
+// (my_project/CGgraph/GraphNuma.cuh:222,240,259) but defines them nowhere;
+// the harness never runs PageRank through Graph_Numa.
+double alpha = 0.85;
+double beta = 0.15;
+unsigned iteN = 20;
+namespace PR_SPACE {
+template <typename G>
+count_type pr_numa(G&, vertex_id_type, countl_type, countl_type, count_type, bool) { return 0; }
+}  // namespace PR_SPACE
+
+#include "my_project/CGgraph/sortNbr.hpp"
+#include "my_project/CGgraph/GraphNuma.cuh"
+
+#include <cstdio>
+#include <cstdlib>
+#include <string>
+#include <unistd.h>
+#include <vector>
+
+int main(int argc, char** argv)
+{
+    if (argc < 9) {
+        fprintf(stderr, "usage: %s alg V E off dest weight root out [runs] [threads]\n", argv[0]);
+        return 2;
+    }
+    int alg = atoi(argv[1]);
+    uint64_t V = strtoull(argv[2], nullptr, 10);
+    uint64_t E = strtoull(argv[3], nullptr, 10);
+    std::string offPath = argv[4], dstPath = argv[5], wPath = argv[6];
+    std::vector<uint32_t> roots;
+    for (char* p = argv[7]; *p;) {
+        roots.push_back((uint32_t)strtoul(p, &p, 10));
+        if (*p == ',') p++;
+        else if (*p) { fprintf(stderr, "bad root list\n"); return 2; }
+    }
+    std::string outPath = argv[8];
+    int runs = argc > 9 ? atoi(argv[9]) : 1;
+    int threads = argc > 10 ? atoi(argv[10]) : 0;
+    if (threads > 0) reSetThreadNum(threads);
+    bool bad_root = roots.empty();
+    for (uint32_t r : roots) bad_root |= r >= V;
+    if (alg < 0 || alg > 2 || runs < 1 || V == 0 || bad_root) {
+        fprintf(stderr, "bad arguments\n");
+        return 2;
+    }
+
+    CSR_Result_type csr;
+    csr.vertexNum = (count_type)V;
+    csr.edgeNum = (countl_type)E;
+    csr.csr_offset = load_binFile<countl_type>(offPath, V + 1);
+    csr.csr_dest = E ? load_binFile<vertex_id_type>(dstPath, E) : new vertex_id_type[1];
+    if (wPath != "-" && E) {
+        csr.csr_weight = load_binFile<edge_data_type>(wPath, E);
+    } else {
+        csr.csr_weight = new edge_data_type[E ? E : 1];
+        for (uint64_t i = 0; i < E; i++) csr.csr_weight[i] = 1;
+    }
+    csr.noZeroOutDegreeNum = (count_type)V;
+
+    // The reference driver sorts every neighbour list and asserts strictly
+    // ascending destinations before any engine runs (main_partition.hpp:146).
+    nbrSort_taskSteal(csr);
+
+    // Graph_Numa frees the arrays it is given (GraphNuma.cuh:417-419).
+    Graph_Numa* engine = new Graph_Numa(csr);
+    std::string ms = "[", edges = "[";
+    for (int r = 0; r < runs; r++) {
+        double t = engine->graphProcess((Algorithm_type)alg, roots[r % roots.size()]);
+        unsigned long long m = 0;
+        for (uint64_t v = 0; v < V; v++)
+            if (engine->vertexValue[v] != VertexValue_MAX) m += engine->outDegree[v];
+        char buf[96];
+        snprintf(buf, sizeof(buf), "%s%.6f", r ? "," : "", t);
+        ms += buf;
+        snprintf(buf, sizeof(buf), "%s%llu", r ? "," : "", m);
+        edges += buf;
+    }
+    ms += "]";
+    edges += "]";
+
+    if (outPath != "-") {
+        FILE* f = fopen(outPath.c_str(), "wb");
+        if (!f) { fprintf(stderr, "cannot open %s\n", outPath.c_str()); _exit(3); }
+        size_t n = fwrite(engine->vertexValue, sizeof(vertex_data_type), V, f);
+        fclose(f);
+        if (n != V) _exit(3);
+    }
+    printf("\n{\"alg\": %d, \"runs\": %d, \"ms\": %s, \"edges\": %s, \"threads\": %llu}\n", alg, runs,
+           ms.c_str(), edges.c_str(), (unsigned long long)ThreadNum);
+    fflush(stdout);
+    // DoubleBuffer<dense_bitset> frees the frontier bitmaps twice when the
+    // engine is destroyed; leave without running destructors.
+    _exit(0);
+}

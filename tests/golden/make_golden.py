@@ -1,0 +1,71 @@
+"""Generates tests/golden/*.npz from the reference's own CPU engine.
+
+Run in a container where the reference is mounted (it builds
+oracle/_ref/cgref_oracle from the reference sources with
+oracle/build_ref.sh).  Each fixture holds a CSR and the uint32 results the
+reference's Graph_Numa engine (my_project/CGgraph/GraphNuma.cuh) produced on
+it: BFS and SSSP from a few roots, CC.  The toy graphs are the reference's own
+fixtures (Basic/Graph/graphFileList.hpp:514-568); the others are seeded
+synthetic graphs built by the oracle's generator twin.
+
+usage: python tests/golden/make_golden.py [reference root]
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from oracle import oracle as O  # noqa: E402
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+# The reference's toy CSRs (Basic/Graph/graphFileList.hpp:514-568).
+TOY = {
+    "toy_0": (
+        [0, 3, 6, 6, 8, 8, 11, 15, 16, 21, 22, 24, 26],
+        [1, 3, 7, 3, 5, 9, 5, 6, 7, 9, 11, 0, 5, 8, 9, 5, 0, 2, 4, 9, 11, 5, 2, 8, 2, 5],
+        [1, 3, 7, 3, 5, 9, 5, 6, 7, 9, 11, 0, 5, 8, 9, 5, 0, 2, 4, 9, 11, 5, 2, 8, 2, 5],
+    ),
+    "toy_1": (
+        [0, 3, 6, 6, 8, 8, 11, 16, 17, 21, 24, 26, 28],
+        [1, 3, 7, 3, 5, 9, 5, 6, 7, 9, 11, 0, 5, 8, 9, 10, 5, 0, 4, 9, 11, 5, 6, 8, 2, 8, 2, 5],
+        [1, 3, 7, 3, 5, 9, 5, 6, 7, 9, 11, 0, 5, 8, 9, 5, 0, 2, 4, 9, 11, 5, 2, 8, 2, 5, 2, 5],
+    ),
+}
+
+
+def graphs():
+    for name, (off, dst, w) in TOY.items():
+        yield name, np.array(off, np.uint32), np.array(dst, np.uint32), np.array(w, np.uint32), [0, 6, 8]
+    off, dst, w = O.rmat_graph(10, 16, seed=7)
+    deg = np.diff(off.astype(np.int64))
+    yield "rmat10_s7", off, dst, w, [int(deg.argmax()), 1, 77]
+    off, dst, w = O.rmat_graph(10, 16, seed=11, symmetrise=True)
+    deg = np.diff(off.astype(np.int64))
+    yield "rmat10_s11_sym", off, dst, w, [int(deg.argmax()), 5]
+    off, dst, w = O.grid_graph(16, 24, seed=3)
+    yield "grid16x24_s3", off, dst, w, [0, 200]
+
+
+def main():
+    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    O.build()
+    if O.build_ref(ref_root) is None:
+        raise SystemExit("reference oracle unavailable")
+    for name, off, dst, w, roots in graphs():
+        out = {"offsets": off, "dest": dst, "weight": w, "roots": np.array(roots, np.uint32)}
+        for r in roots:
+            out[f"bfs_{r}"], _, _ = O.ref_run(off, dst, w, 0, r, threads=2)
+            out[f"sssp_{r}"], _, _ = O.ref_run(off, dst, w, 1, r, threads=2)
+        out["cc"], _, _ = O.ref_run(off, dst, w, 2, 0, threads=2)
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+        print(name, off.size - 1, dst.size, roots)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,182 @@
+"""Edge cases through the C ABI: empty and tiny graphs, unsorted lists (sorted
+by the engine as nbrSort_taskSteal does), invariant violations (status codes,
+never a fault), hubs that take the split-hub paths, self-loops, reordered
+zero-out-degree tails, missing weights, distance overflow, iteration budget."""
+import numpy as np
+import pytest
+
+import cggraph_b200 as cg
+from cggraph_b200 import CgbError
+from cggraph_b200 import _lib as L
+
+pytestmark = pytest.mark.gpu
+
+BFS, SSSP, CC, PR = 0, 1, 2, 3
+VMAX = 999999999
+
+
+def csr_from_edges(V, edges, weights=None):
+    edges = sorted(set(edges)) if weights is None else edges
+    off = np.zeros(V + 1, np.uint32)
+    for u, _ in edges:
+        off[u + 1] += 1
+    off = np.cumsum(off).astype(np.uint32)
+    dst = np.array([v for _, v in edges], np.uint32)
+    w = None if weights is None else np.array(weights, np.uint32)
+    return off, dst, w
+
+
+def check_all(oracle, off, dst, w, roots, **kw):
+    wt = w if w is not None else np.ones(dst.size, np.uint32)
+    with cg.Graph.from_csr(off, dst, w, **kw) as g:
+        for r in roots:
+            np.testing.assert_array_equal(g.run(BFS, r)[0], oracle.bfs(off, dst, r))
+            np.testing.assert_array_equal(g.run(SSSP, r)[0], oracle.sssp(off, dst, wt, r))
+        np.testing.assert_array_equal(g.run(CC)[0], oracle.cc(off, dst))
+        exp = oracle.pagerank(off, dst, 20)
+        got = g.run(PR, 20)[0]
+        assert np.max(np.abs(got - exp) / exp) <= 1e-6
+
+
+def test_no_edges(oracle):
+    off = np.zeros(6, np.uint32)
+    dst = np.zeros(0, np.uint32)
+    with cg.Graph.from_csr(off, dst, None) as g:
+        assert g.run(BFS, 2)[0].tolist() == [VMAX, VMAX, 0, VMAX, VMAX]
+        assert g.run(SSSP, 4)[0].tolist() == [VMAX, VMAX, VMAX, VMAX, 0]
+        assert g.run(CC)[0].tolist() == [0, 1, 2, 3, 4]
+        np.testing.assert_allclose(g.run(PR, 20)[0], np.full(5, 0.15 / 5), rtol=1e-15)
+    with cg.Graph.from_csr(np.zeros(2, np.uint32), dst, None) as g:
+        assert g.run(BFS, 0)[0].tolist() == [0]
+        assert g.run(CC)[0].tolist() == [0]
+
+
+def test_unsorted_lists_are_sorted_with_weights(oracle):
+    off, dst, w = oracle.rmat_graph(11, 16, seed=8)
+    rng = np.random.default_rng(0)
+    d2, w2 = dst.copy(), w.copy()
+    for v in range(off.size - 1):
+        s, e = int(off[v]), int(off[v + 1])
+        p = rng.permutation(e - s)
+        d2[s:e] = dst[s:e][p]
+        w2[s:e] = w[s:e][p]
+    with cg.Graph.from_csr(off, d2, w2) as g:
+        o3, d3, w3 = g.download()
+        np.testing.assert_array_equal(d3, dst)
+        np.testing.assert_array_equal(w3, w)
+        r = int(np.diff(off.astype(np.int64)).argmax())
+        np.testing.assert_array_equal(g.run(SSSP, r)[0], oracle.sssp(off, dst, w, r))
+
+
+@pytest.mark.parametrize("case", ["dup", "off0", "offV", "nonmono", "idV"])
+def test_invalid_csr_is_rejected(case):
+    off = np.array([0, 2, 3, 4], np.uint32)
+    dst = np.array([1, 2, 0, 1], np.uint32)
+    if case == "dup":
+        dst = np.array([1, 1, 0, 1], np.uint32)
+    elif case == "off0":
+        off = np.array([1, 2, 3, 4], np.uint32)
+    elif case == "offV":
+        off = np.array([0, 2, 3, 3], np.uint32)
+    elif case == "nonmono":
+        off = np.array([0, 3, 2, 4], np.uint32)
+    elif case == "idV":
+        dst = np.array([1, 3, 0, 1], np.uint32)
+    with pytest.raises(CgbError) as ei:
+        cg.Graph.from_csr(off, dst, None, vertexNum=3, edgeNum=4)
+    assert ei.value.status == L.EFORMAT
+
+
+def test_bad_root_and_algorithm():
+    off = np.array([0, 1, 1], np.uint32)
+    with cg.Graph.from_csr(off, np.array([1], np.uint32), None) as g:
+        with pytest.raises(CgbError) as ei:
+            g.run(BFS, 2)
+        assert ei.value.status == L.EINVAL
+        with pytest.raises(CgbError):
+            g.run(7, 0)
+        assert g.run(BFS, 0)[0].tolist() == [0, 1]  # still usable
+
+
+def test_hubs_take_split_paths(oracle):
+    """A 40000-leaf out-hub (split across CTAs), a 3000-neighbour vertex (CTA
+    tier), a 100-neighbour vertex (warp tier) and a 20000-in-edge sink (whole-CTA
+    PageRank row)."""
+    V = 60000
+    edges = [(0, v) for v in range(1, 40001)]
+    edges += [(1, v) for v in range(40001, 43001)]
+    edges += [(2, v) for v in range(43001, 43101)]
+    edges += [(v, 59999) for v in range(20000, 40000)]
+    edges += [(59999, 3)]
+    off, dst, _ = csr_from_edges(V, edges)
+    w = (np.arange(dst.size) % 50 + 1).astype(np.uint32)
+    check_all(oracle, off, dst, w, [0, 1, 20001])
+    # symmetrised: the hook-and-compress CC path splits the hub's list too
+    off, dst, _ = csr_from_edges(V, edges + [(v, u) for u, v in edges])
+    w = (np.arange(dst.size) % 50 + 1).astype(np.uint32)
+    check_all(oracle, off, dst, w, [0, 59999])
+
+
+def test_self_loops_and_zero_weights(oracle):
+    edges = [(0, 0), (0, 1), (1, 1), (1, 2), (2, 0), (3, 3)]
+    off, dst, _ = csr_from_edges(4, edges)
+    w = np.array([5, 0, 3, 0, 1, 9], np.uint32)
+    check_all(oracle, off, dst, w, [0, 3])
+
+
+def test_zero_out_degree_tail(oracle):
+    """noZeroOutDegreeNum < V (the reordered layout whose last vertices have no
+    out-edges, main_partition.hpp:78-103)."""
+    rng = np.random.default_rng(1)
+    V, nz = 3000, 2000
+    edges = set()
+    for _ in range(20000):
+        u = int(rng.integers(0, nz))
+        v = int(rng.integers(0, V))
+        if u != v:
+            edges.add((u, v))
+    off, dst, _ = csr_from_edges(V, sorted(edges))
+    w = rng.integers(1, 64, dst.size).astype(np.uint32)
+    assert off[nz] == dst.size
+    check_all(oracle, off, dst, w, [0, 1999], noZeroOutDegreeNum=nz)
+
+
+def test_missing_weights_mean_unit_weights(oracle):
+    off, dst, _ = oracle.rmat_graph(11, 8, seed=4)
+    with cg.Graph.from_csr(off, dst, None) as g:
+        for r in (0, 9):
+            np.testing.assert_array_equal(g.run(SSSP, r)[0], oracle.bfs(off, dst, r))
+
+
+def test_distance_overflow_stays_unreachable(oracle):
+    # 0 -> 1 -> 2 -> 3 with weights 4e8: dist(3) = 1.2e9 >= VertexValue_MAX
+    off, dst, _ = csr_from_edges(4, [(0, 1), (1, 2), (2, 3)])
+    w = np.array([400000000] * 3, np.uint32)
+    with cg.Graph.from_csr(off, dst, w) as g:
+        got = g.run(SSSP, 0)[0]
+    assert got.tolist() == [0, 400000000, 800000000, VMAX]
+    np.testing.assert_array_equal(got, oracle.sssp(off, dst, w, 0))
+
+
+def test_iteration_budget_is_a_status(oracle):
+    off, dst, w = oracle.grid_graph(1, 50)  # a path: 49 levels
+    with cg.Graph.from_csr(off, dst, w) as g:
+        with pytest.raises(CgbError) as ei:
+            g.run(BFS, 0, cg.make_options(max_iterations=5))
+        assert ei.value.status == L.ETIMEOUT
+        np.testing.assert_array_equal(g.run(BFS, 0)[0], oracle.bfs(off, dst, 0))
+
+
+def test_device_buffers_in_and_out(oracle):
+    import torch
+    off, dst, w = oracle.rmat_graph(10, 16, seed=5)
+    t_off = torch.from_numpy(off.view(np.int32)).cuda()
+    t_dst = torch.from_numpy(dst.view(np.int32)).cuda()
+    t_w = torch.from_numpy(w.view(np.int32)).cuda()
+    with cg.Graph.from_csr(t_off, t_dst, t_w, vertexNum=off.size - 1, edgeNum=dst.size) as g:
+        out = torch.empty(off.size - 1, dtype=torch.int32, device="cuda")
+        g.run(SSSP, 3, out=out)
+        np.testing.assert_array_equal(out.cpu().numpy().view(np.uint32), oracle.sssp(off, dst, w, 3))
+        pin = torch.empty(off.size - 1, dtype=torch.int32).pin_memory()
+        g.run(BFS, 3, out=pin)
+        np.testing.assert_array_equal(pin.numpy().view(np.uint32), oracle.bfs(off, dst, 3))

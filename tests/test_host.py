@@ -1,0 +1,55 @@
+"""Host-side mirror of the reference interface (no GPU needed)."""
+import numpy as np
+import pytest
+
+import cggraph_b200 as cg
+from cggraph_b200 import CgbError
+
+
+def test_enum_values_match_reference():
+    # Basic/Graph/basic_struct.hpp:144-151,165-178
+    assert [int(a) for a in (cg.Algorithm_type.BFS, cg.Algorithm_type.SSSP, cg.Algorithm_type.CC,
+                             cg.Algorithm_type.PR)] == [0, 1, 2, 3]
+    assert int(cg.Engine_type.SINGLE_GPU) == 4 and int(cg.Engine_type.MULTI_CORE) == 3
+    assert int(cg.OrderMethod.RCM_LAST_ZERO_OUTDEGREE) == 6 and int(cg.OrderMethod.IN_DEGREE_DEC) == 21
+    assert cg.VertexValue_MAX == 999999999
+
+
+def test_load_bin_file_checks_size(tmp_path):
+    p = tmp_path / "a.bin"
+    np.arange(5, dtype=np.uint32).tofile(p)
+    np.testing.assert_array_equal(cg.load_binFile(str(p), 5), np.arange(5))
+    with pytest.raises(CgbError):
+        cg.load_binFile(str(p), 4)
+    with pytest.raises(CgbError):
+        cg.load_binFile(str(tmp_path / "missing.bin"), 4)
+    cg.save_binArray(str(tmp_path / "b.bin"), np.arange(3, dtype=np.uint32))
+    assert (tmp_path / "b.bin").stat().st_size == 12
+
+
+def test_trimmed_mean():
+    # main_partition.hpp:347-365
+    assert cg.trimmed_mean_ms([5.0, 1.0, 3.0, 100.0]) == 4.0
+    assert cg.trimmed_mean_ms([2.0, 4.0]) == 3.0
+    assert cg.trimmed_mean_ms([7.0]) == 7.0
+
+
+def test_check_bin_result(tmp_path):
+    ref = np.array([0, 1, 2, 999999999], np.uint32)
+    cg.checkBinResult(ref, ref.copy(), 4)
+    p = tmp_path / "g.bin"
+    ref.tofile(p)
+    cg.checkBinResult(str(p), ref.copy(), 4)
+    bad = ref.copy()
+    bad[2] = 5
+    with pytest.raises(AssertionError, match=r"current_array\[2\]"):
+        cg.checkBinResult(ref, bad, 4)
+    # reordered graph: current array indexed through old2new (util.cuh:88-112)
+    old2new = np.array([3, 2, 1, 0])
+    cg.checkBinResult(ref, ref[::-1].copy(), 4, cg.OrderMethod.RCM, old2new)
+
+
+def test_only_single_gpu_engine_is_provided():
+    csr = cg.CSR_Result_type(2, 1, np.array([0, 1, 1], np.uint32), np.array([1], np.uint32), None)
+    with pytest.raises(CgbError, match="SINGLE_GPU"):
+        cg.main_partition(csr, cg.Algorithm_type.BFS, 0, engine_type=cg.Engine_type.COORDINATION)

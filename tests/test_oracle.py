@@ -1,0 +1,91 @@
+"""The oracle (serial C restatement) pinned against the reference's own
+engine: the toy known answers and the golden fixtures that
+tests/golden/make_golden.py produced with Graph_Numa."""
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, load_golden
+
+VMAX = 999999999
+
+
+def test_toy0_known_answers(oracle):
+    g = load_golden("toy_0")
+    off, dst, w = g["offsets"], g["dest"], g["weight"]
+    assert oracle.bfs(off, dst, 0).tolist() == [0, 1, 4, 1, 4, 2, 2, 1, 3, 2, VMAX, 3]
+    assert oracle.sssp(off, dst, w, 0).tolist() == [0, 1, 19, 3, 21, 6, 9, 7, 17, 10, VMAX, 17]
+    assert oracle.cc(off, dst).tolist() == [0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 10, 0]
+
+
+@pytest.mark.parametrize("name", GOLDEN)
+def test_oracle_matches_reference_golden(oracle, name):
+    g = load_golden(name)
+    off, dst, w = g["offsets"], g["dest"], g["weight"]
+    for r in g["roots"].tolist():
+        np.testing.assert_array_equal(oracle.bfs(off, dst, r), g[f"bfs_{r}"])
+        np.testing.assert_array_equal(oracle.sssp(off, dst, w, r), g[f"sssp_{r}"])
+    np.testing.assert_array_equal(oracle.cc(off, dst), g["cc"])
+
+
+def test_unionfind_equals_labelprop_on_symmetric(oracle):
+    g = load_golden("rmat10_s11_sym")
+    a = oracle.cc(g["offsets"], g["dest"])
+    b = oracle.wcc_unionfind(g["offsets"], g["dest"])
+    np.testing.assert_array_equal(a, b)
+
+
+def test_pagerank_push_equals_pull(oracle):
+    g = load_golden("rmat10_s7")
+    off, dst = g["offsets"], g["dest"]
+    p1 = oracle.pagerank(off, dst, 20)
+    io, isrc = oracle.csc(off, dst)
+    p2 = oracle.pagerank_pull_omp(off, io, isrc, 20, threads=2)
+    assert np.max(np.abs(p1 - p2) / p1) < 1e-12
+    # one more hand-checked property: with no in-edges pr = 0.15/N
+    indeg = np.bincount(dst, minlength=off.size - 1)
+    N = off.size - 1
+    assert np.allclose(p1[indeg == 0], 0.15 / N)
+
+
+def test_pagerank_tiny_by_hand(oracle):
+    # 0 -> 1, 1 -> 0, 1 -> 2 ; N = 3
+    off = np.array([0, 1, 3, 3], np.uint32)
+    dst = np.array([1, 0, 2], np.uint32)
+    pr = np.full(3, 1 / 3)
+    for _ in range(5):
+        new = np.full(3, 0.15 / 3)
+        new[1] += 0.85 * pr[0]
+        new[0] += 0.85 * pr[1] / 2
+        new[2] += 0.85 * pr[1] / 2
+        pr = new
+    np.testing.assert_allclose(oracle.pagerank(off, dst, 5), pr, rtol=1e-15)
+
+
+def test_reference_live_on_new_seed(oracle):
+    """The reference engine itself, run here on a graph no fixture holds."""
+    if not oracle.ref_available():
+        pytest.skip("reference oracle binary not built (needs the reference sources)")
+    off, dst, w = oracle.rmat_graph(12, 8, seed=123)
+    root = int(np.diff(off.astype(np.int64)).argmax())
+    for alg, mine in ((0, oracle.bfs(off, dst, root)), (1, oracle.sssp(off, dst, w, root)), (2, oracle.cc(off, dst))):
+        ref, ms, threads = oracle.ref_run(off, dst, w, alg, root, threads=2)
+        np.testing.assert_array_equal(mine, ref)
+
+
+def test_generator_twin_properties(oracle):
+    for sym in (False, True):
+        off, dst, w = oracle.rmat_graph(11, 16, seed=5, symmetrise=sym)
+        V = off.size - 1
+        assert off[0] == 0 and off[-1] == dst.size and np.all(np.diff(off.astype(np.int64)) >= 0)
+        src = np.repeat(np.arange(V), np.diff(off.astype(np.int64)))
+        assert np.all(src != dst), "self-loop"
+        key = src.astype(np.int64) * V + dst
+        assert np.all(np.diff(key) > 0), "not sorted / duplicate"
+        assert w.min() >= 1 and w.max() <= 64
+        if sym:
+            rk = dst.astype(np.int64) * V + src
+            order = np.argsort(rk)
+            np.testing.assert_array_equal(rk[order], key)
+            np.testing.assert_array_equal(w[order], w)
+    off, dst, w = oracle.grid_graph(5, 7)
+    assert off.size == 36 and dst.size == 2 * (5 * 6 + 4 * 7)
