@@ -28,7 +28,8 @@ namespace cgb {
 //   __device__ void edge(bool valid, uint32_t e, uint32_t msg) const;   // warp-collective
 template <class Op, bool kIdentity>
 __global__ void __launch_bounds__(kBlock) k_push_twc(const uint32_t* __restrict__ qin, uint32_t nin, Op op,
-                                                     uint32_t* __restrict__ huge_q, uint32_t* huge_len)
+                                                     uint32_t* __restrict__ huge_q, uint32_t* huge_len,
+                                                     uint32_t huge_cap)
 {
     __shared__ uint32_t s_scan[kBlock / 32 + 1];
     __shared__ uint32_t s_owner, s_start, s_deg, s_msg;
@@ -43,8 +44,9 @@ __global__ void __launch_bounds__(kBlock) k_push_twc(const uint32_t* __restrict_
             uint32_t v = kIdentity ? i : qin[i];
             if (!op.load(v, start, deg, msg)) deg = 0;
             if (deg >= kHugeDeg) {
-                uint32_t slot = atomicAdd(huge_len, 1u);
-                huge_q[slot] = v;  // capacity V: each vertex appears once per frontier
+                // capacity V: each vertex appears at most once per frontier
+                const uint32_t slot = atomicAdd(huge_len, 1u);
+                if (slot < huge_cap) huge_q[slot] = v;
                 deg = 0;
             }
         }
@@ -96,9 +98,9 @@ __global__ void __launch_bounds__(kBlock) k_push_twc(const uint32_t* __restrict_
 // vertices is dealt round-robin to the CTAs of the grid.
 template <class Op>
 __global__ void __launch_bounds__(kBlock) k_push_huge(const uint32_t* __restrict__ huge_q, const uint32_t* huge_len,
-                                                      Op op)
+                                                      uint32_t huge_cap, Op op)
 {
-    const uint32_t n = *huge_len;
+    const uint32_t n = min(*huge_len, huge_cap);
     uint64_t chunk_base = 0;
     for (uint32_t h = 0; h < n; h++) {
         const uint32_t v = huge_q[h];
@@ -123,9 +125,11 @@ inline void launch_push_twc(cgb_graph* g, const uint32_t* qin, uint32_t nin, con
     if (nin == 0) return;
     const uint32_t grid = grid_for(nin, kBlock, kNumSMs * 8);
     g->stats.launches += 2;
-    if (identity) k_push_twc<Op, true><<<grid, kBlock, 0, g->stream>>>(qin, nin, op, g->huge_q, &g->ctr->huge_len);
-    else k_push_twc<Op, false><<<grid, kBlock, 0, g->stream>>>(qin, nin, op, g->huge_q, &g->ctr->huge_len);
-    k_push_huge<Op><<<kNumSMs * 4, kBlock, 0, g->stream>>>(g->huge_q, &g->ctr->huge_len, op);
+    if (identity)
+        k_push_twc<Op, true><<<grid, kBlock, 0, g->stream>>>(qin, nin, op, g->huge_q, &g->ctr->huge_len, g->V);
+    else
+        k_push_twc<Op, false><<<grid, kBlock, 0, g->stream>>>(qin, nin, op, g->huge_q, &g->ctr->huge_len, g->V);
+    k_push_huge<Op><<<kNumSMs * 4, kBlock, 0, g->stream>>>(g->huge_q, &g->ctr->huge_len, g->V, op);
 }
 
 }  // namespace cgb
