@@ -65,3 +65,36 @@ def test_load_files_size_check(lib, tmp_path):
     st = lib.cgb_graph_load_files(str(tmp_path / "nope").encode(), str(dst).encode(), None, 2, 1, 0,
                                   ctypes.byref(h))
     assert st == _lib.EIO
+
+
+def test_cpp_adapter_compiles_and_reports_status(tmp_path, lib):
+    """include/cgb200.hpp (the GraphDeviceWorklist-shaped adapter) compiles
+    against a CSR_Result_type-like struct and links; without a GPU the
+    constructor throws cgb200::error with CGB_ECUDA, with one it runs BFS."""
+    import subprocess
+    src = tmp_path / "adapter.cpp"
+    src.write_text(r'''
+#include "cgb200.hpp"
+#include <cstdio>
+struct CSR_Result_type { uint32_t vertexNum, edgeNum; uint32_t *csr_offset, *csr_dest, *csr_weight;
+                         uint32_t noZeroOutDegreeNum; };
+int main() {
+    uint32_t off[4] = {0, 1, 2, 2}, dst[2] = {1, 2}, w[2] = {5, 7};
+    CSR_Result_type csr{3, 2, off, dst, w, 3};
+    try {
+        cgb200::GraphB200<CSR_Result_type> g(csr, CGB_SSSP);
+        g.graphProcess_device(CGB_SSSP, 0);
+        g.result_D2H();
+        std::printf("%u %u %u\n", g.vertexValue[0], g.vertexValue[1], g.vertexValue[2]);
+    } catch (const cgb200::error& e) {
+        std::printf("status %d\n", (int)e.status);
+    }
+    return 0;
+}
+''')
+    exe = tmp_path / "adapter"
+    libdir = os.path.join(ROOT, "cggraph_b200")
+    subprocess.check_call(["g++", "-std=c++17", "-O1", str(src), "-I", os.path.join(ROOT, "include"), "-L", libdir,
+                           "-lcgb200", f"-Wl,-rpath,{libdir}", "-o", str(exe)])
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120).stdout.strip()
+    assert out in ("0 5 12", "status 5"), out
