@@ -30,7 +30,7 @@ EXPORTS = [
     "cgb_graph_create", "cgb_graph_load_files", "cgb_graph_destroy", "cgb_graph_set_stream", "cgb_graph_info", "cgb_graph_device_csr",
     "cgb_graph_result_device", "cgb_graph_result_download", "cgb_run", "cgb_run_batch", "cgb_run_stats_get", "cgb_trace_get",
     "cgb_last_error_string", "cgb_status_string", "cgb_abi_version", "cgb_gen_rmat", "cgb_gen_grid",
-    "cgb_graph_download",
+    "cgb_graph_download", "cgb_bfs_noalloc",
 ]
 
 

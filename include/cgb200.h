@@ -187,6 +187,28 @@ cgb_status cgb_run_stats_get(const cgb_graph* g, cgb_run_stats* out);
  * receives the number available. */
 cgb_status cgb_trace_get(const cgb_graph* g, cgb_iter_trace* out, uint32_t max_entries, uint32_t* count);
 
+/* --------------------------------------------------- allocation-free BFS */
+
+/* Largest vertex count cgb_bfs_noalloc accepts. */
+#define CGB_NOALLOC_MAX_VERTICES (1u << 20)
+
+/* BFS levels for callers that cannot allocate device memory (a framework
+ * whose caching allocator owns the device's memory, or a serving loop that
+ * forbids cudaMalloc/cudaFree after start-up because they synchronise the
+ * device).  No counterpart in the reference: it is an addition of this
+ * engine.  The caller passes the CSR (device pointers offsets[V+1],
+ * dest[E]), the root and the output levels[V] (device pointer), and a
+ * cudaStream_t (NULL = default stream); results equal cgb_run(CGB_BFS).
+ * Scratch (frontier queues, visited bitmap, counters) lives in one static
+ * device array of about 12.7 MB that every GPU loading the library keeps
+ * until exit; V > CGB_NOALLOC_MAX_VERTICES is rejected with CGB_EINVAL.
+ * The first call on a device looks up the array's device address (make it
+ * before any stream capture).  All calls share the array: calls that overlap
+ * on the GPU race and must be serialised by the caller.  Allocates nothing:
+ * no cudaMalloc, cudaFree or allocating library routine. */
+cgb_status cgb_bfs_noalloc(const uint32_t* offsets, const uint32_t* dest, uint32_t V, uint32_t E, uint32_t root,
+                           uint32_t* levels, void* stream);
+
 /* ---------------------------------------------------------------- misc */
 
 const char* cgb_last_error_string(void);
