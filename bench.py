@@ -56,6 +56,8 @@ def parse_args():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=0, help="0 = same as --steps")
+    p.add_argument("--algorithms", default="bfs,sssp,cc,pr",
+                   help="comma list of bfs,sssp,cc,pr run in each step (default: all four)")
     return p.parse_args()
 
 
@@ -171,11 +173,17 @@ class Dist:
 
 
 # ---------------------------------------------------------------- our arm
-def run_step(gd, gs, root, opts, pr_iters):
-    """One step on resident graphs; returns per-algorithm (edges, ms, stats)."""
+def parse_algs(spec: str) -> list:
+    names = {"bfs": BFS, "sssp": SSSP, "cc": CC, "wcc": CC, "pr": PR, "pagerank": PR}
+    return sorted({names[a.strip().lower()] for a in spec.split(",") if a.strip()})
+
+
+def run_step(gd, gs, root, opts, pr_iters, algs=(BFS, SSSP, CC, PR)):
+    """One step on resident graphs; returns [(algorithm, run stats)]."""
     out = []
-    for g, alg, arg in ((gd, BFS, root), (gd, SSSP, root), (gs, CC, 0), (gd, PR, pr_iters)):
-        _, ms = g.run(alg, arg, opts, to_host=False)
+    for alg in algs:
+        g, arg = {BFS: (gd, root), SSSP: (gd, root), CC: (gs, 0), PR: (gd, pr_iters)}[alg]
+        g.run(alg, arg, opts, to_host=False)
         out.append((alg, g.stats()))
     return out
 
@@ -187,22 +195,25 @@ def bench_cgb200(args, d: Dist):
 
     dev = d.local
     torch.cuda.set_device(dev)
+    algs = parse_algs(args.algorithms)
     gd = cg.Graph.rmat(args.scale, args.edge_factor, args.seed, wmax=64, device=dev)
-    gs = cg.Graph.rmat(args.scale, args.edge_factor, args.seed, symmetrise=True, wmax=0, device=dev)
+    gs = cg.Graph.rmat(args.scale, args.edge_factor, args.seed, symmetrise=True, wmax=0, device=dev) \
+        if CC in algs else None
     off_h, dst_h, w_h = gd.download()
     roots_all = pick_roots(off_h, args.seed, N_ROOTS * d.world)
     roots = roots_all[d.rank::d.world]
-    V, Ed, Es = gd.vertexNum, gd.edgeNum, gs.edgeNum
+    V, Ed, Es = gd.vertexNum, gd.edgeNum, (gs.edgeNum if gs else 0)
 
     stream = torch.cuda.current_stream()
-    gd.set_stream(stream)
-    gs.set_stream(stream)
+    for g in (gd, gs):
+        if g is not None:
+            g.set_stream(stream)
     sched = L.SCHED_LEARNED if args.schedule == "learned" else L.SCHED_HEURISTIC
     warm_opts = cg.make_options(schedule=sched)
     timed_opts = cg.make_options(schedule=sched, flags=L.FLAG_KERNEL_TIMING)
 
     for i in range(args.warmup):
-        run_step(gd, gs, roots[i % len(roots)], warm_opts, args.pr_iters)
+        run_step(gd, gs, roots[i % len(roots)], warm_opts, args.pr_iters, algs)
 
     clocks = Clocks(dev)
     clocks.start()
@@ -219,7 +230,7 @@ def bench_cgb200(args, d: Dist):
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     for k in range(args.steps):
-        for alg, st in run_step(gd, gs, roots[k % len(roots)], timed_opts, args.pr_iters):
+        for alg, st in run_step(gd, gs, roots[k % len(roots)], timed_opts, args.pr_iters, algs):
             per_alg_edges[alg] += st.traversed_edges
             per_alg_ms[alg] += st.ms
             launches += st.launches
@@ -246,7 +257,7 @@ def bench_cgb200(args, d: Dist):
         bytes_per_launch = 12 * Ed + 20 * V + 4
         avg_s = pr_launch_ms / pr_launches / 1e3
         achieved = bytes_per_launch / avg_s / 1e9
-        roof.update({"kernel": "k_pr_pull (+k_pr_huge_rows), one PageRank iteration",
+        roof.update({"kernel": "k_pr_pull (+ hub-row chunk kernels), one PageRank iteration",
                      "alg_bytes_per_launch": bytes_per_launch, "avg_launch_ms": pr_launch_ms / pr_launches,
                      "achieved": achieved, "frac": achieved / peaks["hbm_gbs"], "traffic": None,
                      "dominant_class": L.KERNEL_CLASS_NAMES[dom],
@@ -254,34 +265,37 @@ def bench_cgb200(args, d: Dist):
                                      for c in range(8) if kclass_ms[c] > 0}})
 
     per_alg = {ALG_NAMES[a]: {"gteps": per_alg_edges[a] / (per_alg_ms[a] / 1e3) / 1e9 if per_alg_ms[a] else None,
-                              "ms_per_run": per_alg_ms[a] / args.steps} for a in range(4)}
+                              "ms_per_run": per_alg_ms[a] / args.steps} for a in algs}
+    full = algs == [BFS, SSSP, CC, PR]
 
     # end to end through the C ABI with pinned host buffers
     e2e = None
-    if not args.no_e2e:
+    if not args.no_e2e and full:
         e2e = bench_e2e(args, d, cg, gd, gs, roots, off_h, dst_h, w_h, sched)
 
     # CPU baseline: the reference's own engine on this host (rank 0, N = 1)
     cpu = None
-    if d.world == 1 and not args.no_cpu_baseline:
+    if d.world == 1 and not args.no_cpu_baseline and full:
         try:
             cpu = cpu_baseline(args, gd, gs, off_h, dst_h, w_h, roots)
         except Exception as e:  # reported, not fatal
             cpu = {"value": None, "error": str(e)[-300:]}
 
-    gd.set_stream(None)
-    gs.set_stream(None)
-    gd.close()
-    gs.close()
+    for g in (gd, gs):
+        if g is not None:
+            g.set_stream(None)
+            g.close()
     result = {
         "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": d.world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32 (BFS/SSSP/CC), f64 (PageRank)",
         "data": "synthetic (seeded RMAT, generated on device)",
-        "config": {"workload": f"rmat{args.scale}_ef{args.edge_factor}_bfs_sssp_cc_pr{args.pr_iters}",
+        "config": {"workload": f"rmat{args.scale}_ef{args.edge_factor}_"
+                               + "_".join(ALG_NAMES[a] for a in algs).replace("pagerank", f"pr{args.pr_iters}"),
                    "scale": args.scale, "edge_factor": args.edge_factor, "rmat_abc": [0.57, 0.19, 0.19],
                    "vertices": V, "edges_directed": Ed, "edges_symmetrised": Es, "weights": "uniform [1,64]",
                    "roots": roots, "schedule": args.schedule, "pr_iterations": args.pr_iters,
+                   "algorithms": [ALG_NAMES[a] for a in algs],
                    "l2": "inputs larger than L2 (directed CSR %.2f GB, symmetrised %.2f GB)"
                          % ((4 * (V + 1) + 8 * Ed) / 1e9, (4 * (V + 1) + 4 * Es) / 1e9),
                    "parallelism": f"replicas x{d.world}"},

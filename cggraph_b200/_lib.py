@@ -30,8 +30,10 @@ EXPORTS = [
     "cgb_graph_create", "cgb_graph_load_files", "cgb_graph_destroy", "cgb_graph_set_stream", "cgb_graph_info", "cgb_graph_device_csr",
     "cgb_graph_result_device", "cgb_graph_result_download", "cgb_run", "cgb_run_batch", "cgb_run_stats_get", "cgb_trace_get",
     "cgb_last_error_string", "cgb_status_string", "cgb_abi_version", "cgb_gen_rmat", "cgb_gen_grid",
-    "cgb_graph_download", "cgb_bfs_noalloc",
+    "cgb_graph_download", "cgb_bfs_noalloc", "cgb_policy_load", "cgb_policy_collect", "cgb_policy_train",
+    "cgb_policy_forward", "cgb_policy_loss_grad",
 ]
+POLICY_FEATURES, POLICY_OUTPUTS, POLICY_PARAMS = 24, 9, 6345
 
 
 class Options(ctypes.Structure):
@@ -125,6 +127,13 @@ def lib() -> ctypes.CDLL:
                                    i, i, u32, i, ctypes.POINTER(_P)]
         L.cgb_gen_grid.argtypes = [u32, u32, ctypes.c_uint64, u32, i, ctypes.POINTER(_P)]
         L.cgb_graph_download.argtypes = [_P, _P, _P, _P]
+        L.cgb_bfs_noalloc.argtypes = [_P, _P, u32, u32, u32, _P, _P]
+        L.cgb_policy_load.argtypes = [_P]
+        L.cgb_policy_collect.argtypes = [_P, i, u32, ctypes.POINTER(Options), _P, _P, _P, u32, _u32p]
+        L.cgb_policy_train.argtypes = [_P, _P, _P, u32, u32, u32, ctypes.c_float, ctypes.c_uint64, _P, _P,
+                                       ctypes.POINTER(ctypes.c_float)]
+        L.cgb_policy_forward.argtypes = [_P, _P, u32, _P]
+        L.cgb_policy_loss_grad.argtypes = [_P, _P, _P, _P, u32, ctypes.POINTER(ctypes.c_float), _P]
         for name in EXPORTS:
             f = getattr(L, name)
             if name not in ("cgb_last_error_string", "cgb_status_string", "cgb_abi_version"):

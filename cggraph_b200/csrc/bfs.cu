@@ -21,6 +21,10 @@
 
 namespace cgb {
 
+// Per-CTA accumulators of the top-down op (flushed once per CTA).
+__shared__ unsigned long long s_td_medges;
+__shared__ uint32_t s_td_maxdeg;
+
 struct BfsTdOp {
     const uint32_t* __restrict__ off;
     const uint32_t* __restrict__ dst;
@@ -64,9 +68,23 @@ struct BfsTdOp {
             const unsigned long long s = warp_sum((unsigned long long)deg);
             const uint32_t mx = warp_max(deg);
             if (lane_id() == 0) {
-                atomicAdd(&ctr->medges, s);
-                atomicMax(&ctr->max_deg, mx);
+                atomicAdd(&s_td_medges, s);
+                atomicMax(&s_td_maxdeg, mx);
             }
+        }
+    }
+    __device__ __forceinline__ void block_begin() const
+    {
+        if (threadIdx.x == 0) {
+            s_td_medges = 0;
+            s_td_maxdeg = 0;
+        }
+    }
+    __device__ __forceinline__ void block_end() const
+    {
+        if (threadIdx.x == 0 && s_td_medges) {
+            atomicAdd(&ctr->medges, s_td_medges);
+            atomicMax(&ctr->max_deg, s_td_maxdeg);
         }
     }
 };
@@ -147,9 +165,9 @@ __global__ void __launch_bounds__(kBlock) k_bfs_bu(uint32_t V, const uint32_t* _
 
 static void reset_level_counters(cgb_graph* g, int out)
 {
-    // qlen[out], huge_len, medges, found, max_deg
+    // qlen[out], chunk_len, medges, found, max_deg
     CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->qlen[out], 0, sizeof(uint32_t), g->stream));
-    CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->huge_len, 0, sizeof(uint32_t), g->stream));
+    CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->chunk_len, 0, sizeof(uint32_t), g->stream));
     CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->medges, 0, sizeof(unsigned long long), g->stream));
     CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->found, 0, sizeof(uint32_t), g->stream));
     CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->max_deg, 0, sizeof(uint32_t), g->stream));
@@ -167,6 +185,8 @@ void run_bfs(cgb_graph* g, uint32_t root, const cgb_options& o)
     const uint32_t words = g->words();
     const bool timing = g->flags & CGB_FLAG_KERNEL_TIMING;
     const bool tracing = g->flags & CGB_FLAG_TRACE;
+    PolicySamples* collect = want_pull && !force_pull ? g->collect : nullptr;
+    Policy* pol = (o.schedule == CGB_SCHED_LEARNED && want_pull && !force_pull) ? policy_get() : nullptr;
 
     uint32_t host_root_deg[2];
     CGB_CUDA_TRY(cudaMemcpyAsync(host_root_deg, g->off + root, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost,
@@ -182,46 +202,25 @@ void run_bfs(cgb_graph* g, uint32_t root, const cgb_options& o)
 
     uint32_t cur = 0;  // queue holding the current frontier
     uint64_t nf = (root < g->nz) ? 1 : 0;
+    uint64_t prev_nf = 0;
     uint64_t scout = host_root_deg[1] - host_root_deg[0];
     int64_t edges_to_check = (int64_t)g->E;
     uint32_t maxdeg = (uint32_t)scout;
     uint64_t visited_cnt = 1;
     uint32_t level = 0;
     bool bottom_up = false;
+    bool have_policy_out = false;
     uint64_t awake = 0, old_awake = 0;
     uint32_t* front = g->front_bm;
     uint32_t* next = g->front_bm + words;
     uint64_t iters = 0;
     const uint64_t max_iters = o.max_iterations ? o.max_iterations : (uint64_t)V + 2;
-    Policy* pol = (o.schedule == CGB_SCHED_LEARNED) ? policy_get() : nullptr;
 
-    while (nf > 0) {
-        CGB_REQUIRE(iters < max_iters, CGB_ETIMEOUT, "BFS iteration budget exhausted");
-        // ----- direction decision
-        bool go_pull;
-        if (force_pull) go_pull = true;
-        else if (!want_pull) go_pull = false;
-        else if (pol) {
-            float feat[kPolicyFeatures];
-            policy_features(feat, CGB_BFS, g, nf, scout, (uint64_t)V - visited_cnt,
-                            (uint64_t)std::max<int64_t>(edges_to_check, 0), maxdeg, level, bottom_up ? 1 : 0, 0);
-            int choice = policy_choose_direction(pol, feat);
-            if (choice < 0) {  // fallback: heuristic
-                choice = bottom_up ? ((awake >= old_awake || awake > V / beta) ? 1 : 0)
-                                   : ((double)scout > (double)edges_to_check / alpha ? 1 : 0);
-            }
-            go_pull = choice == 1;
-        } else if (bottom_up) {
-            go_pull = (awake >= old_awake) || ((double)awake > (double)V / beta);
-        } else {
-            go_pull = (double)scout > (double)edges_to_check / alpha;
-        }
-
-        const int out = cur ^ 1;
+    // Queues one level in the given direction (frontier in q[cur] and, when
+    // the last level was pulled, in `front`; next frontier to q[out] / next).
+    auto do_level = [&](bool pull, int out) {
         reset_level_counters(g, out);
-        float it_ms = 0.f;
-        if (tracing) CGB_CUDA_TRY(cudaEventRecord(g->ev_iter[0], g->stream));
-        if (go_pull) {
+        if (pull) {
             if (!bottom_up) {
                 // entering bottom-up: frontier queue -> bitmap
                 if (timing) ktimer_begin(g, CGB_K_FRONTIER);
@@ -229,8 +228,6 @@ void run_bfs(cgb_graph* g, uint32_t root, const cgb_options& o)
                 ++g->stats.launches;
                 k_q2bm<<<grid_for(nf, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(g->q[cur], (uint32_t)nf, front);
                 if (timing) ktimer_end(g);
-                awake = nf;
-                old_awake = 0;
             }
             if (timing) ktimer_begin(g, CGB_K_PULL);
             const uint32_t grid = grid_for((uint64_t)words * 32, kBlock, kNumSMs * 16);
@@ -239,17 +236,96 @@ void run_bfs(cgb_graph* g, uint32_t root, const cgb_options& o)
                                                      next, level + 1, g->nz, g->q[out], &g->ctr->qlen[out], V,
                                                      g->ctr);
             if (timing) ktimer_end(g);
-            std::swap(front, next);
-            g->stats.pulls_bu++;
         } else {
             if (timing) ktimer_begin(g, CGB_K_PUSH);
             BfsTdOp op{g->off, g->dst, g->value, g->visited, level + 1, g->nz, g->q[out], &g->ctr->qlen[out], V, g->ctr};
-            launch_push_twc(g, g->q[cur], (uint32_t)nf, op, false);
+            launch_push(g, g->q[cur], (uint32_t)nf, op, false);
             if (timing) ktimer_end(g);
+        }
+    };
+    auto state_now = [&]() {
+        FeatIn in{};
+        in.alg = CGB_BFS;
+        in.iteration = level;
+        in.prev_dir = bottom_up ? 1 : 0;
+        in.symmetric = g->symmetric == 1;
+        in.V = V;
+        in.E = g->E;
+        in.nf = (double)nf;
+        in.mf = (double)scout;
+        in.unvisited_v = (double)V - (double)visited_cnt;
+        in.unvisited_e = (double)std::max<int64_t>(edges_to_check, 0);
+        in.max_deg = maxdeg;
+        in.prev_nf = (double)prev_nf;
+        return in;
+    };
+
+    while (nf > 0) {
+        CGB_REQUIRE(iters < max_iters, CGB_ETIMEOUT, "BFS iteration budget exhausted");
+        const int out = cur ^ 1;
+        // ----- direction decision
+        const bool heur = bottom_up ? (awake >= old_awake) || ((double)awake > (double)V / beta)
+                                    : (double)scout > (double)edges_to_check / alpha;
+        bool go_pull;
+        if (force_pull) go_pull = true;
+        else if (!want_pull) go_pull = false;
+        else if (collect) {
+            // counterfactual: time both directions from the same state
+            const size_t vbytes = (size_t)V * 4, wbytes = (size_t)words * 4;
+            CGB_CUDA_TRY(cudaMemcpyAsync(collect->save_value, g->value, vbytes, cudaMemcpyDeviceToDevice, g->stream));
+            CGB_CUDA_TRY(cudaMemcpyAsync(collect->save_bm0, g->visited, wbytes, cudaMemcpyDeviceToDevice, g->stream));
+            float ms[kPolicyOutputs] = {};
+            bool have[kPolicyOutputs] = {};
+            for (int d = 0; d < 2; d++) {
+                CGB_CUDA_TRY(cudaEventRecord(g->ev_iter[0], g->stream));
+                do_level(d == 1, out);
+                CGB_CUDA_TRY(cudaEventRecord(g->ev_iter[1], g->stream));
+                sync_counters(g);
+                CGB_CUDA_TRY(cudaEventElapsedTime(&ms[kOutPush + d], g->ev_iter[0], g->ev_iter[1]));
+                have[kOutPush + d] = true;
+                CGB_CUDA_TRY(cudaMemcpyAsync(g->value, collect->save_value, vbytes, cudaMemcpyDeviceToDevice,
+                                             g->stream));
+                CGB_CUDA_TRY(cudaMemcpyAsync(g->visited, collect->save_bm0, wbytes, cudaMemcpyDeviceToDevice,
+                                             g->stream));
+            }
+            policy_log_sample(g, state_now(), ms, have);
+            go_pull = ms[kOutPull] < ms[kOutPush];
+        } else if (pol && have_policy_out) {
+            const int choice = policy_pick_direction(g->h_ctr->policy_out);
+            go_pull = choice < 0 ? heur : choice == 1;
+        } else {
+            go_pull = heur;
+        }
+
+        float it_ms = 0.f;
+        if (tracing) CGB_CUDA_TRY(cudaEventRecord(g->ev_iter[0], g->stream));
+        const FeatIn before = state_now();
+        do_level(go_pull, out);
+        if (go_pull) {
+            if (!bottom_up) {
+                awake = nf;
+                old_awake = 0;
+            }
+            std::swap(front, next);
+            g->stats.pulls_bu++;
+        } else {
             g->stats.pushes_td++;
         }
         if (tracing) CGB_CUDA_TRY(cudaEventRecord(g->ev_iter[1], g->stream));
+        // inference for the next level, fused before the counter read-back;
+        // skipped while both Beamer ratios are far (64x) from their
+        // thresholds, where the choice is not in doubt
+        const double r_alpha = (double)scout * alpha / (double)std::max<int64_t>(edges_to_check, 1);
+        const double r_beta = (double)nf * beta / (double)V;
+        const bool near_boundary = (r_alpha > 1.0 / 64 && r_alpha < 64.0) || (r_beta > 1.0 / 64 && r_beta < 64.0);
+        const bool infer = pol && near_boundary;
+        if (infer) {
+            FeatIn in = before;
+            in.unvisited_e = (double)std::max<int64_t>(edges_to_check - (int64_t)scout, 0);
+            policy_enqueue(pol, g, in, true, go_pull, out);
+        }
         sync_counters(g);
+        have_policy_out = infer;
         if (tracing) {
             CGB_CUDA_TRY(cudaEventElapsedTime(&it_ms, g->ev_iter[0], g->ev_iter[1]));
             cgb_iter_trace t{};
@@ -272,12 +348,13 @@ void run_bfs(cgb_graph* g, uint32_t root, const cgb_options& o)
             awake = g->h_ctr->found;
             visited_cnt += g->h_ctr->found;
         } else {
-            visited_cnt += n_next;  // upper bound when nz < V; only steers the policy
+            visited_cnt += n_next;  // upper bound when nz < V; only steers the schedule
         }
         bottom_up = go_pull;
         edges_to_check -= (int64_t)scout;
         scout = m_next;
         maxdeg = g->h_ctr->max_deg;
+        prev_nf = nf;
         nf = n_next;
         cur = out;
         level++;

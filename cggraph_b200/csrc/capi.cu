@@ -282,6 +282,35 @@ cgb_status cgb_run_batch(cgb_graph* g, int algorithm, const uint32_t* roots, uin
     });
 }
 
+cgb_status cgb_policy_collect(cgb_graph* g, int algorithm, uint32_t root, const cgb_options* opt, float* features,
+                              float* targets, uint8_t* mask, uint32_t max, uint32_t* count)
+{
+    PolicySamples ps{features, targets, mask, max, 0};
+    cgb_status st = guarded([&] {
+        CGB_REQUIRE(g != nullptr && features && targets && mask, CGB_EINVAL, "NULL argument");
+        CGB_REQUIRE(algorithm == CGB_BFS || algorithm == CGB_SSSP, CGB_EINVAL, "samples come from BFS or SSSP runs");
+        CGB_REQUIRE(root < g->V, CGB_EINVAL, "root >= vertexNum");
+        cgb_options o = effective_options(opt);
+        if (o.schedule == CGB_SCHED_FIXED) o.schedule = CGB_SCHED_HEURISTIC;
+        std::lock_guard<std::mutex> lock(g->mu);
+        CGB_CUDA_TRY(cudaSetDevice(g->device));
+        CGB_CUDA_TRY(cudaMalloc((void**)&ps.save_value, (size_t)g->V * 4));
+        CGB_CUDA_TRY(cudaMalloc((void**)&ps.save_bm0, (size_t)g->words() * 4));
+        g->collect = &ps;
+        try {
+            run_one(g, algorithm, root, o);
+        } catch (...) {
+            g->collect = nullptr;
+            throw;
+        }
+        g->collect = nullptr;
+    });
+    if (ps.save_value) cudaFree(ps.save_value);
+    if (ps.save_bm0) cudaFree(ps.save_bm0);
+    if (count) *count = ps.count;
+    return st;
+}
+
 cgb_status cgb_run_stats_get(const cgb_graph* g, cgb_run_stats* out)
 {
     return guarded([&] {

@@ -8,9 +8,13 @@
 //
 // Symmetric graphs (checked once per graph): min-label hooking with pointer
 // jumping, in the sampling order of Afforest (Sutton, Ben-Nun, Barak 2018):
-//   1. comp[v] = v;
-//   2. two rounds that link v with its i-th neighbour only, each followed by
-//      a compress (pointer jumping to the root);
+//   1. comp[v] = min(v, first neighbour) -- lists are sorted, so that is the
+//      smallest neighbour; every pointer goes to a smaller vertex along an
+//      edge, so this is already a valid forest, built without atomics (the
+//      initialisation of ECL-CC, Jaiganesh and Burtscher 2018);
+//   2. one round that links v with its second neighbour, and with its first
+//      one where step 1 left it pointing at itself (first neighbour larger),
+//      each step followed by a compress (pointer jumping to the root);
 //   3. sample comp[] at 1024 hashed vertices and take the most frequent root
 //      as the giant component c;
 //   4. link every remaining edge of each vertex whose root is not c (the
@@ -57,12 +61,26 @@ __global__ void k_cc_init(uint32_t V, uint32_t* comp)
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < V; i += gridDim.x * blockDim.x) comp[i] = i;
 }
 
-__global__ void k_cc_link_round(uint32_t V, const uint32_t* __restrict__ off, const uint32_t* __restrict__ dst,
-                                uint32_t* comp, uint32_t r, DevCounters* ctr)
+// comp[v] = min(v, smallest neighbour) (symmetric graphs, sorted lists).
+__global__ void k_cc_init_min_nbr(uint32_t V, const uint32_t* __restrict__ off, const uint32_t* __restrict__ dst,
+                                  uint32_t* comp)
 {
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
         const uint32_t s = off[v];
-        if (off[v + 1] - s > r) link(v, dst[s + r], comp, ctr);
+        comp[v] = (off[v + 1] > s) ? min(v, dst[s]) : v;
+    }
+}
+
+// Links v with its r-th neighbour; with `first_up` also with its first
+// neighbour when that one is larger than v (the min-neighbour
+// initialisation only covered edge 0 when it pointed down).
+__global__ void k_cc_link_round(uint32_t V, const uint32_t* __restrict__ off, const uint32_t* __restrict__ dst,
+                                uint32_t* comp, uint32_t r, int first_up, DevCounters* ctr)
+{
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+        const uint32_t s = off[v], d = off[v + 1] - s;
+        if (first_up && d > 0 && dst[s] > v) link(v, dst[s], comp, ctr);
+        if (d > r) link(v, dst[s + r], comp, ctr);
     }
 }
 
@@ -109,6 +127,8 @@ struct CcLinkOp {
     {
         if (valid) link(v, dst[e], comp, ctr);
     }
+    __device__ __forceinline__ void block_begin() const {}
+    __device__ __forceinline__ void block_end() const {}
 };
 
 struct CcPropOp {
@@ -143,6 +163,8 @@ struct CcPropOp {
         }
         warp_append(enq, d, qout, qlen, cap, &ctr->overflow);
     }
+    __device__ __forceinline__ void block_begin() const {}
+    __device__ __forceinline__ void block_end() const {}
 };
 
 __global__ void k_zero(uint32_t n, uint32_t* a)
@@ -154,19 +176,23 @@ static void cc_afforest(cgb_graph* g)
 {
     const bool timing = g->flags & CGB_FLAG_KERNEL_TIMING;
     const uint32_t V = g->V;
-    const uint32_t grid = grid_for(V, kBlock, kNumSMs * 8);
+    const uint32_t grid = div_up(V, kBlock);  // one vertex per thread: many CAS chains in flight
     constexpr uint32_t kRounds = 2;
     constexpr uint32_t kSamples = 1024;
 
     if (timing) ktimer_begin(g, CGB_K_INIT);
     ++g->stats.launches;
-    k_cc_init<<<grid, kBlock, 0, g->stream>>>(V, g->value);
+    k_cc_init_min_nbr<<<grid, kBlock, 0, g->stream>>>(V, g->off, g->dst, g->value);
     CGB_CUDA_TRY(cudaMemsetAsync(g->ctr, 0, sizeof(DevCounters), g->stream));
     if (timing) ktimer_end(g);
-    for (uint32_t r = 0; r < kRounds; r++) {
+    if (timing) ktimer_begin(g, CGB_K_COMPRESS);
+    ++g->stats.launches;
+    k_cc_compress<<<grid, kBlock, 0, g->stream>>>(V, g->value);
+    if (timing) ktimer_end(g);
+    for (uint32_t r = 1; r < kRounds; r++) {
         if (timing) ktimer_begin(g, CGB_K_HOOK);
         ++g->stats.launches;
-        k_cc_link_round<<<grid, kBlock, 0, g->stream>>>(V, g->off, g->dst, g->value, r, g->ctr);
+        k_cc_link_round<<<grid, kBlock, 0, g->stream>>>(V, g->off, g->dst, g->value, r, r == 1, g->ctr);
         if (timing) ktimer_end(g);
         if (timing) ktimer_begin(g, CGB_K_COMPRESS);
         ++g->stats.launches;
@@ -191,10 +217,10 @@ static void cc_afforest(cgb_graph* g)
         }
         i = j;
     }
-    CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->huge_len, 0, sizeof(uint32_t), g->stream));
+    CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->chunk_len, 0, sizeof(uint32_t), g->stream));
     if (timing) ktimer_begin(g, CGB_K_HOOK);
     CcLinkOp op{g->off, g->dst, g->value, giant, kRounds, g->ctr};
-    launch_push_twc(g, nullptr, V, op, true);
+    launch_push(g, nullptr, V, op, true);
     if (timing) ktimer_end(g);
     if (timing) ktimer_begin(g, CGB_K_COMPRESS);
     ++g->stats.launches;
@@ -229,10 +255,10 @@ static void cc_propagate(cgb_graph* g, const cgb_options& o)
         it++;
         const int out = cur ^ 1;
         CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->qlen[out], 0, sizeof(uint32_t), g->stream));
-        CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->huge_len, 0, sizeof(uint32_t), g->stream));
+        CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->chunk_len, 0, sizeof(uint32_t), g->stream));
         if (timing) ktimer_begin(g, CGB_K_PUSH);
         CcPropOp op{g->off, g->dst, g->value, g->stamp, it, g->nz, g->q[out], &g->ctr->qlen[out], V, g->ctr};
-        launch_push_twc(g, identity ? nullptr : g->q[cur], (uint32_t)n, op, identity);
+        launch_push(g, identity ? nullptr : g->q[cur], (uint32_t)n, op, identity);
         if (timing) ktimer_end(g);
         sync_counters(g);
         CGB_REQUIRE(!g->h_ctr->overflow, CGB_EOVERFLOW, "CC queue overflow");

@@ -10,17 +10,33 @@
 // Device counters shared by the frontier kernels of one graph.
 struct DevCounters {
     uint32_t qlen[2];         // lengths of the two alternating vertex queues
-    uint32_t huge_len;        // vertices deferred to the split-hub kernel
-    uint32_t far_len[2];      // SSSP far piles
+    uint32_t huge_len;        // vertices deferred to the split-hub kernel (allocation-free BFS)
+    uint32_t far_len[2];      // SSSP: vertices pending in the far bitmap (index 0)
     uint32_t overflow;        // a queue ran out of capacity
     uint32_t link_giveup;     // a CC link loop hit its retry bound
     uint32_t found;           // BFS bottom-up: vertices found this level
     unsigned long long medges;    // sum of out-degrees of the next frontier
     unsigned long long reached_edges;
     uint32_t reached;
-    uint32_t min_far;         // SSSP: smallest distance left in the far pile
+    uint32_t min_far;         // SSSP: smallest distance left in the far bitmap
     uint32_t max_deg;         // max degree of the next frontier
-    uint32_t pad[3];
+    uint32_t chunk_len;       // chunk descriptors queued by k_push_binned
+    uint32_t pad[2];
+    float policy_out[CGB_POLICY_OUTPUTS];  // learned scheduler: predicted log-costs
+};
+
+// Destination of counterfactual training samples (cgb_policy_collect).
+struct PolicySamples {
+    float* features;   // max * CGB_POLICY_FEATURES
+    float* targets;    // max * CGB_POLICY_OUTPUTS
+    uint8_t* mask;     // max * CGB_POLICY_OUTPUTS
+    uint32_t max;
+    uint32_t count;
+    // state snapshots for the trials
+    uint32_t* save_value = nullptr;
+    uint32_t* save_bm0 = nullptr;
+    uint32_t* save_bm1 = nullptr;
+    uint32_t* save_q = nullptr;
 };
 
 struct cgb_graph {
@@ -42,9 +58,25 @@ struct cgb_graph {
     bool csc_owned = false;
     int symmetric = -1;
 
-    // PageRank: in-rows with in-degree >= kPrHuge
-    uint32_t* pr_huge_rows = nullptr;
-    uint32_t n_pr_huge = 0;
+    // PageRank layout: vertices relabelled by out-degree bucket (stable; zero
+    // out-degree last), in-edge CSC over the new ids, out-degree by new id
+    uint32_t* pr_rank = nullptr;     // old id -> new id
+    uint32_t* pr_off = nullptr;      // V+1
+    uint32_t* pr_src = nullptr;      // E
+    uint32_t* pr_outdeg = nullptr;   // V
+    uint2* pr_chunks = nullptr;      // hub rows: (row, first edge) of each kPrChunk-edge chunk
+    uint32_t* pr_chunk_base = nullptr;  // per hub row: index of its first chunk (n_pr_huge + 1)
+    uint32_t* pr_huge_rows = nullptr;   // hub rows (new ids)
+    double* pr_part = nullptr;       // per-chunk partial sums
+    uint32_t n_pr_huge = 0, n_pr_chunks = 0;
+    // sliced ELL (32 rows per slice) of the non-hub rows: edge j of row
+    // 32*s + l at col[slice_ptr[s] + 32*j + l]; padding points at vertex V,
+    // whose contribution is kept at 0
+    uint64_t* pr_slice_ptr = nullptr;   // nslices + 1
+    uint32_t* pr_slice_len = nullptr;   // nslices
+    uint32_t* pr_col = nullptr;
+    uint32_t* pr_hub_bm = nullptr;      // bitmap of hub rows
+    uint64_t pr_sell_size = 0;
     bool pr_ready = false;
 
     // results / algorithm state
@@ -56,12 +88,11 @@ struct cgb_graph {
 
     // frontier workspace
     uint32_t* q[2] = {nullptr, nullptr};  // capacity V each
-    uint32_t* huge_q = nullptr;           // capacity V
+    uint2* chunk_q = nullptr;             // (vertex, chunk) descriptors of big lists
+    uint32_t chunk_cap = 0;
     uint32_t* visited = nullptr;          // bitmap, words = V/32 + 1
     uint32_t* front_bm = nullptr;
     uint32_t* stamp = nullptr;            // uint32[V]
-    uint2* far[2] = {nullptr, nullptr};
-    uint32_t far_cap = 0;
     uint32_t* sample = nullptr;           // CC sampling buffer
 
     DevCounters* ctr = nullptr;       // device
@@ -75,6 +106,7 @@ struct cgb_graph {
 
     cgb_run_stats stats{};
     std::vector<cgb_iter_trace> trace;
+    PolicySamples* collect = nullptr;   // set while cgb_policy_collect runs
     uint32_t flags = 0;
 
     uint32_t words() const { return V / 32 + 1; }
@@ -82,10 +114,13 @@ struct cgb_graph {
 
 namespace cgb {
 
-constexpr uint32_t kPrHuge = 8192;   // PageRank rows handled by a whole CTA
+constexpr uint32_t kPrHuge = 4096;   // PageRank rows split into chunks across CTAs
+constexpr uint32_t kPrChunk = 4096;  // edges per PageRank hub chunk
 constexpr uint32_t kHugeDeg = 16384; // push: hubs split across CTAs
 constexpr uint32_t kCtaDeg = 1024;   // push: CTA-per-vertex tier
 constexpr uint32_t kHugeChunk = 4096;
+constexpr uint32_t kBigDeg = 512;    // binned push: lists cut into chunks
+constexpr uint32_t kChunk = 1024;    // edges per chunk
 
 // graph lifetime and preparation (graph.cu)
 cgb_graph* graph_alloc(uint32_t V, uint32_t E, uint32_t nz, int device, bool with_weight);
@@ -96,7 +131,6 @@ uint32_t sssp_default_delta(const cgb_graph* g);
 
 // workspace management (graph.cu)
 void ensure_frontier(cgb_graph* g);
-void ensure_sssp(cgb_graph* g);
 void ensure_csc(cgb_graph* g);
 void ensure_symmetry_known(cgb_graph* g);
 void ensure_pr(cgb_graph* g);

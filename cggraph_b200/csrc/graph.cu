@@ -136,30 +136,6 @@ __global__ void k_sum_u32(uint32_t n, const uint32_t* __restrict__ a, unsigned l
     if (lane_id() == 0 && s) atomicAdd(out, s);
 }
 
-// For every edge u->v, is v->u present?  (binary search in v's sorted list)
-__global__ void k_check_symmetric(uint32_t V, uint32_t E, const uint32_t* __restrict__ off,
-                                  const uint32_t* __restrict__ dst, uint32_t* asym)
-{
-    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x) {
-        if ((e & 1023u) == 0 && *(volatile uint32_t*)asym) return;
-        const uint32_t u = edge_source(off, V, e);
-        const uint32_t v = dst[e];
-        uint32_t lo = off[v], hi = off[v + 1];
-        bool found = false;
-        while (lo < hi) {
-            const uint32_t mid = (lo + hi) >> 1;
-            const uint32_t x = dst[mid];
-            if (x == u) {
-                found = true;
-                break;
-            }
-            if (x < u) lo = mid + 1;
-            else hi = mid;
-        }
-        if (!found) atomicOr(asym, 1u);
-    }
-}
-
 __global__ void k_collect_heavy_rows(uint32_t V, const uint32_t* __restrict__ in_off, uint32_t th, uint32_t* rows,
                                      uint32_t* n)
 {
@@ -305,51 +281,78 @@ void compute_weight_sum(cgb_graph* g)
     g->sum_w = h;
 }
 
+__global__ void k_compare_u32(uint64_t n, const uint32_t* __restrict__ a, const uint32_t* __restrict__ b,
+                              uint32_t* differ)
+{
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        if ((i & 4095u) == 0 && *(volatile uint32_t*)differ) return;
+        if (a[i] != b[i]) atomicOr(differ, 1u);
+    }
+}
+
+// Builds the transpose (in-edge CSC) by a radix sort of packed (dst, src)
+// keys and compares it with the CSR: equal means the graph is symmetric, the
+// transpose is dropped and the CSR serves both directions.
+static void build_transpose(cgb_graph* g)
+{
+    const uint32_t V = g->V, E = g->E;
+    const uint32_t b = bits_for(V);
+    uint32_t* in_off = dalloc<uint32_t>((size_t)V + 1);
+    uint32_t* in_src = dalloc<uint32_t>(E);
+    if (E == 0) {
+        CGB_CUDA_TRY(cudaMemsetAsync(in_off, 0, ((size_t)V + 1) * sizeof(uint32_t), g->stream));
+    } else {
+        uint64_t* keys = dalloc<uint64_t>(E);
+        uint64_t* alt = dalloc<uint64_t>(E);
+        const uint32_t grid = grid_for(E, kBlock, kNumSMs * 16);
+        k_make_keys<<<grid, kBlock, 0, g->stream>>>(V, E, g->off, g->dst, b, keys, true);
+        radix_sort_u64(g, keys, alt, E, 2 * b);
+        k_split_keys<<<grid, kBlock, 0, g->stream>>>(E, keys, b, in_src);
+        k_offsets_from_keys<<<grid_for((uint64_t)E + 1, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(V, E, keys, b,
+                                                                                                       in_off);
+        CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        dfree(keys);
+        dfree(alt);
+    }
+    uint32_t* differ = dalloc<uint32_t>(1);
+    CGB_CUDA_TRY(cudaMemsetAsync(differ, 0, sizeof(uint32_t), g->stream));
+    k_compare_u32<<<kNumSMs * 8, kBlock, 0, g->stream>>>((uint64_t)V + 1, in_off, g->off, differ);
+    if (E) k_compare_u32<<<kNumSMs * 8, kBlock, 0, g->stream>>>(E, in_src, g->dst, differ);
+    uint32_t h = 0;
+    CGB_CUDA_TRY(cudaMemcpyAsync(&h, differ, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
+    CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    dfree(differ);
+    if (h) {
+        g->symmetric = 0;
+        g->in_off = in_off;
+        g->in_src = in_src;
+        g->csc_owned = true;
+    } else {
+        g->symmetric = 1;
+        dfree(in_off);
+        dfree(in_src);
+        g->in_off = g->off;
+        g->in_src = g->dst;
+        g->csc_owned = false;
+    }
+}
+
 void ensure_symmetry_known(cgb_graph* g)
 {
     if (g->symmetric >= 0) return;
-    uint32_t* d = dalloc<uint32_t>(1);
-    CGB_CUDA_TRY(cudaMemsetAsync(d, 0, sizeof(uint32_t), g->stream));
-    if (g->E)
-        k_check_symmetric<<<grid_for(g->E, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(g->V, g->E, g->off, g->dst,
-                                                                                         d);
-    uint32_t h = 0;
-    CGB_CUDA_TRY(cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
-    CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
-    dfree(d);
-    g->symmetric = h ? 0 : 1;
+    build_transpose(g);
 }
 
 void ensure_csc(cgb_graph* g)
 {
     if (g->in_off) return;
-    ensure_symmetry_known(g);
     if (g->symmetric == 1) {
         g->in_off = g->off;
         g->in_src = g->dst;
         g->csc_owned = false;
         return;
     }
-    const uint32_t V = g->V, E = g->E;
-    const uint32_t b = bits_for(V);
-    g->in_off = dalloc<uint32_t>((size_t)V + 1);
-    g->in_src = dalloc<uint32_t>(E);
-    g->csc_owned = true;
-    if (E == 0) {
-        CGB_CUDA_TRY(cudaMemsetAsync(g->in_off, 0, ((size_t)V + 1) * sizeof(uint32_t), g->stream));
-        return;
-    }
-    uint64_t* keys = dalloc<uint64_t>(E);
-    uint64_t* alt = dalloc<uint64_t>(E);
-    const uint32_t grid = grid_for(E, kBlock, kNumSMs * 16);
-    k_make_keys<<<grid, kBlock, 0, g->stream>>>(V, E, g->off, g->dst, b, keys, true);
-    radix_sort_u64(g, keys, alt, E, 2 * b);
-    k_split_keys<<<grid, kBlock, 0, g->stream>>>(E, keys, b, g->in_src);
-    k_offsets_from_keys<<<grid_for((uint64_t)E + 1, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(V, E, keys, b,
-                                                                                                   g->in_off);
-    CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
-    dfree(keys);
-    dfree(alt);
+    build_transpose(g);
 }
 
 void ensure_frontier(cgb_graph* g)
@@ -358,43 +361,240 @@ void ensure_frontier(cgb_graph* g)
     const uint32_t V = g->V;
     g->q[0] = dalloc<uint32_t>(V);
     g->q[1] = dalloc<uint32_t>(V);
-    g->huge_q = dalloc<uint32_t>(V);
+    g->chunk_cap = (uint32_t)std::min<uint64_t>(3ull * g->E / kChunk + 64, 0xFFFFFFF0ull);
+    g->chunk_q = dalloc<uint2>(g->chunk_cap);
     g->visited = dalloc<uint32_t>(g->words());
     g->front_bm = dalloc<uint32_t>(2 * (size_t)g->words());
     g->stamp = dalloc<uint32_t>(V);
     g->sample = dalloc<uint32_t>(1024);
 }
 
-void ensure_sssp(cgb_graph* g)
+__global__ void k_in_degree(uint32_t E, const uint32_t* __restrict__ dst, uint32_t* indeg)
 {
-    if (g->far[0]) return;
-    if (g->w && g->sum_w == 0) compute_weight_sum(g);
-    uint64_t cap = (uint64_t)g->E + g->V + 1024;
-    if (cap > 0xFFFFFFF0ull) cap = 0xFFFFFFF0ull;
-    g->far_cap = (uint32_t)cap;
-    g->far[0] = dalloc<uint2>(cap);
-    g->far[1] = dalloc<uint2>(cap);
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x)
+        atomicAdd(indeg + dst[e], 1u);
 }
 
+// Sort key of a vertex for the PageRank layout: its out-degree bucket
+// (0 for the largest lists, 32 for none) in the top 6 bits, then its
+// in-degree descending (clamped to 26 bits).
+__global__ void k_pr_bucket(uint32_t V, const uint32_t* __restrict__ off, const uint32_t* __restrict__ indeg,
+                            uint32_t* key, uint32_t* id)
+{
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+        const uint32_t od = off[v + 1] - off[v];
+        const uint32_t bucket = od ? (uint32_t)__clz(od) : 32u;
+        const uint32_t in = min(indeg[v], (1u << 26) - 1);
+        key[v] = (bucket << 26) | ((1u << 26) - 1 - in);
+        id[v] = v;
+    }
+}
+
+// Slice lengths of the sliced ELL: the longest non-hub row of each slice.
+__global__ void k_sell_len(uint32_t V, const uint32_t* __restrict__ off, uint32_t hub, uint32_t* len, uint64_t* width)
+{
+    const uint32_t nslices = (V + 31) / 32;
+    for (uint32_t s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < nslices;
+         s += (gridDim.x * blockDim.x) >> 5) {
+        const uint32_t r = s * 32 + lane_id();
+        uint32_t d = r < V ? off[r + 1] - off[r] : 0;
+        if (d >= hub) d = 0;
+        d = warp_max(d);
+        if (lane_id() == 0) {
+            len[s] = d;
+            width[s] = 32ull * d;
+        }
+    }
+}
+
+__global__ void k_fill_u32(uint64_t n, uint32_t* a, uint32_t v)
+{
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        a[i] = v;
+}
+
+// Scatter the sorted (row, src) keys of the non-hub rows into the sliced ELL
+// and mark the hub rows.
+__global__ void k_sell_fill(uint32_t E, const uint64_t* __restrict__ keys, uint32_t b,
+                            const uint32_t* __restrict__ off, const uint64_t* __restrict__ slice_ptr, uint32_t hub,
+                            uint32_t* col, uint32_t* hub_bm)
+{
+    const uint64_t mask = (1ull << b) - 1;
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x) {
+        const uint64_t k = keys[e];
+        const uint32_t r = (uint32_t)(k >> b);
+        const uint32_t s0 = off[r];
+        if (off[r + 1] - s0 >= hub) {
+            if (e == s0) atomicOr(hub_bm + (r >> 5), 1u << (r & 31u));
+            continue;
+        }
+        col[slice_ptr[r >> 5] + 32ull * (e - s0) + (r & 31u)] = (uint32_t)(k & mask);
+    }
+}
+
+__global__ void k_pr_rank(uint32_t V, const uint32_t* __restrict__ order, const uint32_t* __restrict__ off,
+                          uint32_t* rank, uint32_t* outdeg_new)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < V; i += gridDim.x * blockDim.x) {
+        const uint32_t v = order[i];
+        rank[v] = i;
+        outdeg_new[i] = off[v + 1] - off[v];
+    }
+}
+
+__global__ void k_row_bounds(const uint32_t* __restrict__ rows, uint32_t n, const uint32_t* __restrict__ off,
+                             uint32_t* lohi)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        lohi[i] = off[rows[i]];
+        lohi[n + i] = off[rows[i] + 1];
+    }
+}
+
+// key = rank[dst] << b | rank[src]
+__global__ void k_pr_edge_keys(uint32_t V, uint32_t E, const uint32_t* __restrict__ off,
+                               const uint32_t* __restrict__ dst, const uint32_t* __restrict__ rank, uint32_t b,
+                               uint64_t* keys)
+{
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x) {
+        const uint64_t s = rank[edge_source(off, V, e)];
+        const uint64_t d = rank[dst[e]];
+        keys[e] = (d << b) | s;
+    }
+}
+
+// Sliced ELL of the non-hub rows from the sorted (row, src) keys.
+static void build_sell(cgb_graph* g, const uint64_t* keys, uint32_t b)
+{
+    const uint32_t V = g->V, E = g->E;
+    const uint32_t nslices = (V + 31) / 32;
+    g->pr_slice_len = dalloc<uint32_t>(nslices);
+    g->pr_slice_ptr = dalloc<uint64_t>((size_t)nslices + 1);
+    g->pr_hub_bm = dalloc<uint32_t>(g->words());
+    CGB_CUDA_TRY(cudaMemsetAsync(g->pr_hub_bm, 0, (size_t)g->words() * 4, g->stream));
+    uint64_t* width = dalloc<uint64_t>((size_t)nslices + 1);
+    CGB_CUDA_TRY(cudaMemsetAsync(width + nslices, 0, 8, g->stream));
+    k_sell_len<<<grid_for((uint64_t)nslices * 32, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(
+        V, g->pr_off, kPrHuge, g->pr_slice_len, width);
+    size_t tb = 0;
+    CGB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb, width, g->pr_slice_ptr, (uint64_t)nslices + 1, g->stream));
+    void* temp = dalloc<char>(tb);
+    cudaError_t err =
+        cub::DeviceScan::ExclusiveSum(temp, tb, width, g->pr_slice_ptr, (uint64_t)nslices + 1, g->stream);
+    uint64_t total = 0;
+    CGB_CUDA_TRY(cudaMemcpyAsync(&total, g->pr_slice_ptr + nslices, 8, cudaMemcpyDeviceToHost, g->stream));
+    CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    dfree(temp);
+    dfree(width);
+    CGB_CUDA_TRY(err);
+    g->pr_sell_size = total;
+    g->pr_col = dalloc<uint32_t>(total);
+    k_fill_u32<<<grid_for(total, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(total, g->pr_col, V);
+    if (E)
+        k_sell_fill<<<grid_for(E, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(E, keys, b, g->pr_off,
+                                                                                g->pr_slice_ptr, kPrHuge, g->pr_col,
+                                                                                g->pr_hub_bm);
+    CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+}
+
+// Builds the PageRank layout (see cgb_graph): the relabel keeps every
+// gathered contribution (vertices with out-edges) in one dense prefix of
+// the contrib array, and groups rows of similar size.
 void ensure_pr(cgb_graph* g)
 {
-    ensure_csc(g);
     if (g->pr_ready) return;
-    const uint32_t V = g->V;
+    const uint32_t V = g->V, E = g->E;
+    const uint32_t b = bits_for(V);
     for (int i = 0; i < 2; i++) {
         if (!g->pr[i]) g->pr[i] = dalloc<double>(V);
-        if (!g->contrib[i]) g->contrib[i] = dalloc<double>(V);
+        if (!g->contrib[i]) g->contrib[i] = dalloc<double>((size_t)V + 1);
+        CGB_CUDA_TRY(cudaMemsetAsync(g->contrib[i] + V, 0, sizeof(double), g->stream));  // padding target
     }
-    uint32_t* n = dalloc<uint32_t>(1);
-    CGB_CUDA_TRY(cudaMemsetAsync(n, 0, sizeof(uint32_t), g->stream));
-    uint32_t* rows = dalloc<uint32_t>(V);
-    k_collect_heavy_rows<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, g->in_off, kPrHuge, rows, n);
-    uint32_t h = 0;
-    CGB_CUDA_TRY(cudaMemcpyAsync(&h, n, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
-    CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
-    dfree(n);
-    g->n_pr_huge = h;
-    g->pr_huge_rows = rows;
+    g->pr_rank = dalloc<uint32_t>(V);
+    g->pr_outdeg = dalloc<uint32_t>(V);
+    g->pr_off = dalloc<uint32_t>((size_t)V + 1);
+    g->pr_src = dalloc<uint32_t>(E);
+    // 1. stable order by (out-degree bucket, in-degree descending)
+    {
+        uint32_t* key = dalloc<uint32_t>(V);
+        uint32_t* key2 = dalloc<uint32_t>(V);
+        uint32_t* id = dalloc<uint32_t>(V);
+        uint32_t* id2 = dalloc<uint32_t>(V);
+        CGB_CUDA_TRY(cudaMemsetAsync(key2, 0, (size_t)V * 4, g->stream));
+        if (E) k_in_degree<<<grid_for(E, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(E, g->dst, key2);
+        k_pr_bucket<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, g->off, key2, key, id);
+        cub::DoubleBuffer<uint32_t> kb(key, key2), vb(id, id2);
+        size_t tb = 0;
+        CGB_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tb, kb, vb, (uint64_t)V, 0, 32, g->stream));
+        void* temp = dalloc<char>(tb);
+        cudaError_t err = cub::DeviceRadixSort::SortPairs(temp, tb, kb, vb, (uint64_t)V, 0, 32, g->stream);
+        k_pr_rank<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, vb.Current(), g->off, g->pr_rank,
+                                                                             g->pr_outdeg);
+        CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        dfree(temp);
+        dfree(key);
+        dfree(key2);
+        dfree(id);
+        dfree(id2);
+        CGB_CUDA_TRY(err);
+    }
+    // 2. in-edge CSC over the new ids
+    if (E) {
+        uint64_t* keys = dalloc<uint64_t>(E);
+        uint64_t* alt = dalloc<uint64_t>(E);
+        const uint32_t grid = grid_for(E, kBlock, kNumSMs * 16);
+        k_pr_edge_keys<<<grid, kBlock, 0, g->stream>>>(V, E, g->off, g->dst, g->pr_rank, b, keys);
+        radix_sort_u64(g, keys, alt, E, 2 * b);
+        k_split_keys<<<grid, kBlock, 0, g->stream>>>(E, keys, b, g->pr_src);
+        k_offsets_from_keys<<<grid_for((uint64_t)E + 1, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(V, E, keys, b,
+                                                                                                       g->pr_off);
+        build_sell(g, keys, b);
+        dfree(keys);
+        dfree(alt);
+    } else {
+        CGB_CUDA_TRY(cudaMemsetAsync(g->pr_off, 0, ((size_t)V + 1) * 4, g->stream));
+        build_sell(g, nullptr, b);
+    }
+    // 3. hub rows and their chunk table (host-built; few rows)
+    {
+        uint32_t* n = dalloc<uint32_t>(1);
+        uint32_t* rows = dalloc<uint32_t>(V);
+        CGB_CUDA_TRY(cudaMemsetAsync(n, 0, sizeof(uint32_t), g->stream));
+        k_collect_heavy_rows<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, g->pr_off, kPrHuge, rows,
+                                                                                        n);
+        uint32_t h = 0;
+        CGB_CUDA_TRY(cudaMemcpyAsync(&h, n, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
+        CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        dfree(n);
+        std::vector<uint32_t> hrows(h), lo(h), hi(h);
+        if (h) {
+            CGB_CUDA_TRY(cudaMemcpy(hrows.data(), rows, h * 4ull, cudaMemcpyDeviceToHost));
+            std::sort(hrows.begin(), hrows.end());
+            CGB_CUDA_TRY(cudaMemcpy(rows, hrows.data(), h * 4ull, cudaMemcpyHostToDevice));
+            uint32_t* lohi = dalloc<uint32_t>(2ull * h);
+            k_row_bounds<<<grid_for(h, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(rows, h, g->pr_off, lohi);
+            CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+            CGB_CUDA_TRY(cudaMemcpy(lo.data(), lohi, h * 4ull, cudaMemcpyDeviceToHost));
+            CGB_CUDA_TRY(cudaMemcpy(hi.data(), lohi + h, h * 4ull, cudaMemcpyDeviceToHost));
+            dfree(lohi);
+        }
+        std::vector<uint2> chunks;
+        std::vector<uint32_t> base(h + 1, 0);
+        for (uint32_t i = 0; i < h; i++) {
+            base[i] = (uint32_t)chunks.size();
+            for (uint32_t e = lo[i]; e < hi[i]; e += kPrChunk) chunks.push_back(make_uint2(hrows[i], e));
+        }
+        base[h] = (uint32_t)chunks.size();
+        g->n_pr_huge = h;
+        g->n_pr_chunks = (uint32_t)chunks.size();
+        g->pr_huge_rows = rows;
+        g->pr_chunk_base = dalloc<uint32_t>(h + 1);
+        CGB_CUDA_TRY(cudaMemcpy(g->pr_chunk_base, base.data(), (h + 1) * 4ull, cudaMemcpyHostToDevice));
+        g->pr_chunks = dalloc<uint2>(chunks.size());
+        if (!chunks.empty())
+            CGB_CUDA_TRY(cudaMemcpy(g->pr_chunks, chunks.data(), chunks.size() * sizeof(uint2), cudaMemcpyHostToDevice));
+        g->pr_part = dalloc<double>(chunks.size());
+    }
     g->pr_ready = true;
 }
 
@@ -477,9 +677,11 @@ void graph_free(cgb_graph* g)
         dfree(g->in_off);
         dfree(g->in_src);
     }
-    void* ptrs[] = {g->off, g->dst, g->w, g->pr_huge_rows, g->value, g->pr[0], g->pr[1], g->contrib[0],
-                    g->contrib[1], g->q[0], g->q[1], g->huge_q, g->visited, g->front_bm, g->stamp, g->far[0],
-                    g->far[1], g->sample, g->ctr};
+    void* ptrs[] = {g->off, g->dst, g->w, g->pr_huge_rows, g->pr_rank, g->pr_off, g->pr_src, g->pr_outdeg,
+                    g->pr_chunks, g->pr_chunk_base, g->pr_part, g->pr_slice_ptr, g->pr_slice_len, g->pr_col,
+                    g->pr_hub_bm, g->value, g->pr[0], g->pr[1], g->contrib[0],
+                    g->contrib[1], g->q[0], g->q[1], g->chunk_q, g->visited, g->front_bm, g->stamp, g->sample,
+                    g->ctr};
     for (void* p : ptrs) dfree(p);
     if (g->h_ctr) cudaFreeHost(g->h_ctr);
     for (cudaEvent_t e : g->kev) cudaEventDestroy(e);

@@ -1,27 +1,96 @@
-// Per-iteration schedule policy (learned MLP with heuristic fallback).
+// Per-iteration schedule policy: a small FP32 MLP (24 features -> 64 -> 64
+// -> 9 predicted log-costs) trained on the engine's own counterfactual
+// traces, with the Beamer / fixed-delta heuristic as fallback.
 #pragma once
 
 #include "engine.cuh"
 
 namespace cgb {
 
-constexpr int kPolicyFeatures = 24;
+constexpr int kPolicyFeatures = CGB_POLICY_FEATURES;  // 24
+constexpr int kPolicyHidden = 64;
+constexpr int kPolicyOutputs = CGB_POLICY_OUTPUTS;    // 9
+// parameter layout: W1[24][64] b1[64] W2[64][64] b2[64] W3[64][9] b3[9]
+constexpr int kPolicyParams = CGB_POLICY_PARAMS;
+static_assert(kPolicyParams == kPolicyFeatures * kPolicyHidden + kPolicyHidden + kPolicyHidden * kPolicyHidden +
+                                   kPolicyHidden + kPolicyHidden * kPolicyOutputs + kPolicyOutputs,
+              "parameter count");
+
+// Output heads: predicted log-cost of each choice (lower is better).
+constexpr int kOutPush = 0, kOutPull = 1;  // BFS direction of the next level
+constexpr int kOutDelta0 = 2;              // SSSP delta x kDeltaScale[i] for the next bucket
+constexpr int kNumDeltaChoices = 5;
+__host__ __device__ inline float delta_scale(int i)
+{
+    return i == 0 ? 0.25f : i == 1 ? 0.5f : i == 2 ? 1.f : i == 3 ? 2.f : 4.f;
+}
+
+// Raw quantities at a decision point.  The same function turns them into
+// features on the host (trace logging) and on the device (inference).
+struct FeatIn {
+    uint32_t alg;          // CGB_BFS / CGB_SSSP
+    uint32_t iteration;
+    int32_t prev_dir;      // BFS: last level was pull (1) or push (0)
+    uint32_t symmetric;
+    double V, E;
+    double nf, mf;         // frontier vertices / out-edges of the frontier
+    double unvisited_v, unvisited_e;
+    double max_deg, prev_nf;
+    double delta, base_delta;  // SSSP
+    double far_count, settled; // SSSP
+};
+
+__host__ __device__ inline float lg(double x) { return (float)log1p(x > 0 ? x : 0.0); }
+
+__host__ __device__ inline void policy_features(const FeatIn& in, float* f)
+{
+    const double V = in.V > 1 ? in.V : 1, E = in.E > 1 ? in.E : 1;
+    const double avg = E / V;
+    f[0] = lg(in.nf) / lg(V);
+    f[1] = lg(in.mf) / lg(E);
+    f[2] = (float)(in.nf / V);
+    f[3] = (float)(in.mf / E);
+    f[4] = (float)(in.unvisited_v / V);
+    f[5] = (float)(in.unvisited_e / E);
+    f[6] = lg(in.max_deg) / lg(E);
+    f[7] = lg(in.mf / (in.nf > 1 ? in.nf : 1)) / lg(avg * 64 + 1);
+    f[8] = lg(avg) / 8.f;
+    f[9] = (float)(in.iteration > 256 ? 256 : in.iteration) / 64.f;
+    f[10] = (float)in.prev_dir;
+    f[11] = 1.f;
+    f[12] = (float)(lg(in.nf) - lg(in.prev_nf)) / 8.f;
+    f[13] = (float)(lg(in.mf * 15.0) - lg(in.unvisited_e)) / 8.f;  // Beamer alpha test, in logs
+    f[14] = (float)(lg(in.nf * 18.0) - lg(V)) / 8.f;               // Beamer beta test, in logs
+    f[15] = (float)in.symmetric;
+    f[16] = in.alg == CGB_BFS ? 1.f : 0.f;
+    f[17] = in.alg == CGB_SSSP ? 1.f : 0.f;
+    f[18] = in.base_delta > 0 ? (float)(log(in.delta / in.base_delta) / log(4.0)) : 0.f;
+    f[19] = (float)(in.far_count / V);
+    f[20] = lg(in.far_count) / lg(V);
+    f[21] = lg(V) / 32.f;
+    f[22] = lg(E) / 32.f;
+    f[23] = (float)(in.settled / V);
+}
 
 struct Policy;
 
-// The loaded policy, or nullptr when none is loaded (callers then fall back
-// to the heuristic).
+// The policy loaded on the current device, or nullptr (heuristic fallback).
 Policy* policy_get();
+const float* policy_params_device(Policy* p);
 
-// Fills the 24 features of one iteration.
-void policy_features(float* feat, int algorithm, const cgb_graph* g, uint64_t frontier_vertices,
-                     uint64_t frontier_edges, uint64_t unvisited_vertices, uint64_t unvisited_edges,
-                     uint32_t max_frontier_degree, uint32_t iteration, int prev_direction, uint32_t delta);
+// Queues the network on the graph's stream: features from `in` (with the
+// counters of the level just run patched in when `patch_bfs` is set: next
+// frontier size, its out-edges and max degree, vertices found), outputs
+// into the DevCounters' policy_out, read back by the next sync_counters.
+void policy_enqueue(Policy* p, cgb_graph* g, const FeatIn& in, bool patch_bfs, bool was_pull, int out_q);
 
-// 0 = push, 1 = pull; -1 = no confident choice (use the heuristic).
-int policy_choose_direction(Policy* p, const float* feat);
+// Appends one counterfactual sample (features of `in`, measured ms of the
+// choices flagged in `have`) to g->collect.
+void policy_log_sample(cgb_graph* g, const FeatIn& in, const float* ms, const bool* have);
 
-// Multiplier index for the SSSP delta (see kDeltaScale); -1 = heuristic.
-int policy_choose_delta(Policy* p, const float* feat);
+// Decisions from the outputs read back with the counters; -1 = no
+// confident choice (use the heuristic).
+int policy_pick_direction(const float* out);
+int policy_pick_delta(const float* out);
 
 }  // namespace cgb

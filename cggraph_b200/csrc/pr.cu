@@ -8,148 +8,141 @@
 // engine evaluates the formula in FP64 by pulling over the in-edge CSC, which
 // needs no atomics and gives the same result on every run.
 //
-// One launch per iteration reads contrib[u] = pr[u]/outdeg[u] of the previous
-// iteration and writes both pr' and contrib' (the division is fused into the
-// epilogue), so an iteration streams in_src (4 B/edge), gathers contrib
-// (8 B/edge), and writes 16 B/vertex.
+// Layout (built once per graph, graph.cu ensure_pr): vertices are relabelled
+// by a stable sort on (out-degree bucket floor(log2 outdeg), largest first
+// and zero out-degree last; then in-degree, largest first).  Every
+// contribution that is ever gathered (vertices with out-edges) then lies in
+// one dense prefix of contrib[] (RMAT-24: 7.4 M of 16.8 M vertices, 59 MB,
+// L2-resident), and consecutive rows have nearly equal in-degrees.  Rows are
+// the relabelled vertices in order, so pr'/contrib' writes are coalesced;
+// one last pass maps the result back to the caller's vertex ids.
 //
-// Work split (rows = destination vertices, in natural order so pr' writes are
-// coalesced): a warp owns 32 consecutive rows.
-//   in-degree >= kPrHuge      a whole CTA per row, in k_pr_huge_rows;
-//   32 <= in-degree < kPrHuge the warp walks the row (ballot election) and
-//                             reduces with a fixed shuffle tree;
-//   in-degree < 32            the warp gathers the concatenated short rows 32
-//                             edges at a time: each lane finds its row by a
-//                             5-step shuffle binary search over the warp's
-//                             inclusive degree scan, then a segmented shuffle
-//                             scan sums each row's run and the run's last lane
-//                             adds it to the row's shared-memory accumulator.
-// Every reduction order is fixed by the graph alone, so results are
+// One launch of k_pr_pull per iteration reads contrib[u] = pr[u]/outdeg[u]
+// of the previous iteration and writes pr' and contrib' (the division is
+// fused into the epilogue).  Rows below kPrHuge in-edges are stored as a
+// sliced ELL (SELL-32: 32 consecutive rows per slice, edge j of lane l at
+// slice base + 32j + l, padded to the slice's longest row); ordering rows by
+// in-degree inside each out-degree bucket keeps the padding under 1 % on
+// RMAT.  A warp sums one slice, one row per lane (k_pr_pull).  Rows of
+// kPrHuge or more in-edges are cut into kPrChunk-edge chunks summed by
+// separate CTAs (k_pr_hub_chunks) and combined in chunk order
+// (k_pr_hub_finish).
+// Every summation order is fixed by the graph alone, so results are
 // bit-reproducible.
 #include "engine.cuh"
 
 namespace cgb {
 
-__global__ void k_pr_init(uint32_t V, const uint32_t* __restrict__ off, double* pr, double* contrib)
+__global__ void k_pr_init(uint32_t V, const uint32_t* __restrict__ outdeg, double* pr, double* contrib)
 {
     const double p0 = 1.0 / (double)V;
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
-        const uint32_t deg = off[v + 1] - off[v];
+        const uint32_t deg = outdeg[v];
         pr[v] = p0;
         contrib[v] = deg ? p0 / (double)deg : 0.0;
     }
 }
 
-__device__ __forceinline__ double shfl_d(double x, int src)
-{
-    return __shfl_sync(0xffffffffu, x, src);
-}
-
-__global__ void __launch_bounds__(kBlock) k_pr_pull(uint32_t V, const uint32_t* __restrict__ in_off,
-                                                    const uint32_t* __restrict__ in_src,
-                                                    const uint32_t* __restrict__ off,
+// One warp per 32-row slice of the sliced ELL: in step j every lane loads
+// its row's j-th source (one coalesced 128-byte load per warp) and gathers
+// that contribution; eight steps are issued before they are summed, in j
+// order, so each lane keeps eight gathers in flight.  Padding slots name
+// vertex V, whose contribution is 0.  Hub rows (bit set in hub_bm) are
+// finished by k_pr_hub_finish.  The slice stream and the outputs use
+// evict-first accesses so that L2 keeps the gathered contributions.
+__global__ void __launch_bounds__(kBlock) k_pr_pull(uint32_t V, const uint64_t* __restrict__ slice_ptr,
+                                                    const uint32_t* __restrict__ slice_len,
+                                                    const uint32_t* __restrict__ col,
+                                                    const uint32_t* __restrict__ hub_bm,
+                                                    const uint32_t* __restrict__ outdeg,
                                                     const double* __restrict__ contrib, double* __restrict__ pr_out,
                                                     double* __restrict__ contrib_out, double base, double damp)
 {
-    __shared__ double s_acc[kBlock];
     const uint32_t lane = lane_id();
-    const uint32_t wib = threadIdx.x >> 5;
-    double* acc_w = s_acc + wib * 32;
+    const uint32_t nslices = (V + 31) / 32;
     const uint32_t nwarps = gridDim.x * (kBlock / 32);
-    for (uint32_t grp = blockIdx.x * (kBlock / 32) + wib; grp * 32u < V; grp += nwarps) {
-        const uint32_t r = grp * 32 + lane;
-        uint32_t s = 0, d = 0;
-        if (r < V) {
-            s = in_off[r];
-            d = in_off[r + 1] - s;
-        }
+    for (uint32_t s = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5); s < nslices; s += nwarps) {
+        const uint32_t len = slice_len[s];
+        const uint32_t* c = col + slice_ptr[s] + lane;
         double acc = 0.0;
-        // long rows, one at a time
-        uint32_t lmask = __ballot_sync(0xffffffffu, d >= 32 && d < kPrHuge);
-        while (lmask) {
-            const uint32_t leader = __ffs(lmask) - 1;
-            lmask &= lmask - 1;
-            const uint32_t st = __shfl_sync(0xffffffffu, s, leader);
-            const uint32_t dg = __shfl_sync(0xffffffffu, d, leader);
-            double sum = 0.0;
-            for (uint32_t k = lane; k < dg; k += 32) sum += contrib[in_src[st + k]];
-            sum = warp_sum(sum);
-            if (lane == leader) acc = sum;
-        }
-        // short rows, segmented
-        const uint32_t sd = d < 32 ? d : 0;
-        const uint32_t incl = warp_incl_scan(sd);
-        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-        acc_w[lane] = 0.0;
-        __syncwarp();
-        for (uint32_t base_k = 0; base_k < total; base_k += 32) {
-            const uint32_t k = base_k + lane;
-            const bool valid = k < total;
-            // owner = number of lanes whose inclusive scan is <= k
-            uint32_t j = 0;
+        uint32_t j = 0;
+        for (; j + 8 <= len; j += 8) {
+            uint32_t u[8];
 #pragma unroll
-            for (uint32_t b = 16; b > 0; b >>= 1) {
-                const uint32_t probe = __shfl_sync(0xffffffffu, incl, j + b - 1);
-                if (probe <= k) j += b;
-            }
-            const uint32_t own_incl = __shfl_sync(0xffffffffu, incl, j);
-            const uint32_t own_sd = __shfl_sync(0xffffffffu, sd, j);
-            const uint32_t own_s = __shfl_sync(0xffffffffu, s, j);
-            double val = 0.0;
-            if (valid) val = contrib[in_src[own_s + (k - (own_incl - own_sd))]];
-            // segmented inclusive scan over runs of equal owner
+            for (int t = 0; t < 8; t++) u[t] = __ldcs(c + 32u * (j + t));  // read once: evict first
+            double x[8];
 #pragma unroll
-            for (uint32_t o = 1; o < 32; o <<= 1) {
-                const double nv = shfl_d(val, (int)(lane >= o ? lane - o : lane));
-                const uint32_t no = __shfl_sync(0xffffffffu, j, lane >= o ? lane - o : lane);
-                if (lane >= o && no == j) val += nv;
-            }
-            const uint32_t next_j = __shfl_sync(0xffffffffu, j, lane < 31 ? lane + 1 : lane);
-            const bool next_valid = __shfl_sync(0xffffffffu, (uint32_t)valid, lane < 31 ? lane + 1 : lane);
-            const bool tail = valid && (lane == 31 || !next_valid || next_j != j);
-            if (tail) acc_w[j] += val;
-            __syncwarp();
+            for (int t = 0; t < 8; t++) x[t] = contrib[u[t]];
+#pragma unroll
+            for (int t = 0; t < 8; t++) acc += x[t];
         }
-        if (sd) acc = acc_w[lane];
-        __syncwarp();
-        if (r < V && d < kPrHuge) {
+        for (; j < len; j++) acc += contrib[__ldcs(c + 32u * j)];
+        const uint32_t r = s * 32 + lane;
+        const bool hub = (hub_bm[s] >> lane) & 1u;
+        if (r < V && !hub) {
             const double p = base + damp * acc;
-            const uint32_t od = off[r + 1] - off[r];
-            pr_out[r] = p;
-            contrib_out[r] = od ? p / (double)od : 0.0;
+            const uint32_t od = __ldcs(outdeg + r);
+            __stcs(pr_out + r, p);  // not read again this iteration: keep L2 for the gathers
+            __stcs(contrib_out + r, od ? p / (double)od : 0.0);
         }
     }
 }
 
-// Rows with in-degree >= kPrHuge: one CTA per row, fixed reduction tree.
-__global__ void __launch_bounds__(kBlock) k_pr_huge_rows(const uint32_t* __restrict__ rows, uint32_t n,
-                                                         const uint32_t* __restrict__ in_off,
-                                                         const uint32_t* __restrict__ in_src,
-                                                         const uint32_t* __restrict__ off,
-                                                         const double* __restrict__ contrib, double* pr_out,
-                                                         double* contrib_out, double base, double damp)
+// One CTA per kPrChunk-edge chunk of a hub row: fixed-order partial sum.
+__global__ void __launch_bounds__(kBlock) k_pr_hub_chunks(const uint2* __restrict__ chunks, uint32_t n,
+                                                          const uint32_t* __restrict__ in_off,
+                                                          const uint32_t* __restrict__ in_src,
+                                                          const double* __restrict__ contrib, double* part)
 {
     __shared__ double s_part[kBlock / 32];
-    for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
-        const uint32_t r = rows[i];
-        const uint32_t s = in_off[r], e = in_off[r + 1];
+    for (uint32_t c = blockIdx.x; c < n; c += gridDim.x) {
+        const uint2 ch = chunks[c];
+        const uint32_t e1 = min(in_off[ch.x + 1], ch.y + kPrChunk);
         double sum = 0.0;
-        for (uint32_t k = s + threadIdx.x; k < e; k += kBlock) sum += contrib[in_src[k]];
+        uint32_t k = ch.y + threadIdx.x;
+        for (; k + 3 * kBlock < e1; k += 4 * kBlock) {
+            const uint32_t u0 = in_src[k], u1 = in_src[k + kBlock];
+            const uint32_t u2 = in_src[k + 2 * kBlock], u3 = in_src[k + 3 * kBlock];
+            const double c0 = contrib[u0], c1 = contrib[u1], c2 = contrib[u2], c3 = contrib[u3];
+            sum += c0;
+            sum += c1;
+            sum += c2;
+            sum += c3;
+        }
+        for (; k < e1; k += kBlock) sum += contrib[in_src[k]];
         sum = warp_sum(sum);
         if (lane_id() == 0) s_part[threadIdx.x >> 5] = sum;
         __syncthreads();
         if (threadIdx.x < 32) {
             double t = threadIdx.x < kBlock / 32 ? s_part[threadIdx.x] : 0.0;
             t = warp_sum(t);
-            if (threadIdx.x == 0) {
-                const double p = base + damp * t;
-                const uint32_t od = off[r + 1] - off[r];
-                pr_out[r] = p;
-                contrib_out[r] = od ? p / (double)od : 0.0;
-            }
+            if (threadIdx.x == 0) part[c] = t;
         }
         __syncthreads();
     }
+}
+
+// Hub rows: sum their chunk partials in chunk order, then the epilogue.
+__global__ void k_pr_hub_finish(const uint32_t* __restrict__ rows, uint32_t n, const uint32_t* __restrict__ base_idx,
+                                const double* __restrict__ part, const uint32_t* __restrict__ outdeg, double* pr_out,
+                                double* contrib_out, double base, double damp)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double t = 0.0;
+        for (uint32_t c = base_idx[i]; c < base_idx[i + 1]; c++) t += part[c];
+        const uint32_t r = rows[i];
+        const double p = base + damp * t;
+        const uint32_t od = outdeg[r];
+        pr_out[r] = p;
+        contrib_out[r] = od ? p / (double)od : 0.0;
+    }
+}
+
+// Back to the caller's vertex ids: out[v] = pr[rank[v]].
+__global__ void k_pr_unpermute(uint32_t V, const uint32_t* __restrict__ rank, const double* __restrict__ pr,
+                               double* out)
+{
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) out[v] = pr[rank[v]];
 }
 
 void run_pr(cgb_graph* g, uint32_t iters, const cgb_options& o)
@@ -164,27 +157,37 @@ void run_pr(cgb_graph* g, uint32_t iters, const cgb_options& o)
     CGB_CUDA_TRY(cudaEventRecord(g->ev_start, g->stream));
     if (timing) ktimer_begin(g, CGB_K_INIT);
     ++g->stats.launches;
-    k_pr_init<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, g->off, g->pr[0], g->contrib[0]);
+    k_pr_init<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, g->pr_outdeg, g->pr[0], g->contrib[0]);
     if (timing) ktimer_end(g);
     const uint32_t grid = grid_for(div_up(V, 32), kBlock / 32, kNumSMs * 16);
     int cur = 0;
     for (uint32_t it = 0; it < iters; it++) {
         const int out = cur ^ 1;
         if (timing) ktimer_begin(g, CGB_K_PR);
+        if (g->n_pr_chunks) {
+            ++g->stats.launches;
+            k_pr_hub_chunks<<<std::min<uint32_t>(g->n_pr_chunks, kNumSMs * 8), kBlock, 0, g->stream>>>(
+                g->pr_chunks, g->n_pr_chunks, g->pr_off, g->pr_src, g->contrib[cur], g->pr_part);
+        }
         ++g->stats.launches;
-        k_pr_pull<<<grid, kBlock, 0, g->stream>>>(V, g->in_off, g->in_src, g->off, g->contrib[cur], g->pr[out],
-                                                  g->contrib[out], base, damp);
+        k_pr_pull<<<grid, kBlock, 0, g->stream>>>(V, g->pr_slice_ptr, g->pr_slice_len, g->pr_col, g->pr_hub_bm,
+                                                  g->pr_outdeg, g->contrib[cur], g->pr[out], g->contrib[out], base,
+                                                  damp);
         if (g->n_pr_huge) {
             ++g->stats.launches;
-            k_pr_huge_rows<<<std::min<uint32_t>(g->n_pr_huge, kNumSMs * 8), kBlock, 0, g->stream>>>(
-                g->pr_huge_rows, g->n_pr_huge, g->in_off, g->in_src, g->off, g->contrib[cur], g->pr[out],
+            k_pr_hub_finish<<<grid_for(g->n_pr_huge, kBlock, kNumSMs), kBlock, 0, g->stream>>>(
+                g->pr_huge_rows, g->n_pr_huge, g->pr_chunk_base, g->pr_part, g->pr_outdeg, g->pr[out],
                 g->contrib[out], base, damp);
         }
         if (timing) ktimer_end(g);
         cur = out;
     }
+    // the other pr buffer receives the result in the caller's ids
+    ++g->stats.launches;
+    k_pr_unpermute<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, g->pr_rank, g->pr[cur],
+                                                                               g->pr[cur ^ 1]);
     CGB_CUDA_TRY(cudaEventRecord(g->ev_stop, g->stream));
-    g->result = g->pr[cur];
+    g->result = g->pr[cur ^ 1];
     g->stats.iterations = iters;
 }
 

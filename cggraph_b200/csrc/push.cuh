@@ -23,9 +23,38 @@
 
 namespace cgb {
 
+// Fine-grained tier: a CTA-wide exclusive scan of the (small) remaining
+// degrees packs the lists into shared memory, one edge per thread per round.
+// Every thread of the CTA must call it.
+template <class Op>
+__device__ __forceinline__ void fine_tier(const Op& op, uint32_t start, uint32_t deg, uint32_t msg, uint32_t* s_scan,
+                                          uint32_t* s_edge, uint32_t* s_emsg)
+{
+    const uint32_t tid = threadIdx.x;
+    uint32_t total;
+    const uint32_t rank = block_excl_scan(deg, total, s_scan);
+    uint32_t consumed = 0;
+    for (uint32_t done = 0; done < total; done += kBlock) {
+        while (consumed < deg && rank + consumed < done + kBlock) {
+            s_edge[rank + consumed - done] = start + consumed;
+            s_emsg[rank + consumed - done] = msg;
+            consumed++;
+        }
+        __syncthreads();
+        const uint32_t n = min((uint32_t)kBlock, total - done);
+        const bool valid = tid < n;
+        op.edge(valid, valid ? s_edge[tid] : 0u, valid ? s_emsg[tid] : 0u);
+        __syncthreads();
+    }
+}
+
 // Op interface:
 //   __device__ bool load(uint32_t v, uint32_t& start, uint32_t& deg, uint32_t& msg) const;
 //   __device__ void edge(bool valid, uint32_t e, uint32_t msg) const;   // warp-collective
+// and, for the engine's kernels (k_push_binned, k_push_chunks), per-CTA hooks
+// around all of a CTA's work, each followed / preceded by a CTA barrier:
+//   __device__ void block_begin() const;   // e.g. zero shared accumulators
+//   __device__ void block_end() const;     // e.g. flush them with one atomic
 template <class Op, bool kIdentity>
 __global__ void __launch_bounds__(kBlock) k_push_twc(const uint32_t* __restrict__ qin, uint32_t nin, Op op,
                                                      uint32_t* __restrict__ huge_q, uint32_t* huge_len,
@@ -75,22 +104,7 @@ __global__ void __launch_bounds__(kBlock) k_push_twc(const uint32_t* __restrict_
             if (lane_id() == leader) deg = 0;
             for (uint32_t k = 0; k < dg; k += 32) op.edge(k + lane_id() < dg, st + k + lane_id(), m);
         }
-        // fine-grained tier
-        uint32_t total;
-        const uint32_t rank = block_excl_scan(deg, total, s_scan);
-        uint32_t consumed = 0;
-        for (uint32_t done = 0; done < total; done += kBlock) {
-            while (consumed < deg && rank + consumed < done + kBlock) {
-                s_edge[rank + consumed - done] = start + consumed;
-                s_emsg[rank + consumed - done] = msg;
-                consumed++;
-            }
-            __syncthreads();
-            const uint32_t n = min((uint32_t)kBlock, total - done);
-            const bool valid = tid < n;
-            op.edge(valid, valid ? s_edge[tid] : 0u, valid ? s_emsg[tid] : 0u);
-            __syncthreads();
-        }
+        fine_tier(op, start, deg, msg, s_scan, s_edge, s_emsg);
     }
 }
 
@@ -117,19 +131,97 @@ __global__ void __launch_bounds__(kBlock) k_push_huge(const uint32_t* __restrict
     }
 }
 
-// Launches the TWC expansion (plus the hub kernel) of a queue whose length
-// the host knows.
+// Binned expansion used by the engine.  Lists of at least kBigDeg edges are
+// cut into kChunk-edge chunks whose descriptors (vertex, chunk index) go to a
+// chunk queue; k_push_chunks then deals the chunks across the whole grid, so
+// a frontier of a few hubs keeps every SM busy however few vertices it has.
+// Lists of 32..kBigDeg-1 edges are walked by one warp, shorter ones by the
+// fine-grained tier.  Chunk-queue capacity E/kChunk + E/kBigDeg + 64 bounds
+// any frontier in which each vertex appears once.
+template <class Op, bool kIdentity>
+__global__ void __launch_bounds__(kBlock) k_push_binned(const uint32_t* __restrict__ qin, uint32_t nin, Op op,
+                                                        uint2* __restrict__ chunk_q, uint32_t* chunk_len,
+                                                        uint32_t chunk_cap, uint32_t* overflow)
+{
+    __shared__ uint32_t s_scan[kBlock / 32 + 1];
+    __shared__ uint32_t s_edge[kBlock];
+    __shared__ uint32_t s_emsg[kBlock];
+    op.block_begin();
+    __syncthreads();
+    for (uint32_t base = blockIdx.x * kBlock; base < nin; base += gridDim.x * kBlock) {
+        const uint32_t i = base + threadIdx.x;
+        uint32_t v = 0, start = 0, deg = 0, msg = 0;
+        if (i < nin) {
+            v = kIdentity ? i : qin[i];
+            if (!op.load(v, start, deg, msg)) deg = 0;
+        }
+        // big lists: the warp writes their chunk descriptors together
+        uint32_t bmask;
+        while ((bmask = __ballot_sync(0xffffffffu, deg >= kBigDeg)) != 0) {
+            const uint32_t leader = __ffs(bmask) - 1;
+            const uint32_t bv = __shfl_sync(0xffffffffu, v, leader);
+            const uint32_t nch = (__shfl_sync(0xffffffffu, deg, leader) + kChunk - 1) / kChunk;
+            uint32_t slot = 0;
+            if (lane_id() == 0) slot = atomicAdd(chunk_len, nch);
+            slot = __shfl_sync(0xffffffffu, slot, 0);
+            for (uint32_t c = lane_id(); c < nch; c += 32) {
+                if (slot + c < chunk_cap) chunk_q[slot + c] = make_uint2(bv, c);
+                else atomicOr(overflow, 1u);
+            }
+            if (lane_id() == leader) deg = 0;
+        }
+        // warp tier
+        uint32_t wmask;
+        while ((wmask = __ballot_sync(0xffffffffu, deg >= 32)) != 0) {
+            const uint32_t leader = __ffs(wmask) - 1;
+            const uint32_t st = __shfl_sync(0xffffffffu, start, leader);
+            const uint32_t dg = __shfl_sync(0xffffffffu, deg, leader);
+            const uint32_t m = __shfl_sync(0xffffffffu, msg, leader);
+            if (lane_id() == leader) deg = 0;
+            for (uint32_t k = 0; k < dg; k += 32) op.edge(k + lane_id() < dg, st + k + lane_id(), m);
+        }
+        fine_tier(op, start, deg, msg, s_scan, s_edge, s_emsg);
+    }
+    __syncthreads();
+    op.block_end();
+}
+
+// One CTA per chunk descriptor, grid-stride over the chunk queue.
 template <class Op>
-inline void launch_push_twc(cgb_graph* g, const uint32_t* qin, uint32_t nin, const Op& op, bool identity)
+__global__ void __launch_bounds__(kBlock) k_push_chunks(const uint2* __restrict__ chunk_q, const uint32_t* chunk_len,
+                                                        uint32_t chunk_cap, Op op)
+{
+    const uint32_t n = min(*chunk_len, chunk_cap);
+    if (blockIdx.x >= n) return;
+    op.block_begin();
+    __syncthreads();
+    for (uint32_t c = blockIdx.x; c < n; c += gridDim.x) {
+        const uint2 d = chunk_q[c];
+        uint32_t start, deg, msg;
+        if (!op.load(d.x, start, deg, msg)) continue;
+        const uint32_t cs = d.y * kChunk;
+        const uint32_t ce = min(deg, cs + kChunk);
+        for (uint32_t k = cs; k < ce; k += kBlock) op.edge(k + threadIdx.x < ce, start + k + threadIdx.x, msg);
+    }
+    __syncthreads();
+    op.block_end();
+}
+
+// Launches the binned expansion (plus the chunk kernel) of a queue whose
+// length the host knows.  The chunk-queue length must be zero beforehand.
+template <class Op>
+inline void launch_push(cgb_graph* g, const uint32_t* qin, uint32_t nin, const Op& op, bool identity)
 {
     if (nin == 0) return;
     const uint32_t grid = grid_for(nin, kBlock, kNumSMs * 8);
     g->stats.launches += 2;
     if (identity)
-        k_push_twc<Op, true><<<grid, kBlock, 0, g->stream>>>(qin, nin, op, g->huge_q, &g->ctr->huge_len, g->V);
+        k_push_binned<Op, true><<<grid, kBlock, 0, g->stream>>>(qin, nin, op, g->chunk_q, &g->ctr->chunk_len,
+                                                                 g->chunk_cap, &g->ctr->overflow);
     else
-        k_push_twc<Op, false><<<grid, kBlock, 0, g->stream>>>(qin, nin, op, g->huge_q, &g->ctr->huge_len, g->V);
-    k_push_huge<Op><<<kNumSMs * 4, kBlock, 0, g->stream>>>(g->huge_q, &g->ctr->huge_len, g->V, op);
+        k_push_binned<Op, false><<<grid, kBlock, 0, g->stream>>>(qin, nin, op, g->chunk_q, &g->ctr->chunk_len,
+                                                                  g->chunk_cap, &g->ctr->overflow);
+    k_push_chunks<Op><<<kNumSMs * 8, kBlock, 0, g->stream>>>(g->chunk_q, &g->ctr->chunk_len, g->chunk_cap, op);
 }
 
 }  // namespace cgb

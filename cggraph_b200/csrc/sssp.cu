@@ -1,4 +1,4 @@
-// Delta-stepping SSSP (near/far piles) with atomicMin relaxation.
+// Delta-stepping SSSP (near queue, far bitmap) with atomicMin relaxation.
 //
 // Result semantics follow the reference's SSSP: dist[root] = 0, relaxation
 // dist[d] = min(dist[d], dist[u] + w) applied only when it lowers the value
@@ -10,17 +10,21 @@
 // bit-identical.
 //
 // Schedule: vertices whose tentative distance is below the current threshold
-// form the near queue, which is expanded round after round with the
-// degree-binned push of push.cuh; improvements at or above the threshold go
-// to the far pile as (vertex, distance) pairs.  When the near queue empties
-// the threshold advances by delta and the far pile is split: entries whose
-// distance is stale are dropped, those below the new threshold become the
-// near queue.  A per-vertex stamp keeps each vertex at most once per round.
+// T form the near queue, which is expanded round after round with the
+// degree-binned push of push.cuh; a vertex improved to a distance >= T sets
+// its bit in the far bitmap (V/32 words, L2-resident).  When the near queue
+// empties, the bitmap is split at [T, T + delta): those vertices become the
+// near queue, vertices below T are dropped (any improvement below T was
+// pushed to the near queue and has been expanded), the rest stay.  A near
+// bitmap, cleared before each round, keeps each vertex at most once in a
+// round's queue.
 #include "engine.cuh"
 #include "policy.cuh"
 #include "push.cuh"
 
 namespace cgb {
+
+__shared__ uint32_t s_sssp_newfar;  // per-CTA count of vertices newly set in the far bitmap
 
 template <bool kHasW>
 struct SsspOp {
@@ -28,16 +32,13 @@ struct SsspOp {
     const uint32_t* __restrict__ dst;
     const uint32_t* __restrict__ w;
     uint32_t* dist;
-    uint32_t* stamp;
-    uint32_t it;
+    uint32_t* near_bm;  // dedup of this round's near queue (cleared before the round)
     uint32_t thr;
     uint32_t nz;
     uint32_t* near_out;
     uint32_t* near_len;
     uint32_t cap;
-    uint2* far_out;
-    uint32_t* far_len;
-    uint32_t far_cap;
+    uint32_t* far_bm;
     DevCounters* ctr;
 
     __device__ __forceinline__ bool load(uint32_t v, uint32_t& s, uint32_t& d, uint32_t& m) const
@@ -49,33 +50,48 @@ struct SsspOp {
     }
     __device__ __forceinline__ void edge(bool valid, uint32_t e, uint32_t du) const
     {
-        bool to_near = false, to_far = false;
-        uint32_t d = 0, nd = 0;
+        bool to_near = false, new_far = false;
+        uint32_t d = 0;
         if (valid) {
             d = dst[e];
             const uint64_t cand = (uint64_t)du + (kHasW ? (uint64_t)w[e] : 1ull);
             if (cand < kValueMax) {
-                nd = (uint32_t)cand;
+                const uint32_t nd = (uint32_t)cand;
                 if (nd < dist[d]) {
                     const uint32_t old = atomicMin(dist + d, nd);
                     if (nd < old && d < nz) {
-                        if (nd < thr) to_near = atomicExch(stamp + d, it) != it;
-                        else to_far = true;
+                        if (nd < thr) {
+                            const uint32_t bit = 1u << (d & 31u);
+                            uint32_t* wp = near_bm + (d >> 5);
+                            to_near = !(*wp & bit) && !(atomicOr(wp, bit) & bit);
+                        } else {
+                            const uint32_t bit = 1u << (d & 31u);
+                            uint32_t* wp = far_bm + (d >> 5);
+                            new_far = !(*wp & bit) && !(atomicOr(wp, bit) & bit);
+                        }
                     }
                 }
             }
         }
         warp_append(to_near, d, near_out, near_len, cap, &ctr->overflow);
-        warp_append2(to_far, make_uint2(d, nd), far_out, far_len, far_cap, &ctr->overflow);
+        const uint32_t nf = __popc(__ballot_sync(0xffffffffu, new_far));
+        if (nf && lane_id() == 0) atomicAdd(&s_sssp_newfar, nf);
+    }
+    __device__ __forceinline__ void block_begin() const
+    {
+        if (threadIdx.x == 0) s_sssp_newfar = 0;
+    }
+    __device__ __forceinline__ void block_end() const
+    {
+        if (threadIdx.x == 0 && s_sssp_newfar) atomicAdd(&ctr->far_len[0], s_sssp_newfar);
     }
 };
 
-__global__ void k_sssp_init(uint32_t V, uint32_t* dist, uint32_t* stamp)
+__global__ void k_sssp_init(uint32_t V, uint32_t* dist, uint32_t* far_bm, uint32_t words)
 {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < V; i += gridDim.x * blockDim.x) {
-        dist[i] = kValueMax;
-        stamp[i] = 0;
-    }
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < V; i += stride) dist[i] = kValueMax;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < words; i += stride) far_bm[i] = 0;
 }
 
 __global__ void k_sssp_root(uint32_t* dist, uint32_t root, uint32_t* q0)
@@ -84,34 +100,48 @@ __global__ void k_sssp_root(uint32_t* dist, uint32_t root, uint32_t* q0)
     q0[0] = root;
 }
 
-// Splits the far pile at threshold thr (see file comment).
-__global__ void __launch_bounds__(kBlock) k_sssp_split(const uint2* __restrict__ far_in, uint32_t n,
-                                                       const uint32_t* dist, uint32_t thr, uint32_t* stamp,
-                                                       uint32_t it, uint32_t* near_out, uint32_t* near_len,
-                                                       uint32_t cap, uint2* far_out, uint32_t* far_len,
-                                                       uint32_t far_cap, DevCounters* ctr)
+// Splits the far bitmap at [lo, hi) (see file comment).  One lane per bitmap
+// word; far_len[0] receives the number of vertices left in the bitmap and
+// min_far the smallest distance among them.
+__global__ void __launch_bounds__(kBlock) k_sssp_split(uint32_t words, uint32_t* far_bm, const uint32_t* dist,
+                                                       uint32_t lo, uint32_t hi, uint32_t* near_out,
+                                                       uint32_t* near_len, uint32_t cap, DevCounters* ctr)
 {
-    uint32_t mn = kValueMax;
+    uint32_t mn = kValueMax, left = 0;
     const uint32_t stride = gridDim.x * blockDim.x;
-    const uint32_t n_round = (n + 31u) & ~31u;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_round; i += stride) {
-        bool to_near = false, to_far = false;
-        uint2 ent = make_uint2(0, 0);
-        if (i < n) {
-            ent = far_in[i];
-            if (dist[ent.x] == ent.y) {
-                if (ent.y < thr) to_near = atomicExch(stamp + ent.x, it) != it;
-                else {
-                    to_far = true;
-                    mn = min(mn, ent.y);
+    const uint32_t words_round = (words + 31u) & ~31u;
+    for (uint32_t wi = blockIdx.x * blockDim.x + threadIdx.x; wi < words_round; wi += stride) {
+        uint32_t word = wi < words ? far_bm[wi] : 0u;
+        uint32_t keep = word;
+        // at most 32 near candidates per lane: append them one bit position at a time
+        while (__any_sync(0xffffffffu, word != 0)) {
+            bool to_near = false;
+            uint32_t v = 0;
+            if (word) {
+                const uint32_t b = __ffs(word) - 1;
+                word &= word - 1;
+                v = wi * 32 + b;
+                const uint32_t dv = dist[v];
+                if (dv < hi) {
+                    keep &= ~(1u << b);
+                    to_near = dv >= lo;
+                } else {
+                    mn = min(mn, dv);
                 }
             }
+            warp_append(to_near, v, near_out, near_len, cap, &ctr->overflow);
         }
-        warp_append(to_near, ent.x, near_out, near_len, cap, &ctr->overflow);
-        warp_append2(to_far, ent, far_out, far_len, far_cap, &ctr->overflow);
+        if (wi < words) {
+            if (keep != far_bm[wi]) far_bm[wi] = keep;
+            left += __popc(keep);
+        }
     }
     mn = __reduce_min_sync(0xffffffffu, mn);
-    if (lane_id() == 0 && mn != kValueMax) atomicMin(&ctr->min_far, mn);
+    left = warp_sum(left);
+    if (lane_id() == 0) {
+        if (mn != kValueMax) atomicMin(&ctr->min_far, mn);
+        if (left) atomicAdd(&ctr->far_len[0], left);
+    }
 }
 
 template <bool kHasW>
@@ -120,40 +150,43 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
     const bool timing = g->flags & CGB_FLAG_KERNEL_TIMING;
     const bool tracing = g->flags & CGB_FLAG_TRACE;
     const uint32_t V = g->V;
+    const uint32_t words = g->words();
+    uint32_t* far_bm = g->front_bm;  // the BFS bitmaps are free during SSSP
+    uint32_t* near_bm = g->visited;
     const uint64_t max_iters = o.max_iterations ? o.max_iterations : ~0ull;
     Policy* pol = (o.schedule == CGB_SCHED_LEARNED) ? policy_get() : nullptr;
+    PolicySamples* collect = g->collect;
     const uint32_t base_delta = delta;
 
     CGB_CUDA_TRY(cudaEventRecord(g->ev_start, g->stream));
     if (timing) ktimer_begin(g, CGB_K_INIT);
     ++g->stats.launches;
-    k_sssp_init<<<kNumSMs * 4, kBlock, 0, g->stream>>>(V, g->value, g->stamp);
+    k_sssp_init<<<kNumSMs * 4, kBlock, 0, g->stream>>>(V, g->value, far_bm, words);
     ++g->stats.launches;
     k_sssp_root<<<1, 1, 0, g->stream>>>(g->value, root, g->q[0]);
-    CGB_CUDA_TRY(cudaMemsetAsync(g->ctr, 0, sizeof(DevCounters), g->stream));
     if (timing) ktimer_end(g);
 
-    int cur = 0, fcur = 0;
+    int cur = 0;
     uint64_t nnear = root < g->nz ? 1 : 0;
     uint64_t nfar = 0;
     uint64_t thr = delta;
-    uint32_t it = 1;
     uint64_t iters = 0;
-    uint64_t settled_guess = 0;
+    uint64_t expanded = 0;
 
-    for (;;) {
+    // Near rounds at threshold thr until the near queue is empty.
+    auto near_rounds = [&]() {
         while (nnear > 0) {
             CGB_REQUIRE(iters < max_iters, CGB_ETIMEOUT, "SSSP iteration budget exhausted");
-            it++;
             const int out = cur ^ 1;
             CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->qlen[out], 0, sizeof(uint32_t), g->stream));
-            CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->huge_len, 0, sizeof(uint32_t), g->stream));
+            CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->chunk_len, 0, sizeof(uint32_t), g->stream));
+            CGB_CUDA_TRY(cudaMemsetAsync(near_bm, 0, (size_t)words * sizeof(uint32_t), g->stream));
             if (tracing) CGB_CUDA_TRY(cudaEventRecord(g->ev_iter[0], g->stream));
             if (timing) ktimer_begin(g, CGB_K_PUSH);
-            SsspOp<kHasW> op{g->off, g->dst, g->w, g->value, g->stamp, it, (uint32_t)std::min<uint64_t>(thr, kValueMax),
-                             g->nz, g->q[out], &g->ctr->qlen[out], V, g->far[fcur], &g->ctr->far_len[fcur],
-                             g->far_cap, g->ctr};
-            launch_push_twc(g, g->q[cur], (uint32_t)nnear, op, false);
+            SsspOp<kHasW> op{g->off, g->dst, g->w, g->value, near_bm,
+                             (uint32_t)std::min<uint64_t>(thr, kValueMax), g->nz, g->q[out], &g->ctr->qlen[out], V,
+                             far_bm, g->ctr};
+            launch_push(g, g->q[cur], (uint32_t)nnear, op, false);
             if (timing) ktimer_end(g);
             if (tracing) CGB_CUDA_TRY(cudaEventRecord(g->ev_iter[1], g->stream));
             sync_counters(g);
@@ -165,59 +198,112 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
                 t.iteration = (uint32_t)iters;
                 t.algorithm = CGB_SSSP;
                 t.frontier_vertices = nnear;
-                t.unvisited_vertices = nfar;
+                t.unvisited_vertices = g->h_ctr->far_len[0];
                 t.variant = CGB_VAR_TWC;
                 t.delta = delta;
                 t.ms = ms;
                 g->trace.push_back(t);
             }
-            settled_guess += nnear;
+            expanded += nnear;
             nnear = g->h_ctr->qlen[out];
-            nfar = g->h_ctr->far_len[fcur];
+            nfar = g->h_ctr->far_len[0];
             cur = out;
             iters++;
         }
-        if (nfar == 0) break;
-        if (pol) {
-            float feat[kPolicyFeatures];
-            policy_features(feat, CGB_SSSP, g, nnear, 0, (uint64_t)V - std::min<uint64_t>(settled_guess, V), nfar, 0,
-                            (uint32_t)iters, 0, delta);
-            const int k = policy_choose_delta(pol, feat);
-            if (k >= 0) {
-                static const float scale[5] = {0.25f, 0.5f, 1.f, 2.f, 4.f};
-                delta = std::max<uint32_t>(1u, (uint32_t)(base_delta * scale[k]));
-            }
-        }
-        thr += delta;
-        // split the far pile until the near queue is non-empty or the pile is gone
+    };
+    // Next bucket [thr, thr + d): split the far bitmap (jumping over empty
+    // buckets) until the near queue is non-empty or the bitmap is empty.
+    auto advance = [&](uint32_t d) {
+        uint64_t lo = thr;
+        thr += d;
         for (;;) {
             CGB_REQUIRE(iters < max_iters, CGB_ETIMEOUT, "SSSP iteration budget exhausted");
-            it++;
             const int out = cur ^ 1;
-            const int fout = fcur ^ 1;
             CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->qlen[out], 0, sizeof(uint32_t), g->stream));
-            CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->far_len[fout], 0, sizeof(uint32_t), g->stream));
+            CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->far_len[0], 0, sizeof(uint32_t), g->stream));
             CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->min_far, 0xff, sizeof(uint32_t), g->stream));
             if (timing) ktimer_begin(g, CGB_K_FRONTIER);
             ++g->stats.launches;
-            k_sssp_split<<<grid_for(nfar, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(
-                g->far[fcur], (uint32_t)nfar, g->value, (uint32_t)std::min<uint64_t>(thr, kValueMax), g->stamp, it,
-                g->q[out], &g->ctr->qlen[out], V, g->far[fout], &g->ctr->far_len[fout], g->far_cap, g->ctr);
+            k_sssp_split<<<grid_for(words, kBlock, kNumSMs * 4), kBlock, 0, g->stream>>>(
+                words, far_bm, g->value, (uint32_t)std::min<uint64_t>(lo, kValueMax),
+                (uint32_t)std::min<uint64_t>(thr, kValueMax), g->q[out], &g->ctr->qlen[out], V, g->ctr);
             if (timing) ktimer_end(g);
             sync_counters(g);
-            CGB_REQUIRE(!g->h_ctr->overflow, CGB_EOVERFLOW, "SSSP far pile overflow");
+            CGB_REQUIRE(!g->h_ctr->overflow, CGB_EOVERFLOW, "SSSP queue overflow");
             nnear = g->h_ctr->qlen[out];
-            nfar = g->h_ctr->far_len[fout];
+            nfar = g->h_ctr->far_len[0];
             cur = out;
-            fcur = fout;
             iters++;
             if (nnear > 0 || nfar == 0) break;
-            // every remaining entry is at or above thr: jump to the bucket of the smallest
+            // every vertex left is at or above thr: jump to the bucket of the smallest
             const uint64_t mn = g->h_ctr->min_far;
-            thr = (mn / delta + 1) * (uint64_t)delta;
+            lo = thr;
+            thr = (mn / d + 1) * (uint64_t)d;
         }
-        // the next near rounds append to the pile the split just wrote
-        if (nnear == 0 && nfar == 0) break;
+    };
+    auto state_now = [&]() {
+        FeatIn in{};
+        in.alg = CGB_SSSP;
+        in.iteration = (uint32_t)iters;
+        in.symmetric = g->symmetric == 1;
+        in.V = V;
+        in.E = g->E;
+        in.nf = (double)nnear;
+        in.unvisited_v = (double)V - (double)std::min<uint64_t>(expanded, V);
+        in.delta = delta;
+        in.base_delta = base_delta;
+        in.far_count = (double)nfar;
+        in.settled = (double)std::min<uint64_t>(expanded, V);
+        return in;
+    };
+
+    near_rounds();
+    while (nfar > 0) {
+        uint32_t d = delta;
+        if (collect) {
+            // counterfactual: one bucket phase per delta choice from the same state
+            const size_t vbytes = (size_t)V * 4, wbytes = (size_t)words * 4;
+            CGB_CUDA_TRY(cudaMemcpyAsync(collect->save_value, g->value, vbytes, cudaMemcpyDeviceToDevice, g->stream));
+            CGB_CUDA_TRY(cudaMemcpyAsync(collect->save_bm0, far_bm, wbytes, cudaMemcpyDeviceToDevice, g->stream));
+            const uint64_t s_thr = thr, s_iters = iters, s_exp = expanded, s_far = nfar;
+            const int s_cur = cur;
+            float ms[kPolicyOutputs] = {};
+            bool have[kPolicyOutputs] = {};
+            int best = 2;
+            for (int k = 0; k < kNumDeltaChoices; k++) {
+                const uint32_t dk = std::max<uint32_t>(1u, (uint32_t)(base_delta * delta_scale(k)));
+                CGB_CUDA_TRY(cudaEventRecord(g->ev_iter[0], g->stream));
+                advance(dk);
+                near_rounds();
+                CGB_CUDA_TRY(cudaEventRecord(g->ev_iter[1], g->stream));
+                CGB_CUDA_TRY(cudaEventSynchronize(g->ev_iter[1]));
+                float t = 0.f;
+                CGB_CUDA_TRY(cudaEventElapsedTime(&t, g->ev_iter[0], g->ev_iter[1]));
+                // cost per unit of distance the phase covers (delta x scale)
+                ms[kOutDelta0 + k] = t / delta_scale(k);
+                have[kOutDelta0 + k] = true;
+                if (ms[kOutDelta0 + k] < ms[kOutDelta0 + best]) best = k;
+                CGB_CUDA_TRY(cudaMemcpyAsync(g->value, collect->save_value, vbytes, cudaMemcpyDeviceToDevice,
+                                             g->stream));
+                CGB_CUDA_TRY(cudaMemcpyAsync(far_bm, collect->save_bm0, wbytes, cudaMemcpyDeviceToDevice, g->stream));
+                thr = s_thr;
+                iters = s_iters;
+                expanded = s_exp;
+                nfar = s_far;
+                nnear = 0;
+                cur = s_cur;
+            }
+            policy_log_sample(g, state_now(), ms, have);
+            d = std::max<uint32_t>(1u, (uint32_t)(base_delta * delta_scale(best)));
+        } else if (pol) {
+            policy_enqueue(pol, g, state_now(), false, false, 0);
+            sync_counters(g);
+            const int k = policy_pick_delta(g->h_ctr->policy_out);
+            if (k >= 0) d = std::max<uint32_t>(1u, (uint32_t)(base_delta * delta_scale(k)));
+        }
+        delta = d;
+        advance(d);
+        near_rounds();
     }
     CGB_CUDA_TRY(cudaEventRecord(g->ev_stop, g->stream));
     g->stats.iterations = iters;
@@ -229,7 +315,7 @@ uint32_t sssp_default_delta(const cgb_graph* g)
     if (g->E == 0 || g->V == 0) return 1;
     const double mean_w = g->w ? (double)g->sum_w / (double)g->E : 1.0;
     const double mean_deg = (double)g->E / (double)g->V;
-    double d = 32.0 * mean_w / std::max(1.0, mean_deg);
+    double d = 8.0 * mean_w / std::max(1.0, mean_deg);
     if (d < 1.0) d = 1.0;
     if (d > 1e8) d = 1e8;
     return (uint32_t)d;
@@ -238,7 +324,7 @@ uint32_t sssp_default_delta(const cgb_graph* g)
 void run_sssp(cgb_graph* g, uint32_t root, const cgb_options& o)
 {
     ensure_frontier(g);
-    ensure_sssp(g);
+    if (g->w && g->sum_w == 0) compute_weight_sum(g);
     const uint32_t delta = o.sssp_delta ? o.sssp_delta : sssp_default_delta(g);
     if (g->w) sssp_loop<true>(g, root, delta, o);
     else sssp_loop<false>(g, root, delta, o);

@@ -1,0 +1,88 @@
+"""Trains the learned scheduler and writes cggraph_b200/policy_weights.npy.
+
+Training graphs (seeded, none of them a benchmark input):
+  RMAT scales 18, 20, 22 and 24 (a=.57, b=.19, c=.19, edge factor 16,
+  weights U[1,64]; seeds 2..5, the benchmark uses seed 1) and 2-D grids
+  256x256 to 1024x1024 (weights U[1,1000]).
+For each graph and a few seeded roots the engine records counterfactual
+samples (cgb_policy_collect): every BFS level timed in both directions, every
+SSSP bucket timed with delta x {1/4, 1/2, 1, 2, 4}.  The network is trained
+on the GPU by the engine's own kernels (cgb_policy_train).
+
+  python -m cggraph_b200.train_policy [--quick] [--out PATH] [--epochs N]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+import time
+import zlib
+
+import numpy as np
+
+if __package__ in (None, ""):
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+
+import cggraph_b200 as cg  # noqa: E402
+from cggraph_b200 import policy  # noqa: E402
+
+BFS, SSSP = 0, 1
+
+
+def training_graphs(quick: bool):
+    if quick:
+        yield "rmat16_s2", lambda: cg.Graph.rmat(16, 16, seed=2)
+        yield "grid128_s2", lambda: cg.Graph.grid(128, 128, seed=2)
+        return
+    for scale, seed in ((18, 2), (20, 3), (22, 4), (24, 5)):
+        yield f"rmat{scale}_s{seed}", (lambda s=scale, d=seed: cg.Graph.rmat(s, 16, seed=d))
+    for n, seed in ((256, 2), (512, 3), (1024, 4)):
+        yield f"grid{n}_s{seed}", (lambda n=n, d=seed: cg.Graph.grid(n, n, seed=d))
+
+
+def collect_all(quick: bool, roots_per_graph: int = 3, log=print):
+    Xs, Ts, Ms, info = [], [], [], []
+    for name, make in training_graphs(quick):
+        g = make()
+        off, _, _ = g.download(with_weight=False)
+        deg = np.diff(off.astype(np.int64))
+        rng = np.random.default_rng(zlib.crc32(name.encode()))
+        cand = np.nonzero(deg)[0]
+        roots = [int(deg.argmax())] + [int(x) for x in rng.choice(cand, roots_per_graph - 1, replace=False)]
+        for r in roots:
+            for alg in (BFS, SSSP):
+                t0 = time.time()
+                X, T, M = policy.collect(g, alg, r)
+                Xs.append(X)
+                Ts.append(T)
+                Ms.append(M)
+                info.append({"graph": name, "root": r, "alg": ["bfs", "sssp"][alg], "samples": len(X)})
+                log(f"  {name} root {r} {['bfs', 'sssp'][alg]}: {len(X)} samples ({time.time() - t0:.1f} s)")
+        g.close()
+    return np.concatenate(Xs), np.concatenate(Ts), np.concatenate(Ms), info
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--quick", action="store_true")
+    ap.add_argument("--out", default=policy.DEFAULT_WEIGHTS)
+    ap.add_argument("--epochs", type=int, default=400)
+    ap.add_argument("--seed", type=int, default=0)
+    args = ap.parse_args(argv)
+    X, T, M, info = collect_all(args.quick)
+    print(f"{len(X)} samples; training {args.epochs} epochs on the GPU")
+    t0 = time.time()
+    params, loss = policy.train(X, T, M, epochs=args.epochs, batch=256, lr=3e-3, seed=args.seed)
+    print(f"final mean squared error of log-costs {loss:.4f} ({time.time() - t0:.1f} s)")
+    np.save(args.out, params)
+    np.savez_compressed(os.path.splitext(args.out)[0] + "_data.npz", X=X, T=T, M=M)
+    summary = {"samples": int(len(X)), "epochs": args.epochs, "final_loss": loss, "runs": info}
+    with open(os.path.splitext(args.out)[0] + ".json", "w") as f:
+        json.dump(summary, f, indent=1)
+    return params, loss
+
+
+if __name__ == "__main__":
+    main()

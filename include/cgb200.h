@@ -209,6 +209,45 @@ cgb_status cgb_trace_get(const cgb_graph* g, cgb_iter_trace* out, uint32_t max_e
 cgb_status cgb_bfs_noalloc(const uint32_t* offsets, const uint32_t* dest, uint32_t V, uint32_t E, uint32_t root,
                            uint32_t* levels, void* stream);
 
+/* -------------------------------------------------------- learned policy */
+
+/* The per-iteration scheduler (CGB_SCHED_LEARNED) is an FP32 MLP
+ * CGB_POLICY_FEATURES -> 64 -> 64 -> CGB_POLICY_OUTPUTS whose outputs predict
+ * the log-cost of each choice: [0] BFS next level pushed, [1] pulled,
+ * [2..6] SSSP next bucket with delta x {1/4, 1/2, 1, 2, 4}; [7..8] unused.
+ * Parameters are CGB_POLICY_PARAMS floats: W1[24][64] b1[64] W2[64][64]
+ * b2[64] W3[64][9] b3[9] (row-major, input index first).  The reference has
+ * no scheduler; these entry points have no counterpart in it. */
+#define CGB_POLICY_FEATURES 24
+#define CGB_POLICY_OUTPUTS 9
+#define CGB_POLICY_PARAMS 6345
+
+/* Makes `params` the policy of the current device (NULL unloads it: the
+ * heuristic decides). */
+cgb_status cgb_policy_load(const float* params);
+
+/* Per-iteration training samples of one run: at every decision point the
+ * engine snapshots its state, runs each choice, times it with CUDA events,
+ * restores, and continues with the fastest.  features: max * 24 floats;
+ * targets: max * 9 log-costs; mask: max * 9 (1 where measured).  The run's
+ * result equals a plain cgb_run. */
+cgb_status cgb_policy_collect(cgb_graph* g, int algorithm, uint32_t root, const cgb_options* opt, float* features,
+                              float* targets, uint8_t* mask, uint32_t max, uint32_t* count);
+
+/* Trains the network on the GPU (hand-written forward, backward and Adam
+ * kernels) with masked mean-squared error on the log-costs.  init may be
+ * NULL (seeded initialisation).  Writes the trained parameters and the
+ * final epoch's mean loss. */
+cgb_status cgb_policy_train(const float* features, const float* targets, const uint8_t* mask, uint32_t n,
+                            uint32_t epochs, uint32_t batch, float lr, uint64_t seed, const float* init,
+                            float* params_out, float* final_loss);
+
+/* Forward pass of `params` on n samples (outputs n * 9), and the masked MSE
+ * loss with its full parameter gradient, both on the GPU (for checks). */
+cgb_status cgb_policy_forward(const float* params, const float* features, uint32_t n, float* outputs);
+cgb_status cgb_policy_loss_grad(const float* params, const float* features, const float* targets,
+                                const uint8_t* mask, uint32_t n, float* loss, float* grad);
+
 /* ---------------------------------------------------------------- misc */
 
 const char* cgb_last_error_string(void);

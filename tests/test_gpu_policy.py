@@ -1,0 +1,133 @@
+"""The learned scheduler: GPU forward/backward kernels against the CPU FP64
+oracle, GPU training, counterfactual sample collection, and learned runs
+whose results are bit-identical to the heuristic's (the schedule never
+changes a result).  The gain of the trained network over the heuristic is
+measured by bench.py --schedule learned and by test_learned_gain."""
+import numpy as np
+import pytest
+
+import cggraph_b200 as cg
+from cggraph_b200 import _lib as L
+from cggraph_b200 import policy
+from oracle import mlp_oracle as MO
+
+pytestmark = pytest.mark.gpu
+
+BFS, SSSP = 0, 1
+
+
+def _batch(seed=0, n=300):
+    rng = np.random.default_rng(seed)
+    p = rng.normal(0, 0.15, MO.NPARAMS).astype(np.float32)
+    X = rng.random((n, 24)).astype(np.float32)
+    T = rng.normal(0, 1, (n, 9)).astype(np.float32)
+    M = (rng.random((n, 9)) < 0.4).astype(np.uint8)
+    return p, X, T, M
+
+
+def test_gpu_forward_matches_cpu_oracle():
+    p, X, _, _ = _batch()
+    y_gpu = policy.forward(p, X)
+    y_cpu, _ = MO.forward(p, X)
+    np.testing.assert_allclose(y_gpu, y_cpu, rtol=1e-4, atol=1e-4)
+
+
+def test_gpu_gradient_matches_cpu_oracle():
+    p, X, T, M = _batch(1)
+    l_gpu, g_gpu = policy.loss_grad(p, X, T, M)
+    l_cpu, g_cpu = MO.loss_grad(p, X, T, M)
+    assert abs(l_gpu - l_cpu) <= 1e-4 * abs(l_cpu)
+    scale = np.max(np.abs(g_cpu))
+    assert np.max(np.abs(g_gpu - g_cpu)) <= 1e-4 * scale
+    # and the oracle itself against finite differences on a few entries
+    idx = np.random.default_rng(2).choice(MO.NPARAMS, 20, replace=False)
+    fd = MO.finite_diff(p, X, T, M, idx)
+    assert np.max(np.abs(fd - g_cpu[idx]) / (np.abs(fd) + 1e-6)) < 1e-4
+
+
+def test_gpu_training_fits_a_known_function():
+    rng = np.random.default_rng(3)
+    X = rng.random((2000, 24)).astype(np.float32)
+    T = np.zeros((2000, 9), np.float32)
+    T[:, 0] = X[:, 0] * 2 - X[:, 1]
+    T[:, 1] = np.sin(3 * X[:, 2])
+    M = np.zeros((2000, 9), np.uint8)
+    M[:, :2] = 1
+    p, loss = policy.train(X, T, M, epochs=200, batch=128, lr=3e-3, seed=1)
+    assert loss < 0.01, loss
+    p2, loss2 = policy.train(X, T, M, epochs=200, batch=128, lr=3e-3, seed=1)
+    np.testing.assert_array_equal(p, p2)  # deterministic for a seed
+
+
+def test_collect_samples_and_unchanged_results(oracle):
+    off, dst, w = oracle.rmat_graph(14, 16, seed=9)
+    root = int(np.diff(off.astype(np.int64)).argmax())
+    with cg.Graph.from_csr(off, dst, w) as g:
+        X, T, M = policy.collect(g, BFS, root)
+        assert len(X) >= 3 and np.all(M[:, 0:2] == 1) and np.all(M[:, 2:] == 0)
+        np.testing.assert_array_equal(g.run(BFS, root)[0], oracle.bfs(off, dst, root))
+        X2, T2, M2 = policy.collect(g, SSSP, root)
+        assert len(X2) >= 1 and np.all(M2[:, 2:7] == 1)
+        np.testing.assert_array_equal(g.run(SSSP, root)[0], oracle.sssp(off, dst, w, root))
+        assert np.all(np.isfinite(X)) and np.all(np.isfinite(T))
+
+
+def test_learned_schedule_gives_identical_results(oracle):
+    """Any trained network (here a quick one) changes only timings."""
+    off, dst, w = oracle.rmat_graph(15, 16, seed=4)
+    roots = [int(np.diff(off.astype(np.int64)).argmax()), 3]
+    with cg.Graph.from_csr(off, dst, w) as g:
+        Xs, Ts, Ms = [], [], []
+        for r in roots:
+            for alg in (BFS, SSSP):
+                X, T, M = policy.collect(g, alg, r)
+                Xs.append(X)
+                Ts.append(T)
+                Ms.append(M)
+        p, _ = policy.train(np.concatenate(Xs), np.concatenate(Ts), np.concatenate(Ms), epochs=100)
+        policy.load(p)
+        try:
+            opts = cg.make_options(schedule=L.SCHED_LEARNED)
+            for r in roots + [77]:
+                np.testing.assert_array_equal(g.run(BFS, r, opts)[0], oracle.bfs(off, dst, r))
+                np.testing.assert_array_equal(g.run(SSSP, r, opts)[0], oracle.sssp(off, dst, w, r))
+        finally:
+            policy.load(None)
+    gr_off, gr_dst, gr_w = oracle.grid_graph(40, 60, seed=5)
+    with cg.Graph.from_csr(gr_off, gr_dst, gr_w) as g:
+        policy.load(p)
+        try:
+            opts = cg.make_options(schedule=L.SCHED_LEARNED)
+            np.testing.assert_array_equal(g.run(SSSP, 0, opts)[0], oracle.sssp(gr_off, gr_dst, gr_w, 0))
+        finally:
+            policy.load(None)
+
+
+def test_learned_gain():
+    """The shipped network against the heuristic on held-out graphs (RMAT
+    seed 1, the benchmark's; a 700x700 grid): results identical, time
+    reported; the learned schedule must not lose more than 10 %."""
+    if not policy.load_default():
+        pytest.skip("no trained weights shipped (python -m cggraph_b200.train_policy)")
+    try:
+        res = {}
+        for name, make, alg in (("rmat20", lambda: cg.Graph.rmat(20, 16, seed=1), BFS),
+                                ("rmat20", lambda: cg.Graph.rmat(20, 16, seed=1), SSSP),
+                                ("grid700", lambda: cg.Graph.grid(700, 700, seed=1), SSSP)):
+            with make() as g:
+                t = {}
+                out = {}
+                for sched in (L.SCHED_HEURISTIC, L.SCHED_LEARNED):
+                    o = cg.make_options(schedule=sched)
+                    g.run(alg, 0, o)
+                    best = 1e30
+                    for _ in range(3):
+                        v, ms = g.run(alg, 0, o)
+                        best = min(best, ms)
+                    t[sched], out[sched] = best, v
+                np.testing.assert_array_equal(out[L.SCHED_HEURISTIC], out[L.SCHED_LEARNED])
+                res[(name, alg)] = t[L.SCHED_HEURISTIC] / t[L.SCHED_LEARNED]
+        print("learned / heuristic speed-up:", res)
+        assert all(v > 0.9 for v in res.values()), res
+    finally:
+        policy.load(None)
