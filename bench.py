@@ -52,7 +52,9 @@ def parse_args():
     p.add_argument("--edge-factor", type=int, default=16)
     p.add_argument("--seed", type=int, default=1)
     p.add_argument("--pr-iters", type=int, default=20)
-    p.add_argument("--schedule", choices=["heuristic", "learned"], default="heuristic")
+    p.add_argument("--schedule", choices=["heuristic", "learned"], default="heuristic",
+                   help="schedule of the timed steps (both are compared in 'schedules')")
+    p.add_argument("--no-compare", action="store_true", help="skip the learned-vs-heuristic comparison")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=0, help="0 = same as --steps")
@@ -209,6 +211,10 @@ def bench_cgb200(args, d: Dist):
         if g is not None:
             g.set_stream(stream)
     sched = L.SCHED_LEARNED if args.schedule == "learned" else L.SCHED_HEURISTIC
+    if args.schedule == "learned":
+        from cggraph_b200 import policy
+        if not policy.load_default():
+            raise SystemExit("--schedule learned: no trained policy (python -m cggraph_b200.train_policy)")
     warm_opts = cg.make_options(schedule=sched)
     timed_opts = cg.make_options(schedule=sched, flags=L.FLAG_KERNEL_TIMING)
 
@@ -268,6 +274,13 @@ def bench_cgb200(args, d: Dist):
                               "ms_per_run": per_alg_ms[a] / args.steps} for a in algs}
     full = algs == [BFS, SSSP, CC, PR]
 
+    schedules = None
+    if not args.no_compare and d.world == 1 and (BFS in algs or SSSP in algs):
+        schedules = compare_schedules(args, cg, L, gd, roots[:4], dev)
+        if args.schedule == "learned":
+            from cggraph_b200 import policy
+            policy.load_default()
+
     # end to end through the C ABI with pinned host buffers
     e2e = None
     if not args.no_e2e and full:
@@ -300,6 +313,7 @@ def bench_cgb200(args, d: Dist):
                          % ((4 * (V + 1) + 8 * Ed) / 1e9, (4 * (V + 1) + 4 * Es) / 1e9),
                    "parallelism": f"replicas x{d.world}"},
         "per_algorithm": per_alg,
+        "schedules": schedules,
         "roofline": roof,
         "cpu_baseline": cpu,
         "e2e": e2e,
@@ -307,6 +321,56 @@ def bench_cgb200(args, d: Dist):
         "clocks": clk,
     }
     return result
+
+
+def _best_of(g, alg, root, opts, reps=2):
+    g.run(alg, root, opts, to_host=False)
+    best, st = 1e30, None
+    for _ in range(reps):
+        g.run(alg, root, opts, to_host=False)
+        s = g.stats()
+        if s.ms < best:
+            best, st = s.ms, s
+    return best, st
+
+
+def compare_schedules(args, cg, L, gd, roots, dev):
+    """BFS and SSSP under the heuristic and the learned schedule: on the
+    benchmark graph from its roots, and on the 4800 x 5000 grid (24 M
+    vertices, weights U[1,1000]) from a corner.  Results are bit-identical;
+    only time differs."""
+    from cggraph_b200 import policy
+    if not policy.load_default():
+        return {"note": "no trained policy shipped: learned runs fall back to the heuristic"}
+    out = {}
+    try:
+        cases = [(f"rmat{args.scale}", gd, roots, False)]
+        grid = cg.Graph.grid(4800, 5000, seed=1, device=dev) if args.scale >= 20 else None
+        if grid is not None:
+            cases.append(("grid4800x5000", grid, [0], True))
+        for name, g, rts, own in cases:
+            res = {}
+            for alg, an in ((BFS, "bfs"), (SSSP, "sssp")):
+                t = {}
+                edges = 0
+                for sched, sn in ((L.SCHED_HEURISTIC, "heuristic"), (L.SCHED_LEARNED, "learned")):
+                    tot = 0.0
+                    e = 0
+                    for r in rts:
+                        ms, st = _best_of(g, alg, r, cg.make_options(schedule=sched))
+                        tot += ms
+                        e += st.traversed_edges
+                    t[sn] = tot
+                    edges = e
+                res[an] = {"heuristic_ms": t["heuristic"], "learned_ms": t["learned"],
+                           "heuristic_gteps": edges / t["heuristic"] / 1e6, "learned_gteps": edges / t["learned"] / 1e6,
+                           "learned_speedup": t["heuristic"] / t["learned"]}
+            out[name] = res
+            if own:
+                g.close()
+    finally:
+        policy.load(None)
+    return out
 
 
 def bench_e2e(args, d, cg, gd, gs, roots, off_h, dst_h, w_h, sched):

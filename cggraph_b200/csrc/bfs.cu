@@ -16,6 +16,7 @@
 // The direction switch is Beamer's (alpha = 15, beta = 18) unless the
 // schedule says otherwise.
 #include "engine.cuh"
+#include "persist.cuh"
 #include "policy.cuh"
 #include "push.cuh"
 
@@ -260,12 +261,38 @@ void run_bfs(cgb_graph* g, uint32_t root, const cgb_options& o)
         return in;
     };
 
+    const bool persist_ok = !tracing && o.schedule != CGB_SCHED_FIXED;
     while (nf > 0) {
         CGB_REQUIRE(iters < max_iters, CGB_ETIMEOUT, "BFS iteration budget exhausted");
-        const int out = cur ^ 1;
         // ----- direction decision
         const bool heur = bottom_up ? (awake >= old_awake) || ((double)awake > (double)V / beta)
                                     : (double)scout > (double)edges_to_check / alpha;
+        // small frontiers far from the switch point: run levels on the device
+        if (persist_ok && !heur && nf <= kPersistEnter && maxdeg < kPersistDeg &&
+            (double)scout * alpha * 4.0 <= (double)edges_to_check) {
+            if (timing) ktimer_begin(g, CGB_K_PUSH);
+            const unsigned long long scout_exit = (unsigned long long)((double)edges_to_check / alpha / 4.0);
+            const PersistResult r =
+                bfs_persistent(g, cur, (uint32_t)nf, scout, maxdeg, level, kPersistEnter, scout_exit, kPersistDeg,
+                               (uint32_t)std::min<uint64_t>(max_iters - iters, 1u << 20));
+            if (timing) ktimer_end(g);
+            if (r.levels > 0) {
+                visited_cnt += r.added - nf + r.nf;
+                edges_to_check -= (int64_t)r.scouts;
+                iters += r.levels;
+                level += r.levels;
+                g->stats.pushes_td += r.levels;
+                prev_nf = nf;
+                nf = r.nf;
+                scout = r.scout;
+                maxdeg = r.max_deg;
+                cur = r.cur;
+                bottom_up = false;
+                have_policy_out = false;
+                continue;
+            }
+        }
+        const int out = cur ^ 1;
         bool go_pull;
         if (force_pull) go_pull = true;
         else if (!want_pull) go_pull = false;

@@ -51,6 +51,7 @@ struct cgb_graph {
     uint32_t* dst = nullptr;
     uint32_t* w = nullptr;  // may be null: unit weights
     uint64_t sum_w = 0;     // sum of weights (delta heuristic)
+    uint32_t max_degree = 0;  // longest neighbour list (ensure_frontier)
 
     // in-edge CSC (built on first need; aliases the CSR when symmetric)
     uint32_t* in_off = nullptr;
@@ -94,6 +95,8 @@ struct cgb_graph {
     uint32_t* front_bm = nullptr;
     uint32_t* stamp = nullptr;            // uint32[V]
     uint32_t* sample = nullptr;           // CC sampling buffer
+    uint32_t* aux_bm = nullptr;           // 3 bitmaps: device-resident SSSP near dedup
+    void* persist = nullptr;              // state of the device-resident loops
 
     DevCounters* ctr = nullptr;       // device
     DevCounters* h_ctr = nullptr;     // pinned host mirror

@@ -128,6 +128,15 @@ __global__ void k_narrow(uint32_t n, const uint64_t* __restrict__ a, uint32_t* o
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) o[i] = (uint32_t)a[i];
 }
 
+__global__ void k_max_degree(uint32_t V, const uint32_t* __restrict__ off, uint32_t* out)
+{
+    uint32_t m = 0;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x)
+        m = max(m, off[v + 1] - off[v]);
+    m = warp_max(m);
+    if (lane_id() == 0 && m) atomicMax(out, m);
+}
+
 __global__ void k_sum_u32(uint32_t n, const uint32_t* __restrict__ a, unsigned long long* out)
 {
     unsigned long long s = 0;
@@ -367,12 +376,19 @@ void ensure_frontier(cgb_graph* g)
     g->front_bm = dalloc<uint32_t>(2 * (size_t)g->words());
     g->stamp = dalloc<uint32_t>(V);
     g->sample = dalloc<uint32_t>(1024);
+    g->aux_bm = dalloc<uint32_t>(3 * (size_t)g->words());
+    uint32_t* d = dalloc<uint32_t>(1);
+    CGB_CUDA_TRY(cudaMemsetAsync(d, 0, 4, g->stream));
+    k_max_degree<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, g->off, d);
+    CGB_CUDA_TRY(cudaMemcpyAsync(&g->max_degree, d, 4, cudaMemcpyDeviceToHost, g->stream));
+    CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    dfree(d);
 }
 
-__global__ void k_in_degree(uint32_t E, const uint32_t* __restrict__ dst, uint32_t* indeg)
+__global__ void k_in_degree_from_off(uint32_t V, const uint32_t* __restrict__ in_off, uint32_t* indeg)
 {
-    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x)
-        atomicAdd(indeg + dst[e], 1u);
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x)
+        indeg[v] = in_off[v + 1] - in_off[v];
 }
 
 // Sort key of a vertex for the PageRank layout: its out-degree bucket
@@ -520,8 +536,9 @@ void ensure_pr(cgb_graph* g)
         uint32_t* key2 = dalloc<uint32_t>(V);
         uint32_t* id = dalloc<uint32_t>(V);
         uint32_t* id2 = dalloc<uint32_t>(V);
-        CGB_CUDA_TRY(cudaMemsetAsync(key2, 0, (size_t)V * 4, g->stream));
-        if (E) k_in_degree<<<grid_for(E, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(E, g->dst, key2);
+        // in-degrees from the transpose (shared with bottom-up BFS; no atomics)
+        ensure_csc(g);
+        k_in_degree_from_off<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, g->in_off, key2);
         k_pr_bucket<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, g->off, key2, key, id);
         cub::DoubleBuffer<uint32_t> kb(key, key2), vb(id, id2);
         size_t tb = 0;
@@ -681,7 +698,7 @@ void graph_free(cgb_graph* g)
                     g->pr_chunks, g->pr_chunk_base, g->pr_part, g->pr_slice_ptr, g->pr_slice_len, g->pr_col,
                     g->pr_hub_bm, g->value, g->pr[0], g->pr[1], g->contrib[0],
                     g->contrib[1], g->q[0], g->q[1], g->chunk_q, g->visited, g->front_bm, g->stamp, g->sample,
-                    g->ctr};
+                    g->aux_bm, g->persist, g->ctr};
     for (void* p : ptrs) dfree(p);
     if (g->h_ctr) cudaFreeHost(g->h_ctr);
     for (cudaEvent_t e : g->kev) cudaEventDestroy(e);

@@ -1,0 +1,262 @@
+// Device-resident BFS levels and SSSP near rounds (see persist.cuh).
+#include "persist.cuh"
+
+namespace cgb {
+
+// Shared expansion of one frontier held in qin[0, nf): a warp takes 32
+// frontier vertices; lists of 32 or more edges are walked by the whole warp
+// (ballot election), shorter ones lane by lane.  Visit(valid, e, msg) is
+// warp-collective.
+template <class Visit, class Load>
+__device__ __forceinline__ void expand_small(const uint32_t* __restrict__ qin, uint32_t nf, const Load& load,
+                                             const Visit& visit)
+{
+    const uint32_t lane = lane_id();
+    const uint32_t nwarps = gridDim.x * (kBlock / 32);
+    for (uint32_t base = (blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5)) * 32; base < nf; base += nwarps * 32) {
+        const uint32_t i = base + lane;
+        uint32_t start = 0, deg = 0, msg = 0;
+        if (i < nf) load(qin[i], start, deg, msg);
+        uint32_t wmask;
+        while ((wmask = __ballot_sync(0xffffffffu, deg >= 32)) != 0) {
+            const uint32_t leader = __ffs(wmask) - 1;
+            const uint32_t st = __shfl_sync(0xffffffffu, start, leader);
+            const uint32_t dg = __shfl_sync(0xffffffffu, deg, leader);
+            const uint32_t m = __shfl_sync(0xffffffffu, msg, leader);
+            if (lane == leader) deg = 0;
+            for (uint32_t k = 0; k < dg; k += 32) visit(k + lane < dg, st + k + lane, m);
+        }
+        for (uint32_t j = 0; __any_sync(0xffffffffu, j < deg); j++) visit(j < deg, start + j, msg);
+    }
+}
+
+__device__ __forceinline__ void append(bool pred, uint32_t item, uint32_t* q, uint32_t* ctr, uint32_t cap,
+                                       PersistState* st)
+{
+    const uint32_t want = __ballot_sync(0xffffffffu, pred);
+    if (!want) return;
+    const uint32_t leader = __ffs(want) - 1;
+    uint32_t base = 0;
+    if (lane_id() == leader) base = atomicAdd(ctr, (uint32_t)__popc(want));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (pred) {
+        const uint32_t idx = base + __popc(want & lanemask_lt());
+        if (idx < cap) q[idx] = item;
+        else atomicOr(&st->status, 2u);
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) k_bfs_persistent(const uint32_t* __restrict__ off,
+                                                           const uint32_t* __restrict__ dst, uint32_t* level,
+                                                           uint32_t* visited, uint32_t* q0, uint32_t* q1, uint32_t cap,
+                                                           uint32_t nz, uint32_t start_level, uint32_t cur,
+                                                           uint32_t nf_exit, unsigned long long scout_exit,
+                                                           uint32_t deg_exit, uint32_t max_levels, PersistState* st)
+{
+    uint32_t it = 0;
+    for (; it < max_levels; it++) {
+        const uint32_t s_cur = it % 3, s_next = (it + 1) % 3, s_zero = (it + 2) % 3;
+        const uint32_t nf = *(volatile uint32_t*)&st->qlen[s_cur];
+        const unsigned long long scout = *(volatile unsigned long long*)&st->medges[s_cur];
+        const uint32_t mdeg = *(volatile uint32_t*)&st->max_deg[s_cur];
+        if (nf == 0 || nf > nf_exit || scout > scout_exit || mdeg > deg_exit) break;
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            st->qlen[s_zero] = 0;
+            st->medges[s_zero] = 0;
+            st->max_deg[s_zero] = 0;
+            st->added += nf;
+            st->scouts += scout;
+        }
+        const uint32_t* qin = cur ? q1 : q0;
+        uint32_t* qout = cur ? q0 : q1;
+        const uint32_t next_level = start_level + it + 1;
+        auto load = [&](uint32_t v, uint32_t& s, uint32_t& d, uint32_t& m) {
+            s = off[v];
+            d = off[v + 1] - s;
+            m = 0;
+        };
+        auto visit = [&](bool valid, uint32_t e, uint32_t) {
+            bool win = false;
+            uint32_t d = 0;
+            if (valid) {
+                d = dst[e];
+                const uint32_t bit = 1u << (d & 31u);
+                uint32_t* wp = visited + (d >> 5);
+                if (!(*wp & bit) && !(atomicOr(wp, bit) & bit)) {
+                    win = true;
+                    level[d] = next_level;
+                }
+            }
+            const bool enq = win && d < nz;
+            uint32_t deg = 0;
+            if (enq) deg = off[d + 1] - off[d];
+            append(enq, d, qout, &st->qlen[s_next], cap, st);
+            if (__any_sync(0xffffffffu, enq)) {
+                const unsigned long long sum = warp_sum((unsigned long long)deg);
+                const uint32_t mx = warp_max(deg);
+                if (lane_id() == 0) {
+                    atomicAdd(&st->medges[s_next], sum);
+                    atomicMax(&st->max_deg[s_next], mx);
+                }
+            }
+        };
+        expand_small(qin, nf, load, visit);
+        if (!grid_barrier(st)) break;
+        cur ^= 1;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st->levels = it;
+        st->cur = cur;
+        st->nf = st->qlen[it % 3];
+    }
+}
+
+template <bool kHasW>
+__global__ void __launch_bounds__(kBlock) k_sssp_persistent(const uint32_t* __restrict__ off,
+                                                            const uint32_t* __restrict__ dst,
+                                                            const uint32_t* __restrict__ w, uint32_t* dist,
+                                                            uint32_t* near_bm3, uint32_t words, uint32_t* far_bm,
+                                                            uint32_t* q0, uint32_t* q1, uint32_t cap, uint32_t nz,
+                                                            uint32_t thr, uint32_t cur, uint32_t nf_exit,
+                                                            uint32_t max_rounds, DevCounters* ctr, PersistState* st)
+{
+    uint32_t it = 0;
+    const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x, gthreads = gridDim.x * blockDim.x;
+    for (; it < max_rounds; it++) {
+        const uint32_t s_cur = it % 3, s_next = (it + 1) % 3, s_zero = (it + 2) % 3;
+        const uint32_t nf = *(volatile uint32_t*)&st->qlen[s_cur];
+        if (nf == 0 || nf > nf_exit) break;
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            st->qlen[s_zero] = 0;
+            st->added += nf;
+        }
+        uint32_t* zero_bm = near_bm3 + (size_t)s_zero * words;
+        for (uint32_t i = gtid; i < words; i += gthreads) zero_bm[i] = 0;
+        uint32_t* nbm = near_bm3 + (size_t)s_next * words;
+        const uint32_t* qin = cur ? q1 : q0;
+        uint32_t* qout = cur ? q0 : q1;
+        auto load = [&](uint32_t v, uint32_t& s, uint32_t& d, uint32_t& m) {
+            s = off[v];
+            d = off[v + 1] - s;
+            m = dist[v];
+        };
+        auto visit = [&](bool valid, uint32_t e, uint32_t du) {
+            bool to_near = false, new_far = false;
+            uint32_t d = 0;
+            if (valid && du < kValueMax) {
+                d = dst[e];
+                const uint64_t cand = (uint64_t)du + (kHasW ? (uint64_t)w[e] : 1ull);
+                if (cand < kValueMax) {
+                    const uint32_t nd = (uint32_t)cand;
+                    if (nd < dist[d]) {
+                        const uint32_t old = atomicMin(dist + d, nd);
+                        if (nd < old && d < nz) {
+                            const uint32_t bit = 1u << (d & 31u);
+                            uint32_t* wp = (nd < thr ? nbm : far_bm) + (d >> 5);
+                            const bool fresh = !(*wp & bit) && !(atomicOr(wp, bit) & bit);
+                            to_near = fresh && nd < thr;
+                            new_far = fresh && nd >= thr;
+                        }
+                    }
+                }
+            }
+            append(to_near, d, qout, &st->qlen[s_next], cap, st);
+            const uint32_t nfar = __popc(__ballot_sync(0xffffffffu, new_far));
+            if (nfar && lane_id() == 0) atomicAdd(&ctr->far_len[0], nfar);  // the host loop's far count
+        };
+        expand_small(qin, nf, load, visit);
+        if (!grid_barrier(st)) break;
+        cur ^= 1;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st->levels = it;
+        st->cur = cur;
+        st->nf = st->qlen[it % 3];
+    }
+}
+
+// ----------------------------------------------------------------- host
+static PersistState* persist_state(cgb_graph* g)
+{
+    if (!g->persist) CGB_CUDA_TRY(cudaMalloc(&g->persist, sizeof(PersistState)));
+    return static_cast<PersistState*>(g->persist);
+}
+
+// Host copy of the state after a launch (synchronises the stream).
+static PersistState read_state(cgb_graph* g)
+{
+    PersistState h;
+    CGB_CUDA_TRY(cudaMemcpyAsync(&h, g->persist, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
+    CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    CGB_REQUIRE(!(h.status & 2u), CGB_EOVERFLOW, "device-resident loop: queue overflow");
+    CGB_REQUIRE(!(h.status & 1u), CGB_ETIMEOUT, "device-resident loop: grid barrier gave up");
+    return h;
+}
+
+static void init_state(cgb_graph* g, uint32_t nf, unsigned long long scout, uint32_t max_deg)
+{
+    PersistState h{};
+    h.qlen[0] = nf;
+    h.medges[0] = scout;
+    h.max_deg[0] = max_deg;
+    CGB_CUDA_TRY(cudaMemcpyAsync(g->persist, &h, sizeof(h), cudaMemcpyHostToDevice, g->stream));
+}
+
+PersistResult bfs_persistent(cgb_graph* g, uint32_t cur, uint32_t nf, unsigned long long scout, uint32_t max_deg,
+                             uint32_t level, uint32_t nf_exit, unsigned long long scout_exit, uint32_t deg_exit,
+                             uint32_t max_levels)
+{
+    PersistState* st = persist_state(g);
+    init_state(g, nf, scout, max_deg);
+    static uint32_t grid = 0;
+    if (!grid) grid = cooperative_grid(k_bfs_persistent);
+    uint32_t cap = g->V, nz = g->nz;
+    void* args[] = {&g->off, &g->dst, &g->value, &g->visited, &g->q[0], &g->q[1], &cap, &nz, &level, &cur, &nf_exit,
+                    &scout_exit, &deg_exit, &max_levels, &st};
+    ++g->stats.launches;
+    CGB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_bfs_persistent, grid, kBlock, args, 0, g->stream));
+    const PersistState h = read_state(g);
+    PersistResult r;
+    r.levels = h.levels;
+    r.cur = h.cur;
+    r.nf = h.nf;
+    r.scout = h.medges[h.levels % 3];
+    r.max_deg = h.max_deg[h.levels % 3];
+    r.added = h.added;
+    r.scouts = h.scouts;
+    return r;
+}
+
+PersistResult sssp_persistent(cgb_graph* g, uint32_t cur, uint32_t nf, uint32_t thr, uint32_t* far_bm,
+                              uint32_t nf_exit, uint32_t max_rounds)
+{
+    PersistState* st = persist_state(g);
+    init_state(g, nf, 0, 0);
+    const uint32_t words = g->words();
+    // round 0 appends against near bitmap slot 1; slot 2 is zeroed by round 0
+    CGB_CUDA_TRY(cudaMemsetAsync(g->aux_bm + (size_t)words, 0, (size_t)words * 4, g->stream));
+    uint32_t cap = g->V, nz = g->nz;
+    ++g->stats.launches;
+    if (g->w) {
+        static uint32_t grid = 0;
+        if (!grid) grid = cooperative_grid(k_sssp_persistent<true>);
+        void* args[] = {&g->off, &g->dst, &g->w, &g->value, &g->aux_bm, (void*)&words, &far_bm, &g->q[0], &g->q[1],
+                        &cap, &nz, &thr, &cur, &nf_exit, &max_rounds, &g->ctr, &st};
+        CGB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_sssp_persistent<true>, grid, kBlock, args, 0, g->stream));
+    } else {
+        static uint32_t grid = 0;
+        if (!grid) grid = cooperative_grid(k_sssp_persistent<false>);
+        void* args[] = {&g->off, &g->dst, &g->w, &g->value, &g->aux_bm, (void*)&words, &far_bm, &g->q[0], &g->q[1],
+                        &cap, &nz, &thr, &cur, &nf_exit, &max_rounds, &g->ctr, &st};
+        CGB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_sssp_persistent<false>, grid, kBlock, args, 0, g->stream));
+    }
+    const PersistState h = read_state(g);
+    PersistResult r;
+    r.levels = h.levels;
+    r.cur = h.cur;
+    r.nf = h.nf;
+    r.added = h.added;
+    return r;
+}
+
+}  // namespace cgb

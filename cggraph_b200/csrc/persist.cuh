@@ -1,0 +1,118 @@
+// Device-resident frontier loops for small frontiers (high-diameter graphs).
+//
+// A road-like grid runs thousands of BFS levels / SSSP rounds whose
+// frontiers hold a few thousand vertices; a host-driven loop then pays one
+// launch + one device-to-host read + one synchronisation (tens of
+// microseconds) per level for a few microseconds of work.  These kernels run
+// many levels in one cooperative launch, separated by a grid-wide barrier,
+// and return to the host when the frontier outgrows `nf_exit` (the host
+// loop's binned / bottom-up kernels then take over), when it empties, or
+// after `max_levels`.
+//
+// Counters rotate over three slots: level L appends to slot (L+1)%3, reads
+// its own size from slot L%3, and zeroes slot (L+2)%3, which nobody touches
+// during level L -- so one barrier per level suffices.  The barrier's spin
+// is bounded: on expiry it sets `status` and every CTA leaves the loop.
+#pragma once
+
+#include <algorithm>
+
+#include "engine.cuh"
+
+namespace cgb {
+
+constexpr uint32_t kBarrierSpins = 1u << 22;  // mostly x ~64 ns: gives up after ~0.3 s
+
+// Host-visible state of a device-resident loop.
+struct PersistState {
+    uint32_t qlen[3];          // rotating queue lengths (see file comment)
+    uint32_t bar_count, bar_gen;
+    uint32_t status;           // 1 = a barrier gave up, 2 = queue overflow
+    uint32_t levels;           // levels run by the launch
+    uint32_t cur;              // queue index holding the frontier on exit
+    uint32_t nf;               // frontier size on exit
+    uint32_t max_deg[3];       // rotating: max out-degree of the next frontier
+    unsigned long long medges[3];  // rotating: out-edges of the next frontier
+    unsigned long long added;  // sum of the frontier sizes of the levels run
+    unsigned long long scouts; // sum of their out-edge counts
+};
+
+struct PersistResult {
+    uint32_t levels = 0;       // levels (rounds) run
+    uint32_t cur = 0;          // queue index holding the frontier on exit
+    uint32_t nf = 0;           // frontier size on exit
+    uint32_t max_deg = 0;      // its max out-degree (BFS)
+    unsigned long long scout = 0;   // its out-edges (BFS)
+    unsigned long long added = 0;   // sum of the frontier sizes run
+    unsigned long long scouts = 0;  // sum of their out-edges (BFS)
+};
+
+// Frontiers up to this many vertices, whose lists are all shorter than
+// kPersistDeg, run in the device-resident loops.
+constexpr uint32_t kPersistEnter = 1u << 15;
+constexpr uint32_t kPersistDeg = 2048;
+
+// Runs BFS top-down levels on the device from the frontier q[cur][0, nf)
+// (level `level`, out-edges `scout`, longest list max_deg) until it empties,
+// exceeds nf_exit vertices, scout_exit out-edges or a list of deg_exit
+// edges, or max_levels levels have run.
+PersistResult bfs_persistent(cgb_graph* g, uint32_t cur, uint32_t nf, unsigned long long scout, uint32_t max_deg,
+                             uint32_t level, uint32_t nf_exit, unsigned long long scout_exit, uint32_t deg_exit,
+                             uint32_t max_levels);
+
+// Runs SSSP near rounds at threshold thr on the device from q[cur][0, nf)
+// until the near queue empties, exceeds nf_exit, or max_rounds have run.
+// New far-bitmap entries are added to the counters' far_len[0].  For graphs
+// whose lists are all shorter than kPersistDeg.
+PersistResult sssp_persistent(cgb_graph* g, uint32_t cur, uint32_t nf, uint32_t thr, uint32_t* far_bm,
+                              uint32_t nf_exit, uint32_t max_rounds);
+
+// Grid-wide barrier (every CTA of a cooperative launch must call it).
+// Returns false when the wait gave up (status set by the CTA that gave up).
+__device__ __forceinline__ bool grid_barrier(PersistState* st)
+{
+    __shared__ uint32_t s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile uint32_t* gen = &st->bar_gen;
+        const uint32_t g0 = *gen;
+        __threadfence();
+        const uint32_t arrived = atomicAdd(&st->bar_count, 1u);
+        uint32_t ok = 1;
+        if (arrived == gridDim.x - 1) {
+            st->bar_count = 0;
+            __threadfence();
+            atomicAdd(&st->bar_gen, 1u);
+        } else {
+            uint32_t spins = 0;
+            while (*gen == g0) {
+                if (++spins > kBarrierSpins) {
+                    atomicOr(&st->status, 1u);
+                    ok = 0;
+                    break;
+                }
+                if (spins > 1024) __nanosleep(64);  // spin tight first: levels are short
+            }
+        }
+        __threadfence();
+        s_ok = ok && !(*(volatile uint32_t*)&st->status);
+    }
+    __syncthreads();
+    return s_ok;
+}
+
+// Cooperative grid of `kernel` with kBlock threads: one CTA per SM (enough
+// threads for the frontiers these loops take, and the fewest arrivals per
+// barrier), checked against the occupancy limit.
+template <typename K>
+inline uint32_t cooperative_grid(K kernel)
+{
+    int dev = 0, sms = 0, per_sm = 0;
+    CGB_CUDA_TRY(cudaGetDevice(&dev));
+    CGB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    CGB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBlock, 0));
+    CGB_REQUIRE(per_sm >= 1, CGB_EUNSUPPORTED, "device-resident loop does not fit on an SM");
+    return (uint32_t)sms;
+}
+
+}  // namespace cgb

@@ -233,7 +233,7 @@ int policy_pick_delta(const float* out)
         }
     }
     // keep the heuristic delta unless another choice is clearly cheaper
-    if (best != 2 && out[kOutDelta0 + 2] - bv < kMargin) return -1;
+    if (best != kDeltaUnit && out[kOutDelta0 + kDeltaUnit] - bv < kMargin) return -1;
     return best;
 }
 

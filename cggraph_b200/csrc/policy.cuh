@@ -18,12 +18,10 @@ static_assert(kPolicyParams == kPolicyFeatures * kPolicyHidden + kPolicyHidden +
 
 // Output heads: predicted log-cost of each choice (lower is better).
 constexpr int kOutPush = 0, kOutPull = 1;  // BFS direction of the next level
-constexpr int kOutDelta0 = 2;              // SSSP delta x kDeltaScale[i] for the next bucket
-constexpr int kNumDeltaChoices = 5;
-__host__ __device__ inline float delta_scale(int i)
-{
-    return i == 0 ? 0.25f : i == 1 ? 0.5f : i == 2 ? 1.f : i == 3 ? 2.f : 4.f;
-}
+constexpr int kOutDelta0 = 2;              // SSSP delta x delta_scale(i) for the next bucket
+constexpr int kNumDeltaChoices = 7;        // x {1/4, 1/2, 1, 2, 4, 8, 16}
+constexpr int kDeltaUnit = 2;              // index of x1 (the heuristic delta)
+__host__ __device__ inline float delta_scale(int i) { return 0.25f * (float)(1 << i); }
 
 // Raw quantities at a decision point.  The same function turns them into
 // features on the host (trace logging) and on the device (inference).

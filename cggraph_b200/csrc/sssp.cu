@@ -19,6 +19,7 @@
 // bitmap, cleared before each round, keeps each vertex at most once in a
 // round's queue.
 #include "engine.cuh"
+#include "persist.cuh"
 #include "policy.cuh"
 #include "push.cuh"
 
@@ -174,9 +175,25 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
     uint64_t expanded = 0;
 
     // Near rounds at threshold thr until the near queue is empty.
+    const bool persist_ok = !tracing && o.schedule != CGB_SCHED_FIXED && g->max_degree < kPersistDeg;
     auto near_rounds = [&]() {
         while (nnear > 0) {
             CGB_REQUIRE(iters < max_iters, CGB_ETIMEOUT, "SSSP iteration budget exhausted");
+            if (persist_ok && nnear <= kPersistEnter) {
+                // small near queue: run the rounds on the device
+                if (timing) ktimer_begin(g, CGB_K_PUSH);
+                const PersistResult r =
+                    sssp_persistent(g, cur, (uint32_t)nnear, (uint32_t)std::min<uint64_t>(thr, kValueMax), far_bm,
+                                    kPersistEnter, (uint32_t)std::min<uint64_t>(max_iters - iters, 1u << 20));
+                if (timing) ktimer_end(g);
+                sync_counters(g);
+                iters += r.levels;
+                expanded += r.added;
+                nnear = r.nf;
+                nfar = g->h_ctr->far_len[0];
+                cur = r.cur;
+                if (r.levels > 0) continue;
+            }
             const int out = cur ^ 1;
             CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->qlen[out], 0, sizeof(uint32_t), g->stream));
             CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->chunk_len, 0, sizeof(uint32_t), g->stream));
@@ -269,7 +286,7 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
             const int s_cur = cur;
             float ms[kPolicyOutputs] = {};
             bool have[kPolicyOutputs] = {};
-            int best = 2;
+            int best = kDeltaUnit;
             for (int k = 0; k < kNumDeltaChoices; k++) {
                 const uint32_t dk = std::max<uint32_t>(1u, (uint32_t)(base_delta * delta_scale(k)));
                 CGB_CUDA_TRY(cudaEventRecord(g->ev_iter[0], g->stream));

@@ -5,8 +5,8 @@ The network (24 features -> 64 -> 64 -> 9 log-cost predictions, FP32) lives
 in the engine; this module drives its C entry points (cgb_policy_*):
 
 * ``collect(graph, alg, root)`` -- counterfactual samples of one run: at each
-  BFS level both directions, at each SSSP bucket boundary all five delta
-  multipliers, timed from the same snapshot;
+  BFS level both directions, at each SSSP bucket boundary all seven delta
+  multipliers (x 1/4 .. x 16), timed from the same snapshot;
 * ``train(X, T, M)`` -- masked-MSE training on the GPU by the engine's own
   forward / backward / Adam kernels;
 * ``load(params)`` -- makes a network the policy of CGB_SCHED_LEARNED runs;
@@ -93,6 +93,7 @@ def load_default() -> bool:
 
 def decisions(params, X) -> dict:
     """What the policy would choose for each sample: BFS direction (0 push,
-    1 pull) and SSSP delta index (0..4), before the confidence margin."""
+    1 pull) and SSSP delta index (0..6: x 1/4 .. x 16), before the confidence
+    margin."""
     Y = forward(params, X)
-    return {"direction": np.argmin(Y[:, 0:2], axis=1), "delta": np.argmin(Y[:, 2:7], axis=1)}
+    return {"direction": np.argmin(Y[:, 0:2], axis=1), "delta": np.argmin(Y[:, 2:9], axis=1)}

@@ -6,7 +6,7 @@ Training graphs (seeded, none of them a benchmark input):
   256x256 to 1024x1024 (weights U[1,1000]).
 For each graph and a few seeded roots the engine records counterfactual
 samples (cgb_policy_collect): every BFS level timed in both directions, every
-SSSP bucket timed with delta x {1/4, 1/2, 1, 2, 4}.  The network is trained
+SSSP bucket timed with delta x {1/4, 1/2, 1, 2, 4, 8, 16}.  The network is trained
 on the GPU by the engine's own kernels (cgb_policy_train).
 
   python -m cggraph_b200.train_policy [--quick] [--out PATH] [--epochs N]
@@ -38,7 +38,7 @@ def training_graphs(quick: bool):
         return
     for scale, seed in ((18, 2), (20, 3), (22, 4), (24, 5)):
         yield f"rmat{scale}_s{seed}", (lambda s=scale, d=seed: cg.Graph.rmat(s, 16, seed=d))
-    for n, seed in ((256, 2), (512, 3), (1024, 4)):
+    for n, seed in ((256, 2), (512, 3), (1024, 4), (2048, 6), (4096, 7)):
         yield f"grid{n}_s{seed}", (lambda n=n, d=seed: cg.Graph.grid(n, n, seed=d))
 
 

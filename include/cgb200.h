@@ -214,7 +214,8 @@ cgb_status cgb_bfs_noalloc(const uint32_t* offsets, const uint32_t* dest, uint32
 /* The per-iteration scheduler (CGB_SCHED_LEARNED) is an FP32 MLP
  * CGB_POLICY_FEATURES -> 64 -> 64 -> CGB_POLICY_OUTPUTS whose outputs predict
  * the log-cost of each choice: [0] BFS next level pushed, [1] pulled,
- * [2..6] SSSP next bucket with delta x {1/4, 1/2, 1, 2, 4}; [7..8] unused.
+ * [2..8] SSSP next bucket with delta x {1/4, 1/2, 1, 2, 4, 8, 16} (the cost of
+ * a bucket phase divided by its width).
  * Parameters are CGB_POLICY_PARAMS floats: W1[24][64] b1[64] W2[64][64]
  * b2[64] W3[64][9] b3[9] (row-major, input index first).  The reference has
  * no scheduler; these entry points have no counterpart in it. */
@@ -227,8 +228,9 @@ cgb_status cgb_bfs_noalloc(const uint32_t* offsets, const uint32_t* dest, uint32
 cgb_status cgb_policy_load(const float* params);
 
 /* Per-iteration training samples of one run: at every decision point the
- * engine snapshots its state, runs each choice, times it with CUDA events,
- * restores, and continues with the fastest.  features: max * 24 floats;
+ * engine snapshots its state, runs each choice (BFS: both directions; SSSP:
+ * all seven deltas), times it with CUDA events, restores, and continues with
+ * the fastest.  features: max * 24 floats;
  * targets: max * 9 log-costs; mask: max * 9 (1 where measured).  The run's
  * result equals a plain cgb_run. */
 cgb_status cgb_policy_collect(cgb_graph* g, int algorithm, uint32_t root, const cgb_options* opt, float* features,

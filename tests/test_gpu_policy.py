@@ -67,7 +67,7 @@ def test_collect_samples_and_unchanged_results(oracle):
         assert len(X) >= 3 and np.all(M[:, 0:2] == 1) and np.all(M[:, 2:] == 0)
         np.testing.assert_array_equal(g.run(BFS, root)[0], oracle.bfs(off, dst, root))
         X2, T2, M2 = policy.collect(g, SSSP, root)
-        assert len(X2) >= 1 and np.all(M2[:, 2:7] == 1)
+        assert len(X2) >= 1 and np.all(M2[:, 2:9] == 1)
         np.testing.assert_array_equal(g.run(SSSP, root)[0], oracle.sssp(off, dst, w, root))
         assert np.all(np.isfinite(X)) and np.all(np.isfinite(T))
 
