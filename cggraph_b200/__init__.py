@@ -8,6 +8,7 @@ main_partition, load_binFile, checkBinResult).
 from ._lib import CgbError, LIB_PATH, VALUE_MAX  # noqa: F401
 from .engine import (  # noqa: F401
     Algorithm_type,
+    Batch,
     CSR_Result_type,
     Engine_type,
     Graph,

@@ -31,7 +31,8 @@ EXPORTS = [
     "cgb_graph_result_device", "cgb_graph_result_download", "cgb_run", "cgb_run_batch", "cgb_run_stats_get", "cgb_trace_get",
     "cgb_last_error_string", "cgb_status_string", "cgb_abi_version", "cgb_gen_rmat", "cgb_gen_grid",
     "cgb_graph_download", "cgb_bfs_noalloc", "cgb_policy_load", "cgb_policy_collect", "cgb_policy_train",
-    "cgb_policy_forward", "cgb_policy_loss_grad",
+    "cgb_policy_forward", "cgb_policy_loss_grad", "cgb_batch_create", "cgb_batch_destroy", "cgb_batch_run",
+    "cgb_batch_info", "cgb_batch_stats",
 ]
 POLICY_FEATURES, POLICY_OUTPUTS, POLICY_PARAMS = 24, 9, 6345
 
@@ -134,6 +135,11 @@ def lib() -> ctypes.CDLL:
                                        ctypes.POINTER(ctypes.c_float)]
         L.cgb_policy_forward.argtypes = [_P, _P, u32, _P]
         L.cgb_policy_loss_grad.argtypes = [_P, _P, _P, _P, u32, ctypes.POINTER(ctypes.c_float), _P]
+        L.cgb_batch_create.argtypes = [u32, _P, _P, _P, _P, _P, i, ctypes.POINTER(_P)]
+        L.cgb_batch_destroy.argtypes = [_P]
+        L.cgb_batch_run.argtypes = [_P, i, _P, _P, ctypes.POINTER(ctypes.c_double)]
+        L.cgb_batch_info.argtypes = [_P, _u32p, _u32p, ctypes.POINTER(ctypes.c_int32)]
+        L.cgb_batch_stats.argtypes = [_P, ctypes.POINTER(RunStats)]
         for name in EXPORTS:
             f = getattr(L, name)
             if name not in ("cgb_last_error_string", "cgb_status_string", "cgb_abi_version"):

@@ -261,6 +261,31 @@ cgb_status cgb_run(cgb_graph* g, int algorithm, uint32_t root_or_iters, const cg
     });
 }
 
+// Sum of out-degrees of the reached vertices of n root-major level arrays.
+__global__ void k_batch_reached(uint64_t n, uint32_t V, const uint32_t* __restrict__ val,
+                                const uint32_t* __restrict__ off, DevCounters* ctr)
+{
+    unsigned long long edges = 0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        if (val[i] != kValueMax) {
+            const uint32_t v = (uint32_t)(i % V);
+            edges += off[v + 1] - off[v];
+        }
+    }
+    edges = warp_sum(edges);
+    if (lane_id() == 0 && edges) atomicAdd(&ctr->reached_edges, edges);
+}
+
+static bool is_device_ptr(const void* p)
+{
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
 cgb_status cgb_run_batch(cgb_graph* g, int algorithm, const uint32_t* roots, uint32_t nroots, const cgb_options* opt,
                          uint32_t* out_u32, double* out_ms)
 {
@@ -271,14 +296,69 @@ cgb_status cgb_run_batch(cgb_graph* g, int algorithm, const uint32_t* roots, uin
         const cgb_options o = effective_options(opt);
         std::lock_guard<std::mutex> lock(g->mu);
         CGB_CUDA_TRY(cudaSetDevice(g->device));
-        double total = 0;
-        for (uint32_t i = 0; i < nroots; i++) {
-            run_one(g, algorithm, roots[i], o);
-            total += g->stats.ms;
-            if (out_u32) copy_any(out_u32 + (size_t)i * g->V, g->result, (size_t)g->V * 4, g->stream);
+        const uint64_t V = g->V;
+        if (algorithm == CGB_SSSP || nroots == 1) {
+            double total = 0;
+            uint64_t edges = 0;
+            for (uint32_t i = 0; i < nroots; i++) {
+                run_one(g, algorithm, roots[i], o);
+                total += g->stats.ms;
+                edges += g->stats.traversed_edges;
+                if (out_u32) copy_any(out_u32 + (size_t)i * V, g->result, (size_t)V * 4, g->stream);
+            }
+            CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+            g->stats.ms = total;
+            g->stats.traversed_edges = edges;
+            if (out_ms) *out_ms = total;
+            return;
         }
-        CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
-        if (out_ms) *out_ms = total;
+        // BFS: multi-root passes of up to 64 roots
+        g->stats = cgb_run_stats{};
+        g->flags = o.flags;
+        const bool dev_out = out_u32 && is_device_ptr(out_u32);
+        const uint32_t per = 64;
+        uint32_t* d_roots = nullptr;
+        uint32_t* tmp = nullptr;
+        try {
+            CGB_CUDA_TRY(cudaMalloc((void**)&d_roots, (size_t)per * 4));
+            if (!dev_out) CGB_CUDA_TRY(cudaMalloc((void**)&tmp, (size_t)std::min(per, nroots) * V * 4));
+            double total = 0;
+            uint64_t edges = 0, iters = 0, launches = 0;
+            for (uint32_t s0 = 0; s0 < nroots; s0 += per) {
+                const uint32_t n = std::min(per, nroots - s0);
+                uint32_t* lv = dev_out ? out_u32 + (size_t)s0 * V : tmp;
+                CGB_CUDA_TRY(cudaMemcpyAsync(d_roots, roots + s0, (size_t)n * 4, cudaMemcpyHostToDevice, g->stream));
+                g->stats.launches = 0;
+                CGB_CUDA_TRY(cudaEventRecord(g->ev_start, g->stream));
+                run_msbfs(g, d_roots, n, lv);
+                CGB_CUDA_TRY(cudaEventRecord(g->ev_stop, g->stream));
+                CGB_CUDA_TRY(cudaEventSynchronize(g->ev_stop));
+                float ms = 0.f;
+                CGB_CUDA_TRY(cudaEventElapsedTime(&ms, g->ev_start, g->ev_stop));
+                total += ms;
+                iters += g->stats.iterations;
+                launches += g->stats.launches;
+                CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->reached_edges, 0, 8, g->stream));
+                k_batch_reached<<<kNumSMs * 8, kBlock, 0, g->stream>>>((uint64_t)n * V, (uint32_t)V, lv, g->off, g->ctr);
+                sync_counters(g);
+                edges += g->h_ctr->reached_edges;
+                if (out_u32 && !dev_out)
+                    CGB_CUDA_TRY(cudaMemcpyAsync(out_u32 + (size_t)s0 * V, lv, (size_t)n * V * 4, cudaMemcpyDeviceToHost,
+                                                 g->stream));
+            }
+            CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+            g->stats.ms = total;
+            g->stats.iterations = iters;
+            g->stats.launches = launches;
+            g->stats.traversed_edges = edges;
+            if (out_ms) *out_ms = total;
+        } catch (...) {
+            if (d_roots) cudaFree(d_roots);
+            if (tmp) cudaFree(tmp);
+            throw;
+        }
+        cudaFree(d_roots);
+        if (tmp) cudaFree(tmp);
     });
 }
 

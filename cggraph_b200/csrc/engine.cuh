@@ -39,6 +39,10 @@ struct PolicySamples {
     uint32_t* save_q = nullptr;
 };
 
+namespace cgb {
+struct MsBuffers;
+}
+
 struct cgb_graph {
     int device = 0;
     uint32_t V = 0, E = 0, nz = 0;  // nz = noZeroOutDegreeNum
@@ -97,6 +101,7 @@ struct cgb_graph {
     uint32_t* sample = nullptr;           // CC sampling buffer
     uint32_t* aux_bm = nullptr;           // 3 bitmaps: device-resident SSSP near dedup
     void* persist = nullptr;              // state of the device-resident loops
+    cgb::MsBuffers* ms = nullptr;         // multi-root BFS masks
 
     DevCounters* ctr = nullptr;       // device
     DevCounters* h_ctr = nullptr;     // pinned host mirror
@@ -150,5 +155,7 @@ void run_sssp(cgb_graph* g, uint32_t root, const cgb_options& o);
 void run_cc(cgb_graph* g, const cgb_options& o);
 void run_pr(cgb_graph* g, uint32_t iters, const cgb_options& o);
 void count_reached(cgb_graph* g);  // fills stats.reached / traversed_edges for BFS/SSSP
+void run_msbfs(cgb_graph* g, const uint32_t* d_roots, uint32_t n, uint32_t* level_out);
+void free_msbfs(cgb_graph* g);
 
 }  // namespace cgb

@@ -175,7 +175,155 @@ __global__ void __launch_bounds__(kBlock) k_sssp_persistent(const uint32_t* __re
     }
 }
 
+
+// Whole delta-stepping SSSP on the device (used for graph batches, whose
+// frontiers are small): each round either expands the near queue at the
+// current threshold or, when it is empty and far vertices remain, splits
+// the far bitmap at the next bucket [lo, hi) into a new near queue.  The
+// thresholds, the smallest far distance and the change of the far count
+// rotate over the same three slots as the queue lengths; every CTA keeps
+// the running far count itself by adding the previous round's change, so
+// all CTAs take the same decision each round.
+template <bool kHasW>
+__global__ void __launch_bounds__(kBlock) k_sssp_device(const uint32_t* __restrict__ off,
+                                                        const uint32_t* __restrict__ dst,
+                                                        const uint32_t* __restrict__ w, uint32_t* dist,
+                                                        uint32_t* near_bm3, uint32_t words, uint32_t* far_bm,
+                                                        uint32_t* q0, uint32_t* q1, uint32_t cap, uint32_t nz,
+                                                        uint32_t delta, uint32_t max_rounds, PersistState* st,
+                                                        PersistSssp* sx)
+{
+    uint32_t it = 0, cur = 0, far = 0;
+    const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x, gthreads = gridDim.x * blockDim.x;
+    for (; it < max_rounds; it++) {
+        const uint32_t s_cur = it % 3, s_next = (it + 1) % 3, s_zero = (it + 2) % 3;
+        const uint32_t nf = *(volatile uint32_t*)&st->qlen[s_cur];
+        far += *(volatile uint32_t*)&sx->far_delta[s_cur];
+        const uint64_t thr = *(volatile unsigned long long*)&sx->thr[s_cur];
+        const uint32_t min_far = *(volatile uint32_t*)&sx->min_far[s_cur];
+        if (nf == 0 && far == 0) break;
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            st->qlen[s_zero] = 0;
+            sx->min_far[s_zero] = kValueMax;
+            sx->far_delta[s_zero] = 0;
+            st->added += nf;
+        }
+        uint32_t* zero_bm = near_bm3 + (size_t)s_zero * words;
+        for (uint32_t i = gtid; i < words; i += gthreads) zero_bm[i] = 0;
+        const uint32_t* qin = cur ? q1 : q0;
+        uint32_t* qout = cur ? q0 : q1;
+        if (nf > 0) {
+            // expansion round at threshold thr
+            if (blockIdx.x == 0 && threadIdx.x == 0) sx->thr[s_next] = thr;
+            uint32_t* nbm = near_bm3 + (size_t)s_next * words;
+            const uint32_t t = (uint32_t)(thr < kValueMax ? thr : kValueMax);
+            auto load = [&](uint32_t v, uint32_t& s, uint32_t& d, uint32_t& m) {
+                s = off[v];
+                d = off[v + 1] - s;
+                m = dist[v];
+            };
+            auto visit = [&](bool valid, uint32_t e, uint32_t du) {
+                bool to_near = false, new_far = false;
+                uint32_t d = 0;
+                if (valid && du < kValueMax) {
+                    d = dst[e];
+                    const uint64_t cand = (uint64_t)du + (kHasW ? (uint64_t)w[e] : 1ull);
+                    if (cand < kValueMax) {
+                        const uint32_t nd = (uint32_t)cand;
+                        if (nd < dist[d]) {
+                            const uint32_t old = atomicMin(dist + d, nd);
+                            if (nd < old && d < nz) {
+                                const uint32_t bit = 1u << (d & 31u);
+                                uint32_t* wp = (nd < t ? nbm : far_bm) + (d >> 5);
+                                const bool fresh = !(*wp & bit) && !(atomicOr(wp, bit) & bit);
+                                to_near = fresh && nd < t;
+                                new_far = fresh && nd >= t;
+                            }
+                        }
+                    }
+                }
+                append(to_near, d, qout, &st->qlen[s_next], cap, st);
+                const uint32_t nfar = __popc(__ballot_sync(0xffffffffu, new_far));
+                if (nfar && lane_id() == 0) atomicAdd(&sx->far_delta[s_next], nfar);
+            };
+            expand_small(qin, nf, load, visit);
+        } else {
+            // split round: next bucket [lo, hi); after a split that found
+            // nothing, jump straight to the bucket of the smallest far distance
+            const uint64_t lo = thr;
+            uint64_t hi = thr + delta;
+            if (min_far != kValueMax) {
+                const uint64_t j = ((uint64_t)min_far / delta + 1) * (uint64_t)delta;
+                if (j > hi) hi = j;
+            }
+            if (blockIdx.x == 0 && threadIdx.x == 0) sx->thr[s_next] = hi;
+            const uint32_t lo32 = (uint32_t)(lo < kValueMax ? lo : kValueMax);
+            const uint32_t hi32 = (uint32_t)(hi < kValueMax ? hi : kValueMax);
+            uint32_t mn = kValueMax, cleared = 0;
+            const uint32_t words_round = (words + 31u) & ~31u;
+            for (uint32_t wi = gtid; wi < words_round; wi += gthreads) {
+                uint32_t word = wi < words ? far_bm[wi] : 0u;
+                uint32_t keep = word;
+                while (__any_sync(0xffffffffu, word != 0)) {
+                    bool to_near = false;
+                    uint32_t v = 0;
+                    if (word) {
+                        const uint32_t b = __ffs(word) - 1;
+                        word &= word - 1;
+                        v = wi * 32 + b;
+                        const uint32_t dv = dist[v];
+                        if (dv < hi32) {
+                            keep &= ~(1u << b);
+                            cleared++;
+                            to_near = dv >= lo32;
+                        } else {
+                            mn = min(mn, dv);
+                        }
+                    }
+                    append(to_near, v, qout, &st->qlen[s_next], cap, st);
+                }
+                if (wi < words && keep != far_bm[wi]) far_bm[wi] = keep;
+            }
+            mn = __reduce_min_sync(0xffffffffu, mn);
+            cleared = warp_sum(cleared);
+            if (lane_id() == 0) {
+                if (mn != kValueMax) atomicMin(&sx->min_far[s_next], mn);
+                if (cleared) atomicSub(&sx->far_delta[s_next], cleared);
+            }
+        }
+        if (!grid_barrier(st)) break;
+        cur ^= 1;  // both kinds of round wrote the other queue
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st->levels = it;
+        st->cur = cur;
+        st->nf = st->qlen[it % 3];
+    }
+}
+
 // ----------------------------------------------------------------- host
+void launch_bfs_unbounded(cgb_graph* g, PersistState* st)
+{
+    uint32_t cap = g->V, nz = g->nz, lvl = 0, cur = 0, nf_exit = 0xFFFFFFFFu, deg_exit = 0xFFFFFFFFu;
+    uint32_t max_levels = g->V + 2;
+    unsigned long long scout_exit = ~0ull;
+    void* args[] = {&g->off, &g->dst, &g->value, &g->visited, &g->q[0], &g->q[1], &cap, &nz, &lvl, &cur, &nf_exit,
+                    &scout_exit, &deg_exit, &max_levels, &st};
+    CGB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_bfs_persistent, kNumSMs, kBlock, args, 0, g->stream));
+}
+
+void launch_sssp_device(cgb_graph* g, uint32_t* far_bm, uint32_t delta, PersistState* st, PersistSssp* sx)
+{
+    uint32_t cap = g->V, nz = g->nz, words = g->words(), rounds = 0xFFFFFFF0u;
+    uint32_t* nbm = g->aux_bm;
+    void* args[] = {&g->off, &g->dst, &g->w, &g->value, &nbm, &words, &far_bm, &g->q[0], &g->q[1], &cap, &nz, &delta,
+                    &rounds, &st, &sx};
+    if (g->w)
+        CGB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_sssp_device<true>, kNumSMs, kBlock, args, 0, g->stream));
+    else
+        CGB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_sssp_device<false>, kNumSMs, kBlock, args, 0, g->stream));
+}
+
 static PersistState* persist_state(cgb_graph* g)
 {
     if (!g->persist) CGB_CUDA_TRY(cudaMalloc(&g->persist, sizeof(PersistState)));

@@ -37,6 +37,15 @@ struct PersistState {
     unsigned long long scouts; // sum of their out-edge counts
 };
 
+// Extra state of the whole-device SSSP (k_sssp_device).  Every field
+// rotates over the three slots of the queue lengths, so that what a round
+// reads is never written during that round.
+struct PersistSssp {
+    unsigned long long thr[3];  // threshold of the round
+    uint32_t min_far[3];        // smallest far distance seen by a split
+    uint32_t far_delta[3];      // change of the far-bitmap population made by a round (mod 2^32)
+};
+
 struct PersistResult {
     uint32_t levels = 0;       // levels (rounds) run
     uint32_t cur = 0;          // queue index holding the frontier on exit
@@ -66,6 +75,14 @@ PersistResult bfs_persistent(cgb_graph* g, uint32_t cur, uint32_t nf, unsigned l
 // whose lists are all shorter than kPersistDeg.
 PersistResult sssp_persistent(cgb_graph* g, uint32_t cur, uint32_t nf, uint32_t thr, uint32_t* far_bm,
                               uint32_t nf_exit, uint32_t max_rounds);
+
+// One cooperative launch of k_bfs_persistent with no exit threshold, from
+// the state's qlen[0] roots in q[0] (graph batches).
+void launch_bfs_unbounded(cgb_graph* g, PersistState* st);
+// One cooperative launch of the whole-device SSSP (graph batches).  Expects
+// dist, the far bitmap, slot 1 of the near bitmaps (aux_bm) and `sx` reset,
+// and the roots in q[0] (qlen[0]).
+void launch_sssp_device(cgb_graph* g, uint32_t* far_bm, uint32_t delta, PersistState* st, PersistSssp* sx);
 
 // Grid-wide barrier (every CTA of a cooperative launch must call it).
 // Returns false when the wait gave up (status set by the CTA that gave up).

@@ -129,6 +129,11 @@ def _u32(a):
     return np.ascontiguousarray(a, dtype=np.uint32)
 
 
+def _count(a) -> int:
+    """Element count of a numpy array or a torch tensor."""
+    return int(a.size if isinstance(a, np.ndarray) else a.numel())
+
+
 def make_options(schedule: int = L.SCHED_HEURISTIC, variant: int = L.VAR_AUTO, sssp_delta: int = 0,
                  bfs_alpha: float = 0.0, bfs_beta: float = 0.0, max_iterations: int = 0, flags: int = 0) -> L.Options:
     o = L.Options()
@@ -270,6 +275,81 @@ class Graph:
     def close(self) -> None:
         if self._h is not None and self._h.value:
             check(L.lib().cgb_graph_destroy(self._h))
+        self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many independent graphs solved together (no counterpart in the
+    reference, whose engines take one graph at a time).
+
+    ``Batch(graphs)`` takes a list of ``(offsets, dest, weight)`` CSRs
+    (``weight`` may be None) and concatenates them into one disjoint-union
+    graph in HBM.  ``run(BFS|SSSP, roots)`` traverses every graph from its own
+    root (``roots[i]`` is a local id of graph i) in one cooperative launch,
+    captured into a CUDA graph on first use; ``run(CC)`` labels every graph.
+    Results come back as a list of per-graph arrays in local ids, equal to
+    separate ``Graph.run`` calls.
+    """
+
+    def __init__(self, graphs, device: int = 0):
+        self._h = ctypes.c_void_p()
+        arrs = [(_u32(o), _u32(d), _u32(w)) for o, d, w in graphs]
+        n = len(arrs)
+        if n == 0:
+            raise ValueError("a batch needs at least one graph")
+        self._keep = arrs  # the pointer tables reference these
+        P = ctypes.c_void_p * n
+        offs = P(*[_ptr(o) for o, _, _ in arrs])
+        dsts = P(*[_ptr(d) if _count(d) else None for _, d, _ in arrs])
+        wts = P(*[_ptr(w) if w is not None and _count(w) else None for _, _, w in arrs])
+        self.vertex_counts = np.array([_count(o) - 1 for o, _, _ in arrs], np.uint32)
+        self.edge_counts = np.array([_count(d) for _, d, _ in arrs], np.uint32)
+        any_w = any(w is not None for _, _, w in arrs)
+        check(L.lib().cgb_batch_create(n, offs, dsts, wts if any_w else None, _ptr(self.vertex_counts),
+                                       _ptr(self.edge_counts), device, ctypes.byref(self._h)))
+        self._keep = None
+        self.n = n
+        self.bases = np.concatenate([[0], np.cumsum(self.vertex_counts.astype(np.int64))])
+
+    def run(self, algorithm: int, roots: Optional[Sequence[int]] = None, out=None):
+        """Returns (list of per-graph results, ms); ``out`` may be a host or
+        device buffer of sum(V) uint32 to receive the concatenation instead."""
+        r = None if roots is None else np.ascontiguousarray(roots, dtype=np.uint32)
+        if r is not None and r.size != self.n:
+            raise ValueError("one root per graph")
+        flat = np.empty(int(self.bases[-1]), np.uint32) if out is None else out
+        ms = ctypes.c_double()
+        check(L.lib().cgb_batch_run(self._h, int(algorithm), _ptr(r), _ptr(flat), ctypes.byref(ms)))
+        if out is not None:
+            return out, ms.value
+        return [flat[self.bases[i]:self.bases[i + 1]] for i in range(self.n)], ms.value
+
+    def info(self):
+        """(total vertices, total edges, captured-launch bits: 1 BFS, 2 SSSP)."""
+        v, e, c = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_int32()
+        check(L.lib().cgb_batch_info(self._h, ctypes.byref(v), ctypes.byref(e), ctypes.byref(c)))
+        return v.value, e.value, c.value
+
+    def stats(self) -> L.RunStats:
+        s = L.RunStats()
+        check(L.lib().cgb_batch_stats(self._h, ctypes.byref(s)))
+        return s
+
+    def close(self) -> None:
+        if self._h is not None and self._h.value:
+            check(L.lib().cgb_batch_destroy(self._h))
         self._h = ctypes.c_void_p()
 
     def __enter__(self):

@@ -187,6 +187,31 @@ cgb_status cgb_run_stats_get(const cgb_graph* g, cgb_run_stats* out);
  * receives the number available. */
 cgb_status cgb_trace_get(const cgb_graph* g, cgb_iter_trace* out, uint32_t max_entries, uint32_t* count);
 
+/* ------------------------------------------------------- graph batches */
+
+/* Many independent graphs solved together (no counterpart in the
+ * reference, whose engines take one graph).  The n CSRs (host or device
+ * pointers; weights may be NULL, or an array with NULL entries meaning unit
+ * weights) are concatenated into one disjoint-union graph in HBM; each
+ * graph's invariants are checked as cgb_graph_create checks them. */
+typedef struct cgb_batch cgb_batch;
+cgb_status cgb_batch_create(uint32_t n, const uint32_t* const* offsets, const uint32_t* const* dests,
+                            const uint32_t* const* weights, const uint32_t* vertex_counts,
+                            const uint32_t* edge_counts, int device, cgb_batch** out);
+cgb_status cgb_batch_destroy(cgb_batch* b);
+
+/* BFS or SSSP from roots[i] (a local id of graph i) in every graph at once,
+ * or CC of every graph (roots ignored).  out_u32 receives the concatenated
+ * per-graph results in local ids (sum of V entries), equal to separate
+ * cgb_run calls.  BFS and SSSP run as one cooperative launch, captured into
+ * a CUDA graph on first use and replayed afterwards. */
+cgb_status cgb_batch_run(cgb_batch* b, int algorithm, const uint32_t* roots, uint32_t* out_u32, double* out_ms);
+
+/* Totals of the union, and which runs replay a captured CUDA graph
+ * (bit 0 BFS, bit 1 SSSP). */
+cgb_status cgb_batch_info(const cgb_batch* b, uint32_t* total_vertices, uint32_t* total_edges, int32_t* one_launch);
+cgb_status cgb_batch_stats(const cgb_batch* b, cgb_run_stats* out);
+
 /* --------------------------------------------------- allocation-free BFS */
 
 /* Largest vertex count cgb_bfs_noalloc accepts. */

@@ -146,3 +146,87 @@ def test_batch_equals_single_runs(oracle):
             for i, r in enumerate(roots):
                 exp = oracle.bfs(off, dst, r) if alg == BFS else oracle.sssp(off, dst, w, r)
                 np.testing.assert_array_equal(out[i], exp)
+
+
+def test_multi_root_bfs_passes(oracle):
+    """Bit-packed multi-root BFS: 70 roots (two passes of <= 64), duplicates,
+    a root without out-edges, device-resident output."""
+    import torch
+    off, dst, w = oracle.rmat_graph(14, 16, seed=12)
+    deg = np.diff(off.astype(np.int64))
+    rng = np.random.default_rng(5)
+    roots = [int(x) for x in rng.choice(off.size - 1, 68, replace=False)]
+    roots += [roots[3], int(np.nonzero(deg == 0)[0][0])]
+    with cg.Graph.from_csr(off, dst, w) as g:
+        out, ms = g.run_batch(BFS, roots)
+        assert ms > 0
+        for i, r in enumerate(roots):
+            np.testing.assert_array_equal(out[i], oracle.bfs(off, dst, r), err_msg=f"root {i}")
+        d_out = torch.empty((len(roots), off.size - 1), dtype=torch.int32, device="cuda")
+        g.run_batch(BFS, roots, out=d_out)
+        np.testing.assert_array_equal(d_out.cpu().numpy().view(np.uint32), out)
+        assert g.stats().traversed_edges == sum(int(deg[out[i] != 999999999].sum()) for i in range(len(roots)))
+
+
+def _batch_graphs(oracle):
+    """Uneven graphs: RMAT of scales 8-12 (directed and symmetric), grids,
+    a graph without edges, one with a single vertex."""
+    gs = []
+    for i, scale in enumerate((8, 9, 10, 11, 12, 10, 9)):
+        gs.append(oracle.rmat_graph(scale, 8 + 2 * i, seed=40 + i, symmetrise=bool(i % 2)))
+    gs.append(oracle.grid_graph(17, 23, seed=3))
+    gs.append(oracle.grid_graph(1, 40, seed=4))
+    gs.append((np.zeros(6, np.uint32), np.zeros(0, np.uint32), np.zeros(0, np.uint32)))
+    gs.append((np.zeros(2, np.uint32), np.zeros(0, np.uint32), np.zeros(0, np.uint32)))
+    return gs
+
+
+def test_graph_batch_matches_oracle(oracle):
+    gs = _batch_graphs(oracle)
+    rng = np.random.default_rng(8)
+    with cg.Batch(gs) as b:
+        V, E, _ = b.info()
+        assert V == sum(o.size - 1 for o, _, _ in gs) and E == sum(d.size for _, d, _ in gs)
+        for trial in range(3):
+            roots = [int(rng.integers(0, o.size - 1)) for o, _, _ in gs]
+            outs, ms = b.run(BFS, roots)
+            assert ms > 0
+            for i, (o, d, w) in enumerate(gs):
+                np.testing.assert_array_equal(outs[i], oracle.bfs(o, d, roots[i]), err_msg=f"BFS graph {i}")
+            outs, _ = b.run(SSSP, roots)
+            for i, (o, d, w) in enumerate(gs):
+                np.testing.assert_array_equal(outs[i], oracle.sssp(o, d, w, roots[i]), err_msg=f"SSSP graph {i}")
+        assert b.info()[2] in (0, 1, 2, 3)
+        outs, _ = b.run(CC)
+        for i, (o, d, w) in enumerate(gs):
+            np.testing.assert_array_equal(outs[i], oracle.cc(o, d), err_msg=f"CC graph {i}")
+        st = b.stats()
+        assert st.traversed_edges == E
+
+
+def test_graph_batch_symmetric_cc_and_device_out(oracle):
+    """All-symmetric batch takes the Afforest CC path; results land in a
+    device buffer."""
+    import torch
+    gs = [oracle.rmat_graph(s, 8, seed=60 + s, symmetrise=True) for s in (9, 10, 11, 12)]
+    gs.append(oracle.grid_graph(30, 31, seed=1))
+    with cg.Batch(gs) as b:
+        V = b.info()[0]
+        d_out = torch.empty(V, dtype=torch.int32, device="cuda")
+        b.run(CC, out=d_out)
+        flat = d_out.cpu().numpy().view(np.uint32)
+        assert b.stats().cc_path == 0
+        for i, (o, d, w) in enumerate(gs):
+            np.testing.assert_array_equal(flat[b.bases[i]:b.bases[i + 1]], oracle.cc(o, d))
+
+
+def test_graph_batch_rejects_bad_graph():
+    ok = (np.array([0, 1, 2], np.uint32), np.array([1, 0], np.uint32), None)
+    bad_dest = (np.array([0, 1, 2], np.uint32), np.array([1, 2], np.uint32), None)
+    bad_off = (np.array([0, 2, 1], np.uint32), np.array([1, 0], np.uint32), None)
+    for bad in (bad_dest, bad_off):
+        with pytest.raises(cg.CgbError):
+            cg.Batch([ok, bad])
+    with cg.Batch([ok, ok]) as b:
+        with pytest.raises(cg.CgbError):
+            b.run(BFS, [0, 2])
