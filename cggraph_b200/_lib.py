@@ -21,7 +21,7 @@ STATUS_NAMES = ["CGB_OK", "CGB_EINVAL", "CGB_EFORMAT", "CGB_EIO", "CGB_ENOMEM", 
 # cgb_schedule / cgb_variant / flags / kernel classes
 SCHED_HEURISTIC, SCHED_LEARNED, SCHED_FIXED = 0, 1, 2
 VAR_AUTO, VAR_TWC, VAR_PULL, VAR_PUSH = 0, 1, 2, 3
-FLAG_KERNEL_TIMING, FLAG_TRACE = 0x1, 0x2
+FLAG_KERNEL_TIMING, FLAG_TRACE, FLAG_BATCH_SEQUENTIAL = 0x1, 0x2, 0x4
 K_PUSH, K_PULL, K_PR, K_HOOK, K_COMPRESS, K_FRONTIER, K_INIT, K_OTHER = range(8)
 KERNEL_CLASS_NAMES = ["push", "pull", "pagerank", "hook", "compress", "frontier", "init", "other"]
 

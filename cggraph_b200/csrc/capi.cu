@@ -297,22 +297,24 @@ cgb_status cgb_run_batch(cgb_graph* g, int algorithm, const uint32_t* roots, uin
         std::lock_guard<std::mutex> lock(g->mu);
         CGB_CUDA_TRY(cudaSetDevice(g->device));
         const uint64_t V = g->V;
-        if (algorithm == CGB_SSSP || nroots == 1) {
+        if ((o.flags & CGB_FLAG_BATCH_SEQUENTIAL) || nroots == 1) {
             double total = 0;
-            uint64_t edges = 0;
+            uint64_t edges = 0, launches = 0;
             for (uint32_t i = 0; i < nroots; i++) {
                 run_one(g, algorithm, roots[i], o);
                 total += g->stats.ms;
                 edges += g->stats.traversed_edges;
+                launches += g->stats.launches;
                 if (out_u32) copy_any(out_u32 + (size_t)i * V, g->result, (size_t)V * 4, g->stream);
             }
             CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
             g->stats.ms = total;
             g->stats.traversed_edges = edges;
+            g->stats.launches = launches;
             if (out_ms) *out_ms = total;
             return;
         }
-        // BFS: multi-root passes of up to 64 roots
+        // multi-root passes of up to 64 roots
         g->stats = cgb_run_stats{};
         g->flags = o.flags;
         const bool dev_out = out_u32 && is_device_ptr(out_u32);
@@ -330,7 +332,8 @@ cgb_status cgb_run_batch(cgb_graph* g, int algorithm, const uint32_t* roots, uin
                 CGB_CUDA_TRY(cudaMemcpyAsync(d_roots, roots + s0, (size_t)n * 4, cudaMemcpyHostToDevice, g->stream));
                 g->stats.launches = 0;
                 CGB_CUDA_TRY(cudaEventRecord(g->ev_start, g->stream));
-                run_msbfs(g, d_roots, n, lv);
+                if (algorithm == CGB_BFS) run_msbfs(g, d_roots, n, lv);
+                else run_mssp(g, d_roots, n, lv, o.sssp_delta ? o.sssp_delta : mssp_default_delta(g));
                 CGB_CUDA_TRY(cudaEventRecord(g->ev_stop, g->stream));
                 CGB_CUDA_TRY(cudaEventSynchronize(g->ev_stop));
                 float ms = 0.f;
@@ -351,6 +354,7 @@ cgb_status cgb_run_batch(cgb_graph* g, int algorithm, const uint32_t* roots, uin
             g->stats.iterations = iters;
             g->stats.launches = launches;
             g->stats.traversed_edges = edges;
+            g->stats.alg_bytes = (algorithm == CGB_BFS ? 8 : (g->w ? 12 : 8)) * edges + 12ull * V * nroots;
             if (out_ms) *out_ms = total;
         } catch (...) {
             if (d_roots) cudaFree(d_roots);

@@ -41,6 +41,7 @@ struct PolicySamples {
 
 namespace cgb {
 struct MsBuffers;
+struct MsspBuffers;
 }
 
 struct cgb_graph {
@@ -102,6 +103,7 @@ struct cgb_graph {
     uint32_t* aux_bm = nullptr;           // 3 bitmaps: device-resident SSSP near dedup
     void* persist = nullptr;              // state of the device-resident loops
     cgb::MsBuffers* ms = nullptr;         // multi-root BFS masks
+    cgb::MsspBuffers* mssp = nullptr;     // multi-root SSSP distances and masks
 
     DevCounters* ctr = nullptr;       // device
     DevCounters* h_ctr = nullptr;     // pinned host mirror
@@ -157,5 +159,10 @@ void run_pr(cgb_graph* g, uint32_t iters, const cgb_options& o);
 void count_reached(cgb_graph* g);  // fills stats.reached / traversed_edges for BFS/SSSP
 void run_msbfs(cgb_graph* g, const uint32_t* d_roots, uint32_t n, uint32_t* level_out);
 void free_msbfs(cgb_graph* g);
+// Multi-root SSSP of n <= 64 roots (device array); out (device) receives
+// n * V distances, root-major.
+void run_mssp(cgb_graph* g, const uint32_t* d_roots, uint32_t n, uint32_t* out, uint32_t delta);
+void free_mssp(cgb_graph* g);
+uint32_t mssp_default_delta(cgb_graph* g);
 
 }  // namespace cgb

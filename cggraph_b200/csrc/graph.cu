@@ -695,6 +695,7 @@ void graph_free(cgb_graph* g)
         dfree(g->in_src);
     }
     free_msbfs(g);
+    free_mssp(g);
     void* ptrs[] = {g->off, g->dst, g->w, g->pr_huge_rows, g->pr_rank, g->pr_off, g->pr_src, g->pr_outdeg,
                     g->pr_chunks, g->pr_chunk_base, g->pr_part, g->pr_slice_ptr, g->pr_slice_len, g->pr_col,
                     g->pr_hub_bm, g->value, g->pr[0], g->pr[1], g->contrib[0],

@@ -1,0 +1,412 @@
+// Multi-root SSSP: up to 64 roots per pass, one distance per (vertex, root)
+// and bit-packed per-vertex root masks.
+//
+// Layout: dist[v * 64 + k] (vertex-major), so the 64 distances of a vertex
+// are one 256-byte run; a warp relaxes an edge (v, u) for every root at once,
+// lane k handling roots k and k + 32, with two coalesced 128-byte loads of
+// dist[u][*].  Per vertex two 64-bit masks record which roots still need
+// work: pend (improved below the current threshold: expand next round) and
+// farm (improved at or above it: kept for a later bucket).
+//
+// Delta-stepping with one threshold shared by all roots: rounds expand the
+// near work (pend) until none is left, then a split moves the far pairs of
+// the next bucket [lo, hi) into pend (jumping to the bucket of the smallest
+// far distance when a bucket is empty).  The relaxation is label-correcting
+// (atomicMin; a pair is re-expanded whenever it improves), so the result is
+// the exact shortest-path distance of every pair whatever the order -- equal
+// to n separate cgb_run(CGB_SSSP) results.
+//
+// Work of a round: the queue of vertices with pend != 0 is cut into
+// descriptors of at most kMsEdges edges (hub lists are spread over many
+// warps); a warp takes one descriptor, reads its 32 next edges' targets and
+// weights coalesced, and walks them with shuffles.
+#include "engine.cuh"
+
+namespace cgb {
+
+constexpr uint32_t kMsRoots = 64;   // distance slots per vertex
+constexpr uint32_t kMsEdges = 256;  // edges per work descriptor
+
+struct MsspCounters {
+    uint32_t nq_out;       // entries of the near queue being built
+    uint32_t nfar_live;    // entries of the live far list (expansion rounds append)
+    uint32_t nfar_next;    // entries kept by a split in the other far list
+    uint32_t ndesc;        // descriptors of the round
+    uint32_t min_far;      // smallest far distance >= hi seen by a split
+    uint32_t overflow;
+    unsigned long long relax;  // successful relaxations
+};
+
+struct MsspBuffers {
+    uint32_t* dist = nullptr;               // V * 64
+    unsigned long long* pend = nullptr;     // V
+    unsigned long long* farm = nullptr;     // V
+    unsigned long long* maskq = nullptr;    // V: pend of each queue entry, taken by the descriptor pass
+    uint32_t* far_list[2] = {nullptr, nullptr};  // V each
+    uint4* desc = nullptr;                  // {v, edge begin, edge end, queue index}
+    uint64_t desc_cap = 0;
+    MsspCounters* c = nullptr;
+    MsspCounters* h = nullptr;              // pinned host copy
+};
+
+__global__ void k_mssp_init(uint32_t V, uint4* dist4, unsigned long long* pend, unsigned long long* farm)
+{
+    const uint64_t n4 = (uint64_t)V * (kMsRoots / 4);
+    const uint4 mx = make_uint4(kValueMax, kValueMax, kValueMax, kValueMax);
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += (uint64_t)gridDim.x * blockDim.x)
+        dist4[i] = mx;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+        pend[v] = 0;
+        farm[v] = 0;
+    }
+}
+
+// Roots at distance 0 and queued once each (one thread).
+__global__ void k_mssp_roots(const uint32_t* roots, uint32_t n, uint32_t* dist, unsigned long long* pend, uint32_t* q,
+                             MsspCounters* c)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    uint32_t len = 0;
+    for (uint32_t k = 0; k < n; k++) {
+        const uint32_t r = roots[k];
+        dist[(size_t)r * kMsRoots + k] = 0;
+        if (pend[r] == 0) q[len++] = r;
+        pend[r] |= 1ull << k;
+    }
+    c->nq_out = len;
+}
+
+// Takes (and clears) the pend mask of every queued vertex and cuts its list
+// into descriptors of at most kMsEdges edges.
+__global__ void __launch_bounds__(kBlock) k_mssp_desc(const uint32_t* __restrict__ q, uint32_t nq,
+                                                      const uint32_t* __restrict__ off, unsigned long long* pend,
+                                                      unsigned long long* maskq, uint4* desc, uint64_t cap,
+                                                      MsspCounters* c)
+{
+    const uint32_t n_round = (nq + 31u) & ~31u;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_round; i += gridDim.x * blockDim.x) {
+        uint32_t v = 0, s = 0, d = 0, nd = 0;
+        if (i < nq) {
+            v = q[i];
+            maskq[i] = pend[v];
+            pend[v] = 0;
+            s = off[v];
+            d = off[v + 1] - s;
+            nd = (d + kMsEdges - 1) / kMsEdges;
+        }
+        // warp-inclusive scan of the descriptor counts, one atomic per warp
+        uint32_t incl = nd;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane_id() >= (uint32_t)o) incl += t;
+        }
+        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+        uint32_t base = 0;
+        if (lane_id() == 31 && total) base = atomicAdd(&c->ndesc, total);
+        base = __shfl_sync(0xffffffffu, base, 31);
+        const uint64_t pos = (uint64_t)base + incl - nd;
+        for (uint32_t j = 0; j < nd; j++) {
+            if (pos + j < cap) {
+                const uint32_t eb = s + j * kMsEdges;
+                desc[pos + j] = make_uint4(v, eb, min(eb + kMsEdges, s + d), i);
+            } else {
+                atomicOr(&c->overflow, 1u);
+            }
+        }
+    }
+}
+
+// One near round: relaxes every descriptor's edges for the roots of its
+// vertex's mask.  Pairs improved below thr go to pend (their vertex queued
+// on the 0 -> non-zero transition), the others to farm (vertex listed in
+// the far list on the same transition).
+template <bool kHasW>
+__global__ void __launch_bounds__(kBlock) k_mssp_expand(const uint4* __restrict__ desc, const MsspCounters* cc,
+                                                        const unsigned long long* __restrict__ maskq,
+                                                        const uint32_t* __restrict__ dst,
+                                                        const uint32_t* __restrict__ w, uint32_t* dist,
+                                                        unsigned long long* pend, unsigned long long* farm,
+                                                        uint32_t* qout, uint32_t* far_out, uint32_t cap, uint32_t thr,
+                                                        MsspCounters* c)
+{
+    const uint32_t ndesc = min((uint64_t)cc->ndesc, (uint64_t)0xFFFFFFFFu);
+    const uint32_t lane = lane_id();
+    const uint32_t warps = gridDim.x * (kBlock / 32);
+    unsigned long long relax = 0;
+    for (uint32_t j = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5); j < ndesc; j += warps) {
+        const uint4 d = desc[j];
+        const unsigned long long m = maskq[d.w];
+        const bool a0 = (m >> lane) & 1ull, a1 = (m >> (lane + 32)) & 1ull;
+        const uint32_t* dv_row = dist + (size_t)d.x * kMsRoots;
+        const uint32_t dv0 = a0 ? dv_row[lane] : kValueMax;
+        const uint32_t dv1 = a1 ? dv_row[lane + 32] : kValueMax;
+        const bool s0 = dv0 < kValueMax, s1 = dv1 < kValueMax;
+        for (uint32_t e0 = d.y; e0 < d.z; e0 += 32) {
+            const uint32_t cnt = min(32u, d.z - e0);
+            uint32_t my_u = 0, my_w = 1;
+            if (lane < cnt) {
+                my_u = dst[e0 + lane];
+                if (kHasW) my_w = w[e0 + lane];
+            }
+            // lane t collects the root masks improved through edge t, then
+            // every lane publishes its own edge's masks (32 atomics at once)
+            unsigned long long my_nb = 0, my_fb = 0;
+            for (uint32_t t0 = 0; t0 < cnt; t0 += 4) {
+                uint32_t u[4], wt[4], x0[4], x1[4];
+#pragma unroll
+                for (int i = 0; i < 4; i++) {  // loads first: four targets in flight
+                    const uint32_t t = min(t0 + i, cnt - 1);
+                    u[i] = __shfl_sync(0xffffffffu, my_u, t);
+                    wt[i] = __shfl_sync(0xffffffffu, my_w, t);
+                    const uint32_t* du = dist + (size_t)u[i] * kMsRoots;
+                    x0[i] = s0 ? du[lane] : 0u;
+                    x1[i] = s1 ? du[lane + 32] : 0u;
+                }
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    const uint32_t t = t0 + i;
+                    if (t >= cnt) break;  // warp-uniform
+                    uint32_t* du = dist + (size_t)u[i] * kMsRoots;
+                    bool n0 = false, n1 = false, f0 = false, f1 = false;
+                    const uint64_t c0 = (uint64_t)dv0 + wt[i], c1 = (uint64_t)dv1 + wt[i];
+                    if (s0 && c0 < kValueMax && (uint32_t)c0 < x0[i]) {
+                        const uint32_t old = atomicMin(du + lane, (uint32_t)c0);
+                        if ((uint32_t)c0 < old) {
+                            relax++;
+                            n0 = (uint32_t)c0 < thr;
+                            f0 = !n0;
+                        }
+                    }
+                    if (s1 && c1 < kValueMax && (uint32_t)c1 < x1[i]) {
+                        const uint32_t old = atomicMin(du + lane + 32, (uint32_t)c1);
+                        if ((uint32_t)c1 < old) {
+                            relax++;
+                            n1 = (uint32_t)c1 < thr;
+                            f1 = !n1;
+                        }
+                    }
+                    const unsigned long long nb = (unsigned long long)__ballot_sync(0xffffffffu, n0) |
+                                                  ((unsigned long long)__ballot_sync(0xffffffffu, n1) << 32);
+                    const unsigned long long fb = (unsigned long long)__ballot_sync(0xffffffffu, f0) |
+                                                  ((unsigned long long)__ballot_sync(0xffffffffu, f1) << 32);
+                    if (lane == t) {
+                        my_nb = nb;
+                        my_fb = fb;
+                    }
+                }
+            }
+            const bool qn = my_nb && atomicOr(pend + my_u, my_nb) == 0ull;
+            const bool qf = my_fb && atomicOr(farm + my_u, my_fb) == 0ull;
+            warp_append(qn, my_u, qout, &c->nq_out, cap, &c->overflow);
+            warp_append(qf, my_u, far_out, &c->nfar_live, cap, &c->overflow);
+        }
+    }
+    relax = warp_sum(relax);
+    if (lane == 0 && relax) atomicAdd(&c->relax, relax);
+}
+
+// Split: for every vertex of the far list, its far pairs with lo <= dist <
+// hi go to pend (vertex queued), those below lo were expanded already and
+// are dropped, the rest stay far (vertex kept in the other far list) and
+// their smallest distance is reported.
+__global__ void __launch_bounds__(kBlock) k_mssp_split(const uint32_t* __restrict__ far_in, uint32_t nfar,
+                                                       const uint32_t* __restrict__ dist, unsigned long long* pend,
+                                                       unsigned long long* farm, uint32_t* q, uint32_t* far_out,
+                                                       uint32_t cap, uint32_t lo, uint32_t hi, MsspCounters* c)
+{
+    const uint32_t lane = lane_id();
+    const uint32_t warps = gridDim.x * (kBlock / 32);
+    uint32_t mn = kValueMax;
+    for (uint32_t i = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5); i < nfar; i += warps) {
+        const uint32_t v = far_in[i];
+        const unsigned long long m = farm[v];
+        const bool a0 = (m >> lane) & 1ull, a1 = (m >> (lane + 32)) & 1ull;
+        const uint32_t* row = dist + (size_t)v * kMsRoots;
+        const uint32_t d0 = a0 ? row[lane] : kValueMax, d1 = a1 ? row[lane + 32] : kValueMax;
+        const bool mv0 = a0 && d0 < hi, mv1 = a1 && d1 < hi;
+        const bool nr0 = mv0 && d0 >= lo, nr1 = mv1 && d1 >= lo;
+        if (a0 && !mv0) mn = min(mn, d0);
+        if (a1 && !mv1) mn = min(mn, d1);
+        const unsigned long long moved = (unsigned long long)__ballot_sync(0xffffffffu, mv0) |
+                                         ((unsigned long long)__ballot_sync(0xffffffffu, mv1) << 32);
+        const unsigned long long nearb = (unsigned long long)__ballot_sync(0xffffffffu, nr0) |
+                                         ((unsigned long long)__ballot_sync(0xffffffffu, nr1) << 32);
+        const unsigned long long keep = m & ~moved;
+        if (lane == 0) {
+            if (moved) farm[v] = keep;
+            if (nearb) pend[v] = nearb;  // no expansion runs during a split: v is this warp's alone
+        }
+        if (lane == 0) {
+            if (nearb) {
+                const uint32_t p = atomicAdd(&c->nq_out, 1u);
+                if (p < cap) q[p] = v;
+                else atomicOr(&c->overflow, 1u);
+            }
+            if (keep) {
+                const uint32_t p = atomicAdd(&c->nfar_next, 1u);
+                if (p < cap) far_out[p] = v;
+                else atomicOr(&c->overflow, 1u);
+            }
+        }
+    }
+    mn = __reduce_min_sync(0xffffffffu, mn);
+    if (lane == 0 && mn != kValueMax) atomicMin(&c->min_far, mn);
+}
+
+// dist (vertex-major, 64 slots) -> out[k * V + v] for k < n, through a
+// 32-vertex x 64-root shared tile.
+__global__ void __launch_bounds__(kBlock) k_mssp_out(const uint32_t* __restrict__ dist, uint32_t V, uint32_t n,
+                                                     uint32_t* out)
+{
+    __shared__ uint32_t tile[32][kMsRoots + 1];
+    const uint32_t tiles = (V + 31) / 32;
+    for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+        const uint32_t v0 = t * 32;
+        for (uint32_t i = threadIdx.x; i < 32 * kMsRoots; i += blockDim.x) {
+            const uint32_t r = i / kMsRoots, k = i % kMsRoots;
+            if (v0 + r < V) tile[r][k] = dist[(size_t)(v0 + r) * kMsRoots + k];
+        }
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < 32 * n; i += blockDim.x) {
+            const uint32_t k = i / 32, r = i % 32;
+            if (v0 + r < V) out[(size_t)k * V + v0 + r] = tile[r][k];
+        }
+        __syncthreads();
+    }
+}
+
+static void mssp_alloc(cgb_graph* g)
+{
+    if (g->mssp) return;
+    const uint32_t V = g->V;
+    auto* b = new MsspBuffers();
+    try {
+        CGB_CUDA_TRY(cudaMalloc((void**)&b->dist, (size_t)V * kMsRoots * 4));
+        CGB_CUDA_TRY(cudaMalloc((void**)&b->pend, (size_t)V * 8));
+        CGB_CUDA_TRY(cudaMalloc((void**)&b->farm, (size_t)V * 8));
+        CGB_CUDA_TRY(cudaMalloc((void**)&b->maskq, (size_t)V * 8));
+        CGB_CUDA_TRY(cudaMalloc((void**)&b->far_list[0], (size_t)V * 4));
+        CGB_CUDA_TRY(cudaMalloc((void**)&b->far_list[1], (size_t)V * 4));
+        b->desc_cap = (uint64_t)V + (uint64_t)g->E / kMsEdges + 1;
+        CGB_CUDA_TRY(cudaMalloc((void**)&b->desc, b->desc_cap * sizeof(uint4)));
+        CGB_CUDA_TRY(cudaMalloc((void**)&b->c, sizeof(MsspCounters)));
+        CGB_CUDA_TRY(cudaMallocHost((void**)&b->h, sizeof(MsspCounters)));
+    } catch (...) {
+        g->mssp = b;
+        free_mssp(g);
+        throw;
+    }
+    g->mssp = b;
+}
+
+void free_mssp(cgb_graph* g)
+{
+    MsspBuffers* b = g->mssp;
+    if (!b) return;
+    cudaFree(b->dist);
+    cudaFree(b->pend);
+    cudaFree(b->farm);
+    cudaFree(b->maskq);
+    cudaFree(b->far_list[0]);
+    cudaFree(b->far_list[1]);
+    cudaFree(b->desc);
+    cudaFree(b->c);
+    if (b->h) cudaFreeHost(b->h);
+    delete b;
+    g->mssp = nullptr;
+}
+
+static MsspCounters mssp_sync(cgb_graph* g)
+{
+    MsspBuffers& b = *g->mssp;
+    CGB_CUDA_TRY(cudaMemcpyAsync(b.h, b.c, sizeof(MsspCounters), cudaMemcpyDeviceToHost, g->stream));
+    CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    CGB_REQUIRE(!b.h->overflow, CGB_EOVERFLOW, "multi-root SSSP queue overflow");
+    return *b.h;
+}
+
+__global__ void k_mssp_set(uint32_t* a, uint32_t value) { *a = value; }
+
+uint32_t mssp_default_delta(cgb_graph* g)
+{
+    if (g->w && g->sum_w == 0) compute_weight_sum(g);
+    // a round serves up to 64 roots: wider buckets than one root's (on
+    // RMAT-22/24 rounds stop shrinking beyond about 8x)
+    const uint64_t d = 8ull * sssp_default_delta(g);
+    return (uint32_t)std::min<uint64_t>(d, 100000000ull);
+}
+
+void run_mssp(cgb_graph* g, const uint32_t* d_roots, uint32_t n, uint32_t* out, uint32_t delta)
+{
+    CGB_REQUIRE(n >= 1 && n <= kMsRoots, CGB_EINVAL, "multi-root SSSP takes 1..64 roots per pass");
+    ensure_frontier(g);
+    mssp_alloc(g);
+    MsspBuffers& b = *g->mssp;
+    const uint32_t V = g->V;
+    if (delta == 0) delta = 1;
+    CGB_CUDA_TRY(cudaMemsetAsync(b.c, 0, sizeof(MsspCounters), g->stream));
+    ++g->stats.launches;
+    k_mssp_init<<<kNumSMs * 8, kBlock, 0, g->stream>>>(V, reinterpret_cast<uint4*>(b.dist), b.pend, b.farm);
+    ++g->stats.launches;
+    k_mssp_roots<<<1, 1, 0, g->stream>>>(d_roots, n, b.dist, b.pend, g->q[0], b.c);
+    uint32_t nq = mssp_sync(g).nq_out, nfar = 0;
+    int cur = 0, fcur = 0;  // near queue / far list holding the live entries
+    uint64_t thr = delta;
+    bool last_split_empty = false;
+    uint32_t min_far = kValueMax;
+    uint64_t rounds = 0;
+    while (nq > 0 || nfar > 0) {
+        CGB_REQUIRE(++rounds <= 4ull * V + 64, CGB_ETIMEOUT, "multi-root SSSP round bound exceeded");
+        const int nxt = cur ^ 1;
+        CGB_CUDA_TRY(cudaMemsetAsync(&b.c->nq_out, 0, 4, g->stream));
+        if (nq > 0) {
+            // near round at threshold thr: q[cur] -> q[nxt]
+            const uint32_t t32 = (uint32_t)std::min<uint64_t>(thr, 0xFFFFFFFFull);
+            CGB_CUDA_TRY(cudaMemsetAsync(&b.c->ndesc, 0, 4, g->stream));
+            ++g->stats.launches;
+            k_mssp_desc<<<grid_for(nq, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(g->q[cur], nq, g->off, b.pend,
+                                                                                    b.maskq, b.desc, b.desc_cap, b.c);
+            ++g->stats.launches;
+            if (g->w)
+                k_mssp_expand<true><<<kNumSMs * 8, kBlock, 0, g->stream>>>(b.desc, b.c, b.maskq, g->dst, g->w, b.dist,
+                                                                          b.pend, b.farm, g->q[nxt],
+                                                                          b.far_list[fcur], V, t32, b.c);
+            else
+                k_mssp_expand<false><<<kNumSMs * 8, kBlock, 0, g->stream>>>(b.desc, b.c, b.maskq, g->dst, g->w,
+                                                                           b.dist, b.pend, b.farm, g->q[nxt],
+                                                                           b.far_list[fcur], V, t32, b.c);
+            const MsspCounters h = mssp_sync(g);
+            nq = h.nq_out;
+            nfar = h.nfar_live;
+            last_split_empty = false;
+            g->stats.pushes_td++;
+        } else {
+            // split of the far list at the next bucket [thr, hi): far_list[fcur] -> q[nxt] + far_list[fcur ^ 1]
+            uint64_t hi = thr + delta;
+            if (last_split_empty && min_far != kValueMax)
+                hi = std::max<uint64_t>(hi, ((uint64_t)min_far / delta + 1) * delta);
+            const uint32_t lo32 = (uint32_t)std::min<uint64_t>(thr, 0xFFFFFFFFull);
+            const uint32_t hi32 = (uint32_t)std::min<uint64_t>(hi, 0xFFFFFFFFull);
+            k_mssp_set<<<1, 1, 0, g->stream>>>(&b.c->min_far, kValueMax);
+            CGB_CUDA_TRY(cudaMemsetAsync(&b.c->nfar_next, 0, 4, g->stream));
+            ++g->stats.launches;
+            k_mssp_split<<<grid_for(nfar, kBlock / 32, kNumSMs * 8), kBlock, 0, g->stream>>>(
+                b.far_list[fcur], nfar, b.dist, b.pend, b.farm, g->q[nxt], b.far_list[fcur ^ 1], V, lo32, hi32, b.c);
+            const MsspCounters h = mssp_sync(g);
+            nq = h.nq_out;
+            nfar = h.nfar_next;
+            min_far = h.min_far;
+            fcur ^= 1;
+            k_mssp_set<<<1, 1, 0, g->stream>>>(&b.c->nfar_live, nfar);
+            thr = hi;
+            last_split_empty = nq == 0;
+        }
+        cur = nxt;
+    }
+    ++g->stats.launches;
+    k_mssp_out<<<kNumSMs * 16, kBlock, 0, g->stream>>>(b.dist, V, n, out);
+    g->stats.iterations = rounds;
+    g->stats.sssp_delta = delta;
+}
+
+}  // namespace cgb

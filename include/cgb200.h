@@ -78,6 +78,7 @@ typedef struct cgb_options {
 
 #define CGB_FLAG_KERNEL_TIMING 0x1u /* record per-kernel CUDA-event times (cgb_run_stats) */
 #define CGB_FLAG_TRACE 0x2u         /* log one cgb_iter_trace per iteration */
+#define CGB_FLAG_BATCH_SEQUENTIAL 0x4u /* cgb_run_batch: one cgb_run per root instead of multi-root passes */
 
 typedef struct cgb_graph cgb_graph;
 
@@ -176,8 +177,12 @@ cgb_status cgb_graph_result_download(const cgb_graph* g, void* values);
 cgb_status cgb_run(cgb_graph* g, int algorithm, uint32_t root_or_iters, const cgb_options* opt,
                    uint32_t* out_u32, double* out_f64, double* out_ms);
 
-/* Several roots of BFS or SSSP in one call; out_u32 holds nroots * V values
- * (root-major).  Results equal nroots separate cgb_run calls. */
+/* Several roots of BFS or SSSP in one call (no counterpart in the reference,
+ * whose drivers loop over roots); out_u32 (host or device) holds nroots * V
+ * values, root-major.  Roots run in passes of up to 64 sharing one
+ * traversal with bit-packed per-vertex root masks (CGB_FLAG_BATCH_SEQUENTIAL:
+ * one cgb_run per root instead).  Results equal nroots separate cgb_run
+ * calls; out_ms and the statistics cover all passes. */
 cgb_status cgb_run_batch(cgb_graph* g, int algorithm, const uint32_t* roots, uint32_t nroots,
                          const cgb_options* opt, uint32_t* out_u32, double* out_ms);
 

@@ -168,6 +168,36 @@ def test_multi_root_bfs_passes(oracle):
         assert g.stats().traversed_edges == sum(int(deg[out[i] != 999999999].sum()) for i in range(len(roots)))
 
 
+
+@pytest.mark.parametrize("weighted", [True, False])
+def test_multi_root_sssp_passes(oracle, weighted):
+    """Multi-root SSSP: 70 roots (passes of 64 and 6), a duplicate root, a
+    root without out-edges, several bucket widths, device-resident output,
+    and the one-by-one path giving the same distances."""
+    import torch
+    off, dst, w = oracle.rmat_graph(14, 16, seed=13)
+    if not weighted:
+        w = None
+    deg = np.diff(off.astype(np.int64))
+    rng = np.random.default_rng(6)
+    roots = [int(x) for x in rng.choice(off.size - 1, 68, replace=False)]
+    roots += [roots[5], int(np.nonzero(deg == 0)[0][0])]
+    w_or = w if weighted else np.ones_like(dst)
+    exp = np.stack([oracle.sssp(off, dst, w_or, r) for r in roots])
+    with cg.Graph.from_csr(off, dst, w) as g:
+        out, ms = g.run_batch(SSSP, roots)
+        assert ms > 0
+        np.testing.assert_array_equal(out, exp)
+        assert g.stats().traversed_edges == sum(int(deg[exp[i] != 999999999].sum()) for i in range(len(roots)))
+        for delta in (1, 13, 100000):
+            out, _ = g.run_batch(SSSP, roots[:64], cg.make_options(sssp_delta=delta))
+            np.testing.assert_array_equal(out, exp[:64], err_msg=f"delta {delta}")
+        d_out = torch.empty((len(roots), off.size - 1), dtype=torch.int32, device="cuda")
+        g.run_batch(SSSP, roots, out=d_out)
+        np.testing.assert_array_equal(d_out.cpu().numpy().view(np.uint32), exp)
+        seq, _ = g.run_batch(SSSP, roots[:5], cg.make_options(flags=L.FLAG_BATCH_SEQUENTIAL))
+        np.testing.assert_array_equal(seq, exp[:5])
+
 def _batch_graphs(oracle):
     """Uneven graphs: RMAT of scales 8-12 (directed and symmetric), grids,
     a graph without edges, one with a single vertex."""
