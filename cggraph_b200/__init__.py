@@ -14,6 +14,7 @@ from .engine import (  # noqa: F401
     Graph,
     GraphB200,
     OrderMethod,
+    Server,
     VertexValue_MAX,
     checkBinResult,
     load_binFile,

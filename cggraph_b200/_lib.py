@@ -32,7 +32,8 @@ EXPORTS = [
     "cgb_last_error_string", "cgb_status_string", "cgb_abi_version", "cgb_gen_rmat", "cgb_gen_grid",
     "cgb_graph_download", "cgb_bfs_noalloc", "cgb_policy_load", "cgb_policy_collect", "cgb_policy_train",
     "cgb_policy_forward", "cgb_policy_loss_grad", "cgb_batch_create", "cgb_batch_destroy", "cgb_batch_run",
-    "cgb_batch_info", "cgb_batch_stats",
+    "cgb_batch_info", "cgb_batch_stats", "cgb_server_create", "cgb_server_submit", "cgb_server_start",
+    "cgb_server_wait", "cgb_server_poll", "cgb_server_stats", "cgb_server_destroy",
 ]
 POLICY_FEATURES, POLICY_OUTPUTS, POLICY_PARAMS = 24, 9, 6345
 
@@ -93,6 +94,37 @@ class CgbError(RuntimeError):
 
 _lib = None
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [
+        ("struct_size", ctypes.c_uint32),
+        ("bfs_slots", ctypes.c_uint32),
+        ("sssp_slots", ctypes.c_uint32),
+        ("sssp_delta", ctypes.c_uint32),
+        ("memory_budget", ctypes.c_uint64),
+        ("flags", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 5),
+    ]
+
+
+SERVER_NO_BFS, SERVER_NO_SSSP = 0x1, 0x2
+
+
+class RequestInfo(ctypes.Structure):
+    _fields_ = [
+        ("id", ctypes.c_uint64),
+        ("algorithm", ctypes.c_int32),
+        ("root", ctypes.c_uint32),
+        ("arrival_us", ctypes.c_double),
+        ("admit_us", ctypes.c_double),
+        ("done_us", ctypes.c_double),
+        ("traversed_edges", ctypes.c_uint64),
+        ("reached", ctypes.c_uint32),
+        ("depth", ctypes.c_uint32),
+        ("status", ctypes.c_int32),
+        ("slot", ctypes.c_uint32),
+    ]
+
+
 _P = ctypes.c_void_p
 _u32p = ctypes.POINTER(ctypes.c_uint32)
 
@@ -140,6 +172,14 @@ def lib() -> ctypes.CDLL:
         L.cgb_batch_run.argtypes = [_P, i, _P, _P, ctypes.POINTER(ctypes.c_double)]
         L.cgb_batch_info.argtypes = [_P, _u32p, _u32p, ctypes.POINTER(ctypes.c_int32)]
         L.cgb_batch_stats.argtypes = [_P, ctypes.POINTER(RunStats)]
+        L.cgb_server_create.argtypes = [_P, ctypes.POINTER(ServerConfig), ctypes.POINTER(_P)]
+        L.cgb_server_submit.argtypes = [_P, i, u32, ctypes.c_double, _P, ctypes.POINTER(ctypes.c_uint64)]
+        L.cgb_server_start.argtypes = [_P]
+        L.cgb_server_wait.argtypes = [_P, ctypes.c_double, _u32p]
+        L.cgb_server_poll.argtypes = [_P, ctypes.POINTER(RequestInfo), u32, _u32p]
+        L.cgb_server_stats.argtypes = [_P, ctypes.POINTER(ctypes.c_uint64), _u32p, _u32p,
+                                       ctypes.POINTER(ctypes.c_double)]
+        L.cgb_server_destroy.argtypes = [_P]
         for name in EXPORTS:
             f = getattr(L, name)
             if name not in ("cgb_last_error_string", "cgb_status_string", "cgb_abi_version"):

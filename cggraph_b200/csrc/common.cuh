@@ -87,6 +87,12 @@ __device__ __forceinline__ T warp_sum(T v)
     return v;
 }
 
+__device__ __forceinline__ unsigned long long warp_or(unsigned long long v)
+{
+    for (int o = 16; o > 0; o >>= 1) v |= __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
 __device__ __forceinline__ uint32_t warp_max(uint32_t v)
 {
 #pragma unroll

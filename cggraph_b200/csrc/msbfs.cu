@@ -15,16 +15,10 @@
 //                its masks are written without atomics.
 // Levels go to out[k * V + u] (root-major, 999999999 = unreachable), the
 // layout of cgb_run_batch; they equal k separate cgb_run(CGB_BFS) results.
-#include "engine.cuh"
+#include "msbfs.cuh"
 #include "push.cuh"
 
 namespace cgb {
-
-struct MsBuffers {
-    unsigned long long* seen = nullptr;
-    unsigned long long* front[2] = {nullptr, nullptr};
-    unsigned long long* next = nullptr;
-};
 
 __global__ void k_ms_init(uint32_t V, unsigned long long* seen, unsigned long long* f0, unsigned long long* next)
 {
@@ -56,48 +50,18 @@ __global__ void k_ms_roots(const uint32_t* roots, uint32_t n, uint32_t V, unsign
     }
 }
 
-struct MsTdOp {
-    const uint32_t* __restrict__ off;
-    const uint32_t* __restrict__ dst;
-    const unsigned long long* __restrict__ front;
-    const unsigned long long* seen;
-    unsigned long long* next;
-    uint32_t* qout;
-    uint32_t* qlen;
-    uint32_t cap;
-    DevCounters* ctr;
-
-    __device__ __forceinline__ bool load(uint32_t v, uint32_t& s, uint32_t& d, uint32_t& m) const
-    {
-        s = off[v];
-        d = off[v + 1] - s;
-        m = v;
-        return true;
-    }
-    __device__ __forceinline__ void edge(bool valid, uint32_t e, uint32_t v) const
-    {
-        bool first = false;
-        uint32_t u = 0;
-        if (valid) {
-            u = dst[e];
-            const unsigned long long add = front[v] & ~seen[u];
-            if (add && (next[u] & add) != add) first = atomicOr(next + u, add) == 0ull;
-        }
-        warp_append(first, u, qout, qlen, cap, &ctr->overflow);
-    }
-    __device__ __forceinline__ void block_begin() const {}
-    __device__ __forceinline__ void block_end() const {}
-};
-
 // Moves next into seen / the new frontier for the queued vertices, writes
 // their levels, and keeps those with new roots (and out-edges) active.
 __global__ void __launch_bounds__(kBlock) k_ms_finalize(const uint32_t* __restrict__ q, uint32_t n,
-                                                        unsigned long long* seen, unsigned long long* next,
+                                                        const uint32_t* n_ptr, unsigned long long* seen, unsigned long long* next,
                                                         unsigned long long* fnext, uint32_t* level_out, uint32_t V,
                                                         uint32_t lvl, uint32_t nz, uint32_t* qact, uint32_t* qact_len,
-                                                        uint32_t cap, DevCounters* ctr)
+                                                        uint32_t cap, DevCounters* ctr, const uint32_t* start,
+                                                        unsigned long long* alive)
 {
+    if (n_ptr) n = *n_ptr;
     const uint32_t n_round = (n + 31u) & ~31u;
+    unsigned long long live = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_round; i += gridDim.x * blockDim.x) {
         bool act = false;
         uint32_t u = 0;
@@ -107,12 +71,22 @@ __global__ void __launch_bounds__(kBlock) k_ms_finalize(const uint32_t* __restri
             next[u] = 0;
             if (x) {
                 seen[u] |= x;
-                for (unsigned long long m = x; m; m &= m - 1) level_out[(size_t)(__ffsll(m) - 1) * V + u] = lvl;
+                for (unsigned long long m = x; m; m &= m - 1) {
+                    const uint32_t k = __ffsll(m) - 1;
+                    level_out[(size_t)k * V + u] = start ? lvl - start[k] : lvl;
+                }
                 act = u < nz;
-                if (act) fnext[u] = x;
+                if (act) {
+                    fnext[u] = x;
+                    live |= x;
+                }
             }
         }
         warp_append(act, u, qact, qact_len, cap, &ctr->overflow);
+    }
+    if (alive) {
+        live = warp_or(live);
+        if (lane_id() == 0 && live) atomicOr(alive, live);
     }
 }
 
@@ -129,9 +103,10 @@ __global__ void __launch_bounds__(kBlock) k_ms_bu(uint32_t V, const uint32_t* __
                                                   unsigned long long* seen, unsigned long long* fnext,
                                                   unsigned long long full, uint32_t* level_out, uint32_t lvl,
                                                   uint32_t nz, uint32_t* qact, uint32_t* qact_len, uint32_t cap,
-                                                  DevCounters* ctr)
+                                                  DevCounters* ctr, const uint32_t* start, unsigned long long* alive)
 {
     const uint32_t n_round = (V + 31u) & ~31u;
+    unsigned long long live = 0;
     for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n_round; u += gridDim.x * blockDim.x) {
         bool act = false;
         if (u < V) {
@@ -146,20 +121,30 @@ __global__ void __launch_bounds__(kBlock) k_ms_bu(uint32_t V, const uint32_t* __
                 }
                 if (got) {
                     seen[u] = s | got;
-                    for (unsigned long long m = got; m; m &= m - 1)
-                        level_out[(size_t)(__ffsll(m) - 1) * V + u] = lvl;
+                    for (unsigned long long m = got; m; m &= m - 1) {
+                        const uint32_t k = __ffsll(m) - 1;
+                        level_out[(size_t)k * V + u] = start ? lvl - start[k] : lvl;
+                    }
                     act = u < nz;
-                    if (act) fnext[u] = got;
+                    if (act) {
+                        fnext[u] = got;
+                        live |= got;
+                    }
                 }
             }
         }
         warp_append(act, u, qact, qact_len, cap, &ctr->overflow);
     }
+    if (alive) {
+        live = warp_or(live);
+        if (lane_id() == 0 && live) atomicOr(alive, live);
+    }
 }
 
-__global__ void k_ms_degree_sum(const uint32_t* __restrict__ q, uint32_t n, const uint32_t* __restrict__ off,
-                                DevCounters* ctr)
+__global__ void k_ms_degree_sum(const uint32_t* __restrict__ q, uint32_t n, const uint32_t* n_ptr,
+                                const uint32_t* __restrict__ off, DevCounters* ctr)
 {
+    if (n_ptr) n = *n_ptr;
     unsigned long long s = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t v = q[i];
@@ -169,7 +154,7 @@ __global__ void k_ms_degree_sum(const uint32_t* __restrict__ q, uint32_t n, cons
     if (lane_id() == 0 && s) atomicAdd(&ctr->medges, s);
 }
 
-static unsigned long long* ms_alloc(size_t n)
+unsigned long long* ms_alloc(size_t n)
 {
     void* p = nullptr;
     CGB_CUDA_TRY(cudaMalloc(&p, (n ? n : 1) * 8));
@@ -214,7 +199,7 @@ void run_msbfs(cgb_graph* g, const uint32_t* d_roots, uint32_t n, uint32_t* leve
         CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->medges, 0, 8, g->stream));
         ++g->stats.launches;
         k_ms_degree_sum<<<grid_for(nact, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(g->q[cur], (uint32_t)nact,
-                                                                                      g->off, g->ctr);
+                                                                                      nullptr, g->off, g->ctr);
         sync_counters(g);
         const bool pull = (double)g->h_ctr->medges * alpha > (double)g->E;
         const int nxt = cur ^ 1;
@@ -225,7 +210,7 @@ void run_msbfs(cgb_graph* g, const uint32_t* d_roots, uint32_t n, uint32_t* leve
             ++g->stats.launches;
             k_ms_bu<<<grid_for(V, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(
                 V, g->in_off, g->in_src, fcur, b.seen, fnxt, full, level_out, lvl + 1, g->nz, g->q[nxt],
-                &g->ctr->qlen[nxt], V, g->ctr);
+                &g->ctr->qlen[nxt], V, g->ctr, nullptr, nullptr);
             g->stats.pulls_bu++;
         } else {
             // expansion into next[]: touched vertices are queued once in stamp[]
@@ -239,8 +224,8 @@ void run_msbfs(cgb_graph* g, const uint32_t* d_roots, uint32_t n, uint32_t* leve
             if (touched) {
                 ++g->stats.launches;
                 k_ms_finalize<<<grid_for(touched, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(
-                    g->stamp, touched, b.seen, b.next, fnxt, level_out, V, lvl + 1, g->nz, g->q[nxt],
-                    &g->ctr->qlen[nxt], V, g->ctr);
+                    g->stamp, touched, nullptr, b.seen, b.next, fnxt, level_out, V, lvl + 1, g->nz, g->q[nxt],
+                    &g->ctr->qlen[nxt], V, g->ctr, nullptr, nullptr);
             }
             g->stats.pushes_td++;
         }

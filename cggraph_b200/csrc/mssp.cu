@@ -20,34 +20,9 @@
 // descriptors of at most kMsEdges edges (hub lists are spread over many
 // warps); a warp takes one descriptor, reads its 32 next edges' targets and
 // weights coalesced, and walks them with shuffles.
-#include "engine.cuh"
+#include "mssp.cuh"
 
 namespace cgb {
-
-constexpr uint32_t kMsRoots = 64;   // distance slots per vertex
-constexpr uint32_t kMsEdges = 256;  // edges per work descriptor
-
-struct MsspCounters {
-    uint32_t nq_out;       // entries of the near queue being built
-    uint32_t nfar_live;    // entries of the live far list (expansion rounds append)
-    uint32_t nfar_next;    // entries kept by a split in the other far list
-    uint32_t ndesc;        // descriptors of the round
-    uint32_t min_far;      // smallest far distance >= hi seen by a split
-    uint32_t overflow;
-    unsigned long long relax;  // successful relaxations
-};
-
-struct MsspBuffers {
-    uint32_t* dist = nullptr;               // V * 64
-    unsigned long long* pend = nullptr;     // V
-    unsigned long long* farm = nullptr;     // V
-    unsigned long long* maskq = nullptr;    // V: pend of each queue entry, taken by the descriptor pass
-    uint32_t* far_list[2] = {nullptr, nullptr};  // V each
-    uint4* desc = nullptr;                  // {v, edge begin, edge end, queue index}
-    uint64_t desc_cap = 0;
-    MsspCounters* c = nullptr;
-    MsspCounters* h = nullptr;              // pinned host copy
-};
 
 __global__ void k_mssp_init(uint32_t V, uint4* dist4, unsigned long long* pend, unsigned long long* farm)
 {
@@ -78,11 +53,12 @@ __global__ void k_mssp_roots(const uint32_t* roots, uint32_t n, uint32_t* dist, 
 
 // Takes (and clears) the pend mask of every queued vertex and cuts its list
 // into descriptors of at most kMsEdges edges.
-__global__ void __launch_bounds__(kBlock) k_mssp_desc(const uint32_t* __restrict__ q, uint32_t nq,
+__global__ void __launch_bounds__(kBlock) k_mssp_desc(const uint32_t* __restrict__ q, const uint32_t* nq_ptr,
                                                       const uint32_t* __restrict__ off, unsigned long long* pend,
                                                       unsigned long long* maskq, uint4* desc, uint64_t cap,
                                                       MsspCounters* c)
 {
+    const uint32_t nq = *nq_ptr;
     const uint32_t n_round = (nq + 31u) & ~31u;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_round; i += gridDim.x * blockDim.x) {
         uint32_t v = 0, s = 0, d = 0, nd = 0;
@@ -117,22 +93,27 @@ __global__ void __launch_bounds__(kBlock) k_mssp_desc(const uint32_t* __restrict
 }
 
 // One near round: relaxes every descriptor's edges for the roots of its
-// vertex's mask.  Pairs improved below thr go to pend (their vertex queued
-// on the 0 -> non-zero transition), the others to farm (vertex listed in
-// the far list on the same transition).
+// vertex's mask.  Pairs improved below their root's threshold (thr, or
+// thr_slot[k] per root) go to pend (their vertex queued in qout on the
+// 0 -> non-zero transition), the others to farm (vertex listed in far_out
+// on the same transition).  alive (optional) collects the roots that got
+// near work ([0]) and far work ([1]).
 template <bool kHasW>
 __global__ void __launch_bounds__(kBlock) k_mssp_expand(const uint4* __restrict__ desc, const MsspCounters* cc,
                                                         const unsigned long long* __restrict__ maskq,
                                                         const uint32_t* __restrict__ dst,
                                                         const uint32_t* __restrict__ w, uint32_t* dist,
                                                         unsigned long long* pend, unsigned long long* farm,
-                                                        uint32_t* qout, uint32_t* far_out, uint32_t cap, uint32_t thr,
+                                                        uint32_t* qout, uint32_t* qout_len, uint32_t* far_out,
+                                                        uint32_t* far_len, uint32_t cap, uint32_t thr,
+                                                        const uint32_t* thr_slot, unsigned long long* alive,
                                                         MsspCounters* c)
 {
     const uint32_t ndesc = min((uint64_t)cc->ndesc, (uint64_t)0xFFFFFFFFu);
     const uint32_t lane = lane_id();
     const uint32_t warps = gridDim.x * (kBlock / 32);
-    unsigned long long relax = 0;
+    const uint32_t thr0 = thr_slot ? thr_slot[lane] : thr, thr1 = thr_slot ? thr_slot[lane + 32] : thr;
+    unsigned long long relax = 0, near_live = 0, far_live = 0;
     for (uint32_t j = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5); j < ndesc; j += warps) {
         const uint4 d = desc[j];
         const unsigned long long m = maskq[d.w];
@@ -173,7 +154,7 @@ __global__ void __launch_bounds__(kBlock) k_mssp_expand(const uint4* __restrict_
                         const uint32_t old = atomicMin(du + lane, (uint32_t)c0);
                         if ((uint32_t)c0 < old) {
                             relax++;
-                            n0 = (uint32_t)c0 < thr;
+                            n0 = (uint32_t)c0 < thr0;
                             f0 = !n0;
                         }
                     }
@@ -181,7 +162,7 @@ __global__ void __launch_bounds__(kBlock) k_mssp_expand(const uint4* __restrict_
                         const uint32_t old = atomicMin(du + lane + 32, (uint32_t)c1);
                         if ((uint32_t)c1 < old) {
                             relax++;
-                            n1 = (uint32_t)c1 < thr;
+                            n1 = (uint32_t)c1 < thr1;
                             f1 = !n1;
                         }
                     }
@@ -197,60 +178,89 @@ __global__ void __launch_bounds__(kBlock) k_mssp_expand(const uint4* __restrict_
             }
             const bool qn = my_nb && atomicOr(pend + my_u, my_nb) == 0ull;
             const bool qf = my_fb && atomicOr(farm + my_u, my_fb) == 0ull;
-            warp_append(qn, my_u, qout, &c->nq_out, cap, &c->overflow);
-            warp_append(qf, my_u, far_out, &c->nfar_live, cap, &c->overflow);
+            near_live |= my_nb;
+            far_live |= my_fb;
+            warp_append(qn, my_u, qout, qout_len, cap, &c->overflow);
+            warp_append(qf, my_u, far_out, far_len, cap, &c->overflow);
         }
     }
     relax = warp_sum(relax);
     if (lane == 0 && relax) atomicAdd(&c->relax, relax);
+    if (alive) {
+        near_live = warp_or(near_live);
+        far_live = warp_or(far_live);
+        if (lane == 0 && near_live) atomicOr(alive, near_live);
+        if (lane == 0 && far_live) atomicOr(alive + 1, far_live);
+    }
 }
 
-// Split: for every vertex of the far list, its far pairs with lo <= dist <
-// hi go to pend (vertex queued), those below lo were expanded already and
-// are dropped, the rest stay far (vertex kept in the other far list) and
-// their smallest distance is reported.
-__global__ void __launch_bounds__(kBlock) k_mssp_split(const uint32_t* __restrict__ far_in, uint32_t nfar,
+// Split: for every vertex of the far list and every root k of `adv` (the
+// roots whose near work is done), the far pairs with lo_k <= dist < hi_k go
+// to pend (vertex queued in q on pend's 0 -> non-zero transition), those
+// below lo_k were expanded already and are dropped, and the rest stay far;
+// vertices with far pairs left are written to far_out.  The smallest kept
+// distance >= hi_k is reported per root (min_far_slot) or overall
+// (c->min_far); far_alive (optional) receives the roots with far pairs left.
+// lo_slot / hi_slot (per root) may be NULL for one range [lo, hi).
+__global__ void __launch_bounds__(kBlock) k_mssp_split(const uint32_t* __restrict__ far_in, const uint32_t* nfar_ptr,
                                                        const uint32_t* __restrict__ dist, unsigned long long* pend,
-                                                       unsigned long long* farm, uint32_t* q, uint32_t* far_out,
-                                                       uint32_t cap, uint32_t lo, uint32_t hi, MsspCounters* c)
+                                                       unsigned long long* farm, uint32_t* q, uint32_t* q_len,
+                                                       uint32_t* far_out, uint32_t* far_out_len, uint32_t cap,
+                                                       uint32_t lo, uint32_t hi, const uint32_t* lo_slot,
+                                                       const uint32_t* hi_slot, unsigned long long adv,
+                                                       uint32_t* min_far_slot, unsigned long long* far_alive,
+                                                       MsspCounters* c)
 {
+    const uint32_t nfar = *nfar_ptr;
     const uint32_t lane = lane_id();
     const uint32_t warps = gridDim.x * (kBlock / 32);
-    uint32_t mn = kValueMax;
+    const uint32_t lo0 = lo_slot ? lo_slot[lane] : lo, lo1 = lo_slot ? lo_slot[lane + 32] : lo;
+    const uint32_t hi0 = hi_slot ? hi_slot[lane] : hi, hi1 = hi_slot ? hi_slot[lane + 32] : hi;
+    const bool adv0 = (adv >> lane) & 1ull, adv1 = (adv >> (lane + 32)) & 1ull;
+    uint32_t mn0 = kValueMax, mn1 = kValueMax;
+    unsigned long long live = 0;
     for (uint32_t i = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5); i < nfar; i += warps) {
         const uint32_t v = far_in[i];
         const unsigned long long m = farm[v];
-        const bool a0 = (m >> lane) & 1ull, a1 = (m >> (lane + 32)) & 1ull;
+        const bool a0 = adv0 && ((m >> lane) & 1ull), a1 = adv1 && ((m >> (lane + 32)) & 1ull);
         const uint32_t* row = dist + (size_t)v * kMsRoots;
         const uint32_t d0 = a0 ? row[lane] : kValueMax, d1 = a1 ? row[lane + 32] : kValueMax;
-        const bool mv0 = a0 && d0 < hi, mv1 = a1 && d1 < hi;
-        const bool nr0 = mv0 && d0 >= lo, nr1 = mv1 && d1 >= lo;
-        if (a0 && !mv0) mn = min(mn, d0);
-        if (a1 && !mv1) mn = min(mn, d1);
+        const bool mv0 = a0 && d0 < hi0, mv1 = a1 && d1 < hi1;
+        const bool nr0 = mv0 && d0 >= lo0, nr1 = mv1 && d1 >= lo1;
+        if (a0 && !mv0) mn0 = min(mn0, d0);
+        if (a1 && !mv1) mn1 = min(mn1, d1);
         const unsigned long long moved = (unsigned long long)__ballot_sync(0xffffffffu, mv0) |
                                          ((unsigned long long)__ballot_sync(0xffffffffu, mv1) << 32);
         const unsigned long long nearb = (unsigned long long)__ballot_sync(0xffffffffu, nr0) |
                                          ((unsigned long long)__ballot_sync(0xffffffffu, nr1) << 32);
         const unsigned long long keep = m & ~moved;
+        live |= keep;
         if (lane == 0) {
-            if (moved) farm[v] = keep;
-            if (nearb) pend[v] = nearb;  // no expansion runs during a split: v is this warp's alone
-        }
-        if (lane == 0) {
-            if (nearb) {
-                const uint32_t p = atomicAdd(&c->nq_out, 1u);
+            if (moved) farm[v] = keep;  // no expansion runs during a split: v's far mask is this warp's
+            if (nearb && atomicOr(pend + v, nearb) == 0ull) {
+                const uint32_t p = atomicAdd(q_len, 1u);
                 if (p < cap) q[p] = v;
                 else atomicOr(&c->overflow, 1u);
             }
             if (keep) {
-                const uint32_t p = atomicAdd(&c->nfar_next, 1u);
+                const uint32_t p = atomicAdd(far_out_len, 1u);
                 if (p < cap) far_out[p] = v;
                 else atomicOr(&c->overflow, 1u);
             }
         }
     }
-    mn = __reduce_min_sync(0xffffffffu, mn);
-    if (lane == 0 && mn != kValueMax) atomicMin(&c->min_far, mn);
+    if (min_far_slot) {
+        // per root: mn0 is root lane's, mn1 root lane + 32's, each reduced over the warp's vertices
+        if (mn0 != kValueMax) atomicMin(min_far_slot + lane, mn0);
+        if (mn1 != kValueMax) atomicMin(min_far_slot + lane + 32, mn1);
+    } else {
+        const uint32_t mn = __reduce_min_sync(0xffffffffu, min(mn0, mn1));
+        if (lane == 0 && mn != kValueMax) atomicMin(&c->min_far, mn);
+    }
+    if (far_alive) {
+        live = warp_or(live);
+        if (lane == 0 && live) atomicOr(far_alive, live);
+    }
 }
 
 // dist (vertex-major, 64 slots) -> out[k * V + v] for k < n, through a
@@ -275,10 +285,24 @@ __global__ void __launch_bounds__(kBlock) k_mssp_out(const uint32_t* __restrict_
     }
 }
 
-static void mssp_alloc(cgb_graph* g)
+void mssp_expand(bool weighted, uint32_t grid, cudaStream_t st, const uint4* desc, const MsspCounters* cc,
+                 const unsigned long long* maskq, const uint32_t* dst, const uint32_t* w, uint32_t* dist,
+                 unsigned long long* pend, unsigned long long* farm, uint32_t* qout, uint32_t* qout_len,
+                 uint32_t* far_out, uint32_t* far_len, uint32_t cap, uint32_t thr, const uint32_t* thr_slot,
+                 unsigned long long* alive)
 {
-    if (g->mssp) return;
-    const uint32_t V = g->V;
+    MsspCounters* c = const_cast<MsspCounters*>(cc);
+    if (weighted)
+        k_mssp_expand<true><<<grid, kBlock, 0, st>>>(desc, cc, maskq, dst, w, dist, pend, farm, qout, qout_len, far_out,
+                                                     far_len, cap, thr, thr_slot, alive, c);
+    else
+        k_mssp_expand<false><<<grid, kBlock, 0, st>>>(desc, cc, maskq, dst, w, dist, pend, farm, qout, qout_len,
+                                                      far_out, far_len, cap, thr, thr_slot, alive, c);
+    CGB_CUDA_TRY(cudaGetLastError());
+}
+
+MsspBuffers* mssp_buffers_alloc(uint32_t V, uint64_t E)
+{
     auto* b = new MsspBuffers();
     try {
         CGB_CUDA_TRY(cudaMalloc((void**)&b->dist, (size_t)V * kMsRoots * 4));
@@ -287,21 +311,19 @@ static void mssp_alloc(cgb_graph* g)
         CGB_CUDA_TRY(cudaMalloc((void**)&b->maskq, (size_t)V * 8));
         CGB_CUDA_TRY(cudaMalloc((void**)&b->far_list[0], (size_t)V * 4));
         CGB_CUDA_TRY(cudaMalloc((void**)&b->far_list[1], (size_t)V * 4));
-        b->desc_cap = (uint64_t)V + (uint64_t)g->E / kMsEdges + 1;
+        b->desc_cap = (uint64_t)V + E / kMsEdges + 1;
         CGB_CUDA_TRY(cudaMalloc((void**)&b->desc, b->desc_cap * sizeof(uint4)));
         CGB_CUDA_TRY(cudaMalloc((void**)&b->c, sizeof(MsspCounters)));
         CGB_CUDA_TRY(cudaMallocHost((void**)&b->h, sizeof(MsspCounters)));
     } catch (...) {
-        g->mssp = b;
-        free_mssp(g);
+        mssp_buffers_free(b);
         throw;
     }
-    g->mssp = b;
+    return b;
 }
 
-void free_mssp(cgb_graph* g)
+void mssp_buffers_free(MsspBuffers* b)
 {
-    MsspBuffers* b = g->mssp;
     if (!b) return;
     cudaFree(b->dist);
     cudaFree(b->pend);
@@ -313,6 +335,16 @@ void free_mssp(cgb_graph* g)
     cudaFree(b->c);
     if (b->h) cudaFreeHost(b->h);
     delete b;
+}
+
+static void mssp_alloc(cgb_graph* g)
+{
+    if (!g->mssp) g->mssp = mssp_buffers_alloc(g->V, g->E);
+}
+
+void free_mssp(cgb_graph* g)
+{
+    mssp_buffers_free(g->mssp);
     g->mssp = nullptr;
 }
 
@@ -350,6 +382,7 @@ void run_mssp(cgb_graph* g, const uint32_t* d_roots, uint32_t n, uint32_t* out, 
     ++g->stats.launches;
     k_mssp_roots<<<1, 1, 0, g->stream>>>(d_roots, n, b.dist, b.pend, g->q[0], b.c);
     uint32_t nq = mssp_sync(g).nq_out, nfar = 0;
+    CGB_CUDA_TRY(cudaMemcpyAsync(&b.c->nq_in, &b.c->nq_out, 4, cudaMemcpyDeviceToDevice, g->stream));
     int cur = 0, fcur = 0;  // near queue / far list holding the live entries
     uint64_t thr = delta;
     bool last_split_empty = false;
@@ -364,17 +397,13 @@ void run_mssp(cgb_graph* g, const uint32_t* d_roots, uint32_t n, uint32_t* out, 
             const uint32_t t32 = (uint32_t)std::min<uint64_t>(thr, 0xFFFFFFFFull);
             CGB_CUDA_TRY(cudaMemsetAsync(&b.c->ndesc, 0, 4, g->stream));
             ++g->stats.launches;
-            k_mssp_desc<<<grid_for(nq, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(g->q[cur], nq, g->off, b.pend,
-                                                                                    b.maskq, b.desc, b.desc_cap, b.c);
+            k_mssp_desc<<<grid_for(nq, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(g->q[cur], &b.c->nq_in, g->off,
+                                                                                    b.pend, b.maskq, b.desc,
+                                                                                    b.desc_cap, b.c);
             ++g->stats.launches;
-            if (g->w)
-                k_mssp_expand<true><<<kNumSMs * 8, kBlock, 0, g->stream>>>(b.desc, b.c, b.maskq, g->dst, g->w, b.dist,
-                                                                          b.pend, b.farm, g->q[nxt],
-                                                                          b.far_list[fcur], V, t32, b.c);
-            else
-                k_mssp_expand<false><<<kNumSMs * 8, kBlock, 0, g->stream>>>(b.desc, b.c, b.maskq, g->dst, g->w,
-                                                                           b.dist, b.pend, b.farm, g->q[nxt],
-                                                                           b.far_list[fcur], V, t32, b.c);
+            mssp_expand(g->w != nullptr, kNumSMs * 8, g->stream, b.desc, b.c, b.maskq, g->dst, g->w, b.dist, b.pend,
+                        b.farm, g->q[nxt], &b.c->nq_out, b.far_list[fcur], &b.c->nfar_live, V, t32, nullptr,
+                        nullptr);
             const MsspCounters h = mssp_sync(g);
             nq = h.nq_out;
             nfar = h.nfar_live;
@@ -391,7 +420,8 @@ void run_mssp(cgb_graph* g, const uint32_t* d_roots, uint32_t n, uint32_t* out, 
             CGB_CUDA_TRY(cudaMemsetAsync(&b.c->nfar_next, 0, 4, g->stream));
             ++g->stats.launches;
             k_mssp_split<<<grid_for(nfar, kBlock / 32, kNumSMs * 8), kBlock, 0, g->stream>>>(
-                b.far_list[fcur], nfar, b.dist, b.pend, b.farm, g->q[nxt], b.far_list[fcur ^ 1], V, lo32, hi32, b.c);
+                b.far_list[fcur], &b.c->nfar_live, b.dist, b.pend, b.farm, g->q[nxt], &b.c->nq_out,
+                b.far_list[fcur ^ 1], &b.c->nfar_next, V, lo32, hi32, nullptr, nullptr, ~0ull, nullptr, nullptr, b.c);
             const MsspCounters h = mssp_sync(g);
             nq = h.nq_out;
             nfar = h.nfar_next;
@@ -402,6 +432,7 @@ void run_mssp(cgb_graph* g, const uint32_t* d_roots, uint32_t n, uint32_t* out, 
             last_split_empty = nq == 0;
         }
         cur = nxt;
+        CGB_CUDA_TRY(cudaMemcpyAsync(&b.c->nq_in, &b.c->nq_out, 4, cudaMemcpyDeviceToDevice, g->stream));
     }
     ++g->stats.launches;
     k_mssp_out<<<kNumSMs * 16, kBlock, 0, g->stream>>>(b.dist, V, n, out);

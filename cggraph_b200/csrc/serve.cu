@@ -1,0 +1,762 @@
+// Request server: BFS and SSSP root queries against one resident graph with
+// continuous batching (no counterpart in the reference, whose drivers run
+// one root at a time, my_project/CGgraph/main_partition.hpp:188-227).
+//
+// Each algorithm has a group of up to 64 slots that share one traversal
+// with bit-packed per-vertex root masks (the multi-root engines of
+// msbfs.cu / mssp.cu).  The server thread runs ticks; a tick
+//   1. admits requests whose arrival time has passed into free slots (a
+//      slot is free once the previous occupant's result has been copied
+//      out, and the slots of a group are capped so that their result
+//      regions fit the memory budget);
+//   2. advances every active slot by one BFS level / one SSSP round, all
+//      slots of a group in the same kernels, the BFS group on the graph's
+//      stream and the SSSP group on its own so that the two overlap;
+//   3. retires the slots whose traversal ended (no frontier bits left for
+//      them), copying their results out and freeing the slot.
+// A request admitted while others run starts at its own level 0 (BFS
+// levels are written as tick - start[slot]) and keeps its own delta-stepping
+// buckets (SSSP thresholds per slot), so its result equals a lone cgb_run.
+// All traversal state stays in HBM; the host only decides admissions and
+// reads a few counters per tick.
+#include <string.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <thread>
+#include <vector>
+
+#include "../../include/cgb200.h"
+#include "engine.cuh"
+#include "msbfs.cuh"
+#include "mssp.cuh"
+#include "push.cuh"
+
+namespace cgb {
+
+constexpr uint32_t kSrvSlots = 64;
+
+// ---------------------------------------------------------------- kernels
+
+// Clears the bits of `mask` from every vertex's seen mask (slots reused).
+__global__ void k_srv_clear_bits(uint32_t V, unsigned long long* seen, unsigned long long mask)
+{
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x)
+        if (seen[v] & mask) seen[v] &= ~mask;
+}
+
+// BFS admissions: n pairs (slot, root); roots with out-edges join the
+// current frontier at q[qpos + j] (j = rank among them, computed on the host).
+__global__ void k_srv_bfs_admit(uint32_t n, const uint32_t* __restrict__ slots, const uint32_t* __restrict__ roots,
+                                const uint32_t* __restrict__ qidx, uint32_t V, uint32_t* region,
+                                unsigned long long* seen, unsigned long long* front, uint32_t* q)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t k = slots[i], r = roots[i];
+    region[(size_t)k * V + r] = 0;
+    atomicOr(seen + r, 1ull << k);
+    if (qidx[i] != 0xFFFFFFFFu) {
+        atomicOr(front + r, 1ull << k);
+        q[qidx[i]] = r;
+    }
+}
+
+// Per finished slot (bit k of mask): traversed edges (out-degrees of the
+// reached vertices), reached vertices and the largest finite value of
+// region k.
+__global__ void __launch_bounds__(kBlock) k_srv_stats(const uint32_t* __restrict__ region, uint32_t V,
+                                                      const uint32_t* __restrict__ off, unsigned long long mask,
+                                                      unsigned long long* edges, uint32_t* reached, uint32_t* depth)
+{
+    const uint32_t n_round = (V + 31u) & ~31u;
+    for (unsigned long long m = mask; m; m &= m - 1) {
+        const uint32_t k = __ffsll(m) - 1;
+        const uint32_t* r = region + (size_t)k * V;
+        unsigned long long e = 0;
+        uint32_t cnt = 0, mx = 0;
+        for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n_round; v += gridDim.x * blockDim.x) {
+            if (v < V) {
+                const uint32_t x = r[v];
+                if (x != kValueMax) {
+                    e += off[v + 1] - off[v];
+                    cnt++;
+                    mx = max(mx, x);
+                }
+            }
+        }
+        e = warp_sum(e);
+        cnt = warp_sum(cnt);
+        mx = warp_max(mx);
+        if (lane_id() == 0) {
+            if (e) atomicAdd(edges + k, e);
+            if (cnt) atomicAdd(reached + k, cnt);
+            if (mx) atomicMax(depth + k, mx);
+        }
+    }
+}
+
+// SSSP: distances of the slots in mask back to MAX (slots reused), a warp
+// per vertex with lanes over slots.
+__global__ void k_srv_sp_reset(uint32_t V, uint32_t* dist, unsigned long long mask)
+{
+    const uint32_t lane = lane_id();
+    const bool m0 = (mask >> lane) & 1ull, m1 = (mask >> (lane + 32)) & 1ull;
+    for (uint32_t v = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); v < V; v += gridDim.x * (blockDim.x / 32)) {
+        uint32_t* row = dist + (size_t)v * kMsRoots;
+        if (m0) row[lane] = kValueMax;
+        if (m1) row[lane + 32] = kValueMax;
+    }
+}
+
+// SSSP admissions: dist[root][slot] = 0 and the root queued (once) in q.
+__global__ void k_srv_sp_admit(uint32_t n, const uint32_t* __restrict__ slots, const uint32_t* __restrict__ roots,
+                               uint32_t* dist, unsigned long long* pend, uint32_t* q, uint32_t* q_len, uint32_t cap,
+                               MsspCounters* c)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t k = slots[i], r = roots[i];
+    dist[(size_t)r * kMsRoots + k] = 0;
+    if (atomicOr(pend + r, 1ull << k) == 0ull) {
+        const uint32_t p = atomicAdd(q_len, 1u);
+        if (p < cap) q[p] = r;
+        else atomicOr(&c->overflow, 1u);
+    }
+}
+
+// SSSP results of the slots in mask: region[k * V + v] = dist[v][k],
+// through a 32-vertex x 64-slot shared tile.
+__global__ void __launch_bounds__(kBlock) k_srv_sp_extract(const uint32_t* __restrict__ dist, uint32_t V,
+                                                           unsigned long long mask, uint32_t* region)
+{
+    __shared__ uint32_t tile[32][kMsRoots + 1];
+    __shared__ uint8_t ks[kMsRoots];
+    uint32_t n = 0;
+    for (unsigned long long m = mask; m; m &= m - 1) {
+        if (threadIdx.x == 0) ks[n] = (uint8_t)(__ffsll(m) - 1);
+        n++;
+    }
+    __syncthreads();
+    const uint32_t tiles = (V + 31) / 32;
+    for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+        const uint32_t v0 = t * 32;
+        for (uint32_t i = threadIdx.x; i < 32 * kMsRoots; i += blockDim.x) {
+            const uint32_t r = i / kMsRoots, k = i % kMsRoots;
+            if (v0 + r < V) tile[r][k] = dist[(size_t)(v0 + r) * kMsRoots + k];
+        }
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < 32 * n; i += blockDim.x) {
+            const uint32_t k = ks[i / 32], r = i % 32;
+            if (v0 + r < V) region[(size_t)k * V + v0 + r] = tile[r][k];
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_srv_copy_u32(const uint32_t* src, uint32_t* dst) { *dst = *src; }
+
+// ------------------------------------------------------------------ state
+
+using Clock = std::chrono::steady_clock;
+
+struct SrvReq {
+    cgb_request_info info{};
+    uint32_t* out = nullptr;
+};
+
+enum class SlotState { kFree, kActive };
+
+// Per-slot statistics block (device) and its pinned mirror.
+struct SlotStats {
+    unsigned long long edges[kSrvSlots];
+    uint32_t reached[kSrvSlots];
+    uint32_t depth[kSrvSlots];
+    unsigned long long alive[2];  // BFS: [0] next-frontier slots; SSSP: [0] near work, [1] far work
+    uint32_t min_far[kSrvSlots];
+};
+
+// Host-visible upload block for a tick's admissions and per-slot thresholds.
+struct SlotUpload {
+    uint32_t slots[kSrvSlots];
+    uint32_t roots[kSrvSlots];
+    uint32_t qidx[kSrvSlots];
+    uint32_t start[kSrvSlots];  // BFS: tick of admission
+    uint32_t thr[kSrvSlots];    // SSSP: near threshold per slot
+    uint32_t lo[kSrvSlots];     // SSSP: bucket being split in
+    uint32_t hi[kSrvSlots];
+    uint32_t min_far[kSrvSlots];
+};
+
+struct Group {
+    int alg = CGB_BFS;
+    uint32_t nslots = 0;
+    SlotState state[kSrvSlots];
+    int64_t req[kSrvSlots];
+    bool used[kSrvSlots] = {};
+    uint32_t* region = nullptr;  // nslots * V results
+    SlotStats* d_stats = nullptr;
+    SlotStats* h_stats = nullptr;
+    SlotUpload* d_up = nullptr;
+    SlotUpload* h_up = nullptr;
+    cudaStream_t stream = nullptr;
+    unsigned long long active = 0;
+    std::vector<std::pair<uint32_t, int64_t>> admit;  // (slot, request) of this tick
+    // BFS
+    MsBuffers mb;
+    uint32_t* q[2] = {nullptr, nullptr};
+    uint32_t* touched = nullptr;
+    uint32_t nact = 0, cur = 0, tick = 0;
+    unsigned long long medges = 0;
+    // SSSP
+    MsspBuffers* sp = nullptr;
+    uint32_t delta = 1, fcur = 0;
+    unsigned long long near_alive = 0, far_alive = 0, split_mask = 0;
+    uint64_t thr[kSrvSlots] = {};
+    uint32_t min_far[kSrvSlots];
+    bool last_empty[kSrvSlots] = {};
+};
+
+}  // namespace cgb
+
+using namespace cgb;
+
+struct cgb_server {
+    cgb_graph* g = nullptr;
+    Group grp[2];  // [0] BFS, [1] SSSP
+    std::vector<SrvReq> reqs;
+    std::deque<int64_t> waiting[2];    // submitted, not admitted (arrival order of submission)
+    std::vector<cgb_request_info> done;
+    std::mutex mu;
+    std::condition_variable cv;
+    std::thread th;
+    std::atomic<bool> stop{false};
+    bool started = false;
+    Clock::time_point t0;
+    uint64_t ticks = 0, completed = 0;
+    double busy_ms = 0;
+    cgb_status error = CGB_OK;
+    std::string error_msg;
+};
+
+namespace cgb {
+
+static double us_since(const cgb_server* s, Clock::time_point t)
+{
+    return std::chrono::duration<double, std::micro>(t - s->t0).count();
+}
+
+static void group_alloc(cgb_server* s, Group& G, int alg, uint32_t nslots)
+{
+    cgb_graph* g = s->g;
+    const uint32_t V = g->V;
+    G.alg = alg;
+    G.nslots = nslots;
+    for (uint32_t k = 0; k < kSrvSlots; k++) {
+        G.state[k] = SlotState::kFree;
+        G.req[k] = -1;
+        G.min_far[k] = kValueMax;
+    }
+    if (nslots == 0) return;
+    CGB_CUDA_TRY(cudaMalloc((void**)&G.region, (size_t)nslots * V * 4));
+    CGB_CUDA_TRY(cudaMalloc((void**)&G.d_stats, sizeof(SlotStats)));
+    CGB_CUDA_TRY(cudaMallocHost((void**)&G.h_stats, sizeof(SlotStats)));
+    CGB_CUDA_TRY(cudaMalloc((void**)&G.d_up, sizeof(SlotUpload)));
+    CGB_CUDA_TRY(cudaMallocHost((void**)&G.h_up, sizeof(SlotUpload)));
+    CGB_CUDA_TRY(cudaMemset(G.d_stats, 0, sizeof(SlotStats)));
+    CGB_CUDA_TRY(cudaMemset(G.d_up, 0, sizeof(SlotUpload)));
+    memset(G.h_stats, 0, sizeof(SlotStats));
+    memset(G.h_up, 0, sizeof(SlotUpload));
+    if (alg == CGB_BFS) {
+        G.stream = g->stream;  // the binned push expansion runs on the graph's stream
+        G.mb.seen = ms_alloc(V);
+        G.mb.front[0] = ms_alloc(V);
+        G.mb.front[1] = ms_alloc(V);
+        G.mb.next = ms_alloc(V);
+        CGB_CUDA_TRY(cudaMemset(G.mb.seen, 0, (size_t)V * 8));
+        CGB_CUDA_TRY(cudaMemset(G.mb.front[0], 0, (size_t)V * 8));
+        CGB_CUDA_TRY(cudaMemset(G.mb.front[1], 0, (size_t)V * 8));
+        CGB_CUDA_TRY(cudaMemset(G.mb.next, 0, (size_t)V * 8));
+        CGB_CUDA_TRY(cudaMalloc((void**)&G.q[0], (size_t)V * 4));
+        CGB_CUDA_TRY(cudaMalloc((void**)&G.q[1], (size_t)V * 4));
+        CGB_CUDA_TRY(cudaMalloc((void**)&G.touched, (size_t)V * 4));
+    } else {
+        CGB_CUDA_TRY(cudaStreamCreateWithFlags(&G.stream, cudaStreamNonBlocking));
+        G.sp = mssp_buffers_alloc(V, g->E);
+        CGB_CUDA_TRY(cudaMalloc((void**)&G.q[0], (size_t)V * 4));
+        CGB_CUDA_TRY(cudaMalloc((void**)&G.q[1], (size_t)V * 4));
+        CGB_CUDA_TRY(cudaMemset(G.sp->c, 0, sizeof(MsspCounters)));
+        CGB_CUDA_TRY(cudaMemset(G.sp->pend, 0, (size_t)V * 8));
+        CGB_CUDA_TRY(cudaMemset(G.sp->farm, 0, (size_t)V * 8));
+        k_ms_fill<<<kNumSMs * 8, kBlock>>>((uint64_t)V * kMsRoots, G.sp->dist, kValueMax);  // reused slots reset on admission
+        CGB_CUDA_TRY(cudaGetLastError());
+    }
+}
+
+static void group_free(cgb_server* s, Group& G)
+{
+    cudaFree(G.region);
+    cudaFree(G.d_stats);
+    if (G.h_stats) cudaFreeHost(G.h_stats);
+    cudaFree(G.d_up);
+    if (G.h_up) cudaFreeHost(G.h_up);
+    cudaFree(G.mb.seen);
+    cudaFree(G.mb.front[0]);
+    cudaFree(G.mb.front[1]);
+    cudaFree(G.mb.next);
+    cudaFree(G.q[0]);
+    cudaFree(G.q[1]);
+    cudaFree(G.touched);
+    if (G.sp) mssp_buffers_free(G.sp);
+    if (G.stream && G.stream != s->g->stream) cudaStreamDestroy(G.stream);
+    G = Group();
+}
+
+// ---- BFS group: issue one level for every active slot (no host sync)
+static void bfs_issue(cgb_server* s, Group& G)
+{
+    cgb_graph* g = s->g;
+    const uint32_t V = g->V;
+    cudaStream_t st = G.stream;
+    const uint32_t cur = G.cur, nxt = cur ^ 1;
+    if (!G.admit.empty()) {
+        unsigned long long reuse = 0;
+        uint32_t n = 0, qpos = G.nact;
+        for (auto& a : G.admit) {
+            const uint32_t k = a.first;
+            const SrvReq& R = s->reqs[a.second];
+            if (G.used[k]) reuse |= 1ull << k;
+            G.used[k] = true;
+            G.h_up->slots[n] = k;
+            G.h_up->roots[n] = R.info.root;
+            G.h_up->qidx[n] = R.info.root < g->nz ? qpos++ : 0xFFFFFFFFu;
+            G.h_up->start[k] = G.tick;
+            n++;
+        }
+        G.nact = qpos;
+        if (reuse)
+            k_srv_clear_bits<<<kNumSMs * 8, kBlock, 0, st>>>(V, G.mb.seen, reuse);
+        for (auto& a : G.admit)
+            k_ms_fill<<<kNumSMs * 4, kBlock, 0, st>>>((uint64_t)V, G.region + (size_t)a.first * V, kValueMax);
+        CGB_CUDA_TRY(cudaMemcpyAsync(G.d_up, G.h_up, sizeof(SlotUpload), cudaMemcpyHostToDevice, st));
+        k_srv_bfs_admit<<<1, kSrvSlots, 0, st>>>(n, G.d_up->slots, G.d_up->roots, G.d_up->qidx, V, G.region,
+                                                 G.mb.seen, G.mb.front[cur], G.q[cur]);
+    }
+    CGB_CUDA_TRY(cudaMemsetAsync(&G.d_stats->alive[0], 0, 8, st));
+    CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->qlen[nxt], 0, 4, st));
+    CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->medges, 0, 8, st));
+    CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->overflow, 0, 4, st));
+    if (G.nact == 0) return;
+    const uint32_t lvl = G.tick + 1;
+    const bool pull = (double)G.medges * 15.0 > (double)g->E;
+    if (pull) {
+        k_ms_bu<<<grid_for(V, kBlock, kNumSMs * 16), kBlock, 0, st>>>(
+            V, g->in_off, g->in_src, G.mb.front[cur], G.mb.seen, G.mb.front[nxt], G.active, G.region, lvl, g->nz,
+            G.q[nxt], &g->ctr->qlen[nxt], V, g->ctr, G.d_up->start, &G.d_stats->alive[0]);
+    } else {
+        CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->found, 0, 4, st));
+        CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->chunk_len, 0, 4, st));
+        MsTdOp op{g->off, g->dst, G.mb.front[cur], G.mb.seen, G.mb.next, G.touched, &g->ctr->found, V, g->ctr};
+        launch_push(g, G.q[cur], G.nact, op, false);
+        k_ms_finalize<<<kNumSMs * 8, kBlock, 0, st>>>(G.touched, 0, &g->ctr->found, G.mb.seen, G.mb.next,
+                                                     G.mb.front[nxt], G.region, V, lvl, g->nz, G.q[nxt],
+                                                     &g->ctr->qlen[nxt], V, g->ctr, G.d_up->start,
+                                                     &G.d_stats->alive[0]);
+    }
+    k_ms_clear<<<grid_for(G.nact, kBlock, kNumSMs * 8), kBlock, 0, st>>>(G.q[cur], G.nact, G.mb.front[cur]);
+    k_ms_degree_sum<<<kNumSMs * 4, kBlock, 0, st>>>(G.q[nxt], 0, &g->ctr->qlen[nxt], g->off, g->ctr);
+}
+
+// ---- SSSP group: admissions, per-slot bucket splits, one near round
+static void sp_issue(cgb_server* s, Group& G)
+{
+    cgb_graph* g = s->g;
+    const uint32_t V = g->V;
+    cudaStream_t st = G.stream;
+    MsspBuffers& b = *G.sp;
+    const uint32_t cur = G.cur, nxt = cur ^ 1;
+    unsigned long long admitted = 0;
+    if (!G.admit.empty()) {
+        unsigned long long reuse = 0;
+        uint32_t n = 0;
+        for (auto& a : G.admit) {
+            const uint32_t k = a.first;
+            if (G.used[k]) reuse |= 1ull << k;
+            G.used[k] = true;
+            admitted |= 1ull << k;
+            G.h_up->slots[n] = k;
+            G.h_up->roots[n] = s->reqs[a.second].info.root;
+            G.thr[k] = G.delta;
+            G.last_empty[k] = false;
+            G.min_far[k] = kValueMax;
+            n++;
+        }
+        if (reuse) k_srv_sp_reset<<<kNumSMs * 8, kBlock, 0, st>>>(V, b.dist, reuse);
+        for (uint32_t k = 0; k < kSrvSlots; k++) G.h_up->thr[k] = (uint32_t)std::min<uint64_t>(G.thr[k], 0xFFFFFFFFu);
+        CGB_CUDA_TRY(cudaMemcpyAsync(G.d_up, G.h_up, sizeof(SlotUpload), cudaMemcpyHostToDevice, st));
+        k_srv_sp_admit<<<1, kSrvSlots, 0, st>>>(n, G.d_up->slots, G.d_up->roots, b.dist, b.pend, G.q[cur],
+                                                &b.c->nq_in, V, b.c);
+    }
+    // slots whose near work ran out but which still have far pairs move to their next bucket
+    const unsigned long long adv = G.active & ~admitted & ~G.near_alive & G.far_alive;
+    G.split_mask = adv;
+    if (adv) {
+        for (uint32_t k = 0; k < kSrvSlots; k++) {
+            if (!((adv >> k) & 1ull)) continue;
+            uint64_t hi = G.thr[k] + G.delta;
+            if (G.last_empty[k] && G.min_far[k] != kValueMax)
+                hi = std::max<uint64_t>(hi, ((uint64_t)G.min_far[k] / G.delta + 1) * G.delta);
+            G.h_up->lo[k] = (uint32_t)std::min<uint64_t>(G.thr[k], 0xFFFFFFFFu);
+            G.h_up->hi[k] = (uint32_t)std::min<uint64_t>(hi, 0xFFFFFFFFu);
+            G.thr[k] = hi;
+            G.h_up->min_far[k] = kValueMax;
+        }
+        for (uint32_t k = 0; k < kSrvSlots; k++) G.h_up->thr[k] = (uint32_t)std::min<uint64_t>(G.thr[k], 0xFFFFFFFFu);
+        CGB_CUDA_TRY(cudaMemcpyAsync(G.d_up, G.h_up, sizeof(SlotUpload), cudaMemcpyHostToDevice, st));
+        CGB_CUDA_TRY(cudaMemcpyAsync(G.d_stats->min_far, G.h_up->min_far, sizeof(G.h_up->min_far),
+                                     cudaMemcpyHostToDevice, st));
+        CGB_CUDA_TRY(cudaMemsetAsync(&b.c->nfar_next, 0, 4, st));
+        CGB_CUDA_TRY(cudaMemsetAsync(&G.d_stats->alive[1], 0, 8, st));
+        k_mssp_split<<<kNumSMs * 8, kBlock, 0, st>>>(b.far_list[G.fcur], &b.c->nfar_live, b.dist, b.pend, b.farm,
+                                                     G.q[cur], &b.c->nq_in, b.far_list[G.fcur ^ 1], &b.c->nfar_next,
+                                                     V, 0, 0, G.d_up->lo, G.d_up->hi, adv, G.d_stats->min_far,
+                                                     &G.d_stats->alive[1], b.c);
+        k_srv_copy_u32<<<1, 1, 0, st>>>(&b.c->nfar_next, &b.c->nfar_live);
+        G.fcur ^= 1;
+    }
+    CGB_CUDA_TRY(cudaMemsetAsync(&G.d_stats->alive[0], 0, 8, st));
+    CGB_CUDA_TRY(cudaMemsetAsync(&b.c->nq_out, 0, 4, st));
+    CGB_CUDA_TRY(cudaMemsetAsync(&b.c->ndesc, 0, 4, st));
+    k_mssp_desc<<<kNumSMs * 8, kBlock, 0, st>>>(G.q[cur], &b.c->nq_in, g->off, b.pend, b.maskq, b.desc, b.desc_cap,
+                                                b.c);
+    mssp_expand(g->w != nullptr, kNumSMs * 8, st, b.desc, b.c, b.maskq, g->dst, g->w, b.dist, b.pend, b.farm,
+                G.q[nxt], &b.c->nq_out, b.far_list[G.fcur], &b.c->nfar_live, V, 0, G.d_up->thr, G.d_stats->alive);
+    k_srv_copy_u32<<<1, 1, 0, st>>>(&b.c->nq_out, &b.c->nq_in);
+    CGB_CUDA_TRY(cudaMemcpyAsync(&G.h_stats->alive, &G.d_stats->alive, sizeof(G.h_stats->alive),
+                                 cudaMemcpyDeviceToHost, st));
+    CGB_CUDA_TRY(cudaMemcpyAsync(G.h_stats->min_far, G.d_stats->min_far, sizeof(G.h_stats->min_far),
+                                 cudaMemcpyDeviceToHost, st));
+    CGB_CUDA_TRY(cudaMemcpyAsync(b.h, b.c, sizeof(MsspCounters), cudaMemcpyDeviceToHost, st));
+}
+
+// After the tick's kernels completed: slots whose traversal ended.
+static unsigned long long group_finished(cgb_server* s, Group& G)
+{
+    cgb_graph* g = s->g;
+    if (G.alg == CGB_BFS) {
+        G.nact = g->h_ctr->qlen[G.cur ^ 1];
+        G.medges = g->h_ctr->medges;
+        CGB_REQUIRE(!g->h_ctr->overflow, CGB_EOVERFLOW, "server BFS queue overflow");
+        const unsigned long long alive = G.h_stats->alive[0];
+        G.cur ^= 1;
+        G.tick++;
+        return G.active & ~alive;
+    }
+    CGB_REQUIRE(!G.sp->h->overflow, CGB_EOVERFLOW, "server SSSP queue overflow");
+    G.near_alive = G.h_stats->alive[0];
+    G.far_alive = G.h_stats->alive[1];
+    for (uint32_t k = 0; k < kSrvSlots; k++) {
+        if (!((G.split_mask >> k) & 1ull)) continue;
+        G.min_far[k] = G.h_stats->min_far[k];
+        G.last_empty[k] = !((G.near_alive >> k) & 1ull);
+    }
+    G.cur ^= 1;
+    G.tick++;
+    return G.active & ~(G.near_alive | G.far_alive);
+}
+
+// Results of the finished slots: statistics, copy to the request's buffer.
+static void group_retire(cgb_server* s, Group& G, unsigned long long fin)
+{
+    if (!fin) return;
+    cgb_graph* g = s->g;
+    const uint32_t V = g->V;
+    cudaStream_t st = G.stream;
+    if (G.alg == CGB_SSSP)
+        k_srv_sp_extract<<<kNumSMs * 8, kBlock, 0, st>>>(G.sp->dist, V, fin, G.region);
+    CGB_CUDA_TRY(cudaMemsetAsync(G.d_stats, 0, offsetof(SlotStats, alive), st));
+    k_srv_stats<<<kNumSMs * 4, kBlock, 0, st>>>(G.region, V, g->off, fin, G.d_stats->edges, G.d_stats->reached,
+                                                G.d_stats->depth);
+    for (unsigned long long m = fin; m; m &= m - 1) {
+        const uint32_t k = __builtin_ctzll(m);
+        SrvReq& R = s->reqs[G.req[k]];
+        if (R.out)
+            CGB_CUDA_TRY(cudaMemcpyAsync(R.out, G.region + (size_t)k * V, (size_t)V * 4, cudaMemcpyDefault, st));
+    }
+    CGB_CUDA_TRY(cudaMemcpyAsync(G.h_stats, G.d_stats, offsetof(SlotStats, alive), cudaMemcpyDeviceToHost, st));
+    CGB_CUDA_TRY(cudaStreamSynchronize(st));
+    const double now = us_since(s, Clock::now());
+    std::lock_guard<std::mutex> lk(s->mu);
+    for (unsigned long long m = fin; m; m &= m - 1) {
+        const uint32_t k = __builtin_ctzll(m);
+        SrvReq& R = s->reqs[G.req[k]];
+        R.info.traversed_edges = G.h_stats->edges[k];
+        R.info.reached = G.h_stats->reached[k];
+        R.info.depth = G.h_stats->depth[k];
+        R.info.done_us = now;
+        R.info.status = CGB_OK;
+        s->done.push_back(R.info);
+        s->completed++;
+        G.state[k] = SlotState::kFree;
+        G.req[k] = -1;
+    }
+    G.active &= ~fin;
+    s->cv.notify_all();
+}
+
+// Pairs free slots with requests whose arrival time has passed.
+static void pick_admissions(cgb_server* s, Group& G, std::deque<int64_t>& waiting, double now_us)
+{
+    G.admit.clear();
+    uint32_t k = 0;
+    while (!waiting.empty()) {
+        SrvReq& R = s->reqs[waiting.front()];
+        if (R.info.arrival_us > now_us) break;
+        while (k < G.nslots && G.state[k] != SlotState::kFree) k++;
+        if (k >= G.nslots) break;
+        G.state[k] = SlotState::kActive;
+        G.req[k] = waiting.front();
+        G.active |= 1ull << k;
+        R.info.slot = k;
+        R.info.admit_us = now_us;
+        G.admit.push_back({k, waiting.front()});
+        waiting.pop_front();
+    }
+}
+
+static void server_loop(cgb_server* s)
+{
+    cgb_graph* g = s->g;
+    try {
+        CGB_CUDA_TRY(cudaSetDevice(g->device));
+        while (!s->stop.load()) {
+            double next_arrival = -1;
+            {
+                std::unique_lock<std::mutex> lk(s->mu);
+                const double now = us_since(s, Clock::now());
+                for (int a = 0; a < 2; a++) pick_admissions(s, s->grp[a], s->waiting[a], now);
+                const bool work = s->grp[0].active || s->grp[1].active;
+                if (!work) {
+                    for (int a = 0; a < 2; a++)
+                        if (!s->waiting[a].empty()) {
+                            const double t = s->reqs[s->waiting[a].front()].info.arrival_us;
+                            if (next_arrival < 0 || t < next_arrival) next_arrival = t;
+                        }
+                    if (next_arrival < 0)
+                        s->cv.wait_for(lk, std::chrono::milliseconds(5));
+                    else if (next_arrival > now)
+                        s->cv.wait_for(lk, std::chrono::microseconds((int64_t)(next_arrival - now) + 1));
+                    continue;
+                }
+            }
+            const auto t_tick = Clock::now();
+            std::lock_guard<std::mutex> glk(g->mu);
+            Group& B = s->grp[0];
+            Group& S = s->grp[1];
+            if (B.active) {
+                bfs_issue(s, B);
+                CGB_CUDA_TRY(cudaMemcpyAsync(B.h_stats->alive, B.d_stats->alive, sizeof(B.h_stats->alive),
+                                             cudaMemcpyDeviceToHost, B.stream));
+                CGB_CUDA_TRY(cudaMemcpyAsync(g->h_ctr, g->ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, B.stream));
+            }
+            if (S.active) sp_issue(s, S);
+            if (B.active) CGB_CUDA_TRY(cudaStreamSynchronize(B.stream));
+            if (S.active) CGB_CUDA_TRY(cudaStreamSynchronize(S.stream));
+            const unsigned long long fb = B.active ? group_finished(s, B) : 0;
+            const unsigned long long fs = S.active ? group_finished(s, S) : 0;
+            group_retire(s, B, fb);
+            group_retire(s, S, fs);
+            s->ticks++;
+            s->busy_ms += std::chrono::duration<double, std::milli>(Clock::now() - t_tick).count();
+        }
+    } catch (const Error& e) {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->error = e.code;
+        s->error_msg = e.msg;
+    } catch (const std::exception& e) {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->error = CGB_ECUDA;
+        s->error_msg = e.what();
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->error != CGB_OK) {
+        // requests still admitted or waiting end with the error
+        for (auto& R : s->reqs)
+            if (R.info.done_us == 0 && R.info.status == CGB_OK) {
+                R.info.status = s->error;
+                R.info.done_us = us_since(s, Clock::now());
+                s->done.push_back(R.info);
+                s->completed++;
+            }
+        for (int a = 0; a < 2; a++) s->waiting[a].clear();
+    }
+    s->cv.notify_all();
+}
+
+}  // namespace cgb
+
+template <typename F>
+static cgb_status sguard(F&& f)
+{
+    try {
+        f();
+        return CGB_OK;
+    } catch (const Error& e) {
+        set_error(e.msg);
+        return e.code;
+    } catch (const std::exception& e) {
+        set_error(e.what());
+        return CGB_ECUDA;
+    }
+}
+
+extern "C" {
+
+cgb_status cgb_server_create(cgb_graph* g, const cgb_server_config* cfg, cgb_server** out)
+{
+    return sguard([&] {
+        CGB_REQUIRE(g != nullptr && out != nullptr, CGB_EINVAL, "NULL argument");
+        *out = nullptr;
+        cgb_server_config c{};
+        c.struct_size = sizeof(c);
+        if (cfg) {
+            CGB_REQUIRE(cfg->struct_size >= sizeof(c), CGB_EINVAL, "cgb_server_config.struct_size too small");
+            c = *cfg;
+        }
+        uint32_t nb = c.bfs_slots ? std::min(c.bfs_slots, kSrvSlots) : kSrvSlots;
+        uint32_t ns = c.sssp_slots ? std::min(c.sssp_slots, kSrvSlots) : kSrvSlots;
+        if (c.flags & CGB_SERVER_NO_BFS) nb = 0;
+        if (c.flags & CGB_SERVER_NO_SSSP) ns = 0;
+        const uint64_t per_slot = 4ull * g->V;  // one result region per slot
+        if (c.memory_budget) {
+            const uint64_t fit = c.memory_budget / per_slot;
+            CGB_REQUIRE(fit >= (uint64_t)((nb ? 1 : 0) + (ns ? 1 : 0)), CGB_ENOMEM,
+                        "memory budget holds no result region");
+            // split the regions that fit between the groups in proportion to their slot requests
+            while ((uint64_t)nb + ns > fit) {
+                if (nb >= ns && nb > 1) nb--;
+                else if (ns > 1) ns--;
+                else break;
+            }
+        }
+        std::lock_guard<std::mutex> lock(g->mu);
+        CGB_CUDA_TRY(cudaSetDevice(g->device));
+        ensure_frontier(g);
+        if (nb) ensure_csc(g);
+        if (ns && g->w && g->sum_w == 0) compute_weight_sum(g);
+        cgb_server* s = new cgb_server();
+        s->g = g;
+        try {
+            group_alloc(s, s->grp[0], CGB_BFS, nb);
+            group_alloc(s, s->grp[1], CGB_SSSP, ns);
+            s->grp[1].delta = c.sssp_delta ? c.sssp_delta : sssp_default_delta(g);
+            CGB_CUDA_TRY(cudaDeviceSynchronize());
+        } catch (...) {
+            group_free(s, s->grp[0]);
+            group_free(s, s->grp[1]);
+            delete s;
+            throw;
+        }
+        *out = s;
+    });
+}
+
+cgb_status cgb_server_submit(cgb_server* s, int algorithm, uint32_t root, double arrival_us, uint32_t* out_u32,
+                             uint64_t* id)
+{
+    return sguard([&] {
+        CGB_REQUIRE(s != nullptr, CGB_EINVAL, "server is NULL");
+        CGB_REQUIRE(algorithm == CGB_BFS || algorithm == CGB_SSSP, CGB_EINVAL, "server requests are BFS or SSSP");
+        CGB_REQUIRE(root < s->g->V, CGB_EINVAL, "root >= vertexNum");
+        const int a = algorithm == CGB_BFS ? 0 : 1;
+        CGB_REQUIRE(s->grp[a].nslots > 0, CGB_EUNSUPPORTED, "server has no slots for this algorithm");
+        std::lock_guard<std::mutex> lk(s->mu);
+        CGB_REQUIRE(s->error == CGB_OK, s->error, "server stopped after an error");
+        SrvReq R;
+        R.info.id = s->reqs.size();
+        R.info.algorithm = algorithm;
+        R.info.root = root;
+        R.info.arrival_us = arrival_us;
+        R.info.status = CGB_OK;
+        R.out = out_u32;
+        // keep each queue ordered by arrival time
+        auto& wq = s->waiting[a];
+        s->reqs.push_back(R);
+        const int64_t idx = (int64_t)s->reqs.size() - 1;
+        auto it = wq.end();
+        while (it != wq.begin() && s->reqs[*(it - 1)].info.arrival_us > arrival_us) --it;
+        wq.insert(it, idx);
+        if (id) *id = R.info.id;
+        s->cv.notify_all();
+    });
+}
+
+cgb_status cgb_server_start(cgb_server* s)
+{
+    return sguard([&] {
+        CGB_REQUIRE(s != nullptr, CGB_EINVAL, "server is NULL");
+        CGB_REQUIRE(!s->started, CGB_EINVAL, "server already started");
+        s->t0 = Clock::now();
+        s->started = true;
+        s->th = std::thread(server_loop, s);
+    });
+}
+
+cgb_status cgb_server_wait(cgb_server* s, double timeout_ms, uint32_t* pending)
+{
+    return sguard([&] {
+        CGB_REQUIRE(s != nullptr, CGB_EINVAL, "server is NULL");
+        std::unique_lock<std::mutex> lk(s->mu);
+        const auto until = Clock::now() + std::chrono::microseconds((int64_t)(timeout_ms * 1000.0));
+        while (s->completed < s->reqs.size() && s->error == CGB_OK) {
+            if (s->cv.wait_until(lk, until) == std::cv_status::timeout) break;
+        }
+        if (pending) *pending = (uint32_t)(s->reqs.size() - s->completed);
+        CGB_REQUIRE(s->error == CGB_OK, s->error, s->error_msg);
+    });
+}
+
+cgb_status cgb_server_poll(cgb_server* s, cgb_request_info* out, uint32_t cap, uint32_t* n)
+{
+    return sguard([&] {
+        CGB_REQUIRE(s != nullptr && n != nullptr, CGB_EINVAL, "NULL argument");
+        std::lock_guard<std::mutex> lk(s->mu);
+        const uint32_t k = (uint32_t)std::min<size_t>(cap, s->done.size());
+        if (out) {
+            std::copy(s->done.begin(), s->done.begin() + k, out);
+            s->done.erase(s->done.begin(), s->done.begin() + k);
+        }
+        *n = out ? k : (uint32_t)s->done.size();
+    });
+}
+
+cgb_status cgb_server_stats(const cgb_server* s, uint64_t* ticks, uint32_t* bfs_slots, uint32_t* sssp_slots,
+                            double* busy_ms)
+{
+    return sguard([&] {
+        CGB_REQUIRE(s != nullptr, CGB_EINVAL, "server is NULL");
+        if (ticks) *ticks = s->ticks;
+        if (bfs_slots) *bfs_slots = s->grp[0].nslots;
+        if (sssp_slots) *sssp_slots = s->grp[1].nslots;
+        if (busy_ms) *busy_ms = s->busy_ms;
+    });
+}
+
+cgb_status cgb_server_destroy(cgb_server* s)
+{
+    return sguard([&] {
+        if (!s) return;
+        s->stop.store(true);
+        s->cv.notify_all();
+        if (s->th.joinable()) s->th.join();
+        cudaSetDevice(s->g->device);
+        group_free(s, s->grp[0]);
+        group_free(s, s->grp[1]);
+        delete s;
+    });
+}
+
+}  // extern "C"

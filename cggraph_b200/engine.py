@@ -365,6 +365,82 @@ class Batch:
             pass
 
 
+class Server:
+    """Continuous-batching request server on one resident graph (no
+    counterpart in the reference, whose drivers run one root at a time).
+
+    ``submit(alg, root, arrival_us, out)`` queues a BFS or SSSP query that
+    becomes eligible ``arrival_us`` after ``start()``; admitted queries of an
+    algorithm share each traversal (up to 64 per algorithm, capped by
+    ``memory_budget`` bytes of result regions), and a finished query's slot
+    goes to the next arrival.  ``wait()`` blocks until all have ended;
+    ``poll()`` returns their records (times in microseconds from start).
+    Each result equals ``Graph.run`` of the same query.
+    """
+
+    def __init__(self, graph: "Graph", bfs_slots: int = 0, sssp_slots: int = 0, sssp_delta: int = 0,
+                 memory_budget: int = 0, flags: int = 0):
+        cfg = L.ServerConfig()
+        cfg.struct_size = ctypes.sizeof(L.ServerConfig)
+        cfg.bfs_slots, cfg.sssp_slots, cfg.sssp_delta = bfs_slots, sssp_slots, sssp_delta
+        cfg.memory_budget, cfg.flags = memory_budget, flags
+        self._h = ctypes.c_void_p()
+        self._graph = graph  # the server borrows the graph
+        check(L.lib().cgb_server_create(graph._h, ctypes.byref(cfg), ctypes.byref(self._h)))
+        self._outs = {}
+
+    def submit(self, algorithm: int, root: int, arrival_us: float = 0.0, out=None) -> int:
+        rid = ctypes.c_uint64()
+        check(L.lib().cgb_server_submit(self._h, int(algorithm), int(root), float(arrival_us), _ptr(out),
+                                        ctypes.byref(rid)))
+        if out is not None:
+            self._outs[rid.value] = out
+        return rid.value
+
+    def start(self) -> None:
+        check(L.lib().cgb_server_start(self._h))
+
+    def wait(self, timeout_ms: float = 600000.0) -> int:
+        pending = ctypes.c_uint32()
+        check(L.lib().cgb_server_wait(self._h, float(timeout_ms), ctypes.byref(pending)))
+        return pending.value
+
+    def poll(self):
+        n = ctypes.c_uint32()
+        check(L.lib().cgb_server_poll(self._h, None, 0, ctypes.byref(n)))
+        arr = (L.RequestInfo * max(1, n.value))()
+        check(L.lib().cgb_server_poll(self._h, arr, n.value, ctypes.byref(n)))
+        recs = []
+        for i in range(n.value):
+            r = arr[i]
+            recs.append({f: getattr(r, f) for f, _ in L.RequestInfo._fields_})
+            self._outs.pop(r.id, None)
+        return recs
+
+    def stats(self):
+        t, b, s_, busy = ctypes.c_uint64(), ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_double()
+        check(L.lib().cgb_server_stats(self._h, ctypes.byref(t), ctypes.byref(b), ctypes.byref(s_),
+                                       ctypes.byref(busy)))
+        return {"ticks": t.value, "bfs_slots": b.value, "sssp_slots": s_.value, "busy_ms": busy.value}
+
+    def close(self) -> None:
+        if self._h is not None and self._h.value:
+            check(L.lib().cgb_server_destroy(self._h))
+        self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class GraphB200:
     """Drop-in for ``GraphDeviceWorklist`` (my_project/CGgraph/GraphDevice.cuh:9-269).
 

@@ -217,6 +217,64 @@ cgb_status cgb_batch_run(cgb_batch* b, int algorithm, const uint32_t* roots, uin
 cgb_status cgb_batch_info(const cgb_batch* b, uint32_t* total_vertices, uint32_t* total_edges, int32_t* one_launch);
 cgb_status cgb_batch_stats(const cgb_batch* b, cgb_run_stats* out);
 
+/* ----------------------------------------------------------- serving */
+
+/* A request server on one resident graph (no counterpart in the reference,
+ * whose drivers run one root at a time): BFS and SSSP root queries are
+ * admitted as they arrive into up to 64 slots per algorithm, and all
+ * admitted queries of an algorithm advance together, one level / round per
+ * tick, sharing each edge traversal through bit-packed per-vertex masks;
+ * a query that ends frees its slot for the next arrival (continuous
+ * batching).  Each result equals a lone cgb_run of the same query. */
+typedef struct cgb_server cgb_server;
+
+typedef struct {
+    uint32_t struct_size;    /* sizeof(cgb_server_config) */
+    uint32_t bfs_slots;      /* concurrent BFS queries, <= 64 (0 = 64) */
+    uint32_t sssp_slots;     /* concurrent SSSP queries, <= 64 (0 = 64) */
+    uint32_t sssp_delta;     /* bucket width, 0 = the cgb_run default */
+    uint64_t memory_budget;  /* bytes for per-query result regions (4 * V each); slots are
+                                capped to fit; 0 = no cap */
+    uint32_t flags;          /* CGB_SERVER_* */
+    uint32_t reserved[5];
+} cgb_server_config;
+
+#define CGB_SERVER_NO_BFS 0x1u  /* no BFS slots (saves their masks) */
+#define CGB_SERVER_NO_SSSP 0x2u /* no SSSP slots (saves the 256 B per vertex of distances) */
+
+typedef struct {
+    uint64_t id;
+    int32_t algorithm;
+    uint32_t root;
+    double arrival_us;        /* times relative to cgb_server_start */
+    double admit_us;
+    double done_us;           /* result complete (and copied to out_u32) */
+    uint64_t traversed_edges; /* out-degrees of the reached vertices */
+    uint32_t reached;         /* vertices with a finite result */
+    uint32_t depth;           /* BFS: deepest level; SSSP: largest finite distance */
+    int32_t status;           /* CGB_OK or the error that ended the query */
+    uint32_t slot;
+} cgb_request_info;
+
+cgb_status cgb_server_create(cgb_graph* g, const cgb_server_config* cfg, cgb_server** out);
+/* Queues a query that becomes eligible arrival_us after cgb_server_start
+ * (past times: at once).  out_u32 (host or device, V entries, or NULL)
+ * receives the result when the query ends; it must stay valid until then. */
+cgb_status cgb_server_submit(cgb_server* s, int algorithm, uint32_t root, double arrival_us, uint32_t* out_u32,
+                             uint64_t* id);
+/* Starts the clock and the serving thread. */
+cgb_status cgb_server_start(cgb_server* s);
+/* Waits until every submitted query has ended or timeout_ms passed;
+ * pending receives the number still open. */
+cgb_status cgb_server_wait(cgb_server* s, double timeout_ms, uint32_t* pending);
+/* Moves up to cap records of ended queries into out (out NULL: n = how many
+ * are waiting). */
+cgb_status cgb_server_poll(cgb_server* s, cgb_request_info* out, uint32_t cap, uint32_t* n);
+cgb_status cgb_server_stats(const cgb_server* s, uint64_t* ticks, uint32_t* bfs_slots, uint32_t* sssp_slots,
+                            double* busy_ms);
+/* Stops the serving thread and frees the server (the graph stays). */
+cgb_status cgb_server_destroy(cgb_server* s);
+
 /* --------------------------------------------------- allocation-free BFS */
 
 /* Largest vertex count cgb_bfs_noalloc accepts. */

@@ -98,3 +98,28 @@ int main() {
                            "-lcgb200", f"-Wl,-rpath,{libdir}", "-o", str(exe)])
     out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120).stdout.strip()
     assert out in ("0 5 12", "status 5"), out
+
+
+def test_struct_layouts_match_header(tmp_path):
+    """The ctypes mirrors of the public structs have the C header's sizes
+    and field offsets."""
+    import subprocess
+    from cggraph_b200 import _lib
+    structs = {"cgb_options": _lib.Options, "cgb_run_stats": _lib.RunStats, "cgb_iter_trace": _lib.IterTrace,
+               "cgb_server_config": _lib.ServerConfig, "cgb_request_info": _lib.RequestInfo}
+    lines = ['#include "cgb200.h"', "#include <stdio.h>", "#include <stddef.h>", "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
+        for f, _ in py._fields_:
+            lines.append(f'printf("{cname}.{f} %zu\\n", offsetof({cname}, {f}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = dict(line.rsplit(" ", 1) for line in subprocess.run([str(exe)], check=True, capture_output=True,
+                                                              text=True).stdout.split("\n") if line)
+    for cname, py in structs.items():
+        assert int(got[cname]) == ctypes.sizeof(py), cname
+        for f, _ in py._fields_:
+            assert int(got[f"{cname}.{f}"]) == getattr(py, f).offset, f"{cname}.{f}"
