@@ -58,6 +58,10 @@ def parse_args():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=0, help="0 = same as --steps")
+    p.add_argument("--no-batching", action="store_true", help="skip the multi-root and graph-batch section")
+    p.add_argument("--no-serving", action="store_true", help="skip the request-server section")
+    p.add_argument("--serve-scale", type=int, default=25, help="RMAT scale of the served graph")
+    p.add_argument("--serve-requests", type=int, default=256, help="queries per arrival rate")
     p.add_argument("--algorithms", default="bfs,sssp,cc,pr",
                    help="comma list of bfs,sssp,cc,pr run in each step (default: all four)")
     return p.parse_args()
@@ -294,10 +298,17 @@ def bench_cgb200(args, d: Dist):
         except Exception as e:  # reported, not fatal
             cpu = {"value": None, "error": str(e)[-300:]}
 
+    batching = None
+    if d.world == 1 and not args.no_batching and (BFS in algs or SSSP in algs):
+        batching = bench_batching(args, cg, L, gd, roots, dev)
+
     for g in (gd, gs):
         if g is not None:
             g.set_stream(None)
             g.close()
+    serving = None
+    if d.world == 1 and not args.no_serving and (BFS in algs or SSSP in algs):
+        serving = bench_serving(args, cg, L, dev)
     result = {
         "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": d.world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -314,6 +325,8 @@ def bench_cgb200(args, d: Dist):
                    "parallelism": f"replicas x{d.world}"},
         "per_algorithm": per_alg,
         "schedules": schedules,
+        "batching": batching,
+        "serving": serving,
         "roofline": roof,
         "cpu_baseline": cpu,
         "e2e": e2e,
@@ -370,6 +383,114 @@ def compare_schedules(args, cg, L, gd, roots, dev):
                 g.close()
     finally:
         policy.load(None)
+    return out
+
+
+def bench_batching(args, cg, L, gd, roots, dev):
+    """Batching: 64 BFS and 64 SSSP roots on the benchmark graph in
+    multi-root passes (bit-packed per-vertex root masks) against one run per
+    root; and 256 uneven graphs (RMAT scales 10-16, grids 32x32 to 512x512)
+    as one disjoint-union graph, BFS/SSSP from one root per graph in one
+    captured launch, against one run per graph.  Results are identical
+    (tests); only time differs."""
+    import torch
+    out = {}
+    V = gd.vertexNum
+    off_h, _, _ = gd.download(with_weight=False)
+    rts = pick_roots(off_h, args.seed + 7, 64)
+    d_out = torch.empty((64, V), dtype=torch.int32, device=f"cuda:{dev}")
+    seq = cg.make_options(flags=L.FLAG_BATCH_SEQUENTIAL)
+    for alg, an in ((BFS, "bfs"), (SSSP, "sssp")):
+        gd.run_batch(alg, rts, out=d_out)  # warm-up
+        _, ms_multi = gd.run_batch(alg, rts, out=d_out)
+        edges = gd.stats().traversed_edges
+        _, ms_seq = gd.run_batch(alg, rts, seq, out=d_out)
+        out[f"roots64_{an}"] = {"multi_ms": ms_multi, "one_by_one_ms": ms_seq, "multi_gteps": edges / ms_multi / 1e6,
+                                "one_by_one_gteps": edges / ms_seq / 1e6, "speedup": ms_seq / ms_multi}
+    # 256 uneven graphs
+    rng = np.random.default_rng(args.seed + 11)
+    graphs = []
+    for i in range(256):
+        if i % 2 == 0:
+            h = cg.Graph.rmat(int(rng.integers(10, 17)), 16, seed=1000 + i, wmax=64, device=dev)
+        else:
+            side = int(rng.integers(32, 513))
+            h = cg.Graph.grid(side, side, seed=1000 + i, device=dev)
+        graphs.append(h)
+    csrs = [h.download() for h in graphs]
+    roots_b = [int(rng.integers(0, o.size - 1)) for o, _, _ in csrs]
+    with cg.Batch(csrs, device=dev) as b:
+        tv, te, _ = b.info()
+        res = {"graphs": 256, "vertices": tv, "edges": te}
+        for alg, an in ((BFS, "bfs"), (SSSP, "sssp")):
+            b.run(alg, roots_b)  # first run captures the CUDA graph
+            _, ms_b = b.run(alg, roots_b)
+            edges = b.stats().traversed_edges
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ms_one = 0.0
+            for h, r in zip(graphs, roots_b):
+                h.run(alg, r, to_host=False)
+                ms_one += h.stats().ms
+            torch.cuda.synchronize()
+            wall_one = (time.perf_counter() - t0) * 1e3
+            res[an] = {"batch_ms": ms_b, "one_by_one_device_ms": ms_one, "one_by_one_wall_ms": wall_one,
+                       "batch_gteps": edges / ms_b / 1e6, "one_by_one_gteps": edges / wall_one / 1e6,
+                       "speedup_vs_wall": wall_one / ms_b}
+        res["captured"] = b.info()[2]
+        out["graphs256"] = res
+    for h in graphs:
+        h.close()
+    return out
+
+
+def bench_serving(args, cg, L, dev):
+    """Serving: BFS/SSSP queries (half each, seeded uniform non-isolated
+    roots) with Poisson arrivals at 1k, 5k and 20k req/s against a resident
+    RMAT graph (scale --serve-scale, weights [1,64]), and at 1k req/s against
+    the 4800 x 5000 grid (weights [1,1000]); latency = completion - arrival."""
+    out = {}
+    cases = [(f"rmat{args.serve_scale}", lambda: cg.Graph.rmat(args.serve_scale, 16, args.seed + 3, wmax=64,
+                                                                   device=dev), (1000, 5000, 20000),
+              args.serve_requests)]
+    if args.serve_scale >= 20:
+        cases.append(("grid4800x5000", lambda: cg.Graph.grid(4800, 5000, seed=1, device=dev), (1000,),
+                      max(64, args.serve_requests // 2)))
+    for name, make, rates, nreq in cases:
+        g = make()
+        off_h, _, _ = g.download(with_weight=False)
+        deg = np.diff(off_h.astype(np.int64))
+        nzv = np.nonzero(deg)[0]
+        res = {"vertices": g.vertexNum, "edges": g.edgeNum, "requests_per_rate": nreq}
+        with cg.Server(g) as srv:
+            st = srv.stats()
+            res["slots"] = {"bfs": st["bfs_slots"], "sssp": st["sssp_slots"]}
+        for rate in rates:
+            rng = np.random.default_rng(args.seed * 1000 + rate)
+            arrivals = np.cumsum(rng.exponential(1e6 / rate, nreq))
+            algs_q = rng.integers(0, 2, nreq)
+            roots_q = nzv[rng.integers(0, nzv.size, nreq)]
+            with cg.Server(g) as srv:
+                for a, r, t in zip(algs_q, roots_q, arrivals):
+                    srv.submit(int(a), int(r), float(t))
+                srv.start()
+                srv.wait(600000)
+                recs = srv.poll()
+                sst = srv.stats()
+            lat = np.array([r["done_us"] - r["arrival_us"] for r in recs]) / 1e3
+            makespan = (max(r["done_us"] for r in recs) - min(r["arrival_us"] for r in recs)) / 1e6
+            edges = sum(r["traversed_edges"] for r in recs)
+            per = {}
+            for a, an in ((BFS, "bfs"), (SSSP, "sssp")):
+                la = np.array([r["done_us"] - r["arrival_us"] for r in recs if r["algorithm"] == a]) / 1e3
+                if la.size:
+                    per[an] = {"p50_ms": float(np.percentile(la, 50)), "p99_ms": float(np.percentile(la, 99))}
+            res[f"rate{rate}"] = {"completed": len(recs), "errors": sum(1 for r in recs if r["status"] != 0),
+                                  "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                                  "throughput_req_s": len(recs) / makespan, "gteps": edges / makespan / 1e9,
+                                  "ticks": sst["ticks"], "per_algorithm": per}
+        g.close()
+        out[name] = res
     return out
 
 

@@ -652,7 +652,7 @@ cgb_status cgb_server_create(cgb_graph* g, const cgb_server_config* cfg, cgb_ser
         try {
             group_alloc(s, s->grp[0], CGB_BFS, nb);
             group_alloc(s, s->grp[1], CGB_SSSP, ns);
-            s->grp[1].delta = c.sssp_delta ? c.sssp_delta : sssp_default_delta(g);
+            s->grp[1].delta = c.sssp_delta ? c.sssp_delta : mssp_default_delta(g);
             CGB_CUDA_TRY(cudaDeviceSynchronize());
         } catch (...) {
             group_free(s, s->grp[0]);

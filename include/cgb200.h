@@ -68,7 +68,7 @@ typedef struct cgb_options {
     uint32_t struct_size;   /* sizeof(cgb_options); 0 = all defaults */
     int32_t schedule;       /* cgb_schedule */
     int32_t variant;        /* cgb_variant, for CGB_SCHED_FIXED */
-    uint32_t sssp_delta;    /* 0 = heuristic (mean weight * 32 / mean degree) */
+    uint32_t sssp_delta;    /* 0 = heuristic: 8 * mean weight / mean degree (x8 for multi-root passes) */
     double bfs_alpha;       /* Beamer alpha, 0 = 15 */
     double bfs_beta;        /* Beamer beta, 0 = 18 */
     uint64_t max_iterations;/* 0 = unlimited (V + 1 levels bound BFS anyway) */
@@ -232,7 +232,7 @@ typedef struct {
     uint32_t struct_size;    /* sizeof(cgb_server_config) */
     uint32_t bfs_slots;      /* concurrent BFS queries, <= 64 (0 = 64) */
     uint32_t sssp_slots;     /* concurrent SSSP queries, <= 64 (0 = 64) */
-    uint32_t sssp_delta;     /* bucket width, 0 = the cgb_run default */
+    uint32_t sssp_delta;     /* bucket width, 0 = the multi-root default of cgb_run_batch */
     uint64_t memory_budget;  /* bytes for per-query result regions (4 * V each); slots are
                                 capped to fit; 0 = no cap */
     uint32_t flags;          /* CGB_SERVER_* */
