@@ -33,7 +33,8 @@ EXPORTS = [
     "cgb_graph_download", "cgb_bfs_noalloc", "cgb_policy_load", "cgb_policy_collect", "cgb_policy_train",
     "cgb_policy_forward", "cgb_policy_loss_grad", "cgb_batch_create", "cgb_batch_destroy", "cgb_batch_run",
     "cgb_batch_info", "cgb_batch_stats", "cgb_server_create", "cgb_server_submit", "cgb_server_start",
-    "cgb_server_wait", "cgb_server_poll", "cgb_server_stats", "cgb_server_destroy",
+    "cgb_server_wait", "cgb_server_poll", "cgb_server_stats", "cgb_server_destroy", "cgb_tuning_get",
+    "cgb_tuning_set", "cgb_autotune",
 ]
 POLICY_FEATURES, POLICY_OUTPUTS, POLICY_PARAMS = 24, 9, 6345
 
@@ -93,6 +94,23 @@ class CgbError(RuntimeError):
 
 
 _lib = None
+
+class Tuning(ctypes.Structure):
+    _fields_ = [
+        ("struct_size", ctypes.c_uint32),
+        ("push_big_deg", ctypes.c_uint32),
+        ("push_chunk", ctypes.c_uint32),
+        ("push_ctas_per_sm", ctypes.c_uint32),
+        ("persist_enter", ctypes.c_uint32),
+        ("persist_deg", ctypes.c_uint32),
+        ("ms_edges", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 9),
+    ]
+
+
+TUNE_BATCH, TUNE_KEEP_DEFAULT = 0x1, 0x2
+TUNING_FIELDS = ("push_big_deg", "push_chunk", "push_ctas_per_sm", "persist_enter", "persist_deg", "ms_edges")
+
 
 class ServerConfig(ctypes.Structure):
     _fields_ = [
@@ -180,6 +198,10 @@ def lib() -> ctypes.CDLL:
         L.cgb_server_stats.argtypes = [_P, ctypes.POINTER(ctypes.c_uint64), _u32p, _u32p,
                                        ctypes.POINTER(ctypes.c_double)]
         L.cgb_server_destroy.argtypes = [_P]
+        L.cgb_tuning_get.argtypes = [_P, ctypes.POINTER(Tuning)]
+        L.cgb_tuning_set.argtypes = [_P, ctypes.POINTER(Tuning)]
+        L.cgb_autotune.argtypes = [_P, i, _P, u32, u32, ctypes.POINTER(Tuning), ctypes.POINTER(ctypes.c_double),
+                                   ctypes.POINTER(ctypes.c_double)]
         for name in EXPORTS:
             f = getattr(L, name)
             if name not in ("cgb_last_error_string", "cgb_status_string", "cgb_abi_version"):

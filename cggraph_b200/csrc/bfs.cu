@@ -268,12 +268,12 @@ void run_bfs(cgb_graph* g, uint32_t root, const cgb_options& o)
         const bool heur = bottom_up ? (awake >= old_awake) || ((double)awake > (double)V / beta)
                                     : (double)scout > (double)edges_to_check / alpha;
         // small frontiers far from the switch point: run levels on the device
-        if (persist_ok && !heur && nf <= kPersistEnter && maxdeg < kPersistDeg &&
+        if (persist_ok && !heur && nf <= g->tune.persist_enter && maxdeg < g->tune.persist_deg &&
             (double)scout * alpha * 4.0 <= (double)edges_to_check) {
             if (timing) ktimer_begin(g, CGB_K_PUSH);
             const unsigned long long scout_exit = (unsigned long long)((double)edges_to_check / alpha / 4.0);
             const PersistResult r =
-                bfs_persistent(g, cur, (uint32_t)nf, scout, maxdeg, level, kPersistEnter, scout_exit, kPersistDeg,
+                bfs_persistent(g, cur, (uint32_t)nf, scout, maxdeg, level, g->tune.persist_enter, scout_exit, g->tune.persist_deg,
                                (uint32_t)std::min<uint64_t>(max_iters - iters, 1u << 20));
             if (timing) ktimer_end(g);
             if (r.levels > 0) {

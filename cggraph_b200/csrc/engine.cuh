@@ -44,6 +44,24 @@ struct MsBuffers;
 struct MsspBuffers;
 }
 
+// Launch parameters a graph starts with (cgb_tuning in the C ABI).
+inline cgb_tuning default_tuning()
+{
+    cgb_tuning t{};
+    t.struct_size = sizeof(cgb_tuning);
+    t.push_big_deg = 512;
+    t.push_chunk = 1024;
+    t.push_ctas_per_sm = 8;
+    t.persist_enter = 1u << 15;
+    t.persist_deg = 2048;
+    t.ms_edges = 256;
+    return t;
+}
+
+// Ranges accepted by cgb_tuning_set; buffer capacities are sized for the
+// smallest chunk / descriptor sizes allowed here.
+constexpr uint32_t kMinBigDeg = 128, kMinChunk = 256, kMinMsEdges = 64;
+
 struct cgb_graph {
     int device = 0;
     uint32_t V = 0, E = 0, nz = 0;  // nz = noZeroOutDegreeNum
@@ -57,6 +75,7 @@ struct cgb_graph {
     uint32_t* w = nullptr;  // may be null: unit weights
     uint64_t sum_w = 0;     // sum of weights (delta heuristic)
     uint32_t max_degree = 0;  // longest neighbour list (ensure_frontier)
+    cgb_tuning tune = default_tuning();  // launch parameters (speed only)
 
     // in-edge CSC (built on first need; aliases the CSR when symmetric)
     uint32_t* in_off = nullptr;
@@ -129,8 +148,6 @@ constexpr uint32_t kPrChunk = 4096;  // edges per PageRank hub chunk
 constexpr uint32_t kHugeDeg = 16384; // push: hubs split across CTAs
 constexpr uint32_t kCtaDeg = 1024;   // push: CTA-per-vertex tier
 constexpr uint32_t kHugeChunk = 4096;
-constexpr uint32_t kBigDeg = 512;    // binned push: lists cut into chunks
-constexpr uint32_t kChunk = 1024;    // edges per chunk
 
 // graph lifetime and preparation (graph.cu)
 cgb_graph* graph_alloc(uint32_t V, uint32_t E, uint32_t nz, int device, bool with_weight);

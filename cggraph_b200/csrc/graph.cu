@@ -370,7 +370,9 @@ void ensure_frontier(cgb_graph* g)
     const uint32_t V = g->V;
     g->q[0] = dalloc<uint32_t>(V);
     g->q[1] = dalloc<uint32_t>(V);
-    g->chunk_cap = (uint32_t)std::min<uint64_t>(3ull * g->E / kChunk + 64, 0xFFFFFFF0ull);
+    // any frontier (each vertex once): sum over lists >= big_deg of ceil(deg / chunk)
+    // <= E / chunk + E / big_deg, at the smallest sizes cgb_tuning_set allows
+    g->chunk_cap = (uint32_t)std::min<uint64_t>((uint64_t)g->E / kMinChunk + g->E / kMinBigDeg + 64, 0xFFFFFFF0ull);
     g->chunk_q = dalloc<uint2>(g->chunk_cap);
     g->visited = dalloc<uint32_t>(g->words());
     g->front_bm = dalloc<uint32_t>(2 * (size_t)g->words());

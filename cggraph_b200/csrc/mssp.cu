@@ -17,8 +17,8 @@
 // to n separate cgb_run(CGB_SSSP) results.
 //
 // Work of a round: the queue of vertices with pend != 0 is cut into
-// descriptors of at most kMsEdges edges (hub lists are spread over many
-// warps); a warp takes one descriptor, reads its 32 next edges' targets and
+// descriptors of at most cgb_tuning.ms_edges edges (hub lists are spread
+// over many warps); a warp takes one descriptor, reads its 32 next edges' targets and
 // weights coalesced, and walks them with shuffles.
 #include "mssp.cuh"
 
@@ -52,11 +52,11 @@ __global__ void k_mssp_roots(const uint32_t* roots, uint32_t n, uint32_t* dist, 
 }
 
 // Takes (and clears) the pend mask of every queued vertex and cuts its list
-// into descriptors of at most kMsEdges edges.
+// into descriptors of at most ms_edges edges.
 __global__ void __launch_bounds__(kBlock) k_mssp_desc(const uint32_t* __restrict__ q, const uint32_t* nq_ptr,
                                                       const uint32_t* __restrict__ off, unsigned long long* pend,
                                                       unsigned long long* maskq, uint4* desc, uint64_t cap,
-                                                      MsspCounters* c)
+                                                      MsspCounters* c, uint32_t ms_edges)
 {
     const uint32_t nq = *nq_ptr;
     const uint32_t n_round = (nq + 31u) & ~31u;
@@ -68,7 +68,7 @@ __global__ void __launch_bounds__(kBlock) k_mssp_desc(const uint32_t* __restrict
             pend[v] = 0;
             s = off[v];
             d = off[v + 1] - s;
-            nd = (d + kMsEdges - 1) / kMsEdges;
+            nd = (d + ms_edges - 1) / ms_edges;
         }
         // warp-inclusive scan of the descriptor counts, one atomic per warp
         uint32_t incl = nd;
@@ -83,8 +83,8 @@ __global__ void __launch_bounds__(kBlock) k_mssp_desc(const uint32_t* __restrict
         const uint64_t pos = (uint64_t)base + incl - nd;
         for (uint32_t j = 0; j < nd; j++) {
             if (pos + j < cap) {
-                const uint32_t eb = s + j * kMsEdges;
-                desc[pos + j] = make_uint4(v, eb, min(eb + kMsEdges, s + d), i);
+                const uint32_t eb = s + j * ms_edges;
+                desc[pos + j] = make_uint4(v, eb, min(eb + ms_edges, s + d), i);
             } else {
                 atomicOr(&c->overflow, 1u);
             }
@@ -311,7 +311,7 @@ MsspBuffers* mssp_buffers_alloc(uint32_t V, uint64_t E)
         CGB_CUDA_TRY(cudaMalloc((void**)&b->maskq, (size_t)V * 8));
         CGB_CUDA_TRY(cudaMalloc((void**)&b->far_list[0], (size_t)V * 4));
         CGB_CUDA_TRY(cudaMalloc((void**)&b->far_list[1], (size_t)V * 4));
-        b->desc_cap = (uint64_t)V + E / kMsEdges + 1;
+        b->desc_cap = (uint64_t)V + E / kMinMsEdges + 1;  // any descriptor size cgb_tuning_set allows
         CGB_CUDA_TRY(cudaMalloc((void**)&b->desc, b->desc_cap * sizeof(uint4)));
         CGB_CUDA_TRY(cudaMalloc((void**)&b->c, sizeof(MsspCounters)));
         CGB_CUDA_TRY(cudaMallocHost((void**)&b->h, sizeof(MsspCounters)));
@@ -399,7 +399,8 @@ void run_mssp(cgb_graph* g, const uint32_t* d_roots, uint32_t n, uint32_t* out, 
             ++g->stats.launches;
             k_mssp_desc<<<grid_for(nq, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(g->q[cur], &b.c->nq_in, g->off,
                                                                                     b.pend, b.maskq, b.desc,
-                                                                                    b.desc_cap, b.c);
+                                                                                    b.desc_cap, b.c,
+                                                                                    g->tune.ms_edges);
             ++g->stats.launches;
             mssp_expand(g->w != nullptr, kNumSMs * 8, g->stream, b.desc, b.c, b.maskq, g->dst, g->w, b.dist, b.pend,
                         b.farm, g->q[nxt], &b.c->nq_out, b.far_list[fcur], &b.c->nfar_live, V, t32, nullptr,

@@ -7,7 +7,6 @@
 namespace cgb {
 
 constexpr uint32_t kMsRoots = 64;   // distance slots per vertex
-constexpr uint32_t kMsEdges = 256;  // edges per work descriptor
 
 struct MsspCounters {
     uint32_t nq_in;        // entries of the near queue being expanded
@@ -37,7 +36,7 @@ void mssp_buffers_free(MsspBuffers* b);
 
 __global__ void k_mssp_desc(const uint32_t* __restrict__ q, const uint32_t* nq_ptr, const uint32_t* __restrict__ off,
                             unsigned long long* pend, unsigned long long* maskq, uint4* desc, uint64_t cap,
-                            MsspCounters* c);
+                            MsspCounters* c, uint32_t ms_edges);
 __global__ void k_mssp_split(const uint32_t* __restrict__ far_in, const uint32_t* nfar_ptr,
                              const uint32_t* __restrict__ dist, unsigned long long* pend, unsigned long long* farm,
                              uint32_t* q, uint32_t* q_len, uint32_t* far_out, uint32_t* far_out_len, uint32_t cap,

@@ -56,10 +56,9 @@ struct PersistResult {
     unsigned long long scouts = 0;  // sum of their out-edges (BFS)
 };
 
-// Frontiers up to this many vertices, whose lists are all shorter than
-// kPersistDeg, run in the device-resident loops.
-constexpr uint32_t kPersistEnter = 1u << 15;
-constexpr uint32_t kPersistDeg = 2048;
+// The host loops enter these device-resident loops for frontiers of at
+// most cgb_tuning.persist_enter vertices whose lists are all shorter than
+// cgb_tuning.persist_deg edges.
 
 // Runs BFS top-down levels on the device from the frontier q[cur][0, nf)
 // (level `level`, out-edges `scout`, longest list max_deg) until it empties,
@@ -72,7 +71,7 @@ PersistResult bfs_persistent(cgb_graph* g, uint32_t cur, uint32_t nf, unsigned l
 // Runs SSSP near rounds at threshold thr on the device from q[cur][0, nf)
 // until the near queue empties, exceeds nf_exit, or max_rounds have run.
 // New far-bitmap entries are added to the counters' far_len[0].  For graphs
-// whose lists are all shorter than kPersistDeg.
+// whose lists are all shorter than cgb_tuning.persist_deg.
 PersistResult sssp_persistent(cgb_graph* g, uint32_t cur, uint32_t nf, uint32_t thr, uint32_t* far_bm,
                               uint32_t nf_exit, uint32_t max_rounds);
 

@@ -131,17 +131,19 @@ __global__ void __launch_bounds__(kBlock) k_push_huge(const uint32_t* __restrict
     }
 }
 
-// Binned expansion used by the engine.  Lists of at least kBigDeg edges are
-// cut into kChunk-edge chunks whose descriptors (vertex, chunk index) go to a
+// Binned expansion used by the engine.  Lists of at least big_deg edges are
+// cut into chunk-edge pieces whose descriptors (vertex, chunk index) go to a
 // chunk queue; k_push_chunks then deals the chunks across the whole grid, so
 // a frontier of a few hubs keeps every SM busy however few vertices it has.
-// Lists of 32..kBigDeg-1 edges are walked by one warp, shorter ones by the
-// fine-grained tier.  Chunk-queue capacity E/kChunk + E/kBigDeg + 64 bounds
-// any frontier in which each vertex appears once.
+// Lists of 32..big_deg-1 edges are walked by one warp, shorter ones by the
+// fine-grained tier.  Chunk-queue capacity E/chunk + E/big_deg + 64 bounds
+// any frontier in which each vertex appears once (big_deg and chunk come
+// from the graph's cgb_tuning).
 template <class Op, bool kIdentity>
 __global__ void __launch_bounds__(kBlock) k_push_binned(const uint32_t* __restrict__ qin, uint32_t nin, Op op,
                                                         uint2* __restrict__ chunk_q, uint32_t* chunk_len,
-                                                        uint32_t chunk_cap, uint32_t* overflow)
+                                                        uint32_t chunk_cap, uint32_t* overflow, uint32_t big_deg,
+                                                        uint32_t chunk)
 {
     __shared__ uint32_t s_scan[kBlock / 32 + 1];
     __shared__ uint32_t s_edge[kBlock];
@@ -157,10 +159,10 @@ __global__ void __launch_bounds__(kBlock) k_push_binned(const uint32_t* __restri
         }
         // big lists: the warp writes their chunk descriptors together
         uint32_t bmask;
-        while ((bmask = __ballot_sync(0xffffffffu, deg >= kBigDeg)) != 0) {
+        while ((bmask = __ballot_sync(0xffffffffu, deg >= big_deg)) != 0) {
             const uint32_t leader = __ffs(bmask) - 1;
             const uint32_t bv = __shfl_sync(0xffffffffu, v, leader);
-            const uint32_t nch = (__shfl_sync(0xffffffffu, deg, leader) + kChunk - 1) / kChunk;
+            const uint32_t nch = (__shfl_sync(0xffffffffu, deg, leader) + chunk - 1) / chunk;
             uint32_t slot = 0;
             if (lane_id() == 0) slot = atomicAdd(chunk_len, nch);
             slot = __shfl_sync(0xffffffffu, slot, 0);
@@ -189,7 +191,7 @@ __global__ void __launch_bounds__(kBlock) k_push_binned(const uint32_t* __restri
 // One CTA per chunk descriptor, grid-stride over the chunk queue.
 template <class Op>
 __global__ void __launch_bounds__(kBlock) k_push_chunks(const uint2* __restrict__ chunk_q, const uint32_t* chunk_len,
-                                                        uint32_t chunk_cap, Op op)
+                                                        uint32_t chunk_cap, Op op, uint32_t chunk)
 {
     const uint32_t n = min(*chunk_len, chunk_cap);
     if (blockIdx.x >= n) return;
@@ -199,8 +201,8 @@ __global__ void __launch_bounds__(kBlock) k_push_chunks(const uint2* __restrict_
         const uint2 d = chunk_q[c];
         uint32_t start, deg, msg;
         if (!op.load(d.x, start, deg, msg)) continue;
-        const uint32_t cs = d.y * kChunk;
-        const uint32_t ce = min(deg, cs + kChunk);
+        const uint32_t cs = d.y * chunk;
+        const uint32_t ce = min(deg, cs + chunk);
         for (uint32_t k = cs; k < ce; k += kBlock) op.edge(k + threadIdx.x < ce, start + k + threadIdx.x, msg);
     }
     __syncthreads();
@@ -213,15 +215,19 @@ template <class Op>
 inline void launch_push(cgb_graph* g, const uint32_t* qin, uint32_t nin, const Op& op, bool identity)
 {
     if (nin == 0) return;
-    const uint32_t grid = grid_for(nin, kBlock, kNumSMs * 8);
+    const cgb_tuning& t = g->tune;
+    const uint32_t ctas = kNumSMs * t.push_ctas_per_sm;
+    const uint32_t grid = grid_for(nin, kBlock, ctas);
     g->stats.launches += 2;
     if (identity)
         k_push_binned<Op, true><<<grid, kBlock, 0, g->stream>>>(qin, nin, op, g->chunk_q, &g->ctr->chunk_len,
-                                                                 g->chunk_cap, &g->ctr->overflow);
+                                                                 g->chunk_cap, &g->ctr->overflow, t.push_big_deg,
+                                                                 t.push_chunk);
     else
         k_push_binned<Op, false><<<grid, kBlock, 0, g->stream>>>(qin, nin, op, g->chunk_q, &g->ctr->chunk_len,
-                                                                  g->chunk_cap, &g->ctr->overflow);
-    k_push_chunks<Op><<<kNumSMs * 8, kBlock, 0, g->stream>>>(g->chunk_q, &g->ctr->chunk_len, g->chunk_cap, op);
+                                                                  g->chunk_cap, &g->ctr->overflow, t.push_big_deg,
+                                                                  t.push_chunk);
+    k_push_chunks<Op><<<ctas, kBlock, 0, g->stream>>>(g->chunk_q, &g->ctr->chunk_len, g->chunk_cap, op, t.push_chunk);
 }
 
 }  // namespace cgb

@@ -431,7 +431,7 @@ static void sp_issue(cgb_server* s, Group& G)
     CGB_CUDA_TRY(cudaMemsetAsync(&b.c->nq_out, 0, 4, st));
     CGB_CUDA_TRY(cudaMemsetAsync(&b.c->ndesc, 0, 4, st));
     k_mssp_desc<<<kNumSMs * 8, kBlock, 0, st>>>(G.q[cur], &b.c->nq_in, g->off, b.pend, b.maskq, b.desc, b.desc_cap,
-                                                b.c);
+                                                b.c, g->tune.ms_edges);
     mssp_expand(g->w != nullptr, kNumSMs * 8, st, b.desc, b.c, b.maskq, g->dst, g->w, b.dist, b.pend, b.farm,
                 G.q[nxt], &b.c->nq_out, b.far_list[G.fcur], &b.c->nfar_live, V, 0, G.d_up->thr, G.d_stats->alive);
     k_srv_copy_u32<<<1, 1, 0, st>>>(&b.c->nq_out, &b.c->nq_in);

@@ -175,16 +175,16 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
     uint64_t expanded = 0;
 
     // Near rounds at threshold thr until the near queue is empty.
-    const bool persist_ok = !tracing && o.schedule != CGB_SCHED_FIXED && g->max_degree < kPersistDeg;
+    const bool persist_ok = !tracing && o.schedule != CGB_SCHED_FIXED && g->max_degree < g->tune.persist_deg;
     auto near_rounds = [&]() {
         while (nnear > 0) {
             CGB_REQUIRE(iters < max_iters, CGB_ETIMEOUT, "SSSP iteration budget exhausted");
-            if (persist_ok && nnear <= kPersistEnter) {
+            if (persist_ok && nnear <= g->tune.persist_enter) {
                 // small near queue: run the rounds on the device
                 if (timing) ktimer_begin(g, CGB_K_PUSH);
                 const PersistResult r =
                     sssp_persistent(g, cur, (uint32_t)nnear, (uint32_t)std::min<uint64_t>(thr, kValueMax), far_bm,
-                                    kPersistEnter, (uint32_t)std::min<uint64_t>(max_iters - iters, 1u << 20));
+                                    g->tune.persist_enter, (uint32_t)std::min<uint64_t>(max_iters - iters, 1u << 20));
                 if (timing) ktimer_end(g);
                 sync_counters(g);
                 iters += r.levels;

@@ -1,0 +1,177 @@
+// Launch-parameter tuning of one graph: cgb_tuning_get / cgb_tuning_set and
+// the autotuner (cgb_autotune).
+//
+// The reference fixes its work-distribution thresholds at compile time
+// (WarpDonate / CTA::schedule switch at 16 / 32 / 256 edges,
+// my_project/CGgraph/device_warpDonate.cuh:42-388, device_CTA.cuh:28-112).
+// Here they are per-graph parameters: the out-degree from which a list is
+// cut into chunks, the chunk length, the push grid (CTAs per SM), the
+// frontier size and list length below which the device-resident loops run,
+// and the multi-root SSSP descriptor length.  None of them changes a result.
+//
+// The autotuner is coordinate descent: starting from the graph's current
+// tuning it tries, one field at a time, every candidate value of that field
+// with the others fixed, keeps the fastest, and sweeps the fields twice.  A
+// candidate's score is the summed device time of runs from the given roots
+// (best of two runs per root, after one untimed run), so the starting
+// tuning is always among the candidates and the result is never slower on
+// that measurement.
+#include <vector>
+
+#include "../../include/cgb200.h"
+#include "engine.cuh"
+
+using namespace cgb;
+
+namespace {
+
+bool valid(const cgb_tuning& t)
+{
+    auto pow2 = [](uint32_t x) { return x && !(x & (x - 1)); };
+    return t.push_big_deg >= kMinBigDeg && t.push_big_deg <= 65536 && t.push_chunk >= kMinChunk &&
+           t.push_chunk <= 65536 && pow2(t.push_chunk) && t.push_ctas_per_sm >= 1 && t.push_ctas_per_sm <= 32 &&
+           t.persist_deg >= 64 && t.persist_deg <= 65536 && t.ms_edges >= kMinMsEdges && t.ms_edges <= 4096;
+}
+
+struct Field {
+    uint32_t cgb_tuning::*member;
+    std::vector<uint32_t> values;
+    bool bfs, sssp, ms_bfs, ms_sssp;  // used by: one BFS, one SSSP, multi-root BFS / SSSP passes
+};
+
+std::vector<Field> fields()
+{
+    return {
+        {&cgb_tuning::push_big_deg, {128, 256, 512, 1024, 2048, 4096}, true, true, true, false},
+        {&cgb_tuning::push_chunk, {256, 512, 1024, 2048, 4096}, true, true, true, false},
+        {&cgb_tuning::push_ctas_per_sm, {2, 4, 8, 16}, true, true, true, false},
+        {&cgb_tuning::persist_enter, {0, 4096, 16384, 32768, 131072}, true, true, false, false},
+        {&cgb_tuning::persist_deg, {256, 1024, 2048, 8192}, true, true, false, false},
+        {&cgb_tuning::ms_edges, {64, 128, 256, 512, 1024}, false, false, false, true},
+    };
+}
+
+}  // namespace
+
+extern "C" {
+
+cgb_status cgb_tuning_get(const cgb_graph* g, cgb_tuning* out)
+{
+    if (!g || !out) {
+        set_error("NULL argument");
+        return CGB_EINVAL;
+    }
+    *out = g->tune;
+    return CGB_OK;
+}
+
+cgb_status cgb_tuning_set(cgb_graph* g, const cgb_tuning* t)
+{
+    if (!g || !t) {
+        set_error("NULL argument");
+        return CGB_EINVAL;
+    }
+    if (t->struct_size < sizeof(cgb_tuning)) {
+        set_error("cgb_tuning.struct_size too small");
+        return CGB_EINVAL;
+    }
+    if (!valid(*t)) {
+        set_error("cgb_tuning value out of range");
+        return CGB_EINVAL;
+    }
+    std::lock_guard<std::mutex> lock(g->mu);
+    g->tune = *t;
+    g->tune.struct_size = sizeof(cgb_tuning);
+    return CGB_OK;
+}
+
+cgb_status cgb_autotune(cgb_graph* g, int algorithm, const uint32_t* roots, uint32_t nroots, uint32_t flags,
+                        cgb_tuning* best, double* best_ms, double* start_ms)
+{
+    if (!g || !roots || nroots == 0) {
+        set_error("NULL argument or no roots");
+        return CGB_EINVAL;
+    }
+    if (algorithm != CGB_BFS && algorithm != CGB_SSSP) {
+        set_error("cgb_autotune tunes BFS or SSSP");
+        return CGB_EINVAL;
+    }
+    const bool batch = (flags & CGB_TUNE_BATCH) != 0;
+    const cgb_tuning start = g->tune;
+    // score of the graph's current tuning
+    auto score = [&](double& ms) -> cgb_status {
+        ms = 0;
+        if (batch) {
+            for (uint32_t s0 = 0; s0 < nroots; s0 += 64) {
+                const uint32_t n = std::min(64u, nroots - s0);
+                double best_rep = 1e300;
+                for (int rep = 0; rep < 3; rep++) {
+                    double t = 0;
+                    const cgb_status st = cgb_run_batch(g, algorithm, roots + s0, n, nullptr, nullptr, &t);
+                    if (st != CGB_OK) return st;
+                    if (rep > 0) best_rep = std::min(best_rep, t);
+                }
+                ms += best_rep;
+            }
+        } else {
+            for (uint32_t i = 0; i < nroots; i++) {
+                double best_rep = 1e300;
+                for (int rep = 0; rep < 3; rep++) {
+                    double t = 0;
+                    const cgb_status st = cgb_run(g, algorithm, roots[i], nullptr, nullptr, nullptr, &t);
+                    if (st != CGB_OK) return st;
+                    if (rep > 0) best_rep = std::min(best_rep, t);
+                }
+                ms += best_rep;
+            }
+        }
+        return CGB_OK;
+    };
+    double cur_ms = 0;
+    cgb_status st = score(cur_ms);
+    if (st != CGB_OK) return st;
+    const double first_ms = cur_ms;
+    cgb_tuning cur = start;
+    for (int sweep = 0; sweep < 2; sweep++) {
+        bool moved = false;
+        for (const Field& f : fields()) {
+            const bool used = algorithm == CGB_BFS ? (batch ? f.ms_bfs : f.bfs) : (batch ? f.ms_sssp : f.sssp);
+            if (!used) continue;
+            for (uint32_t v : f.values) {
+                if (cur.*(f.member) == v) continue;
+                cgb_tuning cand = cur;
+                cand.*(f.member) = v;
+                if (!valid(cand)) continue;
+                {
+                    std::lock_guard<std::mutex> lock(g->mu);
+                    g->tune = cand;
+                }
+                double ms = 0;
+                st = score(ms);
+                if (st != CGB_OK) {
+                    std::lock_guard<std::mutex> lock(g->mu);
+                    g->tune = start;
+                    return st;
+                }
+                if (ms < cur_ms) {
+                    cur_ms = ms;
+                    cur = cand;
+                    moved = true;
+                }
+            }
+            std::lock_guard<std::mutex> lock(g->mu);
+            g->tune = cur;
+        }
+        if (!moved) break;
+    }
+    {
+        std::lock_guard<std::mutex> lock(g->mu);
+        g->tune = (flags & CGB_TUNE_KEEP_DEFAULT) ? start : cur;
+    }
+    if (best) *best = cur;
+    if (best_ms) *best_ms = cur_ms;
+    if (start_ms) *start_ms = first_ms;
+    return CGB_OK;
+}
+
+}  // extern "C"

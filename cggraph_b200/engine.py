@@ -265,6 +265,36 @@ class Graph:
         check(L.lib().cgb_run_stats_get(self._h, ctypes.byref(s)))
         return s
 
+    @property
+    def tuning(self) -> dict:
+        """The graph's launch parameters (cgb_tuning; speed only)."""
+        t = L.Tuning()
+        check(L.lib().cgb_tuning_get(self._h, ctypes.byref(t)))
+        return {f: getattr(t, f) for f in L.TUNING_FIELDS}
+
+    @tuning.setter
+    def tuning(self, values: dict) -> None:
+        t = L.Tuning()
+        check(L.lib().cgb_tuning_get(self._h, ctypes.byref(t)))
+        for k, v in values.items():
+            if k not in L.TUNING_FIELDS:
+                raise KeyError(k)
+            setattr(t, k, int(v))
+        t.struct_size = ctypes.sizeof(L.Tuning)
+        check(L.lib().cgb_tuning_set(self._h, ctypes.byref(t)))
+
+    def autotune(self, algorithm: int, roots: Sequence[int], batch: bool = False, keep: bool = True):
+        """Coordinate-descent search of the launch parameters for `algorithm`
+        from `roots` (one run per root, or multi-root passes with batch=True).
+        Returns (best tuning, best ms, starting ms); the best tuning stays on
+        the graph unless keep=False."""
+        r = np.ascontiguousarray(roots, dtype=np.uint32)
+        best, bms, sms = L.Tuning(), ctypes.c_double(), ctypes.c_double()
+        flags = (L.TUNE_BATCH if batch else 0) | (0 if keep else L.TUNE_KEEP_DEFAULT)
+        check(L.lib().cgb_autotune(self._h, int(algorithm), _ptr(r), r.size, flags, ctypes.byref(best),
+                                   ctypes.byref(bms), ctypes.byref(sms)))
+        return {f: getattr(best, f) for f in L.TUNING_FIELDS}, bms.value, sms.value
+
     def trace(self):
         n = ctypes.c_uint32()
         check(L.lib().cgb_trace_get(self._h, None, 0, ctypes.byref(n)))

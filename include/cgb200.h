@@ -192,6 +192,39 @@ cgb_status cgb_run_stats_get(const cgb_graph* g, cgb_run_stats* out);
  * receives the number available. */
 cgb_status cgb_trace_get(const cgb_graph* g, cgb_iter_trace* out, uint32_t max_entries, uint32_t* count);
 
+/* ------------------------------------------------------------ tuning */
+
+/* Launch parameters of a graph's kernels.  They change only speed: every
+ * setting gives the same results.  cgb_graph_create starts from the
+ * defaults below; cgb_autotune searches them for one graph. */
+typedef struct {
+    uint32_t struct_size;      /* sizeof(cgb_tuning) */
+    uint32_t push_big_deg;     /* lists of at least this many edges are cut into chunks (128..65536, default 512) */
+    uint32_t push_chunk;       /* edges per chunk (a power of two, 256..65536, default 1024) */
+    uint32_t push_ctas_per_sm; /* grid of the push kernels, CTAs per SM (1..32, default 8) */
+    uint32_t persist_enter;    /* device-resident loops take frontiers up to this size (0 = never, default 32768) */
+    uint32_t persist_deg;      /* ... whose lists are all shorter than this (64..65536, default 2048) */
+    uint32_t ms_edges;         /* multi-root SSSP: edges per work descriptor (64..4096, default 256) */
+    uint32_t reserved[9];
+} cgb_tuning;
+
+cgb_status cgb_tuning_get(const cgb_graph* g, cgb_tuning* out);
+/* Rejects out-of-range values with CGB_EINVAL and leaves the tuning unchanged. */
+cgb_status cgb_tuning_set(cgb_graph* g, const cgb_tuning* t);
+
+#define CGB_TUNE_BATCH 0x1u /* tune cgb_run_batch passes of the roots (else one cgb_run per root) */
+#define CGB_TUNE_KEEP_DEFAULT 0x2u /* report the best tuning but leave the graph's tuning unchanged */
+
+/* Project-written autotuner (no counterpart in the reference, whose
+ * thresholds are compile-time constants, device_warpDonate.cuh / device_CTA.cuh):
+ * coordinate descent over the cgb_tuning fields that `algorithm` (BFS or
+ * SSSP) uses, starting from the graph's current tuning, scoring each
+ * candidate by the summed device time of runs from `roots` (best of two).
+ * Sets the best tuning on the graph (unless CGB_TUNE_KEEP_DEFAULT) and
+ * reports it with its time and the starting time. */
+cgb_status cgb_autotune(cgb_graph* g, int algorithm, const uint32_t* roots, uint32_t nroots, uint32_t flags,
+                        cgb_tuning* best, double* best_ms, double* start_ms);
+
 /* ------------------------------------------------------- graph batches */
 
 /* Many independent graphs solved together (no counterpart in the
