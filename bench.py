@@ -58,6 +58,8 @@ def parse_args():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=0, help="0 = same as --steps")
+    p.add_argument("--no-autotune", action="store_true",
+                   help="keep the default launch parameters (else cgb_autotune per algorithm, untimed)")
     p.add_argument("--no-batching", action="store_true", help="skip the multi-root and graph-batch section")
     p.add_argument("--no-serving", action="store_true", help="skip the request-server section")
     p.add_argument("--serve-scale", type=int, default=25, help="RMAT scale of the served graph")
@@ -222,6 +224,17 @@ def bench_cgb200(args, d: Dist):
     warm_opts = cg.make_options(schedule=sched)
     timed_opts = cg.make_options(schedule=sched, flags=L.FLAG_KERNEL_TIMING)
 
+    # launch parameters: the project's autotuner, per algorithm, before timing
+    autotune = None
+    if not args.no_autotune:
+        autotune = {}
+        tune_roots = pick_roots(off_h, args.seed + 13, 4)  # not the timed roots
+        for alg, g, rts in ((BFS, gd, tune_roots), (SSSP, gd, tune_roots), (CC, gs, [0])):
+            if alg in algs and g is not None:
+                best, bms, sms = g.autotune(alg, rts)
+                autotune[ALG_NAMES[alg]] = {"default_ms": sms, "tuned_ms": bms, "speedup": sms / bms,
+                                            "tuning": best}
+
     for i in range(args.warmup):
         run_step(gd, gs, roots[i % len(roots)], warm_opts, args.pr_iters, algs)
 
@@ -319,12 +332,14 @@ def bench_cgb200(args, d: Dist):
                    "scale": args.scale, "edge_factor": args.edge_factor, "rmat_abc": [0.57, 0.19, 0.19],
                    "vertices": V, "edges_directed": Ed, "edges_symmetrised": Es, "weights": "uniform [1,64]",
                    "roots": roots, "schedule": args.schedule, "pr_iterations": args.pr_iters,
+                   "launch_parameters": "default" if args.no_autotune else "cgb_autotune per algorithm (untimed)",
                    "algorithms": [ALG_NAMES[a] for a in algs],
                    "l2": "inputs larger than L2 (directed CSR %.2f GB, symmetrised %.2f GB)"
                          % ((4 * (V + 1) + 8 * Ed) / 1e9, (4 * (V + 1) + 4 * Es) / 1e9),
                    "parallelism": f"replicas x{d.world}"},
         "per_algorithm": per_alg,
         "schedules": schedules,
+        "autotune": autotune,
         "batching": batching,
         "serving": serving,
         "roofline": roof,
@@ -398,15 +413,21 @@ def bench_batching(args, cg, L, gd, roots, dev):
     V = gd.vertexNum
     off_h, _, _ = gd.download(with_weight=False)
     rts = pick_roots(off_h, args.seed + 7, 64)
+    tune_rts = pick_roots(off_h, args.seed + 17, 64)
     d_out = torch.empty((64, V), dtype=torch.int32, device=f"cuda:{dev}")
     seq = cg.make_options(flags=L.FLAG_BATCH_SEQUENTIAL)
     for alg, an in ((BFS, "bfs"), (SSSP, "sssp")):
+        tuned = None
+        if not args.no_autotune:
+            best, bms, sms = gd.autotune(alg, tune_rts, batch=True)
+            tuned = {"default_ms": sms, "tuned_ms": bms, "tuning": best}
         gd.run_batch(alg, rts, out=d_out)  # warm-up
         _, ms_multi = gd.run_batch(alg, rts, out=d_out)
         edges = gd.stats().traversed_edges
         _, ms_seq = gd.run_batch(alg, rts, seq, out=d_out)
         out[f"roots64_{an}"] = {"multi_ms": ms_multi, "one_by_one_ms": ms_seq, "multi_gteps": edges / ms_multi / 1e6,
-                                "one_by_one_gteps": edges / ms_seq / 1e6, "speedup": ms_seq / ms_multi}
+                                "one_by_one_gteps": edges / ms_seq / 1e6, "speedup": ms_seq / ms_multi,
+                                "autotune": tuned}
     # 256 uneven graphs
     rng = np.random.default_rng(args.seed + 11)
     graphs = []

@@ -10,6 +10,7 @@ from .engine import (  # noqa: F401
     Algorithm_type,
     Batch,
     CSR_Result_type,
+    DEFAULT_TUNING,
     Engine_type,
     Graph,
     GraphB200,

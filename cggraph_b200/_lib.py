@@ -198,8 +198,8 @@ def lib() -> ctypes.CDLL:
         L.cgb_server_stats.argtypes = [_P, ctypes.POINTER(ctypes.c_uint64), _u32p, _u32p,
                                        ctypes.POINTER(ctypes.c_double)]
         L.cgb_server_destroy.argtypes = [_P]
-        L.cgb_tuning_get.argtypes = [_P, ctypes.POINTER(Tuning)]
-        L.cgb_tuning_set.argtypes = [_P, ctypes.POINTER(Tuning)]
+        L.cgb_tuning_get.argtypes = [_P, i, ctypes.POINTER(Tuning)]
+        L.cgb_tuning_set.argtypes = [_P, i, ctypes.POINTER(Tuning)]
         L.cgb_autotune.argtypes = [_P, i, _P, u32, u32, ctypes.POINTER(Tuning), ctypes.POINTER(ctypes.c_double),
                                    ctypes.POINTER(ctypes.c_double)]
         for name in EXPORTS:

@@ -194,6 +194,7 @@ cgb_status cgb_graph_result_download(const cgb_graph* g, void* values)
 
 static void run_one(cgb_graph* g, int alg, uint32_t root_or_iters, const cgb_options& o)
 {
+    g->tune = g->tune_alg[alg];
     g->stats = cgb_run_stats{};
     g->trace.clear();
     g->flags = o.flags;
@@ -315,7 +316,9 @@ cgb_status cgb_run_batch(cgb_graph* g, int algorithm, const uint32_t* roots, uin
             return;
         }
         // multi-root passes of up to 64 roots
+        g->tune = g->tune_alg[algorithm];
         g->stats = cgb_run_stats{};
+        g->trace.clear();
         g->flags = o.flags;
         const bool dev_out = out_u32 && is_device_ptr(out_u32);
         const uint32_t per = 64;
@@ -332,7 +335,7 @@ cgb_status cgb_run_batch(cgb_graph* g, int algorithm, const uint32_t* roots, uin
                 CGB_CUDA_TRY(cudaMemcpyAsync(d_roots, roots + s0, (size_t)n * 4, cudaMemcpyHostToDevice, g->stream));
                 g->stats.launches = 0;
                 CGB_CUDA_TRY(cudaEventRecord(g->ev_start, g->stream));
-                if (algorithm == CGB_BFS) run_msbfs(g, d_roots, n, lv);
+                if (algorithm == CGB_BFS) run_msbfs(g, d_roots, n, lv, o.bfs_alpha > 0 ? o.bfs_alpha : kMsAlpha);
                 else run_mssp(g, d_roots, n, lv, o.sssp_delta ? o.sssp_delta : mssp_default_delta(g));
                 CGB_CUDA_TRY(cudaEventRecord(g->ev_stop, g->stream));
                 CGB_CUDA_TRY(cudaEventSynchronize(g->ev_stop));

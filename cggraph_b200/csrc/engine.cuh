@@ -21,7 +21,7 @@ struct DevCounters {
     uint32_t min_far;         // SSSP: smallest distance left in the far bitmap
     uint32_t max_deg;         // max degree of the next frontier
     uint32_t chunk_len;       // chunk descriptors queued by k_push_binned
-    uint32_t pad[2];
+    unsigned long long alive; // multi-root BFS: roots with vertices in the next frontier
     float policy_out[CGB_POLICY_OUTPUTS];  // learned scheduler: predicted log-costs
 };
 
@@ -75,7 +75,8 @@ struct cgb_graph {
     uint32_t* w = nullptr;  // may be null: unit weights
     uint64_t sum_w = 0;     // sum of weights (delta heuristic)
     uint32_t max_degree = 0;  // longest neighbour list (ensure_frontier)
-    cgb_tuning tune = default_tuning();  // launch parameters (speed only)
+    cgb_tuning tune_alg[4] = {default_tuning(), default_tuning(), default_tuning(), default_tuning()};
+    cgb_tuning tune = default_tuning();  // active launch parameters: tune_alg of the running algorithm
 
     // in-edge CSC (built on first need; aliases the CSR when symmetric)
     uint32_t* in_off = nullptr;
@@ -174,7 +175,10 @@ void run_sssp(cgb_graph* g, uint32_t root, const cgb_options& o);
 void run_cc(cgb_graph* g, const cgb_options& o);
 void run_pr(cgb_graph* g, uint32_t iters, const cgb_options& o);
 void count_reached(cgb_graph* g);  // fills stats.reached / traversed_edges for BFS/SSSP
-void run_msbfs(cgb_graph* g, const uint32_t* d_roots, uint32_t n, uint32_t* level_out);
+// Multi-root BFS of n <= 64 roots; a level pulls (bottom-up) when the
+// frontier's out-edges times alpha exceed the graph's edges.
+void run_msbfs(cgb_graph* g, const uint32_t* d_roots, uint32_t n, uint32_t* level_out, double alpha);
+constexpr double kMsAlpha = 15.0;  // default alpha of multi-root passes
 void free_msbfs(cgb_graph* g);
 // Multi-root SSSP of n <= 64 roots (device array); out (device) receives
 // n * V distances, root-major.

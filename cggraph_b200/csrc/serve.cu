@@ -204,9 +204,10 @@ struct Group {
     SlotUpload* h_up = nullptr;
     cudaStream_t stream = nullptr;
     unsigned long long active = 0;
+    unsigned long long live = 0;  // BFS: slots with vertices in the current frontier
     std::vector<std::pair<uint32_t, int64_t>> admit;  // (slot, request) of this tick
     // BFS
-    MsBuffers mb;
+    MsBuffers* mb = nullptr;
     uint32_t* q[2] = {nullptr, nullptr};
     uint32_t* touched = nullptr;
     uint32_t nact = 0, cur = 0, tick = 0;
@@ -272,14 +273,11 @@ static void group_alloc(cgb_server* s, Group& G, int alg, uint32_t nslots)
     memset(G.h_up, 0, sizeof(SlotUpload));
     if (alg == CGB_BFS) {
         G.stream = g->stream;  // the binned push expansion runs on the graph's stream
-        G.mb.seen = ms_alloc(V);
-        G.mb.front[0] = ms_alloc(V);
-        G.mb.front[1] = ms_alloc(V);
-        G.mb.next = ms_alloc(V);
-        CGB_CUDA_TRY(cudaMemset(G.mb.seen, 0, (size_t)V * 8));
-        CGB_CUDA_TRY(cudaMemset(G.mb.front[0], 0, (size_t)V * 8));
-        CGB_CUDA_TRY(cudaMemset(G.mb.front[1], 0, (size_t)V * 8));
-        CGB_CUDA_TRY(cudaMemset(G.mb.next, 0, (size_t)V * 8));
+        G.mb = ms_buffers_alloc(V, g->E);
+        CGB_CUDA_TRY(cudaMemset(G.mb->seen, 0, (size_t)V * 8));
+        CGB_CUDA_TRY(cudaMemset(G.mb->front[0], 0, (size_t)V * 8));
+        CGB_CUDA_TRY(cudaMemset(G.mb->front[1], 0, (size_t)V * 8));
+        CGB_CUDA_TRY(cudaMemset(G.mb->next, 0, (size_t)V * 8));
         CGB_CUDA_TRY(cudaMalloc((void**)&G.q[0], (size_t)V * 4));
         CGB_CUDA_TRY(cudaMalloc((void**)&G.q[1], (size_t)V * 4));
         CGB_CUDA_TRY(cudaMalloc((void**)&G.touched, (size_t)V * 4));
@@ -303,10 +301,7 @@ static void group_free(cgb_server* s, Group& G)
     if (G.h_stats) cudaFreeHost(G.h_stats);
     cudaFree(G.d_up);
     if (G.h_up) cudaFreeHost(G.h_up);
-    cudaFree(G.mb.seen);
-    cudaFree(G.mb.front[0]);
-    cudaFree(G.mb.front[1]);
-    cudaFree(G.mb.next);
+    ms_buffers_free(G.mb);
     cudaFree(G.q[0]);
     cudaFree(G.q[1]);
     cudaFree(G.touched);
@@ -333,17 +328,18 @@ static void bfs_issue(cgb_server* s, Group& G)
             G.h_up->slots[n] = k;
             G.h_up->roots[n] = R.info.root;
             G.h_up->qidx[n] = R.info.root < g->nz ? qpos++ : 0xFFFFFFFFu;
+            if (R.info.root < g->nz) G.live |= 1ull << k;
             G.h_up->start[k] = G.tick;
             n++;
         }
         G.nact = qpos;
         if (reuse)
-            k_srv_clear_bits<<<kNumSMs * 8, kBlock, 0, st>>>(V, G.mb.seen, reuse);
+            k_srv_clear_bits<<<kNumSMs * 8, kBlock, 0, st>>>(V, G.mb->seen, reuse);
         for (auto& a : G.admit)
             k_ms_fill<<<kNumSMs * 4, kBlock, 0, st>>>((uint64_t)V, G.region + (size_t)a.first * V, kValueMax);
         CGB_CUDA_TRY(cudaMemcpyAsync(G.d_up, G.h_up, sizeof(SlotUpload), cudaMemcpyHostToDevice, st));
         k_srv_bfs_admit<<<1, kSrvSlots, 0, st>>>(n, G.d_up->slots, G.d_up->roots, G.d_up->qidx, V, G.region,
-                                                 G.mb.seen, G.mb.front[cur], G.q[cur]);
+                                                 G.mb->seen, G.mb->front[cur], G.q[cur]);
     }
     CGB_CUDA_TRY(cudaMemsetAsync(&G.d_stats->alive[0], 0, 8, st));
     CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->qlen[nxt], 0, 4, st));
@@ -353,20 +349,21 @@ static void bfs_issue(cgb_server* s, Group& G)
     const uint32_t lvl = G.tick + 1;
     const bool pull = (double)G.medges * 15.0 > (double)g->E;
     if (pull) {
-        k_ms_bu<<<grid_for(V, kBlock, kNumSMs * 16), kBlock, 0, st>>>(
-            V, g->in_off, g->in_src, G.mb.front[cur], G.mb.seen, G.mb.front[nxt], G.active, G.region, lvl, g->nz,
-            G.q[nxt], &g->ctr->qlen[nxt], V, g->ctr, G.d_up->start, &G.d_stats->alive[0]);
+        MsBuArgs ba{V, g->in_off, g->in_src, G.mb->front[cur], G.mb->seen, G.mb->front[nxt], G.mb->next, G.live,
+                    G.region, lvl, g->nz, G.q[nxt], &g->ctr->qlen[nxt], V, g->ctr, G.d_up->start,
+                    &G.d_stats->alive[0], G.mb->heavy_w, G.mb->heavy_b, G.mb->heavy_len, G.mb->cap_b};
+        ms_bottom_up(ba, st, nullptr);
     } else {
         CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->found, 0, 4, st));
         CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->chunk_len, 0, 4, st));
-        MsTdOp op{g->off, g->dst, G.mb.front[cur], G.mb.seen, G.mb.next, G.touched, &g->ctr->found, V, g->ctr};
+        MsTdOp op{g->off, g->dst, G.mb->front[cur], G.mb->seen, G.mb->next, G.touched, &g->ctr->found, V, g->ctr};
         launch_push(g, G.q[cur], G.nact, op, false);
-        k_ms_finalize<<<kNumSMs * 8, kBlock, 0, st>>>(G.touched, 0, &g->ctr->found, G.mb.seen, G.mb.next,
-                                                     G.mb.front[nxt], G.region, V, lvl, g->nz, G.q[nxt],
+        k_ms_finalize<<<kNumSMs * 8, kBlock, 0, st>>>(G.touched, 0, &g->ctr->found, G.mb->seen, G.mb->next,
+                                                     G.mb->front[nxt], G.region, V, lvl, g->nz, G.q[nxt],
                                                      &g->ctr->qlen[nxt], V, g->ctr, G.d_up->start,
                                                      &G.d_stats->alive[0]);
     }
-    k_ms_clear<<<grid_for(G.nact, kBlock, kNumSMs * 8), kBlock, 0, st>>>(G.q[cur], G.nact, G.mb.front[cur]);
+    k_ms_clear<<<grid_for(G.nact, kBlock, kNumSMs * 8), kBlock, 0, st>>>(G.q[cur], G.nact, G.mb->front[cur]);
     k_ms_degree_sum<<<kNumSMs * 4, kBlock, 0, st>>>(G.q[nxt], 0, &g->ctr->qlen[nxt], g->off, g->ctr);
 }
 
@@ -431,7 +428,7 @@ static void sp_issue(cgb_server* s, Group& G)
     CGB_CUDA_TRY(cudaMemsetAsync(&b.c->nq_out, 0, 4, st));
     CGB_CUDA_TRY(cudaMemsetAsync(&b.c->ndesc, 0, 4, st));
     k_mssp_desc<<<kNumSMs * 8, kBlock, 0, st>>>(G.q[cur], &b.c->nq_in, g->off, b.pend, b.maskq, b.desc, b.desc_cap,
-                                                b.c, g->tune.ms_edges);
+                                                b.c, g->tune_alg[CGB_SSSP].ms_edges);
     mssp_expand(g->w != nullptr, kNumSMs * 8, st, b.desc, b.c, b.maskq, g->dst, g->w, b.dist, b.pend, b.farm,
                 G.q[nxt], &b.c->nq_out, b.far_list[G.fcur], &b.c->nfar_live, V, 0, G.d_up->thr, G.d_stats->alive);
     k_srv_copy_u32<<<1, 1, 0, st>>>(&b.c->nq_out, &b.c->nq_in);
@@ -451,6 +448,7 @@ static unsigned long long group_finished(cgb_server* s, Group& G)
         G.medges = g->h_ctr->medges;
         CGB_REQUIRE(!g->h_ctr->overflow, CGB_EOVERFLOW, "server BFS queue overflow");
         const unsigned long long alive = G.h_stats->alive[0];
+        G.live = alive;
         G.cur ^= 1;
         G.tick++;
         return G.active & ~alive;
@@ -557,6 +555,7 @@ static void server_loop(cgb_server* s)
             Group& B = s->grp[0];
             Group& S = s->grp[1];
             if (B.active) {
+                g->tune = g->tune_alg[CGB_BFS];
                 bfs_issue(s, B);
                 CGB_CUDA_TRY(cudaMemcpyAsync(B.h_stats->alive, B.d_stats->alive, sizeof(B.h_stats->alive),
                                              cudaMemcpyDeviceToHost, B.stream));

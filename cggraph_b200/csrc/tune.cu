@@ -9,8 +9,9 @@
 // frontier size and list length below which the device-resident loops run,
 // and the multi-root SSSP descriptor length.  None of them changes a result.
 //
-// The autotuner is coordinate descent: starting from the graph's current
-// tuning it tries, one field at a time, every candidate value of that field
+// Each algorithm has its own tuning (a run makes its algorithm's tuning the
+// active one).  The autotuner is coordinate descent: starting from the
+// algorithm's current tuning it tries, one field at a time, every candidate value of that field
 // with the others fixed, keeps the fastest, and sweeps the fields twice.  A
 // candidate's score is the summed device time of runs from the given roots
 // (best of two runs per root, after one untimed run), so the starting
@@ -36,18 +37,18 @@ bool valid(const cgb_tuning& t)
 struct Field {
     uint32_t cgb_tuning::*member;
     std::vector<uint32_t> values;
-    bool bfs, sssp, ms_bfs, ms_sssp;  // used by: one BFS, one SSSP, multi-root BFS / SSSP passes
+    bool bfs, sssp, cc, ms_bfs, ms_sssp;  // used by: one BFS, SSSP, CC run; multi-root BFS / SSSP passes
 };
 
 std::vector<Field> fields()
 {
     return {
-        {&cgb_tuning::push_big_deg, {128, 256, 512, 1024, 2048, 4096}, true, true, true, false},
-        {&cgb_tuning::push_chunk, {256, 512, 1024, 2048, 4096}, true, true, true, false},
-        {&cgb_tuning::push_ctas_per_sm, {2, 4, 8, 16}, true, true, true, false},
-        {&cgb_tuning::persist_enter, {0, 4096, 16384, 32768, 131072}, true, true, false, false},
-        {&cgb_tuning::persist_deg, {256, 1024, 2048, 8192}, true, true, false, false},
-        {&cgb_tuning::ms_edges, {64, 128, 256, 512, 1024}, false, false, false, true},
+        {&cgb_tuning::push_big_deg, {128, 256, 512, 1024, 2048, 4096}, true, true, true, true, false},
+        {&cgb_tuning::push_chunk, {256, 512, 1024, 2048, 4096}, true, true, true, true, false},
+        {&cgb_tuning::push_ctas_per_sm, {2, 4, 8, 16}, true, true, true, true, false},
+        {&cgb_tuning::persist_enter, {0, 4096, 16384, 32768, 131072}, true, true, false, false, false},
+        {&cgb_tuning::persist_deg, {256, 1024, 2048, 8192}, true, true, false, false, false},
+        {&cgb_tuning::ms_edges, {64, 128, 256, 512, 1024}, false, false, false, false, true},
     };
 }
 
@@ -55,20 +56,20 @@ std::vector<Field> fields()
 
 extern "C" {
 
-cgb_status cgb_tuning_get(const cgb_graph* g, cgb_tuning* out)
+cgb_status cgb_tuning_get(const cgb_graph* g, int algorithm, cgb_tuning* out)
 {
-    if (!g || !out) {
-        set_error("NULL argument");
+    if (!g || !out || algorithm < 0 || algorithm > CGB_PR) {
+        set_error("NULL argument or unknown algorithm");
         return CGB_EINVAL;
     }
-    *out = g->tune;
+    *out = g->tune_alg[algorithm];
     return CGB_OK;
 }
 
-cgb_status cgb_tuning_set(cgb_graph* g, const cgb_tuning* t)
+cgb_status cgb_tuning_set(cgb_graph* g, int algorithm, const cgb_tuning* t)
 {
-    if (!g || !t) {
-        set_error("NULL argument");
+    if (!g || !t || algorithm < -1 || algorithm > CGB_PR) {
+        set_error("NULL argument or unknown algorithm");
         return CGB_EINVAL;
     }
     if (t->struct_size < sizeof(cgb_tuning)) {
@@ -80,8 +81,11 @@ cgb_status cgb_tuning_set(cgb_graph* g, const cgb_tuning* t)
         return CGB_EINVAL;
     }
     std::lock_guard<std::mutex> lock(g->mu);
-    g->tune = *t;
-    g->tune.struct_size = sizeof(cgb_tuning);
+    for (int a = 0; a <= CGB_PR; a++) {
+        if (algorithm != -1 && a != algorithm) continue;
+        g->tune_alg[a] = *t;
+        g->tune_alg[a].struct_size = sizeof(cgb_tuning);
+    }
     return CGB_OK;
 }
 
@@ -92,12 +96,13 @@ cgb_status cgb_autotune(cgb_graph* g, int algorithm, const uint32_t* roots, uint
         set_error("NULL argument or no roots");
         return CGB_EINVAL;
     }
-    if (algorithm != CGB_BFS && algorithm != CGB_SSSP) {
-        set_error("cgb_autotune tunes BFS or SSSP");
+    const bool batch = (flags & CGB_TUNE_BATCH) != 0;
+    if (algorithm != CGB_BFS && algorithm != CGB_SSSP && !(algorithm == CGB_CC && !batch)) {
+        set_error("cgb_autotune tunes BFS, SSSP (runs or multi-root passes) or CC (runs)");
         return CGB_EINVAL;
     }
-    const bool batch = (flags & CGB_TUNE_BATCH) != 0;
-    const cgb_tuning start = g->tune;
+    cgb_tuning& slot = g->tune_alg[algorithm];
+    const cgb_tuning start = slot;
     // score of the graph's current tuning
     auto score = [&](double& ms) -> cgb_status {
         ms = 0;
@@ -118,7 +123,8 @@ cgb_status cgb_autotune(cgb_graph* g, int algorithm, const uint32_t* roots, uint
                 double best_rep = 1e300;
                 for (int rep = 0; rep < 3; rep++) {
                     double t = 0;
-                    const cgb_status st = cgb_run(g, algorithm, roots[i], nullptr, nullptr, nullptr, &t);
+                    const cgb_status st =
+                        cgb_run(g, algorithm, algorithm == CGB_CC ? 0 : roots[i], nullptr, nullptr, nullptr, &t);
                     if (st != CGB_OK) return st;
                     if (rep > 0) best_rep = std::min(best_rep, t);
                 }
@@ -135,7 +141,9 @@ cgb_status cgb_autotune(cgb_graph* g, int algorithm, const uint32_t* roots, uint
     for (int sweep = 0; sweep < 2; sweep++) {
         bool moved = false;
         for (const Field& f : fields()) {
-            const bool used = algorithm == CGB_BFS ? (batch ? f.ms_bfs : f.bfs) : (batch ? f.ms_sssp : f.sssp);
+            const bool used = algorithm == CGB_CC ? f.cc
+                              : algorithm == CGB_BFS ? (batch ? f.ms_bfs : f.bfs)
+                                                     : (batch ? f.ms_sssp : f.sssp);
             if (!used) continue;
             for (uint32_t v : f.values) {
                 if (cur.*(f.member) == v) continue;
@@ -144,13 +152,13 @@ cgb_status cgb_autotune(cgb_graph* g, int algorithm, const uint32_t* roots, uint
                 if (!valid(cand)) continue;
                 {
                     std::lock_guard<std::mutex> lock(g->mu);
-                    g->tune = cand;
+                    slot = cand;
                 }
                 double ms = 0;
                 st = score(ms);
                 if (st != CGB_OK) {
                     std::lock_guard<std::mutex> lock(g->mu);
-                    g->tune = start;
+                    slot = start;
                     return st;
                 }
                 if (ms < cur_ms) {
@@ -160,13 +168,13 @@ cgb_status cgb_autotune(cgb_graph* g, int algorithm, const uint32_t* roots, uint
                 }
             }
             std::lock_guard<std::mutex> lock(g->mu);
-            g->tune = cur;
+            slot = cur;
         }
         if (!moved) break;
     }
     {
         std::lock_guard<std::mutex> lock(g->mu);
-        g->tune = (flags & CGB_TUNE_KEEP_DEFAULT) ? start : cur;
+        slot = (flags & CGB_TUNE_KEEP_DEFAULT) ? start : cur;
     }
     if (best) *best = cur;
     if (best_ms) *best_ms = cur_ms;

@@ -129,6 +129,10 @@ def _u32(a):
     return np.ascontiguousarray(a, dtype=np.uint32)
 
 
+DEFAULT_TUNING = {"push_big_deg": 512, "push_chunk": 1024, "push_ctas_per_sm": 8, "persist_enter": 1 << 15,
+                  "persist_deg": 2048, "ms_edges": 256}
+
+
 def _count(a) -> int:
     """Element count of a numpy array or a torch tensor."""
     return int(a.size if isinstance(a, np.ndarray) else a.numel())
@@ -265,23 +269,23 @@ class Graph:
         check(L.lib().cgb_run_stats_get(self._h, ctypes.byref(s)))
         return s
 
-    @property
-    def tuning(self) -> dict:
-        """The graph's launch parameters (cgb_tuning; speed only)."""
+    def get_tuning(self, algorithm: int = 0) -> dict:
+        """An algorithm's launch parameters (cgb_tuning; speed only)."""
         t = L.Tuning()
-        check(L.lib().cgb_tuning_get(self._h, ctypes.byref(t)))
+        check(L.lib().cgb_tuning_get(self._h, int(algorithm), ctypes.byref(t)))
         return {f: getattr(t, f) for f in L.TUNING_FIELDS}
 
-    @tuning.setter
-    def tuning(self, values: dict) -> None:
+    def set_tuning(self, values: dict, algorithm: int = -1) -> None:
+        """Changes the given fields of an algorithm's tuning (-1: of every
+        algorithm, starting from BFS's)."""
         t = L.Tuning()
-        check(L.lib().cgb_tuning_get(self._h, ctypes.byref(t)))
+        check(L.lib().cgb_tuning_get(self._h, max(0, int(algorithm)), ctypes.byref(t)))
         for k, v in values.items():
             if k not in L.TUNING_FIELDS:
                 raise KeyError(k)
             setattr(t, k, int(v))
         t.struct_size = ctypes.sizeof(L.Tuning)
-        check(L.lib().cgb_tuning_set(self._h, ctypes.byref(t)))
+        check(L.lib().cgb_tuning_set(self._h, int(algorithm), ctypes.byref(t)))
 
     def autotune(self, algorithm: int, roots: Sequence[int], batch: bool = False, keep: bool = True):
         """Coordinate-descent search of the launch parameters for `algorithm`

@@ -194,9 +194,10 @@ cgb_status cgb_trace_get(const cgb_graph* g, cgb_iter_trace* out, uint32_t max_e
 
 /* ------------------------------------------------------------ tuning */
 
-/* Launch parameters of a graph's kernels.  They change only speed: every
- * setting gives the same results.  cgb_graph_create starts from the
- * defaults below; cgb_autotune searches them for one graph. */
+/* Launch parameters of a graph's kernels, one set per algorithm.  They
+ * change only speed: every setting gives the same results.  cgb_graph_create
+ * starts from the defaults below; cgb_autotune searches them for one graph
+ * and algorithm. */
 typedef struct {
     uint32_t struct_size;      /* sizeof(cgb_tuning) */
     uint32_t push_big_deg;     /* lists of at least this many edges are cut into chunks (128..65536, default 512) */
@@ -208,18 +209,21 @@ typedef struct {
     uint32_t reserved[9];
 } cgb_tuning;
 
-cgb_status cgb_tuning_get(const cgb_graph* g, cgb_tuning* out);
-/* Rejects out-of-range values with CGB_EINVAL and leaves the tuning unchanged. */
-cgb_status cgb_tuning_set(cgb_graph* g, const cgb_tuning* t);
+cgb_status cgb_tuning_get(const cgb_graph* g, int algorithm, cgb_tuning* out);
+/* algorithm -1 sets every algorithm's tuning.  Rejects out-of-range values
+ * with CGB_EINVAL and leaves the tuning unchanged. */
+cgb_status cgb_tuning_set(cgb_graph* g, int algorithm, const cgb_tuning* t);
 
 #define CGB_TUNE_BATCH 0x1u /* tune cgb_run_batch passes of the roots (else one cgb_run per root) */
 #define CGB_TUNE_KEEP_DEFAULT 0x2u /* report the best tuning but leave the graph's tuning unchanged */
 
 /* Project-written autotuner (no counterpart in the reference, whose
  * thresholds are compile-time constants, device_warpDonate.cuh / device_CTA.cuh):
- * coordinate descent over the cgb_tuning fields that `algorithm` (BFS or
- * SSSP) uses, starting from the graph's current tuning, scoring each
- * candidate by the summed device time of runs from `roots` (best of two).
+ * coordinate descent over the cgb_tuning fields that `algorithm` uses (BFS
+ * or SSSP runs or multi-root passes; CC runs, one per entry of `roots`,
+ * whose values are then ignored), starting from the algorithm's current
+ * tuning, scoring each candidate by the summed device time of runs from
+ * `roots` (best of two).
  * Sets the best tuning on the graph (unless CGB_TUNE_KEEP_DEFAULT) and
  * reports it with its time and the starting time. */
 cgb_status cgb_autotune(cgb_graph* g, int algorithm, const uint32_t* roots, uint32_t nroots, uint32_t flags,

@@ -28,7 +28,7 @@ def test_results_identical_under_every_tuning(oracle, sym):
     exp_c = oracle.cc(off, dst)
     with cg.Graph.from_csr(off, dst, w) as g:
         for t in TUNINGS:
-            g.tuning = t
+            g.set_tuning({**cg.DEFAULT_TUNING, **t})
             for r, eb, es in zip(roots, exp_b, exp_s):
                 np.testing.assert_array_equal(g.run(BFS, r)[0], eb, err_msg=str(t))
                 np.testing.assert_array_equal(g.run(SSSP, r)[0], es, err_msg=str(t))
@@ -43,7 +43,7 @@ def test_grid_under_tunings(oracle):
     off, dst, w = oracle.grid_graph(50, 70, seed=8)
     with cg.Graph.from_csr(off, dst, w) as g:
         for t in TUNINGS:
-            g.tuning = t
+            g.set_tuning({**cg.DEFAULT_TUNING, **t})
             np.testing.assert_array_equal(g.run(BFS, 17)[0], oracle.bfs(off, dst, 17))
             np.testing.assert_array_equal(g.run(SSSP, 17)[0], oracle.sssp(off, dst, w, 17))
 
@@ -53,16 +53,17 @@ def test_autotune_and_range_checks(oracle):
     deg = np.diff(off.astype(np.int64))
     roots = [int(x) for x in np.nonzero(deg)[0][:2]]
     with cg.Graph.from_csr(off, dst, w) as g:
-        start = g.tuning
+        assert g.get_tuning(BFS) == cg.DEFAULT_TUNING
         best, best_ms, start_ms = g.autotune(BFS, roots, keep=False)
         assert best_ms <= start_ms
-        assert g.tuning == start
+        assert g.get_tuning(BFS) == cg.DEFAULT_TUNING
         best, best_ms, start_ms = g.autotune(SSSP, roots * 3, batch=True)
         assert best_ms <= start_ms
-        assert g.tuning == best
+        assert g.get_tuning(SSSP) == best
+        assert g.get_tuning(BFS) == cg.DEFAULT_TUNING  # tunings are per algorithm
         np.testing.assert_array_equal(g.run(SSSP, roots[0])[0], oracle.sssp(off, dst, w, roots[0]))
         for bad in ({"push_big_deg": 64}, {"push_chunk": 1000}, {"push_ctas_per_sm": 0}, {"ms_edges": 8192},
                     {"persist_deg": 1}):
             with pytest.raises(cg.CgbError):
-                g.tuning = bad
-        assert g.tuning == best
+                g.set_tuning(bad, SSSP)
+        assert g.get_tuning(SSSP) == best
