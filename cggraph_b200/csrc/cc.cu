@@ -39,20 +39,36 @@ __device__ __forceinline__ uint32_t ld_comp(const uint32_t* comp, uint32_t i)
 }
 
 // Hooks the trees of u and v, larger root under smaller root.
+// Root of x with path halving: each visited vertex is pointed at its
+// grandparent on the way up.  Concurrent halving is benign: a vertex only
+// ever moves to one of its own ancestors, so every pointer still goes to a
+// smaller vertex of the same tree.
+__device__ __forceinline__ uint32_t find_halve(uint32_t x, uint32_t* comp)
+{
+    uint32_t p = ld_comp(comp, x);
+    for (uint32_t steps = 0; p != x && steps < kLinkRetries; steps++) {
+        const uint32_t gp = ld_comp(comp, p);
+        if (gp != p) *((volatile uint32_t*)comp + x) = gp;
+        x = gp;
+        p = ld_comp(comp, x);
+    }
+    return x;
+}
+
 __device__ __forceinline__ void link(uint32_t u, uint32_t v, uint32_t* comp, DevCounters* ctr)
 {
-    uint32_t p1 = ld_comp(comp, u), p2 = ld_comp(comp, v);
+    uint32_t p1 = find_halve(u, comp), p2 = find_halve(v, comp);
     for (uint32_t tries = 0; p1 != p2; tries++) {
         if (tries >= kLinkRetries) {
             atomicOr(&ctr->link_giveup, 1u);
             return;
         }
         const uint32_t high = max(p1, p2), low = min(p1, p2);
-        const uint32_t p_high = ld_comp(comp, high);
-        if (p_high == low) return;
-        if (p_high == high && atomicCAS(comp + high, high, low) == high) return;
-        p1 = ld_comp(comp, ld_comp(comp, high));
-        p2 = ld_comp(comp, low);
+        // hook the larger root under the smaller one; on failure another
+        // thread hooked `high` first: retry from both roots' new roots
+        if (atomicCAS(comp + high, high, low) == high) return;
+        p1 = find_halve(high, comp);
+        p2 = find_halve(low, comp);
     }
 }
 
