@@ -229,7 +229,7 @@ def bench_cgb200(args, d: Dist):
     if not args.no_autotune:
         autotune = {}
         tune_roots = pick_roots(off_h, args.seed + 13, 4)  # not the timed roots
-        for alg, g, rts in ((BFS, gd, tune_roots), (SSSP, gd, tune_roots), (CC, gs, [0])):
+        for alg, g, rts in ((BFS, gd, tune_roots), (SSSP, gd, tune_roots), (CC, gs, [0]), (PR, gd, [5, 5])):
             if alg in algs and g is not None:
                 best, bms, sms = g.autotune(alg, rts)
                 autotune[ALG_NAMES[alg]] = {"default_ms": sms, "tuned_ms": bms, "speedup": sms / bms,

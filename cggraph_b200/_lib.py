@@ -104,12 +104,15 @@ class Tuning(ctypes.Structure):
         ("persist_enter", ctypes.c_uint32),
         ("persist_deg", ctypes.c_uint32),
         ("ms_edges", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32 * 9),
+        ("pr_unroll", ctypes.c_uint32),
+        ("pr_ctas_per_sm", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 7),
     ]
 
 
 TUNE_BATCH, TUNE_KEEP_DEFAULT = 0x1, 0x2
-TUNING_FIELDS = ("push_big_deg", "push_chunk", "push_ctas_per_sm", "persist_enter", "persist_deg", "ms_edges")
+TUNING_FIELDS = ("push_big_deg", "push_chunk", "push_ctas_per_sm", "persist_enter", "persist_deg", "ms_edges",
+                 "pr_unroll", "pr_ctas_per_sm")
 
 
 class ServerConfig(ctypes.Structure):

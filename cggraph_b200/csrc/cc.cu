@@ -100,16 +100,13 @@ __global__ void k_cc_link_round(uint32_t V, const uint32_t* __restrict__ off, co
     }
 }
 
+// Points every vertex at its root (path halving on the way, which shortens
+// the chains that other threads are still walking).
 __global__ void k_cc_compress(uint32_t V, uint32_t* comp)
 {
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
-        uint32_t c = comp[v];
-        uint32_t cc = ld_comp(comp, c);
-        while (c != cc) {
-            c = cc;
-            cc = ld_comp(comp, c);
-        }
-        comp[v] = c;
+        const uint32_t r = find_halve(v, comp);
+        if (ld_comp(comp, v) != r) comp[v] = r;
     }
 }
 
@@ -201,10 +198,7 @@ static void cc_afforest(cgb_graph* g)
     k_cc_init_min_nbr<<<grid, kBlock, 0, g->stream>>>(V, g->off, g->dst, g->value);
     CGB_CUDA_TRY(cudaMemsetAsync(g->ctr, 0, sizeof(DevCounters), g->stream));
     if (timing) ktimer_end(g);
-    if (timing) ktimer_begin(g, CGB_K_COMPRESS);
-    ++g->stats.launches;
-    k_cc_compress<<<grid, kBlock, 0, g->stream>>>(V, g->value);
-    if (timing) ktimer_end(g);
+    // no compress here: the link round's finds halve the init forest's paths
     for (uint32_t r = 1; r < kRounds; r++) {
         if (timing) ktimer_begin(g, CGB_K_HOOK);
         ++g->stats.launches;

@@ -55,6 +55,8 @@ inline cgb_tuning default_tuning()
     t.persist_enter = 1u << 15;
     t.persist_deg = 2048;
     t.ms_edges = 256;
+    t.pr_unroll = 16;
+    t.pr_ctas_per_sm = 128;
     return t;
 }
 

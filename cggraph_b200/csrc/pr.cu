@@ -45,11 +45,12 @@ __global__ void k_pr_init(uint32_t V, const uint32_t* __restrict__ outdeg, doubl
 
 // One warp per 32-row slice of the sliced ELL: in step j every lane loads
 // its row's j-th source (one coalesced 128-byte load per warp) and gathers
-// that contribution; eight steps are issued before they are summed, in j
-// order, so each lane keeps eight gathers in flight.  Padding slots name
+// that contribution; kU steps (cgb_tuning.pr_unroll) are issued before they
+// are summed, in j order, so each lane keeps kU gathers in flight.  Padding slots name
 // vertex V, whose contribution is 0.  Hub rows (bit set in hub_bm) are
 // finished by k_pr_hub_finish.  The slice stream and the outputs use
 // evict-first accesses so that L2 keeps the gathered contributions.
+template <int kU>
 __global__ void __launch_bounds__(kBlock) k_pr_pull(uint32_t V, const uint64_t* __restrict__ slice_ptr,
                                                     const uint32_t* __restrict__ slice_len,
                                                     const uint32_t* __restrict__ col,
@@ -65,18 +66,19 @@ __global__ void __launch_bounds__(kBlock) k_pr_pull(uint32_t V, const uint64_t* 
         const uint32_t len = slice_len[s];
         const uint32_t* c = col + slice_ptr[s] + lane;
         double acc = 0.0;
-        uint32_t j = 0;
-        for (; j + 8 <= len; j += 8) {
-            uint32_t u[8];
+        // kU steps per batch: all their gathers in flight, then summed in
+        // step order; the last batch is predicated (masked steps add
+        // contrib[V] = +0.0, which leaves the sum and its order unchanged)
+        for (uint32_t j = 0; j < len; j += kU) {
+            uint32_t u[kU];
 #pragma unroll
-            for (int t = 0; t < 8; t++) u[t] = __ldcs(c + 32u * (j + t));  // read once: evict first
-            double x[8];
+            for (int t = 0; t < kU; t++) u[t] = j + t < len ? __ldcs(c + 32u * (j + t)) : V;  // read once
+            double x[kU];
 #pragma unroll
-            for (int t = 0; t < 8; t++) x[t] = contrib[u[t]];
+            for (int t = 0; t < kU; t++) x[t] = contrib[u[t]];
 #pragma unroll
-            for (int t = 0; t < 8; t++) acc += x[t];
+            for (int t = 0; t < kU; t++) acc += x[t];
         }
-        for (; j < len; j++) acc += contrib[__ldcs(c + 32u * j)];
         const uint32_t r = s * 32 + lane;
         const bool hub = (hub_bm[s] >> lane) & 1u;
         if (r < V && !hub) {
@@ -159,7 +161,8 @@ void run_pr(cgb_graph* g, uint32_t iters, const cgb_options& o)
     ++g->stats.launches;
     k_pr_init<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, g->pr_outdeg, g->pr[0], g->contrib[0]);
     if (timing) ktimer_end(g);
-    const uint32_t grid = grid_for(div_up(V, 32), kBlock / 32, kNumSMs * 16);
+    const uint32_t grid = grid_for(div_up(V, 32), kBlock / 32, kNumSMs * g->tune.pr_ctas_per_sm);
+    const uint32_t unroll = g->tune.pr_unroll;
     int cur = 0;
     for (uint32_t it = 0; it < iters; it++) {
         const int out = cur ^ 1;
@@ -170,9 +173,9 @@ void run_pr(cgb_graph* g, uint32_t iters, const cgb_options& o)
                 g->pr_chunks, g->n_pr_chunks, g->pr_off, g->pr_src, g->contrib[cur], g->pr_part);
         }
         ++g->stats.launches;
-        k_pr_pull<<<grid, kBlock, 0, g->stream>>>(V, g->pr_slice_ptr, g->pr_slice_len, g->pr_col, g->pr_hub_bm,
-                                                  g->pr_outdeg, g->contrib[cur], g->pr[out], g->contrib[out], base,
-                                                  damp);
+        auto pull = unroll == 4 ? k_pr_pull<4> : unroll == 16 ? k_pr_pull<16> : k_pr_pull<8>;
+        pull<<<grid, kBlock, 0, g->stream>>>(V, g->pr_slice_ptr, g->pr_slice_len, g->pr_col, g->pr_hub_bm,
+                                             g->pr_outdeg, g->contrib[cur], g->pr[out], g->contrib[out], base, damp);
         if (g->n_pr_huge) {
             ++g->stats.launches;
             k_pr_hub_finish<<<grid_for(g->n_pr_huge, kBlock, kNumSMs), kBlock, 0, g->stream>>>(

@@ -31,24 +31,28 @@ bool valid(const cgb_tuning& t)
     auto pow2 = [](uint32_t x) { return x && !(x & (x - 1)); };
     return t.push_big_deg >= kMinBigDeg && t.push_big_deg <= 65536 && t.push_chunk >= kMinChunk &&
            t.push_chunk <= 65536 && pow2(t.push_chunk) && t.push_ctas_per_sm >= 1 && t.push_ctas_per_sm <= 32 &&
-           t.persist_deg >= 64 && t.persist_deg <= 65536 && t.ms_edges >= kMinMsEdges && t.ms_edges <= 4096;
+           t.persist_deg >= 64 && t.persist_deg <= 65536 && t.ms_edges >= kMinMsEdges && t.ms_edges <= 4096 &&
+           (t.pr_unroll == 4 || t.pr_unroll == 8 || t.pr_unroll == 16) && t.pr_ctas_per_sm >= 1 &&
+           t.pr_ctas_per_sm <= 1024;
 }
 
 struct Field {
     uint32_t cgb_tuning::*member;
     std::vector<uint32_t> values;
-    bool bfs, sssp, cc, ms_bfs, ms_sssp;  // used by: one BFS, SSSP, CC run; multi-root BFS / SSSP passes
+    bool bfs, sssp, cc, pr, ms_bfs, ms_sssp;  // used by: one BFS / SSSP / CC / PR run; multi-root passes
 };
 
 std::vector<Field> fields()
 {
     return {
-        {&cgb_tuning::push_big_deg, {128, 256, 512, 1024, 2048, 4096}, true, true, true, true, false},
-        {&cgb_tuning::push_chunk, {256, 512, 1024, 2048, 4096}, true, true, true, true, false},
-        {&cgb_tuning::push_ctas_per_sm, {2, 4, 8, 16}, true, true, true, true, false},
-        {&cgb_tuning::persist_enter, {0, 4096, 16384, 32768, 131072}, true, true, false, false, false},
-        {&cgb_tuning::persist_deg, {256, 1024, 2048, 8192}, true, true, false, false, false},
-        {&cgb_tuning::ms_edges, {64, 128, 256, 512, 1024}, false, false, false, false, true},
+        {&cgb_tuning::push_big_deg, {128, 256, 512, 1024, 2048, 4096}, true, true, true, false, true, false},
+        {&cgb_tuning::push_chunk, {256, 512, 1024, 2048, 4096}, true, true, true, false, true, false},
+        {&cgb_tuning::push_ctas_per_sm, {2, 4, 8, 16}, true, true, true, false, true, false},
+        {&cgb_tuning::persist_enter, {0, 4096, 16384, 32768, 131072}, true, true, false, false, false, false},
+        {&cgb_tuning::persist_deg, {256, 1024, 2048, 8192}, true, true, false, false, false, false},
+        {&cgb_tuning::ms_edges, {64, 128, 256, 512, 1024}, false, false, false, false, false, true},
+        {&cgb_tuning::pr_unroll, {4, 8, 16}, false, false, false, true, false, false},
+        {&cgb_tuning::pr_ctas_per_sm, {16, 32, 64, 128, 256, 1024}, false, false, false, true, false, false},
     };
 }
 
@@ -97,8 +101,8 @@ cgb_status cgb_autotune(cgb_graph* g, int algorithm, const uint32_t* roots, uint
         return CGB_EINVAL;
     }
     const bool batch = (flags & CGB_TUNE_BATCH) != 0;
-    if (algorithm != CGB_BFS && algorithm != CGB_SSSP && !(algorithm == CGB_CC && !batch)) {
-        set_error("cgb_autotune tunes BFS, SSSP (runs or multi-root passes) or CC (runs)");
+    if (algorithm != CGB_BFS && algorithm != CGB_SSSP && !((algorithm == CGB_CC || algorithm == CGB_PR) && !batch)) {
+        set_error("cgb_autotune tunes BFS, SSSP (runs or multi-root passes), CC or PageRank (runs)");
         return CGB_EINVAL;
     }
     cgb_tuning& slot = g->tune_alg[algorithm];
@@ -125,6 +129,7 @@ cgb_status cgb_autotune(cgb_graph* g, int algorithm, const uint32_t* roots, uint
                     double t = 0;
                     const cgb_status st =
                         cgb_run(g, algorithm, algorithm == CGB_CC ? 0 : roots[i], nullptr, nullptr, nullptr, &t);
+                    // (PageRank: roots[i] is the iteration count)
                     if (st != CGB_OK) return st;
                     if (rep > 0) best_rep = std::min(best_rep, t);
                 }
@@ -141,7 +146,8 @@ cgb_status cgb_autotune(cgb_graph* g, int algorithm, const uint32_t* roots, uint
     for (int sweep = 0; sweep < 2; sweep++) {
         bool moved = false;
         for (const Field& f : fields()) {
-            const bool used = algorithm == CGB_CC ? f.cc
+            const bool used = algorithm == CGB_CC   ? f.cc
+                              : algorithm == CGB_PR ? f.pr
                               : algorithm == CGB_BFS ? (batch ? f.ms_bfs : f.bfs)
                                                      : (batch ? f.ms_sssp : f.sssp);
             if (!used) continue;

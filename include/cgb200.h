@@ -206,7 +206,10 @@ typedef struct {
     uint32_t persist_enter;    /* device-resident loops take frontiers up to this size (0 = never, default 32768) */
     uint32_t persist_deg;      /* ... whose lists are all shorter than this (64..65536, default 2048) */
     uint32_t ms_edges;         /* multi-root SSSP: edges per work descriptor (64..4096, default 256) */
-    uint32_t reserved[9];
+    uint32_t pr_unroll;        /* PageRank pull: gathers in flight per lane (4, 8 or 16, default 16) */
+    uint32_t pr_ctas_per_sm;   /* PageRank pull grid, CTAs per SM (1..1024, capped at one 32-row slice
+                                  per warp; default 128) */
+    uint32_t reserved[7];
 } cgb_tuning;
 
 cgb_status cgb_tuning_get(const cgb_graph* g, int algorithm, cgb_tuning* out);
@@ -220,10 +223,10 @@ cgb_status cgb_tuning_set(cgb_graph* g, int algorithm, const cgb_tuning* t);
 /* Project-written autotuner (no counterpart in the reference, whose
  * thresholds are compile-time constants, device_warpDonate.cuh / device_CTA.cuh):
  * coordinate descent over the cgb_tuning fields that `algorithm` uses (BFS
- * or SSSP runs or multi-root passes; CC runs, one per entry of `roots`,
- * whose values are then ignored), starting from the algorithm's current
- * tuning, scoring each candidate by the summed device time of runs from
- * `roots` (best of two).
+ * or SSSP runs or multi-root passes from the roots; CC runs, one per entry
+ * of `roots`, whose values are then ignored; PageRank runs of roots[i]
+ * iterations), starting from the algorithm's current tuning, scoring each
+ * candidate by the summed device time of the runs (best of two).
  * Sets the best tuning on the graph (unless CGB_TUNE_KEEP_DEFAULT) and
  * reports it with its time and the starting time. */
 cgb_status cgb_autotune(cgb_graph* g, int algorithm, const uint32_t* roots, uint32_t nroots, uint32_t flags,

@@ -7,13 +7,14 @@ import cggraph_b200 as cg
 
 pytestmark = pytest.mark.gpu
 
-BFS, SSSP, CC = 0, 1, 2
+BFS, SSSP, CC, PR = 0, 1, 2, 3
 
 TUNINGS = [
     {},
-    {"push_big_deg": 128, "push_chunk": 256, "push_ctas_per_sm": 1, "persist_enter": 0, "ms_edges": 64},
+    {"push_big_deg": 128, "push_chunk": 256, "push_ctas_per_sm": 1, "persist_enter": 0, "ms_edges": 64,
+     "pr_unroll": 4, "pr_ctas_per_sm": 1},
     {"push_big_deg": 65536, "push_chunk": 65536, "push_ctas_per_sm": 32, "persist_enter": 1 << 30,
-     "persist_deg": 65536, "ms_edges": 4096},
+     "persist_deg": 65536, "ms_edges": 4096, "pr_unroll": 16, "pr_ctas_per_sm": 1024},
     {"push_big_deg": 300, "push_chunk": 512, "push_ctas_per_sm": 3, "persist_enter": 100, "persist_deg": 64},
 ]
 
@@ -26,6 +27,7 @@ def test_results_identical_under_every_tuning(oracle, sym):
     exp_b = [oracle.bfs(off, dst, r) for r in roots]
     exp_s = [oracle.sssp(off, dst, w, r) for r in roots]
     exp_c = oracle.cc(off, dst)
+    pr_ref = None
     with cg.Graph.from_csr(off, dst, w) as g:
         for t in TUNINGS:
             g.set_tuning({**cg.DEFAULT_TUNING, **t})
@@ -33,6 +35,10 @@ def test_results_identical_under_every_tuning(oracle, sym):
                 np.testing.assert_array_equal(g.run(BFS, r)[0], eb, err_msg=str(t))
                 np.testing.assert_array_equal(g.run(SSSP, r)[0], es, err_msg=str(t))
             np.testing.assert_array_equal(g.run(CC)[0], exp_c, err_msg=str(t))
+            pr, _ = g.run(PR, 20)
+            if pr_ref is None:
+                pr_ref = pr
+            np.testing.assert_array_equal(pr, pr_ref, err_msg=str(t))  # fixed summation order: bit-identical
             out, _ = g.run_batch(SSSP, roots)
             np.testing.assert_array_equal(out, np.stack(exp_s), err_msg=str(t))
             out, _ = g.run_batch(BFS, roots)
@@ -62,8 +68,10 @@ def test_autotune_and_range_checks(oracle):
         assert g.get_tuning(SSSP) == best
         assert g.get_tuning(BFS) == cg.DEFAULT_TUNING  # tunings are per algorithm
         np.testing.assert_array_equal(g.run(SSSP, roots[0])[0], oracle.sssp(off, dst, w, roots[0]))
+        best_pr, pms, psms = g.autotune(PR, [5, 5])
+        assert pms <= psms and g.get_tuning(PR) == best_pr
         for bad in ({"push_big_deg": 64}, {"push_chunk": 1000}, {"push_ctas_per_sm": 0}, {"ms_edges": 8192},
-                    {"persist_deg": 1}):
+                    {"persist_deg": 1}, {"pr_unroll": 6}, {"pr_ctas_per_sm": 1025}):
             with pytest.raises(cg.CgbError):
                 g.set_tuning(bad, SSSP)
         assert g.get_tuning(SSSP) == best
