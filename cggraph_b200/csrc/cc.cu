@@ -13,10 +13,11 @@
 //      edge, so this is already a valid forest, built without atomics (the
 //      initialisation of ECL-CC, Jaiganesh and Burtscher 2018);
 //   2. one round that links v with its second neighbour, and with its first
-//      one where step 1 left it pointing at itself (first neighbour larger),
-//      each step followed by a compress (pointer jumping to the root);
-//   3. sample comp[] at 1024 hashed vertices and take the most frequent root
-//      as the giant component c;
+//      one where step 1 left it pointing at itself (first neighbour larger);
+//      every find halves the path it walks, so no separate compress pass
+//      runs before step 5;
+//   3. find the roots of 1024 hashed vertices and take the most frequent
+//      one as the giant component c;
 //   4. link every remaining edge of each vertex whose root is not c (the
 //      giant component's own edges can be skipped because every edge leaving
 //      it is seen again from its other, non-giant endpoint), with the
@@ -110,11 +111,11 @@ __global__ void k_cc_compress(uint32_t V, uint32_t* comp)
     }
 }
 
-__global__ void k_cc_sample(uint32_t V, const uint32_t* comp, uint32_t* out, uint32_t n, uint64_t seed)
+__global__ void k_cc_sample(uint32_t V, uint32_t* comp, uint32_t* out, uint32_t n, uint64_t seed)
 {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t v = (uint32_t)(mix64(seed ^ i) % V);
-        out[i] = ld_comp(comp, v);
+        out[i] = find_halve(v, comp);
     }
 }
 
@@ -131,7 +132,7 @@ struct CcLinkOp {
         s = off[v];
         d = off[v + 1] - s;
         m = v;
-        if (ld_comp(comp, v) == giant || d <= skip) return false;
+        if (d <= skip || find_halve(v, comp) == giant) return false;
         s += skip;
         d -= skip;
         return true;
@@ -204,11 +205,8 @@ static void cc_afforest(cgb_graph* g)
         ++g->stats.launches;
         k_cc_link_round<<<grid, kBlock, 0, g->stream>>>(V, g->off, g->dst, g->value, r, r == 1, g->ctr);
         if (timing) ktimer_end(g);
-        if (timing) ktimer_begin(g, CGB_K_COMPRESS);
-        ++g->stats.launches;
-        k_cc_compress<<<grid, kBlock, 0, g->stream>>>(V, g->value);
-        if (timing) ktimer_end(g);
     }
+    // no compress here either: sampling and the final link find roots themselves
     if (timing) ktimer_begin(g, CGB_K_OTHER);
     ++g->stats.launches;
     k_cc_sample<<<4, kBlock, 0, g->stream>>>(V, g->value, g->sample, kSamples, 0xAFF0E57ull);
