@@ -148,31 +148,27 @@ __global__ void __launch_bounds__(kBlock) k_mssp_expand(const uint4* __restrict_
                     const uint32_t t = t0 + i;
                     if (t >= cnt) break;  // warp-uniform
                     uint32_t* du = dist + (size_t)u[i] * kMsRoots;
-                    bool n0 = false, n1 = false, f0 = false, f1 = false;
+                    bool m0 = false, m1 = false, n0 = false, n1 = false;
                     const uint64_t c0 = (uint64_t)dv0 + wt[i], c1 = (uint64_t)dv1 + wt[i];
                     if (s0 && c0 < kValueMax && (uint32_t)c0 < x0[i]) {
-                        const uint32_t old = atomicMin(du + lane, (uint32_t)c0);
-                        if ((uint32_t)c0 < old) {
-                            relax++;
-                            n0 = (uint32_t)c0 < thr0;
-                            f0 = !n0;
-                        }
+                        m0 = (uint32_t)c0 < atomicMin(du + lane, (uint32_t)c0);
+                        n0 = m0 && (uint32_t)c0 < thr0;
                     }
                     if (s1 && c1 < kValueMax && (uint32_t)c1 < x1[i]) {
-                        const uint32_t old = atomicMin(du + lane + 32, (uint32_t)c1);
-                        if ((uint32_t)c1 < old) {
-                            relax++;
-                            n1 = (uint32_t)c1 < thr1;
-                            f1 = !n1;
-                        }
+                        m1 = (uint32_t)c1 < atomicMin(du + lane + 32, (uint32_t)c1);
+                        n1 = m1 && (uint32_t)c1 < thr1;
                     }
-                    const unsigned long long nb = (unsigned long long)__ballot_sync(0xffffffffu, n0) |
-                                                  ((unsigned long long)__ballot_sync(0xffffffffu, n1) << 32);
-                    const unsigned long long fb = (unsigned long long)__ballot_sync(0xffffffffu, f0) |
-                                                  ((unsigned long long)__ballot_sync(0xffffffffu, f1) << 32);
-                    if (lane == t) {
-                        my_nb = nb;
-                        my_fb = fb;
+                    // improved roots; their near / far split only when there are any
+                    const unsigned long long mb = (unsigned long long)__ballot_sync(0xffffffffu, m0) |
+                                                  ((unsigned long long)__ballot_sync(0xffffffffu, m1) << 32);
+                    if (mb) {
+                        relax += (m0 ? 1 : 0) + (m1 ? 1 : 0);
+                        const unsigned long long nb = (unsigned long long)__ballot_sync(0xffffffffu, n0) |
+                                                      ((unsigned long long)__ballot_sync(0xffffffffu, n1) << 32);
+                        if (lane == t) {
+                            my_nb = nb;
+                            my_fb = mb & ~nb;
+                        }
                     }
                 }
             }
