@@ -10,8 +10,9 @@
 //      out, and the slots of a group are capped so that their result
 //      regions fit the memory budget);
 //   2. advances every active slot by one BFS level / one SSSP round, all
-//      slots of a group in the same kernels, the BFS group on the graph's
-//      stream and the SSSP group on its own so that the two overlap;
+//      slots of a group in the same kernels; each group has its own host
+//      thread and stream (the BFS group the graph's), so the two overlap on
+//      the device and short BFS levels never wait for SSSP rounds;
 //   3. retires the slots whose traversal ended (no frontier bits left for
 //      them), copying their results out and freeing the slot.
 // A request admitted while others run starts at its own level 0 (BFS
@@ -205,7 +206,9 @@ struct Group {
     cudaStream_t stream = nullptr;
     unsigned long long active = 0;
     unsigned long long live = 0;  // BFS: slots with vertices in the current frontier
-    std::vector<std::pair<uint32_t, int64_t>> admit;  // (slot, request) of this tick
+    uint32_t root[kSrvSlots];
+    uint32_t* out[kSrvSlots];  // where the slot's result goes (host / device / NULL)
+    std::vector<uint32_t> admit;  // slots admitted this tick (root / out filled under the server lock)
     // BFS
     MsBuffers* mb = nullptr;
     uint32_t* q[2] = {nullptr, nullptr};
@@ -233,12 +236,12 @@ struct cgb_server {
     std::vector<cgb_request_info> done;
     std::mutex mu;
     std::condition_variable cv;
-    std::thread th;
+    std::thread th[2];
     std::atomic<bool> stop{false};
     bool started = false;
     Clock::time_point t0;
-    uint64_t ticks = 0, completed = 0;
-    double busy_ms = 0;
+    uint64_t ticks[2] = {0, 0}, completed = 0;
+    double busy_ms[2] = {0, 0};
     cgb_status error = CGB_OK;
     std::string error_msg;
 };
@@ -320,23 +323,22 @@ static void bfs_issue(cgb_server* s, Group& G)
     if (!G.admit.empty()) {
         unsigned long long reuse = 0;
         uint32_t n = 0, qpos = G.nact;
-        for (auto& a : G.admit) {
-            const uint32_t k = a.first;
-            const SrvReq& R = s->reqs[a.second];
+        for (const uint32_t k : G.admit) {
+            const uint32_t root = G.root[k];
             if (G.used[k]) reuse |= 1ull << k;
             G.used[k] = true;
             G.h_up->slots[n] = k;
-            G.h_up->roots[n] = R.info.root;
-            G.h_up->qidx[n] = R.info.root < g->nz ? qpos++ : 0xFFFFFFFFu;
-            if (R.info.root < g->nz) G.live |= 1ull << k;
+            G.h_up->roots[n] = root;
+            G.h_up->qidx[n] = root < g->nz ? qpos++ : 0xFFFFFFFFu;
+            if (root < g->nz) G.live |= 1ull << k;
             G.h_up->start[k] = G.tick;
             n++;
         }
         G.nact = qpos;
         if (reuse)
             k_srv_clear_bits<<<kNumSMs * 8, kBlock, 0, st>>>(V, G.mb->seen, reuse);
-        for (auto& a : G.admit)
-            k_ms_fill<<<kNumSMs * 4, kBlock, 0, st>>>((uint64_t)V, G.region + (size_t)a.first * V, kValueMax);
+        for (const uint32_t k : G.admit)
+            k_ms_fill<<<kNumSMs * 4, kBlock, 0, st>>>((uint64_t)V, G.region + (size_t)k * V, kValueMax);
         CGB_CUDA_TRY(cudaMemcpyAsync(G.d_up, G.h_up, sizeof(SlotUpload), cudaMemcpyHostToDevice, st));
         k_srv_bfs_admit<<<1, kSrvSlots, 0, st>>>(n, G.d_up->slots, G.d_up->roots, G.d_up->qidx, V, G.region,
                                                  G.mb->seen, G.mb->front[cur], G.q[cur]);
@@ -379,13 +381,12 @@ static void sp_issue(cgb_server* s, Group& G)
     if (!G.admit.empty()) {
         unsigned long long reuse = 0;
         uint32_t n = 0;
-        for (auto& a : G.admit) {
-            const uint32_t k = a.first;
+        for (const uint32_t k : G.admit) {
             if (G.used[k]) reuse |= 1ull << k;
             G.used[k] = true;
             admitted |= 1ull << k;
             G.h_up->slots[n] = k;
-            G.h_up->roots[n] = s->reqs[a.second].info.root;
+            G.h_up->roots[n] = G.root[k];
             G.thr[k] = G.delta;
             G.last_empty[k] = false;
             G.min_far[k] = kValueMax;
@@ -480,9 +481,8 @@ static void group_retire(cgb_server* s, Group& G, unsigned long long fin)
                                                 G.d_stats->depth);
     for (unsigned long long m = fin; m; m &= m - 1) {
         const uint32_t k = __builtin_ctzll(m);
-        SrvReq& R = s->reqs[G.req[k]];
-        if (R.out)
-            CGB_CUDA_TRY(cudaMemcpyAsync(R.out, G.region + (size_t)k * V, (size_t)V * 4, cudaMemcpyDefault, st));
+        if (G.out[k])
+            CGB_CUDA_TRY(cudaMemcpyAsync(G.out[k], G.region + (size_t)k * V, (size_t)V * 4, cudaMemcpyDefault, st));
     }
     CGB_CUDA_TRY(cudaMemcpyAsync(G.h_stats, G.d_stats, offsetof(SlotStats, alive), cudaMemcpyDeviceToHost, st));
     CGB_CUDA_TRY(cudaStreamSynchronize(st));
@@ -517,68 +517,77 @@ static void pick_admissions(cgb_server* s, Group& G, std::deque<int64_t>& waitin
         if (k >= G.nslots) break;
         G.state[k] = SlotState::kActive;
         G.req[k] = waiting.front();
+        G.root[k] = R.info.root;
+        G.out[k] = R.out;
         G.active |= 1ull << k;
         R.info.slot = k;
         R.info.admit_us = now_us;
-        G.admit.push_back({k, waiting.front()});
+        G.admit.push_back(k);
         waiting.pop_front();
     }
 }
 
-static void server_loop(cgb_server* s)
+// The serving loop of one group (a = 0 BFS, 1 SSSP); each group has its
+// own thread and stream, so short BFS levels never wait for SSSP rounds.
+// The BFS group uses the graph's shared scratch (counters, chunk queue) and
+// holds the graph's lock for each tick; the SSSP group touches only its own
+// buffers and the read-only CSR.
+static void group_loop(cgb_server* s, int a)
 {
     cgb_graph* g = s->g;
+    Group& G = s->grp[a];
     try {
         CGB_CUDA_TRY(cudaSetDevice(g->device));
         while (!s->stop.load()) {
-            double next_arrival = -1;
             {
                 std::unique_lock<std::mutex> lk(s->mu);
+                if (s->error != CGB_OK) break;
                 const double now = us_since(s, Clock::now());
-                for (int a = 0; a < 2; a++) pick_admissions(s, s->grp[a], s->waiting[a], now);
-                const bool work = s->grp[0].active || s->grp[1].active;
-                if (!work) {
-                    for (int a = 0; a < 2; a++)
-                        if (!s->waiting[a].empty()) {
-                            const double t = s->reqs[s->waiting[a].front()].info.arrival_us;
-                            if (next_arrival < 0 || t < next_arrival) next_arrival = t;
-                        }
-                    if (next_arrival < 0)
+                pick_admissions(s, G, s->waiting[a], now);
+                if (!G.active) {
+                    if (s->waiting[a].empty()) {
                         s->cv.wait_for(lk, std::chrono::milliseconds(5));
-                    else if (next_arrival > now)
-                        s->cv.wait_for(lk, std::chrono::microseconds((int64_t)(next_arrival - now) + 1));
+                    } else {
+                        const double t = s->reqs[s->waiting[a].front()].info.arrival_us;
+                        if (t > now) s->cv.wait_for(lk, std::chrono::microseconds((int64_t)(t - now) + 1));
+                    }
                     continue;
                 }
             }
             const auto t_tick = Clock::now();
-            std::lock_guard<std::mutex> glk(g->mu);
-            Group& B = s->grp[0];
-            Group& S = s->grp[1];
-            if (B.active) {
+            unsigned long long fin;
+            if (a == 0) {
+                std::lock_guard<std::mutex> glk(g->mu);
                 g->tune = g->tune_alg[CGB_BFS];
-                bfs_issue(s, B);
-                CGB_CUDA_TRY(cudaMemcpyAsync(B.h_stats->alive, B.d_stats->alive, sizeof(B.h_stats->alive),
-                                             cudaMemcpyDeviceToHost, B.stream));
-                CGB_CUDA_TRY(cudaMemcpyAsync(g->h_ctr, g->ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, B.stream));
+                bfs_issue(s, G);
+                CGB_CUDA_TRY(cudaMemcpyAsync(G.h_stats->alive, G.d_stats->alive, sizeof(G.h_stats->alive),
+                                             cudaMemcpyDeviceToHost, G.stream));
+                CGB_CUDA_TRY(cudaMemcpyAsync(g->h_ctr, g->ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, G.stream));
+                CGB_CUDA_TRY(cudaStreamSynchronize(G.stream));
+                fin = group_finished(s, G);
+                group_retire(s, G, fin);
+            } else {
+                sp_issue(s, G);
+                CGB_CUDA_TRY(cudaStreamSynchronize(G.stream));
+                fin = group_finished(s, G);
+                group_retire(s, G, fin);
             }
-            if (S.active) sp_issue(s, S);
-            if (B.active) CGB_CUDA_TRY(cudaStreamSynchronize(B.stream));
-            if (S.active) CGB_CUDA_TRY(cudaStreamSynchronize(S.stream));
-            const unsigned long long fb = B.active ? group_finished(s, B) : 0;
-            const unsigned long long fs = S.active ? group_finished(s, S) : 0;
-            group_retire(s, B, fb);
-            group_retire(s, S, fs);
-            s->ticks++;
-            s->busy_ms += std::chrono::duration<double, std::milli>(Clock::now() - t_tick).count();
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->ticks[a]++;
+            s->busy_ms[a] += std::chrono::duration<double, std::milli>(Clock::now() - t_tick).count();
         }
     } catch (const Error& e) {
         std::lock_guard<std::mutex> lk(s->mu);
-        s->error = e.code;
-        s->error_msg = e.msg;
+        if (s->error == CGB_OK) {
+            s->error = e.code;
+            s->error_msg = e.msg;
+        }
     } catch (const std::exception& e) {
         std::lock_guard<std::mutex> lk(s->mu);
-        s->error = CGB_ECUDA;
-        s->error_msg = e.what();
+        if (s->error == CGB_OK) {
+            s->error = CGB_ECUDA;
+            s->error_msg = e.what();
+        }
     }
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->error != CGB_OK) {
@@ -590,7 +599,7 @@ static void server_loop(cgb_server* s)
                 s->done.push_back(R.info);
                 s->completed++;
             }
-        for (int a = 0; a < 2; a++) s->waiting[a].clear();
+        for (int k = 0; k < 2; k++) s->waiting[k].clear();
     }
     s->cv.notify_all();
 }
@@ -700,7 +709,8 @@ cgb_status cgb_server_start(cgb_server* s)
         CGB_REQUIRE(!s->started, CGB_EINVAL, "server already started");
         s->t0 = Clock::now();
         s->started = true;
-        s->th = std::thread(server_loop, s);
+        for (int a = 0; a < 2; a++)
+            if (s->grp[a].nslots) s->th[a] = std::thread(group_loop, s, a);
     });
 }
 
@@ -737,10 +747,10 @@ cgb_status cgb_server_stats(const cgb_server* s, uint64_t* ticks, uint32_t* bfs_
 {
     return sguard([&] {
         CGB_REQUIRE(s != nullptr, CGB_EINVAL, "server is NULL");
-        if (ticks) *ticks = s->ticks;
+        if (ticks) *ticks = s->ticks[0] + s->ticks[1];
         if (bfs_slots) *bfs_slots = s->grp[0].nslots;
         if (sssp_slots) *sssp_slots = s->grp[1].nslots;
-        if (busy_ms) *busy_ms = s->busy_ms;
+        if (busy_ms) *busy_ms = s->busy_ms[0] + s->busy_ms[1];
     });
 }
 
@@ -750,7 +760,8 @@ cgb_status cgb_server_destroy(cgb_server* s)
         if (!s) return;
         s->stop.store(true);
         s->cv.notify_all();
-        if (s->th.joinable()) s->th.join();
+        for (int a = 0; a < 2; a++)
+            if (s->th[a].joinable()) s->th[a].join();
         cudaSetDevice(s->g->device);
         group_free(s, s->grp[0]);
         group_free(s, s->grp[1]);
