@@ -18,6 +18,7 @@ from .engine import (  # noqa: F401
     Server,
     VertexValue_MAX,
     checkBinResult,
+    chunglu_weight_offset,
     load_binFile,
     main_partition,
     make_options,

@@ -29,7 +29,7 @@ KERNEL_CLASS_NAMES = ["push", "pull", "pagerank", "hook", "compress", "frontier"
 EXPORTS = [
     "cgb_graph_create", "cgb_graph_load_files", "cgb_graph_destroy", "cgb_graph_set_stream", "cgb_graph_info", "cgb_graph_device_csr",
     "cgb_graph_result_device", "cgb_graph_result_download", "cgb_run", "cgb_run_batch", "cgb_run_stats_get", "cgb_trace_get",
-    "cgb_last_error_string", "cgb_status_string", "cgb_abi_version", "cgb_gen_rmat", "cgb_gen_grid",
+    "cgb_last_error_string", "cgb_status_string", "cgb_abi_version", "cgb_gen_rmat", "cgb_gen_grid", "cgb_gen_chunglu",
     "cgb_graph_download", "cgb_bfs_noalloc", "cgb_policy_load", "cgb_policy_collect", "cgb_policy_train",
     "cgb_policy_forward", "cgb_policy_loss_grad", "cgb_batch_create", "cgb_batch_destroy", "cgb_batch_run",
     "cgb_batch_info", "cgb_batch_stats", "cgb_server_create", "cgb_server_submit", "cgb_server_start",
@@ -180,6 +180,7 @@ def lib() -> ctypes.CDLL:
         L.cgb_gen_rmat.argtypes = [u32, u32, ctypes.c_uint64, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                    i, i, u32, i, ctypes.POINTER(_P)]
         L.cgb_gen_grid.argtypes = [u32, u32, ctypes.c_uint64, u32, i, ctypes.POINTER(_P)]
+        L.cgb_gen_chunglu.argtypes = [u32, ctypes.c_uint64, u32, ctypes.c_uint64, i, u32, i, ctypes.POINTER(_P)]
         L.cgb_graph_download.argtypes = [_P, _P, _P, _P]
         L.cgb_bfs_noalloc.argtypes = [_P, _P, u32, u32, u32, _P, _P]
         L.cgb_policy_load.argtypes = [_P]

@@ -15,6 +15,7 @@ namespace cgb {
 cgb_graph* gen_rmat(uint32_t scale, uint32_t ef, uint64_t seed, double a, double b, double c, int scr, int sym,
                     uint32_t wmax, int device);
 cgb_graph* gen_grid(uint32_t rows, uint32_t cols, uint64_t seed, uint32_t wmax, int device);
+cgb_graph* gen_chunglu(uint32_t V, uint64_t draws, uint32_t i0, uint64_t seed, int sym, uint32_t wmax, int device);
 }  // namespace cgb
 
 using namespace cgb;
@@ -430,6 +431,15 @@ cgb_status cgb_gen_grid(uint32_t rows, uint32_t cols, uint64_t seed, uint32_t wm
     return guarded([&] {
         CGB_REQUIRE(out != nullptr, CGB_EINVAL, "out is NULL");
         *out = gen_grid(rows, cols, seed, wmax, device);
+    });
+}
+
+cgb_status cgb_gen_chunglu(uint32_t vertices, uint64_t draws, uint32_t weight_offset, uint64_t seed, int symmetrise,
+                           uint32_t wmax, int device, cgb_graph** out)
+{
+    return guarded([&] {
+        CGB_REQUIRE(out != nullptr, CGB_EINVAL, "out is NULL");
+        *out = gen_chunglu(vertices, draws, weight_offset, seed, symmetrise, wmax, device);
     });
 }
 

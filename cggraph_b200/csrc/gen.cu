@@ -1,4 +1,4 @@
-// Seeded synthetic graphs built directly in HBM (RMAT, 2-D grid).
+// Seeded synthetic graphs built directly in HBM (RMAT, Chung-Lu, 2-D grid).
 // The arithmetic mirrors the oracle's CPU twin exactly (integer quadrant
 // thresholds, splitmix64 counters), so both build the same CSR.
 #include <cub/device/device_radix_sort.cuh>
@@ -103,6 +103,91 @@ __global__ void k_grid_fill(uint32_t rows, uint32_t cols, const uint32_t* __rest
     }
 }
 
+// ------------------------------------------------------------- Chung-Lu
+// Vertex i (before the id permutation) has weight floor(2^40 / (i + i0)), so
+// the expected degree of the rank-i vertex falls as 1 / (i + i0): a power law
+// whose degree distribution has exponent 2 (Zipf rank exponent 1), with the
+// largest expected degree set by i0.  Each draw picks both endpoints with
+// probability proportional to weight, from the exact integer prefix sums
+// (cum[j] = sum of the weights below j), so the CPU twin draws the same
+// edges; the affine maps a*x+b mod V spread out-hubs and in-hubs over the
+// id range independently.
+
+__global__ void k_cl_weights(uint32_t V, uint64_t i0, uint64_t* w)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < V; i += gridDim.x * blockDim.x)
+        w[i] = (1ull << 40) / ((uint64_t)i + i0);
+}
+
+// Largest j < V with cum[j] <= r (cum[0] = 0 <= r < cum[V]): an analytic
+// guess from the inverse of the weight integral, then an exact galloping
+// and binary search against the table.
+__device__ __forceinline__ uint32_t cl_pick(uint64_t r, const uint64_t* __restrict__ cum, uint32_t V, double i0)
+{
+    const double g = i0 * exp((double)r * (1.0 / 1099511627776.0)) - i0;
+    uint32_t j = (uint32_t)fmin(fmax(g, 0.0), (double)(V - 1));
+    uint32_t lo, hi;  // cum[lo] <= r < cum[hi]
+    if (cum[j] <= r) {
+        lo = j;
+        uint32_t step = 1;
+        hi = min(V, j + 1);
+        while (hi < V && cum[hi] <= r) {
+            lo = hi;
+            step *= 2;
+            hi = (uint32_t)min((uint64_t)V, (uint64_t)lo + step);
+        }
+    } else {
+        hi = j;
+        uint32_t step = 1;
+        lo = j > 0 ? j - 1 : 0;
+        while (lo > 0 && cum[lo] > r) {
+            hi = lo;
+            step *= 2;
+            lo = lo > step ? lo - step : 0;
+        }
+    }
+    while (hi - lo > 1) {
+        const uint32_t mid = lo + (hi - lo) / 2;
+        if (cum[mid] <= r) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void k_cl_keys(uint32_t V, uint64_t n, const uint64_t* __restrict__ cum, double i0, uint64_t s_out,
+                          uint64_t s_in, uint64_t a_out, uint64_t b_out, uint64_t a_in, uint64_t b_in, int sym,
+                          uint64_t* keys)
+{
+    const uint64_t W = cum[V];
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t hi = mix64(i);
+        const uint64_t x = cl_pick(mix64(s_out ^ hi) % W, cum, V, i0);
+        const uint64_t y = cl_pick(mix64(s_in ^ hi) % W, cum, V, i0);
+        const uint64_t u = (a_out * x + b_out) % V, v = (a_in * y + b_in) % V;
+        const bool loop = u == v;
+        keys[i] = loop ? kSentinel : ((u << 32) | v);
+        if (sym) keys[n + i] = loop ? kSentinel : ((v << 32) | u);
+    }
+}
+
+static uint64_t gcd64(uint64_t a, uint64_t b)
+{
+    while (b) {
+        const uint64_t t = a % b;
+        a = b;
+        b = t;
+    }
+    return a;
+}
+
+// Affine bijection of [0, V): multiplier coprime with V, both from the seed.
+static void cl_affine(uint32_t V, uint64_t seed, uint64_t tag, uint64_t& a, uint64_t& b)
+{
+    a = V > 1 ? 1 + mix64(seed ^ tag) % (V - 1) : 1;
+    while (gcd64(a, V) != 1) a = a % (V - 1) + 1;
+    b = mix64(seed ^ (tag + 1)) % V;
+}
+
 static void* galloc(size_t bytes)
 {
     void* p = nullptr;
@@ -164,6 +249,89 @@ cgb_graph* gen_rmat(uint32_t scale, uint32_t ef, uint64_t seed, double a, double
         cudaFree(keys);
         cudaFree(alt);
         cudaFree(cnt);
+        if (temp) cudaFree(temp);
+        cudaStreamDestroy(st);
+        if (g) graph_free(g);
+        throw;
+    }
+    cudaFree(keys);
+    cudaFree(alt);
+    cudaFree(cnt);
+    cudaFree(temp);
+    cudaStreamDestroy(st);
+    compute_weight_sum(g);
+    return g;
+}
+
+cgb_graph* gen_chunglu(uint32_t V, uint64_t draws, uint32_t i0, uint64_t seed, int sym, uint32_t wmax, int device)
+{
+    CGB_REQUIRE(V >= 2 && V < 0xFFFFFFFFu && i0 >= 1, CGB_EINVAL, "Chung-Lu needs V >= 2 and weight offset >= 1");
+    const uint64_t total = sym ? 2 * draws : draws;
+    CGB_CUDA_TRY(cudaSetDevice(device));
+    uint64_t a_out, b_out, a_in, b_in;
+    cl_affine(V, seed, 0xC1A0011ull, a_out, b_out);
+    cl_affine(V, seed, 0xC1A0021ull, a_in, b_in);
+    uint32_t bits = 1;
+    while (bits < 32 && (1ull << bits) < V) bits++;
+    cudaStream_t st;
+    CGB_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    uint64_t* cum = nullptr;
+    uint64_t* keys = nullptr;
+    uint64_t* alt = nullptr;
+    uint64_t* cnt = nullptr;
+    void* temp = nullptr;
+    cgb_graph* g = nullptr;
+    try {
+        // exact integer prefix sums of the weights (cum[V] = total weight)
+        cum = (uint64_t*)galloc(((size_t)V + 1) * 8);
+        uint64_t* wts = (uint64_t*)galloc(((size_t)V + 1) * 8);
+        k_cl_weights<<<kNumSMs * 8, kBlock, 0, st>>>(V, i0, wts);
+        CGB_CUDA_TRY(cudaMemsetAsync(wts + V, 0, 8, st));
+        size_t tb = 0;
+        CGB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb, wts, cum, (uint64_t)V + 1, st));
+        void* stemp = galloc(tb);
+        CGB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(stemp, tb, wts, cum, (uint64_t)V + 1, st));
+        CGB_CUDA_TRY(cudaStreamSynchronize(st));
+        cudaFree(stemp);
+        cudaFree(wts);
+        keys = (uint64_t*)galloc(total * 8);
+        k_cl_keys<<<kNumSMs * 16, kBlock, 0, st>>>(V, draws, cum, (double)i0, mix64(seed ^ 0xC1A0001ull),
+                                                   mix64(seed ^ 0xC1A0002ull), a_out, b_out, a_in, b_in, sym, keys);
+        CGB_CUDA_TRY(cudaStreamSynchronize(st));
+        cudaFree(cum);
+        cum = nullptr;
+        alt = (uint64_t*)galloc(total * 8);
+        cnt = (uint64_t*)galloc(8);
+        cub::DoubleBuffer<uint64_t> db(keys, alt);
+        size_t tb1 = 0, tb2 = 0;
+        CGB_CUDA_TRY(cub::DeviceRadixSort::SortKeys(nullptr, tb1, db, total, 0, 32 + (int)bits, st));
+        CGB_CUDA_TRY(cub::DeviceSelect::Unique(nullptr, tb2, keys, alt, cnt, total, st));
+        temp = galloc(std::max(tb1, tb2));
+        CGB_CUDA_TRY(cub::DeviceRadixSort::SortKeys(temp, tb1, db, total, 0, 32 + (int)bits, st));
+        uint64_t* in_unique = db.Current();
+        uint64_t* out_unique = db.Alternate();
+        CGB_CUDA_TRY(cub::DeviceSelect::Unique(temp, tb2, in_unique, out_unique, cnt, total, st));
+        uint64_t m = 0, last = 0;
+        CGB_CUDA_TRY(cudaMemcpyAsync(&m, cnt, 8, cudaMemcpyDeviceToHost, st));
+        CGB_CUDA_TRY(cudaStreamSynchronize(st));
+        if (m) {
+            CGB_CUDA_TRY(cudaMemcpyAsync(&last, out_unique + m - 1, 8, cudaMemcpyDeviceToHost, st));
+            CGB_CUDA_TRY(cudaStreamSynchronize(st));
+            if (last == kSentinel) m--;
+        }
+        CGB_REQUIRE(m < 0xFFFFFFFFull, CGB_EUNSUPPORTED, "Chung-Lu graph has >= 2^32 edges");
+        g = graph_alloc(V, (uint32_t)m, V, device, wmax > 0);
+        k_keys_to_csr<<<kNumSMs * 16, kBlock, 0, st>>>(V, m, out_unique, g->off, g->dst);
+        if (wmax)
+            k_edge_weights<<<kNumSMs * 16, kBlock, 0, st>>>(V, (uint32_t)m, g->off, g->dst, mix64(seed ^ 0x77E16ull),
+                                                            wmax, sym, g->w);
+        CGB_CUDA_TRY(cudaStreamSynchronize(st));
+        if (sym) g->symmetric = 1;
+    } catch (...) {
+        if (cum) cudaFree(cum);
+        if (keys) cudaFree(keys);
+        if (alt) cudaFree(alt);
+        if (cnt) cudaFree(cnt);
         if (temp) cudaFree(temp);
         cudaStreamDestroy(st);
         if (g) graph_free(g);

@@ -129,6 +129,20 @@ def _u32(a):
     return np.ascontiguousarray(a, dtype=np.uint32)
 
 
+def chunglu_weight_offset(vertices: int, draws: int, max_degree: int) -> int:
+    """Weight offset i0 of cgb_gen_chunglu whose largest expected degree,
+    draws / (i0 * ln((vertices + i0) / i0)), is closest to max_degree."""
+    import math
+    best, err = 1, None
+    for i0 in range(1, 1 << 20):
+        d = draws / (i0 * math.log((vertices + i0) / i0))
+        e = abs(d - max_degree)
+        if err is not None and e > err:
+            break
+        best, err = i0, e
+    return best
+
+
 DEFAULT_TUNING = {"push_big_deg": 512, "push_chunk": 1024, "push_ctas_per_sm": 8, "persist_enter": 1 << 15,
                   "persist_deg": 2048, "ms_edges": 256, "pr_unroll": 16, "pr_ctas_per_sm": 128}
 
@@ -201,6 +215,15 @@ class Graph:
     def grid(cls, rows: int, cols: int, seed: int = 1, wmax: int = 1000, device: int = 0) -> "Graph":
         h = ctypes.c_void_p()
         check(L.lib().cgb_gen_grid(rows, cols, seed, wmax, device, ctypes.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def chunglu(cls, vertices: int, draws: int, weight_offset: int, seed: int = 1, symmetrise: bool = False,
+                wmax: int = 64, device: int = 0) -> "Graph":
+        """Seeded Chung-Lu power-law graph (cgb_gen_chunglu)."""
+        h = ctypes.c_void_p()
+        check(L.lib().cgb_gen_chunglu(vertices, draws, weight_offset, seed, int(symmetrise), wmax, device,
+                                      ctypes.byref(h)))
         return cls(h.value)
 
     # ---- queries

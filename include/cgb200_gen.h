@@ -24,6 +24,14 @@ extern "C" {
 cgb_status cgb_gen_rmat(uint32_t scale, uint32_t edge_factor, uint64_t seed, double a, double b, double c,
                         int scramble, int symmetrise, uint32_t wmax, int device, cgb_graph** out);
 
+/* Chung-Lu power-law graph: `draws` edges whose endpoints are both drawn
+ * with probability proportional to a vertex weight floor(2^40 / (i + i0))
+ * (rank-i expected degree ~ 1 / (i + i0): degree-distribution exponent 2,
+ * largest expected degree set by weight_offset = i0), out- and in-ranks
+ * spread over the ids by two seeded affine permutations; self-loops and
+ * duplicates removed, optionally symmetrised, weights as for RMAT. */
+cgb_status cgb_gen_chunglu(uint32_t vertices, uint64_t draws, uint32_t weight_offset, uint64_t seed, int symmetrise,
+                           uint32_t wmax, int device, cgb_graph** out);
 /* rows x cols 4-neighbour grid (undirected), weights uniform in [1, wmax]. */
 cgb_status cgb_gen_grid(uint32_t rows, uint32_t cols, uint64_t seed, uint32_t wmax, int device, cgb_graph** out);
 

@@ -278,6 +278,53 @@ void ora_rmat_edges(uint32_t scale, uint64_t nedges, uint64_t seed, uint64_t t1,
     }
 }
 
+static uint64_t gcd_u64(uint64_t a, uint64_t b)
+{
+    while (b) { uint64_t t = a % b; a = b; b = t; }
+    return a;
+}
+
+static void cl_affine(uint32_t V, uint64_t seed, uint64_t tag, uint64_t* a, uint64_t* b)
+{
+    *a = V > 1 ? 1 + mix64(seed ^ tag) % (V - 1) : 1;
+    while (gcd_u64(*a, V) != 1) *a = *a % (V - 1) + 1;
+    *b = mix64(seed ^ (tag + 1)) % V;
+}
+
+/* Largest j < V with cum[j] <= r. */
+static uint32_t cl_pick(uint64_t r, const uint64_t* cum, uint32_t V)
+{
+    uint32_t lo = 0, hi = V;
+    while (hi - lo > 1) {
+        uint32_t mid = lo + (hi - lo) / 2;
+        if (cum[mid] <= r) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+/* Chung-Lu edge stream of the device generator (gen.cu): vertex weights
+ * floor(2^40 / (i + i0)), both endpoints drawn from the integer prefix sums
+ * with counter-hashed draws, then mapped by two affine permutations. */
+int ora_chunglu_edges(uint32_t V, uint64_t n, uint32_t i0, uint64_t seed, uint32_t* src, uint32_t* dst)
+{
+    uint64_t* cum = (uint64_t*)malloc(sizeof(uint64_t) * ((size_t)V + 1));
+    if (!cum) return -1;
+    cum[0] = 0;
+    for (uint32_t i = 0; i < V; i++) cum[i + 1] = cum[i] + (1ull << 40) / ((uint64_t)i + i0);
+    uint64_t a_out, b_out, a_in, b_in;
+    cl_affine(V, seed, 0xC1A0011ull, &a_out, &b_out);
+    cl_affine(V, seed, 0xC1A0021ull, &a_in, &b_in);
+    uint64_t s_out = mix64(seed ^ 0xC1A0001ull), s_in = mix64(seed ^ 0xC1A0002ull), W = cum[V];
+    for (uint64_t i = 0; i < n; i++) {
+        uint64_t h = mix64(i);
+        uint64_t x = cl_pick(mix64(s_out ^ h) % W, cum, V), y = cl_pick(mix64(s_in ^ h) % W, cum, V);
+        src[i] = (uint32_t)((a_out * x + b_out) % V);
+        dst[i] = (uint32_t)((a_in * y + b_in) % V);
+    }
+    free(cum);
+    return 0;
+}
+
 static int cmp_u64(const void* a, const void* b)
 {
     uint64_t x = *(const uint64_t*)a, y = *(const uint64_t*)b;

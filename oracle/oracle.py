@@ -69,6 +69,9 @@ def lib():
         L.ora_rmat_edges.argtypes = [ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64,
                                      ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, _u32p, _u32p]
         L.ora_build_csr.argtypes = [ctypes.c_uint32, ctypes.c_uint64, _u32p, _u32p, ctypes.c_int, _u32p, _u32p]
+        L.ora_chunglu_edges.argtypes = [ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint64, _u32p,
+                                        _u32p]
+        L.ora_chunglu_edges.restype = ctypes.c_int
         L.ora_build_csr.restype = ctypes.c_int64
         L.ora_edge_weights.argtypes = [ctypes.c_uint32, _u32p, _u32p, ctypes.c_uint64, ctypes.c_uint32,
                                        ctypes.c_int, _u32p]
@@ -193,6 +196,17 @@ def rmat_graph(scale, edge_factor=16, seed=1, symmetrise=False, wmax=64, scrambl
     """(off, dst, w) of the seeded RMAT graph, exactly as the engine builds it."""
     src, dst = rmat_edges(scale, edge_factor, seed, scramble)
     off, d = build_csr(1 << scale, src, dst, symmetrise)
+    w = edge_weights(off, d, seed, wmax, sym_key=symmetrise)
+    return off, d, w
+
+
+def chunglu_graph(V, draws, weight_offset, seed=1, symmetrise=False, wmax=64):
+    """(off, dst, w) of the seeded Chung-Lu graph, exactly as the engine
+    builds it (cggraph_b200/csrc/gen.cu gen_chunglu)."""
+    src = np.empty(draws, np.uint32)
+    dst = np.empty(draws, np.uint32)
+    assert lib().ora_chunglu_edges(V, draws, weight_offset, seed, _p(src), _p(dst)) == 0
+    off, d = build_csr(V, src, dst, symmetrise)
     w = edge_weights(off, d, seed, wmax, sym_key=symmetrise)
     return off, d, w
 

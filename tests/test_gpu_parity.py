@@ -94,6 +94,25 @@ def test_rmat16_all_algorithms(oracle, sym):
         pr_close(got, oracle.pagerank(off, dst, 20))
 
 
+@pytest.mark.parametrize("sym", [False, True])
+def test_chunglu_generator_and_algorithms(oracle, sym):
+    """Chung-Lu power-law graph (non-power-of-two V): the device generator
+    equals its CPU twin bit for bit, and all four algorithms match the oracle."""
+    V, n, i0 = 20011, 300000, 5
+    off, dst, w = oracle.chunglu_graph(V, n, i0, seed=11, symmetrise=sym)
+    with cg.Graph.chunglu(V, n, i0, seed=11, symmetrise=sym) as g:
+        o2, d2, w2 = g.download()
+        np.testing.assert_array_equal(o2, off)
+        np.testing.assert_array_equal(d2, dst)
+        np.testing.assert_array_equal(w2, w)
+        deg = np.diff(off.astype(np.int64))
+        for r in (int(deg.argmax()), int(np.nonzero(deg)[0][5])):
+            np.testing.assert_array_equal(g.run(BFS, r)[0], oracle.bfs(off, dst, r))
+            np.testing.assert_array_equal(g.run(SSSP, r)[0], oracle.sssp(off, dst, w, r))
+        np.testing.assert_array_equal(g.run(CC)[0], oracle.cc(off, dst))
+        pr_close(g.run(PR, 20)[0], oracle.pagerank(off, dst, 20))
+
+
 def test_grid_high_diameter(oracle):
     off, dst, w = oracle.grid_graph(60, 90, seed=4)
     with cg.Graph.from_csr(off, dst, w) as g:

@@ -89,3 +89,24 @@ def test_generator_twin_properties(oracle):
             np.testing.assert_array_equal(w[order], w)
     off, dst, w = oracle.grid_graph(5, 7)
     assert off.size == 36 and dst.size == 2 * (5 * 6 + 4 * 7)
+
+
+def test_chunglu_twin_properties(oracle):
+    """The CPU twin of the Chung-Lu generator: deterministic for a seed,
+    sorted self-loop-free lists, and a largest degree near the expected
+    draws / (i0 ln((V + i0) / i0))."""
+    import math
+    V, n, i0 = 20011, 300000, 5
+    off, dst, w = oracle.chunglu_graph(V, n, i0, seed=7)
+    off2, dst2, w2 = oracle.chunglu_graph(V, n, i0, seed=7)
+    assert np.array_equal(off, off2) and np.array_equal(dst, dst2) and np.array_equal(w, w2)
+    deg = np.diff(off.astype(np.int64))
+    src = np.repeat(np.arange(V), deg)
+    assert (src != dst).all()
+    key = src * V + dst
+    assert (np.diff(key) > 0).all()
+    expect = n / (i0 * math.log((V + i0) / i0))
+    assert expect / 4 < deg.max() < expect * 1.5  # duplicates to in-hubs are removed
+    assert w.min() >= 1 and w.max() <= 64
+    offs, dsts, _ = oracle.chunglu_graph(V, n, i0, seed=7, symmetrise=True)
+    assert dsts.size >= dst.size
