@@ -62,6 +62,10 @@ def parse_args():
                    help="keep the default launch parameters (else cgb_autotune per algorithm, untimed)")
     p.add_argument("--no-batching", action="store_true", help="skip the multi-root and graph-batch section")
     p.add_argument("--no-serving", action="store_true", help="skip the request-server section")
+    p.add_argument("--no-shapes", action="store_true",
+                   help="skip the skewed / high-diameter shapes (Chung-Lu 41.6 M / 1.47 B, 4800 x 5000 grid)")
+    p.add_argument("--shapes-scale", type=float, default=1.0,
+                   help="fraction of the Chung-Lu vertices and draws (1.0 = 41.6 M / 1.47 B)")
     p.add_argument("--serve-scale", type=int, default=25, help="RMAT scale of the served graph")
     p.add_argument("--serve-requests", type=int, default=256, help="queries per arrival rate")
     p.add_argument("--algorithms", default="bfs,sssp,cc,pr",
@@ -322,6 +326,9 @@ def bench_cgb200(args, d: Dist):
     serving = None
     if d.world == 1 and not args.no_serving and (BFS in algs or SSSP in algs):
         serving = bench_serving(args, cg, L, dev)
+    shapes = None
+    if d.world == 1 and not args.no_shapes and algs == [BFS, SSSP, CC, PR]:
+        shapes = bench_shapes(args, cg, L, dev)
     result = {
         "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": d.world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -342,6 +349,7 @@ def bench_cgb200(args, d: Dist):
         "autotune": autotune,
         "batching": batching,
         "serving": serving,
+        "shapes": shapes,
         "roofline": roof,
         "cpu_baseline": cpu,
         "e2e": e2e,
@@ -462,6 +470,60 @@ def bench_batching(args, cg, L, gd, roots, dev):
         out["graphs256"] = res
     for h in graphs:
         h.close()
+    return out
+
+
+def bench_shapes(args, cg, L, dev):
+    """Skewed and high-diameter shapes, all four algorithms under the plain
+    heuristic schedule: a Chung-Lu power-law directed graph of 41.6 M
+    vertices and 1.47 B edge draws (degree-distribution exponent 2, largest
+    expected degree about 3 M, weights [1,64]; its symmetrised copy for CC),
+    and the 4800 x 5000 grid (weights [1,1000]).  One untimed run, then the
+    best of two; GTEPS numerators as in the main line."""
+    out = {}
+
+    def best2(g, alg, arg):
+        g.run(alg, arg, to_host=False)
+        ms = []
+        for _ in range(2):
+            g.run(alg, arg, to_host=False)
+            ms.append(g.stats().ms)
+        return min(ms), g.stats().traversed_edges
+
+    Vc = int(41_600_000 * args.shapes_scale)
+    draws = int(1_470_000_000 * args.shapes_scale)
+    i0 = cg.chunglu_weight_offset(Vc, draws, int(3_000_000 * args.shapes_scale) or 1)
+    t0 = time.perf_counter()
+    g = cg.Graph.chunglu(Vc, draws, i0, seed=args.seed, wmax=64, device=dev)
+    gen_s = time.perf_counter() - t0
+    off_h, _, _ = g.download(with_weight=False)
+    deg = np.diff(off_h.astype(np.int64))
+    roots = pick_roots(off_h, args.seed + 23, 2)
+    res = {"vertices": g.vertexNum, "draws": draws, "edges": g.edgeNum, "weight_offset": i0,
+           "max_out_degree": int(deg.max()), "generate_s": gen_s}
+    for alg in (BFS, SSSP):
+        tot_ms = tot_e = 0
+        for r in roots:
+            ms, e = best2(g, alg, r)
+            tot_ms += ms
+            tot_e += e
+        res[ALG_NAMES[alg]] = {"ms_per_run": tot_ms / len(roots), "gteps": tot_e / tot_ms / 1e6}
+    ms, e = best2(g, PR, args.pr_iters)
+    res["pagerank"] = {"ms_per_run": ms, "gteps": e / ms / 1e6}
+    g.close()
+    s = cg.Graph.chunglu(Vc, draws, i0, seed=args.seed, symmetrise=True, wmax=0, device=dev)
+    ms, e = best2(s, CC, 0)
+    res["cc"] = {"ms_per_run": ms, "gteps": e / ms / 1e6, "edges_symmetrised": s.edgeNum}
+    s.close()
+    out["chunglu"] = res
+    if args.shapes_scale >= 1.0:
+        gr = cg.Graph.grid(4800, 5000, seed=1, device=dev)
+        res = {"vertices": gr.vertexNum, "edges": gr.edgeNum}
+        for alg, arg in ((BFS, 0), (SSSP, 0), (CC, 0), (PR, args.pr_iters)):
+            ms, e = best2(gr, alg, arg)
+            res[ALG_NAMES[alg]] = {"ms_per_run": ms, "gteps": e / ms / 1e6}
+        gr.close()
+        out["grid4800x5000"] = res
     return out
 
 

@@ -130,17 +130,34 @@ def _u32(a):
 
 
 def chunglu_weight_offset(vertices: int, draws: int, max_degree: int) -> int:
-    """Weight offset i0 of cgb_gen_chunglu whose largest expected degree,
-    draws / (i0 * ln((vertices + i0) / i0)), is closest to max_degree."""
-    import math
-    best, err = 1, None
-    for i0 in range(1, 1 << 20):
-        d = draws / (i0 * math.log((vertices + i0) / i0))
-        e = abs(d - max_degree)
-        if err is not None and e > err:
-            break
-        best, err = i0, e
-    return best
+    """Weight offset i0 of cgb_gen_chunglu whose top vertex has about
+    max_degree distinct out-neighbours.  Its draws D0 = draws * p0 land on
+    targets j with probability p_j (p proportional to 1 / (j + i0)), so the
+    expected distinct count is sum_j 1 - (1 - p_j)^D0; it falls as i0 grows,
+    and i0 is found by bisection."""
+    # ranks in geometric bins (p_j varies slowly inside one), the first 4096 one by one
+    edges = np.unique(np.concatenate([np.arange(min(4096, vertices)),
+                                      np.geomspace(min(4096, vertices), vertices, 4000).astype(np.int64),
+                                      [vertices]]))
+    mid = (edges[:-1] + edges[1:] - 1) / 2.0
+    width = np.diff(edges).astype(np.float64)
+
+    def distinct(i0):
+        total = float(np.sum(width / (mid + i0)))  # sum of the weights 1 / (j + i0)
+        p = 1.0 / (mid + i0) / total
+        d0 = draws * (1.0 / i0) / total
+        return float(np.sum(width * -np.expm1(d0 * np.log1p(-p))))
+
+    lo, hi = 1, 4096
+    if distinct(lo) <= max_degree:
+        return lo
+    while hi - lo > 1:
+        m = (lo + hi) // 2
+        if distinct(m) > max_degree:
+            lo = m
+        else:
+            hi = m
+    return lo if abs(distinct(lo) - max_degree) < abs(distinct(hi) - max_degree) else hi
 
 
 DEFAULT_TUNING = {"push_big_deg": 512, "push_chunk": 1024, "push_ctas_per_sm": 8, "persist_enter": 1 << 15,

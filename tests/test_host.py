@@ -53,3 +53,16 @@ def test_only_single_gpu_engine_is_provided():
     csr = cg.CSR_Result_type(2, 1, np.array([0, 1, 1], np.uint32), np.array([1], np.uint32), None)
     with pytest.raises(CgbError, match="SINGLE_GPU"):
         cg.main_partition(csr, cg.Algorithm_type.BFS, 0, engine_type=cg.Engine_type.COORDINATION)
+
+
+def test_chunglu_weight_offset_matches_twin(oracle):
+    """The offset helper's distinct-degree estimate against the CPU twin's
+    actual largest out-degree."""
+    import numpy as np
+    import cggraph_b200 as cg
+    V, n = 20011, 300000
+    i0 = cg.chunglu_weight_offset(V, n, 3000)
+    off, _, _ = oracle.chunglu_graph(V, n, i0, seed=3)
+    top = int(np.diff(off.astype(np.int64)).max())
+    assert 0.8 * 3000 < top < 1.25 * 3000
+    assert cg.chunglu_weight_offset(V, n, 100) > cg.chunglu_weight_offset(V, n, 3000)
