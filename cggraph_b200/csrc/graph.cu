@@ -16,18 +16,66 @@ void set_error(const std::string& msg) { t_last_error = msg; }
 const std::string& last_error() { return t_last_error; }
 
 // --------------------------------------------------------------- allocation
+// Graph buffers come from one stream-ordered memory pool per device that
+// keeps freed memory cached (release threshold: never), so creating a graph
+// after destroying another reuses the same pages: plain cudaFree of tens of
+// GB returns them to the driver and can stall for hundreds of milliseconds.
+// dalloc waits for its allocation, so the memory is usable on every stream;
+// dfree keeps cudaFree's device-wide synchronisation before the release.
+namespace {
+struct DevicePool {
+    cudaMemPool_t pool = nullptr;
+    cudaStream_t stream = nullptr;
+};
+std::mutex g_pool_mu;
+DevicePool g_pools[64];
+
+DevicePool& device_pool()
+{
+    int dev = 0;
+    CGB_CUDA_TRY(cudaGetDevice(&dev));
+    CGB_REQUIRE(dev >= 0 && dev < 64, CGB_EUNSUPPORTED, "device index >= 64");
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    DevicePool& p = g_pools[dev];
+    if (!p.pool) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        CGB_CUDA_TRY(cudaMemPoolCreate(&p.pool, &props));
+        uint64_t keep = ~0ull;
+        CGB_CUDA_TRY(cudaMemPoolSetAttribute(p.pool, cudaMemPoolAttrReleaseThreshold, &keep));
+        CGB_CUDA_TRY(cudaStreamCreateWithFlags(&p.stream, cudaStreamNonBlocking));
+    }
+    return p;
+}
+}  // namespace
+
 template <typename T>
 static T* dalloc(size_t n)
 {
     void* p = nullptr;
     if (n == 0) n = 1;
-    CGB_CUDA_TRY(cudaMalloc(&p, n * sizeof(T)));
+    DevicePool& dp = device_pool();
+    CGB_CUDA_TRY(cudaMallocFromPoolAsync(&p, n * sizeof(T), dp.pool, dp.stream));
+    CGB_CUDA_TRY(cudaStreamSynchronize(dp.stream));
     return (T*)p;
 }
 
 static void dfree(void* p)
 {
-    if (p) cudaFree(p);
+    if (!p) return;
+    DevicePool& dp = device_pool();
+    cudaDeviceSynchronize();  // as cudaFree: nothing may still use p
+    cudaFreeAsync(p, dp.stream);
+}
+
+void memory_trim(int device)
+{
+    CGB_CUDA_TRY(cudaSetDevice(device));
+    DevicePool& dp = device_pool();
+    CGB_CUDA_TRY(cudaStreamSynchronize(dp.stream));
+    CGB_CUDA_TRY(cudaMemPoolTrimTo(dp.pool, 0));
 }
 
 static uint32_t bits_for(uint64_t n)  // bits to represent values < n

@@ -192,6 +192,10 @@ cgb_status cgb_run_stats_get(const cgb_graph* g, cgb_run_stats* out);
  * receives the number available. */
 cgb_status cgb_trace_get(const cgb_graph* g, cgb_iter_trace* out, uint32_t max_entries, uint32_t* count);
 
+/* Graph buffers come from a per-device memory pool that keeps freed memory
+ * for the next graph; this returns the cached memory to the driver. */
+cgb_status cgb_memory_trim(int device);
+
 /* ------------------------------------------------------------ tuning */
 
 /* Launch parameters of a graph's kernels, one set per algorithm.  They

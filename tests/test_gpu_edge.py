@@ -180,3 +180,16 @@ def test_device_buffers_in_and_out(oracle):
         pin = torch.empty(off.size - 1, dtype=torch.int32).pin_memory()
         g.run(BFS, 3, out=pin)
         np.testing.assert_array_equal(pin.numpy().view(np.uint32), oracle.bfs(off, dst, 3))
+
+
+def test_memory_pool_reuse_and_trim(oracle):
+    """Graph buffers come from a caching pool: graphs created after others
+    are destroyed, and after the pool is trimmed, still compute correctly."""
+    from cggraph_b200 import _lib as L
+    off, dst, w = oracle.rmat_graph(12, 8, seed=4)
+    exp = oracle.bfs(off, dst, 3)
+    for trim in (False, True, False):
+        with cg.Graph.from_csr(off, dst, w) as g:
+            np.testing.assert_array_equal(g.run(0, 3)[0], exp)
+        if trim:
+            L.check(L.lib().cgb_memory_trim(0))
