@@ -106,13 +106,14 @@ class Tuning(ctypes.Structure):
         ("ms_edges", ctypes.c_uint32),
         ("pr_unroll", ctypes.c_uint32),
         ("pr_ctas_per_sm", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32 * 7),
+        ("persist_ctas", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 6),
     ]
 
 
 TUNE_BATCH, TUNE_KEEP_DEFAULT = 0x1, 0x2
 TUNING_FIELDS = ("push_big_deg", "push_chunk", "push_ctas_per_sm", "persist_enter", "persist_deg", "ms_edges",
-                 "pr_unroll", "pr_ctas_per_sm")
+                 "pr_unroll", "pr_ctas_per_sm", "persist_ctas")
 
 
 class ServerConfig(ctypes.Structure):

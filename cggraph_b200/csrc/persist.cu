@@ -356,8 +356,9 @@ PersistResult bfs_persistent(cgb_graph* g, uint32_t cur, uint32_t nf, unsigned l
 {
     PersistState* st = persist_state(g);
     init_state(g, nf, scout, max_deg);
-    static uint32_t grid = 0;
-    if (!grid) grid = cooperative_grid(k_bfs_persistent);
+    static uint32_t full = 0;
+    if (!full) full = cooperative_grid(k_bfs_persistent);
+    const uint32_t grid = g->tune.persist_ctas ? std::min(g->tune.persist_ctas, full) : full;
     uint32_t cap = g->V, nz = g->nz;
     void* args[] = {&g->off, &g->dst, &g->value, &g->visited, &g->q[0], &g->q[1], &cap, &nz, &level, &cur, &nf_exit,
                     &scout_exit, &deg_exit, &max_levels, &st};
@@ -386,14 +387,16 @@ PersistResult sssp_persistent(cgb_graph* g, uint32_t cur, uint32_t nf, uint32_t 
     uint32_t cap = g->V, nz = g->nz;
     ++g->stats.launches;
     if (g->w) {
-        static uint32_t grid = 0;
-        if (!grid) grid = cooperative_grid(k_sssp_persistent<true>);
+        static uint32_t full = 0;
+        if (!full) full = cooperative_grid(k_sssp_persistent<true>);
+        const uint32_t grid = g->tune.persist_ctas ? std::min(g->tune.persist_ctas, full) : full;
         void* args[] = {&g->off, &g->dst, &g->w, &g->value, &g->aux_bm, (void*)&words, &far_bm, &g->q[0], &g->q[1],
                         &cap, &nz, &thr, &cur, &nf_exit, &max_rounds, &g->ctr, &st};
         CGB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_sssp_persistent<true>, grid, kBlock, args, 0, g->stream));
     } else {
-        static uint32_t grid = 0;
-        if (!grid) grid = cooperative_grid(k_sssp_persistent<false>);
+        static uint32_t full = 0;
+        if (!full) full = cooperative_grid(k_sssp_persistent<false>);
+        const uint32_t grid = g->tune.persist_ctas ? std::min(g->tune.persist_ctas, full) : full;
         void* args[] = {&g->off, &g->dst, &g->w, &g->value, &g->aux_bm, (void*)&words, &far_bm, &g->q[0], &g->q[1],
                         &cap, &nz, &thr, &cur, &nf_exit, &max_rounds, &g->ctr, &st};
         CGB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_sssp_persistent<false>, grid, kBlock, args, 0, g->stream));

@@ -48,6 +48,39 @@ __device__ __forceinline__ void fine_tier(const Op& op, uint32_t start, uint32_t
     }
 }
 
+// Fine-grained tier of one warp (no CTA barriers): a warp-inclusive scan of
+// the lanes' remaining degrees (each below 32) packs their lists into rounds
+// of 32 edges; in each round every lane takes one edge and finds the lane
+// that owns it -- the last lane whose exclusive prefix is <= the edge's
+// position -- by a 5-step shuffle search.  Called by all 32 lanes.
+template <class Op>
+__device__ __forceinline__ void fine_tier_warp(const Op& op, uint32_t start, uint32_t deg, uint32_t msg)
+{
+    const uint32_t lane = lane_id();
+    uint32_t incl = deg;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (uint32_t)o) incl += t;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    const uint32_t excl = incl - deg;
+    for (uint32_t base = 0; base < total; base += 32) {
+        const uint32_t idx = base + lane;
+        uint32_t o = 0;
+#pragma unroll
+        for (uint32_t step = 16; step >= 1; step >>= 1) {
+            const uint32_t ex = __shfl_sync(0xffffffffu, excl, o + step);
+            if (ex <= idx) o += step;
+        }
+        const uint32_t st = __shfl_sync(0xffffffffu, start, o);
+        const uint32_t ex = __shfl_sync(0xffffffffu, excl, o);
+        const uint32_t m = __shfl_sync(0xffffffffu, msg, o);
+        const bool valid = idx < total;
+        op.edge(valid, valid ? st + (idx - ex) : 0u, m);
+    }
+}
+
 // Op interface:
 //   __device__ bool load(uint32_t v, uint32_t& start, uint32_t& deg, uint32_t& msg) const;
 //   __device__ void edge(bool valid, uint32_t e, uint32_t msg) const;   // warp-collective
@@ -136,7 +169,7 @@ __global__ void __launch_bounds__(kBlock) k_push_huge(const uint32_t* __restrict
 // chunk queue; k_push_chunks then deals the chunks across the whole grid, so
 // a frontier of a few hubs keeps every SM busy however few vertices it has.
 // Lists of 32..big_deg-1 edges are walked by one warp, shorter ones by the
-// fine-grained tier.  Chunk-queue capacity E/chunk + E/big_deg + 64 bounds
+// warp's fine-grained tier (fine_tier_warp).  Chunk-queue capacity E/chunk + E/big_deg + 64 bounds
 // any frontier in which each vertex appears once (big_deg and chunk come
 // from the graph's cgb_tuning).
 template <class Op, bool kIdentity>
@@ -145,9 +178,6 @@ __global__ void __launch_bounds__(kBlock) k_push_binned(const uint32_t* __restri
                                                         uint32_t chunk_cap, uint32_t* overflow, uint32_t big_deg,
                                                         uint32_t chunk)
 {
-    __shared__ uint32_t s_scan[kBlock / 32 + 1];
-    __shared__ uint32_t s_edge[kBlock];
-    __shared__ uint32_t s_emsg[kBlock];
     op.block_begin();
     __syncthreads();
     for (uint32_t base = blockIdx.x * kBlock; base < nin; base += gridDim.x * kBlock) {
@@ -182,7 +212,7 @@ __global__ void __launch_bounds__(kBlock) k_push_binned(const uint32_t* __restri
             if (lane_id() == leader) deg = 0;
             for (uint32_t k = 0; k < dg; k += 32) op.edge(k + lane_id() < dg, st + k + lane_id(), m);
         }
-        fine_tier(op, start, deg, msg, s_scan, s_edge, s_emsg);
+        fine_tier_warp(op, start, deg, msg);
     }
     __syncthreads();
     op.block_end();

@@ -213,7 +213,9 @@ typedef struct {
     uint32_t pr_unroll;        /* PageRank pull: gathers in flight per lane (4, 8 or 16, default 16) */
     uint32_t pr_ctas_per_sm;   /* PageRank pull grid, CTAs per SM (1..1024, capped at one 32-row slice
                                   per warp; default 128) */
-    uint32_t reserved[7];
+    uint32_t persist_ctas;     /* CTAs of the device-resident loops (0 = one per SM, else 1..that;
+                                  fewer CTAs make each level's grid barrier cheaper) */
+    uint32_t reserved[6];
 } cgb_tuning;
 
 cgb_status cgb_tuning_get(const cgb_graph* g, int algorithm, cgb_tuning* out);

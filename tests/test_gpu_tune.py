@@ -15,7 +15,9 @@ TUNINGS = [
      "pr_unroll": 4, "pr_ctas_per_sm": 1},
     {"push_big_deg": 65536, "push_chunk": 65536, "push_ctas_per_sm": 32, "persist_enter": 1 << 30,
      "persist_deg": 65536, "ms_edges": 4096, "pr_unroll": 16, "pr_ctas_per_sm": 1024},
-    {"push_big_deg": 300, "push_chunk": 512, "push_ctas_per_sm": 3, "persist_enter": 100, "persist_deg": 64},
+    {"push_big_deg": 300, "push_chunk": 512, "push_ctas_per_sm": 3, "persist_enter": 100, "persist_deg": 64,
+     "persist_ctas": 5},
+    {"persist_ctas": 1},
 ]
 
 
