@@ -107,13 +107,14 @@ class Tuning(ctypes.Structure):
         ("pr_unroll", ctypes.c_uint32),
         ("pr_ctas_per_sm", ctypes.c_uint32),
         ("persist_ctas", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32 * 6),
+        ("sssp_pull_alpha", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 5),
     ]
 
 
 TUNE_BATCH, TUNE_KEEP_DEFAULT = 0x1, 0x2
 TUNING_FIELDS = ("push_big_deg", "push_chunk", "push_ctas_per_sm", "persist_enter", "persist_deg", "ms_edges",
-                 "pr_unroll", "pr_ctas_per_sm", "persist_ctas")
+                 "pr_unroll", "pr_ctas_per_sm", "persist_ctas", "sssp_pull_alpha")
 
 
 class ServerConfig(ctypes.Structure):

@@ -50,7 +50,7 @@ struct BfsTdOp {
         bool win = false;
         uint32_t d = 0;
         if (valid) {
-            d = dst[e];
+            d = __ldcs(dst + e);  // streamed once: evict first, keep the visited bitmap in L2
             const uint32_t bit = 1u << (d & 31u);
             uint32_t* wp = visited + (d >> 5);
             if (!(*wp & bit)) {

@@ -169,7 +169,7 @@ struct CcPropOp {
         bool enq = false;
         uint32_t d = 0;
         if (valid) {
-            d = dst[e];
+            d = __ldcs(dst + e);  // streamed once: evict first
             if (m < label[d]) {
                 const uint32_t old = atomicMin(label + d, m);
                 if (m < old && d < nz) enq = atomicExch(stamp + d, it) != it;

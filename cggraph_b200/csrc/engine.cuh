@@ -57,6 +57,7 @@ inline cgb_tuning default_tuning()
     t.ms_edges = 256;
     t.pr_unroll = 16;
     t.pr_ctas_per_sm = 128;
+    t.sssp_pull_alpha = 0;
     return t;
 }
 
@@ -84,6 +85,8 @@ struct cgb_graph {
     uint32_t* in_off = nullptr;
     uint32_t* in_src = nullptr;
     bool csc_owned = false;
+    uint32_t* in_w = nullptr;  // weights in CSC order (SSSP pull rounds); may alias w
+    bool in_w_owned = false;
     int symmetric = -1;
 
     // PageRank layout: vertices relabelled by out-degree bucket (stable; zero
@@ -186,6 +189,13 @@ void free_msbfs(cgb_graph* g);
 // n * V distances, root-major.
 void run_mssp(cgb_graph* g, const uint32_t* d_roots, uint32_t n, uint32_t* out, uint32_t delta);
 void free_mssp(cgb_graph* g);
+// Weights in CSC order (in_w); needs the graph's weights.
+void ensure_csc_weights(cgb_graph* g);
+// One pull round of SSSP over the near set q_in[0, nin) at bucket [lo, thr):
+// next near set to qout, new far vertices to far_bm; near_set is a scratch
+// bitmap (words()).  q_in is scratch afterwards.
+void sssp_pull_round(cgb_graph* g, const uint32_t* q_in, uint32_t nin, uint32_t lo, uint32_t thr, uint32_t* qout,
+                     uint32_t* qout_len, uint32_t* far_bm, uint32_t* near_set);
 uint32_t mssp_default_delta(cgb_graph* g);
 
 }  // namespace cgb

@@ -240,6 +240,23 @@ static void radix_sort_u64(cgb_graph* g, uint64_t*& keys, uint64_t*& alt, uint64
     if (db.Current() != keys) std::swap(keys, alt);
 }
 
+// Sorts n (key, value) pairs; on return keys / vals hold the sorted data.
+static void radix_sort_pairs(cgb_graph* g, uint64_t*& keys, uint64_t*& alt, uint32_t*& vals, uint32_t*& valt,
+                             uint64_t n, int end_bit)
+{
+    cub::DoubleBuffer<uint64_t> dk(keys, alt);
+    cub::DoubleBuffer<uint32_t> dv(vals, valt);
+    size_t temp_bytes = 0;
+    CGB_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, dk, dv, n, 0, end_bit, g->stream));
+    void* temp = dalloc<char>(temp_bytes);
+    cudaError_t err = cub::DeviceRadixSort::SortPairs(temp, temp_bytes, dk, dv, n, 0, end_bit, g->stream);
+    CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    dfree(temp);
+    CGB_CUDA_TRY(err);
+    if (dk.Current() != keys) std::swap(keys, alt);
+    if (dv.Current() != vals) std::swap(vals, valt);
+}
+
 // Sorts every neighbour list by destination, weights following
 // (nbrSort_taskSteal, my_project/CGgraph/sortNbr.hpp:8-99).
 static void sort_neighbours(cgb_graph* g)
@@ -363,7 +380,18 @@ static void build_transpose(cgb_graph* g)
         uint64_t* alt = dalloc<uint64_t>(E);
         const uint32_t grid = grid_for(E, kBlock, kNumSMs * 16);
         k_make_keys<<<grid, kBlock, 0, g->stream>>>(V, E, g->off, g->dst, b, keys, true);
-        radix_sort_u64(g, keys, alt, E, 2 * b);
+        if (g->w && !g->in_w) {
+            // weighted: the weights ride along, so SSSP pull rounds find them in CSC order
+            uint32_t* vals = dalloc<uint32_t>(E);
+            uint32_t* valt = dalloc<uint32_t>(E);
+            CGB_CUDA_TRY(cudaMemcpyAsync(vals, g->w, (size_t)E * 4, cudaMemcpyDeviceToDevice, g->stream));
+            radix_sort_pairs(g, keys, alt, vals, valt, E, 2 * b);
+            dfree(valt);
+            g->in_w = vals;
+            g->in_w_owned = true;
+        } else {
+            radix_sort_u64(g, keys, alt, E, 2 * b);
+        }
         k_split_keys<<<grid, kBlock, 0, g->stream>>>(E, keys, b, in_src);
         k_offsets_from_keys<<<grid_for((uint64_t)E + 1, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(V, E, keys, b,
                                                                                                        in_off);
@@ -410,6 +438,47 @@ void ensure_csc(cgb_graph* g)
         return;
     }
     build_transpose(g);
+}
+
+void ensure_csc_weights(cgb_graph* g)
+{
+    if (!g->w || g->in_w) return;
+    ensure_csc(g);
+    if (g->in_w) return;  // built with the transpose
+    // the CSR serves as CSC (symmetric structure): transpose the weights by
+    // sorting (dst, src) keys with the weights as values, then alias w when
+    // they are symmetric too
+    const uint32_t V = g->V, E = g->E, b = bits_for(V);
+    if (E == 0) {
+        g->in_w = g->w;
+        g->in_w_owned = false;
+        return;
+    }
+    uint64_t* keys = dalloc<uint64_t>(E);
+    uint64_t* alt = dalloc<uint64_t>(E);
+    uint32_t* vals = dalloc<uint32_t>(E);
+    uint32_t* valt = dalloc<uint32_t>(E);
+    k_make_keys<<<grid_for(E, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(V, E, g->off, g->dst, b, keys, true);
+    CGB_CUDA_TRY(cudaMemcpyAsync(vals, g->w, (size_t)E * 4, cudaMemcpyDeviceToDevice, g->stream));
+    radix_sort_pairs(g, keys, alt, vals, valt, E, 2 * b);
+    dfree(keys);
+    dfree(alt);
+    dfree(valt);
+    uint32_t* differ = dalloc<uint32_t>(1);
+    CGB_CUDA_TRY(cudaMemsetAsync(differ, 0, 4, g->stream));
+    k_compare_u32<<<kNumSMs * 8, kBlock, 0, g->stream>>>(E, vals, g->w, differ);
+    uint32_t h = 0;
+    CGB_CUDA_TRY(cudaMemcpyAsync(&h, differ, 4, cudaMemcpyDeviceToHost, g->stream));
+    CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    dfree(differ);
+    if (h) {
+        g->in_w = vals;
+        g->in_w_owned = true;
+    } else {
+        dfree(vals);
+        g->in_w = g->w;
+        g->in_w_owned = false;
+    }
 }
 
 void ensure_frontier(cgb_graph* g)
@@ -744,6 +813,7 @@ void graph_free(cgb_graph* g)
         dfree(g->in_off);
         dfree(g->in_src);
     }
+    if (g->in_w_owned) dfree(g->in_w);
     free_msbfs(g);
     free_mssp(g);
     void* ptrs[] = {g->off, g->dst, g->w, g->pr_huge_rows, g->pr_rank, g->pr_off, g->pr_src, g->pr_outdeg,

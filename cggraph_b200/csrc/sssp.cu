@@ -26,6 +26,7 @@
 namespace cgb {
 
 __shared__ uint32_t s_sssp_newfar;  // per-CTA count of vertices newly set in the far bitmap
+__shared__ unsigned long long s_sssp_medges;  // per-CTA out-degree sum of the next near queue
 
 template <bool kHasW>
 struct SsspOp {
@@ -54,8 +55,9 @@ struct SsspOp {
         bool to_near = false, new_far = false;
         uint32_t d = 0;
         if (valid) {
-            d = dst[e];
-            const uint64_t cand = (uint64_t)du + (kHasW ? (uint64_t)w[e] : 1ull);
+            // the edge arrays stream through once: evict first, so L2 keeps dist[] and the bitmaps
+            d = __ldcs(dst + e);
+            const uint64_t cand = (uint64_t)du + (kHasW ? (uint64_t)__ldcs(w + e) : 1ull);
             if (cand < kValueMax) {
                 const uint32_t nd = (uint32_t)cand;
                 if (nd < dist[d]) {
@@ -77,14 +79,23 @@ struct SsspOp {
         warp_append(to_near, d, near_out, near_len, cap, &ctr->overflow);
         const uint32_t nf = __popc(__ballot_sync(0xffffffffu, new_far));
         if (nf && lane_id() == 0) atomicAdd(&s_sssp_newfar, nf);
+        if (__any_sync(0xffffffffu, to_near)) {
+            // out-edges of the next near queue: the next round's push / pull choice
+            const unsigned long long dg = warp_sum((unsigned long long)(to_near ? off[d + 1] - off[d] : 0u));
+            if (dg && lane_id() == 0) atomicAdd(&s_sssp_medges, dg);
+        }
     }
     __device__ __forceinline__ void block_begin() const
     {
-        if (threadIdx.x == 0) s_sssp_newfar = 0;
+        if (threadIdx.x == 0) {
+            s_sssp_newfar = 0;
+            s_sssp_medges = 0;
+        }
     }
     __device__ __forceinline__ void block_end() const
     {
         if (threadIdx.x == 0 && s_sssp_newfar) atomicAdd(&ctr->far_len[0], s_sssp_newfar);
+        if (threadIdx.x == 0 && s_sssp_medges) atomicAdd(&ctr->medges, s_sssp_medges);
     }
 };
 
@@ -106,9 +117,11 @@ __global__ void k_sssp_root(uint32_t* dist, uint32_t root, uint32_t* q0)
 // min_far the smallest distance among them.
 __global__ void __launch_bounds__(kBlock) k_sssp_split(uint32_t words, uint32_t* far_bm, const uint32_t* dist,
                                                        uint32_t lo, uint32_t hi, uint32_t* near_out,
-                                                       uint32_t* near_len, uint32_t cap, DevCounters* ctr)
+                                                       uint32_t* near_len, uint32_t cap, DevCounters* ctr,
+                                                       const uint32_t* __restrict__ off)
 {
     uint32_t mn = kValueMax, left = 0;
+    unsigned long long dg = 0;
     const uint32_t stride = gridDim.x * blockDim.x;
     const uint32_t words_round = (words + 31u) & ~31u;
     for (uint32_t wi = blockIdx.x * blockDim.x + threadIdx.x; wi < words_round; wi += stride) {
@@ -126,6 +139,7 @@ __global__ void __launch_bounds__(kBlock) k_sssp_split(uint32_t words, uint32_t*
                 if (dv < hi) {
                     keep &= ~(1u << b);
                     to_near = dv >= lo;
+                    if (to_near) dg += off[v + 1] - off[v];
                 } else {
                     mn = min(mn, dv);
                 }
@@ -139,9 +153,11 @@ __global__ void __launch_bounds__(kBlock) k_sssp_split(uint32_t words, uint32_t*
     }
     mn = __reduce_min_sync(0xffffffffu, mn);
     left = warp_sum(left);
+    dg = warp_sum(dg);
     if (lane_id() == 0) {
         if (mn != kValueMax) atomicMin(&ctr->min_far, mn);
         if (left) atomicAdd(&ctr->far_len[0], left);
+        if (dg) atomicAdd(&ctr->medges, dg);
     }
 }
 
@@ -171,6 +187,10 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
     uint64_t nnear = root < g->nz ? 1 : 0;
     uint64_t nfar = 0;
     uint64_t thr = delta;
+    uint64_t bucket_lo = 0;      // the current bucket is [bucket_lo, thr): every near vertex is in it
+    uint64_t near_edges = 0;     // out-edges of the near queue (0 = unknown: push)
+    // pull rounds need the in-edges (and their weights in CSC order)
+    const bool pull_ok = o.schedule != CGB_SCHED_FIXED && g->tune.sssp_pull_alpha > 0;
     uint64_t iters = 0;
     uint64_t expanded = 0;
 
@@ -191,19 +211,35 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
                 expanded += r.added;
                 nnear = r.nf;
                 nfar = g->h_ctr->far_len[0];
+                near_edges = 0;  // not counted by the device-resident rounds: push next
                 cur = r.cur;
                 if (r.levels > 0) continue;
             }
             const int out = cur ^ 1;
+            // direction: pull when the near set's out-edges times alpha exceed the graph's edges
+            const bool pull = pull_ok && (double)near_edges * g->tune.sssp_pull_alpha > (double)g->E;
+            if (pull) {
+                ensure_csc(g);
+                ensure_csc_weights(g);
+            }
             CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->qlen[out], 0, sizeof(uint32_t), g->stream));
             CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->chunk_len, 0, sizeof(uint32_t), g->stream));
-            CGB_CUDA_TRY(cudaMemsetAsync(near_bm, 0, (size_t)words * sizeof(uint32_t), g->stream));
+            CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->medges, 0, 8, g->stream));
+            if (!pull) CGB_CUDA_TRY(cudaMemsetAsync(near_bm, 0, (size_t)words * sizeof(uint32_t), g->stream));
             if (tracing) CGB_CUDA_TRY(cudaEventRecord(g->ev_iter[0], g->stream));
-            if (timing) ktimer_begin(g, CGB_K_PUSH);
-            SsspOp<kHasW> op{g->off, g->dst, g->w, g->value, near_bm,
-                             (uint32_t)std::min<uint64_t>(thr, kValueMax), g->nz, g->q[out], &g->ctr->qlen[out], V,
-                             far_bm, g->ctr};
-            launch_push(g, g->q[cur], (uint32_t)nnear, op, false);
+            if (timing) ktimer_begin(g, pull ? CGB_K_PULL : CGB_K_PUSH);
+            if (pull) {
+                sssp_pull_round(g, g->q[cur], (uint32_t)nnear, (uint32_t)std::min<uint64_t>(bucket_lo, kValueMax),
+                                (uint32_t)std::min<uint64_t>(thr, kValueMax), g->q[out], &g->ctr->qlen[out], far_bm,
+                                g->aux_bm);
+                g->stats.pulls_bu++;
+            } else {
+                SsspOp<kHasW> op{g->off, g->dst, g->w, g->value, near_bm,
+                                 (uint32_t)std::min<uint64_t>(thr, kValueMax), g->nz, g->q[out], &g->ctr->qlen[out],
+                                 V, far_bm, g->ctr};
+                launch_push(g, g->q[cur], (uint32_t)nnear, op, false);
+                g->stats.pushes_td++;
+            }
             if (timing) ktimer_end(g);
             if (tracing) CGB_CUDA_TRY(cudaEventRecord(g->ev_iter[1], g->stream));
             sync_counters(g);
@@ -216,7 +252,8 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
                 t.algorithm = CGB_SSSP;
                 t.frontier_vertices = nnear;
                 t.unvisited_vertices = g->h_ctr->far_len[0];
-                t.variant = CGB_VAR_TWC;
+                t.variant = pull ? CGB_VAR_PULL : CGB_VAR_TWC;
+                t.frontier_edges = near_edges;
                 t.delta = delta;
                 t.ms = ms;
                 g->trace.push_back(t);
@@ -224,6 +261,7 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
             expanded += nnear;
             nnear = g->h_ctr->qlen[out];
             nfar = g->h_ctr->far_len[0];
+            near_edges = g->h_ctr->medges;
             cur = out;
             iters++;
         }
@@ -239,18 +277,21 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
             CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->qlen[out], 0, sizeof(uint32_t), g->stream));
             CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->far_len[0], 0, sizeof(uint32_t), g->stream));
             CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->min_far, 0xff, sizeof(uint32_t), g->stream));
+            CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->medges, 0, 8, g->stream));
             if (timing) ktimer_begin(g, CGB_K_FRONTIER);
             ++g->stats.launches;
             k_sssp_split<<<grid_for(words, kBlock, kNumSMs * 4), kBlock, 0, g->stream>>>(
                 words, far_bm, g->value, (uint32_t)std::min<uint64_t>(lo, kValueMax),
-                (uint32_t)std::min<uint64_t>(thr, kValueMax), g->q[out], &g->ctr->qlen[out], V, g->ctr);
+                (uint32_t)std::min<uint64_t>(thr, kValueMax), g->q[out], &g->ctr->qlen[out], V, g->ctr, g->off);
             if (timing) ktimer_end(g);
             sync_counters(g);
             CGB_REQUIRE(!g->h_ctr->overflow, CGB_EOVERFLOW, "SSSP queue overflow");
             nnear = g->h_ctr->qlen[out];
             nfar = g->h_ctr->far_len[0];
+            near_edges = g->h_ctr->medges;
             cur = out;
             iters++;
+            bucket_lo = lo;
             if (nnear > 0 || nfar == 0) break;
             // every vertex left is at or above thr: jump to the bucket of the smallest
             const uint64_t mn = g->h_ctr->min_far;

@@ -215,7 +215,10 @@ typedef struct {
                                   per warp; default 128) */
     uint32_t persist_ctas;     /* CTAs of the device-resident loops (0 = one per SM, else 1..that;
                                   fewer CTAs make each level's grid barrier cheaper) */
-    uint32_t reserved[6];
+    uint32_t sssp_pull_alpha;  /* SSSP rounds pull (scan in-edges of unsettled vertices) when the near
+                                  set's out-edges times this exceed E; 0 = always push (default; on
+                                  RMAT-24 the pull kernels lose to the push, the autotuner may pick it) */
+    uint32_t reserved[5];
 } cgb_tuning;
 
 cgb_status cgb_tuning_get(const cgb_graph* g, int algorithm, cgb_tuning* out);

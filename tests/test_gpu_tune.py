@@ -18,6 +18,8 @@ TUNINGS = [
     {"push_big_deg": 300, "push_chunk": 512, "push_ctas_per_sm": 3, "persist_enter": 100, "persist_deg": 64,
      "persist_ctas": 5},
     {"persist_ctas": 1},
+    {"sssp_pull_alpha": 1000, "persist_enter": 0},
+    {"sssp_pull_alpha": 0},
 ]
 
 
