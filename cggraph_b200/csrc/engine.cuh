@@ -189,6 +189,9 @@ void free_msbfs(cgb_graph* g);
 // n * V distances, root-major.
 void run_mssp(cgb_graph* g, const uint32_t* d_roots, uint32_t n, uint32_t* out, uint32_t delta);
 void free_mssp(cgb_graph* g);
+// Pinned host blocks of at most 256 bytes from process-lifetime slabs.
+void* pinned_small_alloc(size_t bytes);
+void pinned_small_free(void* p);
 // Weights in CSC order (in_w); needs the graph's weights.
 void ensure_csc_weights(cgb_graph* g);
 // One pull round of SSSP over the near set q_in[0, nin) at bucket [lo, thr):

@@ -70,6 +70,36 @@ static void dfree(void* p)
     cudaFreeAsync(p, dp.stream);
 }
 
+// Small pinned host blocks (each graph's counter mirror) come from slabs that
+// live as long as the process: cudaMallocHost / cudaFreeHost per graph cost
+// a driver call each, and freeing pinned memory has stalled for milliseconds.
+namespace {
+constexpr size_t kPinnedSlot = 256, kPinnedSlab = 256 * 1024;
+std::mutex g_pinned_mu;
+std::vector<void*> g_pinned_free;
+}  // namespace
+
+void* pinned_small_alloc(size_t bytes)
+{
+    CGB_REQUIRE(bytes <= kPinnedSlot, CGB_EINVAL, "pinned block too large");
+    std::lock_guard<std::mutex> lock(g_pinned_mu);
+    if (g_pinned_free.empty()) {
+        char* slab = nullptr;
+        CGB_CUDA_TRY(cudaMallocHost((void**)&slab, kPinnedSlab));
+        for (size_t o = 0; o < kPinnedSlab; o += kPinnedSlot) g_pinned_free.push_back(slab + o);
+    }
+    void* p = g_pinned_free.back();
+    g_pinned_free.pop_back();
+    return p;
+}
+
+void pinned_small_free(void* p)
+{
+    if (!p) return;
+    std::lock_guard<std::mutex> lock(g_pinned_mu);
+    g_pinned_free.push_back(p);
+}
+
 void memory_trim(int device)
 {
     CGB_CUDA_TRY(cudaSetDevice(device));
@@ -153,19 +183,6 @@ __global__ void k_split_keys(uint32_t E, const uint64_t* __restrict__ keys, uint
         low[e] = (uint32_t)(keys[e] & mask);
 }
 
-// Offsets from keys sorted by their high part h(e) = keys[e] >> b, with
-// h(n) = V as sentinel: off[v] = min{e : h(e) >= v}, i.e. edge e writes
-// off[v] for h(e-1) < v <= h(e).
-__global__ void k_offsets_from_keys(uint32_t V, uint64_t n, const uint64_t* __restrict__ keys, uint32_t b,
-                                    uint32_t* off)
-{
-    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e <= n; e += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t hi = e < n ? (keys[e] >> b) : V;
-        const uint64_t lo = e == 0 ? 0 : (keys[e - 1] >> b) + 1;
-        for (uint64_t v = lo; v <= hi; v++) off[v] = (uint32_t)e;
-    }
-}
-
 __global__ void k_widen(uint32_t n, const uint32_t* __restrict__ a, uint64_t* o)
 {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) o[i] = a[i];
@@ -238,23 +255,6 @@ static void radix_sort_u64(cgb_graph* g, uint64_t*& keys, uint64_t*& alt, uint64
     dfree(temp);
     CGB_CUDA_TRY(err);
     if (db.Current() != keys) std::swap(keys, alt);
-}
-
-// Sorts n (key, value) pairs; on return keys / vals hold the sorted data.
-static void radix_sort_pairs(cgb_graph* g, uint64_t*& keys, uint64_t*& alt, uint32_t*& vals, uint32_t*& valt,
-                             uint64_t n, int end_bit)
-{
-    cub::DoubleBuffer<uint64_t> dk(keys, alt);
-    cub::DoubleBuffer<uint32_t> dv(vals, valt);
-    size_t temp_bytes = 0;
-    CGB_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, dk, dv, n, 0, end_bit, g->stream));
-    void* temp = dalloc<char>(temp_bytes);
-    cudaError_t err = cub::DeviceRadixSort::SortPairs(temp, temp_bytes, dk, dv, n, 0, end_bit, g->stream);
-    CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
-    dfree(temp);
-    CGB_CUDA_TRY(err);
-    if (dk.Current() != keys) std::swap(keys, alt);
-    if (dv.Current() != vals) std::swap(vals, valt);
 }
 
 // Sorts every neighbour list by destination, weights following
@@ -364,40 +364,101 @@ __global__ void k_compare_u32(uint64_t n, const uint32_t* __restrict__ a, const 
     }
 }
 
+__global__ void k_iota_u32(uint32_t n, uint32_t* a)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = i;
+}
+
+// off[v] = min{j : key[j] >= v} over keys sorted ascending (key(n) = V as
+// sentinel): position j writes off[v] for key(j-1) < v <= key(j).
+__global__ void k_offsets_from_u32(uint32_t V, uint32_t n, const uint32_t* __restrict__ key, uint32_t* off)
+{
+    for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j <= n; j += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t hi = j < n ? key[j] : V;
+        const uint64_t lo = j == 0 ? 0 : (uint64_t)key[j - 1] + 1;
+        for (uint64_t v = lo; v <= hi; v++) off[v] = (uint32_t)j;
+    }
+}
+
+// Source of every edge, in CSR order (consecutive edges share their search
+// path, so the binary searches stay in cache).
+__global__ void k_edge_sources(uint32_t V, uint32_t E, const uint32_t* __restrict__ off, uint32_t* src)
+{
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x)
+        src[e] = edge_source(off, V, e);
+}
+
+__global__ void k_gather_u32(uint32_t n, const uint32_t* __restrict__ idx, const uint32_t* __restrict__ a, uint32_t* out)
+{
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) out[j] = a[idx[j]];
+}
+
+// Stable sort of (key, value) pairs by the key's low `bits` bits: vals_out
+// receives the values in key order, keys_out the keys.
+static void stable_sort_u32(cgb_graph* g, const uint32_t* keys_in, uint32_t* keys_out, const uint32_t* vals_in,
+                            uint32_t* vals_out, uint32_t n, int bits)
+{
+    size_t tb = 0;
+    CGB_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tb, keys_in, keys_out, vals_in, vals_out, (uint64_t)n, 0,
+                                                 bits, g->stream));
+    void* temp = dalloc<char>(tb);
+    cudaError_t err = cub::DeviceRadixSort::SortPairs(temp, tb, keys_in, keys_out, vals_in, vals_out, (uint64_t)n, 0,
+                                                      bits, g->stream);
+    CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    dfree(temp);
+    CGB_CUDA_TRY(err);
+}
+
+// The transpose's source and (optionally) weight arrays: the CSR lists
+// edges by ascending source, so a stable sort on the destination alone
+// (32-bit keys over bits_for(V) bits) orders each in-list by source.
+// dst_sorted receives the destinations in CSC order.
+static void transpose_arrays(cgb_graph* g, uint32_t* dst_sorted, uint32_t* in_src, uint32_t* in_w)
+{
+    const uint32_t E = g->E, V = g->V;
+    const uint32_t grid = grid_for(E, kBlock, kNumSMs * 16);
+    uint32_t* src = dalloc<uint32_t>(E);
+    k_edge_sources<<<grid, kBlock, 0, g->stream>>>(V, E, g->off, src);
+    if (!in_w) {
+        stable_sort_u32(g, g->dst, dst_sorted, src, in_src, E, (int)bits_for(V));
+    } else {
+        uint32_t* iota = dalloc<uint32_t>(E);
+        uint32_t* perm = dalloc<uint32_t>(E);
+        k_iota_u32<<<grid, kBlock, 0, g->stream>>>(E, iota);
+        stable_sort_u32(g, g->dst, dst_sorted, iota, perm, E, (int)bits_for(V));
+        k_gather_u32<<<grid, kBlock, 0, g->stream>>>(E, perm, src, in_src);
+        k_gather_u32<<<grid, kBlock, 0, g->stream>>>(E, perm, g->w, in_w);
+        CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        dfree(iota);
+        dfree(perm);
+    }
+    CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    dfree(src);
+}
+
 // Builds the transpose (in-edge CSC) by a radix sort of packed (dst, src)
 // keys and compares it with the CSR: equal means the graph is symmetric, the
 // transpose is dropped and the CSR serves both directions.
 static void build_transpose(cgb_graph* g)
 {
     const uint32_t V = g->V, E = g->E;
-    const uint32_t b = bits_for(V);
     uint32_t* in_off = dalloc<uint32_t>((size_t)V + 1);
     uint32_t* in_src = dalloc<uint32_t>(E);
     if (E == 0) {
         CGB_CUDA_TRY(cudaMemsetAsync(in_off, 0, ((size_t)V + 1) * sizeof(uint32_t), g->stream));
     } else {
-        uint64_t* keys = dalloc<uint64_t>(E);
-        uint64_t* alt = dalloc<uint64_t>(E);
-        const uint32_t grid = grid_for(E, kBlock, kNumSMs * 16);
-        k_make_keys<<<grid, kBlock, 0, g->stream>>>(V, E, g->off, g->dst, b, keys, true);
-        if (g->w && !g->in_w) {
-            // weighted: the weights ride along, so SSSP pull rounds find them in CSC order
-            uint32_t* vals = dalloc<uint32_t>(E);
-            uint32_t* valt = dalloc<uint32_t>(E);
-            CGB_CUDA_TRY(cudaMemcpyAsync(vals, g->w, (size_t)E * 4, cudaMemcpyDeviceToDevice, g->stream));
-            radix_sort_pairs(g, keys, alt, vals, valt, E, 2 * b);
-            dfree(valt);
-            g->in_w = vals;
-            g->in_w_owned = true;
-        } else {
-            radix_sort_u64(g, keys, alt, E, 2 * b);
-        }
-        k_split_keys<<<grid, kBlock, 0, g->stream>>>(E, keys, b, in_src);
-        k_offsets_from_keys<<<grid_for((uint64_t)E + 1, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(V, E, keys, b,
-                                                                                                       in_off);
+        uint32_t* dsorted = dalloc<uint32_t>(E);
+        uint32_t* in_w = nullptr;
+        if (g->w && !g->in_w) in_w = dalloc<uint32_t>(E);  // SSSP pull rounds find the weights in CSC order
+        transpose_arrays(g, dsorted, in_src, in_w);
+        k_offsets_from_u32<<<grid_for((uint64_t)E + 1, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(V, E, dsorted,
+                                                                                                      in_off);
         CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
-        dfree(keys);
-        dfree(alt);
+        dfree(dsorted);
+        if (in_w) {
+            g->in_w = in_w;
+            g->in_w_owned = true;
+        }
     }
     uint32_t* differ = dalloc<uint32_t>(1);
     CGB_CUDA_TRY(cudaMemsetAsync(differ, 0, sizeof(uint32_t), g->stream));
@@ -448,22 +509,18 @@ void ensure_csc_weights(cgb_graph* g)
     // the CSR serves as CSC (symmetric structure): transpose the weights by
     // sorting (dst, src) keys with the weights as values, then alias w when
     // they are symmetric too
-    const uint32_t V = g->V, E = g->E, b = bits_for(V);
+    const uint32_t V = g->V, E = g->E;
     if (E == 0) {
         g->in_w = g->w;
         g->in_w_owned = false;
         return;
     }
-    uint64_t* keys = dalloc<uint64_t>(E);
-    uint64_t* alt = dalloc<uint64_t>(E);
+    uint32_t* dsorted = dalloc<uint32_t>(E);
+    uint32_t* srcs = dalloc<uint32_t>(E);
     uint32_t* vals = dalloc<uint32_t>(E);
-    uint32_t* valt = dalloc<uint32_t>(E);
-    k_make_keys<<<grid_for(E, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(V, E, g->off, g->dst, b, keys, true);
-    CGB_CUDA_TRY(cudaMemcpyAsync(vals, g->w, (size_t)E * 4, cudaMemcpyDeviceToDevice, g->stream));
-    radix_sort_pairs(g, keys, alt, vals, valt, E, 2 * b);
-    dfree(keys);
-    dfree(alt);
-    dfree(valt);
+    transpose_arrays(g, dsorted, srcs, vals);
+    dfree(dsorted);
+    dfree(srcs);
     uint32_t* differ = dalloc<uint32_t>(1);
     CGB_CUDA_TRY(cudaMemsetAsync(differ, 0, 4, g->stream));
     k_compare_u32<<<kNumSMs * 8, kBlock, 0, g->stream>>>(E, vals, g->w, differ);
@@ -548,25 +605,6 @@ __global__ void k_fill_u32(uint64_t n, uint32_t* a, uint32_t v)
         a[i] = v;
 }
 
-// Scatter the sorted (row, src) keys of the non-hub rows into the sliced ELL
-// and mark the hub rows.
-__global__ void k_sell_fill(uint32_t E, const uint64_t* __restrict__ keys, uint32_t b,
-                            const uint32_t* __restrict__ off, const uint64_t* __restrict__ slice_ptr, uint32_t hub,
-                            uint32_t* col, uint32_t* hub_bm)
-{
-    const uint64_t mask = (1ull << b) - 1;
-    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x) {
-        const uint64_t k = keys[e];
-        const uint32_t r = (uint32_t)(k >> b);
-        const uint32_t s0 = off[r];
-        if (off[r + 1] - s0 >= hub) {
-            if (e == s0) atomicOr(hub_bm + (r >> 5), 1u << (r & 31u));
-            continue;
-        }
-        col[slice_ptr[r >> 5] + 32ull * (e - s0) + (r & 31u)] = (uint32_t)(k & mask);
-    }
-}
-
 __global__ void k_pr_rank(uint32_t V, const uint32_t* __restrict__ order, const uint32_t* __restrict__ off,
                           uint32_t* rank, uint32_t* outdeg_new)
 {
@@ -586,22 +624,44 @@ __global__ void k_row_bounds(const uint32_t* __restrict__ rows, uint32_t n, cons
     }
 }
 
-// key = rank[dst] << b | rank[src]
-__global__ void k_pr_edge_keys(uint32_t V, uint32_t E, const uint32_t* __restrict__ off,
-                               const uint32_t* __restrict__ dst, const uint32_t* __restrict__ rank, uint32_t b,
-                               uint64_t* keys)
+// Edges of the relabelled graph in new-source order: position p of the
+// out-list of order[r] (r = new source) gives key = new destination and
+// value = r; a stable sort by key then lists each new row's sources in
+// ascending new ids.
+__global__ void k_pr_edges(uint32_t V, uint32_t E, const uint32_t* __restrict__ src_off,
+                           const uint32_t* __restrict__ order, const uint32_t* __restrict__ off,
+                           const uint32_t* __restrict__ dst, const uint32_t* __restrict__ rank, uint32_t* key,
+                           uint32_t* val)
 {
-    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x) {
-        const uint64_t s = rank[edge_source(off, V, e)];
-        const uint64_t d = rank[dst[e]];
-        keys[e] = (d << b) | s;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < E; p += gridDim.x * blockDim.x) {
+        const uint32_t r = edge_source(src_off, V, p);
+        key[p] = rank[dst[off[order[r]] + (p - src_off[r])]];
+        val[p] = r;
     }
 }
 
-// Sliced ELL of the non-hub rows from the sorted (row, src) keys.
-static void build_sell(cgb_graph* g, const uint64_t* keys, uint32_t b)
+// SELL columns of the non-hub rows from the relabelled CSC (pr_off,
+// pr_src); hub rows are marked in hub_bm and summed from pr_src.
+__global__ void k_sell_fill(uint32_t V, uint32_t E, const uint32_t* __restrict__ pr_off,
+                            const uint32_t* __restrict__ pr_src, const uint64_t* __restrict__ slice_ptr, uint32_t hub,
+                            uint32_t* col, uint32_t* hub_bm)
 {
-    const uint32_t V = g->V, E = g->E;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < E; p += gridDim.x * blockDim.x) {
+        const uint32_t r = edge_source(pr_off, V, p);
+        const uint32_t j = p - pr_off[r];
+        if (pr_off[r + 1] - pr_off[r] >= hub) {
+            if (j == 0) atomicOr(hub_bm + (r >> 5), 1u << (r & 31u));
+            continue;
+        }
+        col[slice_ptr[r >> 5] + 32ull * j + (r & 31u)] = pr_src[p];
+    }
+}
+
+// Sliced ELL layout of the non-hub rows (slice lengths, offsets, the column
+// array filled with the padding target V); k_sell_fill writes the columns.
+static void build_sell(cgb_graph* g)
+{
+    const uint32_t V = g->V;
     const uint32_t nslices = (V + 31) / 32;
     g->pr_slice_len = dalloc<uint32_t>(nslices);
     g->pr_slice_ptr = dalloc<uint64_t>((size_t)nslices + 1);
@@ -625,11 +685,6 @@ static void build_sell(cgb_graph* g, const uint64_t* keys, uint32_t b)
     g->pr_sell_size = total;
     g->pr_col = dalloc<uint32_t>(total);
     k_fill_u32<<<grid_for(total, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(total, g->pr_col, V);
-    if (E)
-        k_sell_fill<<<grid_for(E, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(E, keys, b, g->pr_off,
-                                                                                g->pr_slice_ptr, kPrHuge, g->pr_col,
-                                                                                g->pr_hub_bm);
-    CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
 }
 
 // Builds the PageRank layout (see cgb_graph): the relabel keeps every
@@ -639,7 +694,6 @@ void ensure_pr(cgb_graph* g)
 {
     if (g->pr_ready) return;
     const uint32_t V = g->V, E = g->E;
-    const uint32_t b = bits_for(V);
     for (int i = 0; i < 2; i++) {
         if (!g->pr[i]) g->pr[i] = dalloc<double>(V);
         if (!g->contrib[i]) g->contrib[i] = dalloc<double>((size_t)V + 1);
@@ -650,6 +704,7 @@ void ensure_pr(cgb_graph* g)
     g->pr_off = dalloc<uint32_t>((size_t)V + 1);
     g->pr_src = dalloc<uint32_t>(E);
     // 1. stable order by (out-degree bucket, in-degree descending)
+    uint32_t* order = nullptr;
     {
         uint32_t* key = dalloc<uint32_t>(V);
         uint32_t* key2 = dalloc<uint32_t>(V);
@@ -670,26 +725,51 @@ void ensure_pr(cgb_graph* g)
         dfree(temp);
         dfree(key);
         dfree(key2);
-        dfree(id);
-        dfree(id2);
         CGB_CUDA_TRY(err);
+        order = vb.Current();
+        dfree(vb.Alternate());
     }
-    // 2. in-edge CSC over the new ids
-    if (E) {
-        uint64_t* keys = dalloc<uint64_t>(E);
-        uint64_t* alt = dalloc<uint64_t>(E);
-        const uint32_t grid = grid_for(E, kBlock, kNumSMs * 16);
-        k_pr_edge_keys<<<grid, kBlock, 0, g->stream>>>(V, E, g->off, g->dst, g->pr_rank, b, keys);
-        radix_sort_u64(g, keys, alt, E, 2 * b);
-        k_split_keys<<<grid, kBlock, 0, g->stream>>>(E, keys, b, g->pr_src);
-        k_offsets_from_keys<<<grid_for((uint64_t)E + 1, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(V, E, keys, b,
-                                                                                                       g->pr_off);
-        build_sell(g, keys, b);
-        dfree(keys);
-        dfree(alt);
-    } else {
-        CGB_CUDA_TRY(cudaMemsetAsync(g->pr_off, 0, ((size_t)V + 1) * 4, g->stream));
-        build_sell(g, nullptr, b);
+    // 2. in-edge CSC over the new ids: the edges enumerated by new source,
+    //    stable-sorted by new destination (one 32-bit sort), so each row
+    //    lists its sources in ascending new ids
+    {
+        // offsets of the new sources' out-lists: exclusive scan of the out-degrees in new order
+        // (pr_outdeg has V entries; the scan of V + 1 reads a zero-padded copy)
+        uint32_t* src_off = dalloc<uint32_t>((size_t)V + 1);
+        uint32_t* od = dalloc<uint32_t>((size_t)V + 1);
+        CGB_CUDA_TRY(cudaMemcpyAsync(od, g->pr_outdeg, (size_t)V * 4, cudaMemcpyDeviceToDevice, g->stream));
+        CGB_CUDA_TRY(cudaMemsetAsync(od + V, 0, 4, g->stream));
+        size_t tb = 0;
+        CGB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb, od, src_off, (uint64_t)V + 1, g->stream));
+        void* temp = dalloc<char>(tb);
+        cudaError_t err = cub::DeviceScan::ExclusiveSum(temp, tb, od, src_off, (uint64_t)V + 1, g->stream);
+        CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        dfree(temp);
+        dfree(od);
+        CGB_CUDA_TRY(err);
+        if (E) {
+            uint32_t* key = dalloc<uint32_t>(E);
+            uint32_t* val = dalloc<uint32_t>(E);
+            uint32_t* kout = dalloc<uint32_t>(E);
+            k_pr_edges<<<grid_for(E, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(V, E, src_off, order, g->off,
+                                                                                   g->dst, g->pr_rank, key, val);
+            stable_sort_u32(g, key, kout, val, g->pr_src, E, (int)bits_for(V));
+            k_offsets_from_u32<<<grid_for((uint64_t)E + 1, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(
+                V, E, kout, g->pr_off);
+            CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+            dfree(key);
+            dfree(val);
+            dfree(kout);
+        } else {
+            CGB_CUDA_TRY(cudaMemsetAsync(g->pr_off, 0, ((size_t)V + 1) * 4, g->stream));
+        }
+        dfree(src_off);
+        build_sell(g);
+        if (E)
+            k_sell_fill<<<grid_for(E, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(
+                V, E, g->pr_off, g->pr_src, g->pr_slice_ptr, kPrHuge, g->pr_col, g->pr_hub_bm);
+        CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        dfree(order);
     }
     // 3. hub rows and their chunk table (host-built; few rows)
     {
@@ -791,7 +871,7 @@ cgb_graph* graph_alloc(uint32_t V, uint32_t E, uint32_t nz, int device, bool wit
         CGB_CUDA_TRY(cudaEventCreate(&g->ev_iter[0]));
         CGB_CUDA_TRY(cudaEventCreate(&g->ev_iter[1]));
         g->ctr = dalloc<DevCounters>(1);
-        CGB_CUDA_TRY(cudaMallocHost((void**)&g->h_ctr, sizeof(DevCounters)));
+        g->h_ctr = static_cast<DevCounters*>(pinned_small_alloc(sizeof(DevCounters)));
         CGB_CUDA_TRY(cudaMemsetAsync(g->ctr, 0, sizeof(DevCounters), g->stream));
         g->off = dalloc<uint32_t>((size_t)V + 1);
         g->dst = dalloc<uint32_t>(E);
@@ -822,7 +902,7 @@ void graph_free(cgb_graph* g)
                     g->contrib[1], g->q[0], g->q[1], g->chunk_q, g->visited, g->front_bm, g->stamp, g->sample,
                     g->aux_bm, g->persist, g->ctr};
     for (void* p : ptrs) dfree(p);
-    if (g->h_ctr) cudaFreeHost(g->h_ctr);
+    pinned_small_free(g->h_ctr);
     for (cudaEvent_t e : g->kev) cudaEventDestroy(e);
     cudaEvent_t evs[] = {g->ev_start, g->ev_stop, g->ev_iter[0], g->ev_iter[1]};
     for (cudaEvent_t e : evs)
