@@ -108,13 +108,15 @@ class Tuning(ctypes.Structure):
         ("pr_ctas_per_sm", ctypes.c_uint32),
         ("persist_ctas", ctypes.c_uint32),
         ("sssp_pull_alpha", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32 * 5),
+        ("cluster_enter", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 4),
     ]
 
 
 TUNE_BATCH, TUNE_KEEP_DEFAULT = 0x1, 0x2
 TUNING_FIELDS = ("push_big_deg", "push_chunk", "push_ctas_per_sm", "persist_enter", "persist_deg", "ms_edges",
-                 "pr_unroll", "pr_ctas_per_sm", "persist_ctas", "sssp_pull_alpha")
+                 "pr_unroll", "pr_ctas_per_sm", "persist_ctas", "sssp_pull_alpha",
+                 "cluster_enter")
 
 
 class ServerConfig(ctypes.Structure):

@@ -1,4 +1,6 @@
 // Device-resident BFS levels and SSSP near rounds (see persist.cuh).
+#include <cooperative_groups.h>
+
 #include "persist.cuh"
 
 namespace cgb {
@@ -7,13 +9,13 @@ namespace cgb {
 // frontier vertices; lists of 32 or more edges are walked by the whole warp
 // (ballot election), shorter ones lane by lane.  Visit(valid, e, msg) is
 // warp-collective.
-template <class Visit, class Load>
+template <int kWarps = kBlock / 32, class Visit, class Load>
 __device__ __forceinline__ void expand_small(const uint32_t* __restrict__ qin, uint32_t nf, const Load& load,
                                              const Visit& visit)
 {
     const uint32_t lane = lane_id();
-    const uint32_t nwarps = gridDim.x * (kBlock / 32);
-    for (uint32_t base = (blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5)) * 32; base < nf; base += nwarps * 32) {
+    const uint32_t nwarps = gridDim.x * kWarps;
+    for (uint32_t base = (blockIdx.x * kWarps + (threadIdx.x >> 5)) * 32; base < nf; base += nwarps * 32) {
         const uint32_t i = base + lane;
         uint32_t start = 0, deg = 0, msg = 0;
         if (i < nf) load(qin[i], start, deg, msg);
@@ -102,6 +104,81 @@ __global__ void __launch_bounds__(kBlock) k_bfs_persistent(const uint32_t* __res
         };
         expand_small(qin, nf, load, visit);
         if (!grid_barrier(st)) break;
+        cur ^= 1;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st->levels = it;
+        st->cur = cur;
+        st->nf = st->qlen[it % 3];
+    }
+}
+
+// The same BFS level loop as one thread-block cluster (kThreads per CTA,
+// up to 16 CTAs): levels are separated by the cluster's hardware barrier,
+// which also orders the global-memory counters and bitmaps at cluster scope,
+// instead of the grid barrier's global-memory round trip.  For frontiers of
+// up to a few thousand vertices (a road-like grid's whole run), where the
+// barrier is most of a level's time.  Every exit decision is read after the
+// barrier from the same counter, so all threads leave together.
+template <int kThreads>
+__global__ void __launch_bounds__(kThreads, 1) k_bfs_cluster(const uint32_t* __restrict__ off,
+                                                             const uint32_t* __restrict__ dst, uint32_t* level,
+                                                             uint32_t* visited, uint32_t* q0, uint32_t* q1,
+                                                             uint32_t cap, uint32_t nz, uint32_t start_level,
+                                                             uint32_t cur, uint32_t nf_exit,
+                                                             unsigned long long scout_exit, uint32_t deg_exit,
+                                                             uint32_t max_levels, PersistState* st)
+{
+    cooperative_groups::cluster_group cluster = cooperative_groups::this_cluster();
+    uint32_t it = 0;
+    for (; it < max_levels; it++) {
+        const uint32_t s_cur = it % 3, s_next = (it + 1) % 3, s_zero = (it + 2) % 3;
+        const uint32_t nf = *(volatile uint32_t*)&st->qlen[s_cur];
+        const unsigned long long scout = *(volatile unsigned long long*)&st->medges[s_cur];
+        const uint32_t mdeg = *(volatile uint32_t*)&st->max_deg[s_cur];
+        if (nf == 0 || nf > nf_exit || scout > scout_exit || mdeg > deg_exit) break;
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            st->qlen[s_zero] = 0;
+            st->medges[s_zero] = 0;
+            st->max_deg[s_zero] = 0;
+            st->added += nf;
+            st->scouts += scout;
+        }
+        const uint32_t* qin = cur ? q1 : q0;
+        uint32_t* qout = cur ? q0 : q1;
+        const uint32_t next_level = start_level + it + 1;
+        auto load = [&](uint32_t v, uint32_t& s, uint32_t& d, uint32_t& m) {
+            s = off[v];
+            d = off[v + 1] - s;
+            m = 0;
+        };
+        auto visit = [&](bool valid, uint32_t e, uint32_t) {
+            bool win = false;
+            uint32_t d = 0;
+            if (valid) {
+                d = dst[e];
+                const uint32_t bit = 1u << (d & 31u);
+                uint32_t* wp = visited + (d >> 5);
+                if (!(*wp & bit) && !(atomicOr(wp, bit) & bit)) {
+                    win = true;
+                    level[d] = next_level;
+                }
+            }
+            const bool enq = win && d < nz;
+            uint32_t deg = 0;
+            if (enq) deg = off[d + 1] - off[d];
+            append(enq, d, qout, &st->qlen[s_next], cap, st);
+            if (__any_sync(0xffffffffu, enq)) {
+                const unsigned long long sum = warp_sum((unsigned long long)deg);
+                const uint32_t mx = warp_max(deg);
+                if (lane_id() == 0) {
+                    atomicAdd(&st->medges[s_next], sum);
+                    atomicMax(&st->max_deg[s_next], mx);
+                }
+            }
+        };
+        expand_small<kThreads / 32>(qin, nf, load, visit);
+        cluster.sync();
         cur ^= 1;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -350,20 +427,74 @@ static void init_state(cgb_graph* g, uint32_t nf, unsigned long long scout, uint
     CGB_CUDA_TRY(cudaMemcpyAsync(g->persist, &h, sizeof(h), cudaMemcpyHostToDevice, g->stream));
 }
 
+// CTAs of the level-loop cluster: 16 when the device schedules such a
+// cluster of kClusterThreads-thread CTAs (a non-portable size), else 8, else
+// 0 (no cluster path).  Decided once per process.
+static uint32_t cluster_size()
+{
+    static int size = -1;
+    if (size >= 0) return (uint32_t)size;
+    size = 0;
+    auto kern = k_bfs_cluster<kClusterThreads>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+        cudaGetLastError();
+    }
+    for (int c : {16, 8}) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(c);
+        cfg.blockDim = dim3(kClusterThreads);
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = c;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int n = 0;
+        if (cudaOccupancyMaxActiveClusters(&n, kern, &cfg) == cudaSuccess && n > 0) {
+            size = c;
+            break;
+        }
+        cudaGetLastError();
+    }
+    return (uint32_t)size;
+}
+
 PersistResult bfs_persistent(cgb_graph* g, uint32_t cur, uint32_t nf, unsigned long long scout, uint32_t max_deg,
                              uint32_t level, uint32_t nf_exit, unsigned long long scout_exit, uint32_t deg_exit,
                              uint32_t max_levels)
 {
     PersistState* st = persist_state(g);
     init_state(g, nf, scout, max_deg);
-    static uint32_t full = 0;
-    if (!full) full = cooperative_grid(k_bfs_persistent);
-    const uint32_t grid = g->tune.persist_ctas ? std::min(g->tune.persist_ctas, full) : full;
     uint32_t cap = g->V, nz = g->nz;
-    void* args[] = {&g->off, &g->dst, &g->value, &g->visited, &g->q[0], &g->q[1], &cap, &nz, &level, &cur, &nf_exit,
-                    &scout_exit, &deg_exit, &max_levels, &st};
     ++g->stats.launches;
-    CGB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_bfs_persistent, grid, kBlock, args, 0, g->stream));
+    const uint32_t csize = cluster_size();
+    if (csize && nf <= g->tune.cluster_enter) {
+        // small frontier: one cluster, hardware barrier between levels; back to
+        // the caller when the frontier outgrows twice the entry size
+        const uint32_t c_exit = std::min(nf_exit, 2 * g->tune.cluster_enter);
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(csize);
+        cfg.blockDim = dim3(kClusterThreads);
+        cfg.stream = g->stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = csize;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        CGB_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_bfs_cluster<kClusterThreads>, g->off, g->dst, g->value, g->visited,
+                                        g->q[0], g->q[1], cap, nz, level, cur, c_exit, scout_exit, deg_exit,
+                                        max_levels, st));
+    } else {
+        static uint32_t full = 0;
+        if (!full) full = cooperative_grid(k_bfs_persistent);
+        const uint32_t grid = g->tune.persist_ctas ? std::min(g->tune.persist_ctas, full) : full;
+        void* args[] = {&g->off, &g->dst, &g->value, &g->visited, &g->q[0], &g->q[1], &cap, &nz, &level, &cur,
+                        &nf_exit, &scout_exit, &deg_exit, &max_levels, &st};
+        CGB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_bfs_persistent, grid, kBlock, args, 0, g->stream));
+    }
     const PersistState h = read_state(g);
     PersistResult r;
     r.levels = h.levels;

@@ -22,6 +22,7 @@
 namespace cgb {
 
 constexpr uint32_t kBarrierSpins = 1u << 22;  // mostly x ~64 ns: gives up after ~0.3 s
+constexpr int kClusterThreads = 1024;          // threads per CTA of the cluster level loop
 
 // Host-visible state of a device-resident loop.
 struct PersistState {

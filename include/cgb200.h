@@ -218,7 +218,9 @@ typedef struct {
     uint32_t sssp_pull_alpha;  /* SSSP rounds pull (scan in-edges of unsettled vertices) when the near
                                   set's out-edges times this exceed E; 0 = always push (default; on
                                   RMAT-24 the pull kernels lose to the push, the autotuner may pick it) */
-    uint32_t reserved[5];
+    uint32_t cluster_enter;    /* BFS frontiers up to this size run their levels in one thread-block
+                                  cluster with a hardware barrier (0 = never, default 8192) */
+    uint32_t reserved[4];
 } cgb_tuning;
 
 cgb_status cgb_tuning_get(const cgb_graph* g, int algorithm, cgb_tuning* out);

@@ -20,6 +20,8 @@ TUNINGS = [
     {"persist_ctas": 1},
     {"sssp_pull_alpha": 1000, "persist_enter": 0},
     {"sssp_pull_alpha": 0},
+    {"cluster_enter": 0},
+    {"cluster_enter": 1 << 20},
 ]
 
 
