@@ -231,10 +231,22 @@ __global__ void __launch_bounds__(kBlock) k_ms_bu_warp(MsBuArgs a)
             got |= warp_or64(x & pending);
         }
         bool act = false;
+        if (got) {
+            // the new roots' levels: lane l writes roots l and l + 32
+#pragma unroll
+            for (uint32_t k = lane; k < 64; k += 32)
+                if ((got >> k) & 1ull) a.level_out[(size_t)k * a.V + u] = a.start ? a.lvl - a.start[k] : a.lvl;
+        }
         if (lane == 0) {
             a.acc[u] = 0;
-            if (got) act = ms_bu_settle(u, s, got, a.seen, a.fnext, a.level_out, a.V, a.lvl, a.nz, a.start);
-            if (act) live |= got;
+            if (got) {
+                a.seen[u] = s | got;
+                act = u < a.nz;
+                if (act) {
+                    a.fnext[u] = got;
+                    live |= got;
+                }
+            }
         }
         warp_append(act, u, a.qact, a.qact_len, a.cap, &a.ctr->overflow);
     }
