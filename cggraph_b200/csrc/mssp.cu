@@ -215,33 +215,47 @@ __global__ void __launch_bounds__(kBlock) k_mssp_split(const uint32_t* __restric
     const bool adv0 = (adv >> lane) & 1ull, adv1 = (adv >> (lane + 32)) & 1ull;
     uint32_t mn0 = kValueMax, mn1 = kValueMax;
     unsigned long long live = 0;
-    for (uint32_t i = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5); i < nfar; i += warps) {
-        const uint32_t v = far_in[i];
-        const unsigned long long m = farm[v];
-        const bool a0 = adv0 && ((m >> lane) & 1ull), a1 = adv1 && ((m >> (lane + 32)) & 1ull);
-        const uint32_t* row = dist + (size_t)v * kMsRoots;
-        const uint32_t d0 = a0 ? row[lane] : kValueMax, d1 = a1 ? row[lane + 32] : kValueMax;
-        const bool mv0 = a0 && d0 < hi0, mv1 = a1 && d1 < hi1;
-        const bool nr0 = mv0 && d0 >= lo0, nr1 = mv1 && d1 >= lo1;
-        if (a0 && !mv0) mn0 = min(mn0, d0);
-        if (a1 && !mv1) mn1 = min(mn1, d1);
-        const unsigned long long moved = (unsigned long long)__ballot_sync(0xffffffffu, mv0) |
-                                         ((unsigned long long)__ballot_sync(0xffffffffu, mv1) << 32);
-        const unsigned long long nearb = (unsigned long long)__ballot_sync(0xffffffffu, nr0) |
-                                         ((unsigned long long)__ballot_sync(0xffffffffu, nr1) << 32);
-        const unsigned long long keep = m & ~moved;
-        live |= keep;
-        if (lane == 0) {
-            if (moved) farm[v] = keep;  // no expansion runs during a split: v's far mask is this warp's
-            if (nearb && atomicOr(pend + v, nearb) == 0ull) {
-                const uint32_t p = atomicAdd(q_len, 1u);
-                if (p < cap) q[p] = v;
-                else atomicOr(&c->overflow, 1u);
-            }
-            if (keep) {
-                const uint32_t p = atomicAdd(far_out_len, 1u);
-                if (p < cap) far_out[p] = v;
-                else atomicOr(&c->overflow, 1u);
+    // a warp takes 32 far vertices; those with no pair of an advancing root
+    // stay far untouched (one aggregated append), the others are processed
+    // one at a time with the lanes over the roots
+    const uint32_t n_round = (nfar + 31u) & ~31u;
+    for (uint32_t base = (blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5)) * 32; base < n_round;
+         base += warps * 32) {
+        const uint32_t i = base + lane;
+        const uint32_t my_v = i < nfar ? far_in[i] : 0;
+        const unsigned long long my_m = i < nfar ? farm[my_v] : 0ull;
+        const bool hit = (my_m & adv) != 0ull;
+        if (i < nfar && !hit) live |= my_m;
+        warp_append(i < nfar && !hit, my_v, far_out, far_out_len, cap, &c->overflow);
+        for (uint32_t hits = __ballot_sync(0xffffffffu, hit); hits; hits &= hits - 1) {
+            const uint32_t src = __ffs(hits) - 1;
+            const uint32_t v = __shfl_sync(0xffffffffu, my_v, src);
+            const unsigned long long m = __shfl_sync(0xffffffffu, my_m, src);
+            const bool a0 = adv0 && ((m >> lane) & 1ull), a1 = adv1 && ((m >> (lane + 32)) & 1ull);
+            const uint32_t* row = dist + (size_t)v * kMsRoots;
+            const uint32_t d0 = a0 ? row[lane] : kValueMax, d1 = a1 ? row[lane + 32] : kValueMax;
+            const bool mv0 = a0 && d0 < hi0, mv1 = a1 && d1 < hi1;
+            const bool nr0 = mv0 && d0 >= lo0, nr1 = mv1 && d1 >= lo1;
+            if (a0 && !mv0) mn0 = min(mn0, d0);
+            if (a1 && !mv1) mn1 = min(mn1, d1);
+            const unsigned long long moved = (unsigned long long)__ballot_sync(0xffffffffu, mv0) |
+                                             ((unsigned long long)__ballot_sync(0xffffffffu, mv1) << 32);
+            const unsigned long long nearb = (unsigned long long)__ballot_sync(0xffffffffu, nr0) |
+                                             ((unsigned long long)__ballot_sync(0xffffffffu, nr1) << 32);
+            const unsigned long long keep = m & ~moved;
+            if (lane == 0) {
+                live |= keep;
+                if (moved) farm[v] = keep;  // no expansion runs during a split: v's far mask is this warp's
+                if (nearb && atomicOr(pend + v, nearb) == 0ull) {
+                    const uint32_t p = atomicAdd(q_len, 1u);
+                    if (p < cap) q[p] = v;
+                    else atomicOr(&c->overflow, 1u);
+                }
+                if (keep) {
+                    const uint32_t p = atomicAdd(far_out_len, 1u);
+                    if (p < cap) far_out[p] = v;
+                    else atomicOr(&c->overflow, 1u);
+                }
             }
         }
     }

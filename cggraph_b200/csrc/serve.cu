@@ -158,6 +158,20 @@ __global__ void __launch_bounds__(kBlock) k_srv_sp_extract(const uint32_t* __res
     }
 }
 
+// The same for a few finished slots (ks[0..n)): reads only their columns (one
+// 32-byte sector per vertex and slot) instead of whole 256-byte rows.
+__global__ void k_srv_sp_extract_cols(const uint32_t* __restrict__ dist, uint32_t V, uint4 ks, uint32_t n,
+                                      uint32_t* region)
+{
+    const uint32_t k[4] = {ks.x, ks.y, ks.z, ks.w};
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+        const uint32_t* row = dist + (size_t)v * kMsRoots;
+#pragma unroll
+        for (uint32_t i = 0; i < 4; i++)
+            if (i < n) region[(size_t)k[i] * V + v] = row[k[i]];
+    }
+}
+
 __global__ void k_srv_copy_u32(const uint32_t* src, uint32_t* dst) { *dst = *src; }
 
 // ------------------------------------------------------------------ state
@@ -474,8 +488,16 @@ static void group_retire(cgb_server* s, Group& G, unsigned long long fin)
     cgb_graph* g = s->g;
     const uint32_t V = g->V;
     cudaStream_t st = G.stream;
-    if (G.alg == CGB_SSSP)
-        k_srv_sp_extract<<<kNumSMs * 8, kBlock, 0, st>>>(G.sp->dist, V, fin, G.region);
+    if (G.alg == CGB_SSSP) {
+        if (__builtin_popcountll(fin) <= 4) {
+            uint32_t k[4] = {0, 0, 0, 0}, n = 0;
+            for (unsigned long long m = fin; m; m &= m - 1) k[n++] = __builtin_ctzll(m);
+            k_srv_sp_extract_cols<<<kNumSMs * 8, kBlock, 0, st>>>(G.sp->dist, V, make_uint4(k[0], k[1], k[2], k[3]), n,
+                                                                  G.region);
+        } else {
+            k_srv_sp_extract<<<kNumSMs * 8, kBlock, 0, st>>>(G.sp->dist, V, fin, G.region);
+        }
+    }
     CGB_CUDA_TRY(cudaMemsetAsync(G.d_stats, 0, offsetof(SlotStats, alive), st));
     k_srv_stats<<<kNumSMs * 4, kBlock, 0, st>>>(G.region, V, g->off, fin, G.d_stats->edges, G.d_stats->reached,
                                                 G.d_stats->depth);
