@@ -369,14 +369,18 @@ __global__ void k_iota_u32(uint32_t n, uint32_t* a)
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = i;
 }
 
-// off[v] = min{j : key[j] >= v} over keys sorted ascending (key(n) = V as
-// sentinel): position j writes off[v] for key(j-1) < v <= key(j).
+// off[v] = min{j : key[j] >= v} over keys sorted ascending, for v in
+// [0, V] (off[V] = n): one lower-bound search per vertex.
 __global__ void k_offsets_from_u32(uint32_t V, uint32_t n, const uint32_t* __restrict__ key, uint32_t* off)
 {
-    for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j <= n; j += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t hi = j < n ? key[j] : V;
-        const uint64_t lo = j == 0 ? 0 : (uint64_t)key[j - 1] + 1;
-        for (uint64_t v = lo; v <= hi; v++) off[v] = (uint32_t)j;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v <= V; v += gridDim.x * blockDim.x) {
+        uint32_t lo = 0, hi = n;
+        while (lo < hi) {
+            const uint32_t mid = lo + (hi - lo) / 2;
+            if (key[mid] < v) lo = mid + 1;
+            else hi = mid;
+        }
+        off[v] = lo;
     }
 }
 
@@ -451,7 +455,7 @@ static void build_transpose(cgb_graph* g)
         uint32_t* in_w = nullptr;
         if (g->w && !g->in_w) in_w = dalloc<uint32_t>(E);  // SSSP pull rounds find the weights in CSC order
         transpose_arrays(g, dsorted, in_src, in_w);
-        k_offsets_from_u32<<<grid_for((uint64_t)E + 1, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(V, E, dsorted,
+        k_offsets_from_u32<<<grid_for((uint64_t)V + 1, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(V, E, dsorted,
                                                                                                       in_off);
         CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
         dfree(dsorted);
@@ -754,7 +758,7 @@ void ensure_pr(cgb_graph* g)
             k_pr_edges<<<grid_for(E, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(V, E, src_off, order, g->off,
                                                                                    g->dst, g->pr_rank, key, val);
             stable_sort_u32(g, key, kout, val, g->pr_src, E, (int)bits_for(V));
-            k_offsets_from_u32<<<grid_for((uint64_t)E + 1, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(
+            k_offsets_from_u32<<<grid_for((uint64_t)V + 1, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(
                 V, E, kout, g->pr_off);
             CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
             dfree(key);
