@@ -364,11 +364,6 @@ __global__ void k_compare_u32(uint64_t n, const uint32_t* __restrict__ a, const 
     }
 }
 
-__global__ void k_iota_u32(uint32_t n, uint32_t* a)
-{
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = i;
-}
-
 // off[v] = min{j : key[j] >= v} over keys sorted ascending, for v in
 // [0, V] (off[V] = n): one lower-bound search per vertex.
 __global__ void k_offsets_from_u32(uint32_t V, uint32_t n, const uint32_t* __restrict__ key, uint32_t* off)
@@ -392,9 +387,20 @@ __global__ void k_edge_sources(uint32_t V, uint32_t E, const uint32_t* __restric
         src[e] = edge_source(off, V, e);
 }
 
-__global__ void k_gather_u32(uint32_t n, const uint32_t* __restrict__ idx, const uint32_t* __restrict__ a, uint32_t* out)
+__global__ void k_pack_u32x2(uint32_t n, const uint32_t* __restrict__ hi, const uint32_t* __restrict__ lo,
+                             uint64_t* out)
 {
-    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) out[j] = a[idx[j]];
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+        out[j] = ((uint64_t)hi[j] << 32) | lo[j];
+}
+
+__global__ void k_unpack_u32x2(uint32_t n, const uint64_t* __restrict__ in, uint32_t* hi, uint32_t* lo)
+{
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const uint64_t x = in[j];
+        hi[j] = (uint32_t)(x >> 32);
+        lo[j] = (uint32_t)x;
+    }
 }
 
 // Stable sort of (key, value) pairs by the key's low `bits` bits: vals_out
@@ -426,15 +432,22 @@ static void transpose_arrays(cgb_graph* g, uint32_t* dst_sorted, uint32_t* in_sr
     if (!in_w) {
         stable_sort_u32(g, g->dst, dst_sorted, src, in_src, E, (int)bits_for(V));
     } else {
-        uint32_t* iota = dalloc<uint32_t>(E);
-        uint32_t* perm = dalloc<uint32_t>(E);
-        k_iota_u32<<<grid, kBlock, 0, g->stream>>>(E, iota);
-        stable_sort_u32(g, g->dst, dst_sorted, iota, perm, E, (int)bits_for(V));
-        k_gather_u32<<<grid, kBlock, 0, g->stream>>>(E, perm, src, in_src);
-        k_gather_u32<<<grid, kBlock, 0, g->stream>>>(E, perm, g->w, in_w);
+        // (source, weight) ride together as one 64-bit value: no gathers afterwards
+        uint64_t* sw = dalloc<uint64_t>(E);
+        uint64_t* sw_sorted = dalloc<uint64_t>(E);
+        k_pack_u32x2<<<grid, kBlock, 0, g->stream>>>(E, src, g->w, sw);
+        size_t tb = 0;
+        CGB_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tb, g->dst, dst_sorted, sw, sw_sorted, (uint64_t)E, 0,
+                                                     (int)bits_for(V), g->stream));
+        void* temp = dalloc<char>(tb);
+        cudaError_t err = cub::DeviceRadixSort::SortPairs(temp, tb, g->dst, dst_sorted, sw, sw_sorted, (uint64_t)E, 0,
+                                                          (int)bits_for(V), g->stream);
+        k_unpack_u32x2<<<grid, kBlock, 0, g->stream>>>(E, sw_sorted, in_src, in_w);
         CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
-        dfree(iota);
-        dfree(perm);
+        dfree(temp);
+        dfree(sw);
+        dfree(sw_sorted);
+        CGB_CUDA_TRY(err);
     }
     CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
     dfree(src);
