@@ -59,6 +59,7 @@ inline cgb_tuning default_tuning()
     t.pr_ctas_per_sm = 128;
     t.sssp_pull_alpha = 0;
     t.cluster_enter = 8192;
+    t.sssp_dense_alpha = 8;
     return t;
 }
 

@@ -99,6 +99,75 @@ struct SsspOp {
     }
 };
 
+// Dense-frontier relaxation: the near set's out-edges lower dist[] with
+// fire-and-forget atomicMin (the result is unused, so it issues as a
+// reduction) and enqueue nothing; k_sssp_dense_scan then finds the improved
+// vertices by comparing dist[] with its snapshot from before the round.
+template <bool kHasW>
+struct SsspDenseOp {
+    const uint32_t* __restrict__ off;
+    const uint32_t* __restrict__ dst;
+    const uint32_t* __restrict__ w;
+    uint32_t* dist;
+
+    __device__ __forceinline__ bool load(uint32_t v, uint32_t& s, uint32_t& d, uint32_t& m) const
+    {
+        s = off[v];
+        d = off[v + 1] - s;
+        m = dist[v];
+        return m < kValueMax;
+    }
+    __device__ __forceinline__ void edge(bool valid, uint32_t e, uint32_t du) const
+    {
+        if (!valid) return;
+        const uint32_t d = __ldcs(dst + e);
+        const uint64_t cand = (uint64_t)du + (kHasW ? (uint64_t)__ldcs(w + e) : 1ull);
+        if (cand < kValueMax && (uint32_t)cand < dist[d]) atomicMin(dist + d, (uint32_t)cand);
+    }
+    __device__ __forceinline__ void block_begin() const {}
+    __device__ __forceinline__ void block_end() const {}
+};
+
+// After a dense round: every vertex whose distance dropped below its snapshot
+// joins the next near queue (below thr) or the far bitmap.  A warp owns one
+// 32-vertex bitmap word, so far bits are set without atomics; the next
+// queue's out-edges and the new far bits are counted.
+__global__ void __launch_bounds__(kBlock) k_sssp_dense_scan(uint32_t V, const uint32_t* __restrict__ dist,
+                                                            const uint32_t* __restrict__ snap, uint32_t thr,
+                                                            uint32_t nz, const uint32_t* __restrict__ off,
+                                                            uint32_t* far_bm, uint32_t* near_out, uint32_t* near_len,
+                                                            uint32_t cap, DevCounters* ctr)
+{
+    const uint32_t n_round = (V + 31u) & ~31u;
+    unsigned long long deg_sum = 0;
+    uint32_t new_far = 0;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n_round; v += gridDim.x * blockDim.x) {
+        bool to_near = false, to_far = false;
+        if (v < V && v < nz) {
+            const uint32_t dv = dist[v];
+            if (dv < snap[v]) {
+                to_near = dv < thr;
+                to_far = !to_near;
+                if (to_near) deg_sum += off[v + 1] - off[v];
+            }
+        }
+        warp_append(to_near, v, near_out, near_len, cap, &ctr->overflow);
+        const uint32_t fm = __ballot_sync(0xffffffffu, to_far);
+        if (fm && lane_id() == 0) {
+            const uint32_t old = far_bm[v >> 5];
+            if (fm & ~old) {
+                far_bm[v >> 5] = old | fm;
+                new_far += __popc(fm & ~old);
+            }
+        }
+    }
+    deg_sum = warp_sum(deg_sum);
+    if (lane_id() == 0) {
+        if (deg_sum) atomicAdd(&ctr->medges, deg_sum);
+        if (new_far) atomicAdd(&ctr->far_len[0], new_far);
+    }
+}
+
 __global__ void k_sssp_init(uint32_t V, uint32_t* dist, uint32_t* far_bm, uint32_t words)
 {
     const uint32_t stride = gridDim.x * blockDim.x;
@@ -216,8 +285,11 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
                 if (r.levels > 0) continue;
             }
             const int out = cur ^ 1;
-            // direction: pull when the near set's out-edges times alpha exceed the graph's edges
+            // direction: pull when the near set's out-edges times alpha exceed the graph's edges;
+            // else a dense frontier when they are a large share by sssp_dense_alpha
             const bool pull = pull_ok && (double)near_edges * g->tune.sssp_pull_alpha > (double)g->E;
+            const bool dense = !pull && o.schedule != CGB_SCHED_FIXED && g->tune.sssp_dense_alpha > 0 &&
+                               (double)near_edges * g->tune.sssp_dense_alpha > (double)g->E;
             if (pull) {
                 ensure_csc(g);
                 ensure_csc_weights(g);
@@ -225,7 +297,7 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
             CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->qlen[out], 0, sizeof(uint32_t), g->stream));
             CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->chunk_len, 0, sizeof(uint32_t), g->stream));
             CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->medges, 0, 8, g->stream));
-            if (!pull) CGB_CUDA_TRY(cudaMemsetAsync(near_bm, 0, (size_t)words * sizeof(uint32_t), g->stream));
+            if (!pull && !dense) CGB_CUDA_TRY(cudaMemsetAsync(near_bm, 0, (size_t)words * sizeof(uint32_t), g->stream));
             if (tracing) CGB_CUDA_TRY(cudaEventRecord(g->ev_iter[0], g->stream));
             if (timing) ktimer_begin(g, pull ? CGB_K_PULL : CGB_K_PUSH);
             if (pull) {
@@ -233,6 +305,15 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
                                 (uint32_t)std::min<uint64_t>(thr, kValueMax), g->q[out], &g->ctr->qlen[out], far_bm,
                                 g->aux_bm);
                 g->stats.pulls_bu++;
+            } else if (dense) {
+                CGB_CUDA_TRY(cudaMemcpyAsync(g->stamp, g->value, (size_t)V * 4, cudaMemcpyDeviceToDevice, g->stream));
+                SsspDenseOp<kHasW> op{g->off, g->dst, g->w, g->value};
+                launch_push(g, g->q[cur], (uint32_t)nnear, op, false);
+                ++g->stats.launches;
+                k_sssp_dense_scan<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(
+                    V, g->value, g->stamp, (uint32_t)std::min<uint64_t>(thr, kValueMax), g->nz, g->off, far_bm,
+                    g->q[out], &g->ctr->qlen[out], V, g->ctr);
+                g->stats.pushes_td++;
             } else {
                 SsspOp<kHasW> op{g->off, g->dst, g->w, g->value, near_bm,
                                  (uint32_t)std::min<uint64_t>(thr, kValueMax), g->nz, g->q[out], &g->ctr->qlen[out],
@@ -252,7 +333,7 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
                 t.algorithm = CGB_SSSP;
                 t.frontier_vertices = nnear;
                 t.unvisited_vertices = g->h_ctr->far_len[0];
-                t.variant = pull ? CGB_VAR_PULL : CGB_VAR_TWC;
+                t.variant = pull ? CGB_VAR_PULL : dense ? CGB_VAR_DENSE : CGB_VAR_TWC;
                 t.frontier_edges = near_edges;
                 t.delta = delta;
                 t.ms = ms;

@@ -33,7 +33,7 @@ bool valid(const cgb_tuning& t)
            t.push_chunk <= 65536 && pow2(t.push_chunk) && t.push_ctas_per_sm >= 1 && t.push_ctas_per_sm <= 32 &&
            t.persist_deg >= 64 && t.persist_deg <= 65536 && t.ms_edges >= kMinMsEdges && t.ms_edges <= 4096 &&
            (t.pr_unroll == 4 || t.pr_unroll == 8 || t.pr_unroll == 16) && t.pr_ctas_per_sm >= 1 &&
-           t.pr_ctas_per_sm <= 1024 && t.persist_ctas <= 4096 && t.sssp_pull_alpha <= 1024 && t.cluster_enter <= (1u << 24);
+           t.pr_ctas_per_sm <= 1024 && t.persist_ctas <= 4096 && t.sssp_pull_alpha <= 1024 && t.cluster_enter <= (1u << 24) && t.sssp_dense_alpha <= 1024;
 }
 
 struct Field {
@@ -53,6 +53,7 @@ std::vector<Field> fields()
         {&cgb_tuning::persist_ctas, {0, 16, 32, 64}, true, true, false, false, false, false},
         {&cgb_tuning::sssp_pull_alpha, {0, 2, 3, 5, 8}, false, true, false, false, false, false},
         {&cgb_tuning::cluster_enter, {0, 2048, 8192, 16384}, true, false, false, false, false, false},
+        {&cgb_tuning::sssp_dense_alpha, {0, 4, 8, 16, 32}, false, true, false, false, false, false},
         {&cgb_tuning::ms_edges, {64, 128, 256, 512, 1024}, false, false, false, false, false, true},
         {&cgb_tuning::pr_unroll, {4, 8, 16}, false, false, false, true, false, false},
         {&cgb_tuning::pr_ctas_per_sm, {16, 32, 64, 128, 256, 1024}, false, false, false, true, false, false},

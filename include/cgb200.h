@@ -60,8 +60,10 @@ typedef enum cgb_schedule {
 typedef enum cgb_variant {
     CGB_VAR_AUTO = 0,
     CGB_VAR_TWC = 1,      /* degree-binned thread / warp / CTA expansion */
-    CGB_VAR_PULL = 2,     /* bottom-up pull over the in-edges (BFS only) */
-    CGB_VAR_PUSH = 3      /* top-down push (BFS: forbid the pull direction) */
+    CGB_VAR_PULL = 2,     /* pull over the in-edges (BFS bottom-up; SSSP pull round) */
+    CGB_VAR_PUSH = 3,     /* top-down push (BFS: forbid the pull direction) */
+    CGB_VAR_DENSE = 4     /* SSSP round with a dense frontier: relax without enqueueing, then
+                             find the improved vertices by one pass over all of them (trace only) */
 } cgb_variant;
 
 typedef struct cgb_options {
@@ -220,7 +222,9 @@ typedef struct {
                                   RMAT-24 the pull kernels lose to the push, the autotuner may pick it) */
     uint32_t cluster_enter;    /* BFS frontiers up to this size run their levels in one thread-block
                                   cluster with a hardware barrier (0 = never, default 8192) */
-    uint32_t reserved[4];
+    uint32_t sssp_dense_alpha; /* SSSP rounds use a dense frontier when the near set's out-edges times
+                                  this exceed E (0 = never, default 8) */
+    uint32_t reserved[3];
 } cgb_tuning;
 
 cgb_status cgb_tuning_get(const cgb_graph* g, int algorithm, cgb_tuning* out);

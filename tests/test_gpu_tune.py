@@ -21,6 +21,8 @@ TUNINGS = [
     {"sssp_pull_alpha": 1000, "persist_enter": 0},
     {"sssp_pull_alpha": 0},
     {"cluster_enter": 0},
+    {"sssp_dense_alpha": 1000},
+    {"sssp_dense_alpha": 0, "sssp_pull_alpha": 0},
     {"cluster_enter": 1 << 20},
 ]
 
