@@ -33,44 +33,97 @@
 namespace cgb {
 
 constexpr uint32_t kLinkRetries = 1u << 20;
+constexpr int kCompressVerts = 4;  // vertices per thread in the compress pass
 
+// Two kinds of access to the forest.  Strong accesses (volatile: no L1,
+// always the current value at L2) and weak ones (plain: may be served from
+// this SM's L1, so possibly stale).  Nearly every path ends at the giant
+// component's root, and strong loads of that one word all queue at one L2
+// slice; weak loads hit L1 instead.  A stale value is still a vertex that
+// was an ancestor once, and pointers only ever move to smaller ancestors,
+// so a weak walk ends at an ancestor of its start: two walks that meet are
+// in one tree, and a vertex it took for a root but is not fails the hooking
+// CAS (which is at L2), after which the roots are found again with strong
+// loads.
+template <bool kStrong>
 __device__ __forceinline__ uint32_t ld_comp(const uint32_t* comp, uint32_t i)
 {
-    return *((volatile const uint32_t*)comp + i);
+    if constexpr (kStrong) return *((volatile const uint32_t*)comp + i);
+    else return comp[i];
 }
 
-// Hooks the trees of u and v, larger root under smaller root.
-// Root of x with path halving: each visited vertex is pointed at its
-// grandparent on the way up.  Concurrent halving is benign: a vertex only
-// ever moves to one of its own ancestors, so every pointer still goes to a
-// smaller vertex of the same tree.
+template <bool kStrong>
+__device__ __forceinline__ void st_comp(uint32_t* comp, uint32_t i, uint32_t v)
+{
+    if constexpr (kStrong) *((volatile uint32_t*)comp + i) = v;
+    else comp[i] = v;
+}
+
+// Roots of x[0..N-1] with path halving: each visited vertex is pointed at
+// its grandparent on the way up.  Concurrent halving is benign: a vertex
+// only ever moves to one of its own ancestors, so every pointer still goes
+// to a smaller vertex of the same tree.  All N paths are walked in one loop
+// (the N loads of a step are independent).
+template <bool kStrong, int N>
+__device__ __forceinline__ void find_roots(uint32_t (&x)[N], uint32_t* comp)
+{
+    uint32_t p[N];
+#pragma unroll
+    for (int i = 0; i < N; i++) p[i] = ld_comp<kStrong>(comp, x[i]);
+    for (uint32_t steps = 0; steps < kLinkRetries; steps++) {
+        bool more = false;
+#pragma unroll
+        for (int i = 0; i < N; i++) more |= p[i] != x[i];
+        if (!more) return;
+        uint32_t gp[N];
+#pragma unroll
+        for (int i = 0; i < N; i++) gp[i] = p[i] != x[i] ? ld_comp<kStrong>(comp, p[i]) : x[i];
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+            if (p[i] != x[i]) {
+                if (gp[i] != p[i]) st_comp<kStrong>(comp, x[i], gp[i]);
+                x[i] = gp[i];
+                p[i] = ld_comp<kStrong>(comp, x[i]);
+            }
+        }
+    }
+}
+
+template <bool kStrong>
 __device__ __forceinline__ uint32_t find_halve(uint32_t x, uint32_t* comp)
 {
-    uint32_t p = ld_comp(comp, x);
-    for (uint32_t steps = 0; p != x && steps < kLinkRetries; steps++) {
-        const uint32_t gp = ld_comp(comp, p);
-        if (gp != p) *((volatile uint32_t*)comp + x) = gp;
-        x = gp;
-        p = ld_comp(comp, x);
-    }
-    return x;
+    uint32_t r[1] = {x};
+    find_roots<kStrong, 1>(r, comp);
+    return r[0];
 }
 
-__device__ __forceinline__ void link(uint32_t u, uint32_t v, uint32_t* comp, DevCounters* ctr)
+// Hooks the trees whose roots were a and b (found a moment ago, possibly by
+// weak loads, so possibly no longer roots): the larger goes under the
+// smaller one.  The CAS succeeds only on a current root; a failed CAS means
+// another thread hooked `high` first (or the walk saw a stale root), and
+// both roots are found again with strong loads.
+__device__ __forceinline__ void hook_roots(uint32_t a, uint32_t b, uint32_t* comp, DevCounters* ctr)
 {
-    uint32_t p1 = find_halve(u, comp), p2 = find_halve(v, comp);
-    for (uint32_t tries = 0; p1 != p2; tries++) {
+    for (uint32_t tries = 0; a != b; tries++) {
         if (tries >= kLinkRetries) {
             atomicOr(&ctr->link_giveup, 1u);
             return;
         }
-        const uint32_t high = max(p1, p2), low = min(p1, p2);
-        // hook the larger root under the smaller one; on failure another
-        // thread hooked `high` first: retry from both roots' new roots
+        const uint32_t high = max(a, b), low = min(a, b);
         if (atomicCAS(comp + high, high, low) == high) return;
-        p1 = find_halve(high, comp);
-        p2 = find_halve(low, comp);
+        uint32_t r[2] = {high, low};
+        find_roots<true, 2>(r, comp);
+        a = r[0];
+        b = r[1];
     }
+}
+
+// Hooks the trees of u and v, larger root under smaller root.
+__device__ __forceinline__ void link(uint32_t u, uint32_t v, uint32_t* comp, DevCounters* ctr)
+{
+    uint32_t r[2] = {u, v};
+    find_roots<false, 2>(r, comp);
+    hook_roots(r[0], r[1], comp, ctr);
 }
 
 __global__ void k_cc_init(uint32_t V, uint32_t* comp)
@@ -102,12 +155,25 @@ __global__ void k_cc_link_round(uint32_t V, const uint32_t* __restrict__ off, co
 }
 
 // Points every vertex at its root (path halving on the way, which shortens
-// the chains that other threads are still walking).
+// the chains that other threads are still walking).  Each thread walks the
+// paths of kN vertices, kN x (grid threads) apart, in one loop.  No hooking
+// runs during this pass, so the set of roots is fixed and weak loads are
+// exact about which vertex is a root (L1 holds nothing from before the
+// launch).
+template <int kN>
 __global__ void k_cc_compress(uint32_t V, uint32_t* comp)
 {
-    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
-        const uint32_t r = find_halve(v, comp);
-        if (ld_comp(comp, v) != r) comp[v] = r;
+    const uint64_t T = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t v0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v0 < V; v0 += kN * T) {
+        uint32_t x[kN];
+#pragma unroll
+        for (int i = 0; i < kN; i++) x[i] = (uint32_t)(v0 + i * T < V ? v0 + i * T : v0);
+        find_roots<false, kN>(x, comp);
+#pragma unroll
+        for (int i = 0; i < kN; i++) {
+            const uint64_t v = v0 + i * T;
+            if (v < V && ld_comp<false>(comp, (uint32_t)v) != x[i]) comp[v] = x[i];
+        }
     }
 }
 
@@ -115,7 +181,7 @@ __global__ void k_cc_sample(uint32_t V, uint32_t* comp, uint32_t* out, uint32_t 
 {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t v = (uint32_t)(mix64(seed ^ i) % V);
-        out[i] = find_halve(v, comp);
+        out[i] = find_halve<true>(v, comp);
     }
 }
 
@@ -132,7 +198,7 @@ struct CcLinkOp {
         s = off[v];
         d = off[v + 1] - s;
         m = v;
-        if (d <= skip || find_halve(v, comp) == giant) return false;
+        if (d <= skip || find_halve<false>(v, comp) == giant) return false;
         s += skip;
         d -= skip;
         return true;
@@ -232,7 +298,7 @@ static void cc_afforest(cgb_graph* g)
     if (timing) ktimer_end(g);
     if (timing) ktimer_begin(g, CGB_K_COMPRESS);
     ++g->stats.launches;
-    k_cc_compress<<<grid, kBlock, 0, g->stream>>>(V, g->value);
+    k_cc_compress<kCompressVerts><<<div_up(V, kBlock * kCompressVerts), kBlock, 0, g->stream>>>(V, g->value);
     if (timing) ktimer_end(g);
     sync_counters(g);
     CGB_REQUIRE(!g->h_ctr->link_giveup, CGB_ETIMEOUT, "CC link retry bound exceeded");
