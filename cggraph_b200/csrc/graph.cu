@@ -165,16 +165,78 @@ __device__ __forceinline__ uint32_t edge_source(const uint32_t* __restrict__ off
     return lo;
 }
 
-// key = src << b | dst (b = bits for V)
-__global__ void k_make_keys(uint32_t V, uint32_t E, const uint32_t* __restrict__ off,
-                            const uint32_t* __restrict__ dst, uint32_t b, uint64_t* keys, bool dst_major)
+// Every edge with its row, tile by tile: a CTA takes kRowTile consecutive
+// edges, finds the rows r0 and r1 of the first and last one by binary search
+// over off, stages off[r0 .. r1 + 1] in shared memory when that range fits
+// (so each edge's search runs there), and calls f(e, r, beg, end) for every
+// edge e of the tile, r being the non-empty row with beg = off[r] <= e <
+// end = off[r + 1].  A tile whose rows do not fit (long runs of empty rows)
+// searches off[r0 .. r1 + 1] in global memory instead.
+constexpr uint32_t kRowTile = 4096;   // edges per tile
+constexpr uint32_t kRowStage = 4096;  // staged offsets per CTA (16 KB)
+
+template <class F>
+__global__ void __launch_bounds__(kBlock) k_edges_by_row(uint32_t V, uint32_t E, const uint32_t* __restrict__ off, F f)
 {
-    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x) {
-        const uint64_t s = edge_source(off, V, e);
-        const uint64_t d = dst[e];
-        keys[e] = dst_major ? ((d << b) | s) : ((s << b) | d);
+    __shared__ uint32_t s_off[kRowStage];
+    __shared__ uint32_t s_r[2];
+    for (uint64_t t0 = (uint64_t)blockIdx.x * kRowTile; t0 < E; t0 += (uint64_t)gridDim.x * kRowTile) {
+        const uint32_t e0 = (uint32_t)t0;
+        const uint32_t e1 = (uint32_t)(t0 + kRowTile < E ? t0 + kRowTile : E);
+        if (threadIdx.x < 2) s_r[threadIdx.x] = edge_source(off, V, threadIdx.x == 0 ? e0 : e1 - 1);
+        __syncthreads();
+        const uint32_t r0 = s_r[0], n = s_r[1] - s_r[0] + 1;  // rows r0 .. r0 + n - 1
+        if (n < kRowStage) {
+            for (uint32_t i = threadIdx.x; i <= n; i += blockDim.x) s_off[i] = off[r0 + i];
+            __syncthreads();
+            for (uint32_t e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+                uint32_t lo = 0, hi = n;  // s_off[lo] <= e < s_off[hi]
+                while (hi - lo > 1) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (s_off[mid] <= e) lo = mid;
+                    else hi = mid;
+                }
+                f(e, r0 + lo, s_off[lo], s_off[lo + 1]);
+            }
+        } else {
+            for (uint32_t e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+                uint32_t lo = r0, hi = r0 + n;  // off[lo] <= e < off[hi]
+                while (hi - lo > 1) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (off[mid] <= e) lo = mid;
+                    else hi = mid;
+                }
+                f(e, lo, off[lo], off[lo + 1]);
+            }
+        }
+        __syncthreads();
     }
 }
+
+template <class F>
+static void launch_edges_by_row(cgb_graph* g, uint32_t V, uint32_t E, const uint32_t* off, const F& f)
+{
+    if (E == 0) return;
+    const uint32_t tiles = div_up(E, kRowTile);
+    k_edges_by_row<<<min(tiles, kNumSMs * 8), kBlock, 0, g->stream>>>(V, E, off, f);
+}
+
+// key = row << b | dst (b = bits for V): sorting the keys sorts every list
+struct RowKeysF {
+    const uint32_t* __restrict__ dst;
+    uint32_t b;
+    uint64_t* keys;
+    __device__ __forceinline__ void operator()(uint32_t e, uint32_t r, uint32_t, uint32_t) const
+    {
+        keys[e] = ((uint64_t)r << b) | dst[e];
+    }
+};
+
+// the source of every edge, in CSR order
+struct RowOutF {
+    uint32_t* rows;
+    __device__ __forceinline__ void operator()(uint32_t e, uint32_t r, uint32_t, uint32_t) const { rows[e] = r; }
+};
 
 __global__ void k_split_keys(uint32_t E, const uint64_t* __restrict__ keys, uint32_t b, uint32_t* low)
 {
@@ -269,7 +331,7 @@ static void sort_neighbours(cgb_graph* g)
     if (g->w) {
         uint64_t* vals = dalloc<uint64_t>(E);
         uint64_t* valt = dalloc<uint64_t>(E);
-        k_make_keys<<<grid, kBlock, 0, g->stream>>>(V, E, g->off, g->dst, b, keys, false);
+        launch_edges_by_row(g, V, E, g->off, RowKeysF{g->dst, b, keys});
         k_widen<<<grid, kBlock, 0, g->stream>>>(E, g->w, vals);
         cub::DoubleBuffer<uint64_t> kb(keys, alt), vb(vals, valt);
         size_t temp_bytes = 0;
@@ -285,7 +347,7 @@ static void sort_neighbours(cgb_graph* g)
         dfree(vals);
         dfree(valt);
     } else {
-        k_make_keys<<<grid, kBlock, 0, g->stream>>>(V, E, g->off, g->dst, b, keys, false);
+        launch_edges_by_row(g, V, E, g->off, RowKeysF{g->dst, b, keys});
         radix_sort_u64(g, keys, alt, E, 2 * b);
         k_split_keys<<<grid, kBlock, 0, g->stream>>>(E, keys, b, g->dst);
         CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
@@ -355,12 +417,22 @@ void compute_weight_sum(cgb_graph* g)
     g->sum_w = h;
 }
 
+// differ = 1 when a and b differ somewhere.  Warps walk the arrays in
+// lockstep; the first warp that sees a difference sets the flag with one
+// atomic, and every warp looks at the flag each 16 steps to stop early.
 __global__ void k_compare_u32(uint64_t n, const uint32_t* __restrict__ a, const uint32_t* __restrict__ b,
                               uint32_t* differ)
 {
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        if ((i & 4095u) == 0 && *(volatile uint32_t*)differ) return;
-        if (a[i] != b[i]) atomicOr(differ, 1u);
+    const uint64_t warps = (uint64_t)gridDim.x * blockDim.x / 32;
+    const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32;
+    uint32_t k = 0;
+    for (uint64_t base = w * 32; base < n; base += warps * 32, k++) {
+        if ((k & 15u) == 0 && *(volatile uint32_t*)differ) return;
+        const uint64_t i = base + lane_id();
+        if (__any_sync(0xffffffffu, i < n && a[i] != b[i])) {
+            if (lane_id() == 0) atomicOr(differ, 1u);
+            return;
+        }
     }
 }
 
@@ -377,14 +449,6 @@ __global__ void k_offsets_from_u32(uint32_t V, uint32_t n, const uint32_t* __res
         }
         off[v] = lo;
     }
-}
-
-// Source of every edge, in CSR order (consecutive edges share their search
-// path, so the binary searches stay in cache).
-__global__ void k_edge_sources(uint32_t V, uint32_t E, const uint32_t* __restrict__ off, uint32_t* src)
-{
-    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x)
-        src[e] = edge_source(off, V, e);
 }
 
 __global__ void k_pack_u32x2(uint32_t n, const uint32_t* __restrict__ hi, const uint32_t* __restrict__ lo,
@@ -428,7 +492,7 @@ static void transpose_arrays(cgb_graph* g, uint32_t* dst_sorted, uint32_t* in_sr
     const uint32_t E = g->E, V = g->V;
     const uint32_t grid = grid_for(E, kBlock, kNumSMs * 16);
     uint32_t* src = dalloc<uint32_t>(E);
-    k_edge_sources<<<grid, kBlock, 0, g->stream>>>(V, E, g->off, src);
+    launch_edges_by_row(g, V, E, g->off, RowOutF{src});
     if (!in_w) {
         stable_sort_u32(g, g->dst, dst_sorted, src, in_src, E, (int)bits_for(V));
     } else {
@@ -465,17 +529,12 @@ static void build_transpose(cgb_graph* g)
         CGB_CUDA_TRY(cudaMemsetAsync(in_off, 0, ((size_t)V + 1) * sizeof(uint32_t), g->stream));
     } else {
         uint32_t* dsorted = dalloc<uint32_t>(E);
-        uint32_t* in_w = nullptr;
-        if (g->w && !g->in_w) in_w = dalloc<uint32_t>(E);  // SSSP pull rounds find the weights in CSC order
-        transpose_arrays(g, dsorted, in_src, in_w);
+        // weights in CSC order are built on first need (ensure_csc_weights)
+        transpose_arrays(g, dsorted, in_src, nullptr);
         k_offsets_from_u32<<<grid_for((uint64_t)V + 1, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(V, E, dsorted,
                                                                                                       in_off);
         CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
         dfree(dsorted);
-        if (in_w) {
-            g->in_w = in_w;
-            g->in_w_owned = true;
-        }
     }
     uint32_t* differ = dalloc<uint32_t>(1);
     CGB_CUDA_TRY(cudaMemsetAsync(differ, 0, sizeof(uint32_t), g->stream));
@@ -522,10 +581,9 @@ void ensure_csc_weights(cgb_graph* g)
 {
     if (!g->w || g->in_w) return;
     ensure_csc(g);
-    if (g->in_w) return;  // built with the transpose
-    // the CSR serves as CSC (symmetric structure): transpose the weights by
-    // sorting (dst, src) keys with the weights as values, then alias w when
-    // they are symmetric too
+    // transpose the weights: a stable sort by destination lists every
+    // in-list by source, the order of in_src; alias w when the result equals
+    // it (a symmetric graph with symmetric weights)
     const uint32_t V = g->V, E = g->E;
     if (E == 0) {
         g->in_w = g->w;
@@ -642,37 +700,42 @@ __global__ void k_row_bounds(const uint32_t* __restrict__ rows, uint32_t n, cons
 }
 
 // Edges of the relabelled graph in new-source order: position p of the
-// out-list of order[r] (r = new source) gives key = new destination and
-// value = r; a stable sort by key then lists each new row's sources in
-// ascending new ids.
-__global__ void k_pr_edges(uint32_t V, uint32_t E, const uint32_t* __restrict__ src_off,
-                           const uint32_t* __restrict__ order, const uint32_t* __restrict__ off,
-                           const uint32_t* __restrict__ dst, const uint32_t* __restrict__ rank, uint32_t* key,
-                           uint32_t* val)
-{
-    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < E; p += gridDim.x * blockDim.x) {
-        const uint32_t r = edge_source(src_off, V, p);
-        key[p] = rank[dst[off[order[r]] + (p - src_off[r])]];
+// out-list of order[r] (r = new source, its list at [beg, end) of the
+// relabelled out-offsets) gives key = new destination and value = r; a
+// stable sort by key then lists each new row's sources in ascending new ids.
+struct PrEdgesF {
+    const uint32_t* __restrict__ order;
+    const uint32_t* __restrict__ off;
+    const uint32_t* __restrict__ dst;
+    const uint32_t* __restrict__ rank;
+    uint32_t* key;
+    uint32_t* val;
+    __device__ __forceinline__ void operator()(uint32_t p, uint32_t r, uint32_t beg, uint32_t) const
+    {
+        key[p] = rank[dst[off[order[r]] + (p - beg)]];
         val[p] = r;
     }
-}
+};
 
-// SELL columns of the non-hub rows from the relabelled CSC (pr_off,
-// pr_src); hub rows are marked in hub_bm and summed from pr_src.
-__global__ void k_sell_fill(uint32_t V, uint32_t E, const uint32_t* __restrict__ pr_off,
-                            const uint32_t* __restrict__ pr_src, const uint64_t* __restrict__ slice_ptr, uint32_t hub,
-                            uint32_t* col, uint32_t* hub_bm)
-{
-    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < E; p += gridDim.x * blockDim.x) {
-        const uint32_t r = edge_source(pr_off, V, p);
-        const uint32_t j = p - pr_off[r];
-        if (pr_off[r + 1] - pr_off[r] >= hub) {
+// SELL columns of the non-hub rows from the relabelled CSC (rows at
+// [beg, end) of pr_src); hub rows are marked in hub_bm and summed from
+// pr_src.
+struct SellFillF {
+    const uint32_t* __restrict__ pr_src;
+    const uint64_t* __restrict__ slice_ptr;
+    uint32_t hub;
+    uint32_t* col;
+    uint32_t* hub_bm;
+    __device__ __forceinline__ void operator()(uint32_t p, uint32_t r, uint32_t beg, uint32_t end) const
+    {
+        const uint32_t j = p - beg;
+        if (end - beg >= hub) {
             if (j == 0) atomicOr(hub_bm + (r >> 5), 1u << (r & 31u));
-            continue;
+            return;
         }
         col[slice_ptr[r >> 5] + 32ull * j + (r & 31u)] = pr_src[p];
     }
-}
+};
 
 // Sliced ELL layout of the non-hub rows (slice lengths, offsets, the column
 // array filled with the padding target V); k_sell_fill writes the columns.
@@ -768,8 +831,7 @@ void ensure_pr(cgb_graph* g)
             uint32_t* key = dalloc<uint32_t>(E);
             uint32_t* val = dalloc<uint32_t>(E);
             uint32_t* kout = dalloc<uint32_t>(E);
-            k_pr_edges<<<grid_for(E, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(V, E, src_off, order, g->off,
-                                                                                   g->dst, g->pr_rank, key, val);
+            launch_edges_by_row(g, V, E, src_off, PrEdgesF{order, g->off, g->dst, g->pr_rank, key, val});
             stable_sort_u32(g, key, kout, val, g->pr_src, E, (int)bits_for(V));
             k_offsets_from_u32<<<grid_for((uint64_t)V + 1, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(
                 V, E, kout, g->pr_off);
@@ -783,8 +845,8 @@ void ensure_pr(cgb_graph* g)
         dfree(src_off);
         build_sell(g);
         if (E)
-            k_sell_fill<<<grid_for(E, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(
-                V, E, g->pr_off, g->pr_src, g->pr_slice_ptr, kPrHuge, g->pr_col, g->pr_hub_bm);
+            launch_edges_by_row(g, V, E, g->pr_off,
+                                SellFillF{g->pr_src, g->pr_slice_ptr, kPrHuge, g->pr_col, g->pr_hub_bm});
         CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
         dfree(order);
     }
