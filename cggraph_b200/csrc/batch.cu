@@ -216,7 +216,7 @@ cgb_status cgb_batch_create(uint32_t n, const uint32_t* const* offsets, const ui
             CGB_CUDA_TRY(cudaMemcpy(b->d_base, b->base.data(), (n + 1) * 4ull, cudaMemcpyHostToDevice));
             CGB_CUDA_TRY(cudaMalloc((void**)&b->sx, sizeof(PersistSssp)));
             ensure_frontier(g);
-            if (!g->persist) CGB_CUDA_TRY(cudaMalloc(&g->persist, sizeof(PersistState)));
+            if (!g->persist) g->persist = pool_alloc(sizeof(PersistState), g->stream);
             b->delta = sssp_default_delta(g);
         } catch (...) {
             if (b->g) graph_free(b->g);

@@ -192,6 +192,9 @@ void free_msbfs(cgb_graph* g);
 void run_mssp(cgb_graph* g, const uint32_t* d_roots, uint32_t n, uint32_t* out, uint32_t delta);
 void free_mssp(cgb_graph* g);
 // Pinned host blocks of at most 256 bytes from process-lifetime slabs.
+// Device memory from the engine's pool, allocated in the order of stream s
+// (and complete on return); released with the graph (graph_free).
+void* pool_alloc(size_t bytes, cudaStream_t s);
 void* pinned_small_alloc(size_t bytes);
 void pinned_small_free(void* p);
 // Weights in CSC order (in_w); needs the graph's weights.

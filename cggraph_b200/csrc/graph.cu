@@ -20,12 +20,17 @@ const std::string& last_error() { return t_last_error; }
 // keeps freed memory cached (release threshold: never), so creating a graph
 // after destroying another reuses the same pages: plain cudaFree of tens of
 // GB returns them to the driver and can stall for hundreds of milliseconds.
-// dalloc waits for its allocation, so the memory is usable on every stream;
-// dfree keeps cudaFree's device-wide synchronisation before the release.
+// dalloc and dfree are ordered on the stream that uses the block (the
+// graph's stream for everything here): a block freed on a stream is reused
+// at once by the next allocation on it, and neither call waits for the
+// device.  A block freed on another graph's stream is reused only once that
+// free has happened (the allocation never waits for the other stream);
+// otherwise the pool grows, and keeps what it grew by for later graphs.
+// graph_alloc completes the graph's own buffers before returning, so they
+// are usable on every stream.
 namespace {
 struct DevicePool {
     cudaMemPool_t pool = nullptr;
-    cudaStream_t stream = nullptr;
 };
 std::mutex g_pool_mu;
 DevicePool g_pools[64];
@@ -45,29 +50,35 @@ DevicePool& device_pool()
         CGB_CUDA_TRY(cudaMemPoolCreate(&p.pool, &props));
         uint64_t keep = ~0ull;
         CGB_CUDA_TRY(cudaMemPoolSetAttribute(p.pool, cudaMemPoolAttrReleaseThreshold, &keep));
-        CGB_CUDA_TRY(cudaStreamCreateWithFlags(&p.stream, cudaStreamNonBlocking));
+        // a block freed on one graph's stream is reused only once that free
+        // has happened (never by making the allocation wait for that stream)
+        int no = 0;
+        CGB_CUDA_TRY(cudaMemPoolSetAttribute(p.pool, cudaMemPoolReuseAllowInternalDependencies, &no));
     }
     return p;
 }
 }  // namespace
 
 template <typename T>
-static T* dalloc(size_t n)
+static T* dalloc(size_t n, cudaStream_t s)
 {
     void* p = nullptr;
     if (n == 0) n = 1;
-    DevicePool& dp = device_pool();
-    CGB_CUDA_TRY(cudaMallocFromPoolAsync(&p, n * sizeof(T), dp.pool, dp.stream));
-    CGB_CUDA_TRY(cudaStreamSynchronize(dp.stream));
+    CGB_CUDA_TRY(cudaMallocFromPoolAsync(&p, n * sizeof(T), device_pool().pool, s));
     return (T*)p;
 }
 
-static void dfree(void* p)
+static void dfree(void* p, cudaStream_t s)
 {
     if (!p) return;
-    DevicePool& dp = device_pool();
-    cudaDeviceSynchronize();  // as cudaFree: nothing may still use p
-    cudaFreeAsync(p, dp.stream);
+    cudaFreeAsync(p, s);
+}
+
+void* pool_alloc(size_t bytes, cudaStream_t s)
+{
+    void* p = dalloc<char>(bytes, s);
+    CGB_CUDA_TRY(cudaStreamSynchronize(s));
+    return p;
 }
 
 // Small pinned host blocks (each graph's counter mirror) come from slabs that
@@ -104,8 +115,19 @@ void memory_trim(int device)
 {
     CGB_CUDA_TRY(cudaSetDevice(device));
     DevicePool& dp = device_pool();
-    CGB_CUDA_TRY(cudaStreamSynchronize(dp.stream));
+    CGB_CUDA_TRY(cudaDeviceSynchronize());  // every pending free has happened
     CGB_CUDA_TRY(cudaMemPoolTrimTo(dp.pool, 0));
+}
+
+void memory_info(int device, uint64_t* reserved, uint64_t* used)
+{
+    CGB_CUDA_TRY(cudaSetDevice(device));
+    DevicePool& dp = device_pool();
+    uint64_t r = 0, u = 0;
+    CGB_CUDA_TRY(cudaMemPoolGetAttribute(dp.pool, cudaMemPoolAttrReservedMemCurrent, &r));
+    CGB_CUDA_TRY(cudaMemPoolGetAttribute(dp.pool, cudaMemPoolAttrUsedMemCurrent, &u));
+    if (reserved) *reserved = r;
+    if (used) *used = u;
 }
 
 static uint32_t bits_for(uint64_t n)  // bits to represent values < n
@@ -138,19 +160,44 @@ __global__ void k_mark_heads(uint32_t V, const uint32_t* __restrict__ off, uint3
 }
 
 // bad |= 8 for an id >= V; unsorted |= 1 where a list is not strictly
-// ascending; dup |= 1 where it has equal neighbours.
+// ascending; dup |= 1 where it has equal neighbours.  A warp reads 32 x 8
+// consecutive entries with independent loads and takes each entry's
+// successor from the next lane (the last lane reads one entry more).
+constexpr uint32_t kCheckRuns = 8;
+
 __global__ void k_check_edges(uint32_t V, uint32_t E, const uint32_t* __restrict__ dst,
                               const uint32_t* __restrict__ heads, uint32_t* flags)
 {
-    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x) {
-        const uint32_t d = dst[e];
-        if (d >= V) atomicOr(flags, 8u);
-        if (e + 1 < E && !((heads[(e + 1) >> 5] >> ((e + 1) & 31u)) & 1u)) {
-            const uint32_t d2 = dst[e + 1];
-            if (d > d2) atomicOr(flags + 1, 1u);
-            else if (d == d2) atomicOr(flags + 2, 1u);
+    const uint64_t warps = (uint64_t)gridDim.x * blockDim.x / 32;
+    const uint32_t lane = lane_id();
+    uint32_t bad = 0, unsorted = 0, dup = 0;
+    for (uint64_t base = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32 * 32 * kCheckRuns; base < E;
+         base += warps * 32 * kCheckRuns) {
+        uint32_t d[kCheckRuns], nx[kCheckRuns], hw[kCheckRuns];
+#pragma unroll
+        for (uint32_t k = 0; k < kCheckRuns; k++) {
+            const uint64_t e = base + k * 32 + lane;
+            d[k] = e < E ? dst[e] : 0;
+            nx[k] = (lane == 31 && e + 1 < E) ? dst[e + 1] : 0;
+            hw[k] = e + 1 < E ? heads[(e + 1) >> 5] : 0;
+        }
+#pragma unroll
+        for (uint32_t k = 0; k < kCheckRuns; k++) {
+            const uint64_t e = base + k * 32 + lane;
+            const uint32_t down = __shfl_down_sync(0xffffffffu, d[k], 1);
+            const uint32_t next = lane == 31 ? nx[k] : down;
+            if (e < E) {
+                bad |= d[k] >= V;
+                if (e + 1 < E && !((hw[k] >> ((e + 1) & 31u)) & 1u)) {
+                    unsorted |= d[k] > next;
+                    dup |= d[k] == next;
+                }
+            }
         }
     }
+    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(flags, 8u);
+    if (__any_sync(0xffffffffu, unsorted) && lane == 0) atomicOr(flags + 1, 1u);
+    if (__any_sync(0xffffffffu, dup) && lane == 0) atomicOr(flags + 2, 1u);
 }
 
 // Source vertex of edge e: last v with off[v] <= e (skipping empty lists).
@@ -165,38 +212,100 @@ __device__ __forceinline__ uint32_t edge_source(const uint32_t* __restrict__ off
     return lo;
 }
 
-// Every edge with its row, tile by tile: a CTA takes kRowTile consecutive
-// edges, finds the rows r0 and r1 of the first and last one by binary search
-// over off, stages off[r0 .. r1 + 1] in shared memory when that range fits
-// (so each edge's search runs there), and calls f(e, r, beg, end) for every
-// edge e of the tile, r being the non-empty row with beg = off[r] <= e <
-// end = off[r + 1].  A tile whose rows do not fit (long runs of empty rows)
-// searches off[r0 .. r1 + 1] in global memory instead.
-constexpr uint32_t kRowTile = 4096;   // edges per tile
-constexpr uint32_t kRowStage = 4096;  // staged offsets per CTA (16 KB)
+// Every edge with its row, tile by tile.  trow[t] is the row of tile t's
+// first edge (trow[ntiles] that of the last edge), found for all tiles at
+// once by k_tile_rows.  A CTA stages off[trow[t] .. trow[t + 1] + 1] in
+// shared memory and marks the first edge of every row that starts inside
+// the tile with that row's index; each warp then takes 32 edges at a time
+// and gives each the last mark at or before it (a max-scan across the
+// lanes, carried from round to round), starting from the row of its first
+// edge.  For every edge e of the tile, r being the non-empty row with beg =
+// off[r] <= e < end = off[r + 1], it calls f.store(e, r, beg, end,
+// f.load(e, r, beg, end)) with the warp's lanes on consecutive edges; the
+// loads of F::kBatch rounds are issued before their stores, so a functor's
+// gathers can be in flight together (a larger batch holds more registers:
+// worth it for a long chain of dependent gathers, not for one or two).  A tile spanning kRowStage rows or
+// more (long runs of empty rows) searches off in global memory per edge
+// instead.  Each thread works on its own copy of f; f.tile_end() runs on
+// every thread after each tile (the warp still converged), and f.stop() is
+// asked before each tile (a functor that has found its answer ends the
+// pass).
+constexpr uint32_t kRowTile = 4096;        // edges per tile
+constexpr uint32_t kRowStage = 4096 + 64;  // staged offsets per CTA: a tile of one-edge rows fits
+
+__global__ void k_tile_rows(uint32_t V, uint32_t E, const uint32_t* __restrict__ off, uint32_t ntiles, uint32_t* trow)
+{
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t <= ntiles; t += gridDim.x * blockDim.x) {
+        const uint64_t e = (uint64_t)t * kRowTile;
+        trow[t] = edge_source(off, V, (uint32_t)(e < E ? e : E - 1));
+    }
+}
 
 template <class F>
-__global__ void __launch_bounds__(kBlock) k_edges_by_row(uint32_t V, uint32_t E, const uint32_t* __restrict__ off, F f)
+__global__ void __launch_bounds__(kBlock) k_edges_by_row(uint32_t E, const uint32_t* __restrict__ off,
+                                                         const uint32_t* __restrict__ trow, F fp)
 {
+    F f = fp;
+    constexpr uint32_t kSeg = kRowTile / (kBlock / 32);  // edges per warp and tile
+    constexpr uint32_t kRounds = kSeg / 32;
+    constexpr uint32_t kBatch = F::kBatch;  // rounds whose loads are issued before their stores
     __shared__ uint32_t s_off[kRowStage];
+    __shared__ uint16_t s_mark[kRowTile];  // 1 + row index at a row's first edge, else 0
     __shared__ uint32_t s_r[2];
+    __shared__ bool s_stop;
+    const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
     for (uint64_t t0 = (uint64_t)blockIdx.x * kRowTile; t0 < E; t0 += (uint64_t)gridDim.x * kRowTile) {
         const uint32_t e0 = (uint32_t)t0;
         const uint32_t e1 = (uint32_t)(t0 + kRowTile < E ? t0 + kRowTile : E);
-        if (threadIdx.x < 2) s_r[threadIdx.x] = edge_source(off, V, threadIdx.x == 0 ? e0 : e1 - 1);
+        if (threadIdx.x == 0) s_stop = f.stop();  // one read, so the whole CTA agrees
+        if (threadIdx.x < 2) s_r[threadIdx.x] = trow[t0 / kRowTile + threadIdx.x];
+        for (uint32_t i = threadIdx.x; i < kRowTile; i += blockDim.x) s_mark[i] = 0;
         __syncthreads();
-        const uint32_t r0 = s_r[0], n = s_r[1] - s_r[0] + 1;  // rows r0 .. r0 + n - 1
+        if (s_stop) return;
+        const uint32_t r0 = s_r[0], n = s_r[1] - s_r[0] + 1;  // rows r0 .. r0 + n - 1 cover the tile
         if (n < kRowStage) {
             for (uint32_t i = threadIdx.x; i <= n; i += blockDim.x) s_off[i] = off[r0 + i];
             __syncthreads();
-            for (uint32_t e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
-                uint32_t lo = 0, hi = n;  // s_off[lo] <= e < s_off[hi]
+            // rows after r0 (which holds e0) that start inside the tile
+            for (uint32_t i = 1 + threadIdx.x; i < n; i += blockDim.x) {
+                const uint32_t b = s_off[i];
+                if (s_off[i + 1] > b && b < e1) s_mark[b - e0] = (uint16_t)(i + 1);
+            }
+            __syncthreads();
+            const uint32_t sb = e0 + warp * kSeg;
+            if (sb < e1) {
+                uint32_t lo = 0, hi = n;  // the row of sb: s_off[lo] <= sb < s_off[hi]
                 while (hi - lo > 1) {
                     const uint32_t mid = (lo + hi) >> 1;
-                    if (s_off[mid] <= e) lo = mid;
+                    if (s_off[mid] <= sb) lo = mid;
                     else hi = mid;
                 }
-                f(e, r0 + lo, s_off[lo], s_off[lo + 1]);
+                // rows of all rounds first, then the calls: their loads are
+                // independent of one another and can be in flight together
+                uint32_t carry = lo, rel[kRounds];
+#pragma unroll
+                for (uint32_t k = 0; k < kRounds; k++) {
+                    const uint32_t x = s_mark[warp * kSeg + k * 32 + lane];  // 0 past e1
+                    // the last marked lane at or below this one names the row
+                    const uint32_t below = __ballot_sync(0xffffffffu, x != 0) & (0xffffffffu >> (31 - lane));
+                    const uint32_t y = __shfl_sync(0xffffffffu, x, below ? 31 - __clz(below) : 0);
+                    rel[k] = below ? y - 1 : carry;
+                    carry = __shfl_sync(0xffffffffu, rel[k], 31);
+                }
+#pragma unroll
+                for (uint32_t k0 = 0; k0 < kRounds; k0 += kBatch) {
+                    typename F::Val v[kBatch];
+#pragma unroll
+                    for (uint32_t k = 0; k < kBatch; k++) {
+                        const uint32_t e = sb + (k0 + k) * 32 + lane, q = rel[k0 + k];
+                        if (e < e1) v[k] = f.load(e, r0 + q, s_off[q], s_off[q + 1]);
+                    }
+#pragma unroll
+                    for (uint32_t k = 0; k < kBatch; k++) {
+                        const uint32_t e = sb + (k0 + k) * 32 + lane, q = rel[k0 + k];
+                        if (e < e1) f.store(e, r0 + q, s_off[q], s_off[q + 1], v[k]);
+                    }
+                }
             }
         } else {
             for (uint32_t e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
@@ -206,9 +315,10 @@ __global__ void __launch_bounds__(kBlock) k_edges_by_row(uint32_t V, uint32_t E,
                     if (off[mid] <= e) lo = mid;
                     else hi = mid;
                 }
-                f(e, lo, off[lo], off[lo + 1]);
+                f.store(e, lo, off[lo], off[lo + 1], f.load(e, lo, off[lo], off[lo + 1]));
             }
         }
+        f.tile_end();
         __syncthreads();
     }
 }
@@ -218,24 +328,37 @@ static void launch_edges_by_row(cgb_graph* g, uint32_t V, uint32_t E, const uint
 {
     if (E == 0) return;
     const uint32_t tiles = div_up(E, kRowTile);
-    k_edges_by_row<<<min(tiles, kNumSMs * 8), kBlock, 0, g->stream>>>(V, E, off, f);
+    uint32_t* trow = dalloc<uint32_t>((size_t)tiles + 1, g->stream);
+    k_tile_rows<<<grid_for((uint64_t)tiles + 1, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, E, off, tiles, trow);
+    k_edges_by_row<<<min(tiles, kNumSMs * 8), kBlock, 0, g->stream>>>(E, off, trow, f);  // 24 KB each
+    dfree(trow, g->stream);
 }
 
 // key = row << b | dst (b = bits for V): sorting the keys sorts every list
 struct RowKeysF {
+    static constexpr uint32_t kBatch = 1;
+    __device__ __forceinline__ bool stop() const { return false; }
+    __device__ __forceinline__ void tile_end() {}
     const uint32_t* __restrict__ dst;
     uint32_t b;
-    uint64_t* keys;
-    __device__ __forceinline__ void operator()(uint32_t e, uint32_t r, uint32_t, uint32_t) const
+    uint64_t* __restrict__ keys;
+    using Val = uint32_t;
+    __device__ __forceinline__ Val load(uint32_t e, uint32_t, uint32_t, uint32_t) const { return __ldg(dst + e); }
+    __device__ __forceinline__ void store(uint32_t e, uint32_t r, uint32_t, uint32_t, Val d)
     {
-        keys[e] = ((uint64_t)r << b) | dst[e];
+        keys[e] = ((uint64_t)r << b) | d;
     }
 };
 
 // the source of every edge, in CSR order
 struct RowOutF {
-    uint32_t* rows;
-    __device__ __forceinline__ void operator()(uint32_t e, uint32_t r, uint32_t, uint32_t) const { rows[e] = r; }
+    static constexpr uint32_t kBatch = 1;
+    __device__ __forceinline__ bool stop() const { return false; }
+    __device__ __forceinline__ void tile_end() {}
+    uint32_t* __restrict__ rows;
+    using Val = uint32_t;
+    __device__ __forceinline__ Val load(uint32_t, uint32_t, uint32_t, uint32_t) const { return 0; }
+    __device__ __forceinline__ void store(uint32_t e, uint32_t r, uint32_t, uint32_t, Val) { rows[e] = r; }
 };
 
 __global__ void k_split_keys(uint32_t E, const uint64_t* __restrict__ keys, uint32_t b, uint32_t* low)
@@ -311,10 +434,10 @@ static void radix_sort_u64(cgb_graph* g, uint64_t*& keys, uint64_t*& alt, uint64
     cub::DoubleBuffer<uint64_t> db(keys, alt);
     size_t temp_bytes = 0;
     CGB_CUDA_TRY(cub::DeviceRadixSort::SortKeys(nullptr, temp_bytes, db, n, 0, end_bit, g->stream));
-    void* temp = dalloc<char>(temp_bytes);
+    void* temp = dalloc<char>(temp_bytes, g->stream);
     cudaError_t err = cub::DeviceRadixSort::SortKeys(temp, temp_bytes, db, n, 0, end_bit, g->stream);
     CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
-    dfree(temp);
+    dfree(temp, g->stream);
     CGB_CUDA_TRY(err);
     if (db.Current() != keys) std::swap(keys, alt);
 }
@@ -325,58 +448,58 @@ static void sort_neighbours(cgb_graph* g)
 {
     const uint32_t V = g->V, E = g->E;
     const uint32_t b = bits_for(V);
-    uint64_t* keys = dalloc<uint64_t>(E);
-    uint64_t* alt = dalloc<uint64_t>(E);
+    uint64_t* keys = dalloc<uint64_t>(E, g->stream);
+    uint64_t* alt = dalloc<uint64_t>(E, g->stream);
     const uint32_t grid = grid_for(E, kBlock, kNumSMs * 16);
     if (g->w) {
-        uint64_t* vals = dalloc<uint64_t>(E);
-        uint64_t* valt = dalloc<uint64_t>(E);
+        uint64_t* vals = dalloc<uint64_t>(E, g->stream);
+        uint64_t* valt = dalloc<uint64_t>(E, g->stream);
         launch_edges_by_row(g, V, E, g->off, RowKeysF{g->dst, b, keys});
         k_widen<<<grid, kBlock, 0, g->stream>>>(E, g->w, vals);
         cub::DoubleBuffer<uint64_t> kb(keys, alt), vb(vals, valt);
         size_t temp_bytes = 0;
         CGB_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, kb, vb, (uint64_t)E, 0, 2 * b, g->stream));
-        void* temp = dalloc<char>(temp_bytes);
+        void* temp = dalloc<char>(temp_bytes, g->stream);
         cudaError_t err = cub::DeviceRadixSort::SortPairs(temp, temp_bytes, kb, vb, (uint64_t)E, 0, 2 * b, g->stream);
         CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
-        dfree(temp);
+        dfree(temp, g->stream);
         CGB_CUDA_TRY(err);
         k_split_keys<<<grid, kBlock, 0, g->stream>>>(E, kb.Current(), b, g->dst);
         k_narrow<<<grid, kBlock, 0, g->stream>>>(E, vb.Current(), g->w);
         CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
-        dfree(vals);
-        dfree(valt);
+        dfree(vals, g->stream);
+        dfree(valt, g->stream);
     } else {
         launch_edges_by_row(g, V, E, g->off, RowKeysF{g->dst, b, keys});
         radix_sort_u64(g, keys, alt, E, 2 * b);
         k_split_keys<<<grid, kBlock, 0, g->stream>>>(E, keys, b, g->dst);
         CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
     }
-    dfree(keys);
-    dfree(alt);
+    dfree(keys, g->stream);
+    dfree(alt, g->stream);
 }
 
 void validate_and_sort(cgb_graph* g)
 {
     const uint32_t V = g->V, E = g->E;
-    uint32_t* flags = dalloc<uint32_t>(4);
+    uint32_t* flags = dalloc<uint32_t>(4, g->stream);
     CGB_CUDA_TRY(cudaMemsetAsync(flags, 0, 4 * sizeof(uint32_t), g->stream));
     k_check_offsets<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, E, g->off, flags);
     uint32_t h[4];
     CGB_CUDA_TRY(cudaMemcpyAsync(h, flags, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
     CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
     if (h[0]) {
-        dfree(flags);
+        dfree(flags, g->stream);
         if (h[0] & 2u) throw Error{CGB_EFORMAT, "csr_offset[0] != 0"};
         if (h[0] & 4u) throw Error{CGB_EFORMAT, "csr_offset[V] != E"};
         throw Error{CGB_EFORMAT, "csr_offset is not non-decreasing"};
     }
     if (E == 0) {
-        dfree(flags);
+        dfree(flags, g->stream);
         return;
     }
     const uint32_t hw = E / 32 + 2;
-    uint32_t* heads = dalloc<uint32_t>(hw);
+    uint32_t* heads = dalloc<uint32_t>(hw, g->stream);
     for (int pass = 0; pass < 2; pass++) {
         CGB_CUDA_TRY(cudaMemsetAsync(heads, 0, hw * sizeof(uint32_t), g->stream));
         CGB_CUDA_TRY(cudaMemsetAsync(flags, 0, 4 * sizeof(uint32_t), g->stream));
@@ -385,8 +508,8 @@ void validate_and_sort(cgb_graph* g)
         CGB_CUDA_TRY(cudaMemcpyAsync(h, flags, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
         CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
         if (h[0] & 8u) {
-            dfree(heads);
-            dfree(flags);
+            dfree(heads, g->stream);
+            dfree(flags, g->stream);
             throw Error{CGB_EFORMAT, "csr_dest holds a vertex id >= V"};
         }
         if (pass == 0 && h[1]) {
@@ -394,26 +517,26 @@ void validate_and_sort(cgb_graph* g)
             continue;
         }
         if (h[1] || h[2]) {
-            dfree(heads);
-            dfree(flags);
+            dfree(heads, g->stream);
+            dfree(flags, g->stream);
             throw Error{CGB_EFORMAT, "neighbour list not strictly ascending after sorting (duplicate edge)"};
         }
         break;
     }
-    dfree(heads);
-    dfree(flags);
+    dfree(heads, g->stream);
+    dfree(flags, g->stream);
 }
 
 void compute_weight_sum(cgb_graph* g)
 {
     if (!g->w || g->E == 0) return;
-    unsigned long long* d = dalloc<unsigned long long>(1);
+    unsigned long long* d = dalloc<unsigned long long>(1, g->stream);
     CGB_CUDA_TRY(cudaMemsetAsync(d, 0, sizeof(unsigned long long), g->stream));
     k_sum_u32<<<grid_for(g->E, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(g->E, g->w, d);
     unsigned long long h = 0;
     CGB_CUDA_TRY(cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
     CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
-    dfree(d);
+    dfree(d, g->stream);
     g->sum_w = h;
 }
 
@@ -475,11 +598,11 @@ static void stable_sort_u32(cgb_graph* g, const uint32_t* keys_in, uint32_t* key
     size_t tb = 0;
     CGB_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tb, keys_in, keys_out, vals_in, vals_out, (uint64_t)n, 0,
                                                  bits, g->stream));
-    void* temp = dalloc<char>(tb);
+    void* temp = dalloc<char>(tb, g->stream);
     cudaError_t err = cub::DeviceRadixSort::SortPairs(temp, tb, keys_in, keys_out, vals_in, vals_out, (uint64_t)n, 0,
                                                       bits, g->stream);
     CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
-    dfree(temp);
+    dfree(temp, g->stream);
     CGB_CUDA_TRY(err);
 }
 
@@ -491,30 +614,162 @@ static void transpose_arrays(cgb_graph* g, uint32_t* dst_sorted, uint32_t* in_sr
 {
     const uint32_t E = g->E, V = g->V;
     const uint32_t grid = grid_for(E, kBlock, kNumSMs * 16);
-    uint32_t* src = dalloc<uint32_t>(E);
+    uint32_t* src = dalloc<uint32_t>(E, g->stream);
     launch_edges_by_row(g, V, E, g->off, RowOutF{src});
     if (!in_w) {
         stable_sort_u32(g, g->dst, dst_sorted, src, in_src, E, (int)bits_for(V));
     } else {
         // (source, weight) ride together as one 64-bit value: no gathers afterwards
-        uint64_t* sw = dalloc<uint64_t>(E);
-        uint64_t* sw_sorted = dalloc<uint64_t>(E);
+        uint64_t* sw = dalloc<uint64_t>(E, g->stream);
+        uint64_t* sw_sorted = dalloc<uint64_t>(E, g->stream);
         k_pack_u32x2<<<grid, kBlock, 0, g->stream>>>(E, src, g->w, sw);
         size_t tb = 0;
         CGB_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tb, g->dst, dst_sorted, sw, sw_sorted, (uint64_t)E, 0,
                                                      (int)bits_for(V), g->stream));
-        void* temp = dalloc<char>(tb);
+        void* temp = dalloc<char>(tb, g->stream);
         cudaError_t err = cub::DeviceRadixSort::SortPairs(temp, tb, g->dst, dst_sorted, sw, sw_sorted, (uint64_t)E, 0,
                                                           (int)bits_for(V), g->stream);
         k_unpack_u32x2<<<grid, kBlock, 0, g->stream>>>(E, sw_sorted, in_src, in_w);
         CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
-        dfree(temp);
-        dfree(sw);
-        dfree(sw_sorted);
+        dfree(temp, g->stream);
+        dfree(sw, g->stream);
+        dfree(sw_sorted, g->stream);
         CGB_CUDA_TRY(err);
     }
     CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
-    dfree(src);
+    dfree(src, g->stream);
+}
+
+static void exclusive_sum_u32(cgb_graph* g, const uint32_t* in, uint32_t* out, uint64_t n)
+{
+    size_t tb = 0;
+    CGB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb, in, out, n, g->stream));
+    void* temp = dalloc<char>(tb, g->stream);
+    cudaError_t err = cub::DeviceScan::ExclusiveSum(temp, tb, in, out, n, g->stream);
+    dfree(temp, g->stream);
+    CGB_CUDA_TRY(err);
+}
+
+// Symmetry without a full transpose.  Lists are strictly ascending, so the
+// entries of v below v are a prefix of its list and those above v a suffix;
+// the lower triangle in CSR order is sorted by (v, u).  The graph is
+// symmetric exactly when the upper-triangle edges (u, v), u < v, stably
+// sorted by v, are the lower triangle: the same pairs (v, u) in the same
+// order (a self-loop is its own mirror).  Only those edges are sorted.
+__global__ void k_sym_counts(uint32_t V, const uint32_t* __restrict__ off, const uint32_t* __restrict__ dst,
+                             uint32_t* lower, uint32_t* upper)
+{
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+        const uint32_t beg = off[v], end = off[v + 1];
+        uint32_t lo = beg, hi = end;  // first entry >= v
+        while (lo < hi) {
+            const uint32_t mid = lo + (hi - lo) / 2;
+            if (dst[mid] < v) lo = mid + 1;
+            else hi = mid;
+        }
+        lower[v] = lo - beg;
+        upper[v] = end - lo - ((lo < end && dst[lo] == v) ? 1u : 0u);
+    }
+}
+
+// The upper-triangle edges in CSR order: key = v, value = u; u's entries
+// above u are the last upper[u] = uoff[u + 1] - uoff[u] of its list.
+struct SymUpperF {
+    static constexpr uint32_t kBatch = 1;
+    __device__ __forceinline__ bool stop() const { return false; }
+    __device__ __forceinline__ void tile_end() {}
+    const uint32_t* __restrict__ dst;
+    const uint32_t* __restrict__ uoff;
+    uint32_t* __restrict__ key;
+    uint32_t* __restrict__ val;
+    struct Val {
+        uint32_t d, pos;
+    };
+    __device__ __forceinline__ Val load(uint32_t e, uint32_t u, uint32_t, uint32_t end) const
+    {
+        const uint32_t a = __ldg(uoff + u), b = __ldg(uoff + u + 1);
+        return Val{__ldg(dst + e), a + (e - (end - (b - a)))};
+    }
+    __device__ __forceinline__ void store(uint32_t, uint32_t u, uint32_t, uint32_t, Val x)
+    {
+        if (x.d > u) {
+            key[x.pos] = x.d;
+            val[x.pos] = u;
+        }
+    }
+};
+
+// Lower-triangle edge (v, d), d < v, the j-th of v's list, against position
+// loff[v] + j of the sorted upper-triangle edges.
+struct SymCompareF {
+    static constexpr uint32_t kBatch = 1;
+    const uint32_t* __restrict__ dst;
+    const uint32_t* __restrict__ loff;
+    const uint32_t* __restrict__ skey;
+    const uint32_t* __restrict__ sval;
+    uint32_t* differ;
+    bool bad = false;  // this thread's mismatches since the last tile end
+    __device__ __forceinline__ bool stop() const { return *(volatile const uint32_t*)differ != 0; }
+    using Val = bool;
+    __device__ __forceinline__ Val load(uint32_t e, uint32_t v, uint32_t beg, uint32_t) const
+    {
+        const uint32_t d = __ldg(dst + e);
+        if (d >= v) return false;
+        const uint32_t i = __ldg(loff + v) + (e - beg);
+        return __ldg(skey + i) != v || __ldg(sval + i) != d;
+    }
+    __device__ __forceinline__ void store(uint32_t, uint32_t, uint32_t, uint32_t, Val x) { bad |= x; }
+    __device__ __forceinline__ void tile_end()
+    {
+        if (__any_sync(0xffffffffu, bad) && lane_id() == 0) atomicOr(differ, 1u);
+        bad = false;
+    }
+};
+
+static bool check_symmetric(cgb_graph* g)
+{
+    const uint32_t V = g->V, E = g->E;
+    if (E == 0) return true;
+    uint32_t* lower = dalloc<uint32_t>((size_t)V + 1, g->stream);
+    uint32_t* upper = dalloc<uint32_t>((size_t)V + 1, g->stream);
+    uint32_t* loff = dalloc<uint32_t>((size_t)V + 1, g->stream);
+    uint32_t* uoff = dalloc<uint32_t>((size_t)V + 1, g->stream);
+    CGB_CUDA_TRY(cudaMemsetAsync(lower + V, 0, 4, g->stream));
+    CGB_CUDA_TRY(cudaMemsetAsync(upper + V, 0, 4, g->stream));
+    k_sym_counts<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, g->off, g->dst, lower, upper);
+    exclusive_sum_u32(g, lower, loff, (uint64_t)V + 1);
+    exclusive_sum_u32(g, upper, uoff, (uint64_t)V + 1);
+    uint32_t tot[2] = {0, 0};
+    CGB_CUDA_TRY(cudaMemcpyAsync(&tot[0], loff + V, 4, cudaMemcpyDeviceToHost, g->stream));
+    CGB_CUDA_TRY(cudaMemcpyAsync(&tot[1], uoff + V, 4, cudaMemcpyDeviceToHost, g->stream));
+    CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    dfree(lower, g->stream);
+    dfree(upper, g->stream);
+    bool sym = tot[0] == tot[1];
+    if (sym && tot[1] > 0) {
+        const uint32_t n = tot[1];
+        uint32_t* key = dalloc<uint32_t>(n, g->stream);
+        uint32_t* val = dalloc<uint32_t>(n, g->stream);
+        uint32_t* skey = dalloc<uint32_t>(n, g->stream);
+        uint32_t* sval = dalloc<uint32_t>(n, g->stream);
+        uint32_t* differ = dalloc<uint32_t>(1, g->stream);
+        launch_edges_by_row(g, V, E, g->off, SymUpperF{g->dst, uoff, key, val});
+        stable_sort_u32(g, key, skey, val, sval, n, (int)bits_for(V));
+        dfree(key, g->stream);
+        dfree(val, g->stream);
+        CGB_CUDA_TRY(cudaMemsetAsync(differ, 0, 4, g->stream));
+        launch_edges_by_row(g, V, E, g->off, SymCompareF{g->dst, loff, skey, sval, differ});
+        uint32_t h = 0;
+        CGB_CUDA_TRY(cudaMemcpyAsync(&h, differ, 4, cudaMemcpyDeviceToHost, g->stream));
+        CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        sym = h == 0;
+        dfree(skey, g->stream);
+        dfree(sval, g->stream);
+        dfree(differ, g->stream);
+    }
+    dfree(loff, g->stream);
+    dfree(uoff, g->stream);
+    return sym;
 }
 
 // Builds the transpose (in-edge CSC) by a radix sort of packed (dst, src)
@@ -523,27 +778,27 @@ static void transpose_arrays(cgb_graph* g, uint32_t* dst_sorted, uint32_t* in_sr
 static void build_transpose(cgb_graph* g)
 {
     const uint32_t V = g->V, E = g->E;
-    uint32_t* in_off = dalloc<uint32_t>((size_t)V + 1);
-    uint32_t* in_src = dalloc<uint32_t>(E);
+    uint32_t* in_off = dalloc<uint32_t>((size_t)V + 1, g->stream);
+    uint32_t* in_src = dalloc<uint32_t>(E, g->stream);
     if (E == 0) {
         CGB_CUDA_TRY(cudaMemsetAsync(in_off, 0, ((size_t)V + 1) * sizeof(uint32_t), g->stream));
     } else {
-        uint32_t* dsorted = dalloc<uint32_t>(E);
+        uint32_t* dsorted = dalloc<uint32_t>(E, g->stream);
         // weights in CSC order are built on first need (ensure_csc_weights)
         transpose_arrays(g, dsorted, in_src, nullptr);
         k_offsets_from_u32<<<grid_for((uint64_t)V + 1, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(V, E, dsorted,
                                                                                                       in_off);
         CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
-        dfree(dsorted);
+        dfree(dsorted, g->stream);
     }
-    uint32_t* differ = dalloc<uint32_t>(1);
+    uint32_t* differ = dalloc<uint32_t>(1, g->stream);
     CGB_CUDA_TRY(cudaMemsetAsync(differ, 0, sizeof(uint32_t), g->stream));
     k_compare_u32<<<kNumSMs * 8, kBlock, 0, g->stream>>>((uint64_t)V + 1, in_off, g->off, differ);
     if (E) k_compare_u32<<<kNumSMs * 8, kBlock, 0, g->stream>>>(E, in_src, g->dst, differ);
     uint32_t h = 0;
     CGB_CUDA_TRY(cudaMemcpyAsync(&h, differ, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
     CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
-    dfree(differ);
+    dfree(differ, g->stream);
     if (h) {
         g->symmetric = 0;
         g->in_off = in_off;
@@ -551,18 +806,20 @@ static void build_transpose(cgb_graph* g)
         g->csc_owned = true;
     } else {
         g->symmetric = 1;
-        dfree(in_off);
-        dfree(in_src);
+        dfree(in_off, g->stream);
+        dfree(in_src, g->stream);
         g->in_off = g->off;
         g->in_src = g->dst;
         g->csc_owned = false;
     }
 }
 
+// The half-size check above; the transpose itself is built only when a run
+// needs the in-edges (ensure_csc).
 void ensure_symmetry_known(cgb_graph* g)
 {
     if (g->symmetric >= 0) return;
-    build_transpose(g);
+    g->symmetric = check_symmetric(g) ? 1 : 0;
 }
 
 void ensure_csc(cgb_graph* g)
@@ -584,30 +841,30 @@ void ensure_csc_weights(cgb_graph* g)
     // transpose the weights: a stable sort by destination lists every
     // in-list by source, the order of in_src; alias w when the result equals
     // it (a symmetric graph with symmetric weights)
-    const uint32_t V = g->V, E = g->E;
+    const uint32_t E = g->E;
     if (E == 0) {
         g->in_w = g->w;
         g->in_w_owned = false;
         return;
     }
-    uint32_t* dsorted = dalloc<uint32_t>(E);
-    uint32_t* srcs = dalloc<uint32_t>(E);
-    uint32_t* vals = dalloc<uint32_t>(E);
+    uint32_t* dsorted = dalloc<uint32_t>(E, g->stream);
+    uint32_t* srcs = dalloc<uint32_t>(E, g->stream);
+    uint32_t* vals = dalloc<uint32_t>(E, g->stream);
     transpose_arrays(g, dsorted, srcs, vals);
-    dfree(dsorted);
-    dfree(srcs);
-    uint32_t* differ = dalloc<uint32_t>(1);
+    dfree(dsorted, g->stream);
+    dfree(srcs, g->stream);
+    uint32_t* differ = dalloc<uint32_t>(1, g->stream);
     CGB_CUDA_TRY(cudaMemsetAsync(differ, 0, 4, g->stream));
     k_compare_u32<<<kNumSMs * 8, kBlock, 0, g->stream>>>(E, vals, g->w, differ);
     uint32_t h = 0;
     CGB_CUDA_TRY(cudaMemcpyAsync(&h, differ, 4, cudaMemcpyDeviceToHost, g->stream));
     CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
-    dfree(differ);
+    dfree(differ, g->stream);
     if (h) {
         g->in_w = vals;
         g->in_w_owned = true;
     } else {
-        dfree(vals);
+        dfree(vals, g->stream);
         g->in_w = g->w;
         g->in_w_owned = false;
     }
@@ -617,23 +874,23 @@ void ensure_frontier(cgb_graph* g)
 {
     if (g->q[0]) return;
     const uint32_t V = g->V;
-    g->q[0] = dalloc<uint32_t>(V);
-    g->q[1] = dalloc<uint32_t>(V);
+    g->q[0] = dalloc<uint32_t>(V, g->stream);
+    g->q[1] = dalloc<uint32_t>(V, g->stream);
     // any frontier (each vertex once): sum over lists >= big_deg of ceil(deg / chunk)
     // <= E / chunk + E / big_deg, at the smallest sizes cgb_tuning_set allows
     g->chunk_cap = (uint32_t)std::min<uint64_t>((uint64_t)g->E / kMinChunk + g->E / kMinBigDeg + 64, 0xFFFFFFF0ull);
-    g->chunk_q = dalloc<uint2>(g->chunk_cap);
-    g->visited = dalloc<uint32_t>(g->words());
-    g->front_bm = dalloc<uint32_t>(2 * (size_t)g->words());
-    g->stamp = dalloc<uint32_t>(V);
-    g->sample = dalloc<uint32_t>(1024);
-    g->aux_bm = dalloc<uint32_t>(3 * (size_t)g->words());
-    uint32_t* d = dalloc<uint32_t>(1);
+    g->chunk_q = dalloc<uint2>(g->chunk_cap, g->stream);
+    g->visited = dalloc<uint32_t>(g->words(), g->stream);
+    g->front_bm = dalloc<uint32_t>(2 * (size_t)g->words(), g->stream);
+    g->stamp = dalloc<uint32_t>(V, g->stream);
+    g->sample = dalloc<uint32_t>(1024, g->stream);
+    g->aux_bm = dalloc<uint32_t>(3 * (size_t)g->words(), g->stream);
+    uint32_t* d = dalloc<uint32_t>(1, g->stream);
     CGB_CUDA_TRY(cudaMemsetAsync(d, 0, 4, g->stream));
     k_max_degree<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, g->off, d);
     CGB_CUDA_TRY(cudaMemcpyAsync(&g->max_degree, d, 4, cudaMemcpyDeviceToHost, g->stream));
     CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
-    dfree(d);
+    dfree(d, g->stream);
 }
 
 __global__ void k_in_degree_from_off(uint32_t V, const uint32_t* __restrict__ in_off, uint32_t* indeg)
@@ -674,12 +931,6 @@ __global__ void k_sell_len(uint32_t V, const uint32_t* __restrict__ off, uint32_
     }
 }
 
-__global__ void k_fill_u32(uint64_t n, uint32_t* a, uint32_t v)
-{
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
-        a[i] = v;
-}
-
 __global__ void k_pr_rank(uint32_t V, const uint32_t* __restrict__ order, const uint32_t* __restrict__ off,
                           uint32_t* rank, uint32_t* outdeg_new)
 {
@@ -704,67 +955,81 @@ __global__ void k_row_bounds(const uint32_t* __restrict__ rows, uint32_t n, cons
 // relabelled out-offsets) gives key = new destination and value = r; a
 // stable sort by key then lists each new row's sources in ascending new ids.
 struct PrEdgesF {
+    static constexpr uint32_t kBatch = 8;
+    __device__ __forceinline__ bool stop() const { return false; }
+    __device__ __forceinline__ void tile_end() {}
     const uint32_t* __restrict__ order;
     const uint32_t* __restrict__ off;
     const uint32_t* __restrict__ dst;
     const uint32_t* __restrict__ rank;
-    uint32_t* key;
-    uint32_t* val;
-    __device__ __forceinline__ void operator()(uint32_t p, uint32_t r, uint32_t beg, uint32_t) const
+    uint32_t* __restrict__ key;
+    uint32_t* __restrict__ val;
+    using Val = uint32_t;
+    __device__ __forceinline__ Val load(uint32_t p, uint32_t r, uint32_t beg, uint32_t) const
     {
-        key[p] = rank[dst[off[order[r]] + (p - beg)]];
+        return __ldg(rank + __ldg(dst + __ldg(off + __ldg(order + r)) + (p - beg)));
+    }
+    __device__ __forceinline__ void store(uint32_t p, uint32_t r, uint32_t, uint32_t, Val k)
+    {
+        key[p] = k;
         val[p] = r;
     }
 };
 
-// SELL columns of the non-hub rows from the relabelled CSC (rows at
-// [beg, end) of pr_src); hub rows are marked in hub_bm and summed from
-// pr_src.
-struct SellFillF {
-    const uint32_t* __restrict__ pr_src;
-    const uint64_t* __restrict__ slice_ptr;
-    uint32_t hub;
-    uint32_t* col;
-    uint32_t* hub_bm;
-    __device__ __forceinline__ void operator()(uint32_t p, uint32_t r, uint32_t beg, uint32_t end) const
-    {
-        const uint32_t j = p - beg;
-        if (end - beg >= hub) {
-            if (j == 0) atomicOr(hub_bm + (r >> 5), 1u << (r & 31u));
-            return;
-        }
-        col[slice_ptr[r >> 5] + 32ull * j + (r & 31u)] = pr_src[p];
+// SELL columns from the relabelled CSC, one warp per 32-row slice, lane i
+// on row 32s + i: column j of the slice is 32 consecutive words, so every
+// store is coalesced, and each lane reads its own row front to back.
+// Positions past a row's end hold the padding target V; hub rows (hub
+// in-edges or more) are summed from pr_src instead, keep only padding here
+// and are marked in hub_bm (one word per slice, written whole).
+__global__ void k_sell_fill(uint32_t V, const uint32_t* __restrict__ pr_off, const uint32_t* __restrict__ pr_src,
+                            const uint64_t* __restrict__ slice_ptr, const uint32_t* __restrict__ slice_len,
+                            uint32_t hub, uint32_t* col, uint32_t* hub_bm)
+{
+    const uint32_t nslices = (V + 31) / 32;
+    const uint32_t lane = lane_id();
+    for (uint32_t sl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; sl < nslices;
+         sl += (gridDim.x * blockDim.x) >> 5) {
+        const uint32_t r = sl * 32 + lane;
+        const uint32_t beg = r < V ? pr_off[r] : 0;
+        const uint32_t len = r < V ? pr_off[r + 1] - beg : 0;
+        const bool is_hub = len >= hub;
+        const uint32_t hubs = __ballot_sync(0xffffffffu, is_hub);
+        if (lane == 0) hub_bm[sl] = hubs;
+        const uint32_t use = is_hub ? 0 : len;
+        uint32_t* c = col + slice_ptr[sl] + lane;
+        const uint32_t width = slice_len[sl];
+        for (uint32_t j = 0; j < width; j++) c[32ull * j] = j < use ? pr_src[beg + j] : V;
     }
-};
+}
 
-// Sliced ELL layout of the non-hub rows (slice lengths, offsets, the column
-// array filled with the padding target V); k_sell_fill writes the columns.
+// Sliced ELL layout of the non-hub rows (slice lengths, offsets and the
+// column array); k_sell_fill writes the columns and their padding.
 static void build_sell(cgb_graph* g)
 {
     const uint32_t V = g->V;
     const uint32_t nslices = (V + 31) / 32;
-    g->pr_slice_len = dalloc<uint32_t>(nslices);
-    g->pr_slice_ptr = dalloc<uint64_t>((size_t)nslices + 1);
-    g->pr_hub_bm = dalloc<uint32_t>(g->words());
+    g->pr_slice_len = dalloc<uint32_t>(nslices, g->stream);
+    g->pr_slice_ptr = dalloc<uint64_t>((size_t)nslices + 1, g->stream);
+    g->pr_hub_bm = dalloc<uint32_t>(g->words(), g->stream);
     CGB_CUDA_TRY(cudaMemsetAsync(g->pr_hub_bm, 0, (size_t)g->words() * 4, g->stream));
-    uint64_t* width = dalloc<uint64_t>((size_t)nslices + 1);
+    uint64_t* width = dalloc<uint64_t>((size_t)nslices + 1, g->stream);
     CGB_CUDA_TRY(cudaMemsetAsync(width + nslices, 0, 8, g->stream));
     k_sell_len<<<grid_for((uint64_t)nslices * 32, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(
         V, g->pr_off, kPrHuge, g->pr_slice_len, width);
     size_t tb = 0;
     CGB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb, width, g->pr_slice_ptr, (uint64_t)nslices + 1, g->stream));
-    void* temp = dalloc<char>(tb);
+    void* temp = dalloc<char>(tb, g->stream);
     cudaError_t err =
         cub::DeviceScan::ExclusiveSum(temp, tb, width, g->pr_slice_ptr, (uint64_t)nslices + 1, g->stream);
     uint64_t total = 0;
     CGB_CUDA_TRY(cudaMemcpyAsync(&total, g->pr_slice_ptr + nslices, 8, cudaMemcpyDeviceToHost, g->stream));
     CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
-    dfree(temp);
-    dfree(width);
+    dfree(temp, g->stream);
+    dfree(width, g->stream);
     CGB_CUDA_TRY(err);
     g->pr_sell_size = total;
-    g->pr_col = dalloc<uint32_t>(total);
-    k_fill_u32<<<grid_for(total, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(total, g->pr_col, V);
+    g->pr_col = dalloc<uint32_t>(total, g->stream);
 }
 
 // Builds the PageRank layout (see cgb_graph): the relabel keeps every
@@ -775,21 +1040,21 @@ void ensure_pr(cgb_graph* g)
     if (g->pr_ready) return;
     const uint32_t V = g->V, E = g->E;
     for (int i = 0; i < 2; i++) {
-        if (!g->pr[i]) g->pr[i] = dalloc<double>(V);
-        if (!g->contrib[i]) g->contrib[i] = dalloc<double>((size_t)V + 1);
+        if (!g->pr[i]) g->pr[i] = dalloc<double>(V, g->stream);
+        if (!g->contrib[i]) g->contrib[i] = dalloc<double>((size_t)V + 1, g->stream);
         CGB_CUDA_TRY(cudaMemsetAsync(g->contrib[i] + V, 0, sizeof(double), g->stream));  // padding target
     }
-    g->pr_rank = dalloc<uint32_t>(V);
-    g->pr_outdeg = dalloc<uint32_t>(V);
-    g->pr_off = dalloc<uint32_t>((size_t)V + 1);
-    g->pr_src = dalloc<uint32_t>(E);
+    g->pr_rank = dalloc<uint32_t>(V, g->stream);
+    g->pr_outdeg = dalloc<uint32_t>(V, g->stream);
+    g->pr_off = dalloc<uint32_t>((size_t)V + 1, g->stream);
+    g->pr_src = dalloc<uint32_t>(E, g->stream);
     // 1. stable order by (out-degree bucket, in-degree descending)
     uint32_t* order = nullptr;
     {
-        uint32_t* key = dalloc<uint32_t>(V);
-        uint32_t* key2 = dalloc<uint32_t>(V);
-        uint32_t* id = dalloc<uint32_t>(V);
-        uint32_t* id2 = dalloc<uint32_t>(V);
+        uint32_t* key = dalloc<uint32_t>(V, g->stream);
+        uint32_t* key2 = dalloc<uint32_t>(V, g->stream);
+        uint32_t* id = dalloc<uint32_t>(V, g->stream);
+        uint32_t* id2 = dalloc<uint32_t>(V, g->stream);
         // in-degrees from the transpose (shared with bottom-up BFS; no atomics)
         ensure_csc(g);
         k_in_degree_from_off<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, g->in_off, key2);
@@ -797,17 +1062,17 @@ void ensure_pr(cgb_graph* g)
         cub::DoubleBuffer<uint32_t> kb(key, key2), vb(id, id2);
         size_t tb = 0;
         CGB_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tb, kb, vb, (uint64_t)V, 0, 32, g->stream));
-        void* temp = dalloc<char>(tb);
+        void* temp = dalloc<char>(tb, g->stream);
         cudaError_t err = cub::DeviceRadixSort::SortPairs(temp, tb, kb, vb, (uint64_t)V, 0, 32, g->stream);
         k_pr_rank<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, vb.Current(), g->off, g->pr_rank,
                                                                              g->pr_outdeg);
         CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
-        dfree(temp);
-        dfree(key);
-        dfree(key2);
+        dfree(temp, g->stream);
+        dfree(key, g->stream);
+        dfree(key2, g->stream);
         CGB_CUDA_TRY(err);
         order = vb.Current();
-        dfree(vb.Alternate());
+        dfree(vb.Alternate(), g->stream);
     }
     // 2. in-edge CSC over the new ids: the edges enumerated by new source,
     //    stable-sorted by new destination (one 32-bit sort), so each row
@@ -815,63 +1080,65 @@ void ensure_pr(cgb_graph* g)
     {
         // offsets of the new sources' out-lists: exclusive scan of the out-degrees in new order
         // (pr_outdeg has V entries; the scan of V + 1 reads a zero-padded copy)
-        uint32_t* src_off = dalloc<uint32_t>((size_t)V + 1);
-        uint32_t* od = dalloc<uint32_t>((size_t)V + 1);
+        uint32_t* src_off = dalloc<uint32_t>((size_t)V + 1, g->stream);
+        uint32_t* od = dalloc<uint32_t>((size_t)V + 1, g->stream);
         CGB_CUDA_TRY(cudaMemcpyAsync(od, g->pr_outdeg, (size_t)V * 4, cudaMemcpyDeviceToDevice, g->stream));
         CGB_CUDA_TRY(cudaMemsetAsync(od + V, 0, 4, g->stream));
         size_t tb = 0;
         CGB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb, od, src_off, (uint64_t)V + 1, g->stream));
-        void* temp = dalloc<char>(tb);
+        void* temp = dalloc<char>(tb, g->stream);
         cudaError_t err = cub::DeviceScan::ExclusiveSum(temp, tb, od, src_off, (uint64_t)V + 1, g->stream);
         CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
-        dfree(temp);
-        dfree(od);
+        dfree(temp, g->stream);
+        dfree(od, g->stream);
         CGB_CUDA_TRY(err);
         if (E) {
-            uint32_t* key = dalloc<uint32_t>(E);
-            uint32_t* val = dalloc<uint32_t>(E);
-            uint32_t* kout = dalloc<uint32_t>(E);
+            uint32_t* key = dalloc<uint32_t>(E, g->stream);
+            uint32_t* val = dalloc<uint32_t>(E, g->stream);
+            uint32_t* kout = dalloc<uint32_t>(E, g->stream);
             launch_edges_by_row(g, V, E, src_off, PrEdgesF{order, g->off, g->dst, g->pr_rank, key, val});
             stable_sort_u32(g, key, kout, val, g->pr_src, E, (int)bits_for(V));
             k_offsets_from_u32<<<grid_for((uint64_t)V + 1, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(
                 V, E, kout, g->pr_off);
             CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
-            dfree(key);
-            dfree(val);
-            dfree(kout);
+            dfree(key, g->stream);
+            dfree(val, g->stream);
+            dfree(kout, g->stream);
         } else {
             CGB_CUDA_TRY(cudaMemsetAsync(g->pr_off, 0, ((size_t)V + 1) * 4, g->stream));
         }
-        dfree(src_off);
+        dfree(src_off, g->stream);
         build_sell(g);
         if (E)
-            launch_edges_by_row(g, V, E, g->pr_off,
-                                SellFillF{g->pr_src, g->pr_slice_ptr, kPrHuge, g->pr_col, g->pr_hub_bm});
+            k_sell_fill<<<grid_for((uint64_t)(V + 31) / 32 * 32, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(
+                V, g->pr_off, g->pr_src, g->pr_slice_ptr, g->pr_slice_len, kPrHuge, g->pr_col, g->pr_hub_bm);
         CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
-        dfree(order);
+        dfree(order, g->stream);
     }
     // 3. hub rows and their chunk table (host-built; few rows)
     {
-        uint32_t* n = dalloc<uint32_t>(1);
-        uint32_t* rows = dalloc<uint32_t>(V);
+        uint32_t* n = dalloc<uint32_t>(1, g->stream);
+        uint32_t* rows = dalloc<uint32_t>(V, g->stream);
         CGB_CUDA_TRY(cudaMemsetAsync(n, 0, sizeof(uint32_t), g->stream));
         k_collect_heavy_rows<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, g->pr_off, kPrHuge, rows,
                                                                                         n);
         uint32_t h = 0;
         CGB_CUDA_TRY(cudaMemcpyAsync(&h, n, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
         CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
-        dfree(n);
+        dfree(n, g->stream);
         std::vector<uint32_t> hrows(h), lo(h), hi(h);
         if (h) {
-            CGB_CUDA_TRY(cudaMemcpy(hrows.data(), rows, h * 4ull, cudaMemcpyDeviceToHost));
-            std::sort(hrows.begin(), hrows.end());
-            CGB_CUDA_TRY(cudaMemcpy(rows, hrows.data(), h * 4ull, cudaMemcpyHostToDevice));
-            uint32_t* lohi = dalloc<uint32_t>(2ull * h);
-            k_row_bounds<<<grid_for(h, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(rows, h, g->pr_off, lohi);
+            // copies on the graph's stream (pageable host memory: each waits)
+            CGB_CUDA_TRY(cudaMemcpyAsync(hrows.data(), rows, h * 4ull, cudaMemcpyDeviceToHost, g->stream));
             CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
-            CGB_CUDA_TRY(cudaMemcpy(lo.data(), lohi, h * 4ull, cudaMemcpyDeviceToHost));
-            CGB_CUDA_TRY(cudaMemcpy(hi.data(), lohi + h, h * 4ull, cudaMemcpyDeviceToHost));
-            dfree(lohi);
+            std::sort(hrows.begin(), hrows.end());
+            CGB_CUDA_TRY(cudaMemcpyAsync(rows, hrows.data(), h * 4ull, cudaMemcpyHostToDevice, g->stream));
+            uint32_t* lohi = dalloc<uint32_t>(2ull * h, g->stream);
+            k_row_bounds<<<grid_for(h, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(rows, h, g->pr_off, lohi);
+            CGB_CUDA_TRY(cudaMemcpyAsync(lo.data(), lohi, h * 4ull, cudaMemcpyDeviceToHost, g->stream));
+            CGB_CUDA_TRY(cudaMemcpyAsync(hi.data(), lohi + h, h * 4ull, cudaMemcpyDeviceToHost, g->stream));
+            CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+            dfree(lohi, g->stream);
         }
         std::vector<uint2> chunks;
         std::vector<uint32_t> base(h + 1, 0);
@@ -883,12 +1150,14 @@ void ensure_pr(cgb_graph* g)
         g->n_pr_huge = h;
         g->n_pr_chunks = (uint32_t)chunks.size();
         g->pr_huge_rows = rows;
-        g->pr_chunk_base = dalloc<uint32_t>(h + 1);
-        CGB_CUDA_TRY(cudaMemcpy(g->pr_chunk_base, base.data(), (h + 1) * 4ull, cudaMemcpyHostToDevice));
-        g->pr_chunks = dalloc<uint2>(chunks.size());
+        g->pr_chunk_base = dalloc<uint32_t>(h + 1, g->stream);
+        CGB_CUDA_TRY(cudaMemcpyAsync(g->pr_chunk_base, base.data(), (h + 1) * 4ull, cudaMemcpyHostToDevice, g->stream));
+        g->pr_chunks = dalloc<uint2>(chunks.size(), g->stream);
         if (!chunks.empty())
-            CGB_CUDA_TRY(cudaMemcpy(g->pr_chunks, chunks.data(), chunks.size() * sizeof(uint2), cudaMemcpyHostToDevice));
-        g->pr_part = dalloc<double>(chunks.size());
+            CGB_CUDA_TRY(cudaMemcpyAsync(g->pr_chunks, chunks.data(), chunks.size() * sizeof(uint2),
+                                         cudaMemcpyHostToDevice, g->stream));
+        CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));  // base and chunks go out of scope
+        g->pr_part = dalloc<double>(chunks.size(), g->stream);
     }
     g->pr_ready = true;
 }
@@ -949,13 +1218,16 @@ cgb_graph* graph_alloc(uint32_t V, uint32_t E, uint32_t nz, int device, bool wit
         CGB_CUDA_TRY(cudaEventCreate(&g->ev_stop));
         CGB_CUDA_TRY(cudaEventCreate(&g->ev_iter[0]));
         CGB_CUDA_TRY(cudaEventCreate(&g->ev_iter[1]));
-        g->ctr = dalloc<DevCounters>(1);
+        g->ctr = dalloc<DevCounters>(1, g->stream);
         g->h_ctr = static_cast<DevCounters*>(pinned_small_alloc(sizeof(DevCounters)));
         CGB_CUDA_TRY(cudaMemsetAsync(g->ctr, 0, sizeof(DevCounters), g->stream));
-        g->off = dalloc<uint32_t>((size_t)V + 1);
-        g->dst = dalloc<uint32_t>(E);
-        if (with_weight) g->w = dalloc<uint32_t>(E);
-        g->value = dalloc<uint32_t>(V);
+        g->off = dalloc<uint32_t>((size_t)V + 1, g->stream);
+        g->dst = dalloc<uint32_t>(E, g->stream);
+        if (with_weight) g->w = dalloc<uint32_t>(E, g->stream);
+        g->value = dalloc<uint32_t>(V, g->stream);
+        // the buffers are stream-ordered allocations: complete them, so the
+        // graph is usable on every stream from here on
+        CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
     } catch (...) {
         graph_free(g);
         throw;
@@ -969,10 +1241,10 @@ void graph_free(cgb_graph* g)
     cudaSetDevice(g->device);
     if (g->stream) cudaStreamSynchronize(g->stream);
     if (g->csc_owned) {
-        dfree(g->in_off);
-        dfree(g->in_src);
+        dfree(g->in_off, g->stream);
+        dfree(g->in_src, g->stream);
     }
-    if (g->in_w_owned) dfree(g->in_w);
+    if (g->in_w_owned) dfree(g->in_w, g->stream);
     free_msbfs(g);
     free_mssp(g);
     void* ptrs[] = {g->off, g->dst, g->w, g->pr_huge_rows, g->pr_rank, g->pr_off, g->pr_src, g->pr_outdeg,
@@ -980,7 +1252,7 @@ void graph_free(cgb_graph* g)
                     g->pr_hub_bm, g->value, g->pr[0], g->pr[1], g->contrib[0],
                     g->contrib[1], g->q[0], g->q[1], g->chunk_q, g->visited, g->front_bm, g->stamp, g->sample,
                     g->aux_bm, g->persist, g->ctr};
-    for (void* p : ptrs) dfree(p);
+    for (void* p : ptrs) dfree(p, g->stream);
     pinned_small_free(g->h_ctr);
     for (cudaEvent_t e : g->kev) cudaEventDestroy(e);
     cudaEvent_t evs[] = {g->ev_start, g->ev_stop, g->ev_iter[0], g->ev_iter[1]};

@@ -403,7 +403,7 @@ void launch_sssp_device(cgb_graph* g, uint32_t* far_bm, uint32_t delta, PersistS
 
 static PersistState* persist_state(cgb_graph* g)
 {
-    if (!g->persist) CGB_CUDA_TRY(cudaMalloc(&g->persist, sizeof(PersistState)));
+    if (!g->persist) g->persist = pool_alloc(sizeof(PersistState), g->stream);
     return static_cast<PersistState*>(g->persist);
 }
 

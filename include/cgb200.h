@@ -198,6 +198,11 @@ cgb_status cgb_trace_get(const cgb_graph* g, cgb_iter_trace* out, uint32_t max_e
  * for the next graph; this returns the cached memory to the driver. */
 cgb_status cgb_memory_trim(int device);
 
+/* The pool's size on a device: *reserved bytes held from the driver and
+ * *used bytes handed out to live allocations (either pointer may be NULL).
+ * Engine-specific (no reference counterpart): for monitoring the pool. */
+cgb_status cgb_memory_info(int device, uint64_t* reserved, uint64_t* used);
+
 /* ------------------------------------------------------------ tuning */
 
 /* Launch parameters of a graph's kernels, one set per algorithm.  They

@@ -124,6 +124,38 @@ def test_self_loops_and_zero_weights(oracle):
     check_all(oracle, off, dst, w, [0, 3])
 
 
+def test_symmetry_check_when_cc_runs_first(oracle):
+    """With CC as the first run, symmetry is decided without a transpose: the
+    upper-triangle edges sorted by destination against the lower triangle.
+    Graphs whose lower and upper counts agree while their edges do not mirror
+    must take label propagation (cc_path 1), symmetric ones hooking (0)."""
+    # symmetric, with self-loops and an isolated vertex
+    sym = [(0, 0), (0, 2), (2, 0), (1, 3), (3, 1), (3, 3), (2, 3), (3, 2)]
+    # one lower and one upper edge that are not mirrors: 0 -> 1, 2 -> 0
+    skew = [(0, 1), (2, 0)]
+    cases = [(5, sym, 0), (3, skew, 1)]
+    # a symmetric RMAT graph, then the same with one mirror (v, u), u < v,
+    # moved to (v, u') for a u' < v outside v's list: every count is kept
+    off, dst, _ = oracle.rmat_graph(10, 8, seed=5, symmetrise=True)
+    V = off.size - 1
+    edges = [(u, int(dst[e])) for u in range(V) for e in range(int(off[u]), int(off[u + 1]))]
+    cases.append((V, edges, 0))
+    es = set(edges)
+    v = next(x for x in range(V - 1, 0, -1) if any(d < x for (s, d) in edges if s == x))
+    u = next(d for (s, d) in edges if s == v and d < v)
+    u2 = next(y for y in range(v) if (v, y) not in es)
+    moved = sorted((es - {(v, u)}) | {(v, u2)})
+    cases.append((V, moved, 1))
+    for V, edges, path in cases:
+        off, dst, _ = csr_from_edges(V, edges)
+        with cg.Graph.from_csr(off, dst, None) as g:
+            np.testing.assert_array_equal(g.run(CC)[0], oracle.cc(off, dst))
+            assert g.stats().cc_path == path
+            assert g.symmetric == (1 if path == 0 else 0)
+            r = int(np.argmax(np.diff(off.astype(np.int64))))
+            np.testing.assert_array_equal(g.run(BFS, r)[0], oracle.bfs(off, dst, r))
+
+
 def test_zero_out_degree_tail(oracle):
     """noZeroOutDegreeNum < V (the reordered layout whose last vertices have no
     out-edges, main_partition.hpp:78-103)."""
@@ -188,8 +220,12 @@ def test_memory_pool_reuse_and_trim(oracle):
     from cggraph_b200 import _lib as L
     off, dst, w = oracle.rmat_graph(12, 8, seed=4)
     exp = oracle.bfs(off, dst, 3)
+    import ctypes
+    reserved, used = ctypes.c_uint64(), ctypes.c_uint64()
     for trim in (False, True, False):
         with cg.Graph.from_csr(off, dst, w) as g:
             np.testing.assert_array_equal(g.run(0, 3)[0], exp)
+            L.check(L.lib().cgb_memory_info(0, ctypes.byref(reserved), ctypes.byref(used)))
+            assert used.value >= 4 * (off.size + 2 * dst.size) and reserved.value >= used.value
         if trim:
             L.check(L.lib().cgb_memory_trim(0))
