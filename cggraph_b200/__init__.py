@@ -22,6 +22,9 @@ from .engine import (  # noqa: F401
     load_binFile,
     main_partition,
     make_options,
+    memory_info,
+    memory_reserve,
+    memory_trim,
     save_binArray,
     trimmed_mean_ms,
 )

@@ -34,7 +34,7 @@ EXPORTS = [
     "cgb_policy_forward", "cgb_policy_loss_grad", "cgb_batch_create", "cgb_batch_destroy", "cgb_batch_run",
     "cgb_batch_info", "cgb_batch_stats", "cgb_server_create", "cgb_server_submit", "cgb_server_start",
     "cgb_server_wait", "cgb_server_poll", "cgb_server_stats", "cgb_server_destroy", "cgb_tuning_get",
-    "cgb_tuning_set", "cgb_autotune", "cgb_memory_trim", "cgb_memory_info",
+    "cgb_tuning_set", "cgb_autotune", "cgb_memory_trim", "cgb_memory_info", "cgb_memory_reserve",
 ]
 POLICY_FEATURES, POLICY_OUTPUTS, POLICY_PARAMS = 24, 9, 6345
 
@@ -209,6 +209,7 @@ def lib() -> ctypes.CDLL:
         L.cgb_server_destroy.argtypes = [_P]
         L.cgb_memory_trim.argtypes = [i]
         L.cgb_memory_info.argtypes = [i, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
+        L.cgb_memory_reserve.argtypes = [i, ctypes.c_uint64]
         L.cgb_tuning_get.argtypes = [_P, i, ctypes.POINTER(Tuning)]
         L.cgb_tuning_set.argtypes = [_P, i, ctypes.POINTER(Tuning)]
         L.cgb_autotune.argtypes = [_P, i, _P, u32, u32, ctypes.POINTER(Tuning), ctypes.POINTER(ctypes.c_double),

@@ -18,6 +18,7 @@ cgb_graph* gen_grid(uint32_t rows, uint32_t cols, uint64_t seed, uint32_t wmax, 
 cgb_graph* gen_chunglu(uint32_t V, uint64_t draws, uint32_t i0, uint64_t seed, int sym, uint32_t wmax, int device);
 void memory_trim(int device);
 void memory_info(int device, uint64_t* reserved, uint64_t* used);
+void memory_reserve(int device, uint64_t bytes);
 }  // namespace cgb
 
 using namespace cgb;
@@ -444,6 +445,11 @@ cgb_status cgb_memory_trim(int device)
 cgb_status cgb_memory_info(int device, uint64_t* reserved, uint64_t* used)
 {
     return guarded([&] { memory_info(device, reserved, used); });
+}
+
+cgb_status cgb_memory_reserve(int device, uint64_t bytes)
+{
+    return guarded([&] { memory_reserve(device, bytes); });
 }
 
 cgb_status cgb_gen_chunglu(uint32_t vertices, uint64_t draws, uint32_t weight_offset, uint64_t seed, int symmetrise,

@@ -119,6 +119,29 @@ void memory_trim(int device)
     CGB_CUDA_TRY(cudaMemPoolTrimTo(dp.pool, 0));
 }
 
+// Grows the pool to at least `bytes` reserved: one allocation that brings
+// the used amount up to `bytes` (the pool reserves at least what is in
+// use), freed again; the pool keeps it (release threshold: never) and
+// splits it for later allocations.
+void memory_reserve(int device, uint64_t bytes)
+{
+    CGB_CUDA_TRY(cudaSetDevice(device));
+    DevicePool& dp = device_pool();
+    uint64_t r = 0, u = 0;
+    CGB_CUDA_TRY(cudaMemPoolGetAttribute(dp.pool, cudaMemPoolAttrReservedMemCurrent, &r));
+    CGB_CUDA_TRY(cudaMemPoolGetAttribute(dp.pool, cudaMemPoolAttrUsedMemCurrent, &u));
+    if (r >= bytes) return;
+    cudaStream_t s = nullptr;
+    CGB_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    void* p = nullptr;
+    cudaError_t err = cudaMallocFromPoolAsync(&p, bytes - u, dp.pool, s);
+    if (err == cudaSuccess) err = cudaFreeAsync(p, s);
+    cudaError_t err2 = cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+    CGB_CUDA_TRY(err);
+    CGB_CUDA_TRY(err2);
+}
+
 void memory_info(int device, uint64_t* reserved, uint64_t* used)
 {
     CGB_CUDA_TRY(cudaSetDevice(device));

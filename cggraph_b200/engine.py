@@ -171,6 +171,23 @@ def _count(a) -> int:
     return int(a.size if isinstance(a, np.ndarray) else a.numel())
 
 
+def memory_info(device: int = 0):
+    """(reserved, used) bytes of the engine's memory pool on `device`."""
+    r, u = ctypes.c_uint64(), ctypes.c_uint64()
+    check(L.lib().cgb_memory_info(device, ctypes.byref(r), ctypes.byref(u)))
+    return r.value, u.value
+
+
+def memory_reserve(nbytes: int, device: int = 0) -> None:
+    """Grow the memory pool to at least `nbytes` reserved (cgb_memory_reserve)."""
+    check(L.lib().cgb_memory_reserve(device, int(nbytes)))
+
+
+def memory_trim(device: int = 0) -> None:
+    """Return the pool's cached memory to the driver (cgb_memory_trim)."""
+    check(L.lib().cgb_memory_trim(device))
+
+
 def make_options(schedule: int = L.SCHED_HEURISTIC, variant: int = L.VAR_AUTO, sssp_delta: int = 0,
                  bfs_alpha: float = 0.0, bfs_beta: float = 0.0, max_iterations: int = 0, flags: int = 0) -> L.Options:
     o = L.Options()

@@ -203,6 +203,12 @@ cgb_status cgb_memory_trim(int device);
  * Engine-specific (no reference counterpart): for monitoring the pool. */
 cgb_status cgb_memory_info(int device, uint64_t* reserved, uint64_t* used);
 
+/* Grows the pool to at least `bytes` reserved (no-op when it holds that much
+ * already). Growing the pool costs driver time; a process that creates and
+ * destroys graphs repeatedly can pay it once, up front. Engine-specific (no
+ * reference counterpart). */
+cgb_status cgb_memory_reserve(int device, uint64_t bytes);
+
 /* ------------------------------------------------------------ tuning */
 
 /* Launch parameters of a graph's kernels, one set per algorithm.  They

@@ -229,3 +229,11 @@ def test_memory_pool_reuse_and_trim(oracle):
             assert used.value >= 4 * (off.size + 2 * dst.size) and reserved.value >= used.value
         if trim:
             L.check(L.lib().cgb_memory_trim(0))
+    # an explicit reservation holds at least what was asked, and graphs still work
+    r0, _ = cg.memory_info()
+    cg.memory_reserve(r0 + (256 << 20))
+    r1, _ = cg.memory_info()
+    assert r1 >= r0 + (256 << 20)
+    with cg.Graph.from_csr(off, dst, w) as g:
+        np.testing.assert_array_equal(g.run(0, 3)[0], exp)
+    cg.memory_trim()
