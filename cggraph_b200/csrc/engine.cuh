@@ -137,6 +137,10 @@ struct cgb_graph {
 
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     cudaEvent_t ev_iter[2] = {nullptr, nullptr};
+    // PageRank hub chunks run beside the sliced pull: a second stream forked
+    // from and joined to `stream` by these events (created on first use)
+    cudaStream_t aux_stream = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     std::vector<cudaEvent_t> kev;     // per-launch timing events (pairs)
     size_t kev_used = 0;
     std::vector<int> kev_class;

@@ -1278,9 +1278,10 @@ void graph_free(cgb_graph* g)
     for (void* p : ptrs) dfree(p, g->stream);
     pinned_small_free(g->h_ctr);
     for (cudaEvent_t e : g->kev) cudaEventDestroy(e);
-    cudaEvent_t evs[] = {g->ev_start, g->ev_stop, g->ev_iter[0], g->ev_iter[1]};
+    cudaEvent_t evs[] = {g->ev_start, g->ev_stop, g->ev_iter[0], g->ev_iter[1], g->ev_fork, g->ev_join};
     for (cudaEvent_t e : evs)
         if (e) cudaEventDestroy(e);
+    if (g->aux_stream) cudaStreamDestroy(g->aux_stream);
     if (g->own_stream) cudaStreamDestroy(g->own_stream);
     delete g;
 }

@@ -25,8 +25,8 @@
 // in-degree inside each out-degree bucket keeps the padding under 1 % on
 // RMAT.  A warp sums one slice, one row per lane (k_pr_pull).  Rows of
 // kPrHuge or more in-edges are cut into kPrChunk-edge chunks summed by
-// separate CTAs (k_pr_hub_chunks) and combined in chunk order
-// (k_pr_hub_finish).
+// separate CTAs (k_pr_hub_chunks, on a second stream beside the pull) and
+// combined in chunk order (k_pr_hub_finish).
 // Every summation order is fixed by the graph alone, so results are
 // bit-reproducible.
 #include "engine.cuh"
@@ -163,19 +163,32 @@ void run_pr(cgb_graph* g, uint32_t iters, const cgb_options& o)
     if (timing) ktimer_end(g);
     const uint32_t grid = grid_for(div_up(V, 32), kBlock / 32, kNumSMs * g->tune.pr_ctas_per_sm);
     const uint32_t unroll = g->tune.pr_unroll;
+    // hub chunks on a second stream, beside the pull (they read the same
+    // contributions and write only the chunk partials); joined before the
+    // hub rows are finished
+    const bool fork = g->n_pr_chunks > 0;
+    if (fork && !g->aux_stream) {
+        CGB_CUDA_TRY(cudaStreamCreateWithFlags(&g->aux_stream, cudaStreamNonBlocking));
+        CGB_CUDA_TRY(cudaEventCreateWithFlags(&g->ev_fork, cudaEventDisableTiming));
+        CGB_CUDA_TRY(cudaEventCreateWithFlags(&g->ev_join, cudaEventDisableTiming));
+    }
     int cur = 0;
     for (uint32_t it = 0; it < iters; it++) {
         const int out = cur ^ 1;
         if (timing) ktimer_begin(g, CGB_K_PR);
-        if (g->n_pr_chunks) {
+        if (fork) {
             ++g->stats.launches;
-            k_pr_hub_chunks<<<std::min<uint32_t>(g->n_pr_chunks, kNumSMs * 8), kBlock, 0, g->stream>>>(
+            CGB_CUDA_TRY(cudaEventRecord(g->ev_fork, g->stream));
+            CGB_CUDA_TRY(cudaStreamWaitEvent(g->aux_stream, g->ev_fork, 0));
+            k_pr_hub_chunks<<<std::min<uint32_t>(g->n_pr_chunks, kNumSMs * 8), kBlock, 0, g->aux_stream>>>(
                 g->pr_chunks, g->n_pr_chunks, g->pr_off, g->pr_src, g->contrib[cur], g->pr_part);
+            CGB_CUDA_TRY(cudaEventRecord(g->ev_join, g->aux_stream));
         }
         ++g->stats.launches;
         auto pull = unroll == 4 ? k_pr_pull<4> : unroll == 16 ? k_pr_pull<16> : k_pr_pull<8>;
         pull<<<grid, kBlock, 0, g->stream>>>(V, g->pr_slice_ptr, g->pr_slice_len, g->pr_col, g->pr_hub_bm,
                                              g->pr_outdeg, g->contrib[cur], g->pr[out], g->contrib[out], base, damp);
+        if (fork) CGB_CUDA_TRY(cudaStreamWaitEvent(g->stream, g->ev_join, 0));
         if (g->n_pr_huge) {
             ++g->stats.launches;
             k_pr_hub_finish<<<grid_for(g->n_pr_huge, kBlock, kNumSMs), kBlock, 0, g->stream>>>(
