@@ -18,6 +18,7 @@ struct DevCounters {
     unsigned long long medges;    // sum of out-degrees of the next frontier
     unsigned long long reached_edges;
     uint32_t reached;
+    uint32_t touched;         // SSSP: vertices whose distance left infinity this run (root excluded)
     uint32_t min_far;         // SSSP: smallest distance left in the far bitmap
     uint32_t max_deg;         // max degree of the next frontier
     uint32_t chunk_len;       // chunk descriptors queued by k_push_binned
@@ -59,7 +60,7 @@ inline cgb_tuning default_tuning()
     t.pr_ctas_per_sm = 128;
     t.sssp_pull_alpha = 0;
     t.cluster_enter = 8192;
-    t.sssp_dense_alpha = 8;
+    t.sssp_dense_alpha = 4;
     return t;
 }
 

@@ -27,6 +27,7 @@ namespace cgb {
 
 __shared__ uint32_t s_sssp_newfar;  // per-CTA count of vertices newly set in the far bitmap
 __shared__ unsigned long long s_sssp_medges;  // per-CTA out-degree sum of the next near queue
+__shared__ uint32_t s_sssp_touched;  // per-CTA count of vertices reached for the first time
 
 template <bool kHasW>
 struct SsspOp {
@@ -52,7 +53,7 @@ struct SsspOp {
     }
     __device__ __forceinline__ void edge(bool valid, uint32_t e, uint32_t du) const
     {
-        bool to_near = false, new_far = false;
+        bool to_near = false, new_far = false, first = false;
         uint32_t d = 0;
         if (valid) {
             // the edge arrays stream through once: evict first, so L2 keeps dist[] and the bitmaps
@@ -62,6 +63,7 @@ struct SsspOp {
                 const uint32_t nd = (uint32_t)cand;
                 if (nd < dist[d]) {
                     const uint32_t old = atomicMin(dist + d, nd);
+                    first = old == kValueMax;
                     if (nd < old && d < nz) {
                         if (nd < thr) {
                             const uint32_t bit = 1u << (d & 31u);
@@ -79,6 +81,8 @@ struct SsspOp {
         warp_append(to_near, d, near_out, near_len, cap, &ctr->overflow);
         const uint32_t nf = __popc(__ballot_sync(0xffffffffu, new_far));
         if (nf && lane_id() == 0) atomicAdd(&s_sssp_newfar, nf);
+        const uint32_t nt = __popc(__ballot_sync(0xffffffffu, first));
+        if (nt && lane_id() == 0) atomicAdd(&s_sssp_touched, nt);
         if (__any_sync(0xffffffffu, to_near)) {
             // out-edges of the next near queue: the next round's push / pull choice
             const unsigned long long dg = warp_sum((unsigned long long)(to_near ? off[d + 1] - off[d] : 0u));
@@ -90,12 +94,14 @@ struct SsspOp {
         if (threadIdx.x == 0) {
             s_sssp_newfar = 0;
             s_sssp_medges = 0;
+            s_sssp_touched = 0;
         }
     }
     __device__ __forceinline__ void block_end() const
     {
         if (threadIdx.x == 0 && s_sssp_newfar) atomicAdd(&ctr->far_len[0], s_sssp_newfar);
         if (threadIdx.x == 0 && s_sssp_medges) atomicAdd(&ctr->medges, s_sssp_medges);
+        if (threadIdx.x == 0 && s_sssp_touched) atomicAdd(&ctr->touched, s_sssp_touched);
     }
 };
 
@@ -140,12 +146,13 @@ __global__ void __launch_bounds__(kBlock) k_sssp_dense_scan(uint32_t V, const ui
 {
     const uint32_t n_round = (V + 31u) & ~31u;
     unsigned long long deg_sum = 0;
-    uint32_t new_far = 0;
+    uint32_t new_far = 0, touched = 0;
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n_round; v += gridDim.x * blockDim.x) {
         bool to_near = false, to_far = false;
-        if (v < V && v < nz) {
-            const uint32_t dv = dist[v];
-            if (dv < snap[v]) {
+        if (v < V) {
+            const uint32_t dv = dist[v], sv = snap[v];
+            touched += (sv == kValueMax && dv < kValueMax) ? 1u : 0u;
+            if (v < nz && dv < sv) {
                 to_near = dv < thr;
                 to_far = !to_near;
                 if (to_near) deg_sum += off[v + 1] - off[v];
@@ -162,9 +169,11 @@ __global__ void __launch_bounds__(kBlock) k_sssp_dense_scan(uint32_t V, const ui
         }
     }
     deg_sum = warp_sum(deg_sum);
+    touched = warp_sum(touched);
     if (lane_id() == 0) {
         if (deg_sum) atomicAdd(&ctr->medges, deg_sum);
         if (new_far) atomicAdd(&ctr->far_len[0], new_far);
+        if (touched) atomicAdd(&ctr->touched, touched);
     }
 }
 
@@ -258,6 +267,8 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
     uint64_t thr = delta;
     uint64_t bucket_lo = 0;      // the current bucket is [bucket_lo, thr): every near vertex is in it
     uint64_t near_edges = 0;     // out-edges of the near queue (0 = unknown: push)
+    double touch_rate = 0.0;     // vertices reached for the first time per edge, last push or dense round
+    uint64_t touched_seen = 0;   // ctr->touched after that round
     // pull rounds need the in-edges (and their weights in CSC order)
     const bool pull_ok = o.schedule != CGB_SCHED_FIXED && g->tune.sssp_pull_alpha > 0;
     uint64_t iters = 0;
@@ -286,10 +297,16 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
             }
             const int out = cur ^ 1;
             // direction: pull when the near set's out-edges times alpha exceed the graph's edges;
-            // else a dense frontier when they are a large share by sssp_dense_alpha
+            // else a dense frontier when they are many for what the round will change.  A push
+            // round pays an atomic with a returned value and a queue append per improvement, a
+            // dense round a reduction per edge plus one pass over V.  While the search reaches
+            // new territory nearly every edge improves its target, so the out-edges are weighted
+            // by the previous round's first touches per edge, floored at 1/8 for the rounds that
+            // mostly lower known distances
             const bool pull = pull_ok && (double)near_edges * g->tune.sssp_pull_alpha > (double)g->E;
             const bool dense = !pull && o.schedule != CGB_SCHED_FIXED && g->tune.sssp_dense_alpha > 0 &&
-                               (double)near_edges * g->tune.sssp_dense_alpha > (double)g->E;
+                               (double)near_edges * g->tune.sssp_dense_alpha * std::max(touch_rate, 0.125) >
+                                   (double)V;
             if (pull) {
                 ensure_csc(g);
                 ensure_csc_weights(g);
@@ -340,6 +357,10 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
                 g->trace.push_back(t);
             }
             expanded += nnear;
+            if (!pull && near_edges > 0) {
+                touch_rate = (double)(g->h_ctr->touched - touched_seen) / (double)near_edges;
+                touched_seen = g->h_ctr->touched;
+            }
             nnear = g->h_ctr->qlen[out];
             nfar = g->h_ctr->far_len[0];
             near_edges = g->h_ctr->medges;

@@ -53,7 +53,7 @@ std::vector<Field> fields()
         {&cgb_tuning::persist_ctas, {0, 16, 32, 64}, true, true, false, false, false, false},
         {&cgb_tuning::sssp_pull_alpha, {0, 2, 3, 5, 8}, false, true, false, false, false, false},
         {&cgb_tuning::cluster_enter, {0, 2048, 8192, 16384}, true, false, false, false, false, false},
-        {&cgb_tuning::sssp_dense_alpha, {0, 4, 8, 16, 32}, false, true, false, false, false, false},
+        {&cgb_tuning::sssp_dense_alpha, {0, 2, 4, 8, 16}, false, true, false, false, false, false},
         {&cgb_tuning::ms_edges, {64, 128, 256, 512, 1024}, false, false, false, false, false, true},
         {&cgb_tuning::pr_unroll, {4, 8, 16}, false, false, false, true, false, false},
         {&cgb_tuning::pr_ctas_per_sm, {16, 32, 64, 128, 256, 1024}, false, false, false, true, false, false},

@@ -234,7 +234,8 @@ typedef struct {
     uint32_t cluster_enter;    /* BFS frontiers up to this size run their levels in one thread-block
                                   cluster with a hardware barrier (0 = never, default 8192) */
     uint32_t sssp_dense_alpha; /* SSSP rounds use a dense frontier when the near set's out-edges times
-                                  this exceed E (0 = never, default 8) */
+                                  this times max(first touches per edge in the previous round, 1/8)
+                                  exceed V (0 = never, default 4) */
     uint32_t reserved[3];
 } cgb_tuning;
 
