@@ -14,9 +14,9 @@ PageRank = E x iterations.  `value` = all numerators of the K timed steps /
 their device time (CUDA events on the engine's stream, max over ranks).
 `e2e` = the same through the C ABI from pinned host buffers: every step
 uploads both CSRs (cgb_graph_create), runs the four algorithms and reads
-every result back into host memory; the symmetrised graph (CC) is
-uploaded and processed by a second host thread while the directed graph's
-algorithms run.
+every result back into host memory.  Uploads run back to back on a second
+host thread (the directed graph's weights, which only SSSP reads, then the
+symmetrised graph and its CC) while the directed graph's algorithms run.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 """
@@ -597,32 +597,45 @@ def bench_e2e(args, d, cg, gd, gs, roots, off_h, dst_h, w_h, sched):
     steps = args.e2e_steps or args.steps
 
     def step(root):
-        # The symmetrised graph is an independent graph with its own stream:
-        # a second host thread uploads it and runs CC once the directed
-        # graph's upload is done, so that upload overlaps the directed
-        # graph's algorithms instead of following them.
+        # The host-to-device link is the step's serial resource, so uploads go
+        # back to back while the GPU computes: the directed CSR's structure
+        # first; then, on a second host thread, its weights (only SSSP reads
+        # them; cgb_graph_set_weights) while BFS and PageRank run, and the
+        # symmetrised graph (an independent graph with its own stream) while
+        # SSSP runs, followed by its CC.
         box = {}
+        weights_in = threading.Event()
+        g = cg.Graph.from_csr(t_off, t_dst, None, vertexNum=V, edgeNum=gd.edgeNum, device=d.local)
 
-        def symmetrised():
+        def uploads():
+            try:
+                g.set_weights(t_w)
+            except BaseException as e:  # re-raised on the main thread
+                box["error"] = e
+            finally:
+                weights_in.set()
+            if "error" in box:
+                return
             try:
                 h = cg.Graph.from_csr(t_soff, t_sdst, None, vertexNum=V, edgeNum=gs.edgeNum, device=d.local)
                 h.run(CC, 0, opts, out=out_c)
                 box["edges"] = h.stats().traversed_edges
                 h.close()
-            except BaseException as e:  # re-raised on the main thread
+            except BaseException as e:
                 box["error"] = e
 
         edges = 0
-        g = cg.Graph.from_csr(t_off, t_dst, t_w, vertexNum=V, edgeNum=gd.edgeNum, device=d.local)
-        th = threading.Thread(target=symmetrised)
+        th = threading.Thread(target=uploads)
         th.start()
         try:
             g.run(BFS, root, opts, out=out_b)
             edges += g.stats().traversed_edges
-            g.run(SSSP, root, opts, out=out_s)
-            edges += g.stats().traversed_edges
             g.run(PR, args.pr_iters, opts, out=out_p)
             edges += g.stats().traversed_edges
+            weights_in.wait()
+            if "error" not in box:
+                g.run(SSSP, root, opts, out=out_s)
+                edges += g.stats().traversed_edges
             g.close()
         finally:
             th.join()
@@ -657,9 +670,10 @@ def bench_e2e(args, d, cg, gd, gs, roots, off_h, dst_h, w_h, sched):
             "ms_per_step": s_max * 1e3 / steps, "steps": steps,
             "step_ms": [round((b - a) * 1e3, 1) for a, b in zip(marks, marks[1:])],
             "pool_reserved_gb_after_step": pool_gb,
-            "what": "cgb_graph_create(directed CSR, host pinned) + BFS + SSSP + PR(20) -> host, destroy; "
-                    "a second host thread, started once the directed CSR is uploaded: "
-                    "cgb_graph_create(symmetrised CSR) + CC -> host, destroy; wall clock"}
+            "what": "cgb_graph_create(directed CSR structure, host pinned) + BFS + PR(20) + SSSP -> host, destroy; "
+                    "a second host thread, started once that structure is uploaded: cgb_graph_set_weights "
+                    "(directed weights, before the SSSP), then cgb_graph_create(symmetrised CSR) + CC -> host, "
+                    "destroy; wall clock"}
 
 
 def write_csr_files(dirpath, prefix, off, dst, w):

@@ -262,7 +262,7 @@ cgb_status cgb_batch_run(cgb_batch* b, int algorithm, const uint32_t* roots, uin
         CGB_REQUIRE(algorithm == CGB_BFS || algorithm == CGB_SSSP || algorithm == CGB_CC, CGB_EINVAL,
                     "batch runs are BFS, SSSP or CC");
         cgb_graph* g = b->g;
-        std::lock_guard<std::mutex> lock(g->mu);
+        std::lock_guard<GraphMutex> lock(g->mu);
         CGB_CUDA_TRY(cudaSetDevice(g->device));
         g->stats = cgb_run_stats{};
         if (algorithm == CGB_CC) {

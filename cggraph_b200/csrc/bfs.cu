@@ -189,8 +189,8 @@ void run_bfs(cgb_graph* g, uint32_t root, const cgb_options& o)
     PolicySamples* collect = want_pull && !force_pull ? g->collect : nullptr;
     Policy* pol = (o.schedule == CGB_SCHED_LEARNED && want_pull && !force_pull) ? policy_get() : nullptr;
 
-    uint32_t host_root_deg[2];
-    CGB_CUDA_TRY(cudaMemcpyAsync(host_root_deg, g->off + root, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+    PinnedArray<uint32_t> host_root_deg(2);  // pinned: see pinned_acquire
+    CGB_CUDA_TRY(cudaMemcpyAsync(host_root_deg.data(), g->off + root, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost,
                                  g->stream));
     CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
     CGB_CUDA_TRY(cudaEventRecord(g->ev_start, g->stream));

@@ -147,10 +147,19 @@ cgb_status cgb_graph_set_stream(cgb_graph* g, void* stream)
 {
     return guarded([&] {
         CGB_REQUIRE(g != nullptr, CGB_EINVAL, "graph is NULL");
-        std::lock_guard<std::mutex> lock(g->mu);
+        std::lock_guard<GraphMutex> lock(g->mu);
         CGB_CUDA_TRY(cudaSetDevice(g->device));
         CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
         g->stream = stream ? (cudaStream_t)stream : g->own_stream;
+    });
+}
+
+cgb_status cgb_graph_set_weights(cgb_graph* g, const uint32_t* weight)
+{
+    return guarded([&] {
+        CGB_REQUIRE(g != nullptr, CGB_EINVAL, "graph is NULL");
+        CGB_REQUIRE(weight != nullptr || g->E == 0, CGB_EINVAL, "weight is NULL");
+        graph_set_weights(g, weight);
     });
 }
 
@@ -253,7 +262,7 @@ cgb_status cgb_run(cgb_graph* g, int algorithm, uint32_t root_or_iters, const cg
         if (algorithm == CGB_BFS || algorithm == CGB_SSSP)
             CGB_REQUIRE(root_or_iters < g->V, CGB_EINVAL, "root >= vertexNum");
         const cgb_options o = effective_options(opt);
-        std::lock_guard<std::mutex> lock(g->mu);
+        std::lock_guard<GraphMutex> lock(g->mu);
         CGB_CUDA_TRY(cudaSetDevice(g->device));
         run_one(g, algorithm, root_or_iters, o);
         if (algorithm == CGB_PR) {
@@ -299,7 +308,7 @@ cgb_status cgb_run_batch(cgb_graph* g, int algorithm, const uint32_t* roots, uin
         CGB_REQUIRE(algorithm == CGB_BFS || algorithm == CGB_SSSP, CGB_EINVAL, "batch runs are BFS or SSSP");
         for (uint32_t i = 0; i < nroots; i++) CGB_REQUIRE(roots[i] < g->V, CGB_EINVAL, "root >= vertexNum");
         const cgb_options o = effective_options(opt);
-        std::lock_guard<std::mutex> lock(g->mu);
+        std::lock_guard<GraphMutex> lock(g->mu);
         CGB_CUDA_TRY(cudaSetDevice(g->device));
         const uint64_t V = g->V;
         if ((o.flags & CGB_FLAG_BATCH_SEQUENTIAL) || nroots == 1) {
@@ -383,7 +392,7 @@ cgb_status cgb_policy_collect(cgb_graph* g, int algorithm, uint32_t root, const 
         CGB_REQUIRE(root < g->V, CGB_EINVAL, "root >= vertexNum");
         cgb_options o = effective_options(opt);
         if (o.schedule == CGB_SCHED_FIXED) o.schedule = CGB_SCHED_HEURISTIC;
-        std::lock_guard<std::mutex> lock(g->mu);
+        std::lock_guard<GraphMutex> lock(g->mu);
         CGB_CUDA_TRY(cudaSetDevice(g->device));
         CGB_CUDA_TRY(cudaMalloc((void**)&ps.save_value, (size_t)g->V * 4));
         CGB_CUDA_TRY(cudaMalloc((void**)&ps.save_bm0, (size_t)g->words() * 4));

@@ -277,10 +277,10 @@ static void cc_afforest(cgb_graph* g)
     ++g->stats.launches;
     k_cc_sample<<<4, kBlock, 0, g->stream>>>(V, g->value, g->sample, kSamples, 0xAFF0E57ull);
     if (timing) ktimer_end(g);
-    std::vector<uint32_t> h(kSamples);
+    PinnedArray<uint32_t> h(kSamples);  // pinned: a pageable copy would wait on other threads' copies
     CGB_CUDA_TRY(cudaMemcpyAsync(h.data(), g->sample, kSamples * sizeof(uint32_t), cudaMemcpyDeviceToHost, g->stream));
     CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
-    std::sort(h.begin(), h.end());
+    std::sort(h.data(), h.data() + kSamples);
     uint32_t giant = h[0], best = 0;
     for (uint32_t i = 0; i < kSamples;) {
         uint32_t j = i;

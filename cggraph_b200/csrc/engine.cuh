@@ -45,6 +45,17 @@ struct MsBuffers;
 struct MsspBuffers;
 }
 
+// A graph's lock.  Taking it also swaps in weights that
+// cgb_graph_set_weights uploaded while the graph was busy, so they take
+// effect at the next entry point that uses the graph.
+struct GraphMutex {
+    std::mutex m;
+    struct cgb_graph* owner = nullptr;
+    void lock();
+    bool try_lock();
+    void unlock() { m.unlock(); }
+};
+
 // Launch parameters a graph starts with (cgb_tuning in the C ABI).
 inline cgb_tuning default_tuning()
 {
@@ -73,7 +84,11 @@ struct cgb_graph {
     uint32_t V = 0, E = 0, nz = 0;  // nz = noZeroOutDegreeNum
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
-    std::mutex mu;
+    GraphMutex mu;
+    // weights uploaded by cgb_graph_set_weights while the graph was busy
+    std::mutex pending_mu;
+    uint32_t* pending_w = nullptr;
+    uint64_t pending_sum_w = 0;
 
     // CSR (always resident)
     uint32_t* off = nullptr;
@@ -90,6 +105,9 @@ struct cgb_graph {
     bool csc_owned = false;
     uint32_t* in_w = nullptr;  // weights in CSC order (SSSP pull rounds); may alias w
     bool in_w_owned = false;
+    bool lists_resorted = false;
+    void* h_persist = nullptr;  // pinned host copy of the device-resident loop state
+    size_t h_persist_bytes = 0;  // create sorted the neighbour lists (weights follow that order)
     int symmetric = -1;
 
     // PageRank layout: vertices relabelled by out-degree bucket (stable; zero
@@ -152,6 +170,7 @@ struct cgb_graph {
     uint32_t flags = 0;
 
     uint32_t words() const { return V / 32 + 1; }
+    cgb_graph() { mu.owner = this; }
 };
 
 namespace cgb {
@@ -165,6 +184,8 @@ constexpr uint32_t kHugeChunk = 4096;
 // graph lifetime and preparation (graph.cu)
 cgb_graph* graph_alloc(uint32_t V, uint32_t E, uint32_t nz, int device, bool with_weight);
 void graph_free(cgb_graph* g);
+// Attaches or replaces the edge weights (cgb_graph_set_weights).
+void graph_set_weights(cgb_graph* g, const uint32_t* weight);
 void validate_and_sort(cgb_graph* g);
 void compute_weight_sum(cgb_graph* g);
 uint32_t sssp_default_delta(const cgb_graph* g);
@@ -201,6 +222,25 @@ void free_mssp(cgb_graph* g);
 // (and complete on return); released with the graph (graph_free).
 void* pool_alloc(size_t bytes, cudaStream_t s);
 void* pinned_small_alloc(size_t bytes);
+// Pinned host memory for small transfers, from a process-wide pool.
+void* pinned_acquire(size_t bytes);
+void pinned_release(void* p, size_t bytes);
+// A small transfer from pinned host memory by a kernel (no copy engine).
+void h2d_small(void* dst, const void* pinned_src, size_t bytes, cudaStream_t s);
+
+// n values of T in pinned host memory for the scope of a transfer (the
+// stream must be synchronised before the block goes out of scope).
+template <typename T>
+struct PinnedArray {
+    T* p;
+    size_t n;
+    explicit PinnedArray(size_t count) : p(static_cast<T*>(pinned_acquire(count * sizeof(T)))), n(count) {}
+    ~PinnedArray() { pinned_release(p, n * sizeof(T)); }
+    PinnedArray(const PinnedArray&) = delete;
+    PinnedArray& operator=(const PinnedArray&) = delete;
+    T& operator[](size_t i) { return p[i]; }
+    T* data() { return p; }
+};
 void pinned_small_free(void* p);
 // Weights in CSC order (in_w); needs the graph's weights.
 void ensure_csc_weights(cgb_graph* g);

@@ -111,6 +111,72 @@ void pinned_small_free(void* p)
     g_pinned_free.push_back(p);
 }
 
+// Pinned host blocks for the engine's own small transfers (flags, counts,
+// samples, hub-row tables), by power-of-two size class, reused and kept
+// until exit.  A copy to or from pageable memory is staged by the driver
+// and waits for everything queued before it on its stream; while it waits,
+// other threads' pageable copies wait too (a counter read behind a 2 GB
+// upload held another graph's PageRank layout for 45 ms).
+namespace {
+std::mutex g_pinned_big_mu;
+std::vector<void*> g_pinned_big_free[40];
+int pinned_class(size_t bytes)
+{
+    int c = 9;  // 512 bytes
+    while (((size_t)1 << c) < bytes) c++;
+    return c;
+}
+}  // namespace
+
+void* pinned_acquire(size_t bytes)
+{
+    if (bytes <= kPinnedSlot) return pinned_small_alloc(kPinnedSlot);
+    const int c = pinned_class(bytes);
+    CGB_REQUIRE(c < 40, CGB_EINVAL, "pinned block too large");
+    {
+        std::lock_guard<std::mutex> lock(g_pinned_big_mu);
+        if (!g_pinned_big_free[c].empty()) {
+            void* p = g_pinned_big_free[c].back();
+            g_pinned_big_free[c].pop_back();
+            return p;
+        }
+    }
+    void* p = nullptr;
+    CGB_CUDA_TRY(cudaMallocHost(&p, (size_t)1 << c));
+    return p;
+}
+
+void pinned_release(void* p, size_t bytes)
+{
+    if (!p) return;
+    if (bytes <= kPinnedSlot) {
+        pinned_small_free(p);
+        return;
+    }
+    std::lock_guard<std::mutex> lock(g_pinned_big_mu);
+    g_pinned_big_free[pinned_class(bytes)].push_back(p);
+}
+
+// Small host-to-device transfers by a kernel that reads the pinned source
+// through its device mapping, not by a copy engine: a copy engine works in
+// order, and a small copy queued behind another graph's multi-GB upload
+// waited for all of it (about 40 ms).  `src` must come from pinned_acquire
+// (or another cudaMallocHost block); `bytes` is a multiple of 4.
+__global__ void k_copy_words_from_host(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst, uint64_t n)
+{
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        dst[i] = src[i];
+}
+
+void h2d_small(void* dst, const void* pinned_src, size_t bytes, cudaStream_t s)
+{
+    const uint64_t n = bytes / 4;
+    if (!n) return;
+    k_copy_words_from_host<<<grid_for(n, kBlock, kNumSMs), kBlock, 0, s>>>(static_cast<const uint32_t*>(pinned_src),
+                                                                           static_cast<uint32_t*>(dst), n);
+    CGB_CUDA_TRY(cudaGetLastError());
+}
+
 void memory_trim(int device)
 {
     CGB_CUDA_TRY(cudaSetDevice(device));
@@ -119,10 +185,13 @@ void memory_trim(int device)
     CGB_CUDA_TRY(cudaMemPoolTrimTo(dp.pool, 0));
 }
 
-// Grows the pool to at least `bytes` reserved: one allocation that brings
-// the used amount up to `bytes` (the pool reserves at least what is in
-// use), freed again; the pool keeps it (release threshold: never) and
-// splits it for later allocations.
+// Grows the pool to at least `bytes` reserved: allocations of at most
+// kReserveChunk each that bring the used amount up to `bytes` (the pool
+// reserves at least what is in use), freed again; the pool keeps them
+// (release threshold: never) for later allocations.  One block of many GB
+// is avoided: buffers placed in such a block ran PageRank 2.6x slower here.
+constexpr uint64_t kReserveChunk = 1ull << 30;
+
 void memory_reserve(int device, uint64_t bytes)
 {
     CGB_CUDA_TRY(cudaSetDevice(device));
@@ -133,9 +202,16 @@ void memory_reserve(int device, uint64_t bytes)
     if (r >= bytes) return;
     cudaStream_t s = nullptr;
     CGB_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-    void* p = nullptr;
-    cudaError_t err = cudaMallocFromPoolAsync(&p, bytes - u, dp.pool, s);
-    if (err == cudaSuccess) err = cudaFreeAsync(p, s);
+    std::vector<void*> blocks;
+    cudaError_t err = cudaSuccess;
+    for (uint64_t need = bytes - u; need > 0 && err == cudaSuccess;) {
+        const uint64_t n = std::min(need, kReserveChunk);
+        void* p = nullptr;
+        err = cudaMallocFromPoolAsync(&p, n, dp.pool, s);
+        if (err == cudaSuccess) blocks.push_back(p);
+        need -= n;
+    }
+    for (void* p : blocks) cudaFreeAsync(p, s);
     cudaError_t err2 = cudaStreamSynchronize(s);
     cudaStreamDestroy(s);
     CGB_CUDA_TRY(err);
@@ -508,8 +584,8 @@ void validate_and_sort(cgb_graph* g)
     uint32_t* flags = dalloc<uint32_t>(4, g->stream);
     CGB_CUDA_TRY(cudaMemsetAsync(flags, 0, 4 * sizeof(uint32_t), g->stream));
     k_check_offsets<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, E, g->off, flags);
-    uint32_t h[4];
-    CGB_CUDA_TRY(cudaMemcpyAsync(h, flags, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
+    PinnedArray<uint32_t> h(4);
+    CGB_CUDA_TRY(cudaMemcpyAsync(h.data(), flags, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, g->stream));
     CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
     if (h[0]) {
         dfree(flags, g->stream);
@@ -528,7 +604,7 @@ void validate_and_sort(cgb_graph* g)
         CGB_CUDA_TRY(cudaMemsetAsync(flags, 0, 4 * sizeof(uint32_t), g->stream));
         k_mark_heads<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, g->off, heads);
         k_check_edges<<<grid_for(E, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(V, E, g->dst, heads, flags);
-        CGB_CUDA_TRY(cudaMemcpyAsync(h, flags, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
+        CGB_CUDA_TRY(cudaMemcpyAsync(h.data(), flags, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, g->stream));
         CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
         if (h[0] & 8u) {
             dfree(heads, g->stream);
@@ -537,6 +613,7 @@ void validate_and_sort(cgb_graph* g)
         }
         if (pass == 0 && h[1]) {
             sort_neighbours(g);
+            g->lists_resorted = true;
             continue;
         }
         if (h[1] || h[2]) {
@@ -556,16 +633,82 @@ void compute_weight_sum(cgb_graph* g)
     unsigned long long* d = dalloc<unsigned long long>(1, g->stream);
     CGB_CUDA_TRY(cudaMemsetAsync(d, 0, sizeof(unsigned long long), g->stream));
     k_sum_u32<<<grid_for(g->E, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(g->E, g->w, d);
-    unsigned long long h = 0;
-    CGB_CUDA_TRY(cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
+    PinnedArray<unsigned long long> h(1);
+    CGB_CUDA_TRY(cudaMemcpyAsync(h.data(), d, sizeof(unsigned long long), cudaMemcpyDeviceToHost, g->stream));
     CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
     dfree(d, g->stream);
-    g->sum_w = h;
+    g->sum_w = h[0];
 }
 
 // differ = 1 when a and b differ somewhere.  Warps walk the arrays in
 // lockstep; the first warp that sees a difference sets the flag with one
 // atomic, and every warp looks at the flag each 16 steps to stop early.
+// Weights given after create (cgb_graph_set_weights) are uploaded and summed
+// on a private stream without holding the graph, then left pending; whoever
+// takes the graph's lock next swaps them in (GraphMutex::lock), at once if
+// the graph is idle.  Weights in CSC order are rebuilt on their next use.
+static void swap_in_pending_weights(cgb_graph* g) noexcept
+{
+    uint32_t* w = nullptr;
+    uint64_t sum = 0;
+    {
+        std::lock_guard<std::mutex> pl(g->pending_mu);
+        w = g->pending_w;
+        sum = g->pending_sum_w;
+        g->pending_w = nullptr;
+    }
+    if (!w) return;
+    cudaSetDevice(g->device);
+    // stream-ordered frees: after every earlier use of the old weights
+    if (g->in_w_owned) dfree(g->in_w, g->stream);
+    g->in_w = nullptr;
+    g->in_w_owned = false;
+    if (g->w) dfree(g->w, g->stream);
+    g->w = w;
+    g->sum_w = sum;
+}
+
+void graph_set_weights(cgb_graph* g, const uint32_t* weight)
+{
+    CGB_REQUIRE(!g->lists_resorted, CGB_EINVAL,
+                "weights must be given to cgb_graph_create when it had to sort the neighbour lists");
+    const uint32_t E = g->E;
+    if (E == 0) return;
+    CGB_CUDA_TRY(cudaSetDevice(g->device));
+    cudaStream_t s = nullptr;
+    CGB_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    uint32_t* w = nullptr;
+    unsigned long long* sum = nullptr;
+    PinnedArray<unsigned long long> hs(1);
+    try {
+        w = dalloc<uint32_t>(E, s);
+        sum = dalloc<unsigned long long>(1, s);
+        CGB_CUDA_TRY(cudaMemcpyAsync(w, weight, (size_t)E * 4, cudaMemcpyDefault, s));
+        CGB_CUDA_TRY(cudaMemsetAsync(sum, 0, sizeof(unsigned long long), s));
+        k_sum_u32<<<grid_for(E, kBlock, kNumSMs * 8), kBlock, 0, s>>>(E, w, sum);
+        CGB_CUDA_TRY(cudaMemcpyAsync(hs.data(), sum, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+        CGB_CUDA_TRY(cudaStreamSynchronize(s));
+    } catch (...) {
+        dfree(w, s);
+        dfree(sum, s);
+        cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+        throw;
+    }
+    dfree(sum, s);
+    CGB_CUDA_TRY(cudaStreamSynchronize(s));
+    CGB_CUDA_TRY(cudaStreamDestroy(s));
+    uint32_t* replaced = nullptr;
+    {
+        std::lock_guard<std::mutex> pl(g->pending_mu);
+        replaced = g->pending_w;  // weights set twice while the graph stayed busy
+        g->pending_w = w;
+        g->pending_sum_w = hs[0];
+    }
+    if (replaced) dfree(replaced, g->stream);
+    if (g->mu.try_lock()) g->mu.unlock();  // idle graph: swapped in now
+}
+
 __global__ void k_compare_u32(uint64_t n, const uint32_t* __restrict__ a, const uint32_t* __restrict__ b,
                               uint32_t* differ)
 {
@@ -762,7 +905,7 @@ static bool check_symmetric(cgb_graph* g)
     k_sym_counts<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, g->off, g->dst, lower, upper);
     exclusive_sum_u32(g, lower, loff, (uint64_t)V + 1);
     exclusive_sum_u32(g, upper, uoff, (uint64_t)V + 1);
-    uint32_t tot[2] = {0, 0};
+    PinnedArray<uint32_t> tot(2);
     CGB_CUDA_TRY(cudaMemcpyAsync(&tot[0], loff + V, 4, cudaMemcpyDeviceToHost, g->stream));
     CGB_CUDA_TRY(cudaMemcpyAsync(&tot[1], uoff + V, 4, cudaMemcpyDeviceToHost, g->stream));
     CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
@@ -782,10 +925,10 @@ static bool check_symmetric(cgb_graph* g)
         dfree(val, g->stream);
         CGB_CUDA_TRY(cudaMemsetAsync(differ, 0, 4, g->stream));
         launch_edges_by_row(g, V, E, g->off, SymCompareF{g->dst, loff, skey, sval, differ});
-        uint32_t h = 0;
-        CGB_CUDA_TRY(cudaMemcpyAsync(&h, differ, 4, cudaMemcpyDeviceToHost, g->stream));
+        PinnedArray<uint32_t> h(1);
+        CGB_CUDA_TRY(cudaMemcpyAsync(h.data(), differ, 4, cudaMemcpyDeviceToHost, g->stream));
         CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
-        sym = h == 0;
+        sym = h[0] == 0;
         dfree(skey, g->stream);
         dfree(sval, g->stream);
         dfree(differ, g->stream);
@@ -818,11 +961,11 @@ static void build_transpose(cgb_graph* g)
     CGB_CUDA_TRY(cudaMemsetAsync(differ, 0, sizeof(uint32_t), g->stream));
     k_compare_u32<<<kNumSMs * 8, kBlock, 0, g->stream>>>((uint64_t)V + 1, in_off, g->off, differ);
     if (E) k_compare_u32<<<kNumSMs * 8, kBlock, 0, g->stream>>>(E, in_src, g->dst, differ);
-    uint32_t h = 0;
-    CGB_CUDA_TRY(cudaMemcpyAsync(&h, differ, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
+    PinnedArray<uint32_t> h(1);
+    CGB_CUDA_TRY(cudaMemcpyAsync(h.data(), differ, 4, cudaMemcpyDeviceToHost, g->stream));
     CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
     dfree(differ, g->stream);
-    if (h) {
+    if (h[0]) {
         g->symmetric = 0;
         g->in_off = in_off;
         g->in_src = in_src;
@@ -879,11 +1022,11 @@ void ensure_csc_weights(cgb_graph* g)
     uint32_t* differ = dalloc<uint32_t>(1, g->stream);
     CGB_CUDA_TRY(cudaMemsetAsync(differ, 0, 4, g->stream));
     k_compare_u32<<<kNumSMs * 8, kBlock, 0, g->stream>>>(E, vals, g->w, differ);
-    uint32_t h = 0;
-    CGB_CUDA_TRY(cudaMemcpyAsync(&h, differ, 4, cudaMemcpyDeviceToHost, g->stream));
+    PinnedArray<uint32_t> h(1);
+    CGB_CUDA_TRY(cudaMemcpyAsync(h.data(), differ, 4, cudaMemcpyDeviceToHost, g->stream));
     CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
     dfree(differ, g->stream);
-    if (h) {
+    if (h[0]) {
         g->in_w = vals;
         g->in_w_owned = true;
     } else {
@@ -911,8 +1054,10 @@ void ensure_frontier(cgb_graph* g)
     uint32_t* d = dalloc<uint32_t>(1, g->stream);
     CGB_CUDA_TRY(cudaMemsetAsync(d, 0, 4, g->stream));
     k_max_degree<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, g->off, d);
-    CGB_CUDA_TRY(cudaMemcpyAsync(&g->max_degree, d, 4, cudaMemcpyDeviceToHost, g->stream));
+    PinnedArray<uint32_t> md(1);
+    CGB_CUDA_TRY(cudaMemcpyAsync(md.data(), d, 4, cudaMemcpyDeviceToHost, g->stream));
     CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    g->max_degree = md[0];
     dfree(d, g->stream);
 }
 
@@ -1045,9 +1190,10 @@ static void build_sell(cgb_graph* g)
     void* temp = dalloc<char>(tb, g->stream);
     cudaError_t err =
         cub::DeviceScan::ExclusiveSum(temp, tb, width, g->pr_slice_ptr, (uint64_t)nslices + 1, g->stream);
-    uint64_t total = 0;
-    CGB_CUDA_TRY(cudaMemcpyAsync(&total, g->pr_slice_ptr + nslices, 8, cudaMemcpyDeviceToHost, g->stream));
+    PinnedArray<uint64_t> tp(1);
+    CGB_CUDA_TRY(cudaMemcpyAsync(tp.data(), g->pr_slice_ptr + nslices, 8, cudaMemcpyDeviceToHost, g->stream));
     CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    const uint64_t total = tp[0];
     dfree(temp, g->stream);
     dfree(width, g->stream);
     CGB_CUDA_TRY(err);
@@ -1145,42 +1291,44 @@ void ensure_pr(cgb_graph* g)
         CGB_CUDA_TRY(cudaMemsetAsync(n, 0, sizeof(uint32_t), g->stream));
         k_collect_heavy_rows<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, g->pr_off, kPrHuge, rows,
                                                                                         n);
-        uint32_t h = 0;
-        CGB_CUDA_TRY(cudaMemcpyAsync(&h, n, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
+        PinnedArray<uint32_t> hn(1);
+        CGB_CUDA_TRY(cudaMemcpyAsync(hn.data(), n, 4, cudaMemcpyDeviceToHost, g->stream));
         CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        const uint32_t h = hn[0];
         dfree(n, g->stream);
-        std::vector<uint32_t> hrows(h), lo(h), hi(h);
+        // pinned staging for every transfer here (see pinned_acquire, h2d_small)
+        PinnedArray<uint32_t> hrows(std::max<uint32_t>(h, 1)), lohi_h(2 * (size_t)std::max<uint32_t>(h, 1));
         if (h) {
-            // copies on the graph's stream (pageable host memory: each waits)
             CGB_CUDA_TRY(cudaMemcpyAsync(hrows.data(), rows, h * 4ull, cudaMemcpyDeviceToHost, g->stream));
             CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
-            std::sort(hrows.begin(), hrows.end());
-            CGB_CUDA_TRY(cudaMemcpyAsync(rows, hrows.data(), h * 4ull, cudaMemcpyHostToDevice, g->stream));
+            std::sort(hrows.data(), hrows.data() + h);
+            h2d_small(rows, hrows.data(), h * 4ull, g->stream);
             uint32_t* lohi = dalloc<uint32_t>(2ull * h, g->stream);
             k_row_bounds<<<grid_for(h, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(rows, h, g->pr_off, lohi);
-            CGB_CUDA_TRY(cudaMemcpyAsync(lo.data(), lohi, h * 4ull, cudaMemcpyDeviceToHost, g->stream));
-            CGB_CUDA_TRY(cudaMemcpyAsync(hi.data(), lohi + h, h * 4ull, cudaMemcpyDeviceToHost, g->stream));
+            CGB_CUDA_TRY(cudaMemcpyAsync(lohi_h.data(), lohi, 2ull * h * 4, cudaMemcpyDeviceToHost, g->stream));
             CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
             dfree(lohi, g->stream);
         }
-        std::vector<uint2> chunks;
-        std::vector<uint32_t> base(h + 1, 0);
+        uint64_t nch = 0;
+        for (uint32_t i = 0; i < h; i++) nch += (lohi_h[h + i] - lohi_h[i] + kPrChunk - 1) / kPrChunk;
+        PinnedArray<uint2> chunks(std::max<uint64_t>(nch, 1));
+        PinnedArray<uint32_t> base(h + 1);
+        uint32_t c = 0;
         for (uint32_t i = 0; i < h; i++) {
-            base[i] = (uint32_t)chunks.size();
-            for (uint32_t e = lo[i]; e < hi[i]; e += kPrChunk) chunks.push_back(make_uint2(hrows[i], e));
+            base[i] = c;
+            for (uint32_t e = lohi_h[i]; e < lohi_h[h + i]; e += kPrChunk) chunks[c++] = make_uint2(hrows[i], e);
         }
-        base[h] = (uint32_t)chunks.size();
+        base[h] = c;
         g->n_pr_huge = h;
-        g->n_pr_chunks = (uint32_t)chunks.size();
+        g->n_pr_chunks = c;
         g->pr_huge_rows = rows;
         g->pr_chunk_base = dalloc<uint32_t>(h + 1, g->stream);
-        CGB_CUDA_TRY(cudaMemcpyAsync(g->pr_chunk_base, base.data(), (h + 1) * 4ull, cudaMemcpyHostToDevice, g->stream));
-        g->pr_chunks = dalloc<uint2>(chunks.size(), g->stream);
-        if (!chunks.empty())
-            CGB_CUDA_TRY(cudaMemcpyAsync(g->pr_chunks, chunks.data(), chunks.size() * sizeof(uint2),
-                                         cudaMemcpyHostToDevice, g->stream));
-        CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));  // base and chunks go out of scope
-        g->pr_part = dalloc<double>(chunks.size(), g->stream);
+        h2d_small(g->pr_chunk_base, base.data(), (h + 1) * 4ull, g->stream);
+        g->pr_chunks = dalloc<uint2>(c, g->stream);
+        if (c)
+            h2d_small(g->pr_chunks, chunks.data(), (size_t)c * sizeof(uint2), g->stream);
+        CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));  // the pinned tables go out of scope
+        g->pr_part = dalloc<double>(c, g->stream);
     }
     g->pr_ready = true;
 }
@@ -1268,6 +1416,7 @@ void graph_free(cgb_graph* g)
         dfree(g->in_src, g->stream);
     }
     if (g->in_w_owned) dfree(g->in_w, g->stream);
+    if (g->pending_w) dfree(g->pending_w, g->stream);
     free_msbfs(g);
     free_mssp(g);
     void* ptrs[] = {g->off, g->dst, g->w, g->pr_huge_rows, g->pr_rank, g->pr_off, g->pr_src, g->pr_outdeg,
@@ -1277,6 +1426,7 @@ void graph_free(cgb_graph* g)
                     g->aux_bm, g->persist, g->ctr};
     for (void* p : ptrs) dfree(p, g->stream);
     pinned_small_free(g->h_ctr);
+    pinned_release(g->h_persist, g->h_persist_bytes);
     for (cudaEvent_t e : g->kev) cudaEventDestroy(e);
     cudaEvent_t evs[] = {g->ev_start, g->ev_stop, g->ev_iter[0], g->ev_iter[1], g->ev_fork, g->ev_join};
     for (cudaEvent_t e : evs)
@@ -1287,3 +1437,16 @@ void graph_free(cgb_graph* g)
 }
 
 }  // namespace cgb
+
+void GraphMutex::lock()
+{
+    m.lock();
+    cgb::swap_in_pending_weights(owner);
+}
+
+bool GraphMutex::try_lock()
+{
+    if (!m.try_lock()) return false;
+    cgb::swap_in_pending_weights(owner);
+    return true;
+}

@@ -407,12 +407,24 @@ static PersistState* persist_state(cgb_graph* g)
     return static_cast<PersistState*>(g->persist);
 }
 
+// The graph's pinned host block for the state (pinned: a pageable copy waits
+// for other threads' pageable copies, see pinned_acquire).
+static PersistState* host_state(cgb_graph* g)
+{
+    if (!g->h_persist) {
+        g->h_persist = pinned_acquire(sizeof(PersistState));
+        g->h_persist_bytes = sizeof(PersistState);
+    }
+    return static_cast<PersistState*>(g->h_persist);
+}
+
 // Host copy of the state after a launch (synchronises the stream).
 static PersistState read_state(cgb_graph* g)
 {
-    PersistState h;
-    CGB_CUDA_TRY(cudaMemcpyAsync(&h, g->persist, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
+    PersistState* hp = host_state(g);
+    CGB_CUDA_TRY(cudaMemcpyAsync(hp, g->persist, sizeof(PersistState), cudaMemcpyDeviceToHost, g->stream));
     CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    const PersistState h = *hp;
     CGB_REQUIRE(!(h.status & 2u), CGB_EOVERFLOW, "device-resident loop: queue overflow");
     CGB_REQUIRE(!(h.status & 1u), CGB_ETIMEOUT, "device-resident loop: grid barrier gave up");
     return h;
@@ -420,11 +432,15 @@ static PersistState read_state(cgb_graph* g)
 
 static void init_state(cgb_graph* g, uint32_t nf, unsigned long long scout, uint32_t max_deg)
 {
-    PersistState h{};
+    // the graph's pinned state block: its previous copy has completed, since
+    // every launch is followed by read_state (a synchronisation)
+    PersistState& h = *host_state(g);
+    h = PersistState{};
     h.qlen[0] = nf;
     h.medges[0] = scout;
     h.max_deg[0] = max_deg;
-    CGB_CUDA_TRY(cudaMemcpyAsync(g->persist, &h, sizeof(h), cudaMemcpyHostToDevice, g->stream));
+    static_assert(sizeof(PersistState) % 4 == 0, "copied as words");
+    h2d_small(g->persist, &h, sizeof(PersistState), g->stream);
 }
 
 // CTAs of the level-loop cluster: 16 when the device schedules such a

@@ -579,7 +579,7 @@ static void group_loop(cgb_server* s, int a)
             const auto t_tick = Clock::now();
             unsigned long long fin;
             if (a == 0) {
-                std::lock_guard<std::mutex> glk(g->mu);
+                std::lock_guard<GraphMutex> glk(g->mu);
                 g->tune = g->tune_alg[CGB_BFS];
                 bfs_issue(s, G);
                 CGB_CUDA_TRY(cudaMemcpyAsync(G.h_stats->alive, G.d_stats->alive, sizeof(G.h_stats->alive),
@@ -672,7 +672,7 @@ cgb_status cgb_server_create(cgb_graph* g, const cgb_server_config* cfg, cgb_ser
                 else break;
             }
         }
-        std::lock_guard<std::mutex> lock(g->mu);
+        std::lock_guard<GraphMutex> lock(g->mu);
         CGB_CUDA_TRY(cudaSetDevice(g->device));
         ensure_frontier(g);
         if (nb) ensure_csc(g);

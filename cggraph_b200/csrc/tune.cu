@@ -88,7 +88,7 @@ cgb_status cgb_tuning_set(cgb_graph* g, int algorithm, const cgb_tuning* t)
         set_error("cgb_tuning value out of range");
         return CGB_EINVAL;
     }
-    std::lock_guard<std::mutex> lock(g->mu);
+    std::lock_guard<GraphMutex> lock(g->mu);
     for (int a = 0; a <= CGB_PR; a++) {
         if (algorithm != -1 && a != algorithm) continue;
         g->tune_alg[a] = *t;
@@ -161,13 +161,13 @@ cgb_status cgb_autotune(cgb_graph* g, int algorithm, const uint32_t* roots, uint
                 cand.*(f.member) = v;
                 if (!valid(cand)) continue;
                 {
-                    std::lock_guard<std::mutex> lock(g->mu);
+                    std::lock_guard<GraphMutex> lock(g->mu);
                     slot = cand;
                 }
                 double ms = 0;
                 st = score(ms);
                 if (st != CGB_OK) {
-                    std::lock_guard<std::mutex> lock(g->mu);
+                    std::lock_guard<GraphMutex> lock(g->mu);
                     slot = start;
                     return st;
                 }
@@ -177,13 +177,13 @@ cgb_status cgb_autotune(cgb_graph* g, int algorithm, const uint32_t* roots, uint
                     moved = true;
                 }
             }
-            std::lock_guard<std::mutex> lock(g->mu);
+            std::lock_guard<GraphMutex> lock(g->mu);
             slot = cur;
         }
         if (!moved) break;
     }
     {
-        std::lock_guard<std::mutex> lock(g->mu);
+        std::lock_guard<GraphMutex> lock(g->mu);
         slot = (flags & CGB_TUNE_KEEP_DEFAULT) ? start : cur;
     }
     if (best) *best = cur;

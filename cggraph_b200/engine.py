@@ -281,6 +281,13 @@ class Graph:
             ptr = stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
         check(L.lib().cgb_graph_set_stream(self._h, ptr))
 
+    def set_weights(self, weight) -> None:
+        """Attach (or replace) the edge weights, E values in CSR order
+        (cgb_graph_set_weights); safe to call from another thread while a
+        BFS, CC or PageRank run uses the graph."""
+        weight = _u32(weight)
+        check(L.lib().cgb_graph_set_weights(self._h, _ptr(weight)))
+
     def download(self, with_weight: bool = True):
         off = np.empty(self.vertexNum + 1, np.uint32)
         dst = np.empty(max(1, self.edgeNum), np.uint32)

@@ -153,6 +153,18 @@ cgb_status cgb_graph_destroy(cgb_graph* g);
  * its stream. */
 cgb_status cgb_graph_set_stream(cgb_graph* g, void* stream);
 
+/* Attaches edge weights to a graph created without them, or replaces its
+ * weights: E values in the graph's CSR order, in host or device memory. Only
+ * SSSP reads weights, so a caller can upload them while BFS, CC or PageRank
+ * run on the same graph from another thread: the upload does not wait for
+ * the graph. When it returns, the weights are in effect for every later
+ * call on the graph (a run already in progress finishes with the old ones;
+ * SSSP without weights uses unit weights). Not while a request server runs
+ * on the graph. CGB_EINVAL when cgb_graph_create had to sort the neighbour
+ * lists (give the weights to create then). Engine-specific (no reference
+ * counterpart). */
+cgb_status cgb_graph_set_weights(cgb_graph* g, const uint32_t* weight);
+
 /* V, E and whether the graph is symmetric (-1 = not yet known). */
 cgb_status cgb_graph_info(const cgb_graph* g, uint32_t* V, uint32_t* E, int32_t* symmetric);
 

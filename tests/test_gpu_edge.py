@@ -156,6 +156,51 @@ def test_symmetry_check_when_cc_runs_first(oracle):
             np.testing.assert_array_equal(g.run(BFS, r)[0], oracle.bfs(off, dst, r))
 
 
+def test_weights_attached_after_create(oracle):
+    """cgb_graph_set_weights: unit weights until weights arrive, the given
+    weights after, replacements honoured, and an upload from another thread
+    while BFS and PageRank run leaves every result unchanged."""
+    import threading
+    off, dst, w = oracle.rmat_graph(14, 16, seed=12)
+    w2 = (w[::-1] % 50 + 1).astype(np.uint32)
+    deg = np.diff(off.astype(np.int64))
+    r = int(deg.argmax())
+    exp_bfs = oracle.bfs(off, dst, r)
+    exp_pr = oracle.pagerank(off, dst, 20)
+    with cg.Graph.from_csr(off, dst, None) as g:
+        np.testing.assert_array_equal(g.run(SSSP, r)[0], exp_bfs)  # no weights yet: unit weights
+        g.set_weights(w)
+        np.testing.assert_array_equal(g.run(SSSP, r)[0], oracle.sssp(off, dst, w, r))
+        g.set_weights(w2)
+        np.testing.assert_array_equal(g.run(SSSP, r)[0], oracle.sssp(off, dst, w2, r))
+    with cg.Graph.from_csr(off, dst, None) as g:
+        err = []
+
+        def upload():
+            try:
+                g.set_weights(w)
+            except Exception as e:  # reported on the main thread
+                err.append(e)
+
+        th = threading.Thread(target=upload)
+        th.start()
+        for _ in range(3):
+            np.testing.assert_array_equal(g.run(BFS, r)[0], exp_bfs)
+            got = g.run(PR, 20)[0]
+            assert np.max(np.abs(got - exp_pr) / exp_pr) <= 1e-6
+        th.join()
+        assert not err, err
+        np.testing.assert_array_equal(g.run(SSSP, r)[0], oracle.sssp(off, dst, w, r))
+    # lists that create had to sort: the weights' order is unknown, so refused
+    d2 = dst.copy()
+    for v in range(off.size - 1):
+        d2[off[v]:off[v + 1]] = d2[off[v]:off[v + 1]][::-1]
+    with cg.Graph.from_csr(off, d2, None) as g:
+        with pytest.raises(CgbError) as ei:
+            g.set_weights(w)
+        assert ei.value.status == L.EINVAL
+
+
 def test_zero_out_degree_tail(oracle):
     """noZeroOutDegreeNum < V (the reordered layout whose last vertices have no
     out-edges, main_partition.hpp:78-103)."""
