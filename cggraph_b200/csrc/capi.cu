@@ -138,6 +138,32 @@ cgb_status cgb_graph_load_files(const char* off_path, const char* dst_path, cons
     return st;
 }
 
+cgb_status cgb_graph_create_from_edges(const uint32_t* records, uint64_t num_edges, uint32_t V, int device,
+                                       cgb_graph** out)
+{
+    return guarded([&] {
+        CGB_REQUIRE(out != nullptr, CGB_EINVAL, "out is NULL");
+        *out = nullptr;
+        *out = graph_from_edges(records, num_edges, V, device);
+    });
+}
+
+cgb_status cgb_graph_load_edge_file(const char* path, uint32_t V, int device, cgb_graph** out)
+{
+    return guarded([&] {
+        CGB_REQUIRE(out != nullptr, CGB_EINVAL, "out is NULL");
+        *out = nullptr;
+        CGB_REQUIRE(path != nullptr, CGB_EINVAL, "path is NULL");
+        struct stat st;
+        if (stat(path, &st) != 0) throw Error{CGB_EIO, std::string("Bin File [") + path + "] Not Exist"};
+        const uint64_t bytes = (uint64_t)st.st_size;
+        if (bytes % 12 != 0)
+            throw Error{CGB_EIO, std::string("edge file size is not a whole number of 12-byte records: ") + path};
+        const std::vector<uint32_t> rec = load_array(path, bytes / 4);
+        *out = graph_from_edges(rec.data(), bytes / 12, V, device);
+    });
+}
+
 cgb_status cgb_graph_destroy(cgb_graph* g)
 {
     return guarded([&] { graph_free(g); });

@@ -221,6 +221,11 @@ void free_mssp(cgb_graph* g);
 // Device memory from the engine's pool, allocated in the order of stream s
 // (and complete on return); released with the graph (graph_free).
 void* pool_alloc(size_t bytes, cudaStream_t s);
+// Releases pool memory in the order of stream s.
+void pool_free(void* p, cudaStream_t s);
+// A graph from an edge list of packed (source, destination, weight) u32
+// records in host or device memory (cgb_graph_create_from_edges).
+cgb_graph* graph_from_edges(const uint32_t* records, uint64_t E, uint32_t V, int device);
 void* pinned_small_alloc(size_t bytes);
 // Pinned host memory for small transfers, from a process-wide pool.
 void* pinned_acquire(size_t bytes);

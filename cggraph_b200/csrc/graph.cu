@@ -74,6 +74,8 @@ static void dfree(void* p, cudaStream_t s)
     cudaFreeAsync(p, s);
 }
 
+void pool_free(void* p, cudaStream_t s) { dfree(p, s); }
+
 void* pool_alloc(size_t bytes, cudaStream_t s)
 {
     void* p = dalloc<char>(bytes, s);

@@ -239,6 +239,26 @@ class Graph:
         return cls(h.value)
 
     @classmethod
+    def from_edges(cls, records, vertexNum: int, device: int = 0) -> "Graph":
+        """Graph from an edge list: packed uint32 (source, destination, weight)
+        records, shape (E, 3) or flat, host or device memory
+        (cgb_graph_create_from_edges)."""
+        records = _u32(records)
+        n = records.size // 3 if isinstance(records, np.ndarray) else records.numel() // 3
+        h = ctypes.c_void_p()
+        check(L.lib().cgb_graph_create_from_edges(_ptr(records) if n else None, n, vertexNum, device,
+                                                  ctypes.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def load_edge_file(cls, path: str, vertexNum: int, device: int = 0) -> "Graph":
+        """Graph from the reference's binary edge-list file: 12-byte records
+        (source, destination, weight) (cgb_graph_load_edge_file)."""
+        h = ctypes.c_void_p()
+        check(L.lib().cgb_graph_load_edge_file(path.encode(), vertexNum, device, ctypes.byref(h)))
+        return cls(h.value)
+
+    @classmethod
     def rmat(cls, scale: int, edge_factor: int = 16, seed: int = 1, a: float = 0.57, b: float = 0.19,
              c: float = 0.19, scramble: bool = True, symmetrise: bool = False, wmax: int = 64,
              device: int = 0) -> "Graph":

@@ -145,6 +145,21 @@ cgb_status cgb_graph_create(const uint32_t* offsets, const uint32_t* dest, const
 cgb_status cgb_graph_load_files(const char* offsets_path, const char* dest_path, const char* weight_path,
                                 uint32_t V, uint32_t E, int device, cgb_graph** out);
 
+/* Builds the graph from an edge list: num_edges packed records of three
+ * uint32 {source, destination, weight} (host or device memory), in any
+ * order. The CSR is built on the device: lists grouped by source and sorted
+ * by destination, weights following. CGB_EFORMAT for a self-loop, an id >= V
+ * or a duplicate edge, as the reference's reader asserts. Replaces
+ * GraphBinReader::group_load_directedGraph + sort_nbr + getStruct_csrResult
+ * (Basic/Graph/graphBinReader.hpp:89-208,213-227,286-322). */
+cgb_status cgb_graph_create_from_edges(const uint32_t* records, uint64_t num_edges, uint32_t V, int device,
+                                       cgb_graph** out);
+
+/* The same from a binary edge-list file (the reference's has_csrFile = 0
+ * input, main_partition.hpp:105-116): the edge count is the file size / 12,
+ * and a size that is not a whole number of records is CGB_EIO. */
+cgb_status cgb_graph_load_edge_file(const char* path, uint32_t V, int device, cgb_graph** out);
+
 cgb_status cgb_graph_destroy(cgb_graph* g);
 
 /* Runs all later work of this graph on `stream` (a cudaStream_t of the

@@ -159,6 +159,40 @@ def num_threads() -> int:
 RMAT_ABC = (0.57, 0.19, 0.19)
 
 
+class EdgeListError(ValueError):
+    """A record set the reference's edge-list reader rejects."""
+
+
+def edge_list_to_csr(records, V):
+    """CSR (offsets, dest, weight) from packed (src, dst, weight) uint32
+    records, as the reference's reader builds it: self-loops rejected
+    (Basic/Graph/graphBinReader.hpp:150), lists grouped by source
+    (:159-190), each sorted by destination (sort_nbr, :213-227) and required
+    strictly ascending (check_sortNbr, :238-254), offsets from the
+    out-degrees (build_csr, :286-322).  numpy, not the engine's method."""
+    rec = np.asarray(records, dtype=np.uint32).reshape(-1, 3)
+    src, dst, w = rec[:, 0].astype(np.int64), rec[:, 1].astype(np.int64), rec[:, 2]
+    if np.any(src == dst):
+        raise EdgeListError("self-loop")
+    if rec.size and (src.max() >= V or dst.max() >= V):
+        raise EdgeListError("id >= V")
+    order = np.lexsort((dst, src))
+    src, dst, w = src[order], dst[order], w[order]
+    if np.any((src[1:] == src[:-1]) & (dst[1:] == dst[:-1])):
+        raise EdgeListError("duplicate edge")
+    off = np.zeros(V + 1, np.int64)
+    np.add.at(off, src + 1, 1)
+    return np.cumsum(off).astype(np.uint32), dst.astype(np.uint32), w.astype(np.uint32)
+
+
+def csr_to_edge_list(off, dst, w, seed=0):
+    """Packed (src, dst, weight) records of a CSR, in a seeded random order."""
+    off = np.asarray(off, dtype=np.int64)
+    src = np.repeat(np.arange(off.size - 1, dtype=np.uint32), np.diff(off))
+    rec = np.stack([src, np.asarray(dst, np.uint32), np.asarray(w, np.uint32)], axis=1)
+    return rec[np.random.default_rng(seed).permutation(len(rec))].copy()
+
+
 def rmat_thresholds(a=0.57, b=0.19, c=0.19):
     """Quadrant thresholds in units of 2^-32 (floor), shared with the engine."""
     t1 = int(a * 2**32)

@@ -201,6 +201,40 @@ def test_weights_attached_after_create(oracle):
         assert ei.value.status == L.EINVAL
 
 
+def test_edge_list_input(oracle, tmp_path):
+    """The reference's other input format: packed (src, dst, weight) records,
+    in any order, in memory or as a .bin file.  The CSR built on the device
+    equals the oracle's restatement of the reference's reader; self-loops,
+    ids >= V and duplicates are CGB_EFORMAT, a ragged file CGB_EIO."""
+    off, dst, w = oracle.rmat_graph(13, 16, seed=9)
+    V = off.size - 1
+    rec = oracle.csr_to_edge_list(off, dst, w, seed=4)
+    o2, d2, w2 = oracle.edge_list_to_csr(rec, V)
+    path = tmp_path / "edges.bin"
+    rec.tofile(path)
+    for make in (lambda: cg.Graph.from_edges(rec, V), lambda: cg.Graph.load_edge_file(str(path), V)):
+        with make() as g:
+            o3, d3, w3 = g.download()
+            np.testing.assert_array_equal(o3, o2)
+            np.testing.assert_array_equal(d3, d2)
+            np.testing.assert_array_equal(w3, w2)
+            r = int(np.diff(off.astype(np.int64)).argmax())
+            np.testing.assert_array_equal(g.run(SSSP, r)[0], oracle.sssp(off, dst, w, r))
+    with cg.Graph.from_edges(np.zeros((0, 3), np.uint32), 7) as g:
+        assert g.run(BFS, 3)[0].tolist() == [VMAX, VMAX, VMAX, 0, VMAX, VMAX, VMAX]
+    for bad in ([[5, 5, 1]], [[0, V, 1]], [[1, 2, 3], [1, 2, 4]]):
+        with pytest.raises(CgbError) as ei:
+            cg.Graph.from_edges(np.array(bad, np.uint32), V)
+        assert ei.value.status == L.EFORMAT
+    ragged = tmp_path / "ragged.bin"
+    rec.tofile(ragged)
+    with open(ragged, "ab") as f:
+        f.write(b"\0" * 4)
+    with pytest.raises(CgbError) as ei:
+        cg.Graph.load_edge_file(str(ragged), V)
+    assert ei.value.status == L.EIO
+
+
 def test_zero_out_degree_tail(oracle):
     """noZeroOutDegreeNum < V (the reordered layout whose last vertices have no
     out-edges, main_partition.hpp:78-103)."""

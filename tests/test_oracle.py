@@ -110,3 +110,18 @@ def test_chunglu_twin_properties(oracle):
     assert w.min() >= 1 and w.max() <= 64
     offs, dsts, _ = oracle.chunglu_graph(V, n, i0, seed=7, symmetrise=True)
     assert dsts.size >= dst.size
+
+
+def test_edge_list_oracle_round_trip(oracle):
+    """The edge-list reader restatement: a CSR turned into shuffled records
+    comes back unchanged; self-loops, ids >= V and duplicates are rejected."""
+    off, dst, w = oracle.rmat_graph(10, 8, seed=3)
+    rec = oracle.csr_to_edge_list(off, dst, w, seed=1)
+    o2, d2, w2 = oracle.edge_list_to_csr(rec, off.size - 1)
+    np.testing.assert_array_equal(o2, off)
+    np.testing.assert_array_equal(d2, dst)
+    np.testing.assert_array_equal(w2, w)
+    V = off.size - 1
+    for bad in ([[5, 5, 1]], [[0, V, 1]], [[1, 2, 3], [1, 2, 4]]):
+        with pytest.raises(oracle.EdgeListError):
+            oracle.edge_list_to_csr(np.array(bad, np.uint32), V)
