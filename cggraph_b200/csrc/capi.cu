@@ -164,6 +164,19 @@ cgb_status cgb_graph_load_edge_file(const char* path, uint32_t V, int device, cg
     });
 }
 
+cgb_status cgb_graph_reorder(cgb_graph* g, int order_method, uint32_t* old2new, uint32_t* no_zero_out_degree_num,
+                             cgb_graph** out)
+{
+    return guarded([&] {
+        CGB_REQUIRE(out != nullptr, CGB_EINVAL, "out is NULL");
+        *out = nullptr;
+        CGB_REQUIRE(g != nullptr, CGB_EINVAL, "graph is NULL");
+        std::lock_guard<GraphMutex> lock(g->mu);
+        CGB_CUDA_TRY(cudaSetDevice(g->device));
+        *out = graph_reorder(g, order_method, old2new, no_zero_out_degree_num);
+    });
+}
+
 cgb_status cgb_graph_destroy(cgb_graph* g)
 {
     return guarded([&] { graph_free(g); });

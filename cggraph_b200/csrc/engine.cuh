@@ -226,6 +226,8 @@ void pool_free(void* p, cudaStream_t s);
 // A graph from an edge list of packed (source, destination, weight) u32
 // records in host or device memory (cgb_graph_create_from_edges).
 cgb_graph* graph_from_edges(const uint32_t* records, uint64_t E, uint32_t V, int device);
+// Relabelled copy of g in a degree order (cgb_graph_reorder).
+cgb_graph* graph_reorder(cgb_graph* g, int method, uint32_t* old2new_out, uint32_t* nz_out);
 void* pinned_small_alloc(size_t bytes);
 // Pinned host memory for small transfers, from a process-wide pool.
 void* pinned_acquire(size_t bytes);

@@ -1438,6 +1438,118 @@ void graph_free(cgb_graph* g)
     delete g;
 }
 
+// ------------------------------------------------------------------ reorder
+// Relabelled copies of a graph, the deterministic orders of the reference's
+// Reorder (my_project/CGgraph/Reorder.hpp): vertices sorted by degree,
+// largest first, ties by ascending id (sortDegree, :251-292).  IN_DEGREE_DEC
+// sorts by in-degree (:211-240); NORMAL_OUTDEGREE_DEC by out-degree, which
+// puts the vertices without out-edges last and gives noZeroOutDegreeNum
+// (main_partition.hpp:78-104 reads it for that order).  new id = rank in the
+// order, old2new[v] = new id of v.  The new CSR lists every row's
+// neighbours by new id, weights following.
+
+__global__ void k_degree_desc_key(uint32_t V, const uint32_t* __restrict__ off, uint32_t* key, uint32_t* id)
+{
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+        key[v] = ~(off[v + 1] - off[v]);  // ascending key = descending degree
+        id[v] = v;
+    }
+}
+
+__global__ void k_reorder_rows(uint32_t V, const uint32_t* __restrict__ order, const uint32_t* __restrict__ off,
+                               uint32_t* old2new, uint32_t* new_deg, uint32_t* nonzero)
+{
+    uint32_t nz = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < V; i += gridDim.x * blockDim.x) {
+        const uint32_t u = order[i];
+        old2new[u] = i;
+        const uint32_t d = off[u + 1] - off[u];
+        new_deg[i] = d;
+        nz += d ? 1u : 0u;
+    }
+    nz = warp_sum(nz);
+    if (lane_id() == 0 && nz) atomicAdd(nonzero, nz);
+}
+
+// Row r of the relabelled graph is the old row order[r]: its entries with
+// their ids mapped, weights alongside.
+struct ReorderRowsF {
+    static constexpr uint32_t kBatch = 8;
+    __device__ __forceinline__ bool stop() const { return false; }
+    __device__ __forceinline__ void tile_end() {}
+    const uint32_t* __restrict__ order;
+    const uint32_t* __restrict__ off;
+    const uint32_t* __restrict__ dst;
+    const uint32_t* __restrict__ w;
+    const uint32_t* __restrict__ old2new;
+    uint32_t* __restrict__ new_dst;
+    uint32_t* __restrict__ new_w;
+    struct Val {
+        uint32_t d, wt;
+    };
+    __device__ __forceinline__ Val load(uint32_t p, uint32_t r, uint32_t beg, uint32_t) const
+    {
+        const uint32_t e = __ldg(off + __ldg(order + r)) + (p - beg);
+        return Val{__ldg(old2new + __ldg(dst + e)), w ? __ldg(w + e) : 0u};
+    }
+    __device__ __forceinline__ void store(uint32_t p, uint32_t, uint32_t, uint32_t, Val x)
+    {
+        new_dst[p] = x.d;
+        if (new_w) new_w[p] = x.wt;
+    }
+};
+
+cgb_graph* graph_reorder(cgb_graph* g, int method, uint32_t* old2new_out, uint32_t* nz_out)
+{
+    CGB_REQUIRE(method == CGB_ORDER_IN_DEGREE_DEC || method == CGB_ORDER_NORMAL_OUTDEGREE_DEC, CGB_EUNSUPPORTED,
+                "order method: IN_DEGREE_DEC (21) and NORMAL_OUTDEGREE_DEC (12) are built");
+    const uint32_t V = g->V, E = g->E;
+    const bool by_in = method == CGB_ORDER_IN_DEGREE_DEC;
+    if (by_in) ensure_csc(g);
+    const uint32_t* deg_off = by_in ? g->in_off : g->off;
+    cudaStream_t s = g->stream;
+    uint32_t* key = dalloc<uint32_t>(V, s);
+    uint32_t* key2 = dalloc<uint32_t>(V, s);
+    uint32_t* id = dalloc<uint32_t>(V, s);
+    uint32_t* order = dalloc<uint32_t>(V, s);
+    uint32_t* old2new = dalloc<uint32_t>(V, s);
+    uint32_t* new_deg = dalloc<uint32_t>((size_t)V + 1, s);
+    uint32_t* nonzero = dalloc<uint32_t>(1, s);
+    k_degree_desc_key<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, s>>>(V, deg_off, key, id);
+    stable_sort_u32(g, key, key2, id, order, V, 32);
+    CGB_CUDA_TRY(cudaMemsetAsync(nonzero, 0, 4, s));
+    CGB_CUDA_TRY(cudaMemsetAsync(new_deg + V, 0, 4, s));
+    k_reorder_rows<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, s>>>(V, order, g->off, old2new, new_deg, nonzero);
+    PinnedArray<uint32_t> hn(1);
+    CGB_CUDA_TRY(cudaMemcpyAsync(hn.data(), nonzero, 4, cudaMemcpyDeviceToHost, s));
+    CGB_CUDA_TRY(cudaStreamSynchronize(s));
+    // out-degree order: every vertex with out-edges comes before every one without
+    const uint32_t nz = by_in ? V : hn[0];
+    cgb_graph* r = nullptr;
+    try {
+        r = graph_alloc(V, E, nz, g->device, g->w != nullptr && E > 0);
+        exclusive_sum_u32(g, new_deg, r->off, (uint64_t)V + 1);
+        CGB_CUDA_TRY(cudaStreamSynchronize(s));
+        launch_edges_by_row(g, V, E, r->off, ReorderRowsF{order, g->off, g->dst, g->w, old2new, r->dst, r->w});
+        if (old2new_out)
+            CGB_CUDA_TRY(cudaMemcpyAsync(old2new_out, old2new, (size_t)V * 4, cudaMemcpyDefault, s));
+        CGB_CUDA_TRY(cudaStreamSynchronize(s));
+        validate_and_sort(r);  // lists sorted by new id, weights following
+        compute_weight_sum(r);
+    } catch (...) {
+        cudaStreamSynchronize(s);
+        for (void* p : {(void*)key, (void*)key2, (void*)id, (void*)order, (void*)old2new, (void*)new_deg, (void*)nonzero})
+            dfree(p, s);
+        if (r) graph_free(r);
+        throw;
+    }
+    for (void* p : {(void*)key, (void*)key2, (void*)id, (void*)order, (void*)old2new, (void*)new_deg, (void*)nonzero})
+        dfree(p, s);
+    CGB_CUDA_TRY(cudaStreamSynchronize(s));
+    if (nz_out) *nz_out = nz;
+    return r;
+}
+
 }  // namespace cgb
 
 void GraphMutex::lock()

@@ -308,6 +308,16 @@ class Graph:
         weight = _u32(weight)
         check(L.lib().cgb_graph_set_weights(self._h, _ptr(weight)))
 
+    def reorder(self, order_method: int):
+        """Relabelled copy in a degree order (cgb_graph_reorder):
+        (graph, old2new uint32[V], noZeroOutDegreeNum)."""
+        old2new = np.empty(self.vertexNum, np.uint32)
+        nz = ctypes.c_uint32()
+        h = ctypes.c_void_p()
+        check(L.lib().cgb_graph_reorder(self._h, int(order_method), _ptr(old2new), ctypes.byref(nz),
+                                        ctypes.byref(h)))
+        return Graph(h.value), old2new, nz.value
+
     def download(self, with_weight: bool = True):
         off = np.empty(self.vertexNum + 1, np.uint32)
         dst = np.empty(max(1, self.edgeNum), np.uint32)

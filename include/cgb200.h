@@ -160,6 +160,24 @@ cgb_status cgb_graph_create_from_edges(const uint32_t* records, uint64_t num_edg
  * and a size that is not a whole number of records is CGB_EIO. */
 cgb_status cgb_graph_load_edge_file(const char* path, uint32_t V, int device, cgb_graph** out);
 
+/* OrderMethod values (Basic/Graph/basic_struct.hpp:41-76) that cgb_graph_reorder builds. */
+#define CGB_ORDER_NATIVE 0
+#define CGB_ORDER_NORMAL_OUTDEGREE_DEC 12
+#define CGB_ORDER_IN_DEGREE_DEC 21
+
+/* A relabelled copy of g (on g's device): vertices sorted by degree,
+ * largest first, ties by ascending id, as the reference's Reorder sorts them
+ * (my_project/CGgraph/Reorder.hpp:251-292). CGB_ORDER_IN_DEGREE_DEC sorts by
+ * in-degree (Reorder.hpp:211-240); CGB_ORDER_NORMAL_OUTDEGREE_DEC by
+ * out-degree, so the vertices without out-edges come last and the new
+ * graph's noZeroOutDegreeNum is their start. old2new (V entries, host or
+ * device memory, may be NULL) receives the new id of every vertex, for
+ * rootTranfer and checkBinResult; *no_zero_out_degree_num (may be NULL) the
+ * new graph's noZeroOutDegreeNum. Other order methods (the BFS-based
+ * MY_BFS_*, RCM, GORDER) are CGB_EUNSUPPORTED. */
+cgb_status cgb_graph_reorder(cgb_graph* g, int order_method, uint32_t* old2new,
+                             uint32_t* no_zero_out_degree_num, cgb_graph** out);
+
 cgb_status cgb_graph_destroy(cgb_graph* g);
 
 /* Runs all later work of this graph on `stream` (a cudaStream_t of the

@@ -193,6 +193,32 @@ def csr_to_edge_list(off, dst, w, seed=0):
     return rec[np.random.default_rng(seed).permutation(len(rec))].copy()
 
 
+def reorder(off, dst, w, method):
+    """Relabelled CSR of the deterministic degree orders of the reference's
+    Reorder: vertices by degree, largest first, ties by ascending id
+    (my_project/CGgraph/Reorder.hpp:251-292); method 21 = IN_DEGREE_DEC (in-
+    degree, :211-240), 12 = NORMAL_OUTDEGREE_DEC (out-degree: the vertices
+    without out-edges last, noZeroOutDegreeNum before them).  Rows list their
+    neighbours by new id, weights following.  Returns (off, dst, w, old2new,
+    noZeroOutDegreeNum).  numpy, not the engine's method."""
+    off = np.asarray(off, dtype=np.int64)
+    dst = np.asarray(dst, dtype=np.int64)
+    V = off.size - 1
+    outdeg = np.diff(off)
+    deg = np.bincount(dst, minlength=V) if method == 21 else outdeg
+    order = np.lexsort((np.arange(V), -deg))
+    old2new = np.empty(V, np.int64)
+    old2new[order] = np.arange(V)
+    src = np.repeat(np.arange(V), outdeg)
+    ns, nd = old2new[src], old2new[dst]
+    k = np.lexsort((nd, ns))
+    noff = np.zeros(V + 1, np.int64)
+    np.add.at(noff, ns + 1, 1)
+    nw = None if w is None else np.asarray(w, np.uint32)[k]
+    nz = V if method == 21 else int(np.count_nonzero(outdeg))
+    return (np.cumsum(noff).astype(np.uint32), nd[k].astype(np.uint32), nw, old2new.astype(np.uint32), nz)
+
+
 def rmat_thresholds(a=0.57, b=0.19, c=0.19):
     """Quadrant thresholds in units of 2^-32 (floor), shared with the engine."""
     t1 = int(a * 2**32)

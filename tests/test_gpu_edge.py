@@ -235,6 +235,38 @@ def test_edge_list_input(oracle, tmp_path):
     assert ei.value.status == L.EIO
 
 
+def test_reorder_degree_orders(oracle):
+    """cgb_graph_reorder: IN_DEGREE_DEC and NORMAL_OUTDEGREE_DEC relabel the
+    graph exactly as the oracle's restatement of the reference's Reorder
+    (CSR, old2new, noZeroOutDegreeNum); BFS, SSSP and CC on the relabelled
+    graph from old2new[root] give the original results under old2new
+    (rootTranfer), CC matches the oracle on the relabelled graph, and other
+    order methods are CGB_EUNSUPPORTED."""
+    off, dst, w = oracle.rmat_graph(13, 16, seed=14)
+    deg = np.diff(off.astype(np.int64))
+    r = int(deg.argmax())
+    exp = {BFS: oracle.bfs(off, dst, r), SSSP: oracle.sssp(off, dst, w, r)}
+    with cg.Graph.from_csr(off, dst, w) as g:
+        for method in (cg.OrderMethod.NORMAL_OUTDEGREE_DEC, cg.OrderMethod.IN_DEGREE_DEC):
+            o2, d2, w2, m2, nz2 = oracle.reorder(off, dst, w, int(method))
+            h, old2new, nz = g.reorder(method)
+            with h:
+                np.testing.assert_array_equal(old2new, m2)
+                assert nz == nz2
+                o3, d3, w3 = h.download()
+                np.testing.assert_array_equal(o3, o2)
+                np.testing.assert_array_equal(d3, d2)
+                np.testing.assert_array_equal(w3, w2)
+                for alg in (BFS, SSSP):
+                    np.testing.assert_array_equal(h.run(alg, int(old2new[r]))[0][old2new], exp[alg])
+                # CC labels are minimum ids (on this directed graph, of the vertices that
+                # reach each one), so they depend on the ids: parity on the relabelled graph
+                np.testing.assert_array_equal(h.run(CC)[0], oracle.cc(o2, d2))
+        with pytest.raises(CgbError) as ei:
+            g.reorder(cg.OrderMethod.MY_BFS_OUT)
+        assert ei.value.status == L.EUNSUPPORTED
+
+
 def test_zero_out_degree_tail(oracle):
     """noZeroOutDegreeNum < V (the reordered layout whose last vertices have no
     out-edges, main_partition.hpp:78-103)."""

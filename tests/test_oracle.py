@@ -125,3 +125,24 @@ def test_edge_list_oracle_round_trip(oracle):
     for bad in ([[5, 5, 1]], [[0, V, 1]], [[1, 2, 3], [1, 2, 4]]):
         with pytest.raises(oracle.EdgeListError):
             oracle.edge_list_to_csr(np.array(bad, np.uint32), V)
+
+
+def test_reorder_oracle_properties(oracle):
+    """The degree orders: a permutation, degrees non-increasing along the new
+    ids, vertices without out-edges last for NORMAL_OUTDEGREE_DEC, and the
+    relabelled graph is the old one with its ids mapped."""
+    off, dst, w = oracle.rmat_graph(10, 8, seed=6)
+    V = off.size - 1
+    for method in (12, 21):
+        o2, d2, w2, old2new, nz = oracle.reorder(off, dst, w, method)
+        assert sorted(old2new.tolist()) == list(range(V))
+        deg = np.bincount(dst, minlength=V) if method == 21 else np.diff(off.astype(np.int64))
+        new_deg = np.empty(V, np.int64)
+        new_deg[old2new] = deg
+        assert np.all(np.diff(new_deg) <= 0)
+        if method == 12:
+            assert nz == np.count_nonzero(deg) and np.all(np.diff(o2.astype(np.int64))[nz:] == 0)
+        src = np.repeat(np.arange(V), np.diff(off.astype(np.int64)))
+        old = sorted(zip(old2new[src].tolist(), old2new[dst].tolist(), w.tolist()))
+        s2 = np.repeat(np.arange(V), np.diff(o2.astype(np.int64)))
+        assert old == sorted(zip(s2.tolist(), d2.tolist(), w2.tolist()))
