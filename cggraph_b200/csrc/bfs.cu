@@ -164,14 +164,20 @@ __global__ void __launch_bounds__(kBlock) k_bfs_bu(uint32_t V, const uint32_t* _
     }
 }
 
+__global__ void k_level_reset(DevCounters* ctr, int out)
+{
+    ctr->qlen[out] = 0;
+    ctr->chunk_len = 0;
+    ctr->medges = 0;
+    ctr->found = 0;
+    ctr->max_deg = 0;
+}
+
+// qlen[out], chunk_len, medges, found, max_deg: one launch, not five memsets
 static void reset_level_counters(cgb_graph* g, int out)
 {
-    // qlen[out], chunk_len, medges, found, max_deg
-    CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->qlen[out], 0, sizeof(uint32_t), g->stream));
-    CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->chunk_len, 0, sizeof(uint32_t), g->stream));
-    CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->medges, 0, sizeof(unsigned long long), g->stream));
-    CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->found, 0, sizeof(uint32_t), g->stream));
-    CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->max_deg, 0, sizeof(uint32_t), g->stream));
+    ++g->stats.launches;
+    k_level_reset<<<1, 1, 0, g->stream>>>(g->ctr, out);
 }
 
 void run_bfs(cgb_graph* g, uint32_t root, const cgb_options& o)

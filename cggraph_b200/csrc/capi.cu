@@ -377,14 +377,18 @@ cgb_status cgb_run_batch(cgb_graph* g, int algorithm, const uint32_t* roots, uin
         uint32_t* d_roots = nullptr;
         uint32_t* tmp = nullptr;
         try {
-            CGB_CUDA_TRY(cudaMalloc((void**)&d_roots, (size_t)per * 4));
-            if (!dev_out) CGB_CUDA_TRY(cudaMalloc((void**)&tmp, (size_t)std::min(per, nroots) * V * 4));
+            // pool memory, ordered on the graph's stream (cudaMalloc / cudaFree of the
+            // result staging, up to 64 x V words, cost a device-wide synchronisation)
+            d_roots = static_cast<uint32_t*>(pool_alloc((size_t)per * 4, g->stream));
+            if (!dev_out) tmp = static_cast<uint32_t*>(pool_alloc((size_t)std::min(per, nroots) * V * 4, g->stream));
+            PinnedArray<uint32_t> h_roots(per);
             double total = 0;
             uint64_t edges = 0, iters = 0, launches = 0;
             for (uint32_t s0 = 0; s0 < nroots; s0 += per) {
                 const uint32_t n = std::min(per, nroots - s0);
                 uint32_t* lv = dev_out ? out_u32 + (size_t)s0 * V : tmp;
-                CGB_CUDA_TRY(cudaMemcpyAsync(d_roots, roots + s0, (size_t)n * 4, cudaMemcpyHostToDevice, g->stream));
+                std::copy(roots + s0, roots + s0 + n, h_roots.data());
+                h2d_small(d_roots, h_roots.data(), (size_t)n * 4, g->stream);
                 g->stats.launches = 0;
                 CGB_CUDA_TRY(cudaEventRecord(g->ev_start, g->stream));
                 if (algorithm == CGB_BFS) run_msbfs(g, d_roots, n, lv, o.bfs_alpha > 0 ? o.bfs_alpha : kMsAlpha);
@@ -412,12 +416,13 @@ cgb_status cgb_run_batch(cgb_graph* g, int algorithm, const uint32_t* roots, uin
             g->stats.alg_bytes = (algorithm == CGB_BFS ? 8 : (g->w ? 12 : 8)) * edges + 12ull * V * nroots;
             if (out_ms) *out_ms = total;
         } catch (...) {
-            if (d_roots) cudaFree(d_roots);
-            if (tmp) cudaFree(tmp);
+            cudaStreamSynchronize(g->stream);
+            pool_free(d_roots, g->stream);
+            pool_free(tmp, g->stream);
             throw;
         }
-        cudaFree(d_roots);
-        if (tmp) cudaFree(tmp);
+        pool_free(d_roots, g->stream);
+        pool_free(tmp, g->stream);
     });
 }
 

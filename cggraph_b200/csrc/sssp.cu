@@ -177,6 +177,29 @@ __global__ void __launch_bounds__(kBlock) k_sssp_dense_scan(uint32_t V, const ui
     }
 }
 
+// Counters of the next round (and, for a push round, the near-dedup bitmap)
+// reset by one launch instead of one memset each: rounds are short, and a
+// run has dozens of them.
+__global__ void k_sssp_round_reset(DevCounters* ctr, int out, uint32_t* bm, uint32_t words)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ctr->qlen[out] = 0;
+        ctr->chunk_len = 0;
+        ctr->medges = 0;
+    }
+    if (bm)
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < words; i += gridDim.x * blockDim.x) bm[i] = 0;
+}
+
+// The same before a bucket split: next queue, far count, smallest far distance.
+__global__ void k_sssp_split_reset(DevCounters* ctr, int out)
+{
+    ctr->qlen[out] = 0;
+    ctr->far_len[0] = 0;
+    ctr->min_far = 0xFFFFFFFFu;
+    ctr->medges = 0;
+}
+
 __global__ void k_sssp_init(uint32_t V, uint32_t* dist, uint32_t* far_bm, uint32_t words)
 {
     const uint32_t stride = gridDim.x * blockDim.x;
@@ -311,10 +334,9 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
                 ensure_csc(g);
                 ensure_csc_weights(g);
             }
-            CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->qlen[out], 0, sizeof(uint32_t), g->stream));
-            CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->chunk_len, 0, sizeof(uint32_t), g->stream));
-            CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->medges, 0, 8, g->stream));
-            if (!pull && !dense) CGB_CUDA_TRY(cudaMemsetAsync(near_bm, 0, (size_t)words * sizeof(uint32_t), g->stream));
+            ++g->stats.launches;
+            k_sssp_round_reset<<<(!pull && !dense) ? kNumSMs * 2 : 1, kBlock, 0, g->stream>>>(
+                g->ctr, out, (!pull && !dense) ? near_bm : nullptr, words);
             if (tracing) CGB_CUDA_TRY(cudaEventRecord(g->ev_iter[0], g->stream));
             if (timing) ktimer_begin(g, pull ? CGB_K_PULL : CGB_K_PUSH);
             if (pull) {
@@ -376,10 +398,8 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
         for (;;) {
             CGB_REQUIRE(iters < max_iters, CGB_ETIMEOUT, "SSSP iteration budget exhausted");
             const int out = cur ^ 1;
-            CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->qlen[out], 0, sizeof(uint32_t), g->stream));
-            CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->far_len[0], 0, sizeof(uint32_t), g->stream));
-            CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->min_far, 0xff, sizeof(uint32_t), g->stream));
-            CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->medges, 0, 8, g->stream));
+            ++g->stats.launches;
+            k_sssp_split_reset<<<1, 1, 0, g->stream>>>(g->ctr, out);
             if (timing) ktimer_begin(g, CGB_K_FRONTIER);
             ++g->stats.launches;
             k_sssp_split<<<grid_for(words, kBlock, kNumSMs * 4), kBlock, 0, g->stream>>>(
