@@ -52,6 +52,17 @@ public:
         check(cgb_graph_create(csr.csr_offset, csr.csr_dest, csr.csr_weight, csr.vertexNum, csr.edgeNum,
                                csr.noZeroOutDegreeNum, device, &g_));
     }
+    // The reference's other input (has_csrFile = 0, main_partition.hpp:105-116):
+    // a binary edge list of 12-byte (src, dst, weight) records, built into the
+    // CSR on the device (cgb_graph_load_edge_file).
+    GraphB200(const std::string& edge_file, uint32_t vertices, int algorithm, int device = 0,
+              const cgb_options* opt = nullptr)
+        : algorithm_(algorithm), opt_(opt ? *opt : cgb_options{})
+    {
+        check(cgb_graph_load_edge_file(edge_file.c_str(), vertices, device, &g_));
+        check(cgb_graph_info(g_, &vertexNum, &edgeNum, nullptr));
+        noZeroOutDegreeNum = vertexNum;
+    }
     GraphB200(const GraphB200&) = delete;
     GraphB200& operator=(const GraphB200&) = delete;
     ~GraphB200() { cgb_graph_destroy(g_); }
@@ -76,6 +87,9 @@ public:
             check(cgb_graph_result_download(g_, vertexValue.data()));
         }
     }
+
+    // Attaches or replaces the edge weights (cgb_graph_set_weights).
+    void setWeights(const uint32_t* weight) { check(cgb_graph_set_weights(g_, weight)); }
 
     cgb_graph* handle() const { return g_; }
 

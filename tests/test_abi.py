@@ -70,7 +70,8 @@ def test_load_files_size_check(lib, tmp_path):
 def test_cpp_adapter_compiles_and_reports_status(tmp_path, lib):
     """include/cgb200.hpp (the GraphDeviceWorklist-shaped adapter) compiles
     against a CSR_Result_type-like struct and links; without a GPU the
-    constructor throws cgb200::error with CGB_ECUDA, with one it runs BFS."""
+    constructors throw cgb200::error with CGB_ECUDA, with one they run SSSP
+    (from the CSR, and from an edge-list file given its weights later)."""
     import subprocess
     src = tmp_path / "adapter.cpp"
     src.write_text(r'''
@@ -89,15 +90,29 @@ int main() {
     } catch (const cgb200::error& e) {
         std::printf("status %d\n", (int)e.status);
     }
+    try {
+        cgb200::GraphB200<CSR_Result_type> g(std::string(EDGE_FILE), 3, CGB_SSSP);
+        uint32_t w2[2] = {5, 7};
+        g.setWeights(w2);
+        g.graphProcess_device(CGB_SSSP, 0);
+        g.result_D2H();
+        std::printf("%u %u %u\n", g.vertexValue[0], g.vertexValue[1], g.vertexValue[2]);
+    } catch (const cgb200::error& e) {
+        std::printf("status %d\n", (int)e.status);
+    }
     return 0;
 }
 ''')
+    edges = tmp_path / "edges.bin"
+    import struct
+    edges.write_bytes(struct.pack("<6I", 1, 2, 1, 0, 1, 1))  # (src, dst, w) records; weights replaced later
     exe = tmp_path / "adapter"
     libdir = os.path.join(ROOT, "cggraph_b200")
-    subprocess.check_call(["g++", "-std=c++17", "-O1", str(src), "-I", os.path.join(ROOT, "include"), "-L", libdir,
+    subprocess.check_call(["g++", "-std=c++17", "-O1", f'-DEDGE_FILE="{edges}"', str(src), "-I",
+                           os.path.join(ROOT, "include"), "-L", libdir,
                            "-lcgb200", f"-Wl,-rpath,{libdir}", "-o", str(exe)])
     out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120).stdout.strip()
-    assert out in ("0 5 12", "status 5"), out
+    assert out in ("0 5 12\n0 5 12", "status 5\nstatus 5"), out
 
 
 def test_struct_layouts_match_header(tmp_path):
