@@ -188,12 +188,9 @@ static void cl_affine(uint32_t V, uint64_t seed, uint64_t tag, uint64_t& a, uint
     b = mix64(seed ^ (tag + 1)) % V;
 }
 
-static void* galloc(size_t bytes)
-{
-    void* p = nullptr;
-    CGB_CUDA_TRY(cudaMalloc(&p, bytes ? bytes : 1));
-    return p;
-}
+// Scratch from the engine's pool, ordered on the generator's stream (a
+// cudaFree would synchronise the whole device).
+static void* galloc(size_t bytes, cudaStream_t st) { return pool_alloc(bytes ? bytes : 1, st); }
 
 cgb_graph* gen_rmat(uint32_t scale, uint32_t ef, uint64_t seed, double a, double b, double c, int scr, int sym,
                     uint32_t wmax, int device)
@@ -212,9 +209,9 @@ cgb_graph* gen_rmat(uint32_t scale, uint32_t ef, uint64_t seed, double a, double
     const uint64_t cc = mix64(seed ^ 0x5C0A13ull);
     cudaStream_t st;
     CGB_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-    uint64_t* keys = (uint64_t*)galloc(total * 8);
-    uint64_t* alt = (uint64_t*)galloc(total * 8);
-    uint64_t* cnt = (uint64_t*)galloc(8);
+    uint64_t* keys = (uint64_t*)galloc(total * 8, st);
+    uint64_t* alt = (uint64_t*)galloc(total * 8, st);
+    uint64_t* cnt = (uint64_t*)galloc(8, st);
     void* temp = nullptr;
     cgb_graph* g = nullptr;
     try {
@@ -224,18 +221,19 @@ cgb_graph* gen_rmat(uint32_t scale, uint32_t ef, uint64_t seed, double a, double
         CGB_CUDA_TRY(cub::DeviceRadixSort::SortKeys(nullptr, tb, db, total, 0, 32 + (int)scale, st));
         uint64_t* in_unique = nullptr;
         CGB_CUDA_TRY(cub::DeviceSelect::Unique(nullptr, tb2, keys, alt, cnt, total, st));
-        temp = galloc(std::max(tb, tb2));
+        temp = galloc(std::max(tb, tb2), st);
         CGB_CUDA_TRY(cub::DeviceRadixSort::SortKeys(temp, tb, db, total, 0, 32 + (int)scale, st));
         in_unique = db.Current();
         uint64_t* out_unique = db.Alternate();
         CGB_CUDA_TRY(cub::DeviceSelect::Unique(temp, tb2, in_unique, out_unique, cnt, total, st));
-        uint64_t m = 0, last = 0;
-        CGB_CUDA_TRY(cudaMemcpyAsync(&m, cnt, 8, cudaMemcpyDeviceToHost, st));
+        PinnedArray<uint64_t> hm(2);  // pinned: see pinned_acquire
+        CGB_CUDA_TRY(cudaMemcpyAsync(hm.data(), cnt, 8, cudaMemcpyDeviceToHost, st));
         CGB_CUDA_TRY(cudaStreamSynchronize(st));
+        uint64_t m = hm[0];
         if (m) {
-            CGB_CUDA_TRY(cudaMemcpyAsync(&last, out_unique + m - 1, 8, cudaMemcpyDeviceToHost, st));
+            CGB_CUDA_TRY(cudaMemcpyAsync(hm.data() + 1, out_unique + m - 1, 8, cudaMemcpyDeviceToHost, st));
             CGB_CUDA_TRY(cudaStreamSynchronize(st));
-            if (last == kSentinel) m--;
+            if (hm[1] == kSentinel) m--;
         }
         CGB_REQUIRE(m < 0xFFFFFFFFull, CGB_EUNSUPPORTED, "RMAT graph has >= 2^32 edges");
         g = graph_alloc(V, (uint32_t)m, V, device, wmax > 0);
@@ -246,18 +244,20 @@ cgb_graph* gen_rmat(uint32_t scale, uint32_t ef, uint64_t seed, double a, double
         CGB_CUDA_TRY(cudaStreamSynchronize(st));
         if (sym) g->symmetric = 1;
     } catch (...) {
-        cudaFree(keys);
-        cudaFree(alt);
-        cudaFree(cnt);
-        if (temp) cudaFree(temp);
-        cudaStreamDestroy(st);
+        pool_free(keys, st);
+        pool_free(alt, st);
+        pool_free(cnt, st);
+        if (temp) pool_free(temp, st);
+        cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
         if (g) graph_free(g);
         throw;
     }
-    cudaFree(keys);
-    cudaFree(alt);
-    cudaFree(cnt);
-    cudaFree(temp);
+    pool_free(keys, st);
+    pool_free(alt, st);
+    pool_free(cnt, st);
+    pool_free(temp, st);
+    cudaStreamSynchronize(st);
     cudaStreamDestroy(st);
     compute_weight_sum(g);
     return g;
@@ -283,41 +283,42 @@ cgb_graph* gen_chunglu(uint32_t V, uint64_t draws, uint32_t i0, uint64_t seed, i
     cgb_graph* g = nullptr;
     try {
         // exact integer prefix sums of the weights (cum[V] = total weight)
-        cum = (uint64_t*)galloc(((size_t)V + 1) * 8);
-        uint64_t* wts = (uint64_t*)galloc(((size_t)V + 1) * 8);
+        cum = (uint64_t*)galloc(((size_t)V + 1) * 8, st);
+        uint64_t* wts = (uint64_t*)galloc(((size_t)V + 1) * 8, st);
         k_cl_weights<<<kNumSMs * 8, kBlock, 0, st>>>(V, i0, wts);
         CGB_CUDA_TRY(cudaMemsetAsync(wts + V, 0, 8, st));
         size_t tb = 0;
         CGB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb, wts, cum, (uint64_t)V + 1, st));
-        void* stemp = galloc(tb);
+        void* stemp = galloc(tb, st);
         CGB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(stemp, tb, wts, cum, (uint64_t)V + 1, st));
         CGB_CUDA_TRY(cudaStreamSynchronize(st));
-        cudaFree(stemp);
-        cudaFree(wts);
-        keys = (uint64_t*)galloc(total * 8);
+        pool_free(stemp, st);
+        pool_free(wts, st);
+        keys = (uint64_t*)galloc(total * 8, st);
         k_cl_keys<<<kNumSMs * 16, kBlock, 0, st>>>(V, draws, cum, (double)i0, mix64(seed ^ 0xC1A0001ull),
                                                    mix64(seed ^ 0xC1A0002ull), a_out, b_out, a_in, b_in, sym, keys);
         CGB_CUDA_TRY(cudaStreamSynchronize(st));
-        cudaFree(cum);
+        pool_free(cum, st);
         cum = nullptr;
-        alt = (uint64_t*)galloc(total * 8);
-        cnt = (uint64_t*)galloc(8);
+        alt = (uint64_t*)galloc(total * 8, st);
+        cnt = (uint64_t*)galloc(8, st);
         cub::DoubleBuffer<uint64_t> db(keys, alt);
         size_t tb1 = 0, tb2 = 0;
         CGB_CUDA_TRY(cub::DeviceRadixSort::SortKeys(nullptr, tb1, db, total, 0, 32 + (int)bits, st));
         CGB_CUDA_TRY(cub::DeviceSelect::Unique(nullptr, tb2, keys, alt, cnt, total, st));
-        temp = galloc(std::max(tb1, tb2));
+        temp = galloc(std::max(tb1, tb2), st);
         CGB_CUDA_TRY(cub::DeviceRadixSort::SortKeys(temp, tb1, db, total, 0, 32 + (int)bits, st));
         uint64_t* in_unique = db.Current();
         uint64_t* out_unique = db.Alternate();
         CGB_CUDA_TRY(cub::DeviceSelect::Unique(temp, tb2, in_unique, out_unique, cnt, total, st));
-        uint64_t m = 0, last = 0;
-        CGB_CUDA_TRY(cudaMemcpyAsync(&m, cnt, 8, cudaMemcpyDeviceToHost, st));
+        PinnedArray<uint64_t> hm(2);  // pinned: see pinned_acquire
+        CGB_CUDA_TRY(cudaMemcpyAsync(hm.data(), cnt, 8, cudaMemcpyDeviceToHost, st));
         CGB_CUDA_TRY(cudaStreamSynchronize(st));
+        uint64_t m = hm[0];
         if (m) {
-            CGB_CUDA_TRY(cudaMemcpyAsync(&last, out_unique + m - 1, 8, cudaMemcpyDeviceToHost, st));
+            CGB_CUDA_TRY(cudaMemcpyAsync(hm.data() + 1, out_unique + m - 1, 8, cudaMemcpyDeviceToHost, st));
             CGB_CUDA_TRY(cudaStreamSynchronize(st));
-            if (last == kSentinel) m--;
+            if (hm[1] == kSentinel) m--;
         }
         CGB_REQUIRE(m < 0xFFFFFFFFull, CGB_EUNSUPPORTED, "Chung-Lu graph has >= 2^32 edges");
         g = graph_alloc(V, (uint32_t)m, V, device, wmax > 0);
@@ -328,19 +329,21 @@ cgb_graph* gen_chunglu(uint32_t V, uint64_t draws, uint32_t i0, uint64_t seed, i
         CGB_CUDA_TRY(cudaStreamSynchronize(st));
         if (sym) g->symmetric = 1;
     } catch (...) {
-        if (cum) cudaFree(cum);
-        if (keys) cudaFree(keys);
-        if (alt) cudaFree(alt);
-        if (cnt) cudaFree(cnt);
-        if (temp) cudaFree(temp);
-        cudaStreamDestroy(st);
+        if (cum) pool_free(cum, st);
+        if (keys) pool_free(keys, st);
+        if (alt) pool_free(alt, st);
+        if (cnt) pool_free(cnt, st);
+        if (temp) pool_free(temp, st);
+        cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
         if (g) graph_free(g);
         throw;
     }
-    cudaFree(keys);
-    cudaFree(alt);
-    cudaFree(cnt);
-    cudaFree(temp);
+    pool_free(keys, st);
+    pool_free(alt, st);
+    pool_free(cnt, st);
+    pool_free(temp, st);
+    cudaStreamSynchronize(st);
     cudaStreamDestroy(st);
     compute_weight_sum(g);
     return g;
@@ -358,12 +361,12 @@ cgb_graph* gen_grid(uint32_t rows, uint32_t cols, uint64_t seed, uint32_t wmax, 
     uint32_t* deg = nullptr;
     void* temp = nullptr;
     try {
-        deg = (uint32_t*)galloc(((size_t)V + 1) * 4);
+        deg = (uint32_t*)galloc(((size_t)V + 1) * 4, g->stream);
         k_grid_deg<<<kNumSMs * 8, kBlock, 0, g->stream>>>(rows, cols, deg);
         CGB_CUDA_TRY(cudaMemsetAsync(deg + V, 0, 4, g->stream));
         size_t tb = 0;
         CGB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb, deg, g->off, (uint64_t)V + 1, g->stream));
-        temp = galloc(tb);
+        temp = galloc(tb, g->stream);
         CGB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(temp, tb, deg, g->off, (uint64_t)V + 1, g->stream));
         k_grid_fill<<<kNumSMs * 8, kBlock, 0, g->stream>>>(rows, cols, g->off, g->dst);
         if (wmax)
@@ -371,13 +374,13 @@ cgb_graph* gen_grid(uint32_t rows, uint32_t cols, uint64_t seed, uint32_t wmax, 
                                                                    1, g->w);
         CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
     } catch (...) {
-        if (deg) cudaFree(deg);
-        if (temp) cudaFree(temp);
+        if (deg) pool_free(deg, g->stream);
+        if (temp) pool_free(temp, g->stream);
         graph_free(g);
         throw;
     }
-    cudaFree(deg);
-    cudaFree(temp);
+    pool_free(deg, g->stream);
+    pool_free(temp, g->stream);
     g->symmetric = 1;
     compute_weight_sum(g);
     return g;
