@@ -1499,10 +1499,411 @@ struct ReorderRowsF {
     }
 };
 
+// ---------------------------------------------------------- BFS-based orders
+// The reference's MY_BFS_* orders (Reorder.hpp:294-535) run one queue BFS
+// after another on the CPU: start vertices in start-list order (degree
+// descending, ties by id), each popped vertex queueing its unvisited
+// neighbours by child degree, largest first, the vertices without out-edges
+// set aside in the order they are met.  The same sequence follows from three
+// data-parallel facts.
+//  1. The vertices with out-edges split into BFS trees: v belongs to the tree
+//     of the lowest start-list rank r that reaches v (a vertex reaching v is
+//     either a root or reached by a lower-ranked one), at depth
+//     dist(root, v).  label = (r << 32 | depth) is the lexicographic minimum
+//     over every vertex reaching v, the fixpoint of
+//     label[v] = min(label[v], label[u] + 1) over edges u -> v from
+//     label[v] = rank[v] << 32: one frontier round per depth.
+//  2. The queue holds the trees by rank, each level by level, and a level in
+//     the order of (queue index of the first parent that lists the vertex,
+//     child degree descending, list index).  So level d+1 is built from
+//     level d in queue order: every child is claimed by its lowest-index
+//     parent, parents emit their claimed children in list order, and a
+//     stable radix sort on (parent index, ~degree) orders them.  Level
+//     indices order the vertices of one tree and level as queue positions
+//     do, and across trees by tree rank.
+//  3. Concatenated, the levels are in (depth, level index) order; a stable
+//     sort on the tree rank turns that into the queue sequence.
+// The vertices without out-edges follow in the order the reference appends
+// them: at the first visit of a parent that lists them (by visit position,
+// then list index), or, when no parent is visited before their own turn in
+// the start list, at that turn, which falls after every tree of a lower
+// rank.  Equal child degrees keep list order; the reference's std::sort
+// does the same for lists of at most 16 entries and may permute ties in
+// longer ones.
+
+constexpr uint64_t kNoLabel = ~0ull;  // vertices without out-edges
+
+__global__ void k_in_degree(uint32_t E, const uint32_t* __restrict__ dst, uint32_t* indeg)
+{
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < E; e += stride)
+        atomicAdd(indeg + __ldg(dst + e), 1u);
+}
+
+// Ascending keys: start degree descending (ties keep id order through the
+// stable sort), child degree descending (saturated to 32 bits; only one
+// vertex can have 2^32 or more incident edges).
+__global__ void k_bfs_order_keys(uint32_t V, const uint32_t* __restrict__ off, const uint32_t* __restrict__ indeg,
+                                 int method, uint32_t* start_key, uint32_t* id, uint32_t* child_key)
+{
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += stride) {
+        const uint32_t od = off[v + 1] - off[v], in = indeg[v];
+        start_key[v] = ~(method == CGB_ORDER_MY_IMAX_BFS_IN ? in : od);
+        id[v] = (uint32_t)v;
+        const uint64_t cd = method == CGB_ORDER_MY_BFS_OUT      ? (uint64_t)od
+                            : method == CGB_ORDER_MY_BFS_OUT_IN ? (uint64_t)od + in
+                                                                : (uint64_t)in;
+        child_key[v] = ~(uint32_t)(cd < 0xffffffffull ? cd : 0xffffffffull);
+    }
+}
+
+// label and rank from the start list; the vertices with out-edges form the
+// first frontier.  ctr[0] counts it, ctr[1] is the (unreachable) overflow.
+__global__ void k_bfs_order_init(uint32_t V, const uint32_t* __restrict__ off, const uint32_t* __restrict__ start_list,
+                                 uint64_t* label, uint32_t* rank, uint32_t* front, uint32_t* ctr)
+{
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i0 = blockIdx.x * (uint64_t)blockDim.x; i0 < V; i0 += stride) {  // warp-uniform trip count
+        const uint64_t i = i0 + threadIdx.x;
+        bool nz = false;
+        uint32_t v = 0;
+        if (i < V) {
+            v = start_list[i];
+            nz = off[v + 1] > off[v];
+            label[v] = nz ? (i << 32) : kNoLabel;
+            rank[v] = (uint32_t)i;
+        }
+        warp_append(nz, v, front, ctr, V, ctr + 1);
+    }
+}
+
+// One round of label[v] = min(label[v], label[u] + 1), a warp per frontier
+// vertex u.  A vertex lowered in this round joins the next frontier once
+// (stamp).  A stale read of label[u] only delays: u was lowered in this
+// round, so it is in the next frontier too.
+__global__ void k_bfs_order_relax(const uint32_t* __restrict__ off, const uint32_t* __restrict__ dst, uint64_t* label,
+                                  const uint32_t* __restrict__ front, uint32_t nfront, uint32_t* next, uint32_t* ctr,
+                                  uint32_t* stamp, uint32_t round, uint32_t cap)
+{
+    const uint32_t lane = lane_id();
+    const uint64_t warps = (uint64_t)gridDim.x * blockDim.x / 32;
+    for (uint64_t w = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / 32; w < nfront; w += warps) {
+        const uint32_t u = front[w];
+        const uint64_t cand = label[u] + 1;
+        const uint64_t end = off[u + 1];
+        for (uint64_t e0 = off[u]; e0 < end; e0 += 32) {
+            bool push = false;
+            uint32_t v = 0;
+            if (e0 + lane < end) {
+                v = __ldg(dst + e0 + lane);
+                const uint64_t cur = label[v];
+                if (cur != kNoLabel && cand < cur) {
+                    const uint64_t old = atomicMin((unsigned long long*)(label + v), (unsigned long long)cand);
+                    push = cand < old && atomicExch(stamp + v, round) != round;
+                }
+            }
+            warp_append(push, v, next, ctr, cap, ctr + 1);
+        }
+    }
+}
+
+// The roots (label == rank << 32) in rank order: flags for a compaction.
+__global__ void k_bfs_order_root_flags(uint32_t V, const uint32_t* __restrict__ start_list,
+                                       const uint64_t* __restrict__ label, uint32_t* flag)
+{
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < V; i += stride)
+        flag[i] = label[start_list[i]] == (i << 32) ? 1u : 0u;
+    if (blockIdx.x == 0 && threadIdx.x == 0) flag[V] = 0;
+}
+
+__global__ void k_scatter_flagged(uint32_t n, const uint32_t* __restrict__ flag, const uint32_t* __restrict__ idx,
+                                  const uint32_t* __restrict__ item, uint32_t* out)
+{
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += stride)
+        if (flag[i]) out[idx[i]] = item[i];
+}
+
+// Level d+1 from level d (P[0, n) in queue order), a warp per parent.  A
+// child v of parent u has label[v] == label[u] + 1: the same tree, one level
+// down.  claim: the lowest parent index wins; count: children per parent;
+// emit: each parent's children in list order at start[i], with the sort key
+// (parent index << 32 | ~child degree).
+enum class LevelPass { kClaim, kCount, kEmit };
+
+template <LevelPass kPass>
+__global__ void k_bfs_order_level(const uint32_t* __restrict__ off, const uint32_t* __restrict__ dst,
+                                  const uint64_t* __restrict__ label, const uint32_t* __restrict__ P, uint32_t n,
+                                  uint32_t* par, uint32_t* cnt, const uint32_t* __restrict__ start,
+                                  const uint32_t* __restrict__ child_key, uint32_t* C, uint64_t* K)
+{
+    const uint32_t lane = lane_id();
+    const uint64_t warps = (uint64_t)gridDim.x * blockDim.x / 32;
+    for (uint64_t w = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / 32; w < n; w += warps) {
+        const uint32_t i = (uint32_t)w;
+        const uint32_t u = P[i];
+        const uint64_t t = label[u] + 1;
+        const uint64_t end = off[u + 1];
+        uint32_t c = 0;
+        const uint32_t base = kPass == LevelPass::kEmit ? start[i] : 0u;
+        for (uint64_t e0 = off[u]; e0 < end; e0 += 32) {
+            bool mine = false;
+            uint32_t v = 0;
+            if (e0 + lane < end) {
+                v = __ldg(dst + e0 + lane);
+                if (label[v] == t) {
+                    if (kPass == LevelPass::kClaim) {
+                        if (par[v] > i) atomicMin(par + v, i);
+                    } else {
+                        mine = par[v] == i;
+                    }
+                }
+            }
+            if (kPass == LevelPass::kCount) {
+                c += mine ? 1u : 0u;
+            } else if (kPass == LevelPass::kEmit) {
+                const uint32_t b = __ballot_sync(0xffffffffu, mine);
+                if (mine) {
+                    const uint32_t at = base + c + __popc(b & lanemask_lt());
+                    C[at] = v;
+                    K[at] = ((uint64_t)i << 32) | child_key[v];
+                }
+                c += __popc(b);
+            }
+        }
+        if (kPass == LevelPass::kCount) {
+            c = warp_sum(c);
+            if (lane == 0) cnt[i] = c;
+        }
+    }
+}
+
+__global__ void k_bfs_order_tree_key(uint32_t n, const uint32_t* __restrict__ lv, const uint64_t* __restrict__ label,
+                                     uint32_t* key)
+{
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < n; j += stride)
+        key[j] = (uint32_t)(label[lv[j]] >> 32);
+}
+
+// Vertices without out-edges: zp = lowest queue position of a parent that
+// lists them (first pass), zj = their index in that parent's list (second).
+template <bool kIndex>
+__global__ void k_bfs_order_zero_parent(const uint32_t* __restrict__ off, const uint32_t* __restrict__ dst,
+                                        const uint64_t* __restrict__ label, const uint32_t* __restrict__ order,
+                                        uint32_t n, uint32_t* zp, uint32_t* zj)
+{
+    const uint32_t lane = lane_id();
+    const uint64_t warps = (uint64_t)gridDim.x * blockDim.x / 32;
+    for (uint64_t w = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / 32; w < n; w += warps) {
+        const uint32_t i = (uint32_t)w;
+        const uint32_t u = order[i];
+        const uint64_t beg = off[u], end = off[u + 1];
+        for (uint64_t e = beg + lane; e < end; e += 32) {
+            const uint32_t z = __ldg(dst + e);
+            if (label[z] != kNoLabel) continue;
+            if (kIndex) {
+                if (zp[z] == i) zj[z] = (uint32_t)(e - beg);
+            } else if (zp[z] > i) {
+                atomicMin(zp + z, i);
+            }
+        }
+    }
+}
+
+__global__ void k_bfs_order_zero_list(uint32_t V, const uint64_t* __restrict__ label, uint32_t* zl, uint32_t* ctr)
+{
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t v0 = blockIdx.x * (uint64_t)blockDim.x; v0 < V; v0 += stride) {
+        const uint64_t v = v0 + threadIdx.x;
+        warp_append(v < V && label[v] == kNoLabel, (uint32_t)v, zl, ctr, V, ctr + 1);
+    }
+}
+
+// Sort keys of the vertices without out-edges, met at (visit position zp,
+// list index zj) or at their own start-list turn k, which comes after the
+// P(k) queue positions of the trees ranked below k: hi = 2 zp + 1, lo = zj,
+// or hi = 2 P(k), lo = k.
+__global__ void k_bfs_order_zero_keys(uint32_t Z, const uint32_t* __restrict__ zl, const uint32_t* __restrict__ zp,
+                                      const uint32_t* __restrict__ zj, const uint32_t* __restrict__ rank,
+                                      const uint32_t* __restrict__ tree_sorted, uint32_t n, uint32_t* lo, uint64_t* hi)
+{
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < Z; i += stride) {
+        const uint32_t z = zl[i], k = rank[z];
+        uint32_t a = 0, b = n;  // first tree_sorted entry >= k
+        while (a < b) {
+            const uint32_t m = a + (b - a) / 2;
+            if (tree_sorted[m] < k) a = m + 1;
+            else b = m;
+        }
+        if (zp[z] < a) {
+            hi[i] = 2ull * zp[z] + 1;
+            lo[i] = zj[z];
+        } else {
+            hi[i] = 2ull * a;
+            lo[i] = k;
+        }
+    }
+}
+
+static void sort_pairs_u64(cgb_graph* g, const uint64_t* kin, uint64_t* kout, const uint32_t* vin, uint32_t* vout,
+                           uint64_t n, int bits)
+{
+    size_t tb = 0;
+    CGB_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tb, kin, kout, vin, vout, n, 0, bits, g->stream));
+    void* temp = dalloc<char>(tb, g->stream);
+    cudaError_t err = cub::DeviceRadixSort::SortPairs(temp, tb, kin, kout, vin, vout, n, 0, bits, g->stream);
+    CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    dfree(temp, g->stream);
+    CGB_CUDA_TRY(err);
+}
+
+// Pool allocations on the graph's stream, returned when the scope ends.
+struct ScopedPool {
+    cudaStream_t s;
+    std::vector<void*> held;
+    explicit ScopedPool(cudaStream_t st) : s(st) {}
+    template <typename T>
+    T* get(size_t n)
+    {
+        T* p = dalloc<T>(n ? n : 1, s);
+        held.push_back(p);
+        return p;
+    }
+    ~ScopedPool()
+    {
+        cudaStreamSynchronize(s);
+        for (void* p : held) dfree(p, s);
+    }
+};
+
+static uint32_t read_u32(cgb_graph* g, const uint32_t* d)
+{
+    PinnedArray<uint32_t> h(1);
+    CGB_CUDA_TRY(cudaMemcpyAsync(h.data(), d, 4, cudaMemcpyDeviceToHost, g->stream));
+    CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    return h[0];
+}
+
+// order[i] = old id of new vertex i; returns the number of vertices with
+// out-edges (they come first).
+static uint32_t bfs_vertex_order(cgb_graph* g, int method, uint32_t* order)
+{
+    const uint32_t V = g->V, E = g->E;
+    cudaStream_t s = g->stream;
+    ScopedPool pool(s);
+    const uint32_t gv = grid_for(V, kBlock, kNumSMs * 8);
+    const uint32_t gw = kNumSMs * 16;  // warp-per-vertex kernels
+    uint32_t* indeg = pool.get<uint32_t>(V);
+    uint32_t* skey = pool.get<uint32_t>(V);
+    uint32_t* skey2 = pool.get<uint32_t>(V);
+    uint32_t* ids = pool.get<uint32_t>(V);
+    uint32_t* start_list = pool.get<uint32_t>(V);
+    uint32_t* child_key = pool.get<uint32_t>(V);
+    uint32_t* rank = pool.get<uint32_t>(V);
+    uint64_t* label = pool.get<uint64_t>(V);
+    uint32_t* fa = pool.get<uint32_t>(V);
+    uint32_t* fb = pool.get<uint32_t>(V);
+    uint32_t* stamp = pool.get<uint32_t>(V);
+    uint32_t* par = pool.get<uint32_t>(V);
+    uint32_t* ctr = pool.get<uint32_t>(2);
+    uint32_t* lv = pool.get<uint32_t>(V);
+    uint32_t* flag = pool.get<uint32_t>((size_t)V + 1);
+    uint32_t* idx = pool.get<uint32_t>((size_t)V + 1);
+    uint32_t* C = pool.get<uint32_t>(V);
+    uint64_t* K = pool.get<uint64_t>(V);
+    uint64_t* K2 = pool.get<uint64_t>(V);
+    CGB_CUDA_TRY(cudaMemsetAsync(indeg, 0, (size_t)V * 4, s));
+    if (E) k_in_degree<<<grid_for(E, kBlock, kNumSMs * 8), kBlock, 0, s>>>(E, g->dst, indeg);
+    k_bfs_order_keys<<<gv, kBlock, 0, s>>>(V, g->off, indeg, method, skey, ids, child_key);
+    stable_sort_u32(g, skey, skey2, ids, start_list, V, 32);
+
+    // 1. labels (tree rank << 32 | depth)
+    CGB_CUDA_TRY(cudaMemsetAsync(ctr, 0, 8, s));
+    k_bfs_order_init<<<gv, kBlock, 0, s>>>(V, g->off, start_list, label, rank, fa, ctr);
+    uint32_t nfront = read_u32(g, ctr);
+    const uint32_t n_out = nfront;  // vertices with out-edges
+    CGB_CUDA_TRY(cudaMemsetAsync(stamp, 0, (size_t)V * 4, s));
+    for (uint32_t round = 1; nfront; round++) {
+        CGB_CUDA_TRY(cudaMemsetAsync(ctr, 0, 8, s));
+        k_bfs_order_relax<<<grid_for((uint64_t)nfront * 32, kBlock, gw), kBlock, 0, s>>>(
+            g->off, g->dst, label, fa, nfront, fb, ctr, stamp, round, V);
+        nfront = read_u32(g, ctr);
+        std::swap(fa, fb);
+    }
+
+    // 2. levels in queue order, concatenated into lv; level 0 = the roots by rank
+    k_bfs_order_root_flags<<<gv, kBlock, 0, s>>>(V, start_list, label, flag);
+    exclusive_sum_u32(g, flag, idx, (uint64_t)V + 1);
+    k_scatter_flagged<<<gv, kBlock, 0, s>>>(V, flag, idx, start_list, lv);
+    uint32_t n = read_u32(g, idx + V);
+    uint64_t done = 0;
+    uint32_t* cnt = flag;  // reused: n + 1 <= V + 1 entries
+    uint32_t* start = idx;
+    CGB_CUDA_TRY(cudaMemsetAsync(par, 0xff, (size_t)V * 4, s));
+    while (n) {
+        const uint32_t* P = lv + done;
+        const uint32_t gl = grid_for((uint64_t)n * 32, kBlock, gw);
+        k_bfs_order_level<LevelPass::kClaim><<<gl, kBlock, 0, s>>>(g->off, g->dst, label, P, n, par, nullptr,
+                                                                    nullptr, nullptr, nullptr, nullptr);
+        k_bfs_order_level<LevelPass::kCount><<<gl, kBlock, 0, s>>>(g->off, g->dst, label, P, n, par, cnt, nullptr,
+                                                                    nullptr, nullptr, nullptr);
+        CGB_CUDA_TRY(cudaMemsetAsync(cnt + n, 0, 4, s));
+        exclusive_sum_u32(g, cnt, start, (uint64_t)n + 1);
+        const uint32_t m = read_u32(g, start + n);
+        CGB_REQUIRE(done + n + m <= n_out, CGB_EOVERFLOW, "BFS order: level sizes exceed the vertices with out-edges");
+        if (m) {
+            k_bfs_order_level<LevelPass::kEmit><<<gl, kBlock, 0, s>>>(g->off, g->dst, label, P, n, par, nullptr,
+                                                                       start, child_key, C, K);
+            sort_pairs_u64(g, K, K2, C, lv + done + n, m, 32 + (int)bits_for(n));
+        }
+        done += n;
+        n = m;
+    }
+    CGB_REQUIRE(done == n_out, CGB_EOVERFLOW, "BFS order: a vertex with out-edges was not placed");
+
+    // 3. queue sequence: the levels stably sorted by tree rank
+    if (n_out) {
+        k_bfs_order_tree_key<<<gv, kBlock, 0, s>>>(n_out, lv, label, skey);
+        stable_sort_u32(g, skey, skey2, lv, order, n_out, (int)bits_for(V));
+    }
+    const uint32_t* tree_sorted = skey2;
+
+    // 4. the vertices without out-edges
+    const uint32_t Z = V - n_out;
+    if (Z) {
+        uint32_t* zp = par;
+        uint32_t* zj = stamp;
+        CGB_CUDA_TRY(cudaMemsetAsync(zp, 0xff, (size_t)V * 4, s));
+        if (n_out) {
+            const uint32_t gz = grid_for((uint64_t)n_out * 32, kBlock, gw);
+            k_bfs_order_zero_parent<false><<<gz, kBlock, 0, s>>>(g->off, g->dst, label, order, n_out, zp, zj);
+            k_bfs_order_zero_parent<true><<<gz, kBlock, 0, s>>>(g->off, g->dst, label, order, n_out, zp, zj);
+        }
+        CGB_CUDA_TRY(cudaMemsetAsync(ctr, 0, 8, s));
+        k_bfs_order_zero_list<<<gv, kBlock, 0, s>>>(V, label, fa, ctr);
+        CGB_REQUIRE(read_u32(g, ctr) == Z, CGB_EOVERFLOW, "BFS order: vertex count without out-edges");
+        // (hi, lo) pairs are distinct: sort by lo, then stably by hi
+        k_bfs_order_zero_keys<<<gv, kBlock, 0, s>>>(Z, fa, zp, zj, rank, tree_sorted, n_out, fb, K);
+        stable_sort_u32(g, fb, cnt, fa, C, Z, 32);
+        k_bfs_order_zero_keys<<<gv, kBlock, 0, s>>>(Z, C, zp, zj, rank, tree_sorted, n_out, fb, K);
+        sort_pairs_u64(g, K, K2, C, order + n_out, Z, (int)bits_for(2ull * n_out + 2));
+    }
+    CGB_CUDA_TRY(cudaStreamSynchronize(s));
+    return n_out;
+}
+
 cgb_graph* graph_reorder(cgb_graph* g, int method, uint32_t* old2new_out, uint32_t* nz_out)
 {
-    CGB_REQUIRE(method == CGB_ORDER_IN_DEGREE_DEC || method == CGB_ORDER_NORMAL_OUTDEGREE_DEC, CGB_EUNSUPPORTED,
-                "order method: IN_DEGREE_DEC (21) and NORMAL_OUTDEGREE_DEC (12) are built");
+    const bool bfs = method == CGB_ORDER_MY_BFS_OUT || method == CGB_ORDER_MY_BFS_IN ||
+                     method == CGB_ORDER_MY_BFS_OUT_IN || method == CGB_ORDER_MY_IMAX_BFS_IN;
+    CGB_REQUIRE(method == CGB_ORDER_IN_DEGREE_DEC || method == CGB_ORDER_NORMAL_OUTDEGREE_DEC || bfs,
+                CGB_EUNSUPPORTED,
+                "order method: IN_DEGREE_DEC (21), NORMAL_OUTDEGREE_DEC (12) and the BFS orders "
+                "MY_BFS_OUT (16), MY_BFS_IN (17), MY_BFS_OUT_IN (18), MY_IMAX_BFS_IN (20) are built");
     const uint32_t V = g->V, E = g->E;
     const bool by_in = method == CGB_ORDER_IN_DEGREE_DEC;
     if (by_in) ensure_csc(g);
@@ -1515,15 +1916,19 @@ cgb_graph* graph_reorder(cgb_graph* g, int method, uint32_t* old2new_out, uint32
     uint32_t* old2new = dalloc<uint32_t>(V, s);
     uint32_t* new_deg = dalloc<uint32_t>((size_t)V + 1, s);
     uint32_t* nonzero = dalloc<uint32_t>(1, s);
-    k_degree_desc_key<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, s>>>(V, deg_off, key, id);
-    stable_sort_u32(g, key, key2, id, order, V, 32);
+    if (bfs) {
+        bfs_vertex_order(g, method, order);  // vertices with out-edges first
+    } else {
+        k_degree_desc_key<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, s>>>(V, deg_off, key, id);
+        stable_sort_u32(g, key, key2, id, order, V, 32);
+    }
     CGB_CUDA_TRY(cudaMemsetAsync(nonzero, 0, 4, s));
     CGB_CUDA_TRY(cudaMemsetAsync(new_deg + V, 0, 4, s));
     k_reorder_rows<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, s>>>(V, order, g->off, old2new, new_deg, nonzero);
     PinnedArray<uint32_t> hn(1);
     CGB_CUDA_TRY(cudaMemcpyAsync(hn.data(), nonzero, 4, cudaMemcpyDeviceToHost, s));
     CGB_CUDA_TRY(cudaStreamSynchronize(s));
-    // out-degree order: every vertex with out-edges comes before every one without
+    // out-degree and BFS orders: every vertex with out-edges comes before every one without
     const uint32_t nz = by_in ? V : hn[0];
     cgb_graph* r = nullptr;
     try {

@@ -163,6 +163,10 @@ cgb_status cgb_graph_load_edge_file(const char* path, uint32_t V, int device, cg
 /* OrderMethod values (Basic/Graph/basic_struct.hpp:41-76) that cgb_graph_reorder builds. */
 #define CGB_ORDER_NATIVE 0
 #define CGB_ORDER_NORMAL_OUTDEGREE_DEC 12
+#define CGB_ORDER_MY_BFS_OUT 16
+#define CGB_ORDER_MY_BFS_IN 17
+#define CGB_ORDER_MY_BFS_OUT_IN 18
+#define CGB_ORDER_MY_IMAX_BFS_IN 20
 #define CGB_ORDER_IN_DEGREE_DEC 21
 
 /* A relabelled copy of g (on g's device): vertices sorted by degree,
@@ -173,8 +177,18 @@ cgb_status cgb_graph_load_edge_file(const char* path, uint32_t V, int device, cg
  * graph's noZeroOutDegreeNum is their start. old2new (V entries, host or
  * device memory, may be NULL) receives the new id of every vertex, for
  * rootTranfer and checkBinResult; *no_zero_out_degree_num (may be NULL) the
- * new graph's noZeroOutDegreeNum. Other order methods (the BFS-based
- * MY_BFS_*, RCM, GORDER) are CGB_EUNSUPPORTED. */
+ * new graph's noZeroOutDegreeNum.
+ * The BFS orders (Reorder.hpp:294-535) list the vertices with out-edges in
+ * the order of queue BFSs started from them by degree, largest first
+ * (out-degree; in-degree for CGB_ORDER_MY_IMAX_BFS_IN), each vertex queueing
+ * its unvisited neighbours by degree, largest first (out-degree for
+ * MY_BFS_OUT, in-degree for MY_BFS_IN and MY_IMAX_BFS_IN, their sum for
+ * MY_BFS_OUT_IN; equal degrees in list order), followed by the vertices
+ * without out-edges in the order the BFSs meet them; noZeroOutDegreeNum is
+ * their start. Other order methods (RCM, GORDER, MY_IMAX_BFS_OUT, which the
+ * reference leaves undefined) are CGB_EUNSUPPORTED. The relabelled lists are
+ * sorted by new id, as the reference's driver sorts them after loading
+ * (main_partition.hpp:146). */
 cgb_status cgb_graph_reorder(cgb_graph* g, int order_method, uint32_t* old2new,
                              uint32_t* no_zero_out_degree_num, cgb_graph** out);
 

@@ -388,3 +388,80 @@ int64_t ora_grid_csr(uint32_t rows, uint32_t cols, uint32_t* off, uint32_t* dst)
     off[(uint64_t)rows * cols] = (uint32_t)e;
     return (int64_t)e;
 }
+
+/* ------------------------------------------------------- BFS-based orders */
+/* The reference's MY_BFS_* vertex orders (my_project/CGgraph/Reorder.hpp):
+ *  - start list: all vertices by degree, largest first, ties by ascending id
+ *    (sortDegree, :251-292): out-degree for MY_BFS_OUT/IN/OUT_IN (16/17/18,
+ *    :64-67,99-103,133-137), in-degree for MY_IMAX_BFS_IN (20, :167-171);
+ *  - each start vertex not yet visited either joins the zero-out-degree list
+ *    (no out-edges) or roots a queue BFS (:304-320);
+ *  - a popped vertex sends its unvisited neighbours without out-edges to the
+ *    zero list in list order, sorts the rest by child degree, largest first
+ *    (out-degree :340-345, in-degree :421-426, in+out :503-508), and queues
+ *    those still unvisited in that order (:330-360);
+ *  - the order is the BFS visit sequence, then the zero list (:366-372).
+ * The reference sorts the children with std::sort; that is an insertion
+ * sort, hence stable, for lists of at most 16 entries, and unstable beyond.
+ * Here the sort is stable at every length: equal degrees keep list order.
+ * Returns the number of vertices with out-edges, or < 0 on error. */
+typedef struct { uint64_t deg; uint32_t pos; uint32_t v; } ora_child_t;
+
+static int cmp_child(const void* a, const void* b)
+{
+    const ora_child_t* x = (const ora_child_t*)a;
+    const ora_child_t* y = (const ora_child_t*)b;
+    if (x->deg != y->deg) return x->deg > y->deg ? -1 : 1;
+    return (x->pos > y->pos) - (x->pos < y->pos);
+}
+
+int64_t ora_bfs_order(uint32_t V, const uint32_t* off, const uint32_t* dst, int method, uint32_t* order)
+{
+    if (method != 16 && method != 17 && method != 18 && method != 20) return -1;
+    const uint32_t E = off[V];
+    uint64_t* outd = (uint64_t*)calloc((size_t)V + 1, sizeof(uint64_t));
+    uint64_t* ind = (uint64_t*)calloc((size_t)V + 1, sizeof(uint64_t));
+    ora_child_t* sv = (ora_child_t*)malloc(sizeof(ora_child_t) * ((size_t)V + 1));
+    ora_child_t* tmp = (ora_child_t*)malloc(sizeof(ora_child_t) * ((size_t)E + 1));
+    uint32_t* zero = (uint32_t*)malloc(sizeof(uint32_t) * ((size_t)V + 1));
+    unsigned char* seen = (unsigned char*)calloc((size_t)V + 1, 1);
+    if (!outd || !ind || !sv || !tmp || !zero || !seen) {
+        free(outd); free(ind); free(sv); free(tmp); free(zero); free(seen);
+        return -2;
+    }
+    for (uint32_t v = 0; v < V; v++) outd[v] = off[v + 1] - off[v];
+    for (uint32_t e = 0; e < E; e++) ind[dst[e]]++;
+    for (uint32_t v = 0; v < V; v++) {
+        sv[v].deg = method == 20 ? ind[v] : outd[v];
+        sv[v].pos = v; /* ties by ascending id */
+        sv[v].v = v;
+    }
+    qsort(sv, V, sizeof(ora_child_t), cmp_child);
+    uint64_t n = 0, nz = 0; /* order[0, n) is the BFS sequence and the queue */
+    for (uint32_t k = 0; k < V; k++) {
+        uint32_t s = sv[k].v;
+        if (seen[s]) continue;
+        seen[s] = 1;
+        if (outd[s] == 0) { zero[nz++] = s; continue; }
+        uint64_t head = n;
+        order[n++] = s;
+        while (head < n) {
+            uint32_t u = order[head++];
+            uint32_t m = 0;
+            for (uint32_t e = off[u]; e < off[u + 1]; e++) {
+                uint32_t d = dst[e];
+                if (outd[d] == 0 && !seen[d]) { seen[d] = 1; zero[nz++] = d; continue; }
+                tmp[m].deg = method == 16 ? outd[d] : method == 18 ? outd[d] + ind[d] : ind[d];
+                tmp[m].pos = m;
+                tmp[m].v = d;
+                m++;
+            }
+            qsort(tmp, m, sizeof(ora_child_t), cmp_child);
+            for (uint32_t i = 0; i < m; i++)
+                if (!seen[tmp[i].v]) { seen[tmp[i].v] = 1; order[n++] = tmp[i].v; }
+        }
+    }
+    memcpy(order + n, zero, sizeof(uint32_t) * nz);
+    free(outd); free(ind); free(sv); free(tmp); free(zero); free(seen);
+    return (int64_t)n;
+}

@@ -77,6 +77,8 @@ def lib():
                                        ctypes.c_int, _u32p]
         L.ora_grid_csr.argtypes = [ctypes.c_uint32, ctypes.c_uint32, _u32p, _u32p]
         L.ora_grid_csr.restype = ctypes.c_int64
+        L.ora_bfs_order.argtypes = [ctypes.c_uint32, _u32p, _u32p, ctypes.c_int, _u32p]
+        L.ora_bfs_order.restype = ctypes.c_int64
         for f in (L.ora_bfs, L.ora_sssp, L.ora_cc, L.ora_wcc_unionfind, L.ora_pagerank, L.ora_pagerank_pull_omp):
             f.restype = ctypes.c_int
         _lib = L
@@ -199,14 +201,19 @@ def reorder(off, dst, w, method):
     (my_project/CGgraph/Reorder.hpp:251-292); method 21 = IN_DEGREE_DEC (in-
     degree, :211-240), 12 = NORMAL_OUTDEGREE_DEC (out-degree: the vertices
     without out-edges last, noZeroOutDegreeNum before them).  Rows list their
-    neighbours by new id, weights following.  Returns (off, dst, w, old2new,
+    neighbours by new id, weights following.  The BFS-based orders
+    (BFS_ORDERS) come from ``bfs_order``.  Returns (off, dst, w, old2new,
     noZeroOutDegreeNum).  numpy, not the engine's method."""
     off = np.asarray(off, dtype=np.int64)
     dst = np.asarray(dst, dtype=np.int64)
     V = off.size - 1
     outdeg = np.diff(off)
-    deg = np.bincount(dst, minlength=V) if method == 21 else outdeg
-    order = np.lexsort((np.arange(V), -deg))
+    if method in BFS_ORDERS:
+        order, nz = bfs_order(off, dst, method)
+    else:
+        deg = np.bincount(dst, minlength=V) if method == 21 else outdeg
+        order = np.lexsort((np.arange(V), -deg))
+        nz = V if method == 21 else int(np.count_nonzero(outdeg))
     old2new = np.empty(V, np.int64)
     old2new[order] = np.arange(V)
     src = np.repeat(np.arange(V), outdeg)
@@ -215,8 +222,38 @@ def reorder(off, dst, w, method):
     noff = np.zeros(V + 1, np.int64)
     np.add.at(noff, ns + 1, 1)
     nw = None if w is None else np.asarray(w, np.uint32)[k]
-    nz = V if method == 21 else int(np.count_nonzero(outdeg))
     return (np.cumsum(noff).astype(np.uint32), nd[k].astype(np.uint32), nw, old2new.astype(np.uint32), nz)
+
+
+# MY_BFS_OUT, MY_BFS_IN, MY_BFS_OUT_IN, MY_IMAX_BFS_IN
+# (OrderMethod, Basic/Graph/basic_struct.hpp:41-76)
+BFS_ORDERS = (16, 17, 18, 20)
+
+
+def bfs_order(off, dst, method):
+    """The reference's MY_BFS_* vertex order (my_project/CGgraph/Reorder.hpp:
+    294-535) by the serial C restatement: returns (order, number of vertices
+    with out-edges); order[i] = old id of new vertex i.  Children of equal
+    degree keep their list order (the reference's std::sort does so for
+    lists of at most 16 entries)."""
+    off, dst = _u32(off), _u32(dst)
+    V = off.size - 1
+    order = np.empty(V, np.uint32)
+    nz = lib().ora_bfs_order(V, _p(off), _p(dst), int(method), _p(order))
+    if nz < 0:
+        raise ValueError(f"bfs_order: method {method} ({nz})")
+    return order, int(nz)
+
+
+def cap_lists(off, dst, w, k):
+    """The CSR keeping the first k entries of every list."""
+    off = np.asarray(off, dtype=np.int64)
+    V = off.size - 1
+    src = np.repeat(np.arange(V), np.diff(off))
+    keep = (np.arange(dst.size) - off[src]) < k
+    noff = np.zeros(V + 1, np.int64)
+    np.add.at(noff, src[keep] + 1, 1)
+    return np.cumsum(noff).astype(np.uint32), dst[keep].copy(), w[keep].copy()
 
 
 def rmat_thresholds(a=0.57, b=0.19, c=0.19):
@@ -296,6 +333,34 @@ def ref_run_files(paths, V, E, alg, roots, runs, threads=0):
             raise RuntimeError(f"cgref_oracle failed ({r.returncode}): {r.stderr[-2000:]}")
         line = [l for l in r.stdout.splitlines() if l.startswith("{")][-1]
         return json.loads(line)
+
+
+def ref_reorder(off, dst, w, method, tmpdir=None):
+    """Run the reference's Reorder (my_project/CGgraph/Reorder.hpp:58-241) in
+    its toy-graph mode on a CSR.  Returns (order, (off, dst, w)): order[i] =
+    old id of new vertex i, and the relabelled CSR the reference builds, each
+    list in the old list order with new ids (Reorder.hpp:538-620)."""
+    if not ref_available():
+        raise RuntimeError("reference oracle binary not built (oracle/build_ref.sh)")
+    off, dst = _u32(off), _u32(dst)
+    V, E = off.size - 1, dst.size
+    with tempfile.TemporaryDirectory(dir=tmpdir) as d:
+        paths = [os.path.join(d, n) for n in ("off.bin", "dst.bin", "w.bin")]
+        off.tofile(paths[0])
+        dst.tofile(paths[1])
+        if w is not None:
+            _u32(w).tofile(paths[2])
+        args = [REF_BIN, "reorder", str(int(method)), str(V), str(E), paths[0], paths[1],
+                paths[2] if w is not None else "-"]
+        r = subprocess.run(args, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"cgref_oracle reorder failed ({r.returncode}): {r.stderr[-2000:]}")
+    lines = {}
+    for l in r.stdout.splitlines():
+        for key in ("old:", "csr_offset:", "csr_dest:", "csr_weight:"):
+            if l.startswith(key):
+                lines[key] = np.array(l[len(key):].split(), dtype=np.uint64).astype(np.uint32)
+    return lines["old:"], (lines["csr_offset:"], lines["csr_dest:"], lines["csr_weight:"])
 
 
 def ref_available() -> bool:

@@ -14,6 +14,13 @@
 // the run's traversed-edge count (sum of out-degrees of reached vertices).
 // The values of the last run (uint32 per vertex, 999999999 = unreachable)
 // are written to out.bin.
+//
+// usage: cgref_oracle reorder <method> <V> <E> <offsets.bin> <dest.bin> <weight.bin|->
+//   runs the reference's Reorder::generateReorderGraphFile
+//   (my_project/CGgraph/Reorder.hpp:58-241) in its toy-graph mode, which
+//   prints the order as a line "old: <old id of new 0> <old id of new 1> ..."
+//   and writes no files; the relabelled CSR it builds (get_CSR_reorder) is
+//   then printed as "csr_offset:", "csr_dest:" and "csr_weight:" lines.
 
 #include "Basic/basic_include.cuh"
 #include "my_project/CGgraph/host_algorithm.hpp"
@@ -31,6 +38,7 @@ count_type pr_numa(G&, vertex_id_type, countl_type, countl_type, count_type, boo
 
 #include "my_project/CGgraph/sortNbr.hpp"
 #include "my_project/CGgraph/GraphNuma.cuh"
+#include "my_project/CGgraph/Reorder.hpp"
 
 #include <cstdio>
 #include <cstdlib>
@@ -38,8 +46,50 @@ count_type pr_numa(G&, vertex_id_type, countl_type, countl_type, count_type, boo
 #include <unistd.h>
 #include <vector>
 
+static void print_u32_line(const char* name, const uint32_t* a, uint64_t n)
+{
+    printf("\n%s", name);
+    for (uint64_t i = 0; i < n; i++) printf(" %u", a[i]);
+    printf("\n");
+}
+
+static int run_reorder(int argc, char** argv)
+{
+    if (argc < 8) {
+        fprintf(stderr, "usage: %s reorder method V E off dest weight\n", argv[0]);
+        return 2;
+    }
+    int method = atoi(argv[2]);
+    uint64_t V = strtoull(argv[3], nullptr, 10);
+    uint64_t E = strtoull(argv[4], nullptr, 10);
+    if (V == 0) return 2;
+    CSR_Result_type csr;
+    csr.vertexNum = (count_type)V;
+    csr.edgeNum = (countl_type)E;
+    csr.csr_offset = load_binFile<countl_type>(argv[5], V + 1);
+    csr.csr_dest = E ? load_binFile<vertex_id_type>(argv[6], E) : new vertex_id_type[1];
+    if (std::string(argv[7]) != "-" && E) {
+        csr.csr_weight = load_binFile<edge_data_type>(argv[7], E);
+    } else {
+        csr.csr_weight = new edge_data_type[E ? E : 1];
+        for (uint64_t i = 0; i < E; i++) csr.csr_weight[i] = 1;
+    }
+    std::vector<offset_type> outDeg(V), inDeg(V, 0);
+    for (uint64_t v = 0; v < V; v++) outDeg[v] = csr.csr_offset[v + 1] - csr.csr_offset[v];
+    for (uint64_t e = 0; e < E; e++) inDeg[csr.csr_dest[e]]++;
+    Reorder reorder(csr, outDeg.data(), inDeg.data());
+    reorder.generateReorderGraphFile((OrderMethod)method, "harness", true);
+    CSR_Result_type r = reorder.get_CSR_reorder();
+    print_u32_line("csr_offset:", r.csr_offset, V + 1);
+    print_u32_line("csr_dest:", r.csr_dest, E);
+    print_u32_line("csr_weight:", r.csr_weight, E);
+    fflush(stdout);
+    _exit(0);
+}
+
 int main(int argc, char** argv)
 {
+    if (argc > 1 && std::string(argv[1]) == "reorder") return run_reorder(argc, argv);
     if (argc < 9) {
         fprintf(stderr, "usage: %s alg V E off dest weight root out [runs] [threads]\n", argv[0]);
         return 2;

@@ -8,7 +8,14 @@ it: BFS and SSSP from a few roots, CC.  The toy graphs are the reference's own
 fixtures (Basic/Graph/graphFileList.hpp:514-568); the others are seeded
 synthetic graphs built by the oracle's generator twin.
 
-usage: python tests/golden/make_golden.py [reference root]
+The fixtures under reorder/ hold the vertex orders of the reference's
+Reorder (my_project/CGgraph/Reorder.hpp) for its BFS-based methods on graphs
+whose lists have at most 16 entries, where the reference's child sort is
+stable and so fully determined (order_<method>, order[i] = old id of new
+vertex i), and the relabelled CSR the reference builds for MY_BFS_OUT
+(csr_offset_16, csr_dest_16, csr_weight_16; lists in old list order).
+
+usage: python tests/golden/make_golden.py [reference root] [--reorder-only]
 """
 from __future__ import annotations
 
@@ -52,11 +59,41 @@ def graphs():
     yield "grid16x24_s3", off, dst, w, [0, 200]
 
 
+BFS_ORDER_METHODS = (16, 17, 18, 20)  # MY_BFS_OUT, MY_BFS_IN, MY_BFS_OUT_IN, MY_IMAX_BFS_IN
+
+
+def reorder_graphs():
+    for name, (off, dst, w) in TOY.items():
+        yield name, np.array(off, np.uint32), np.array(dst, np.uint32), np.array(w, np.uint32)
+    yield ("rmat10_s7_cap16",) + O.cap_lists(*O.rmat_graph(10, 16, seed=7), 16)
+    yield ("rmat11_s9_cap16",) + O.cap_lists(*O.rmat_graph(11, 4, seed=9), 16)
+    yield ("grid16x24_s3",) + O.grid_graph(16, 24, seed=3)
+
+
+def make_reorder():
+    d = os.path.join(HERE, "reorder")
+    os.makedirs(d, exist_ok=True)
+    for name, off, dst, w in reorder_graphs():
+        assert np.diff(off.astype(np.int64)).max() <= 16
+        out = {"offsets": off, "dest": dst, "weight": w}
+        for m in BFS_ORDER_METHODS:
+            order, csr = O.ref_reorder(off, dst, w, m)
+            out[f"order_{m}"] = order
+            if m == 16:
+                out["csr_offset_16"], out["csr_dest_16"], out["csr_weight_16"] = csr
+        np.savez_compressed(os.path.join(d, f"{name}.npz"), **out)
+        print("reorder", name, off.size - 1, dst.size)
+
+
 def main():
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    ref_root = args[0] if args else "/root/reference"
     O.build()
     if O.build_ref(ref_root) is None:
         raise SystemExit("reference oracle unavailable")
+    make_reorder()
+    if "--reorder-only" in sys.argv:
+        return
     for name, off, dst, w, roots in graphs():
         out = {"offsets": off, "dest": dst, "weight": w, "roots": np.array(roots, np.uint32)}
         for r in roots:

@@ -262,9 +262,58 @@ def test_reorder_degree_orders(oracle):
                 # CC labels are minimum ids (on this directed graph, of the vertices that
                 # reach each one), so they depend on the ids: parity on the relabelled graph
                 np.testing.assert_array_equal(h.run(CC)[0], oracle.cc(o2, d2))
-        with pytest.raises(CgbError) as ei:
-            g.reorder(cg.OrderMethod.MY_BFS_OUT)
-        assert ei.value.status == L.EUNSUPPORTED
+        for method in (cg.OrderMethod.RCM, cg.OrderMethod.MY_IMAX_BFS_OUT):
+            with pytest.raises(CgbError) as ei:
+                g.reorder(method)
+            assert ei.value.status == L.EUNSUPPORTED
+
+
+def bfs_order_graphs(oracle):
+    """The reference-pinned fixtures, then graphs with long lists (ties among
+    many children), many small trees, no edges, and unreached vertices."""
+    import os
+
+    from conftest import GOLDEN_DIR
+
+    d = os.path.join(GOLDEN_DIR, "reorder")
+    for f in sorted(os.listdir(d)):
+        g = np.load(os.path.join(d, f))
+        yield f[:-4], g["offsets"], g["dest"], g["weight"]
+    yield ("rmat13_s14",) + oracle.rmat_graph(13, 16, seed=14)
+    yield ("rmat12_s3_sym",) + oracle.rmat_graph(12, 8, seed=3, symmetrise=True)
+    rng = np.random.default_rng(5)
+    V = 5000
+    edges = {(int(u), int(v)) for u, v in rng.integers(0, V, (6000, 2)) if u != v}
+    off, dst, _ = csr_from_edges(V, sorted(edges))
+    yield "sparse_forest", off, dst, rng.integers(1, 64, dst.size).astype(np.uint32)
+    yield "no_edges", np.zeros(65, np.uint32), np.zeros(0, np.uint32), np.zeros(0, np.uint32)
+    yield ("grid40x50",) + oracle.grid_graph(40, 50)
+
+
+def test_reorder_bfs_orders(oracle):
+    """cgb_graph_reorder for MY_BFS_OUT, MY_BFS_IN, MY_BFS_OUT_IN and
+    MY_IMAX_BFS_IN: old2new, the relabelled CSR and noZeroOutDegreeNum equal
+    the oracle's restatement of the reference's Reorder (itself pinned to the
+    reference on the fixtures); BFS and SSSP on the relabelled graph from
+    old2new[root] give the original results under old2new."""
+    for name, off, dst, w in bfs_order_graphs(oracle):
+        V = off.size - 1
+        with cg.Graph.from_csr(off, dst, w) as g:
+            for method in oracle.BFS_ORDERS:
+                o2, d2, w2, m2, nz2 = oracle.reorder(off, dst, w, method)
+                h, old2new, nz = g.reorder(method)
+                with h:
+                    np.testing.assert_array_equal(old2new, m2, err_msg=f"{name} method {method}")
+                    assert nz == nz2, (name, method)
+                    o3, d3, w3 = h.download()
+                    np.testing.assert_array_equal(o3, o2)
+                    np.testing.assert_array_equal(d3, d2)
+                    np.testing.assert_array_equal(w3, w2)
+                    if method == 16 and dst.size:
+                        r = int(np.diff(off.astype(np.int64)).argmax())
+                        np.testing.assert_array_equal(h.run(BFS, int(old2new[r]))[0][old2new], oracle.bfs(off, dst, r))
+                        np.testing.assert_array_equal(h.run(SSSP, int(old2new[r]))[0][old2new],
+                                                      oracle.sssp(off, dst, w, r))
 
 
 def test_zero_out_degree_tail(oracle):

@@ -1,10 +1,12 @@
 """The oracle (serial C restatement) pinned against the reference's own
 engine: the toy known answers and the golden fixtures that
 tests/golden/make_golden.py produced with Graph_Numa."""
+import os
+
 import numpy as np
 import pytest
 
-from conftest import GOLDEN, load_golden
+from conftest import GOLDEN, GOLDEN_DIR, load_golden
 
 VMAX = 999999999
 
@@ -146,3 +148,82 @@ def test_reorder_oracle_properties(oracle):
         old = sorted(zip(old2new[src].tolist(), old2new[dst].tolist(), w.tolist()))
         s2 = np.repeat(np.arange(V), np.diff(o2.astype(np.int64)))
         assert old == sorted(zip(s2.tolist(), d2.tolist(), w2.tolist()))
+
+
+REORDER_DIR = os.path.join(GOLDEN_DIR, "reorder")
+REORDER_GOLDEN = sorted(f[:-4] for f in os.listdir(REORDER_DIR) if f.endswith(".npz"))
+
+
+def sort_rows(off, dst, w):
+    """Every list sorted by destination, weights following."""
+    off = off.astype(np.int64)
+    src = np.repeat(np.arange(off.size - 1), np.diff(off))
+    k = np.lexsort((dst, src))
+    return dst[k], w[k]
+
+
+@pytest.mark.parametrize("name", REORDER_GOLDEN)
+def test_bfs_order_oracle_matches_reference_golden(oracle, name):
+    """The BFS-based orders of the reference's Reorder (fixtures made by
+    tests/golden/make_golden.py with the reference itself): the oracle's order
+    is the reference's, and its relabelled CSR is the reference's with every
+    list sorted by new id."""
+    g = dict(np.load(os.path.join(REORDER_DIR, name + ".npz")))
+    off, dst, w = g["offsets"], g["dest"], g["weight"]
+    nz_ref = int(np.count_nonzero(np.diff(off.astype(np.int64))))
+    for m in oracle.BFS_ORDERS:
+        order, nz = oracle.bfs_order(off, dst, m)
+        np.testing.assert_array_equal(order, g[f"order_{m}"], err_msg=f"method {m}")
+        assert nz == nz_ref
+    o2, d2, w2, old2new, nz = oracle.reorder(off, dst, w, 16)
+    np.testing.assert_array_equal(o2, g["csr_offset_16"])
+    rd, rw = sort_rows(g["csr_offset_16"], g["csr_dest_16"], g["csr_weight_16"])
+    np.testing.assert_array_equal(d2, rd)
+    np.testing.assert_array_equal(w2, rw)
+    np.testing.assert_array_equal(old2new[g["order_16"]], np.arange(off.size - 1))
+
+
+def test_bfs_order_reference_live(oracle):
+    """The reference's Reorder itself on graphs no fixture holds: lists of at
+    most 16 entries give the same order exactly."""
+    if not oracle.ref_available():
+        pytest.skip("reference oracle binary not built (needs the reference sources)")
+    for seed in (21, 22):
+        off, dst, w = oracle.cap_lists(*oracle.rmat_graph(11, 8, seed=seed), 16)
+        for m in oracle.BFS_ORDERS:
+            ref, _ = oracle.ref_reorder(off, dst, w, m)
+            np.testing.assert_array_equal(oracle.bfs_order(off, dst, m)[0], ref)
+
+
+def test_bfs_order_oracle_properties(oracle):
+    """On lists of any length: a permutation with the vertices with out-edges
+    first; trees rooted in start-list order; every other vertex with
+    out-edges after its parent (the first-placed vertex listing it), parents
+    in queue order and each parent's children by degree, largest first."""
+    off, dst, w = oracle.rmat_graph(11, 16, seed=8)
+    V = off.size - 1
+    outdeg = np.diff(off.astype(np.int64))
+    indeg = np.bincount(dst, minlength=V)
+    src = np.repeat(np.arange(V), outdeg)
+    for m in oracle.BFS_ORDERS:
+        order, nz = oracle.bfs_order(off, dst, m)
+        assert sorted(order.tolist()) == list(range(V))
+        assert nz == np.count_nonzero(outdeg)
+        assert np.all(outdeg[order[:nz]] > 0) and np.all(outdeg[order[nz:]] == 0)
+        pos = np.empty(V, np.int64)
+        pos[order] = np.arange(V)
+        first_in = np.full(V, V, np.int64)
+        np.minimum.at(first_in, dst, pos[src])
+        v = order[:nz]
+        parent = first_in[v]
+        root = parent > np.arange(nz)
+        start_deg = indeg if m == 20 else outdeg
+        rk = np.lexsort((np.arange(V), -start_deg))
+        rank = np.empty(V, np.int64)
+        rank[rk] = np.arange(V)
+        assert np.all(np.diff(rank[v[root]]) > 0)
+        pp = parent[~root]
+        assert np.all(np.diff(pp) >= 0)
+        child_deg = {16: outdeg, 18: outdeg + indeg}.get(m, indeg)[v[~root]]
+        same = np.diff(pp) == 0
+        assert np.all(np.diff(child_deg)[same] <= 0)
