@@ -309,8 +309,10 @@ class Graph:
         check(L.lib().cgb_graph_set_weights(self._h, _ptr(weight)))
 
     def reorder(self, order_method: int):
-        """Relabelled copy in a degree order (cgb_graph_reorder):
-        (graph, old2new uint32[V], noZeroOutDegreeNum)."""
+        """Relabelled copy in one of the reference's vertex orders
+        (cgb_graph_reorder: IN_DEGREE_DEC, NORMAL_OUTDEGREE_DEC, MY_BFS_OUT,
+        MY_BFS_IN, MY_BFS_OUT_IN, MY_IMAX_BFS_IN): (graph, old2new uint32[V],
+        noZeroOutDegreeNum)."""
         old2new = np.empty(self.vertexNum, np.uint32)
         nz = ctypes.c_uint32()
         h = ctypes.c_void_p()

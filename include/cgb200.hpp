@@ -16,11 +16,13 @@
 #define CGB200_HPP
 
 #include <cstdint>
+#include <cstdio>
 #include <stdexcept>
 #include <string>
 #include <vector>
 
 #include "cgb200.h"
+#include "cgb200_gen.h"
 
 namespace cgb200 {
 
@@ -98,6 +100,88 @@ private:
     int algorithm_;
     int last_ = -1;
     cgb_options opt_;
+};
+
+// The surface of the reference's Reorder (my_project/CGgraph/Reorder.hpp:6-60,
+// 243-246, 538-620) over cgb_graph_reorder: the order and the relabelled CSR
+// are built on the device, so the degree arrays the reference's constructor
+// takes are not needed.  generateReorderGraphFile writes the five files of
+// saveCSR_reorderFile (offsets, dest, weight, old2new, addition = the number
+// of vertices without out-edges, absent for IN_DEGREE_DEC); the reference
+// derives their names from its graph folder, here they are given.  The
+// relabelled lists are sorted by new id, as the reference's driver sorts them
+// after loading (main_partition.hpp:146).
+//
+//   cgb200::ReorderB200<CSR_Result_type> reorder(csrResult);
+//   reorder.generateReorderGraphFile(CGB_ORDER_MY_BFS_OUT, off, dest, weight, old2new, addition);
+//   CSR_Result_type r = reorder.get_CSR_reorder();   // host arrays owned by `reorder`
+template <typename CsrResult>
+class ReorderB200 {
+public:
+    uint32_t vertexNum = 0;
+    uint32_t edgeNum = 0;
+    uint32_t zeroOutDegreeNum = 0;
+    std::vector<uint32_t> old2new;
+
+    explicit ReorderB200(const CsrResult& csr, int device = 0) : vertexNum(csr.vertexNum), edgeNum(csr.edgeNum)
+    {
+        check(cgb_graph_create(csr.csr_offset, csr.csr_dest, csr.csr_weight, csr.vertexNum, csr.edgeNum,
+                               csr.vertexNum, device, &g_));
+    }
+    ReorderB200(const ReorderB200&) = delete;
+    ReorderB200& operator=(const ReorderB200&) = delete;
+    ~ReorderB200() { cgb_graph_destroy(g_); }
+
+    // Builds the order and the relabelled CSR (host copies kept for
+    // get_CSR_reorder); writes the files when their names are non-empty.
+    void generateReorderGraphFile(int orderMethod, const std::string& csrOffsetFile = "",
+                                  const std::string& csrDestFile = "", const std::string& csrWeightFile = "",
+                                  const std::string& old2newFile = "", const std::string& additionFile = "")
+    {
+        cgb_graph* r = nullptr;
+        uint32_t nz = 0;
+        old2new.resize(vertexNum);
+        check(cgb_graph_reorder(g_, orderMethod, old2new.data(), &nz, &r));
+        off_.resize((size_t)vertexNum + 1);
+        dst_.resize(edgeNum ? edgeNum : 1);
+        w_.resize(edgeNum ? edgeNum : 1);
+        const cgb_status st = cgb_graph_download(r, off_.data(), dst_.data(), w_.data());
+        cgb_graph_destroy(r);
+        check(st);
+        zeroOutDegreeNum = vertexNum - nz;
+        write(csrOffsetFile, off_.data(), (size_t)vertexNum + 1);
+        write(csrDestFile, dst_.data(), edgeNum);
+        write(csrWeightFile, w_.data(), edgeNum);
+        write(old2newFile, old2new.data(), vertexNum);
+        if (orderMethod == CGB_ORDER_IN_DEGREE_DEC) write(additionFile, nullptr, 0);
+        else write(additionFile, &zeroOutDegreeNum, 1);
+    }
+
+    CsrResult get_CSR_reorder()
+    {
+        CsrResult c{};
+        c.vertexNum = vertexNum;
+        c.edgeNum = edgeNum;
+        c.csr_offset = off_.data();
+        c.csr_dest = dst_.data();
+        c.csr_weight = w_.data();
+        c.noZeroOutDegreeNum = vertexNum - zeroOutDegreeNum;
+        return c;
+    }
+
+private:
+    static void write(const std::string& path, const uint32_t* a, size_t n)
+    {
+        if (path.empty()) return;
+        FILE* f = std::fopen(path.c_str(), "wb");
+        if (!f) throw error(CGB_EIO, "cannot open " + path);
+        const size_t m = n ? std::fwrite(a, sizeof(uint32_t), n, f) : 0;
+        const bool ok = std::fclose(f) == 0 && m == n;
+        if (!ok) throw error(CGB_EIO, "cannot write " + path);
+    }
+
+    cgb_graph* g_ = nullptr;
+    std::vector<uint32_t> off_, dst_, w_;
 };
 
 }  // namespace cgb200

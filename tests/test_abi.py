@@ -67,11 +67,9 @@ def test_load_files_size_check(lib, tmp_path):
     assert st == _lib.EIO
 
 
-def test_cpp_adapter_compiles_and_reports_status(tmp_path, lib):
-    """include/cgb200.hpp (the GraphDeviceWorklist-shaped adapter) compiles
-    against a CSR_Result_type-like struct and links; without a GPU the
-    constructors throw cgb200::error with CGB_ECUDA, with one they run SSSP
-    (from the CSR, and from an edge-list file given its weights later)."""
+def run_cpp_adapter(tmp_path):
+    """Compiles a main_partition-style driver against include/cgb200.hpp and
+    returns its output."""
     import subprocess
     src = tmp_path / "adapter.cpp"
     src.write_text(r'''
@@ -87,6 +85,15 @@ int main() {
         g.graphProcess_device(CGB_SSSP, 0);
         g.result_D2H();
         std::printf("%u %u %u\n", g.vertexValue[0], g.vertexValue[1], g.vertexValue[2]);
+    } catch (const cgb200::error& e) {
+        std::printf("status %d\n", (int)e.status);
+    }
+    try {
+        cgb200::ReorderB200<CSR_Result_type> reorder(csr);
+        reorder.generateReorderGraphFile(CGB_ORDER_MY_BFS_OUT, std::string(EDGE_FILE) + ".off");
+        CSR_Result_type r = reorder.get_CSR_reorder();
+        std::printf("%u %u %u %u\n", reorder.old2new[0], reorder.old2new[2], r.noZeroOutDegreeNum,
+                    r.csr_offset[3]);
     } catch (const cgb200::error& e) {
         std::printf("status %d\n", (int)e.status);
     }
@@ -111,8 +118,28 @@ int main() {
     subprocess.check_call(["g++", "-std=c++17", "-O1", f'-DEDGE_FILE="{edges}"', str(src), "-I",
                            os.path.join(ROOT, "include"), "-L", libdir,
                            "-lcgb200", f"-Wl,-rpath,{libdir}", "-o", str(exe)])
-    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120).stdout.strip()
-    assert out in ("0 5 12\n0 5 12", "status 5\nstatus 5"), out
+    return subprocess.run([str(exe)], capture_output=True, text=True, timeout=120).stdout.strip()
+
+
+# SSSP on the path 0 -> 1 -> 2 (weights 5, 7); its MY_BFS_OUT order is 0, 1,
+# then 2 (no out-edges) last; SSSP again from the edge-list file.
+ADAPTER_GPU_OUT = "0 5 12\n0 2 2 2\n0 5 12"
+
+
+def test_cpp_adapter_compiles_and_reports_status(tmp_path, lib):
+    """include/cgb200.hpp (the GraphDeviceWorklist- and Reorder-shaped
+    adapters) compiles against a CSR_Result_type-like struct and links;
+    without a GPU the constructors throw cgb200::error with CGB_ECUDA."""
+    import torch
+    out = run_cpp_adapter(tmp_path)
+    assert out == (ADAPTER_GPU_OUT if torch.cuda.is_available() else "status 5\nstatus 5\nstatus 5"), out
+
+
+@pytest.mark.gpu
+def test_cpp_adapter_runs(tmp_path, lib):
+    """The adapters on a GPU: SSSP from the CSR and from an edge-list file
+    given its weights later, and the relabelling of the Reorder adapter."""
+    assert run_cpp_adapter(tmp_path) == ADAPTER_GPU_OUT
 
 
 def test_struct_layouts_match_header(tmp_path):
