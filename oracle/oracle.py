@@ -15,6 +15,7 @@ Only tests/, the smoke check and the benchmark's CPU-baseline leg import this.
 from __future__ import annotations
 
 import ctypes
+import signal
 import json
 import os
 import subprocess
@@ -361,6 +362,35 @@ def ref_reorder(off, dst, w, method, tmpdir=None):
             if l.startswith(key):
                 lines[key] = np.array(l[len(key):].split(), dtype=np.uint64).astype(np.uint32)
     return lines["old:"], (lines["csr_offset:"], lines["csr_dest:"], lines["csr_weight:"])
+
+
+def ref_edge_list(records, V, tmpdir=None):
+    """Run the reference's edge-list reader (GraphBinReader,
+    Basic/Graph/graphBinReader.hpp:89-325) on packed (src, dst, weight)
+    records.  Returns (off, dst, w), or None when the reader rejects the
+    input: a self-loop fails its assert_msg (exit status 1,
+    graphBinReader.hpp:160), a duplicate edge its assert on strictly
+    ascending lists (SIGABRT, :272).  Ids >= V are outside what the reader
+    checks; they are not passed."""
+    if not ref_available():
+        raise RuntimeError("reference oracle binary not built (oracle/build_ref.sh)")
+    rec = np.ascontiguousarray(records, dtype=np.uint32).reshape(-1, 3)
+    if rec.size and int(rec[:, :2].max()) >= V:
+        raise ValueError("ids >= V are not passed to the reference reader")
+    with tempfile.TemporaryDirectory(dir=tmpdir) as d:
+        path = os.path.join(d, "edges.bin")
+        rec.tofile(path)
+        r = subprocess.run([REF_BIN, "edges", str(int(V)), path], capture_output=True, text=True)
+    if r.returncode in (1, -signal.SIGABRT):
+        return None
+    if r.returncode != 0:
+        raise RuntimeError(f"cgref_oracle edges failed ({r.returncode}): {r.stderr[-2000:]}")
+    lines = {}
+    for l in r.stdout.splitlines():
+        for key in ("csr_offset:", "csr_dest:", "csr_weight:"):
+            if l.startswith(key):
+                lines[key] = np.array(l[len(key):].split(), dtype=np.uint64).astype(np.uint32)
+    return lines["csr_offset:"], lines["csr_dest:"], lines["csr_weight:"]
 
 
 def ref_available() -> bool:

@@ -21,6 +21,15 @@
 //   prints the order as a line "old: <old id of new 0> <old id of new 1> ..."
 //   and writes no files; the relabelled CSR it builds (get_CSR_reorder) is
 //   then printed as "csr_offset:", "csr_dest:" and "csr_weight:" lines.
+//
+// usage: cgref_oracle edges <V> <edges.bin>
+//   runs the reference's edge-list reader on a file of packed 12-byte
+//   (src, dst, weight) records: GraphBinReader::group_load_directedGraph,
+//   sort_nbr and getStruct_csrResult (Basic/Graph/graphBinReader.hpp:89-325,
+//   as main_partition.hpp:105-112 calls them) with one OpenMP thread, since
+//   the reader appends to per-vertex vectors from its parallel loop; prints
+//   the CSR as above.  Self-loops and duplicates end the process with the
+//   reader's own assertion (exit status 1).
 
 #include "Basic/basic_include.cuh"
 #include "my_project/CGgraph/host_algorithm.hpp"
@@ -39,6 +48,7 @@ count_type pr_numa(G&, vertex_id_type, countl_type, countl_type, count_type, boo
 #include "my_project/CGgraph/sortNbr.hpp"
 #include "my_project/CGgraph/GraphNuma.cuh"
 #include "my_project/CGgraph/Reorder.hpp"
+#include "Basic/Graph/graphBinReader.hpp"
 
 #include <cstdio>
 #include <cstdlib>
@@ -87,9 +97,31 @@ static int run_reorder(int argc, char** argv)
     _exit(0);
 }
 
+static int run_edges(int argc, char** argv)
+{
+    if (argc < 4) {
+        fprintf(stderr, "usage: %s edges V edges.bin\n", argv[0]);
+        return 2;
+    }
+    uint64_t V = strtoull(argv[2], nullptr, 10);
+    if (V == 0) return 2;
+    reSetThreadNum(1);
+    SharedMemory::GraphBinReader reader(GraphRepresentation::CSR);
+    reader.group_load_directedGraph(argv[3], (count_type)V);
+    reader.sort_nbr();
+    CSR_Result_type r;
+    reader.getStruct_csrResult(r);
+    print_u32_line("csr_offset:", r.csr_offset, V + 1);
+    print_u32_line("csr_dest:", r.csr_dest, r.edgeNum);
+    print_u32_line("csr_weight:", r.csr_weight, r.edgeNum);
+    fflush(stdout);
+    _exit(0);
+}
+
 int main(int argc, char** argv)
 {
     if (argc > 1 && std::string(argv[1]) == "reorder") return run_reorder(argc, argv);
+    if (argc > 1 && std::string(argv[1]) == "edges") return run_edges(argc, argv);
     if (argc < 9) {
         fprintf(stderr, "usage: %s alg V E off dest weight root out [runs] [threads]\n", argv[0]);
         return 2;

@@ -15,7 +15,12 @@ stable and so fully determined (order_<method>, order[i] = old id of new
 vertex i), and the relabelled CSR the reference builds for MY_BFS_OUT
 (csr_offset_16, csr_dest_16, csr_weight_16; lists in old list order).
 
-usage: python tests/golden/make_golden.py [reference root] [--reorder-only]
+The fixtures under edgelist/ hold packed (src, dst, weight) records and the
+CSR the reference's edge-list reader (Basic/Graph/graphBinReader.hpp,
+GraphBinReader) builds from them, or rejected = 1 where the reader's
+assertions stop it (a self-loop, a duplicate edge).
+
+usage: python tests/golden/make_golden.py [reference root] [--reorder-only | --edgelist-only]
 """
 from __future__ import annotations
 
@@ -85,14 +90,41 @@ def make_reorder():
         print("reorder", name, off.size - 1, dst.size)
 
 
+def edge_list_cases():
+    off, dst, w = O.rmat_graph(10, 8, seed=3)
+    yield "rmat10_s3", O.csr_to_edge_list(off, dst, w, seed=1), off.size - 1
+    off, dst, w = O.grid_graph(12, 9, seed=2)
+    yield "grid12x9_s2", O.csr_to_edge_list(off, dst, w, seed=2), off.size - 1
+    yield "toy0_records", O.csr_to_edge_list(*(np.array(a, np.uint32) for a in TOY["toy_0"]), seed=3), 12
+    yield "empty", np.zeros((0, 3), np.uint32), 5
+    yield "self_loop", np.array([[0, 1, 4], [2, 2, 1], [1, 0, 3]], np.uint32), 3
+    yield "duplicate", np.array([[0, 1, 4], [1, 2, 1], [0, 1, 3]], np.uint32), 3
+
+
+def make_edge_lists():
+    d = os.path.join(HERE, "edgelist")
+    os.makedirs(d, exist_ok=True)
+    for name, rec, V in edge_list_cases():
+        out = {"records": rec, "V": np.array([V], np.uint32)}
+        r = O.ref_edge_list(rec, V)
+        out["rejected"] = np.array([r is None], np.uint8)
+        if r is not None:
+            out["offsets"], out["dest"], out["weight"] = r
+        np.savez_compressed(os.path.join(d, f"{name}.npz"), **out)
+        print("edgelist", name, V, len(rec), "rejected" if r is None else "")
+
+
 def main():
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
     ref_root = args[0] if args else "/root/reference"
     O.build()
     if O.build_ref(ref_root) is None:
         raise SystemExit("reference oracle unavailable")
-    make_reorder()
-    if "--reorder-only" in sys.argv:
+    if "--edgelist-only" not in sys.argv:
+        make_reorder()
+    if "--reorder-only" not in sys.argv:
+        make_edge_lists()
+    if "--reorder-only" in sys.argv or "--edgelist-only" in sys.argv:
         return
     for name, off, dst, w, roots in graphs():
         out = {"offsets": off, "dest": dst, "weight": w, "roots": np.array(roots, np.uint32)}

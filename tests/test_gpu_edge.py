@@ -235,6 +235,30 @@ def test_edge_list_input(oracle, tmp_path):
     assert ei.value.status == L.EIO
 
 
+def test_edge_list_reference_fixtures():
+    """The device edge-list loader on the records of the fixtures the
+    reference's own reader (GraphBinReader) produced: the same CSR, and
+    CGB_EFORMAT where the reader's assertions stop it."""
+    import os
+
+    from conftest import GOLDEN_DIR
+
+    d = os.path.join(GOLDEN_DIR, "edgelist")
+    for f in sorted(os.listdir(d)):
+        g = dict(np.load(os.path.join(d, f)))
+        V = int(g["V"][0])
+        if g["rejected"][0]:
+            with pytest.raises(CgbError) as ei:
+                cg.Graph.from_edges(g["records"], V)
+            assert ei.value.status == L.EFORMAT, f
+            continue
+        with cg.Graph.from_edges(g["records"], V) as h:
+            o, dd, w = h.download()
+            np.testing.assert_array_equal(o, g["offsets"], err_msg=f)
+            np.testing.assert_array_equal(dd, g["dest"], err_msg=f)
+            np.testing.assert_array_equal(w, g["weight"], err_msg=f)
+
+
 def test_reorder_degree_orders(oracle):
     """cgb_graph_reorder: IN_DEGREE_DEC and NORMAL_OUTDEGREE_DEC relabel the
     graph exactly as the oracle's restatement of the reference's Reorder

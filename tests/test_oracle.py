@@ -227,3 +227,35 @@ def test_bfs_order_oracle_properties(oracle):
         child_deg = {16: outdeg, 18: outdeg + indeg}.get(m, indeg)[v[~root]]
         same = np.diff(pp) == 0
         assert np.all(np.diff(child_deg)[same] <= 0)
+
+
+EDGELIST_DIR = os.path.join(GOLDEN_DIR, "edgelist")
+EDGELIST_GOLDEN = sorted(f[:-4] for f in os.listdir(EDGELIST_DIR) if f.endswith(".npz"))
+
+
+@pytest.mark.parametrize("name", EDGELIST_GOLDEN)
+def test_edge_list_oracle_matches_reference_golden(oracle, name):
+    """The edge-list restatement against the reference's own reader
+    (fixtures made by tests/golden/make_golden.py with GraphBinReader): the
+    same CSR, and a rejection exactly where the reader's assertions stop it."""
+    g = dict(np.load(os.path.join(EDGELIST_DIR, name + ".npz")))
+    V = int(g["V"][0])
+    if g["rejected"][0]:
+        with pytest.raises(oracle.EdgeListError):
+            oracle.edge_list_to_csr(g["records"], V)
+        return
+    off, dst, w = oracle.edge_list_to_csr(g["records"], V)
+    np.testing.assert_array_equal(off, g["offsets"])
+    np.testing.assert_array_equal(dst, g["dest"])
+    np.testing.assert_array_equal(w, g["weight"])
+
+
+def test_edge_list_reference_live(oracle):
+    """The reference's reader itself on records no fixture holds."""
+    if not oracle.ref_available():
+        pytest.skip("reference oracle binary not built (needs the reference sources)")
+    off, dst, w = oracle.rmat_graph(11, 8, seed=31)
+    rec = oracle.csr_to_edge_list(off, dst, w, seed=5)
+    ref = oracle.ref_edge_list(rec, off.size - 1)
+    for a, b in zip(oracle.edge_list_to_csr(rec, off.size - 1), ref):
+        np.testing.assert_array_equal(a, b)
