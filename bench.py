@@ -142,6 +142,12 @@ def pick_roots(offsets: np.ndarray, seed: int, n: int) -> list:
     return [int(x) for x in rng.choice(cand, size=min(n, cand.size), replace=False)]
 
 
+# DRAM bytes (read + write) of one k_pr_pull launch, from one ncu capture of the
+# same bench workload (--algorithms pr), keyed by (scale, edge factor, seed);
+# profiles/pr_pull_rmat24_dram.md holds the command and the figures.
+PR_PULL_DRAM_BYTES = {(24, 16, 1): 1.16e9 + 250.26e6, (22, 16, 1): 250.19e6 + 23.33e6}
+
+
 def load_peaks() -> dict:
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -288,7 +294,10 @@ def bench_cgb200(args, d: Dist):
         achieved = bytes_per_launch / avg_s / 1e9
         roof.update({"kernel": "k_pr_pull (+ hub-row chunk kernels), one PageRank iteration",
                      "alg_bytes_per_launch": bytes_per_launch, "avg_launch_ms": pr_launch_ms / pr_launches,
-                     "achieved": achieved, "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                     "achieved": achieved, "frac": achieved / peaks["hbm_gbs"],
+                     "traffic": PR_PULL_DRAM_BYTES.get((args.scale, args.edge_factor, args.seed)),
+                     "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one k_pr_pull launch, "
+                                       "ncu capture of this workload (hub-row chunk kernels not included)",
                      "dominant_class": L.KERNEL_CLASS_NAMES[dom],
                      "class_share": {L.KERNEL_CLASS_NAMES[c]: round(kclass_ms[c] / max(1e-9, sum(kclass_ms)), 4)
                                      for c in range(8) if kclass_ms[c] > 0}})
