@@ -142,9 +142,9 @@ def pick_roots(offsets: np.ndarray, seed: int, n: int) -> list:
     return [int(x) for x in rng.choice(cand, size=min(n, cand.size), replace=False)]
 
 
-# DRAM bytes (read + write) of one k_pr_pull launch, from one ncu capture of the
-# same bench workload (--algorithms pr), keyed by (scale, edge factor, seed);
-# profiles/pr_pull_rmat24_dram.md holds the command and the figures.
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_pr_pull
+# launch, from a one-pass ncu capture of this bench with --algorithms pr on the
+# same graph, keyed by (scale, edge factor, seed).
 PR_PULL_DRAM_BYTES = {(24, 16, 1): 1.16e9 + 250.26e6, (22, 16, 1): 250.19e6 + 23.33e6}
 
 

@@ -304,6 +304,7 @@ def bfs_order_graphs(oracle):
         g = np.load(os.path.join(d, f))
         yield f[:-4], g["offsets"], g["dest"], g["weight"]
     yield ("rmat13_s14",) + oracle.rmat_graph(13, 16, seed=14)
+    yield ("rmat17_s2",) + oracle.rmat_graph(17, 16, seed=2)
     yield ("rmat12_s3_sym",) + oracle.rmat_graph(12, 8, seed=3, symmetrise=True)
     rng = np.random.default_rng(5)
     V = 5000
