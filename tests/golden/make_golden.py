@@ -9,11 +9,12 @@ fixtures (Basic/Graph/graphFileList.hpp:514-568); the others are seeded
 synthetic graphs built by the oracle's generator twin.
 
 The fixtures under reorder/ hold the vertex orders of the reference's
-Reorder (my_project/CGgraph/Reorder.hpp) for its BFS-based methods on graphs
-whose lists have at most 16 entries, where the reference's child sort is
-stable and so fully determined (order_<method>, order[i] = old id of new
-vertex i), and the relabelled CSR the reference builds for MY_BFS_OUT
-(csr_offset_16, csr_dest_16, csr_weight_16; lists in old list order).
+Reorder (my_project/CGgraph/Reorder.hpp) for its BFS-based methods and
+IN_DEGREE_DEC on graphs whose lists have at most 16 entries, where the
+reference's child sort is stable and so fully determined (order_<method>,
+order[i] = old id of new vertex i), and the relabelled CSR the reference
+builds for MY_BFS_OUT (csr_offset_16, csr_dest_16, csr_weight_16; lists in
+old list order).
 
 The fixtures under edgelist/ hold packed (src, dst, weight) records and the
 CSR the reference's edge-list reader (Basic/Graph/graphBinReader.hpp,
@@ -64,7 +65,8 @@ def graphs():
     yield "grid16x24_s3", off, dst, w, [0, 200]
 
 
-BFS_ORDER_METHODS = (16, 17, 18, 20)  # MY_BFS_OUT, MY_BFS_IN, MY_BFS_OUT_IN, MY_IMAX_BFS_IN
+# MY_BFS_OUT, MY_BFS_IN, MY_BFS_OUT_IN, MY_IMAX_BFS_IN, IN_DEGREE_DEC
+REORDER_METHODS = (16, 17, 18, 20, 21)
 
 
 def reorder_graphs():
@@ -81,7 +83,7 @@ def make_reorder():
     for name, off, dst, w in reorder_graphs():
         assert np.diff(off.astype(np.int64)).max() <= 16
         out = {"offsets": off, "dest": dst, "weight": w}
-        for m in BFS_ORDER_METHODS:
+        for m in REORDER_METHODS:
             order, csr = O.ref_reorder(off, dst, w, m)
             out[f"order_{m}"] = order
             if m == 16:

@@ -164,10 +164,10 @@ def sort_rows(off, dst, w):
 
 @pytest.mark.parametrize("name", REORDER_GOLDEN)
 def test_bfs_order_oracle_matches_reference_golden(oracle, name):
-    """The BFS-based orders of the reference's Reorder (fixtures made by
-    tests/golden/make_golden.py with the reference itself): the oracle's order
-    is the reference's, and its relabelled CSR is the reference's with every
-    list sorted by new id."""
+    """The BFS-based orders and IN_DEGREE_DEC of the reference's Reorder
+    (fixtures made by tests/golden/make_golden.py with the reference itself):
+    the oracle's order is the reference's, and its relabelled CSR is the
+    reference's with every list sorted by new id."""
     g = dict(np.load(os.path.join(REORDER_DIR, name + ".npz")))
     off, dst, w = g["offsets"], g["dest"], g["weight"]
     nz_ref = int(np.count_nonzero(np.diff(off.astype(np.int64))))
@@ -175,6 +175,8 @@ def test_bfs_order_oracle_matches_reference_golden(oracle, name):
         order, nz = oracle.bfs_order(off, dst, m)
         np.testing.assert_array_equal(order, g[f"order_{m}"], err_msg=f"method {m}")
         assert nz == nz_ref
+    _, _, _, old2new_in, _ = oracle.reorder(off, dst, w, 21)  # IN_DEGREE_DEC
+    np.testing.assert_array_equal(np.argsort(old2new_in), g["order_21"])
     o2, d2, w2, old2new, nz = oracle.reorder(off, dst, w, 16)
     np.testing.assert_array_equal(o2, g["csr_offset_16"])
     rd, rw = sort_rows(g["csr_offset_16"], g["csr_dest_16"], g["csr_weight_16"])
@@ -184,10 +186,14 @@ def test_bfs_order_oracle_matches_reference_golden(oracle, name):
 
 
 def test_bfs_order_reference_live(oracle):
-    """The reference's Reorder itself on graphs no fixture holds: lists of at
-    most 16 entries give the same order exactly."""
+    """The reference's Reorder itself on graphs no fixture holds: the same
+    IN_DEGREE_DEC order, and the same BFS orders on lists of at most 16
+    entries."""
     if not oracle.ref_available():
         pytest.skip("reference oracle binary not built (needs the reference sources)")
+    off, dst, w = oracle.rmat_graph(11, 16, seed=23)  # IN_DEGREE_DEC: a total order, any list length
+    ref, _ = oracle.ref_reorder(off, dst, w, 21)
+    np.testing.assert_array_equal(np.argsort(oracle.reorder(off, dst, w, 21)[3]), ref)
     for seed in (21, 22):
         off, dst, w = oracle.cap_lists(*oracle.rmat_graph(11, 8, seed=seed), 16)
         for m in oracle.BFS_ORDERS:
