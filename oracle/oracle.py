@@ -393,6 +393,50 @@ def ref_edge_list(records, V, tmpdir=None):
     return lines["csr_offset:"], lines["csr_dest:"], lines["csr_weight:"]
 
 
+def _csr_lines(stdout, keys=("csr_offset:", "csr_dest:", "csr_weight:")):
+    lines = {}
+    for l in stdout.splitlines():
+        for key in keys:
+            if l.startswith(key):
+                lines[key] = np.array(l[len(key):].split(), dtype=np.uint64).astype(np.uint32)
+    return [lines[k] for k in keys]
+
+
+def ref_sort_neighbours(off, dst, w, tmpdir=None):
+    """Run the reference's nbrSort_taskSteal (my_project/CGgraph/sortNbr.hpp:
+    8-99) on a CSR.  Returns the sorted (off, dst, w), or None when its
+    strictly-ascending check fails (a repeated destination; exit status 1)."""
+    if not ref_available():
+        raise RuntimeError("reference oracle binary not built (oracle/build_ref.sh)")
+    off, dst, w = _u32(off), _u32(dst), _u32(w)
+    with tempfile.TemporaryDirectory(dir=tmpdir) as d:
+        paths = [os.path.join(d, n) for n in ("off.bin", "dst.bin", "w.bin")]
+        for a, pth in zip((off, dst, w), paths):
+            a.tofile(pth)
+        r = subprocess.run([REF_BIN, "sortnbr", str(off.size - 1), str(dst.size)] + paths,
+                           capture_output=True, text=True)
+    if r.returncode == 1:
+        return None
+    if r.returncode != 0:
+        raise RuntimeError(f"cgref_oracle sortnbr failed ({r.returncode}): {r.stderr[-2000:]}")
+    return tuple(_csr_lines(r.stdout))
+
+
+def sort_neighbours(off, dst, w):
+    """Every list sorted by destination, weights following, as the reference
+    driver's nbrSort_taskSteal does (my_project/CGgraph/sortNbr.hpp:8-99);
+    a repeated destination in a list raises EdgeListError (its assert_msg,
+    :88-93).  numpy, not the engine's method."""
+    off = np.asarray(off, dtype=np.int64)
+    dst = np.asarray(dst, dtype=np.uint32)
+    src = np.repeat(np.arange(off.size - 1), np.diff(off))
+    k = np.lexsort((dst, src))
+    d2 = dst[k]
+    if np.any((src[1:] == src[:-1]) & (d2[1:] == d2[:-1])):
+        raise EdgeListError("repeated destination in a list")
+    return off.astype(np.uint32), d2, np.asarray(w, np.uint32)[k]
+
+
 def ref_available() -> bool:
     return os.path.exists(REF_BIN)
 

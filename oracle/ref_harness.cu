@@ -29,7 +29,13 @@
 //   as main_partition.hpp:105-112 calls them) with one OpenMP thread, since
 //   the reader appends to per-vertex vectors from its parallel loop; prints
 //   the CSR as above.  Self-loops and duplicates end the process with the
-//   reader's own assertion (exit status 1).
+//   reader's own assertions.
+//
+// usage: cgref_oracle sortnbr <V> <E> <offsets.bin> <dest.bin> <weight.bin>
+//   runs nbrSort_taskSteal (my_project/CGgraph/sortNbr.hpp:8-99), the sort the
+//   reference driver applies to every loaded CSR (main_partition.hpp:146), and
+//   prints the CSR as above; a list with a repeated destination fails its
+//   strictly-ascending assert_msg (exit status 1).
 
 #include "Basic/basic_include.cuh"
 #include "my_project/CGgraph/host_algorithm.hpp"
@@ -118,8 +124,32 @@ static int run_edges(int argc, char** argv)
     _exit(0);
 }
 
+static int run_sortnbr(int argc, char** argv)
+{
+    if (argc < 7) {
+        fprintf(stderr, "usage: %s sortnbr V E off dest weight\n", argv[0]);
+        return 2;
+    }
+    uint64_t V = strtoull(argv[2], nullptr, 10);
+    uint64_t E = strtoull(argv[3], nullptr, 10);
+    if (V == 0) return 2;
+    CSR_Result_type csr;
+    csr.vertexNum = (count_type)V;
+    csr.edgeNum = (countl_type)E;
+    csr.csr_offset = load_binFile<countl_type>(argv[4], V + 1);
+    csr.csr_dest = E ? load_binFile<vertex_id_type>(argv[5], E) : new vertex_id_type[1];
+    csr.csr_weight = E ? load_binFile<edge_data_type>(argv[6], E) : new edge_data_type[1];
+    nbrSort_taskSteal(csr);
+    print_u32_line("csr_offset:", csr.csr_offset, V + 1);
+    print_u32_line("csr_dest:", csr.csr_dest, E);
+    print_u32_line("csr_weight:", csr.csr_weight, E);
+    fflush(stdout);
+    _exit(0);
+}
+
 int main(int argc, char** argv)
 {
+    if (argc > 1 && std::string(argv[1]) == "sortnbr") return run_sortnbr(argc, argv);
     if (argc > 1 && std::string(argv[1]) == "reorder") return run_reorder(argc, argv);
     if (argc > 1 && std::string(argv[1]) == "edges") return run_edges(argc, argv);
     if (argc < 9) {

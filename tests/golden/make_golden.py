@@ -21,7 +21,13 @@ CSR the reference's edge-list reader (Basic/Graph/graphBinReader.hpp,
 GraphBinReader) builds from them, or rejected = 1 where the reader's
 assertions stop it (a self-loop, a duplicate edge).
 
-usage: python tests/golden/make_golden.py [reference root] [--reorder-only | --edgelist-only]
+The fixtures under sortnbr/ hold CSRs with shuffled lists and what the
+reference driver's neighbour sort (nbrSort_taskSteal,
+my_project/CGgraph/sortNbr.hpp) makes of them, or rejected = 1 where its
+strictly-ascending check stops it (a repeated destination).
+
+usage: python tests/golden/make_golden.py [reference root]
+                                          [--reorder-only | --edgelist-only | --sortnbr-only]
 """
 from __future__ import annotations
 
@@ -116,17 +122,53 @@ def make_edge_lists():
         print("edgelist", name, V, len(rec), "rejected" if r is None else "")
 
 
+def shuffled_lists(off, dst, w, seed):
+    rng = np.random.default_rng(seed)
+    d, ww = dst.copy(), w.copy()
+    for v in range(off.size - 1):
+        a, b = int(off[v]), int(off[v + 1])
+        p = rng.permutation(b - a)
+        d[a:b], ww[a:b] = d[a:b][p], ww[a:b][p]
+    return off, d, ww
+
+
+def sortnbr_cases():
+    yield ("rmat10_s3_shuffled",) + shuffled_lists(*O.rmat_graph(10, 8, seed=3), seed=1)
+    yield ("rmat9_s5_sym_shuffled",) + shuffled_lists(*O.rmat_graph(9, 16, seed=5, symmetrise=True), seed=2)
+    off, dst, w = O.rmat_graph(9, 8, seed=6)
+    v = int(np.argmax(np.diff(off.astype(np.int64)) >= 3))
+    d = dst.copy()
+    d[off[v] + 1] = d[off[v]]
+    yield "repeated_destination", off, d, w
+
+
+def make_sortnbr():
+    d = os.path.join(HERE, "sortnbr")
+    os.makedirs(d, exist_ok=True)
+    for name, off, dst, w in sortnbr_cases():
+        out = {"offsets": off, "dest": dst, "weight": w}
+        r = O.ref_sort_neighbours(off, dst, w)
+        out["rejected"] = np.array([r is None], np.uint8)
+        if r is not None:
+            out["sorted_offsets"], out["sorted_dest"], out["sorted_weight"] = r
+        np.savez_compressed(os.path.join(d, f"{name}.npz"), **out)
+        print("sortnbr", name, off.size - 1, dst.size, "rejected" if r is None else "")
+
+
 def main():
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
     ref_root = args[0] if args else "/root/reference"
     O.build()
     if O.build_ref(ref_root) is None:
         raise SystemExit("reference oracle unavailable")
-    if "--edgelist-only" not in sys.argv:
+    only = [a for a in sys.argv if a.endswith("-only")]
+    if not only or "--reorder-only" in only:
         make_reorder()
-    if "--reorder-only" not in sys.argv:
+    if not only or "--edgelist-only" in only:
         make_edge_lists()
-    if "--reorder-only" in sys.argv or "--edgelist-only" in sys.argv:
+    if not only or "--sortnbr-only" in only:
+        make_sortnbr()
+    if only:
         return
     for name, off, dst, w, roots in graphs():
         out = {"offsets": off, "dest": dst, "weight": w, "roots": np.array(roots, np.uint32)}

@@ -259,6 +259,29 @@ def test_edge_list_reference_fixtures():
             np.testing.assert_array_equal(w, g["weight"], err_msg=f)
 
 
+def test_neighbour_sort_reference_fixtures():
+    """cgb_graph_create on CSRs with shuffled lists gives the lists the
+    reference driver's nbrSort_taskSteal makes of them (fixtures made with the
+    reference), and CGB_EFORMAT where its strictly-ascending check fails."""
+    import os
+
+    from conftest import GOLDEN_DIR
+
+    d = os.path.join(GOLDEN_DIR, "sortnbr")
+    for f in sorted(os.listdir(d)):
+        g = dict(np.load(os.path.join(d, f)))
+        if g["rejected"][0]:
+            with pytest.raises(CgbError) as ei:
+                cg.Graph.from_csr(g["offsets"], g["dest"], g["weight"])
+            assert ei.value.status == L.EFORMAT, f
+            continue
+        with cg.Graph.from_csr(g["offsets"], g["dest"], g["weight"]) as h:
+            o, dd, w = h.download()
+            np.testing.assert_array_equal(o, g["sorted_offsets"], err_msg=f)
+            np.testing.assert_array_equal(dd, g["sorted_dest"], err_msg=f)
+            np.testing.assert_array_equal(w, g["sorted_weight"], err_msg=f)
+
+
 def test_reorder_degree_orders(oracle):
     """cgb_graph_reorder: IN_DEGREE_DEC and NORMAL_OUTDEGREE_DEC relabel the
     graph exactly as the oracle's restatement of the reference's Reorder

@@ -265,3 +265,22 @@ def test_edge_list_reference_live(oracle):
     ref = oracle.ref_edge_list(rec, off.size - 1)
     for a, b in zip(oracle.edge_list_to_csr(rec, off.size - 1), ref):
         np.testing.assert_array_equal(a, b)
+
+
+SORTNBR_DIR = os.path.join(GOLDEN_DIR, "sortnbr")
+SORTNBR_GOLDEN = sorted(f[:-4] for f in os.listdir(SORTNBR_DIR) if f.endswith(".npz"))
+
+
+@pytest.mark.parametrize("name", SORTNBR_GOLDEN)
+def test_neighbour_sort_oracle_matches_reference_golden(oracle, name):
+    """The neighbour-sort restatement against the reference driver's
+    nbrSort_taskSteal (fixtures made with the reference itself): the same
+    sorted CSR, and a rejection where its check stops it."""
+    g = dict(np.load(os.path.join(SORTNBR_DIR, name + ".npz")))
+    if g["rejected"][0]:
+        with pytest.raises(oracle.EdgeListError):
+            oracle.sort_neighbours(g["offsets"], g["dest"], g["weight"])
+        return
+    for a, b in zip(oracle.sort_neighbours(g["offsets"], g["dest"], g["weight"]),
+                    (g["sorted_offsets"], g["sorted_dest"], g["sorted_weight"])):
+        np.testing.assert_array_equal(a, b)
