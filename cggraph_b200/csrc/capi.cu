@@ -88,7 +88,7 @@ cgb_status cgb_graph_create(const uint32_t* offsets, const uint32_t* dest, const
         CGB_REQUIRE(offsets != nullptr, CGB_EINVAL, "offsets is NULL");
         CGB_REQUIRE(E == 0 || dest != nullptr, CGB_EINVAL, "dest is NULL");
         CGB_REQUIRE(V >= 1, CGB_EINVAL, "V must be >= 1");
-        CGB_REQUIRE(V < 0xFFFFFFFFu && E < 0xFFFFFFFFu, CGB_EUNSUPPORTED, "V and E must be < 2^32 - 1");
+        CGB_REQUIRE(V <= kMaxGraphSize && E <= kMaxGraphSize, CGB_EUNSUPPORTED, "V and E must be at most 2^32 - 2^24");
         cgb_graph* g = graph_alloc(V, E, nz, device, weight != nullptr && E > 0);
         try {
             copy_any(g->off, offsets, ((size_t)V + 1) * 4, g->stream);

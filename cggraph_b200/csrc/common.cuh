@@ -14,6 +14,9 @@ constexpr uint32_t kValueMax = CGB_VALUE_MAX;  // VertexValue_MAX, Basic/Graph/b
 constexpr int kBlock = 256;                    // threads per CTA for the frontier kernels
 constexpr int kWarp = 32;
 constexpr int kNumSMs = 148;                   // B200
+// Largest V and E of a graph.  Kernels step 32-bit indices by a grid stride
+// below 2^24, so indices up to 2^32 - 2^24 never wrap.
+constexpr uint32_t kMaxGraphSize = 0xFF000000u;
 
 // Error state of the calling thread (cgb_last_error_string).
 void set_error(const std::string& msg);

@@ -73,7 +73,7 @@ static uint32_t key_bits(uint64_t n)
 cgb_graph* graph_from_edges(const uint32_t* records, uint64_t E, uint32_t V, int device)
 {
     CGB_REQUIRE(V >= 1, CGB_EINVAL, "V must be >= 1");
-    CGB_REQUIRE(V < 0xFFFFFFFFu && E < 0xFFFFFFFFu, CGB_EUNSUPPORTED, "V and E must be < 2^32 - 1");
+    CGB_REQUIRE(V <= kMaxGraphSize && E <= kMaxGraphSize, CGB_EUNSUPPORTED, "V and E must be at most 2^32 - 2^24");
     CGB_REQUIRE(E == 0 || records != nullptr, CGB_EINVAL, "records is NULL");
     cgb_graph* g = graph_alloc(V, (uint32_t)E, V, device, E > 0);
     cudaStream_t s = g->stream;

@@ -1378,6 +1378,7 @@ void ktimer_collect(cgb_graph* g)
 // --------------------------------------------------------------- lifetime
 cgb_graph* graph_alloc(uint32_t V, uint32_t E, uint32_t nz, int device, bool with_weight)
 {
+    CGB_REQUIRE(V <= kMaxGraphSize && E <= kMaxGraphSize, CGB_EUNSUPPORTED, "V and E must be at most 2^32 - 2^24");
     CGB_CUDA_TRY(cudaSetDevice(device));
     cgb_graph* g = new cgb_graph();
     g->device = device;

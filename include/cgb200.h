@@ -132,8 +132,9 @@ typedef struct cgb_iter_trace {
  * offsets[V] == E, dest[e] < V; neighbour lists are sorted by dest on the
  * device (weights follow, as nbrSort_taskSteal does) and must then be
  * strictly ascending (no duplicate edges).  weight may be NULL (SSSP then
- * uses weight 1).  no_zero_out_degree_num = 0 means V.  The caller keeps
- * ownership of its arrays.  Replaces GraphDeviceWorklist's constructor and
+ * uses weight 1).  no_zero_out_degree_num = 0 means V.  V and E are at
+ * most 2^32 - 2^24 (CGB_EUNSUPPORTED beyond; the reference's uint32 count types
+ * end at 2^32 - 1).  The caller keeps ownership of its arrays.  Replaces GraphDeviceWorklist's constructor and
  * csrToDevice() (GraphDevice.cuh:48-71,208-221). */
 cgb_status cgb_graph_create(const uint32_t* offsets, const uint32_t* dest, const uint32_t* weight,
                             uint32_t V, uint32_t E, uint32_t no_zero_out_degree_num, int device,

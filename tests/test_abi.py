@@ -49,6 +49,11 @@ def test_argument_errors_are_status_codes(lib):
     assert b"offsets" in lib.cgb_last_error_string()
     assert lib.cgb_run(None, 0, 0, None, None, None, None) == _lib.EINVAL
     assert lib.cgb_status_string(_lib.EFORMAT) == b"invalid CSR"
+    # sizes beyond 2^32 - 2^24 are refused before any array is read
+    one = (ctypes.c_uint32 * 2)()
+    for V, E in ((0xFF000001, 0), (4, 0xFF000001)):
+        assert lib.cgb_graph_create(one, one, None, V, E, 0, 0, ctypes.byref(h)) == _lib.EUNSUPPORTED
+        assert b"2^32 - 2^24" in lib.cgb_last_error_string()
 
 
 def test_load_files_size_check(lib, tmp_path):
