@@ -161,7 +161,8 @@ cgb_status cgb_batch_create(uint32_t n, const uint32_t* const* offsets, const ui
             Et += Es[i];
             any_w |= weights && weights[i];
         }
-        CGB_REQUIRE(Vt < 0xFFFFFFFFull && Et < 0xFFFFFFFFull, CGB_EUNSUPPORTED, "batch exceeds 2^32 vertices or edges");
+        CGB_REQUIRE(Vt <= kMaxGraphSize && Et <= kMaxGraphSize, CGB_EUNSUPPORTED,
+                    "batch exceeds 2^32 - 2^24 vertices or edges");
         cgb_batch* b = new cgb_batch();
         try {
             b->n = n;
