@@ -27,7 +27,7 @@ KERNEL_CLASS_NAMES = ["push", "pull", "pagerank", "hook", "compress", "frontier"
 
 # Exported symbols, exactly as declared in include/*.h.
 EXPORTS = [
-    "cgb_graph_create", "cgb_graph_load_files", "cgb_graph_create_from_edges", "cgb_graph_load_edge_file", "cgb_graph_reorder", "cgb_graph_destroy", "cgb_graph_set_stream", "cgb_graph_set_weights", "cgb_graph_info", "cgb_graph_device_csr",
+    "cgb_graph_create", "cgb_graph_load_files", "cgb_graph_create_from_edges", "cgb_graph_load_edge_file", "cgb_graph_reorder", "cgb_graph_partition", "cgb_graph_destroy", "cgb_graph_set_stream", "cgb_graph_set_weights", "cgb_graph_info", "cgb_graph_device_csr",
     "cgb_graph_result_device", "cgb_graph_result_download", "cgb_run", "cgb_run_batch", "cgb_run_stats_get", "cgb_trace_get",
     "cgb_last_error_string", "cgb_status_string", "cgb_abi_version", "cgb_gen_rmat", "cgb_gen_grid", "cgb_gen_chunglu",
     "cgb_graph_download", "cgb_bfs_noalloc", "cgb_policy_load", "cgb_policy_collect", "cgb_policy_train",
@@ -94,6 +94,16 @@ class CgbError(RuntimeError):
 
 
 _lib = None
+
+class PartitionInfo(ctypes.Structure):
+    """cgb_partition_info (include/cgb200.h)."""
+    _fields_ = [
+        ("segment_num", ctypes.c_uint32),
+        ("bucket_start", ctypes.c_uint32 * 5),
+        ("can_hold_all", ctypes.c_int32),
+        ("reached_bucket", ctypes.c_uint32),
+    ]
+
 
 class Tuning(ctypes.Structure):
     _fields_ = [
@@ -172,6 +182,7 @@ def lib() -> ctypes.CDLL:
         L.cgb_graph_create_from_edges.argtypes = [_P, ctypes.c_uint64, u32, i, ctypes.POINTER(_P)]
         L.cgb_graph_load_edge_file.argtypes = [ctypes.c_char_p, u32, i, ctypes.POINTER(_P)]
         L.cgb_graph_reorder.argtypes = [_P, i, _P, _u32p, ctypes.POINTER(_P)]
+        L.cgb_graph_partition.argtypes = [_P, i, ctypes.c_uint32, _P, _P, _P, _P, _P, ctypes.POINTER(PartitionInfo)]
         L.cgb_graph_set_stream.argtypes = [_P, _P]
         L.cgb_graph_set_weights.argtypes = [_P, _P]
         L.cgb_graph_info.argtypes = [_P, _u32p, _u32p, ctypes.POINTER(ctypes.c_int32)]

@@ -177,6 +177,26 @@ cgb_status cgb_graph_reorder(cgb_graph* g, int order_method, uint32_t* old2new, 
     });
 }
 
+cgb_status cgb_graph_partition(cgb_graph* g, int algorithm, uint32_t num_devices, const uint64_t* device_mem_bytes,
+                               uint32_t* seg_order, uint32_t* seg_edges, int32_t* seg_owner,
+                               uint32_t* device_segments, cgb_partition_info* info)
+{
+    return guarded([&] {
+        CGB_REQUIRE(g != nullptr && info != nullptr, CGB_EINVAL, "graph or info is NULL");
+        CGB_REQUIRE(num_devices >= 1, CGB_EINVAL, "num_devices must be >= 1");
+        CGB_REQUIRE(algorithm >= CGB_BFS && algorithm <= CGB_PR, CGB_EINVAL, "unknown algorithm");
+        if (!device_mem_bytes) {
+            int n = 0;
+            CGB_CUDA_TRY(cudaGetDeviceCount(&n));
+            CGB_REQUIRE(num_devices <= (uint32_t)n, CGB_EINVAL, "num_devices exceeds the visible devices");
+        }
+        std::lock_guard<GraphMutex> lock(g->mu);
+        CGB_CUDA_TRY(cudaSetDevice(g->device));
+        graph_partition(g, algorithm, num_devices, device_mem_bytes, seg_order, seg_edges, seg_owner,
+                        device_segments, info);
+    });
+}
+
 cgb_status cgb_graph_destroy(cgb_graph* g)
 {
     return guarded([&] { graph_free(g); });

@@ -226,8 +226,11 @@ void pool_free(void* p, cudaStream_t s);
 // A graph from an edge list of packed (source, destination, weight) u32
 // records in host or device memory (cgb_graph_create_from_edges).
 cgb_graph* graph_from_edges(const uint32_t* records, uint64_t E, uint32_t V, int device);
-// Relabelled copy of g in a degree order (cgb_graph_reorder).
+// Relabelled copy of g in one of the reference's vertex orders (cgb_graph_reorder).
 cgb_graph* graph_reorder(cgb_graph* g, int method, uint32_t* old2new_out, uint32_t* nz_out);
+// The reference's two-level segment partition over GPUs (cgb_graph_partition).
+void graph_partition(cgb_graph* g, int algorithm, uint32_t ndev, const uint64_t* mem_bytes, uint32_t* seg_order,
+                     uint32_t* seg_edges, int32_t* seg_owner, uint32_t* device_segments, cgb_partition_info* info);
 void* pinned_small_alloc(size_t bytes);
 // Pinned host memory for small transfers, from a process-wide pool.
 void* pinned_acquire(size_t bytes);

@@ -320,6 +320,27 @@ class Graph:
                                         ctypes.byref(h)))
         return Graph(h.value), old2new, nz.value
 
+    def partition(self, algorithm: int, num_devices: int, device_mem_bytes=None) -> dict:
+        """The reference's two-level segment partition over GPUs
+        (cgb_graph_partition, TwoLevelPartition): segments of 1024 vertices
+        sorted by degree into four buckets and dealt to the GPUs while their
+        memory holds them.  Returns segment_num, bucket_start, can_hold_all,
+        reached_bucket, seg_order, seg_edges, seg_owner (-1 = host) and
+        device_segments."""
+        info = L.PartitionInfo()
+        n = (self.vertexNum + 1023) // 1024  # noZeroOutDegreeNum <= V
+        order = np.empty(max(1, n), np.uint32)
+        edges = np.empty(max(1, n), np.uint32)
+        owner = np.empty(max(1, n), np.int32)
+        per_dev = np.empty(num_devices, np.uint32)
+        mem = None if device_mem_bytes is None else np.ascontiguousarray(device_mem_bytes, np.uint64)
+        check(L.lib().cgb_graph_partition(self._h, int(algorithm), int(num_devices), _ptr(mem), _ptr(order),
+                                          _ptr(edges), _ptr(owner), _ptr(per_dev), ctypes.byref(info)))
+        n = info.segment_num
+        return {"segment_num": n, "bucket_start": list(info.bucket_start), "can_hold_all": bool(info.can_hold_all),
+                "reached_bucket": info.reached_bucket, "seg_order": order[:n], "seg_edges": edges[:n],
+                "seg_owner": owner[:n], "device_segments": per_dev}
+
     def download(self, with_weight: bool = True):
         off = np.empty(self.vertexNum + 1, np.uint32)
         dst = np.empty(max(1, self.edgeNum), np.uint32)

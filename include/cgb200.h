@@ -193,6 +193,35 @@ cgb_status cgb_graph_load_edge_file(const char* path, uint32_t V, int device, cg
 cgb_status cgb_graph_reorder(cgb_graph* g, int order_method, uint32_t* old2new,
                              uint32_t* no_zero_out_degree_num, cgb_graph** out);
 
+/* The reference's two-level partition of a graph over GPUs
+ * (my_project/CGgraph/Two-level_partition.cuh:213-444), the plan its
+ * CPU+GPU co-execution engine runs on. The vertices with out-edges,
+ * [0, noZeroOutDegreeNum), are cut into segments of CGB_SEGMENT_SIZE
+ * vertices; segments are sorted by average degree (edges / vertices, an
+ * integer quotient; ties by segment id) and cut into four buckets (degree up
+ * to 16, up to 32, up to 256, above); then dealt to num_devices GPUs bucket
+ * by bucket, segment j of a bucket to GPU (j + j / num_devices) %
+ * num_devices, each GPU taking 4 bytes per edge (8 for CGB_SSSP) out of its
+ * memory less 4 V + 4 (noZeroOutDegreeNum + 1) bytes and a 1 GiB reserve,
+ * until a GPU would reach zero; that segment and all after it stay with the
+ * host (owner -1). device_mem_bytes (num_devices entries) may be NULL: the
+ * total memory of devices 0 .. num_devices - 1. Output arrays may be NULL:
+ * seg_order (segment_num entries) the segment ids in sorted order,
+ * seg_edges and seg_owner (segment_num, by segment id), device_segments
+ * (num_devices) the segments each GPU takes. The per-GPU CSR copies the
+ * reference then builds are not made. */
+#define CGB_SEGMENT_SIZE 1024
+typedef struct cgb_partition_info {
+    uint32_t segment_num;     /* ceil(noZeroOutDegreeNum / CGB_SEGMENT_SIZE) */
+    uint32_t bucket_start[5]; /* bucket b = sorted positions [bucket_start[b], bucket_start[b + 1]) */
+    int32_t can_hold_all;     /* canHoldAllSegment: every segment went to a GPU */
+    uint32_t reached_bucket;  /* the last bucket the deal entered */
+} cgb_partition_info;
+
+cgb_status cgb_graph_partition(cgb_graph* g, int algorithm, uint32_t num_devices, const uint64_t* device_mem_bytes,
+                               uint32_t* seg_order, uint32_t* seg_edges, int32_t* seg_owner,
+                               uint32_t* device_segments, cgb_partition_info* info);
+
 cgb_status cgb_graph_destroy(cgb_graph* g);
 
 /* Runs all later work of this graph on `stream` (a cudaStream_t of the

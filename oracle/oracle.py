@@ -257,6 +257,57 @@ def cap_lists(off, dst, w, k):
     return np.cumsum(noff).astype(np.uint32), dst[keep].copy(), w[keep].copy()
 
 
+def two_level_partition(off, nz, algorithm, device_mem_bytes):
+    """The reference's TwoLevelPartition plan (my_project/CGgraph/
+    Two-level_partition.cuh), restated line by line in Python: segments of
+    1024 vertices over [0, nz) with edges and integer degree edges / vertices
+    (get_SegmentInfo, :213-259); sorted by (degree, id) and cut at the first
+    degree >= 17, 33 and 257 (partition_buckets, :267-342); dealt bucket by
+    bucket to GPU (j + j // n) % n while that GPU's memory, less 4 V +
+    4 (nz + 1) bytes and 2^30 reserved, stays above zero after taking 4 bytes
+    per edge (8 for SSSP) (partition_GPU, :350-444).  Parity unpinned: the
+    reference's partitioner queries and fills the GPUs in its constructor, so
+    it does not run without them; this follows its source."""
+    off = np.asarray(off, dtype=np.int64)
+    V = off.size - 1
+    n_dev = len(device_mem_bytes)
+    nseg = (nz + 1023) // 1024
+    seg = []
+    for s in range(nseg):
+        b, e = s * 1024, min((s + 1) * 1024, nz)
+        m = int(off[e] - off[b])
+        seg.append((m // (e - b), s, m))
+    seg.sort(key=lambda t: (t[0], t[1]))
+    degs = [t[0] for t in seg]
+    import bisect
+    bucket = [0] + [bisect.bisect_left(degs, x) for x in (17, 33, 257)] + [nseg]
+    cap = [int(m) - (V * 4 + (nz + 1) * 4 + (1 << 30)) for m in device_mem_bytes]
+    per_edge = 8 if algorithm == 1 else 4
+    owner = [-1] * nseg
+    count = [0] * n_dev
+    all_fit, reached = True, 0
+    for b in range(4):
+        if not all_fit:
+            break
+        reached = b
+        for j in range(bucket[b + 1] - bucket[b]):
+            dev = (j + j // n_dev) % n_dev
+            _, sid, m = seg[bucket[b] + j]
+            cap[dev] -= m * per_edge
+            if cap[dev] <= 0:
+                cap[dev] += m * per_edge
+                all_fit = False
+                break
+            owner[sid] = dev
+            count[dev] += 1
+    edges = [0] * nseg
+    for _, sid, m in seg:
+        edges[sid] = m
+    return {"segment_num": nseg, "bucket_start": bucket, "can_hold_all": all_fit, "reached_bucket": reached,
+            "seg_order": np.array([t[1] for t in seg], np.uint32), "seg_edges": np.array(edges, np.uint32),
+            "seg_owner": np.array(owner, np.int32), "device_segments": np.array(count, np.uint32)}
+
+
 def rmat_thresholds(a=0.57, b=0.19, c=0.19):
     """Quadrant thresholds in units of 2^-32 (floor), shared with the engine."""
     t1 = int(a * 2**32)

@@ -154,7 +154,7 @@ def test_struct_layouts_match_header(tmp_path):
     from cggraph_b200 import _lib
     structs = {"cgb_options": _lib.Options, "cgb_run_stats": _lib.RunStats, "cgb_iter_trace": _lib.IterTrace,
                "cgb_server_config": _lib.ServerConfig, "cgb_request_info": _lib.RequestInfo,
-               "cgb_tuning": _lib.Tuning}
+               "cgb_tuning": _lib.Tuning, "cgb_partition_info": _lib.PartitionInfo}
     lines = ['#include "cgb200.h"', "#include <stdio.h>", "#include <stddef.h>", "int main(void) {"]
     for cname, py in structs.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')

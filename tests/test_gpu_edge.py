@@ -445,3 +445,34 @@ def test_memory_pool_reuse_and_trim(oracle):
     with cg.Graph.from_csr(off, dst, w) as g:
         np.testing.assert_array_equal(g.run(0, 3)[0], exp)
     cg.memory_trim()
+
+
+def test_two_level_partition(oracle):
+    """cgb_graph_partition equals the restatement of the reference's
+    TwoLevelPartition: segment order, edges, buckets, owners and per-GPU
+    counts, for room enough and for GPUs that fill up part way, with a
+    zero-out-degree tail, for BFS and SSSP."""
+    off, dst, w = oracle.rmat_graph(16, 16, seed=9)
+    V = off.size - 1
+    with cg.Graph.from_csr(off, dst, w) as g0:
+        h, old2new, nz = g0.reorder(cg.OrderMethod.NORMAL_OUTDEGREE_DEC)
+    o2, d2, w2 = h.download()
+    h.close()
+    cases = [(off, dst, w, V), (o2, d2, w2, nz)]
+    off_g, dst_g, w_g = oracle.grid_graph(100, 130)
+    cases.append((off_g, dst_g, w_g, off_g.size - 1))
+    for o, d, ww, n in cases:
+        Vc = o.size - 1
+        base = Vc * 4 + (n + 1) * 4 + (1 << 30)
+        with cg.Graph.from_csr(o, d, ww, noZeroOutDegreeNum=n) as g:
+            for alg in (BFS, SSSP):
+                for mem in ([1 << 40], [1 << 40] * 3, [base + d.size, base + d.size // 3],
+                            [base + 2 * d.size, base + d.size, base + 5]):
+                    got = g.partition(alg, len(mem), mem)
+                    exp = oracle.two_level_partition(o, n, alg, mem)
+                    for k in ("segment_num", "bucket_start", "can_hold_all", "reached_bucket"):
+                        assert got[k] == exp[k], (k, alg, mem)
+                    for k in ("seg_order", "seg_edges", "seg_owner", "device_segments"):
+                        np.testing.assert_array_equal(got[k], exp[k], err_msg=f"{k} {alg} {mem}")
+            got = g.partition(BFS, 1)  # the device's own memory: everything fits
+            assert got["can_hold_all"] and np.all(got["seg_owner"] == 0)

@@ -284,3 +284,39 @@ def test_neighbour_sort_oracle_matches_reference_golden(oracle, name):
     for a, b in zip(oracle.sort_neighbours(g["offsets"], g["dest"], g["weight"]),
                     (g["sorted_offsets"], g["sorted_dest"], g["sorted_weight"])):
         np.testing.assert_array_equal(a, b)
+
+
+def test_two_level_partition_oracle_by_hand(oracle):
+    """The partition restatement on a graph worked by hand: 3 segments over
+    nz = 2100 vertices of degrees 1, 40 and 300 (segment 2 has 52 vertices),
+    two GPUs with room for exactly the first two segments' edges."""
+    V, nz = 2200, 2100
+    deg = np.zeros(V, np.int64)
+    deg[0:1024] = 1
+    deg[1024:2048] = 40
+    deg[2048:2100] = 300
+    off = np.concatenate([[0], np.cumsum(deg)])
+    r = oracle.two_level_partition(off, nz, 0, [1 << 40, 1 << 40])
+    assert r["segment_num"] == 3 and r["bucket_start"] == [0, 1, 1, 2, 3]
+    assert r["seg_order"].tolist() == [0, 1, 2] and r["seg_edges"].tolist() == [1024, 40960, 15600]
+    # bucket 0: j = 0 -> GPU 0; bucket 2: j = 0 -> GPU 0; bucket 3: j = 0 -> GPU 0
+    assert r["seg_owner"].tolist() == [0, 0, 0] and r["can_hold_all"] and r["reached_bucket"] == 3
+    base = V * 4 + (nz + 1) * 4 + (1 << 30)
+    r = oracle.two_level_partition(off, nz, 0, [base + 4 * (1024 + 40960) + 1, base])
+    assert r["seg_owner"].tolist() == [0, 0, -1] and not r["can_hold_all"] and r["reached_bucket"] == 3
+    r = oracle.two_level_partition(off, nz, 1, [base + 4 * (1024 + 40960) + 1, base])  # SSSP: 8 bytes per edge
+    assert r["seg_owner"].tolist() == [0, -1, -1] and r["reached_bucket"] == 2
+    assert r["device_segments"].tolist() == [1, 0]
+
+
+def test_two_level_partition_oracle_round_robin(oracle):
+    """With room for everything, each bucket is dealt as (j + j // n) % n."""
+    off, dst, w = oracle.rmat_graph(14, 16, seed=2)
+    V = off.size - 1
+    r = oracle.two_level_partition(off, V, 0, [1 << 45] * 3)
+    assert r["can_hold_all"] and np.all(r["seg_owner"] >= 0)
+    for b in range(4):
+        ids = r["seg_order"][r["bucket_start"][b]:r["bucket_start"][b + 1]]
+        j = np.arange(ids.size)
+        np.testing.assert_array_equal(r["seg_owner"][ids], (j + j // 3) % 3)
+    assert int(r["seg_edges"].astype(np.int64).sum()) == dst.size
