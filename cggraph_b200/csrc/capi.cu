@@ -105,13 +105,9 @@ cgb_status cgb_graph_create(const uint32_t* offsets, const uint32_t* dest, const
     });
 }
 
-static std::vector<uint32_t> load_array(const char* path, uint64_t length)
+// The first `length` words of a file that holds at least that many.
+static std::vector<uint32_t> read_words(const char* path, uint64_t length)
 {
-    struct stat st;
-    CGB_REQUIRE(path != nullptr, CGB_EINVAL, "path is NULL");
-    if (stat(path, &st) != 0) throw Error{CGB_EIO, std::string("Bin File [") + path + "] Not Exist"};
-    if ((uint64_t)st.st_size != length * 4)
-        throw Error{CGB_EIO, std::string("(total_bytes / utilSize != length) for ") + path};
     std::vector<uint32_t> a(length);
     FILE* f = std::fopen(path, "rb");
     if (!f) throw Error{CGB_EIO, std::string("cannot open ") + path};
@@ -119,6 +115,24 @@ static std::vector<uint32_t> load_array(const char* path, uint64_t length)
     std::fclose(f);
     if (got != length) throw Error{CGB_EIO, std::string("short read on ") + path};
     return a;
+}
+
+static uint64_t file_bytes(const char* path)
+{
+    struct stat st;
+    CGB_REQUIRE(path != nullptr, CGB_EINVAL, "path is NULL");
+    if (stat(path, &st) != 0) throw Error{CGB_EIO, std::string("Bin File [") + path + "] Not Exist"};
+    return (uint64_t)st.st_size;
+}
+
+// load_binFile (Basic/Other/IO.hpp:44-92): the file must hold `length`
+// whole elements, total_bytes / 4 == length; trailing bytes short of an
+// element are ignored, as there.
+static std::vector<uint32_t> load_array(const char* path, uint64_t length)
+{
+    if (file_bytes(path) / 4 != length)
+        throw Error{CGB_EIO, std::string("(total_bytes / utilSize != length) for ") + path};
+    return read_words(path, length);
 }
 
 cgb_status cgb_graph_load_files(const char* off_path, const char* dst_path, const char* w_path, uint32_t V,
@@ -153,14 +167,11 @@ cgb_status cgb_graph_load_edge_file(const char* path, uint32_t V, int device, cg
     return guarded([&] {
         CGB_REQUIRE(out != nullptr, CGB_EINVAL, "out is NULL");
         *out = nullptr;
-        CGB_REQUIRE(path != nullptr, CGB_EINVAL, "path is NULL");
-        struct stat st;
-        if (stat(path, &st) != 0) throw Error{CGB_EIO, std::string("Bin File [") + path + "] Not Exist"};
-        const uint64_t bytes = (uint64_t)st.st_size;
-        if (bytes % 12 != 0)
-            throw Error{CGB_EIO, std::string("edge file size is not a whole number of 12-byte records: ") + path};
-        const std::vector<uint32_t> rec = load_array(path, bytes / 4);
-        *out = graph_from_edges(rec.data(), bytes / 12, V, device);
+        // the reader takes total_bytes / 12 records and ignores a trailing
+        // partial one (graphBinReader.hpp:92-93,152)
+        const uint64_t E = file_bytes(path) / 12;
+        const std::vector<uint32_t> rec = read_words(path, E * 3);
+        *out = graph_from_edges(rec.data(), E, V, device);
     });
 }
 

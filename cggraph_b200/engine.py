@@ -93,12 +93,13 @@ class CSR_Result_type:
 
 
 def load_binFile(path: str, length: int, dtype=np.uint32) -> np.ndarray:
-    """Reads a raw little-endian array, requiring file bytes == length * itemsize
-    (Basic/Other/IO.hpp:44-92, which asserts the same)."""
+    """Reads a raw little-endian array of `length` whole elements, requiring
+    file bytes // itemsize == length; trailing bytes short of an element are
+    ignored (Basic/Other/IO.hpp:44-92, which asserts the same quotient)."""
     if not os.path.exists(path):
         raise CgbError(L.EIO, f"Bin File [{path}] Not Exist")
     itemsize = np.dtype(dtype).itemsize
-    if os.path.getsize(path) // itemsize != length or os.path.getsize(path) % itemsize:
+    if os.path.getsize(path) // itemsize != length:
         raise CgbError(L.EIO, f"(total_bytes / utilSize != length) In Function load_binFile({path})")
     return np.fromfile(path, dtype=dtype, count=length)
 

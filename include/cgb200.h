@@ -158,7 +158,8 @@ cgb_status cgb_graph_create_from_edges(const uint32_t* records, uint64_t num_edg
 
 /* The same from a binary edge-list file (the reference's has_csrFile = 0
  * input, main_partition.hpp:105-116): the edge count is the file size / 12,
- * and a size that is not a whole number of records is CGB_EIO. */
+ * rounded down; trailing bytes short of a record are ignored, as the
+ * reference's reader ignores them. */
 cgb_status cgb_graph_load_edge_file(const char* path, uint32_t V, int device, cgb_graph** out);
 
 /* OrderMethod values (Basic/Graph/basic_struct.hpp:41-76) that cgb_graph_reorder builds. */

@@ -56,6 +56,48 @@ def test_argument_errors_are_status_codes(lib):
         assert b"2^32 - 2^24" in lib.cgb_last_error_string()
 
 
+def test_file_sizes_follow_the_reference(lib, tmp_path):
+    """load_binFile takes a file of total_bytes / 4 == length elements and
+    ignores trailing bytes short of one; the edge-list reader takes
+    total_bytes / 12 records and ignores a trailing partial one.  Accepted
+    files get past the size check (CGB_ECUDA without a GPU); the reference's
+    own loaders accept and reject the same files when its harness is built."""
+    import subprocess
+    import numpy as np
+    from cggraph_b200 import _lib
+    from oracle import oracle as O
+    off, dst, w = O.rmat_graph(8, 8, seed=1)
+    V, E = off.size - 1, dst.size
+    po, pd, pw = (tmp_path / n for n in ("off.bin", "dst.bin", "w.bin"))
+    off.tofile(po)
+    w.tofile(pw)
+    h = ctypes.c_void_p()
+    for extra, accepted in ((b"", True), (b"\7\7", True), (b"\7\7\7\7", False)):
+        pd.write_bytes(dst.tobytes() + extra)
+        st = lib.cgb_graph_load_files(str(po).encode(), str(pd).encode(), str(pw).encode(), V, E, 0,
+                                      ctypes.byref(h))
+        assert (st != _lib.EIO) == accepted, (extra, st)
+        if st == _lib.OK:
+            lib.cgb_graph_destroy(h)
+        if O.ref_available():
+            r = subprocess.run([O.REF_BIN, "0", str(V), str(E), str(po), str(pd), str(pw), "0", "-"],
+                               capture_output=True)
+            assert (r.returncode == 0) == accepted, (extra, r.returncode)
+    rec = O.csr_to_edge_list(off, dst, w, seed=2)
+    pe = tmp_path / "edges.bin"
+    for extra in (b"", b"\1" * 5, b"\1" * 11):
+        pe.write_bytes(rec.tobytes() + extra)
+        st = lib.cgb_graph_load_edge_file(str(pe).encode(), V, 0, ctypes.byref(h))
+        assert st != _lib.EIO, (extra, st)
+        if st == _lib.OK:
+            lib.cgb_graph_destroy(h)
+        if O.ref_available():
+            ref = O._csr_lines(subprocess.run([O.REF_BIN, "edges", str(V), str(pe)], capture_output=True,
+                                              text=True).stdout)
+            for a, b in zip(ref, (off, dst, w)):
+                np.testing.assert_array_equal(a, b)
+
+
 def test_load_files_size_check(lib, tmp_path):
     """load_binFile's size assertion becomes CGB_EIO (Basic/Other/IO.hpp:50-52)."""
     import numpy as np
