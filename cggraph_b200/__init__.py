@@ -25,6 +25,7 @@ from .engine import (  # noqa: F401
     memory_info,
     memory_reserve,
     memory_trim,
+    reorder_graph,
     save_binArray,
     trimmed_mean_ms,
 )

@@ -643,20 +643,53 @@ def trimmed_mean_ms(times: Sequence[float]) -> float:
     return sum(t) / len(t)
 
 
+def reorder_graph(csr_result: CSR_Result_type, orderMethod: OrderMethod, files: Optional[dict] = None,
+                  device: int = 0) -> dict:
+    """Reorder::generateReorderGraphFile (my_project/CGgraph/Reorder.hpp:58-241)
+    over cgb_graph_reorder: the relabelled CSR (lists sorted by new id), old2new
+    and the number of vertices without out-edges.  With ``files`` (keys
+    "offsets", "dest", "weight", "old2new", "addition" -> paths) it writes the
+    five files saveCSR_reorderFile writes (:538-700): the addition file holds
+    that count, and is empty for IN_DEGREE_DEC, whose order keeps no
+    zero-out-degree tail."""
+    with Graph.from_csr(csr_result.csr_offset, csr_result.csr_dest, csr_result.csr_weight, device=device) as g:
+        h, old2new, nz = g.reorder(orderMethod)
+        with h:
+            off, dst, w = h.download(with_weight=csr_result.csr_weight is not None)
+    V = csr_result.vertexNum
+    zero = V - nz
+    if files:
+        save_binArray(files["offsets"], off)
+        save_binArray(files["dest"], dst)
+        if w is not None:
+            save_binArray(files["weight"], w)
+        save_binArray(files["old2new"], old2new)
+        extra = np.zeros(0, np.uint32) if orderMethod == OrderMethod.IN_DEGREE_DEC else np.array([zero], np.uint32)
+        save_binArray(files["addition"], extra)
+    csr = CSR_Result_type(V, csr_result.edgeNum, off, dst, w, nz)
+    return {"csr": csr, "old2new": old2new, "zeroOutDegreeNum": zero}
+
+
 def main_partition(csr_result: CSR_Result_type, algorithm: Algorithm_type, root: int = 0, runs: int = 1,
                    engine_type: Engine_type = Engine_type.SINGLE_GPU, orderMethod: OrderMethod = OrderMethod.NATIVE,
                    rootTranfer: bool = True, old2new: Optional[np.ndarray] = None, device: int = 0,
-                   options: Optional[L.Options] = None) -> dict:
+                   options: Optional[L.Options] = None, reorder_files: Optional[dict] = None) -> dict:
     """The SINGLE_GPU branch of main_partition() (main_partition.hpp:319-383).
 
     Returns {"times": per-run ms, "total_run_time_ms": trimmed mean,
     "vertexValue": result} -- the printed ``[Total Run Time]`` and the array
     the reference then hands to checkBinResult.  A root outside [0, V)
     returns without running, as the reference's ``do { if (root < 0 ||
-    root >= vertices) break; ... } while (0)`` does."""
+    root >= vertices) break; ... } while (0)`` does.
+
+    Engine_type.REORDER is the preprocessing branch (:466-487): the graph in
+    IN_DEGREE_DEC order, written to ``reorder_files`` when given; it returns
+    reorder_graph's result."""
+    if engine_type == Engine_type.REORDER:
+        return reorder_graph(csr_result, OrderMethod.IN_DEGREE_DEC, reorder_files, device)
     if engine_type != Engine_type.SINGLE_GPU:
         raise CgbError(L.EUNSUPPORTED, f"Engine_type {Engine_type(engine_type).name} is not provided by this engine "
-                                       "(only the SINGLE_GPU path is rebuilt)")
+                                       "(only the SINGLE_GPU path and the REORDER preprocessing are rebuilt)")
     engine = GraphB200(csr_result, algorithm, device=device, options=options)
     try:
         times = []

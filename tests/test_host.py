@@ -66,3 +66,60 @@ def test_chunglu_weight_offset_matches_twin(oracle):
     top = int(np.diff(off.astype(np.int64)).max())
     assert 0.8 * 3000 < top < 1.25 * 3000
     assert cg.chunglu_weight_offset(V, n, 100) > cg.chunglu_weight_offset(V, n, 3000)
+
+
+def test_reorder_engine_type_writes_the_reference_files(tmp_path, monkeypatch):
+    """main_partition(Engine_type.REORDER) is the reference's preprocessing
+    branch (main_partition.hpp:466-487): the IN_DEGREE_DEC relabelling, written
+    as saveCSR_reorderFile's five files.  The device call is replaced by the
+    oracle's restatement here, so only the host logic is under test."""
+    import cggraph_b200.engine as E
+    from oracle import oracle as O
+
+    off, dst, w = O.rmat_graph(9, 8, seed=4)
+    V = off.size - 1
+
+    class FakeReordered:
+        def __init__(self, method):
+            self.o, self.d, self.w, self.m, self.nz = O.reorder(off, dst, w, int(method))
+
+        def __enter__(self):
+            return self
+
+        def __exit__(self, *exc):
+            return False
+
+        def download(self, with_weight=True):
+            return self.o, self.d, (self.w if with_weight else None)
+
+    class FakeGraph:
+        @classmethod
+        def from_csr(cls, o, d, ww=None, device=0):
+            assert o is off and d is dst and ww is w
+            return cls()
+
+        def __enter__(self):
+            return self
+
+        def __exit__(self, *exc):
+            return False
+
+        def reorder(self, method):
+            h = FakeReordered(method)
+            return h, h.m, h.nz
+
+    monkeypatch.setattr(E, "Graph", FakeGraph)
+    files = {k: str(tmp_path / f"{k}.bin") for k in ("offsets", "dest", "weight", "old2new", "addition")}
+    csr = cg.CSR_Result_type(V, dst.size, off, dst, w)
+    r = cg.main_partition(csr, cg.Algorithm_type.BFS, engine_type=cg.Engine_type.REORDER, reorder_files=files)
+    o2, d2, w2, m2, nz = O.reorder(off, dst, w, 21)
+    np.testing.assert_array_equal(np.fromfile(files["offsets"], np.uint32), o2)
+    np.testing.assert_array_equal(np.fromfile(files["dest"], np.uint32), d2)
+    np.testing.assert_array_equal(np.fromfile(files["weight"], np.uint32), w2)
+    np.testing.assert_array_equal(np.fromfile(files["old2new"], np.uint32), m2)
+    assert np.fromfile(files["addition"], np.uint32).size == 0  # IN_DEGREE_DEC keeps no zero tail
+    assert r["zeroOutDegreeNum"] == V - nz and r["csr"].noZeroOutDegreeNum == nz
+    r = cg.reorder_graph(csr, cg.OrderMethod.MY_BFS_OUT, files)
+    o2, d2, w2, m2, nz = O.reorder(off, dst, w, 16)
+    np.testing.assert_array_equal(np.fromfile(files["old2new"], np.uint32), m2)
+    assert np.fromfile(files["addition"], np.uint32).tolist() == [V - nz]
