@@ -684,12 +684,23 @@ def main_partition(csr_result: CSR_Result_type, algorithm: Algorithm_type, root:
 
     Engine_type.REORDER is the preprocessing branch (:466-487): the graph in
     IN_DEGREE_DEC order, written to ``reorder_files`` when given; it returns
-    reorder_graph's result."""
+    reorder_graph's result.  Engine_type.COMPUTE_INDEGREE (:459-464) returns
+    the degrees and the 100 vertices of largest in-degree."""
     if engine_type == Engine_type.REORDER:
         return reorder_graph(csr_result, OrderMethod.IN_DEGREE_DEC, reorder_files, device)
+    if engine_type == Engine_type.COMPUTE_INDEGREE:
+        # Compute_indegree (Compute_indegree.cuh:114-195): the degrees, and the
+        # 100 vertices of largest in-degree it prints (ties here by id; the
+        # reference's std::sort leaves their order open)
+        off = np.asarray(csr_result.csr_offset, np.int64)
+        outdeg = np.diff(off).astype(np.uint32)
+        indeg = np.bincount(np.asarray(csr_result.csr_dest)[: csr_result.edgeNum],
+                            minlength=csr_result.vertexNum).astype(np.uint32)
+        top = np.lexsort((np.arange(csr_result.vertexNum), -indeg.astype(np.int64)))[:100]
+        return {"inDegree": indeg, "outDegree": outdeg, "top": [(int(v), int(indeg[v])) for v in top]}
     if engine_type != Engine_type.SINGLE_GPU:
         raise CgbError(L.EUNSUPPORTED, f"Engine_type {Engine_type(engine_type).name} is not provided by this engine "
-                                       "(only the SINGLE_GPU path and the REORDER preprocessing are rebuilt)")
+                                       "(only the SINGLE_GPU path and the REORDER / COMPUTE_INDEGREE preprocessing are rebuilt)")
     engine = GraphB200(csr_result, algorithm, device=device, options=options)
     try:
         times = []

@@ -123,3 +123,14 @@ def test_reorder_engine_type_writes_the_reference_files(tmp_path, monkeypatch):
     o2, d2, w2, m2, nz = O.reorder(off, dst, w, 16)
     np.testing.assert_array_equal(np.fromfile(files["old2new"], np.uint32), m2)
     assert np.fromfile(files["addition"], np.uint32).tolist() == [V - nz]
+
+
+def test_compute_indegree_engine_type():
+    """main_partition(Engine_type.COMPUTE_INDEGREE): the degrees and the
+    vertices of largest in-degree (Compute_indegree.cuh:114-195)."""
+    off = np.array([0, 2, 3, 5, 5], np.uint32)
+    dst = np.array([1, 3, 3, 0, 3], np.uint32)
+    csr = cg.CSR_Result_type(4, 5, off, dst, None)
+    r = cg.main_partition(csr, cg.Algorithm_type.BFS, engine_type=cg.Engine_type.COMPUTE_INDEGREE)
+    assert r["inDegree"].tolist() == [1, 1, 0, 3] and r["outDegree"].tolist() == [2, 1, 2, 0]
+    assert r["top"] == [(3, 3), (0, 1), (1, 1), (2, 0)]
