@@ -320,3 +320,27 @@ def test_two_level_partition_oracle_round_robin(oracle):
         j = np.arange(ids.size)
         np.testing.assert_array_equal(r["seg_owner"][ids], (j + j // 3) % 3)
     assert int(r["seg_edges"].astype(np.int64).sum()) == dst.size
+
+
+def overflow_graph():
+    """Distances that cross VertexValue_MAX: a path of weight 4e8 steps, a
+    detour ending exactly below MAX, and an edge of weight 4e9."""
+    edges = sorted([(0, 1, 400000000), (1, 2, 400000000), (2, 3, 400000000), (3, 4, 5), (0, 5, 999999998),
+                    (5, 4, 1), (0, 4, 4000000000)])
+    off = np.zeros(7, np.int64)
+    for u, _, _ in edges:
+        off[u + 1] += 1
+    return (np.cumsum(off).astype(np.uint32), np.array([e[1] for e in edges], np.uint32),
+            np.array([e[2] for e in edges], np.uint32))
+
+
+def test_sssp_overflow_rule_known_answer(oracle):
+    """SSSP lowers a distance only below 999999999: vertex 3 (1.2e9 away),
+    vertex 4 (999999999 via the detour, 4e9 direct) keep 999999999.  The
+    expected values are the reference engine's output on this graph
+    (Graph_Numa through the harness), rerun below when it is built."""
+    off, dst, w = overflow_graph()
+    expect = [0, 400000000, 800000000, VMAX, VMAX, 999999998]
+    assert oracle.sssp(off, dst, w, 0).tolist() == expect
+    if oracle.ref_available():
+        assert oracle.ref_run(off, dst, w, 1, 0)[0].tolist() == expect
