@@ -344,3 +344,25 @@ def test_sssp_overflow_rule_known_answer(oracle):
     assert oracle.sssp(off, dst, w, 0).tolist() == expect
     if oracle.ref_available():
         assert oracle.ref_run(off, dst, w, 1, 0)[0].tolist() == expect
+
+
+def test_toy0_other_roots_known_answers(oracle):
+    """toy_0 from a root without out-edges (2), a root no vertex reaches (10)
+    and one whose reach is partial (11): the reference engine's BFS and SSSP
+    outputs (Graph_Numa through the harness), rerun below when it is built."""
+    g = load_golden("toy_0")
+    off, dst, w = g["offsets"], g["dest"], g["weight"]
+    M = VMAX
+    expect = {
+        (2, 0): [M, M, 0, M, M, M, M, M, M, M, M, M],
+        (2, 1): [M, M, 0, M, M, M, M, M, M, M, M, M],
+        (10, 0): [2, 3, 1, 3, 2, 3, 4, 3, 1, 2, 0, 2],
+        (10, 1): [8, 9, 2, 11, 12, 14, 17, 15, 8, 17, 0, 19],
+        (11, 0): [M, M, 1, M, M, 1, M, 2, M, 2, M, 0],
+        (11, 1): [M, M, 2, M, M, 5, M, 12, M, 14, M, 0],
+    }
+    for (r, alg), e in expect.items():
+        got = oracle.bfs(off, dst, r) if alg == 0 else oracle.sssp(off, dst, w, r)
+        assert got.tolist() == e, (r, alg)
+        if oracle.ref_available():
+            assert oracle.ref_run(off, dst, w, alg, r)[0].tolist() == e, (r, alg)
