@@ -8,7 +8,13 @@ Two independent checkers for the engine's results, never used by the engine:
 * ``_ref/cgref_oracle`` -- the reference's own MULTI_CORE engine
   (Graph_Numa, my_project/CGgraph/GraphNuma.cuh:9-698) built from the reference
   sources by ``build_ref.sh``; it reads the CSR as the three raw files of
-  load_binFile (Basic/Other/IO.hpp:44-92).
+  load_binFile (Basic/Other/IO.hpp:44-92).  Its other modes run the
+  reference's Reorder, edge-list reader and neighbour sort.
+
+The numpy restatements of preprocessing (edge list, neighbour sort, vertex
+orders) are pinned to those modes by fixtures under tests/golden/.  One
+restatement is not: ``two_level_partition`` (parity unpinned), since the
+reference's partitioner needs GPUs to be constructed.
 
 Only tests/, the smoke check and the benchmark's CPU-baseline leg import this.
 """
