@@ -595,6 +595,16 @@ void validate_and_sort(cgb_graph* g)
         if (h[0] & 4u) throw Error{CGB_EFORMAT, "csr_offset[V] != E"};
         throw Error{CGB_EFORMAT, "csr_offset is not non-decreasing"};
     }
+    // the vertices from noZeroOutDegreeNum on hold no edges: csr_offset[nz] == E
+    // (the driver's RCM_LAST_ZERO_OUTDEGREE_check, main_partition.hpp:88-101)
+    if (g->nz < V) {
+        CGB_CUDA_TRY(cudaMemcpyAsync(h.data(), g->off + g->nz, sizeof(uint32_t), cudaMemcpyDeviceToHost, g->stream));
+        CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        if (h[0] != E) {
+            dfree(flags, g->stream);
+            throw Error{CGB_EFORMAT, "a vertex at or above noZeroOutDegreeNum has out-edges (csr_offset[noZeroOutDegreeNum] != E)"};
+        }
+    }
     if (E == 0) {
         dfree(flags, g->stream);
         return;

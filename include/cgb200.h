@@ -132,7 +132,10 @@ typedef struct cgb_iter_trace {
  * offsets[V] == E, dest[e] < V; neighbour lists are sorted by dest on the
  * device (weights follow, as nbrSort_taskSteal does) and must then be
  * strictly ascending (no duplicate edges).  weight may be NULL (SSSP then
- * uses weight 1).  no_zero_out_degree_num = 0 means V.  V and E are at
+ * uses weight 1).  no_zero_out_degree_num = 0 means V; the vertices from it
+ * on must have no out-edges, offsets[no_zero_out_degree_num] == E (the
+ * driver's RCM_LAST_ZERO_OUTDEGREE_check, main_partition.hpp:88-101), else
+ * CGB_EFORMAT.  V and E are at
  * most 2^32 - 2^24 (CGB_EUNSUPPORTED beyond; the reference's uint32 count types
  * end at 2^32 - 1).  The caller keeps ownership of its arrays.  Replaces GraphDeviceWorklist's constructor and
  * csrToDevice() (GraphDevice.cuh:48-71,208-221). */

@@ -382,6 +382,10 @@ def test_zero_out_degree_tail(oracle):
     w = rng.integers(1, 64, dst.size).astype(np.uint32)
     assert off[nz] == dst.size
     check_all(oracle, off, dst, w, [0, 1999], noZeroOutDegreeNum=nz)
+    # edges at or above noZeroOutDegreeNum are refused, as the driver's check refuses them
+    with pytest.raises(CgbError) as ei:
+        cg.Graph.from_csr(off, dst, w, noZeroOutDegreeNum=1000)
+    assert ei.value.status == L.EFORMAT
 
 
 def test_missing_weights_mean_unit_weights(oracle):
