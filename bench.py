@@ -159,10 +159,16 @@ def load_peaks() -> dict:
 
 # ------------------------------------------------------------------ dist
 class Dist:
+    """One process per GPU (torchrun); replicas only, so the collectives are
+    the barrier and the max / sum reductions of cggraph_b200.replicas."""
+
     def __init__(self, want_gpus: int):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        if want_gpus != self.world:
+            raise SystemExit(f"--gpus {want_gpus} but WORLD_SIZE={self.world}: launch one process per GPU with "
+                             f"python -m torch.distributed.run --nproc-per-node {want_gpus} bench.py --gpus {want_gpus}")
         self.pg = False
         if self.world > 1:
             import torch
@@ -172,24 +178,37 @@ class Dist:
                                     device_id=torch.device("cuda", self.local))
             self.pg = True
 
+    def shard(self, items):
+        from cggraph_b200.replicas import shard
+        return shard(items, self.rank, self.world)
+
     def barrier(self):
         if self.pg:
             import torch.distributed as dist
             dist.barrier(device_ids=[self.local])
 
     def reduce(self, x: float, op: str) -> float:
-        if not self.pg:
-            return float(x)
-        import torch
-        import torch.distributed as dist
-        t = torch.tensor([float(x)], dtype=torch.float64, device=f"cuda:{self.local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
-        return float(t.item())
+        from cggraph_b200.replicas import max_over_ranks, sum_over_ranks
+        dev = f"cuda:{self.local}" if self.pg else None
+        return max_over_ranks(x, dev) if op == "max" else sum_over_ranks(x, dev)
 
     def close(self):
         if self.pg:
             import torch.distributed as dist
             dist.destroy_process_group()
+
+
+def workload_config(args, V, Ed, Es, roots, algs) -> dict:
+    """The workload both arms run (the same dict in each arm's JSON line)."""
+    return {"workload": f"rmat{args.scale}_ef{args.edge_factor}_"
+                        + "_".join(ALG_NAMES[a] for a in algs).replace("pagerank", f"pr{args.pr_iters}"),
+            "scale": args.scale, "edge_factor": args.edge_factor, "rmat_abc": [0.57, 0.19, 0.19],
+            "seed": args.seed, "vertices": V, "edges_directed": Ed, "edges_symmetrised": Es,
+            "weights": "uniform [1,64]", "roots": roots, "pr_iterations": args.pr_iters,
+            "algorithms": [ALG_NAMES[a] for a in algs],
+            "cc": "components of the symmetrised graph",
+            "l2": "inputs larger than L2 (directed CSR %.2f GB)" % ((4 * (V + 1) + 8 * Ed) / 1e9),
+            "parallelism": f"replicas x{args.gpus}"}
 
 
 # ---------------------------------------------------------------- our arm
@@ -198,14 +217,26 @@ def parse_algs(spec: str) -> list:
     return sorted({names[a.strip().lower()] for a in spec.split(",") if a.strip()})
 
 
-def run_step(gd, gs, root, opts, pr_iters, algs=(BFS, SSSP, CC, PR)):
-    """One step on resident graphs; returns [(algorithm, run stats)]."""
+def run_step(gd, root, opts, cc_opts, pr_iters, algs=(BFS, SSSP, CC, PR)):
+    """One step on the resident graph; returns [(algorithm, run stats)].  CC
+    runs as weak components of the directed graph (CGB_FLAG_CC_WEAK): the
+    labels of CC on the symmetrised graph, with no symmetrised copy."""
     out = []
     for alg in algs:
-        g, arg = {BFS: (gd, root), SSSP: (gd, root), CC: (gs, 0), PR: (gd, pr_iters)}[alg]
-        g.run(alg, arg, opts, to_host=False)
-        out.append((alg, g.stats()))
+        arg = {BFS: root, SSSP: root, CC: 0, PR: pr_iters}[alg]
+        gd.run(alg, arg, cc_opts if alg == CC else opts, to_host=False)
+        out.append((alg, gd.stats()))
     return out
+
+
+def symmetrised_edges(cg, args, dev, keep_host=False):
+    """Edge count of the symmetrised graph (the CC numerator), from the
+    device generator; with keep_host, also its CSR in host memory."""
+    gs = cg.Graph.rmat(args.scale, args.edge_factor, args.seed, symmetrise=True, wmax=0, device=dev)
+    Es = gs.edgeNum
+    host = gs.download(with_weight=False)[:2] if keep_host else None
+    gs.close()
+    return Es, host
 
 
 def bench_cgb200(args, d: Dist):
@@ -216,18 +247,15 @@ def bench_cgb200(args, d: Dist):
     dev = d.local
     torch.cuda.set_device(dev)
     algs = parse_algs(args.algorithms)
+    Es, sym_host = symmetrised_edges(cg, args, dev, keep_host=d.world == 1 and not args.no_cpu_baseline)
     gd = cg.Graph.rmat(args.scale, args.edge_factor, args.seed, wmax=64, device=dev)
-    gs = cg.Graph.rmat(args.scale, args.edge_factor, args.seed, symmetrise=True, wmax=0, device=dev) \
-        if CC in algs else None
     off_h, dst_h, w_h = gd.download()
     roots_all = pick_roots(off_h, args.seed, N_ROOTS * d.world)
-    roots = roots_all[d.rank::d.world]
-    V, Ed, Es = gd.vertexNum, gd.edgeNum, (gs.edgeNum if gs else 0)
+    roots = d.shard(roots_all)
+    V, Ed = gd.vertexNum, gd.edgeNum
 
     stream = torch.cuda.current_stream()
-    for g in (gd, gs):
-        if g is not None:
-            g.set_stream(stream)
+    gd.set_stream(stream)
     sched = L.SCHED_LEARNED if args.schedule == "learned" else L.SCHED_HEURISTIC
     if args.schedule == "learned":
         from cggraph_b200 import policy
@@ -235,20 +263,22 @@ def bench_cgb200(args, d: Dist):
             raise SystemExit("--schedule learned: no trained policy (python -m cggraph_b200.train_policy)")
     warm_opts = cg.make_options(schedule=sched)
     timed_opts = cg.make_options(schedule=sched, flags=L.FLAG_KERNEL_TIMING)
+    warm_cc = cg.make_options(schedule=sched, flags=L.FLAG_CC_WEAK)
+    timed_cc = cg.make_options(schedule=sched, flags=L.FLAG_KERNEL_TIMING | L.FLAG_CC_WEAK)
 
     # launch parameters: the project's autotuner, per algorithm, before timing
     autotune = None
     if not args.no_autotune:
         autotune = {}
         tune_roots = pick_roots(off_h, args.seed + 13, 4)  # not the timed roots
-        for alg, g, rts in ((BFS, gd, tune_roots), (SSSP, gd, tune_roots), (CC, gs, [0]), (PR, gd, [5, 5])):
-            if alg in algs and g is not None:
-                best, bms, sms = g.autotune(alg, rts)
+        for alg, rts in ((BFS, tune_roots), (SSSP, tune_roots), (CC, [0]), (PR, [5, 5])):
+            if alg in algs:
+                best, bms, sms = gd.autotune(alg, rts, cc_weak=alg == CC)
                 autotune[ALG_NAMES[alg]] = {"default_ms": sms, "tuned_ms": bms, "speedup": sms / bms,
                                             "tuning": best}
 
     for i in range(args.warmup):
-        run_step(gd, gs, roots[i % len(roots)], warm_opts, args.pr_iters, algs)
+        run_step(gd, roots[i % len(roots)], warm_opts, warm_cc, args.pr_iters, algs)
 
     clocks = Clocks(dev)
     clocks.start()
@@ -265,8 +295,9 @@ def bench_cgb200(args, d: Dist):
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     for k in range(args.steps):
-        for alg, st in run_step(gd, gs, roots[k % len(roots)], timed_opts, args.pr_iters, algs):
-            per_alg_edges[alg] += st.traversed_edges
+        for alg, st in run_step(gd, roots[k % len(roots)], timed_opts, timed_cc, args.pr_iters, algs):
+            # CC: the edges of the symmetrised graph, whose components it computes
+            per_alg_edges[alg] += Es if alg == CC else st.traversed_edges
             per_alg_ms[alg] += st.ms
             launches += st.launches
             for c in range(8):
@@ -316,24 +347,23 @@ def bench_cgb200(args, d: Dist):
     # end to end through the C ABI with pinned host buffers
     e2e = None
     if not args.no_e2e and full:
-        e2e = bench_e2e(args, d, cg, gd, gs, roots, off_h, dst_h, w_h, sched)
+        e2e = bench_e2e(args, d, cg, gd, roots, off_h, dst_h, w_h, Es, sched)
 
     # CPU baseline: the reference's own engine on this host (rank 0, N = 1)
     cpu = None
     if d.world == 1 and not args.no_cpu_baseline and full:
         try:
-            cpu = cpu_baseline(args, gd, gs, off_h, dst_h, w_h, roots)
+            cpu = cpu_baseline(args, V, Ed, Es, off_h, dst_h, w_h, sym_host, roots)
         except Exception as e:  # reported, not fatal
             cpu = {"value": None, "error": str(e)[-300:]}
+    sym_host = None
 
     batching = None
     if d.world == 1 and not args.no_batching and (BFS in algs or SSSP in algs):
         batching = bench_batching(args, cg, L, gd, roots, dev)
 
-    for g in (gd, gs):
-        if g is not None:
-            g.set_stream(None)
-            g.close()
+    gd.set_stream(None)
+    gd.close()
     serving = None
     if d.world == 1 and not args.no_serving and (BFS in algs or SSSP in algs):
         serving = bench_serving(args, cg, L, dev)
@@ -344,17 +374,11 @@ def bench_cgb200(args, d: Dist):
         "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": d.world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32 (BFS/SSSP/CC), f64 (PageRank)",
-        "data": "synthetic (seeded RMAT, generated on device)",
-        "config": {"workload": f"rmat{args.scale}_ef{args.edge_factor}_"
-                               + "_".join(ALG_NAMES[a] for a in algs).replace("pagerank", f"pr{args.pr_iters}"),
-                   "scale": args.scale, "edge_factor": args.edge_factor, "rmat_abc": [0.57, 0.19, 0.19],
-                   "vertices": V, "edges_directed": Ed, "edges_symmetrised": Es, "weights": "uniform [1,64]",
-                   "roots": roots, "schedule": args.schedule, "pr_iterations": args.pr_iters,
+        "data": "synthetic (seeded RMAT)",
+        "config": workload_config(args, V, Ed, Es, roots_all, algs),
+        "engine": {"schedule": args.schedule, "roots_this_rank": roots,
                    "launch_parameters": "default" if args.no_autotune else "cgb_autotune per algorithm (untimed)",
-                   "algorithms": [ALG_NAMES[a] for a in algs],
-                   "l2": "inputs larger than L2 (directed CSR %.2f GB, symmetrised %.2f GB)"
-                         % ((4 * (V + 1) + 8 * Ed) / 1e9, (4 * (V + 1) + 4 * Es) / 1e9),
-                   "parallelism": f"replicas x{d.world}"},
+                   "cc": "weak components of the directed graph (CGB_FLAG_CC_WEAK)"},
         "per_algorithm": per_alg,
         "schedules": schedules,
         "autotune": autotune,
@@ -591,61 +615,47 @@ def bench_serving(args, cg, L, dev):
 E2E_POOL_HEADROOM = 32 << 30  # bytes added to the pool before the e2e steps
 
 
-def bench_e2e(args, d, cg, gd, gs, roots, off_h, dst_h, w_h, sched):
+def bench_e2e(args, d, cg, gd, roots, off_h, dst_h, w_h, Es, sched):
     import torch
+    from cggraph_b200 import _lib as L
     V = gd.vertexNum
-    soff_h, sdst_h, _ = gs.download(with_weight=False)
     pin = lambda a: torch.from_numpy(a.view(np.int32)).pin_memory()  # noqa: E731
     t_off, t_dst, t_w = pin(off_h), pin(dst_h), pin(w_h)
-    t_soff, t_sdst = pin(soff_h), pin(sdst_h)
     out_b = torch.empty(V, dtype=torch.int32).pin_memory()
     out_s = torch.empty(V, dtype=torch.int32).pin_memory()
     out_c = torch.empty(V, dtype=torch.int32).pin_memory()
     out_p = torch.empty(V, dtype=torch.float64).pin_memory()
     opts = cg.make_options(schedule=sched)
+    cc_opts = cg.make_options(schedule=sched, flags=L.FLAG_CC_WEAK)
     steps = args.e2e_steps or args.steps
 
     def step(root):
-        # The host-to-device link is the step's serial resource, so uploads go
-        # back to back while the GPU computes, the smallest last: the directed
-        # CSR's structure first; then, on a second host thread, the
-        # symmetrised graph (an independent graph with its own stream) while
-        # BFS and PageRank run, and the directed weights (only SSSP reads
-        # them; cgb_graph_set_weights) while CC runs.  SSSP is all that
-        # follows the last upload.
+        # The host-to-device link is the step's serial resource.  The graph's
+        # structure goes first; a second host thread then uploads the weights
+        # (only SSSP reads them; cgb_graph_set_weights) while BFS, PageRank and
+        # CC (weak components of the directed graph) run; SSSP follows.
         box = {}
-        sym_in, weights_in = threading.Event(), threading.Event()
+        weights_in = threading.Event()
         g = cg.Graph.from_csr(t_off, t_dst, None, vertexNum=V, edgeNum=gd.edgeNum, device=d.local)
 
-        def uploads():
+        def upload_weights():
             try:
-                box["h"] = cg.Graph.from_csr(t_soff, t_sdst, None, vertexNum=V, edgeNum=gs.edgeNum, device=d.local)
+                g.set_weights(t_w)
             except BaseException as e:  # re-raised on the main thread
-                box["error"] = e
-            finally:
-                sym_in.set()
-            try:
-                if "error" not in box:
-                    g.set_weights(t_w)
-            except BaseException as e:
                 box["error"] = e
             finally:
                 weights_in.set()
 
         edges = 0
-        th = threading.Thread(target=uploads)
+        th = threading.Thread(target=upload_weights)
         th.start()
         try:
             g.run(BFS, root, opts, out=out_b)
             edges += g.stats().traversed_edges
             g.run(PR, args.pr_iters, opts, out=out_p)
             edges += g.stats().traversed_edges
-            sym_in.wait()
-            if "h" in box:
-                h = box["h"]
-                h.run(CC, 0, opts, out=out_c)
-                edges += h.stats().traversed_edges
-                h.close()
+            g.run(CC, 0, cc_opts, out=out_c)
+            edges += Es
             weights_in.wait()
             if "error" not in box:
                 g.run(SSSP, root, opts, out=out_s)
@@ -657,8 +667,8 @@ def bench_e2e(args, d, cg, gd, gs, roots, off_h, dst_h, w_h, sched):
             raise box["error"]
         return edges
 
-    # The pool is grown once, up front, to hold both graphs of a step at their
-    # peak (as a long-running process would): growing it costs driver time.
+    # The pool is grown once, up front, to hold a step's graph at its peak
+    # (as a long-running process would): growing it costs driver time.
     r0, _ = cg.memory_info(d.local)
     cg.memory_reserve(r0 + E2E_POOL_HEADROOM, d.local)
     for k in range(max(1, args.warmup)):  # warm-up: pinned pages touched, layouts of the same size cached
@@ -678,17 +688,15 @@ def bench_e2e(args, d, cg, gd, gs, roots, off_h, dst_h, w_h, sched):
     d.barrier()
     s_max = d.reduce(t1 - t0, "max")
     edges = d.reduce(edges, "sum")
-    h2d = 4 * (V + 1) + 8 * gd.edgeNum + 4 * (V + 1) + 4 * gs.edgeNum
+    h2d = 4 * (V + 1) + 8 * gd.edgeNum
     d2h = 4 * V * 3 + 8 * V
     return {"value": edges / s_max / 1e9, "unit": "GTEPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
             "ms_per_step": s_max * 1e3 / steps, "steps": steps,
             "step_ms": [round((b - a) * 1e3, 1) for a, b in zip(marks, marks[1:])],
             "pool_reserved_gb_after_step": pool_gb,
-            "what": "cgb_graph_create(directed CSR structure, host pinned) + BFS + PR(20) -> host; "
-                    "a second host thread, started once that structure is uploaded, uploads the symmetrised "
-                    "CSR (cgb_graph_create) and then the directed weights (cgb_graph_set_weights); "
-                    "CC on the symmetrised graph and SSSP -> host once their uploads are in; destroy; "
-                    "wall clock"}
+            "what": "cgb_graph_create(directed CSR structure, host pinned) + BFS + PR(20) + CC (weak components) "
+                    "-> host while a second host thread uploads the weights (cgb_graph_set_weights); SSSP -> host "
+                    "once they are in; destroy; wall clock"}
 
 
 def write_csr_files(dirpath, prefix, off, dst, w):
@@ -702,17 +710,16 @@ def write_csr_files(dirpath, prefix, off, dst, w):
     return paths
 
 
-def cpu_baseline(args, gd, gs, off_h, dst_h, w_h, roots):
+def cpu_baseline(args, V, Ed, Es, off_h, dst_h, w_h, sym_host, roots):
     from oracle import oracle as O
     if not O.ref_available():
         return {"value": None, "unit": "GTEPS", "error": "reference harness oracle/_ref/cgref_oracle not built"}
     threads = os.cpu_count() or 1
-    soff, sdst, _ = gs.download(with_weight=False)
+    soff, sdst = sym_host
     tmp = "/dev/shm" if os.path.isdir("/dev/shm") else None
     with tempfile.TemporaryDirectory(dir=tmp) as dd:
         pd = write_csr_files(dd, "d", off_h, dst_h, w_h)
         ps = write_csr_files(dd, "s", soff, sdst, None)
-        V, Ed, Es = gd.vertexNum, gd.edgeNum, gs.edgeNum
         r3 = roots[:3]
         ib = O.ref_run_files(pd, V, Ed, 0, r3, len(r3), threads)
         isp = O.ref_run_files(pd, V, Ed, 1, r3, len(r3), threads)
@@ -735,33 +742,30 @@ def cpu_baseline(args, gd, gs, off_h, dst_h, w_h, roots):
 
 
 # ------------------------------------------------------------ reference arm
-def bench_reference(args, d: Dist):
+def bench_reference(args):
     """The reference's own CPU implementation (Graph_Numa, built from the
     reference sources into oracle/_ref) on this host's cores, same workload
     and metric.  PageRank uses the FP64 OpenMP port because the reference's
-    PageRank does not build.  Input synthesis (the seeded RMAT CSR) is done
-    before any timing."""
-    if d.rank != 0:
-        return None
+    PageRank does not build.  The input (the seeded RMAT CSR and its
+    symmetrised copy, which the reference's CC needs) is made before any
+    timing by the oracle's CPU twin of the generator, so nothing of the
+    engine is loaded in this arm."""
     from oracle import oracle as O
     if not O.ref_available():
         return {"impl": "reference", "unavailable": "reference harness oracle/_ref/cgref_oracle was not built"}
-    import cggraph_b200 as cg
     threads = os.cpu_count() or 1
-    gd = cg.Graph.rmat(args.scale, args.edge_factor, args.seed, wmax=64, device=d.local)
-    gs = cg.Graph.rmat(args.scale, args.edge_factor, args.seed, symmetrise=True, wmax=0, device=d.local)
-    off_h, dst_h, w_h = gd.download()
-    soff, sdst, _ = gs.download(with_weight=False)
-    V, Ed, Es = gd.vertexNum, gd.edgeNum, gs.edgeNum
-    gd.close()
-    gs.close()
-    roots = pick_roots(off_h, args.seed, N_ROOTS)
+    algs = [BFS, SSSP, CC, PR]
+    off_h, dst_h, w_h = O.rmat_graph(args.scale, args.edge_factor, args.seed, wmax=64)
+    soff, sdst, _ = O.rmat_graph(args.scale, args.edge_factor, args.seed, symmetrise=True, wmax=0)
+    V, Ed, Es = off_h.size - 1, dst_h.size, sdst.size
+    roots_all = pick_roots(off_h, args.seed, N_ROOTS * args.gpus)
     n = args.warmup + args.steps
-    seq = [roots[i % len(roots)] for i in range(n)]
+    seq = [roots_all[i % len(roots_all)] for i in range(n)]
     tmp = "/dev/shm" if os.path.isdir("/dev/shm") else None
     with tempfile.TemporaryDirectory(dir=tmp) as dd:
         pd = write_csr_files(dd, "d", off_h, dst_h, w_h)
         ps = write_csr_files(dd, "s", soff, sdst, None)
+        del soff, sdst
         ib = O.ref_run_files(pd, V, Ed, 0, seq, n, threads)
         isp = O.ref_run_files(pd, V, Ed, 1, seq, n, threads)
         ic = O.ref_run_files(ps, V, Es, 2, [0], n, threads)
@@ -776,13 +780,11 @@ def bench_reference(args, d: Dist):
     ms = sum(ib["ms"][w:]) + sum(isp["ms"][w:]) + sum(ic["ms"][w:]) + sum(pr_ms[w:])
     value = edges / (ms / 1e3) / 1e9
     return {
-        "metric": METRIC, "value": value, "unit": "GTEPS", "impl": "reference", "n_gpus": d.world,
+        "metric": METRIC, "value": value, "unit": "GTEPS", "impl": "reference", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32 (BFS/SSSP/CC), f64 (PageRank)",
         "data": "synthetic (seeded RMAT)",
-        "config": {"workload": f"rmat{args.scale}_ef{args.edge_factor}_bfs_sssp_cc_pr{args.pr_iters}",
-                   "scale": args.scale, "edge_factor": args.edge_factor, "vertices": V, "edges_directed": Ed,
-                   "edges_symmetrised": Es, "roots": roots, "pr_iterations": args.pr_iters},
+        "config": workload_config(args, V, Ed, Es, roots_all, algs),
         "per_algorithm": {
             "bfs": sum(ib["edges"][w:]) / (sum(ib["ms"][w:]) / 1e3) / 1e9,
             "sssp": sum(isp["edges"][w:]) / (sum(isp["ms"][w:]) / 1e3) / 1e9,
@@ -797,12 +799,14 @@ def bench_reference(args, d: Dist):
 
 def main():
     args = parse_args()
+    if args.impl == "reference":
+        # CPU only: under torchrun rank 0 alone runs it, the other ranks exit at once
+        if int(os.environ.get("RANK", "0")) == 0:
+            print(json.dumps(bench_reference(args)), flush=True)
+        return
     d = Dist(args.gpus)
     try:
-        if args.impl == "reference":
-            res = bench_reference(args, d)
-        else:
-            res = bench_cgb200(args, d)
+        res = bench_cgb200(args, d)
         if d.rank == 0 and res is not None:
             print(json.dumps(res), flush=True)
     finally:

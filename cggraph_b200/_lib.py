@@ -21,7 +21,7 @@ STATUS_NAMES = ["CGB_OK", "CGB_EINVAL", "CGB_EFORMAT", "CGB_EIO", "CGB_ENOMEM", 
 # cgb_schedule / cgb_variant / flags / kernel classes
 SCHED_HEURISTIC, SCHED_LEARNED, SCHED_FIXED = 0, 1, 2
 VAR_AUTO, VAR_TWC, VAR_PULL, VAR_PUSH, VAR_DENSE = 0, 1, 2, 3, 4
-FLAG_KERNEL_TIMING, FLAG_TRACE, FLAG_BATCH_SEQUENTIAL = 0x1, 0x2, 0x4
+FLAG_KERNEL_TIMING, FLAG_TRACE, FLAG_BATCH_SEQUENTIAL, FLAG_CC_WEAK = 0x1, 0x2, 0x4, 0x8
 K_PUSH, K_PULL, K_PR, K_HOOK, K_COMPRESS, K_FRONTIER, K_INIT, K_OTHER = range(8)
 KERNEL_CLASS_NAMES = ["push", "pull", "pagerank", "hook", "compress", "frontier", "init", "other"]
 
@@ -124,7 +124,7 @@ class Tuning(ctypes.Structure):
     ]
 
 
-TUNE_BATCH, TUNE_KEEP_DEFAULT = 0x1, 0x2
+TUNE_BATCH, TUNE_KEEP_DEFAULT, TUNE_CC_WEAK = 0x1, 0x2, 0x4
 TUNING_FIELDS = ("push_big_deg", "push_chunk", "push_ctas_per_sm", "persist_enter", "persist_deg", "ms_edges",
                  "pr_unroll", "pr_ctas_per_sm", "persist_ctas", "sssp_pull_alpha",
                  "cluster_enter", "sssp_dense_alpha")

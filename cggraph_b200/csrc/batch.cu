@@ -136,7 +136,7 @@ static void enqueue_batch_run(cgb_batch* b, int alg)
     PersistState* st = static_cast<PersistState*>(g->persist);
     uint32_t* far_bm = alg == 1 ? g->front_bm : nullptr;
     CGB_CUDA_TRY(cudaMemsetAsync(st, 0, sizeof(PersistState), g->stream));
-    k_batch_init<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, g->value, g->visited, words, far_bm,
+    k_batch_init<<<grid_for(V, kBlock, num_sms() * 8), kBlock, 0, g->stream>>>(V, g->value, g->visited, words, far_bm,
                                                                              g->aux_bm + words);
     k_batch_roots<<<1, 1, 0, g->stream>>>(b->d_roots, b->d_base, b->n, g->nz, g->value, g->visited, g->q[0], st,
                                           alg == 1 ? b->sx : nullptr, b->delta);
@@ -183,11 +183,11 @@ cgb_status cgb_batch_create(uint32_t n, const uint32_t* const* offsets, const ui
                     tmp_cap = need;
                 }
                 CGB_CUDA_TRY(cudaMemcpyAsync(tmp, offsets[i], ((size_t)Vs[i] + 1) * 4, cudaMemcpyDefault, g->stream));
-                k_union_off<<<grid_for(Vs[i], kBlock, kNumSMs * 4), kBlock, 0, g->stream>>>(tmp, Vs[i], Es[i], (uint32_t)eb,
+                k_union_off<<<grid_for(Vs[i], kBlock, num_sms() * 4), kBlock, 0, g->stream>>>(tmp, Vs[i], Es[i], (uint32_t)eb,
                                                                                            g->off + vb, bad);
                 if (Es[i]) {
                     CGB_CUDA_TRY(cudaMemcpyAsync(tmp, dests[i], (size_t)Es[i] * 4, cudaMemcpyDefault, g->stream));
-                    k_union_dst<<<grid_for(Es[i], kBlock, kNumSMs * 4), kBlock, 0, g->stream>>>(tmp, Es[i], Vs[i],
+                    k_union_dst<<<grid_for(Es[i], kBlock, num_sms() * 4), kBlock, 0, g->stream>>>(tmp, Es[i], Vs[i],
                                                                                                 (uint32_t)vb,
                                                                                                 g->dst + eb, bad);
                     if (g->w) {
@@ -195,7 +195,7 @@ cgb_status cgb_batch_create(uint32_t n, const uint32_t* const* offsets, const ui
                             CGB_CUDA_TRY(cudaMemcpyAsync(g->w + eb, weights[i], (size_t)Es[i] * 4, cudaMemcpyDefault,
                                                          g->stream));
                         else
-                            k_fill_ones<<<grid_for(Es[i], kBlock, kNumSMs * 4), kBlock, 0, g->stream>>>(Es[i], g->w + eb);
+                            k_fill_ones<<<grid_for(Es[i], kBlock, num_sms() * 4), kBlock, 0, g->stream>>>(Es[i], g->w + eb);
                     }
                 }
                 CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));  // tmp is reused
@@ -271,7 +271,7 @@ cgb_status cgb_batch_run(cgb_batch* b, int algorithm, const uint32_t* roots, uin
             o.struct_size = sizeof(o);
             CGB_CUDA_TRY(cudaMemsetAsync(g->ctr, 0, sizeof(DevCounters), g->stream));
             run_cc(g, o);  // records ev_start itself
-            k_batch_local_labels<<<grid_for(g->V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(g->V, b->d_base, b->n,
+            k_batch_local_labels<<<grid_for(g->V, kBlock, num_sms() * 8), kBlock, 0, g->stream>>>(g->V, b->d_base, b->n,
                                                                                                 g->value);
         } else {
             CGB_REQUIRE(roots != nullptr, CGB_EINVAL, "roots is NULL");

@@ -202,7 +202,7 @@ void run_bfs(cgb_graph* g, uint32_t root, const cgb_options& o)
     CGB_CUDA_TRY(cudaEventRecord(g->ev_start, g->stream));
     if (timing) ktimer_begin(g, CGB_K_INIT);
     ++g->stats.launches;
-    k_bfs_init<<<kNumSMs * 4, kBlock, 0, g->stream>>>(V, g->value, g->visited, words);
+    k_bfs_init<<<num_sms() * 4, kBlock, 0, g->stream>>>(V, g->value, g->visited, words);
     ++g->stats.launches;
     k_bfs_root<<<1, 1, 0, g->stream>>>(g->value, g->visited, root, g->q[0]);
     if (timing) ktimer_end(g);
@@ -233,11 +233,11 @@ void run_bfs(cgb_graph* g, uint32_t root, const cgb_options& o)
                 if (timing) ktimer_begin(g, CGB_K_FRONTIER);
                 CGB_CUDA_TRY(cudaMemsetAsync(front, 0, words * sizeof(uint32_t), g->stream));
                 ++g->stats.launches;
-                k_q2bm<<<grid_for(nf, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(g->q[cur], (uint32_t)nf, front);
+                k_q2bm<<<grid_for(nf, kBlock, num_sms() * 8), kBlock, 0, g->stream>>>(g->q[cur], (uint32_t)nf, front);
                 if (timing) ktimer_end(g);
             }
             if (timing) ktimer_begin(g, CGB_K_PULL);
-            const uint32_t grid = grid_for((uint64_t)words * 32, kBlock, kNumSMs * 16);
+            const uint32_t grid = grid_for((uint64_t)words * 32, kBlock, num_sms() * 16);
             ++g->stats.launches;
             k_bfs_bu<<<grid, kBlock, 0, g->stream>>>(V, g->in_off, g->in_src, g->off, g->value, g->visited, front,
                                                      next, level + 1, g->nz, g->q[out], &g->ctr->qlen[out], V,

@@ -432,7 +432,7 @@ cgb_status cgb_run_batch(cgb_graph* g, int algorithm, const uint32_t* roots, uin
                 iters += g->stats.iterations;
                 launches += g->stats.launches;
                 CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->reached_edges, 0, 8, g->stream));
-                k_batch_reached<<<kNumSMs * 8, kBlock, 0, g->stream>>>((uint64_t)n * V, (uint32_t)V, lv, g->off, g->ctr);
+                k_batch_reached<<<num_sms() * 8, kBlock, 0, g->stream>>>((uint64_t)n * V, (uint32_t)V, lv, g->off, g->ctr);
                 sync_counters(g);
                 edges += g->h_ctr->reached_edges;
                 if (out_u32 && !dev_out)

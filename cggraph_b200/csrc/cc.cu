@@ -27,6 +27,16 @@
 // holds throughout and each final root is its component's minimum id.
 //
 // Directed graphs: the reference's own label propagation, frontier-driven.
+//
+// Weak components (CGB_FLAG_CC_WEAK): the same hooking over the edges taken
+// as undirected, read from both the CSR (out-lists) and the CSC (in-lists),
+// both sorted.  The labels equal the reference's CC run on the symmetrised
+// graph, without a symmetrised copy of the graph: step 1 points v at the
+// smallest of its first out- and in-neighbour, step 2 links v with the first
+// two of each list, step 4 links the remaining out- and in-edges of every
+// vertex outside the giant component.  An edge u -> v is skipped only when
+// both u (its out-list) and v (its in-list) were found in the giant
+// component, and then it joins nothing new.
 #include "engine.cuh"
 #include "push.cuh"
 
@@ -141,6 +151,39 @@ __global__ void k_cc_init_min_nbr(uint32_t V, const uint32_t* __restrict__ off, 
     }
 }
 
+// Weak components: comp[v] = min(v, smallest out-neighbour, smallest
+// in-neighbour).
+__global__ void k_cc_init_min_nbr_weak(uint32_t V, const uint32_t* __restrict__ off,
+                                       const uint32_t* __restrict__ dst, const uint32_t* __restrict__ in_off,
+                                       const uint32_t* __restrict__ in_src, uint32_t* comp)
+{
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+        const uint32_t s = off[v], is = in_off[v];
+        uint32_t c = v;
+        if (off[v + 1] > s) c = min(c, dst[s]);
+        if (in_off[v + 1] > is) c = min(c, in_src[is]);
+        comp[v] = c;
+    }
+}
+
+// Weak components: links v with the first two entries of its out- and
+// in-list, except the one k_cc_init_min_nbr_weak already pointed it at.
+__global__ void k_cc_link_round_weak(uint32_t V, const uint32_t* __restrict__ off, const uint32_t* __restrict__ dst,
+                                     const uint32_t* __restrict__ in_off, const uint32_t* __restrict__ in_src,
+                                     uint32_t* comp, DevCounters* ctr)
+{
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+        const uint32_t s = off[v], d = off[v + 1] - s;
+        const uint32_t is = in_off[v], id = in_off[v + 1] - is;
+        const uint32_t o0 = d > 0 ? dst[s] : v, i0 = id > 0 ? in_src[is] : v;
+        const uint32_t init = min(v, min(o0, i0));
+        if (o0 != init) link(v, o0, comp, ctr);
+        if (i0 != init && i0 != o0) link(v, i0, comp, ctr);
+        if (d > 1) link(v, dst[s + 1], comp, ctr);
+        if (id > 1) link(v, in_src[is + 1], comp, ctr);
+    }
+}
+
 // Links v with its r-th neighbour; with `first_up` also with its first
 // neighbour when that one is larger than v (the min-neighbour
 // initialisation only covered edge 0 when it pointed down).
@@ -252,7 +295,9 @@ __global__ void k_zero(uint32_t n, uint32_t* a)
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = 0;
 }
 
-static void cc_afforest(cgb_graph* g)
+// Afforest over the out-lists (symmetric graphs), or over the out- and
+// in-lists (weak components of any graph).
+static void cc_afforest(cgb_graph* g, bool weak)
 {
     const bool timing = g->flags & CGB_FLAG_KERNEL_TIMING;
     const uint32_t V = g->V;
@@ -262,14 +307,21 @@ static void cc_afforest(cgb_graph* g)
 
     if (timing) ktimer_begin(g, CGB_K_INIT);
     ++g->stats.launches;
-    k_cc_init_min_nbr<<<grid, kBlock, 0, g->stream>>>(V, g->off, g->dst, g->value);
+    if (weak)
+        k_cc_init_min_nbr_weak<<<grid, kBlock, 0, g->stream>>>(V, g->off, g->dst, g->in_off, g->in_src, g->value);
+    else
+        k_cc_init_min_nbr<<<grid, kBlock, 0, g->stream>>>(V, g->off, g->dst, g->value);
     CGB_CUDA_TRY(cudaMemsetAsync(g->ctr, 0, sizeof(DevCounters), g->stream));
     if (timing) ktimer_end(g);
     // no compress here: the link round's finds halve the init forest's paths
     for (uint32_t r = 1; r < kRounds; r++) {
         if (timing) ktimer_begin(g, CGB_K_HOOK);
         ++g->stats.launches;
-        k_cc_link_round<<<grid, kBlock, 0, g->stream>>>(V, g->off, g->dst, g->value, r, r == 1, g->ctr);
+        if (weak)
+            k_cc_link_round_weak<<<grid, kBlock, 0, g->stream>>>(V, g->off, g->dst, g->in_off, g->in_src, g->value,
+                                                                 g->ctr);
+        else
+            k_cc_link_round<<<grid, kBlock, 0, g->stream>>>(V, g->off, g->dst, g->value, r, r == 1, g->ctr);
         if (timing) ktimer_end(g);
     }
     // no compress here either: sampling and the final link find roots themselves
@@ -295,6 +347,11 @@ static void cc_afforest(cgb_graph* g)
     if (timing) ktimer_begin(g, CGB_K_HOOK);
     CcLinkOp op{g->off, g->dst, g->value, giant, kRounds, g->ctr};
     launch_push(g, nullptr, V, op, true);
+    if (weak) {
+        CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->chunk_len, 0, sizeof(uint32_t), g->stream));
+        CcLinkOp iop{g->in_off, g->in_src, g->value, giant, kRounds, g->ctr};
+        launch_push(g, nullptr, V, iop, true);
+    }
     if (timing) ktimer_end(g);
     if (timing) ktimer_begin(g, CGB_K_COMPRESS);
     ++g->stats.launches;
@@ -303,14 +360,14 @@ static void cc_afforest(cgb_graph* g)
     sync_counters(g);
     CGB_REQUIRE(!g->h_ctr->link_giveup, CGB_ETIMEOUT, "CC link retry bound exceeded");
     g->stats.iterations = kRounds + 1;
-    g->stats.cc_path = 0;
+    g->stats.cc_path = weak ? 2 : 0;
 }
 
 static void cc_propagate(cgb_graph* g, const cgb_options& o)
 {
     const bool timing = g->flags & CGB_FLAG_KERNEL_TIMING;
     const uint32_t V = g->V;
-    const uint32_t grid = grid_for(V, kBlock, kNumSMs * 8);
+    const uint32_t grid = grid_for(V, kBlock, num_sms() * 8);
     const uint64_t max_iters = o.max_iterations ? o.max_iterations : (uint64_t)V + 2;
     if (timing) ktimer_begin(g, CGB_K_INIT);
     ++g->stats.launches;
@@ -348,9 +405,14 @@ static void cc_propagate(cgb_graph* g, const cgb_options& o)
 void run_cc(cgb_graph* g, const cgb_options& o)
 {
     ensure_frontier(g);
-    ensure_symmetry_known(g);
+    const bool weak = o.flags & CGB_FLAG_CC_WEAK;
+    // weak components read the in-lists (the CSR itself when the graph is
+    // known to be symmetric); no symmetry check is needed for them
+    if (weak) ensure_csc(g);
+    else ensure_symmetry_known(g);
     CGB_CUDA_TRY(cudaEventRecord(g->ev_start, g->stream));
-    if (g->symmetric == 1) cc_afforest(g);
+    if (weak) cc_afforest(g, g->in_off != g->off);
+    else if (g->symmetric == 1) cc_afforest(g, false);
     else cc_propagate(g, o);
     CGB_CUDA_TRY(cudaEventRecord(g->ev_stop, g->stream));
 }

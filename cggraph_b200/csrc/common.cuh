@@ -13,7 +13,9 @@ namespace cgb {
 constexpr uint32_t kValueMax = CGB_VALUE_MAX;  // VertexValue_MAX, Basic/Graph/basic_def.hpp:18
 constexpr int kBlock = 256;                    // threads per CTA for the frontier kernels
 constexpr int kWarp = 32;
-constexpr int kNumSMs = 148;                   // B200
+// SM count of the current device (148 on a B200), cached per device: the
+// grids of the frontier kernels are sized in multiples of it.
+int num_sms();
 // Largest V and E of a graph.  Kernels step 32-bit indices by a grid stride
 // below 2^24, so indices up to 2^32 - 2^24 never wrap.
 constexpr uint32_t kMaxGraphSize = 0xFF000000u;

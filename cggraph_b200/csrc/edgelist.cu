@@ -97,14 +97,14 @@ cgb_graph* graph_from_edges(const uint32_t* records, uint64_t E, uint32_t V, int
             auto* flags = static_cast<uint32_t*>(alloc(4));
             CGB_CUDA_TRY(cudaMemcpyAsync(rec, records, E * 12, cudaMemcpyDefault, s));
             CGB_CUDA_TRY(cudaMemsetAsync(flags, 0, 4, s));
-            const uint32_t grid = grid_for(E, kBlock, kNumSMs * 16);
+            const uint32_t grid = grid_for(E, kBlock, num_sms() * 16);
             k_records_to_keys<<<grid, kBlock, 0, s>>>(E, rec, V, b, keys, vals, flags);
             size_t tb = 0;
             CGB_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tb, keys, keys_out, vals, vals_out, E, 0, 2 * b, s));
             void* temp = alloc(tb);
             CGB_CUDA_TRY(cub::DeviceRadixSort::SortPairs(temp, tb, keys, keys_out, vals, vals_out, E, 0, 2 * b, s));
             k_unpack_sorted<<<grid, kBlock, 0, s>>>(E, keys_out, vals_out, b, src, g->dst, g->w, flags);
-            k_offsets_from_sources<<<grid_for((uint64_t)V + 1, kBlock, kNumSMs * 16), kBlock, 0, s>>>(V, E, src,
+            k_offsets_from_sources<<<grid_for((uint64_t)V + 1, kBlock, num_sms() * 16), kBlock, 0, s>>>(V, E, src,
                                                                                                      g->off);
             PinnedArray<uint32_t> h(1);
             CGB_CUDA_TRY(cudaMemcpyAsync(h.data(), flags, 4, cudaMemcpyDeviceToHost, s));

@@ -215,7 +215,7 @@ cgb_graph* gen_rmat(uint32_t scale, uint32_t ef, uint64_t seed, double a, double
     void* temp = nullptr;
     cgb_graph* g = nullptr;
     try {
-        k_rmat_keys<<<kNumSMs * 16, kBlock, 0, st>>>(scale, n, mix64(seed), t1, t2, t3, scr, m1, m2, cc, sym, keys);
+        k_rmat_keys<<<num_sms() * 16, kBlock, 0, st>>>(scale, n, mix64(seed), t1, t2, t3, scr, m1, m2, cc, sym, keys);
         cub::DoubleBuffer<uint64_t> db(keys, alt);
         size_t tb = 0, tb2 = 0;
         CGB_CUDA_TRY(cub::DeviceRadixSort::SortKeys(nullptr, tb, db, total, 0, 32 + (int)scale, st));
@@ -237,9 +237,9 @@ cgb_graph* gen_rmat(uint32_t scale, uint32_t ef, uint64_t seed, double a, double
         }
         CGB_REQUIRE(m < 0xFFFFFFFFull, CGB_EUNSUPPORTED, "RMAT graph has >= 2^32 edges");
         g = graph_alloc(V, (uint32_t)m, V, device, wmax > 0);
-        k_keys_to_csr<<<kNumSMs * 16, kBlock, 0, st>>>(V, m, out_unique, g->off, g->dst);
+        k_keys_to_csr<<<num_sms() * 16, kBlock, 0, st>>>(V, m, out_unique, g->off, g->dst);
         if (wmax)
-            k_edge_weights<<<kNumSMs * 16, kBlock, 0, st>>>(V, (uint32_t)m, g->off, g->dst, mix64(seed ^ 0x77E16ull),
+            k_edge_weights<<<num_sms() * 16, kBlock, 0, st>>>(V, (uint32_t)m, g->off, g->dst, mix64(seed ^ 0x77E16ull),
                                                             wmax, sym, g->w);
         CGB_CUDA_TRY(cudaStreamSynchronize(st));
         if (sym) g->symmetric = 1;
@@ -285,7 +285,7 @@ cgb_graph* gen_chunglu(uint32_t V, uint64_t draws, uint32_t i0, uint64_t seed, i
         // exact integer prefix sums of the weights (cum[V] = total weight)
         cum = (uint64_t*)galloc(((size_t)V + 1) * 8, st);
         uint64_t* wts = (uint64_t*)galloc(((size_t)V + 1) * 8, st);
-        k_cl_weights<<<kNumSMs * 8, kBlock, 0, st>>>(V, i0, wts);
+        k_cl_weights<<<num_sms() * 8, kBlock, 0, st>>>(V, i0, wts);
         CGB_CUDA_TRY(cudaMemsetAsync(wts + V, 0, 8, st));
         size_t tb = 0;
         CGB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb, wts, cum, (uint64_t)V + 1, st));
@@ -295,7 +295,7 @@ cgb_graph* gen_chunglu(uint32_t V, uint64_t draws, uint32_t i0, uint64_t seed, i
         pool_free(stemp, st);
         pool_free(wts, st);
         keys = (uint64_t*)galloc(total * 8, st);
-        k_cl_keys<<<kNumSMs * 16, kBlock, 0, st>>>(V, draws, cum, (double)i0, mix64(seed ^ 0xC1A0001ull),
+        k_cl_keys<<<num_sms() * 16, kBlock, 0, st>>>(V, draws, cum, (double)i0, mix64(seed ^ 0xC1A0001ull),
                                                    mix64(seed ^ 0xC1A0002ull), a_out, b_out, a_in, b_in, sym, keys);
         CGB_CUDA_TRY(cudaStreamSynchronize(st));
         pool_free(cum, st);
@@ -322,9 +322,9 @@ cgb_graph* gen_chunglu(uint32_t V, uint64_t draws, uint32_t i0, uint64_t seed, i
         }
         CGB_REQUIRE(m < 0xFFFFFFFFull, CGB_EUNSUPPORTED, "Chung-Lu graph has >= 2^32 edges");
         g = graph_alloc(V, (uint32_t)m, V, device, wmax > 0);
-        k_keys_to_csr<<<kNumSMs * 16, kBlock, 0, st>>>(V, m, out_unique, g->off, g->dst);
+        k_keys_to_csr<<<num_sms() * 16, kBlock, 0, st>>>(V, m, out_unique, g->off, g->dst);
         if (wmax)
-            k_edge_weights<<<kNumSMs * 16, kBlock, 0, st>>>(V, (uint32_t)m, g->off, g->dst, mix64(seed ^ 0x77E16ull),
+            k_edge_weights<<<num_sms() * 16, kBlock, 0, st>>>(V, (uint32_t)m, g->off, g->dst, mix64(seed ^ 0x77E16ull),
                                                             wmax, sym, g->w);
         CGB_CUDA_TRY(cudaStreamSynchronize(st));
         if (sym) g->symmetric = 1;
@@ -362,15 +362,15 @@ cgb_graph* gen_grid(uint32_t rows, uint32_t cols, uint64_t seed, uint32_t wmax, 
     void* temp = nullptr;
     try {
         deg = (uint32_t*)galloc(((size_t)V + 1) * 4, g->stream);
-        k_grid_deg<<<kNumSMs * 8, kBlock, 0, g->stream>>>(rows, cols, deg);
+        k_grid_deg<<<num_sms() * 8, kBlock, 0, g->stream>>>(rows, cols, deg);
         CGB_CUDA_TRY(cudaMemsetAsync(deg + V, 0, 4, g->stream));
         size_t tb = 0;
         CGB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb, deg, g->off, (uint64_t)V + 1, g->stream));
         temp = galloc(tb, g->stream);
         CGB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(temp, tb, deg, g->off, (uint64_t)V + 1, g->stream));
-        k_grid_fill<<<kNumSMs * 8, kBlock, 0, g->stream>>>(rows, cols, g->off, g->dst);
+        k_grid_fill<<<num_sms() * 8, kBlock, 0, g->stream>>>(rows, cols, g->off, g->dst);
         if (wmax)
-            k_edge_weights<<<kNumSMs * 16, kBlock, 0, g->stream>>>(V, E, g->off, g->dst, mix64(seed ^ 0x77E16ull), wmax,
+            k_edge_weights<<<num_sms() * 16, kBlock, 0, g->stream>>>(V, E, g->off, g->dst, mix64(seed ^ 0x77E16ull), wmax,
                                                                    1, g->w);
         CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
     } catch (...) {

@@ -1,5 +1,7 @@
 // Resident graph: upload, validation, neighbour sort, in-edge CSC, symmetry
 // check, workspaces and kernel timers.
+#include <atomic>
+
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
@@ -9,6 +11,23 @@
 #include "engine.cuh"
 
 namespace cgb {
+
+int num_sms()
+{
+    constexpr int kMaxDevices = 64;
+    static std::atomic<int> cache[kMaxDevices];
+    int dev = 0;
+    CGB_CUDA_TRY(cudaGetDevice(&dev));
+    CGB_REQUIRE(dev >= 0 && dev < kMaxDevices, CGB_EUNSUPPORTED, "device ordinal out of range");
+    int v = cache[dev].load(std::memory_order_relaxed);
+    if (v == 0) {
+        CGB_CUDA_TRY(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev));
+        CGB_REQUIRE(v > 0, CGB_ECUDA, "device reports no multiprocessors");
+        cache[dev].store(v, std::memory_order_relaxed);
+    }
+    return v;
+}
+
 
 // ------------------------------------------------------------------ errors
 static thread_local std::string t_last_error;
@@ -174,7 +193,7 @@ void h2d_small(void* dst, const void* pinned_src, size_t bytes, cudaStream_t s)
 {
     const uint64_t n = bytes / 4;
     if (!n) return;
-    k_copy_words_from_host<<<grid_for(n, kBlock, kNumSMs), kBlock, 0, s>>>(static_cast<const uint32_t*>(pinned_src),
+    k_copy_words_from_host<<<grid_for(n, kBlock, num_sms()), kBlock, 0, s>>>(static_cast<const uint32_t*>(pinned_src),
                                                                            static_cast<uint32_t*>(dst), n);
     CGB_CUDA_TRY(cudaGetLastError());
 }
@@ -430,8 +449,8 @@ static void launch_edges_by_row(cgb_graph* g, uint32_t V, uint32_t E, const uint
     if (E == 0) return;
     const uint32_t tiles = div_up(E, kRowTile);
     uint32_t* trow = dalloc<uint32_t>((size_t)tiles + 1, g->stream);
-    k_tile_rows<<<grid_for((uint64_t)tiles + 1, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, E, off, tiles, trow);
-    k_edges_by_row<<<min(tiles, kNumSMs * 8), kBlock, 0, g->stream>>>(E, off, trow, f);  // 24 KB each
+    k_tile_rows<<<grid_for((uint64_t)tiles + 1, kBlock, num_sms() * 8), kBlock, 0, g->stream>>>(V, E, off, tiles, trow);
+    k_edges_by_row<<<min(tiles, num_sms() * 8), kBlock, 0, g->stream>>>(E, off, trow, f);  // 24 KB each
     dfree(trow, g->stream);
 }
 
@@ -551,7 +570,7 @@ static void sort_neighbours(cgb_graph* g)
     const uint32_t b = bits_for(V);
     uint64_t* keys = dalloc<uint64_t>(E, g->stream);
     uint64_t* alt = dalloc<uint64_t>(E, g->stream);
-    const uint32_t grid = grid_for(E, kBlock, kNumSMs * 16);
+    const uint32_t grid = grid_for(E, kBlock, num_sms() * 16);
     if (g->w) {
         uint64_t* vals = dalloc<uint64_t>(E, g->stream);
         uint64_t* valt = dalloc<uint64_t>(E, g->stream);
@@ -585,7 +604,7 @@ void validate_and_sort(cgb_graph* g)
     const uint32_t V = g->V, E = g->E;
     uint32_t* flags = dalloc<uint32_t>(4, g->stream);
     CGB_CUDA_TRY(cudaMemsetAsync(flags, 0, 4 * sizeof(uint32_t), g->stream));
-    k_check_offsets<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, E, g->off, flags);
+    k_check_offsets<<<grid_for(V, kBlock, num_sms() * 8), kBlock, 0, g->stream>>>(V, E, g->off, flags);
     PinnedArray<uint32_t> h(4);
     CGB_CUDA_TRY(cudaMemcpyAsync(h.data(), flags, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, g->stream));
     CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
@@ -614,8 +633,8 @@ void validate_and_sort(cgb_graph* g)
     for (int pass = 0; pass < 2; pass++) {
         CGB_CUDA_TRY(cudaMemsetAsync(heads, 0, hw * sizeof(uint32_t), g->stream));
         CGB_CUDA_TRY(cudaMemsetAsync(flags, 0, 4 * sizeof(uint32_t), g->stream));
-        k_mark_heads<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, g->off, heads);
-        k_check_edges<<<grid_for(E, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(V, E, g->dst, heads, flags);
+        k_mark_heads<<<grid_for(V, kBlock, num_sms() * 8), kBlock, 0, g->stream>>>(V, g->off, heads);
+        k_check_edges<<<grid_for(E, kBlock, num_sms() * 16), kBlock, 0, g->stream>>>(V, E, g->dst, heads, flags);
         CGB_CUDA_TRY(cudaMemcpyAsync(h.data(), flags, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, g->stream));
         CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
         if (h[0] & 8u) {
@@ -644,7 +663,7 @@ void compute_weight_sum(cgb_graph* g)
     if (!g->w || g->E == 0) return;
     unsigned long long* d = dalloc<unsigned long long>(1, g->stream);
     CGB_CUDA_TRY(cudaMemsetAsync(d, 0, sizeof(unsigned long long), g->stream));
-    k_sum_u32<<<grid_for(g->E, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(g->E, g->w, d);
+    k_sum_u32<<<grid_for(g->E, kBlock, num_sms() * 8), kBlock, 0, g->stream>>>(g->E, g->w, d);
     PinnedArray<unsigned long long> h(1);
     CGB_CUDA_TRY(cudaMemcpyAsync(h.data(), d, sizeof(unsigned long long), cudaMemcpyDeviceToHost, g->stream));
     CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
@@ -697,7 +716,7 @@ void graph_set_weights(cgb_graph* g, const uint32_t* weight)
         sum = dalloc<unsigned long long>(1, s);
         CGB_CUDA_TRY(cudaMemcpyAsync(w, weight, (size_t)E * 4, cudaMemcpyDefault, s));
         CGB_CUDA_TRY(cudaMemsetAsync(sum, 0, sizeof(unsigned long long), s));
-        k_sum_u32<<<grid_for(E, kBlock, kNumSMs * 8), kBlock, 0, s>>>(E, w, sum);
+        k_sum_u32<<<grid_for(E, kBlock, num_sms() * 8), kBlock, 0, s>>>(E, w, sum);
         CGB_CUDA_TRY(cudaMemcpyAsync(hs.data(), sum, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
         CGB_CUDA_TRY(cudaStreamSynchronize(s));
     } catch (...) {
@@ -791,7 +810,7 @@ static void stable_sort_u32(cgb_graph* g, const uint32_t* keys_in, uint32_t* key
 static void transpose_arrays(cgb_graph* g, uint32_t* dst_sorted, uint32_t* in_src, uint32_t* in_w)
 {
     const uint32_t E = g->E, V = g->V;
-    const uint32_t grid = grid_for(E, kBlock, kNumSMs * 16);
+    const uint32_t grid = grid_for(E, kBlock, num_sms() * 16);
     uint32_t* src = dalloc<uint32_t>(E, g->stream);
     launch_edges_by_row(g, V, E, g->off, RowOutF{src});
     if (!in_w) {
@@ -914,7 +933,7 @@ static bool check_symmetric(cgb_graph* g)
     uint32_t* uoff = dalloc<uint32_t>((size_t)V + 1, g->stream);
     CGB_CUDA_TRY(cudaMemsetAsync(lower + V, 0, 4, g->stream));
     CGB_CUDA_TRY(cudaMemsetAsync(upper + V, 0, 4, g->stream));
-    k_sym_counts<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, g->off, g->dst, lower, upper);
+    k_sym_counts<<<grid_for(V, kBlock, num_sms() * 8), kBlock, 0, g->stream>>>(V, g->off, g->dst, lower, upper);
     exclusive_sum_u32(g, lower, loff, (uint64_t)V + 1);
     exclusive_sum_u32(g, upper, uoff, (uint64_t)V + 1);
     PinnedArray<uint32_t> tot(2);
@@ -964,15 +983,15 @@ static void build_transpose(cgb_graph* g)
         uint32_t* dsorted = dalloc<uint32_t>(E, g->stream);
         // weights in CSC order are built on first need (ensure_csc_weights)
         transpose_arrays(g, dsorted, in_src, nullptr);
-        k_offsets_from_u32<<<grid_for((uint64_t)V + 1, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(V, E, dsorted,
+        k_offsets_from_u32<<<grid_for((uint64_t)V + 1, kBlock, num_sms() * 16), kBlock, 0, g->stream>>>(V, E, dsorted,
                                                                                                       in_off);
         CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
         dfree(dsorted, g->stream);
     }
     uint32_t* differ = dalloc<uint32_t>(1, g->stream);
     CGB_CUDA_TRY(cudaMemsetAsync(differ, 0, sizeof(uint32_t), g->stream));
-    k_compare_u32<<<kNumSMs * 8, kBlock, 0, g->stream>>>((uint64_t)V + 1, in_off, g->off, differ);
-    if (E) k_compare_u32<<<kNumSMs * 8, kBlock, 0, g->stream>>>(E, in_src, g->dst, differ);
+    k_compare_u32<<<num_sms() * 8, kBlock, 0, g->stream>>>((uint64_t)V + 1, in_off, g->off, differ);
+    if (E) k_compare_u32<<<num_sms() * 8, kBlock, 0, g->stream>>>(E, in_src, g->dst, differ);
     PinnedArray<uint32_t> h(1);
     CGB_CUDA_TRY(cudaMemcpyAsync(h.data(), differ, 4, cudaMemcpyDeviceToHost, g->stream));
     CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
@@ -1033,7 +1052,7 @@ void ensure_csc_weights(cgb_graph* g)
     dfree(srcs, g->stream);
     uint32_t* differ = dalloc<uint32_t>(1, g->stream);
     CGB_CUDA_TRY(cudaMemsetAsync(differ, 0, 4, g->stream));
-    k_compare_u32<<<kNumSMs * 8, kBlock, 0, g->stream>>>(E, vals, g->w, differ);
+    k_compare_u32<<<num_sms() * 8, kBlock, 0, g->stream>>>(E, vals, g->w, differ);
     PinnedArray<uint32_t> h(1);
     CGB_CUDA_TRY(cudaMemcpyAsync(h.data(), differ, 4, cudaMemcpyDeviceToHost, g->stream));
     CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
@@ -1065,7 +1084,7 @@ void ensure_frontier(cgb_graph* g)
     g->aux_bm = dalloc<uint32_t>(3 * (size_t)g->words(), g->stream);
     uint32_t* d = dalloc<uint32_t>(1, g->stream);
     CGB_CUDA_TRY(cudaMemsetAsync(d, 0, 4, g->stream));
-    k_max_degree<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, g->off, d);
+    k_max_degree<<<grid_for(V, kBlock, num_sms() * 8), kBlock, 0, g->stream>>>(V, g->off, d);
     PinnedArray<uint32_t> md(1);
     CGB_CUDA_TRY(cudaMemcpyAsync(md.data(), d, 4, cudaMemcpyDeviceToHost, g->stream));
     CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
@@ -1195,7 +1214,7 @@ static void build_sell(cgb_graph* g)
     CGB_CUDA_TRY(cudaMemsetAsync(g->pr_hub_bm, 0, (size_t)g->words() * 4, g->stream));
     uint64_t* width = dalloc<uint64_t>((size_t)nslices + 1, g->stream);
     CGB_CUDA_TRY(cudaMemsetAsync(width + nslices, 0, 8, g->stream));
-    k_sell_len<<<grid_for((uint64_t)nslices * 32, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(
+    k_sell_len<<<grid_for((uint64_t)nslices * 32, kBlock, num_sms() * 8), kBlock, 0, g->stream>>>(
         V, g->pr_off, kPrHuge, g->pr_slice_len, width);
     size_t tb = 0;
     CGB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb, width, g->pr_slice_ptr, (uint64_t)nslices + 1, g->stream));
@@ -1238,14 +1257,14 @@ void ensure_pr(cgb_graph* g)
         uint32_t* id2 = dalloc<uint32_t>(V, g->stream);
         // in-degrees from the transpose (shared with bottom-up BFS; no atomics)
         ensure_csc(g);
-        k_in_degree_from_off<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, g->in_off, key2);
-        k_pr_bucket<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, g->off, key2, key, id);
+        k_in_degree_from_off<<<grid_for(V, kBlock, num_sms() * 8), kBlock, 0, g->stream>>>(V, g->in_off, key2);
+        k_pr_bucket<<<grid_for(V, kBlock, num_sms() * 8), kBlock, 0, g->stream>>>(V, g->off, key2, key, id);
         cub::DoubleBuffer<uint32_t> kb(key, key2), vb(id, id2);
         size_t tb = 0;
         CGB_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tb, kb, vb, (uint64_t)V, 0, 32, g->stream));
         void* temp = dalloc<char>(tb, g->stream);
         cudaError_t err = cub::DeviceRadixSort::SortPairs(temp, tb, kb, vb, (uint64_t)V, 0, 32, g->stream);
-        k_pr_rank<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, vb.Current(), g->off, g->pr_rank,
+        k_pr_rank<<<grid_for(V, kBlock, num_sms() * 8), kBlock, 0, g->stream>>>(V, vb.Current(), g->off, g->pr_rank,
                                                                              g->pr_outdeg);
         CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
         dfree(temp, g->stream);
@@ -1279,7 +1298,7 @@ void ensure_pr(cgb_graph* g)
             uint32_t* kout = dalloc<uint32_t>(E, g->stream);
             launch_edges_by_row(g, V, E, src_off, PrEdgesF{order, g->off, g->dst, g->pr_rank, key, val});
             stable_sort_u32(g, key, kout, val, g->pr_src, E, (int)bits_for(V));
-            k_offsets_from_u32<<<grid_for((uint64_t)V + 1, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(
+            k_offsets_from_u32<<<grid_for((uint64_t)V + 1, kBlock, num_sms() * 16), kBlock, 0, g->stream>>>(
                 V, E, kout, g->pr_off);
             CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
             dfree(key, g->stream);
@@ -1291,7 +1310,7 @@ void ensure_pr(cgb_graph* g)
         dfree(src_off, g->stream);
         build_sell(g);
         if (E)
-            k_sell_fill<<<grid_for((uint64_t)(V + 31) / 32 * 32, kBlock, kNumSMs * 16), kBlock, 0, g->stream>>>(
+            k_sell_fill<<<grid_for((uint64_t)(V + 31) / 32 * 32, kBlock, num_sms() * 16), kBlock, 0, g->stream>>>(
                 V, g->pr_off, g->pr_src, g->pr_slice_ptr, g->pr_slice_len, kPrHuge, g->pr_col, g->pr_hub_bm);
         CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
         dfree(order, g->stream);
@@ -1301,7 +1320,7 @@ void ensure_pr(cgb_graph* g)
         uint32_t* n = dalloc<uint32_t>(1, g->stream);
         uint32_t* rows = dalloc<uint32_t>(V, g->stream);
         CGB_CUDA_TRY(cudaMemsetAsync(n, 0, sizeof(uint32_t), g->stream));
-        k_collect_heavy_rows<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, g->pr_off, kPrHuge, rows,
+        k_collect_heavy_rows<<<grid_for(V, kBlock, num_sms() * 8), kBlock, 0, g->stream>>>(V, g->pr_off, kPrHuge, rows,
                                                                                         n);
         PinnedArray<uint32_t> hn(1);
         CGB_CUDA_TRY(cudaMemcpyAsync(hn.data(), n, 4, cudaMemcpyDeviceToHost, g->stream));
@@ -1316,7 +1335,7 @@ void ensure_pr(cgb_graph* g)
             std::sort(hrows.data(), hrows.data() + h);
             h2d_small(rows, hrows.data(), h * 4ull, g->stream);
             uint32_t* lohi = dalloc<uint32_t>(2ull * h, g->stream);
-            k_row_bounds<<<grid_for(h, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(rows, h, g->pr_off, lohi);
+            k_row_bounds<<<grid_for(h, kBlock, num_sms() * 8), kBlock, 0, g->stream>>>(rows, h, g->pr_off, lohi);
             CGB_CUDA_TRY(cudaMemcpyAsync(lohi_h.data(), lohi, 2ull * h * 4, cudaMemcpyDeviceToHost, g->stream));
             CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
             dfree(lohi, g->stream);
@@ -1349,7 +1368,7 @@ void count_reached(cgb_graph* g)
 {
     CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->reached_edges, 0, sizeof(unsigned long long), g->stream));
     CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->reached, 0, sizeof(uint32_t), g->stream));
-    k_count_reached<<<grid_for(g->V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(g->V, g->value, g->off, g->ctr);
+    k_count_reached<<<grid_for(g->V, kBlock, num_sms() * 8), kBlock, 0, g->stream>>>(g->V, g->value, g->off, g->ctr);
     sync_counters(g);
     g->stats.reached = g->h_ctr->reached;
     g->stats.traversed_edges = g->h_ctr->reached_edges;
@@ -1806,8 +1825,8 @@ static uint32_t bfs_vertex_order(cgb_graph* g, int method, uint32_t* order)
     const uint32_t V = g->V, E = g->E;
     cudaStream_t s = g->stream;
     ScopedPool pool(s);
-    const uint32_t gv = grid_for(V, kBlock, kNumSMs * 8);
-    const uint32_t gw = kNumSMs * 16;  // warp-per-vertex kernels
+    const uint32_t gv = grid_for(V, kBlock, num_sms() * 8);
+    const uint32_t gw = num_sms() * 16;  // warp-per-vertex kernels
     uint32_t* indeg = pool.get<uint32_t>(V);
     uint32_t* skey = pool.get<uint32_t>(V);
     uint32_t* skey2 = pool.get<uint32_t>(V);
@@ -1828,7 +1847,7 @@ static uint32_t bfs_vertex_order(cgb_graph* g, int method, uint32_t* order)
     uint64_t* K = pool.get<uint64_t>(V);
     uint64_t* K2 = pool.get<uint64_t>(V);
     CGB_CUDA_TRY(cudaMemsetAsync(indeg, 0, (size_t)V * 4, s));
-    if (E) k_in_degree<<<grid_for(E, kBlock, kNumSMs * 8), kBlock, 0, s>>>(E, g->dst, indeg);
+    if (E) k_in_degree<<<grid_for(E, kBlock, num_sms() * 8), kBlock, 0, s>>>(E, g->dst, indeg);
     k_bfs_order_keys<<<gv, kBlock, 0, s>>>(V, g->off, indeg, method, skey, ids, child_key);
     stable_sort_u32(g, skey, skey2, ids, start_list, V, 32);
 
@@ -1930,12 +1949,12 @@ cgb_graph* graph_reorder(cgb_graph* g, int method, uint32_t* old2new_out, uint32
     if (bfs) {
         bfs_vertex_order(g, method, order);  // vertices with out-edges first
     } else {
-        k_degree_desc_key<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, s>>>(V, deg_off, key, id);
+        k_degree_desc_key<<<grid_for(V, kBlock, num_sms() * 8), kBlock, 0, s>>>(V, deg_off, key, id);
         stable_sort_u32(g, key, key2, id, order, V, 32);
     }
     CGB_CUDA_TRY(cudaMemsetAsync(nonzero, 0, 4, s));
     CGB_CUDA_TRY(cudaMemsetAsync(new_deg + V, 0, 4, s));
-    k_reorder_rows<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, s>>>(V, order, g->off, old2new, new_deg, nonzero);
+    k_reorder_rows<<<grid_for(V, kBlock, num_sms() * 8), kBlock, 0, s>>>(V, order, g->off, old2new, new_deg, nonzero);
     PinnedArray<uint32_t> hn(1);
     CGB_CUDA_TRY(cudaMemcpyAsync(hn.data(), nonzero, 4, cudaMemcpyDeviceToHost, s));
     CGB_CUDA_TRY(cudaStreamSynchronize(s));

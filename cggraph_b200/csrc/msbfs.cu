@@ -329,10 +329,10 @@ __global__ void __launch_bounds__(kBlock) k_ms_bu_settle(MsBuArgs a)
 void ms_bottom_up(const MsBuArgs& a, cudaStream_t st, uint64_t* launches)
 {
     CGB_CUDA_TRY(cudaMemsetAsync(a.heavy_len, 0, 8, st));
-    k_ms_bu_light<<<grid_for(a.V, kBlock, kNumSMs * 8), kBlock, 0, st>>>(a);
-    k_ms_bu_warp<<<kNumSMs * 8, kBlock, 0, st>>>(a);
-    k_ms_bu_chunks<<<kNumSMs * 4, kBlock, 0, st>>>(a);
-    k_ms_bu_settle<<<kNumSMs, kBlock, 0, st>>>(a);
+    k_ms_bu_light<<<grid_for(a.V, kBlock, num_sms() * 8), kBlock, 0, st>>>(a);
+    k_ms_bu_warp<<<num_sms() * 8, kBlock, 0, st>>>(a);
+    k_ms_bu_chunks<<<num_sms() * 4, kBlock, 0, st>>>(a);
+    k_ms_bu_settle<<<num_sms(), kBlock, 0, st>>>(a);
     if (launches) *launches += 4;
 }
 
@@ -368,12 +368,12 @@ void run_msbfs(cgb_graph* g, const uint32_t* d_roots, uint32_t n, uint32_t* leve
     // Invariant at the start of a level: front[cur] is non-zero only at the
     // vertices of the active queue q[cur]; front[cur ^ 1] and next are zero.
     const unsigned long long full = n == 64 ? ~0ull : ((1ull << n) - 1);
-    const uint32_t gridV = grid_for(V, kBlock, kNumSMs * 8);
+    const uint32_t gridV = grid_for(V, kBlock, num_sms() * 8);
     ++g->stats.launches;
     k_ms_init<<<gridV, kBlock, 0, g->stream>>>(V, b.seen, b.front[0], b.next);
     CGB_CUDA_TRY(cudaMemsetAsync(b.front[1], 0, (size_t)V * 8, g->stream));
     ++g->stats.launches;
-    k_ms_fill<<<kNumSMs * 8, kBlock, 0, g->stream>>>((uint64_t)n * V, level_out, kValueMax);
+    k_ms_fill<<<num_sms() * 8, kBlock, 0, g->stream>>>((uint64_t)n * V, level_out, kValueMax);
     CGB_CUDA_TRY(cudaMemsetAsync(g->ctr, 0, sizeof(DevCounters), g->stream));
     ++g->stats.launches;
     k_ms_roots<<<1, 1, 0, g->stream>>>(d_roots, n, V, b.seen, b.front[0], level_out, g->q[0], &g->ctr->qlen[0], g->nz,
@@ -391,7 +391,7 @@ void run_msbfs(cgb_graph* g, const uint32_t* d_roots, uint32_t n, uint32_t* leve
         // direction: out-edges of the active vertices against the graph's edges
         CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->medges, 0, 8, g->stream));
         ++g->stats.launches;
-        k_ms_degree_sum<<<grid_for(nact, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(g->q[cur], (uint32_t)nact,
+        k_ms_degree_sum<<<grid_for(nact, kBlock, num_sms() * 8), kBlock, 0, g->stream>>>(g->q[cur], (uint32_t)nact,
                                                                                       nullptr, g->off, g->ctr);
         sync_counters(g);
         const bool pull = (double)g->h_ctr->medges * alpha > (double)g->E;
@@ -420,14 +420,14 @@ void run_msbfs(cgb_graph* g, const uint32_t* d_roots, uint32_t n, uint32_t* leve
             const uint32_t touched = g->h_ctr->found;
             if (touched) {
                 ++g->stats.launches;
-                k_ms_finalize<<<grid_for(touched, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(
+                k_ms_finalize<<<grid_for(touched, kBlock, num_sms() * 8), kBlock, 0, g->stream>>>(
                     g->stamp, touched, nullptr, b.seen, b.next, fnxt, level_out, V, lvl + 1, g->nz, g->q[nxt],
                     &g->ctr->qlen[nxt], V, g->ctr, nullptr, &g->ctr->alive);
             }
             g->stats.pushes_td++;
         }
         ++g->stats.launches;
-        k_ms_clear<<<grid_for(nact, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(g->q[cur], (uint32_t)nact, fcur);
+        k_ms_clear<<<grid_for(nact, kBlock, num_sms() * 8), kBlock, 0, g->stream>>>(g->q[cur], (uint32_t)nact, fcur);
         sync_counters(g);
         CGB_REQUIRE(!g->h_ctr->overflow, CGB_EOVERFLOW, "multi-root BFS queue overflow");
         if (tracing) {

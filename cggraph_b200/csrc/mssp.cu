@@ -388,7 +388,7 @@ void run_mssp(cgb_graph* g, const uint32_t* d_roots, uint32_t n, uint32_t* out, 
     if (delta == 0) delta = 1;
     CGB_CUDA_TRY(cudaMemsetAsync(b.c, 0, sizeof(MsspCounters), g->stream));
     ++g->stats.launches;
-    k_mssp_init<<<kNumSMs * 8, kBlock, 0, g->stream>>>(V, reinterpret_cast<uint4*>(b.dist), b.pend, b.farm);
+    k_mssp_init<<<num_sms() * 8, kBlock, 0, g->stream>>>(V, reinterpret_cast<uint4*>(b.dist), b.pend, b.farm);
     ++g->stats.launches;
     k_mssp_roots<<<1, 1, 0, g->stream>>>(d_roots, n, b.dist, b.pend, g->q[0], b.c);
     uint32_t nq = mssp_sync(g).nq_out, nfar = 0;
@@ -407,12 +407,12 @@ void run_mssp(cgb_graph* g, const uint32_t* d_roots, uint32_t n, uint32_t* out, 
             const uint32_t t32 = (uint32_t)std::min<uint64_t>(thr, 0xFFFFFFFFull);
             CGB_CUDA_TRY(cudaMemsetAsync(&b.c->ndesc, 0, 4, g->stream));
             ++g->stats.launches;
-            k_mssp_desc<<<grid_for(nq, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(g->q[cur], &b.c->nq_in, g->off,
+            k_mssp_desc<<<grid_for(nq, kBlock, num_sms() * 8), kBlock, 0, g->stream>>>(g->q[cur], &b.c->nq_in, g->off,
                                                                                     b.pend, b.maskq, b.desc,
                                                                                     b.desc_cap, b.c,
                                                                                     g->tune.ms_edges);
             ++g->stats.launches;
-            mssp_expand(g->w != nullptr, kNumSMs * 8, g->stream, b.desc, b.c, b.maskq, g->dst, g->w, b.dist, b.pend,
+            mssp_expand(g->w != nullptr, num_sms() * 8, g->stream, b.desc, b.c, b.maskq, g->dst, g->w, b.dist, b.pend,
                         b.farm, g->q[nxt], &b.c->nq_out, b.far_list[fcur], &b.c->nfar_live, V, t32, nullptr,
                         nullptr);
             const MsspCounters h = mssp_sync(g);
@@ -430,7 +430,7 @@ void run_mssp(cgb_graph* g, const uint32_t* d_roots, uint32_t n, uint32_t* out, 
             k_mssp_set<<<1, 1, 0, g->stream>>>(&b.c->min_far, kValueMax);
             CGB_CUDA_TRY(cudaMemsetAsync(&b.c->nfar_next, 0, 4, g->stream));
             ++g->stats.launches;
-            k_mssp_split<<<grid_for(nfar, kBlock / 32, kNumSMs * 8), kBlock, 0, g->stream>>>(
+            k_mssp_split<<<grid_for(nfar, kBlock / 32, num_sms() * 8), kBlock, 0, g->stream>>>(
                 b.far_list[fcur], &b.c->nfar_live, b.dist, b.pend, b.farm, g->q[nxt], &b.c->nq_out,
                 b.far_list[fcur ^ 1], &b.c->nfar_next, V, lo32, hi32, nullptr, nullptr, ~0ull, nullptr, nullptr, b.c);
             const MsspCounters h = mssp_sync(g);
@@ -446,7 +446,7 @@ void run_mssp(cgb_graph* g, const uint32_t* d_roots, uint32_t n, uint32_t* out, 
         CGB_CUDA_TRY(cudaMemcpyAsync(&b.c->nq_in, &b.c->nq_out, 4, cudaMemcpyDeviceToDevice, g->stream));
     }
     ++g->stats.launches;
-    k_mssp_out<<<kNumSMs * 16, kBlock, 0, g->stream>>>(b.dist, V, n, out);
+    k_mssp_out<<<num_sms() * 16, kBlock, 0, g->stream>>>(b.dist, V, n, out);
     g->stats.iterations = rounds;
     g->stats.sssp_delta = delta;
 }

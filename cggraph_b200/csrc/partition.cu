@@ -79,7 +79,7 @@ void graph_partition(cgb_graph* g, int algorithm, uint32_t ndev, const uint64_t*
         auto* key2 = static_cast<uint32_t*>(held.get((size_t)nseg * 4));
         auto* id = static_cast<uint32_t*>(held.get((size_t)nseg * 4));
         auto* id2 = static_cast<uint32_t*>(held.get((size_t)nseg * 4));
-        k_segment_keys<<<grid_for(nseg, kBlock, kNumSMs * 4), kBlock, 0, s>>>(nseg, nz, g->off, edges, key, id);
+        k_segment_keys<<<grid_for(nseg, kBlock, num_sms() * 4), kBlock, 0, s>>>(nseg, nz, g->off, edges, key, id);
         size_t tb = 0;
         CGB_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tb, key, key2, id, id2, (uint64_t)nseg, 0, 32, s));
         void* temp = held.get(tb);

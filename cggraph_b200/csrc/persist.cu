@@ -386,7 +386,7 @@ void launch_bfs_unbounded(cgb_graph* g, PersistState* st)
     unsigned long long scout_exit = ~0ull;
     void* args[] = {&g->off, &g->dst, &g->value, &g->visited, &g->q[0], &g->q[1], &cap, &nz, &lvl, &cur, &nf_exit,
                     &scout_exit, &deg_exit, &max_levels, &st};
-    CGB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_bfs_persistent, kNumSMs, kBlock, args, 0, g->stream));
+    CGB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_bfs_persistent, num_sms(), kBlock, args, 0, g->stream));
 }
 
 void launch_sssp_device(cgb_graph* g, uint32_t* far_bm, uint32_t delta, PersistState* st, PersistSssp* sx)
@@ -396,9 +396,9 @@ void launch_sssp_device(cgb_graph* g, uint32_t* far_bm, uint32_t delta, PersistS
     void* args[] = {&g->off, &g->dst, &g->w, &g->value, &nbm, &words, &far_bm, &g->q[0], &g->q[1], &cap, &nz, &delta,
                     &rounds, &st, &sx};
     if (g->w)
-        CGB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_sssp_device<true>, kNumSMs, kBlock, args, 0, g->stream));
+        CGB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_sssp_device<true>, num_sms(), kBlock, args, 0, g->stream));
     else
-        CGB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_sssp_device<false>, kNumSMs, kBlock, args, 0, g->stream));
+        CGB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_sssp_device<false>, num_sms(), kBlock, args, 0, g->stream));
 }
 
 static PersistState* persist_state(cgb_graph* g)

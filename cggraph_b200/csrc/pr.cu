@@ -159,9 +159,9 @@ void run_pr(cgb_graph* g, uint32_t iters, const cgb_options& o)
     CGB_CUDA_TRY(cudaEventRecord(g->ev_start, g->stream));
     if (timing) ktimer_begin(g, CGB_K_INIT);
     ++g->stats.launches;
-    k_pr_init<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, g->pr_outdeg, g->pr[0], g->contrib[0]);
+    k_pr_init<<<grid_for(V, kBlock, num_sms() * 8), kBlock, 0, g->stream>>>(V, g->pr_outdeg, g->pr[0], g->contrib[0]);
     if (timing) ktimer_end(g);
-    const uint32_t grid = grid_for(div_up(V, 32), kBlock / 32, kNumSMs * g->tune.pr_ctas_per_sm);
+    const uint32_t grid = grid_for(div_up(V, 32), kBlock / 32, num_sms() * g->tune.pr_ctas_per_sm);
     const uint32_t unroll = g->tune.pr_unroll;
     // hub chunks on a second stream, beside the pull (they read the same
     // contributions and write only the chunk partials); joined before the
@@ -180,7 +180,7 @@ void run_pr(cgb_graph* g, uint32_t iters, const cgb_options& o)
             ++g->stats.launches;
             CGB_CUDA_TRY(cudaEventRecord(g->ev_fork, g->stream));
             CGB_CUDA_TRY(cudaStreamWaitEvent(g->aux_stream, g->ev_fork, 0));
-            k_pr_hub_chunks<<<std::min<uint32_t>(g->n_pr_chunks, kNumSMs * 8), kBlock, 0, g->aux_stream>>>(
+            k_pr_hub_chunks<<<std::min<uint32_t>(g->n_pr_chunks, num_sms() * 8), kBlock, 0, g->aux_stream>>>(
                 g->pr_chunks, g->n_pr_chunks, g->pr_off, g->pr_src, g->contrib[cur], g->pr_part);
             CGB_CUDA_TRY(cudaEventRecord(g->ev_join, g->aux_stream));
         }
@@ -191,7 +191,7 @@ void run_pr(cgb_graph* g, uint32_t iters, const cgb_options& o)
         if (fork) CGB_CUDA_TRY(cudaStreamWaitEvent(g->stream, g->ev_join, 0));
         if (g->n_pr_huge) {
             ++g->stats.launches;
-            k_pr_hub_finish<<<grid_for(g->n_pr_huge, kBlock, kNumSMs), kBlock, 0, g->stream>>>(
+            k_pr_hub_finish<<<grid_for(g->n_pr_huge, kBlock, num_sms()), kBlock, 0, g->stream>>>(
                 g->pr_huge_rows, g->n_pr_huge, g->pr_chunk_base, g->pr_part, g->pr_outdeg, g->pr[out],
                 g->contrib[out], base, damp);
         }
@@ -200,7 +200,7 @@ void run_pr(cgb_graph* g, uint32_t iters, const cgb_options& o)
     }
     // the other pr buffer receives the result in the caller's ids
     ++g->stats.launches;
-    k_pr_unpermute<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(V, g->pr_rank, g->pr[cur],
+    k_pr_unpermute<<<grid_for(V, kBlock, num_sms() * 8), kBlock, 0, g->stream>>>(V, g->pr_rank, g->pr[cur],
                                                                                g->pr[cur ^ 1]);
     CGB_CUDA_TRY(cudaEventRecord(g->ev_stop, g->stream));
     g->result = g->pr[cur ^ 1];

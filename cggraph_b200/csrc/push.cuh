@@ -246,7 +246,7 @@ inline void launch_push(cgb_graph* g, const uint32_t* qin, uint32_t nin, const O
 {
     if (nin == 0) return;
     const cgb_tuning& t = g->tune;
-    const uint32_t ctas = kNumSMs * t.push_ctas_per_sm;
+    const uint32_t ctas = num_sms() * t.push_ctas_per_sm;
     const uint32_t grid = grid_for(nin, kBlock, ctas);
     g->stats.launches += 2;
     if (identity)

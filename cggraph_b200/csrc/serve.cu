@@ -306,7 +306,7 @@ static void group_alloc(cgb_server* s, Group& G, int alg, uint32_t nslots)
         CGB_CUDA_TRY(cudaMemset(G.sp->c, 0, sizeof(MsspCounters)));
         CGB_CUDA_TRY(cudaMemset(G.sp->pend, 0, (size_t)V * 8));
         CGB_CUDA_TRY(cudaMemset(G.sp->farm, 0, (size_t)V * 8));
-        k_ms_fill<<<kNumSMs * 8, kBlock>>>((uint64_t)V * kMsRoots, G.sp->dist, kValueMax);  // reused slots reset on admission
+        k_ms_fill<<<num_sms() * 8, kBlock>>>((uint64_t)V * kMsRoots, G.sp->dist, kValueMax);  // reused slots reset on admission
         CGB_CUDA_TRY(cudaGetLastError());
     }
 }
@@ -350,9 +350,9 @@ static void bfs_issue(cgb_server* s, Group& G)
         }
         G.nact = qpos;
         if (reuse)
-            k_srv_clear_bits<<<kNumSMs * 8, kBlock, 0, st>>>(V, G.mb->seen, reuse);
+            k_srv_clear_bits<<<num_sms() * 8, kBlock, 0, st>>>(V, G.mb->seen, reuse);
         for (const uint32_t k : G.admit)
-            k_ms_fill<<<kNumSMs * 4, kBlock, 0, st>>>((uint64_t)V, G.region + (size_t)k * V, kValueMax);
+            k_ms_fill<<<num_sms() * 4, kBlock, 0, st>>>((uint64_t)V, G.region + (size_t)k * V, kValueMax);
         CGB_CUDA_TRY(cudaMemcpyAsync(G.d_up, G.h_up, sizeof(SlotUpload), cudaMemcpyHostToDevice, st));
         k_srv_bfs_admit<<<1, kSrvSlots, 0, st>>>(n, G.d_up->slots, G.d_up->roots, G.d_up->qidx, V, G.region,
                                                  G.mb->seen, G.mb->front[cur], G.q[cur]);
@@ -374,13 +374,13 @@ static void bfs_issue(cgb_server* s, Group& G)
         CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->chunk_len, 0, 4, st));
         MsTdOp op{g->off, g->dst, G.mb->front[cur], G.mb->seen, G.mb->next, G.touched, &g->ctr->found, V, g->ctr};
         launch_push(g, G.q[cur], G.nact, op, false);
-        k_ms_finalize<<<kNumSMs * 8, kBlock, 0, st>>>(G.touched, 0, &g->ctr->found, G.mb->seen, G.mb->next,
+        k_ms_finalize<<<num_sms() * 8, kBlock, 0, st>>>(G.touched, 0, &g->ctr->found, G.mb->seen, G.mb->next,
                                                      G.mb->front[nxt], G.region, V, lvl, g->nz, G.q[nxt],
                                                      &g->ctr->qlen[nxt], V, g->ctr, G.d_up->start,
                                                      &G.d_stats->alive[0]);
     }
-    k_ms_clear<<<grid_for(G.nact, kBlock, kNumSMs * 8), kBlock, 0, st>>>(G.q[cur], G.nact, G.mb->front[cur]);
-    k_ms_degree_sum<<<kNumSMs * 4, kBlock, 0, st>>>(G.q[nxt], 0, &g->ctr->qlen[nxt], g->off, g->ctr);
+    k_ms_clear<<<grid_for(G.nact, kBlock, num_sms() * 8), kBlock, 0, st>>>(G.q[cur], G.nact, G.mb->front[cur]);
+    k_ms_degree_sum<<<num_sms() * 4, kBlock, 0, st>>>(G.q[nxt], 0, &g->ctr->qlen[nxt], g->off, g->ctr);
 }
 
 // ---- SSSP group: admissions, per-slot bucket splits, one near round
@@ -406,7 +406,7 @@ static void sp_issue(cgb_server* s, Group& G)
             G.min_far[k] = kValueMax;
             n++;
         }
-        if (reuse) k_srv_sp_reset<<<kNumSMs * 8, kBlock, 0, st>>>(V, b.dist, reuse);
+        if (reuse) k_srv_sp_reset<<<num_sms() * 8, kBlock, 0, st>>>(V, b.dist, reuse);
         for (uint32_t k = 0; k < kSrvSlots; k++) G.h_up->thr[k] = (uint32_t)std::min<uint64_t>(G.thr[k], 0xFFFFFFFFu);
         CGB_CUDA_TRY(cudaMemcpyAsync(G.d_up, G.h_up, sizeof(SlotUpload), cudaMemcpyHostToDevice, st));
         k_srv_sp_admit<<<1, kSrvSlots, 0, st>>>(n, G.d_up->slots, G.d_up->roots, b.dist, b.pend, G.q[cur],
@@ -432,7 +432,7 @@ static void sp_issue(cgb_server* s, Group& G)
                                      cudaMemcpyHostToDevice, st));
         CGB_CUDA_TRY(cudaMemsetAsync(&b.c->nfar_next, 0, 4, st));
         CGB_CUDA_TRY(cudaMemsetAsync(&G.d_stats->alive[1], 0, 8, st));
-        k_mssp_split<<<kNumSMs * 8, kBlock, 0, st>>>(b.far_list[G.fcur], &b.c->nfar_live, b.dist, b.pend, b.farm,
+        k_mssp_split<<<num_sms() * 8, kBlock, 0, st>>>(b.far_list[G.fcur], &b.c->nfar_live, b.dist, b.pend, b.farm,
                                                      G.q[cur], &b.c->nq_in, b.far_list[G.fcur ^ 1], &b.c->nfar_next,
                                                      V, 0, 0, G.d_up->lo, G.d_up->hi, adv, G.d_stats->min_far,
                                                      &G.d_stats->alive[1], b.c);
@@ -442,9 +442,9 @@ static void sp_issue(cgb_server* s, Group& G)
     CGB_CUDA_TRY(cudaMemsetAsync(&G.d_stats->alive[0], 0, 8, st));
     CGB_CUDA_TRY(cudaMemsetAsync(&b.c->nq_out, 0, 4, st));
     CGB_CUDA_TRY(cudaMemsetAsync(&b.c->ndesc, 0, 4, st));
-    k_mssp_desc<<<kNumSMs * 8, kBlock, 0, st>>>(G.q[cur], &b.c->nq_in, g->off, b.pend, b.maskq, b.desc, b.desc_cap,
+    k_mssp_desc<<<num_sms() * 8, kBlock, 0, st>>>(G.q[cur], &b.c->nq_in, g->off, b.pend, b.maskq, b.desc, b.desc_cap,
                                                 b.c, g->tune_alg[CGB_SSSP].ms_edges);
-    mssp_expand(g->w != nullptr, kNumSMs * 8, st, b.desc, b.c, b.maskq, g->dst, g->w, b.dist, b.pend, b.farm,
+    mssp_expand(g->w != nullptr, num_sms() * 8, st, b.desc, b.c, b.maskq, g->dst, g->w, b.dist, b.pend, b.farm,
                 G.q[nxt], &b.c->nq_out, b.far_list[G.fcur], &b.c->nfar_live, V, 0, G.d_up->thr, G.d_stats->alive);
     k_srv_copy_u32<<<1, 1, 0, st>>>(&b.c->nq_out, &b.c->nq_in);
     CGB_CUDA_TRY(cudaMemcpyAsync(&G.h_stats->alive, &G.d_stats->alive, sizeof(G.h_stats->alive),
@@ -492,14 +492,14 @@ static void group_retire(cgb_server* s, Group& G, unsigned long long fin)
         if (__builtin_popcountll(fin) <= 4) {
             uint32_t k[4] = {0, 0, 0, 0}, n = 0;
             for (unsigned long long m = fin; m; m &= m - 1) k[n++] = __builtin_ctzll(m);
-            k_srv_sp_extract_cols<<<kNumSMs * 8, kBlock, 0, st>>>(G.sp->dist, V, make_uint4(k[0], k[1], k[2], k[3]), n,
+            k_srv_sp_extract_cols<<<num_sms() * 8, kBlock, 0, st>>>(G.sp->dist, V, make_uint4(k[0], k[1], k[2], k[3]), n,
                                                                   G.region);
         } else {
-            k_srv_sp_extract<<<kNumSMs * 8, kBlock, 0, st>>>(G.sp->dist, V, fin, G.region);
+            k_srv_sp_extract<<<num_sms() * 8, kBlock, 0, st>>>(G.sp->dist, V, fin, G.region);
         }
     }
     CGB_CUDA_TRY(cudaMemsetAsync(G.d_stats, 0, offsetof(SlotStats, alive), st));
-    k_srv_stats<<<kNumSMs * 4, kBlock, 0, st>>>(G.region, V, g->off, fin, G.d_stats->edges, G.d_stats->reached,
+    k_srv_stats<<<num_sms() * 4, kBlock, 0, st>>>(G.region, V, g->off, fin, G.d_stats->edges, G.d_stats->reached,
                                                 G.d_stats->depth);
     for (unsigned long long m = fin; m; m &= m - 1) {
         const uint32_t k = __builtin_ctzll(m);

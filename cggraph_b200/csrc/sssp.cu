@@ -279,7 +279,7 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
     CGB_CUDA_TRY(cudaEventRecord(g->ev_start, g->stream));
     if (timing) ktimer_begin(g, CGB_K_INIT);
     ++g->stats.launches;
-    k_sssp_init<<<kNumSMs * 4, kBlock, 0, g->stream>>>(V, g->value, far_bm, words);
+    k_sssp_init<<<num_sms() * 4, kBlock, 0, g->stream>>>(V, g->value, far_bm, words);
     ++g->stats.launches;
     k_sssp_root<<<1, 1, 0, g->stream>>>(g->value, root, g->q[0]);
     if (timing) ktimer_end(g);
@@ -335,7 +335,7 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
                 ensure_csc_weights(g);
             }
             ++g->stats.launches;
-            k_sssp_round_reset<<<(!pull && !dense) ? kNumSMs * 2 : 1, kBlock, 0, g->stream>>>(
+            k_sssp_round_reset<<<(!pull && !dense) ? num_sms() * 2 : 1, kBlock, 0, g->stream>>>(
                 g->ctr, out, (!pull && !dense) ? near_bm : nullptr, words);
             if (tracing) CGB_CUDA_TRY(cudaEventRecord(g->ev_iter[0], g->stream));
             if (timing) ktimer_begin(g, pull ? CGB_K_PULL : CGB_K_PUSH);
@@ -349,7 +349,7 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
                 SsspDenseOp<kHasW> op{g->off, g->dst, g->w, g->value};
                 launch_push(g, g->q[cur], (uint32_t)nnear, op, false);
                 ++g->stats.launches;
-                k_sssp_dense_scan<<<grid_for(V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(
+                k_sssp_dense_scan<<<grid_for(V, kBlock, num_sms() * 8), kBlock, 0, g->stream>>>(
                     V, g->value, g->stamp, (uint32_t)std::min<uint64_t>(thr, kValueMax), g->nz, g->off, far_bm,
                     g->q[out], &g->ctr->qlen[out], V, g->ctr);
                 g->stats.pushes_td++;
@@ -402,7 +402,7 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
             k_sssp_split_reset<<<1, 1, 0, g->stream>>>(g->ctr, out);
             if (timing) ktimer_begin(g, CGB_K_FRONTIER);
             ++g->stats.launches;
-            k_sssp_split<<<grid_for(words, kBlock, kNumSMs * 4), kBlock, 0, g->stream>>>(
+            k_sssp_split<<<grid_for(words, kBlock, num_sms() * 4), kBlock, 0, g->stream>>>(
                 words, far_bm, g->value, (uint32_t)std::min<uint64_t>(lo, kValueMax),
                 (uint32_t)std::min<uint64_t>(thr, kValueMax), g->q[out], &g->ctr->qlen[out], V, g->ctr, g->off);
             if (timing) ktimer_end(g);

@@ -251,7 +251,7 @@ void sssp_pull_round(cgb_graph* g, const uint32_t* q_in, uint32_t nin, uint32_t 
 {
     const uint32_t words = g->words();
     CGB_CUDA_TRY(cudaMemsetAsync(near_set, 0, (size_t)words * 4, g->stream));
-    k_sp_near_bitmap<<<grid_for(nin, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(q_in, nin, near_set);
+    k_sp_near_bitmap<<<grid_for(nin, kBlock, num_sms() * 8), kBlock, 0, g->stream>>>(q_in, nin, near_set);
     CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->huge_len, 0, 4, g->stream));
     CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->found, 0, 4, g->stream));
     PullArgs a{};
@@ -277,10 +277,10 @@ void sssp_pull_round(cgb_graph* g, const uint32_t* q_in, uint32_t nin, uint32_t 
     a.off = g->off;
     a.ctr = g->ctr;
     g->stats.launches += 5;
-    k_sp_pull_light<<<grid_for(g->V, kBlock, kNumSMs * 8), kBlock, 0, g->stream>>>(a);
-    k_sp_pull_warp<<<kNumSMs * 4, kBlock, 0, g->stream>>>(a);
-    k_sp_pull_chunks<<<kNumSMs * 4, kBlock, 0, g->stream>>>(a);
-    k_sp_pull_settle<<<kNumSMs, kBlock, 0, g->stream>>>(a);
+    k_sp_pull_light<<<grid_for(g->V, kBlock, num_sms() * 8), kBlock, 0, g->stream>>>(a);
+    k_sp_pull_warp<<<num_sms() * 4, kBlock, 0, g->stream>>>(a);
+    k_sp_pull_chunks<<<num_sms() * 4, kBlock, 0, g->stream>>>(a);
+    k_sp_pull_settle<<<num_sms(), kBlock, 0, g->stream>>>(a);
 }
 
 }  // namespace cgb

@@ -111,6 +111,9 @@ cgb_status cgb_autotune(cgb_graph* g, int algorithm, const uint32_t* roots, uint
     }
     cgb_tuning& slot = g->tune_alg[algorithm];
     const cgb_tuning start = slot;
+    cgb_options run_opt{};
+    run_opt.struct_size = sizeof(cgb_options);
+    run_opt.flags = (algorithm == CGB_CC && (flags & CGB_TUNE_CC_WEAK)) ? CGB_FLAG_CC_WEAK : 0u;
     // score of the graph's current tuning
     auto score = [&](double& ms) -> cgb_status {
         ms = 0;
@@ -132,7 +135,7 @@ cgb_status cgb_autotune(cgb_graph* g, int algorithm, const uint32_t* roots, uint
                 for (int rep = 0; rep < 3; rep++) {
                     double t = 0;
                     const cgb_status st =
-                        cgb_run(g, algorithm, algorithm == CGB_CC ? 0 : roots[i], nullptr, nullptr, nullptr, &t);
+                        cgb_run(g, algorithm, algorithm == CGB_CC ? 0 : roots[i], &run_opt, nullptr, nullptr, &t);
                     // (PageRank: roots[i] is the iteration count)
                     if (st != CGB_OK) return st;
                     if (rep > 0) best_rep = std::min(best_rep, t);

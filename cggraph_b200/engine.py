@@ -407,14 +407,17 @@ class Graph:
         t.struct_size = ctypes.sizeof(L.Tuning)
         check(L.lib().cgb_tuning_set(self._h, int(algorithm), ctypes.byref(t)))
 
-    def autotune(self, algorithm: int, roots: Sequence[int], batch: bool = False, keep: bool = True):
+    def autotune(self, algorithm: int, roots: Sequence[int], batch: bool = False, keep: bool = True,
+                 cc_weak: bool = False):
         """Coordinate-descent search of the launch parameters for `algorithm`
-        from `roots` (one run per root, or multi-root passes with batch=True).
-        Returns (best tuning, best ms, starting ms); the best tuning stays on
-        the graph unless keep=False."""
+        from `roots` (one run per root, or multi-root passes with batch=True;
+        CC as weak components with cc_weak=True).  Returns (best tuning, best
+        ms, starting ms); the best tuning stays on the graph unless
+        keep=False."""
         r = np.ascontiguousarray(roots, dtype=np.uint32)
         best, bms, sms = L.Tuning(), ctypes.c_double(), ctypes.c_double()
-        flags = (L.TUNE_BATCH if batch else 0) | (0 if keep else L.TUNE_KEEP_DEFAULT)
+        flags = (L.TUNE_BATCH if batch else 0) | (0 if keep else L.TUNE_KEEP_DEFAULT) | \
+            (L.TUNE_CC_WEAK if cc_weak else 0)
         check(L.lib().cgb_autotune(self._h, int(algorithm), _ptr(r), r.size, flags, ctypes.byref(best),
                                    ctypes.byref(bms), ctypes.byref(sms)))
         return {f: getattr(best, f) for f in L.TUNING_FIELDS}, bms.value, sms.value

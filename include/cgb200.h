@@ -81,6 +81,10 @@ typedef struct cgb_options {
 #define CGB_FLAG_KERNEL_TIMING 0x1u /* record per-kernel CUDA-event times (cgb_run_stats) */
 #define CGB_FLAG_TRACE 0x2u         /* log one cgb_iter_trace per iteration */
 #define CGB_FLAG_BATCH_SEQUENTIAL 0x4u /* cgb_run_batch: one cgb_run per root instead of multi-root passes */
+#define CGB_FLAG_CC_WEAK 0x8u /* CC over the edges taken as undirected (weak components): labels equal the
+                                 reference's CC on the symmetrised graph, with no symmetrised copy; on a
+                                 directed graph without it CC is the reference's label propagation along
+                                 out-edges */
 
 typedef struct cgb_graph cgb_graph;
 
@@ -96,7 +100,8 @@ typedef struct cgb_run_stats {
     uint64_t kernel_launches[8];
     uint64_t pushes_td, pulls_bu; /* BFS: levels run top-down / bottom-up */
     uint32_t sssp_delta;      /* delta used */
-    int32_t cc_path;          /* 0 = hook+compress (symmetric), 1 = label propagation */
+    int32_t cc_path;          /* 0 = hook+compress (symmetric), 1 = label propagation,
+                                 2 = hook+compress over out- and in-lists (CGB_FLAG_CC_WEAK) */
     uint64_t launches;        /* kernels launched by the run */
 } cgb_run_stats;
 
@@ -339,6 +344,7 @@ cgb_status cgb_tuning_set(cgb_graph* g, int algorithm, const cgb_tuning* t);
 
 #define CGB_TUNE_BATCH 0x1u /* tune cgb_run_batch passes of the roots (else one cgb_run per root) */
 #define CGB_TUNE_KEEP_DEFAULT 0x2u /* report the best tuning but leave the graph's tuning unchanged */
+#define CGB_TUNE_CC_WEAK 0x4u /* tune CC runs with CGB_FLAG_CC_WEAK (weak components) */
 
 /* Project-written autotuner (no counterpart in the reference, whose
  * thresholds are compile-time constants, device_warpDonate.cuh / device_CTA.cuh):

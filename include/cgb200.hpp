@@ -1,7 +1,8 @@
 // C++ adapter with the surface of the reference's SINGLE_GPU engine,
 // GraphDeviceWorklist (my_project/CGgraph/GraphDevice.cuh:9-269), so that a
 // main_partition()-style driver (my_project/CGgraph/main_partition.hpp:319-383)
-// swaps engines by changing one type name.  Header-only over the C ABI of
+// swaps engines by changing one type name (and reads PageRank results from
+// vertexValuePr).  Header-only over the C ABI of
 // cgb200.h; link with -lcgb200.
 //
 //   GraphB200 engine(csrResult, Algorithm_type::BFS);          // uploads the CSR
@@ -9,9 +10,11 @@
 //   engine.result_D2H();                                      // fills vertexValue
 //
 // Where the reference calls assert_msg / exit(1), this adapter throws
-// cgb200::error carrying the C status code.  vertexValue is uint32[V] for
-// BFS / SSSP / CC; after PageRank, vertexValuePr holds double[V] (the
-// reference's uint32 PageRank cannot represent the result).
+// cgb200::error carrying the C status code.  vertexValue is a raw pointer to
+// uint32[V] host values for BFS / SSSP / CC, owned by the engine as the
+// reference's is (GraphDevice.cuh:21,183); after PageRank, vertexValuePr
+// points at double[V] (the reference's uint32 PageRank cannot represent the
+// result).
 #ifndef CGB200_HPP
 #define CGB200_HPP
 
@@ -44,8 +47,8 @@ public:
     uint32_t vertexNum = 0;
     uint32_t edgeNum = 0;
     uint32_t noZeroOutDegreeNum = 0;
-    std::vector<uint32_t> vertexValue;
-    std::vector<double> vertexValuePr;
+    uint32_t* vertexValue = nullptr;  // uint32[V], valid for the engine's lifetime
+    double* vertexValuePr = nullptr;  // double[V], valid for the engine's lifetime
 
     GraphB200(const CsrResult& csr, int algorithm, int device = 0, const cgb_options* opt = nullptr)
         : vertexNum(csr.vertexNum), edgeNum(csr.edgeNum), noZeroOutDegreeNum(csr.noZeroOutDegreeNum),
@@ -53,6 +56,7 @@ public:
     {
         check(cgb_graph_create(csr.csr_offset, csr.csr_dest, csr.csr_weight, csr.vertexNum, csr.edgeNum,
                                csr.noZeroOutDegreeNum, device, &g_));
+        allocValues();
     }
     // The reference's other input (has_csrFile = 0, main_partition.hpp:105-116):
     // a binary edge list of 12-byte (src, dst, weight) records, built into the
@@ -64,6 +68,7 @@ public:
         check(cgb_graph_load_edge_file(edge_file.c_str(), vertices, device, &g_));
         check(cgb_graph_info(g_, &vertexNum, &edgeNum, nullptr));
         noZeroOutDegreeNum = vertexNum;
+        allocValues();
     }
     GraphB200(const GraphB200&) = delete;
     GraphB200& operator=(const GraphB200&) = delete;
@@ -82,11 +87,11 @@ public:
     void result_D2H()
     {
         if (last_ == CGB_PR) {
-            vertexValuePr.resize(vertexNum);
-            check(cgb_graph_result_download(g_, vertexValuePr.data()));
+            pr_.resize(vertexNum);
+            vertexValuePr = pr_.data();
+            check(cgb_graph_result_download(g_, vertexValuePr));
         } else {
-            vertexValue.resize(vertexNum);
-            check(cgb_graph_result_download(g_, vertexValue.data()));
+            check(cgb_graph_result_download(g_, vertexValue));
         }
     }
 
@@ -96,10 +101,18 @@ public:
     cgb_graph* handle() const { return g_; }
 
 private:
+    void allocValues()
+    {
+        values_.assign(vertexNum, 0u);
+        vertexValue = values_.data();
+    }
+
     cgb_graph* g_ = nullptr;
     int algorithm_;
     int last_ = -1;
     cgb_options opt_;
+    std::vector<uint32_t> values_;
+    std::vector<double> pr_;
 };
 
 // The surface of the reference's Reorder (my_project/CGgraph/Reorder.hpp:6-60,

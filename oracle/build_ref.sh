@@ -20,11 +20,13 @@
 #   7 my_project/CGgraph/GraphNuma.cuh:53 member "active" used at :297 but never declared
 # libnuma and TBB are replaced by the headers in oracle/refshim/.
 #
-# usage: oracle/build_ref.sh [reference root, default /root/reference]
+# usage: oracle/build_ref.sh [reference root]
+# The reference root is the argument, else $CGGRAPH_REFERENCE_ROOT, else
+# /root/reference (where the build container mounts it).
 set -euo pipefail
 
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${1:-/root/reference}/CGgraph"
+REF="${1:-${CGGRAPH_REFERENCE_ROOT:-/root/reference}}/CGgraph"
 OUT="$HERE/_ref"
 SRC="$OUT/src"
 

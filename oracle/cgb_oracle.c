@@ -189,6 +189,23 @@ int ora_pagerank(uint32_t V, const uint32_t* off, const uint32_t* dst, uint32_t 
     return 0;
 }
 
+/* In-edge CSC of a CSR by a counting sort on the destination: sources are
+ * visited in ascending order, so every in-list comes out ascending. */
+int ora_csc(uint32_t V, const uint32_t* off, const uint32_t* dst, uint32_t* in_off, uint32_t* in_src)
+{
+    uint32_t* fill = (uint32_t*)malloc(sizeof(uint32_t) * ((size_t)V + 1));
+    if (!fill) return -2;
+    memset(in_off, 0, sizeof(uint32_t) * ((size_t)V + 1));
+    uint32_t E = off[V];
+    for (uint32_t e = 0; e < E; e++) in_off[dst[e] + 1]++;
+    for (uint32_t v = 0; v < V; v++) in_off[v + 1] += in_off[v];
+    memcpy(fill, in_off, sizeof(uint32_t) * ((size_t)V + 1));
+    for (uint32_t u = 0; u < V; u++)
+        for (uint32_t e = off[u]; e < off[u + 1]; e++) in_src[fill[dst[e]]++] = u;
+    free(fill);
+    return 0;
+}
+
 /* OpenMP FP64 pull over a CSC (in_off/in_src), used as the timed CPU
  * baseline for PageRank since the reference's own PageRank does not build. */
 int ora_pagerank_pull_omp(uint32_t V, const uint32_t* off, const uint32_t* in_off, const uint32_t* in_src,
@@ -264,6 +281,8 @@ void ora_rmat_edges(uint32_t scale, uint64_t nedges, uint64_t seed, uint64_t t1,
     uint64_t m2 = mix64(seed ^ 0x5C0A12ull) | 1ull;
     uint64_t c = mix64(seed ^ 0x5C0A13ull);
     uint64_t s = mix64(seed);
+    /* each edge depends only on its index: the stream is the same for any thread count */
+#pragma omp parallel for schedule(static)
     for (uint64_t i = 0; i < nedges; i++) {
         uint64_t u = 0, v = 0;
         for (uint32_t l = 0; l < scale; l++) {
@@ -315,6 +334,7 @@ int ora_chunglu_edges(uint32_t V, uint64_t n, uint32_t i0, uint64_t seed, uint32
     cl_affine(V, seed, 0xC1A0011ull, &a_out, &b_out);
     cl_affine(V, seed, 0xC1A0021ull, &a_in, &b_in);
     uint64_t s_out = mix64(seed ^ 0xC1A0001ull), s_in = mix64(seed ^ 0xC1A0002ull), W = cum[V];
+#pragma omp parallel for schedule(static)
     for (uint64_t i = 0; i < n; i++) {
         uint64_t h = mix64(i);
         uint64_t x = cl_pick(mix64(s_out ^ h) % W, cum, V), y = cl_pick(mix64(s_in ^ h) % W, cum, V);
@@ -325,35 +345,71 @@ int ora_chunglu_edges(uint32_t V, uint64_t n, uint32_t i0, uint64_t seed, uint32
     return 0;
 }
 
-static int cmp_u64(const void* a, const void* b)
+static int cmp_u32(const void* a, const void* b)
 {
-    uint64_t x = *(const uint64_t*)a, y = *(const uint64_t*)b;
+    uint32_t x = *(const uint32_t*)a, y = *(const uint32_t*)b;
     return (x > y) - (x < y);
 }
 
 /* Edge list -> CSR: drops self-loops, optionally adds reverse edges, sorts
  * by (src, dst), removes duplicates.  Returns E, or -1 on allocation failure.
- * off must hold V+1 entries; dst_out must hold (symmetrise ? 2 : 1) * n entries. */
+ * off must hold V+1 entries; dst_out must hold (symmetrise ? 2 : 1) * n entries.
+ * Bucketed by source (counts, prefix sums, scatter), each list sorted and
+ * deduplicated on its own, then the lists packed: the same CSR as one sort
+ * of all (src, dst) pairs, for any thread count. */
 int64_t ora_build_csr(uint32_t V, uint64_t n, const uint32_t* src, const uint32_t* dst, int symmetrise,
                       uint32_t* off, uint32_t* dst_out)
 {
-    uint64_t cap = symmetrise ? 2 * n : n;
-    uint64_t* k = (uint64_t*)malloc(sizeof(uint64_t) * (cap ? cap : 1));
-    if (!k) return -1;
-    uint64_t m = 0;
+    uint64_t* pos = (uint64_t*)calloc((size_t)V + 1, sizeof(uint64_t));
+    uint32_t* len = (uint32_t*)malloc(sizeof(uint32_t) * ((size_t)V + 1));
+    if (!pos || !len) { free(pos); free(len); return -1; }
+#pragma omp parallel for schedule(static)
     for (uint64_t i = 0; i < n; i++) {
         if (src[i] == dst[i]) continue;
-        k[m++] = ((uint64_t)src[i] << 32) | dst[i];
-        if (symmetrise) k[m++] = ((uint64_t)dst[i] << 32) | src[i];
+#pragma omp atomic
+        pos[src[i] + 1]++;
+        if (symmetrise) {
+#pragma omp atomic
+            pos[dst[i] + 1]++;
+        }
     }
-    qsort(k, m, sizeof(uint64_t), cmp_u64);
+    for (uint32_t v = 0; v < V; v++) pos[v + 1] += pos[v];
+    uint64_t* fill = (uint64_t*)malloc(sizeof(uint64_t) * ((size_t)V + 1));
+    if (!fill) { free(pos); free(len); return -1; }
+    memcpy(fill, pos, sizeof(uint64_t) * ((size_t)V + 1));
+#pragma omp parallel for schedule(static)
+    for (uint64_t i = 0; i < n; i++) {
+        if (src[i] == dst[i]) continue;
+        uint64_t k;
+#pragma omp atomic capture
+        k = fill[src[i]]++;
+        dst_out[k] = dst[i];
+        if (symmetrise) {
+#pragma omp atomic capture
+            k = fill[dst[i]]++;
+            dst_out[k] = src[i];
+        }
+    }
+    free(fill);
+#pragma omp parallel for schedule(dynamic, 4096)
+    for (uint32_t v = 0; v < V; v++) {
+        uint32_t* l = dst_out + pos[v];
+        uint64_t m = pos[v + 1] - pos[v], k = 0;
+        if (m > 1) qsort(l, m, sizeof(uint32_t), cmp_u32);
+        for (uint64_t i = 0; i < m; i++)
+            if (i == 0 || l[i] != l[i - 1]) l[k++] = l[i];
+        len[v] = (uint32_t)k;
+    }
+    /* pack the deduplicated lists in place, front to back */
     uint64_t E = 0;
-    for (uint64_t i = 0; i < m; i++)
-        if (i == 0 || k[i] != k[i - 1]) k[E++] = k[i];
-    memset(off, 0, sizeof(uint32_t) * ((size_t)V + 1));
-    for (uint64_t i = 0; i < E; i++) { off[(k[i] >> 32) + 1]++; dst_out[i] = (uint32_t)k[i]; }
-    for (uint32_t v = 0; v < V; v++) off[v + 1] += off[v];
-    free(k);
+    for (uint32_t v = 0; v < V; v++) {
+        off[v] = (uint32_t)E;
+        if (E != pos[v]) memmove(dst_out + E, dst_out + pos[v], sizeof(uint32_t) * len[v]);
+        E += len[v];
+    }
+    off[V] = (uint32_t)E;
+    free(pos);
+    free(len);
     return (int64_t)E;
 }
 
@@ -363,6 +419,7 @@ void ora_edge_weights(uint32_t V, const uint32_t* off, const uint32_t* dst, uint
                       int sym_key, uint32_t* w)
 {
     uint64_t s = mix64(seed ^ 0x77E16ull);
+#pragma omp parallel for schedule(dynamic, 4096)
     for (uint32_t u = 0; u < V; u++)
         for (uint32_t e = off[u]; e < off[u + 1]; e++) {
             uint32_t a = u, b = dst[e];

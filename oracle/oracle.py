@@ -48,11 +48,13 @@ def build(force: bool = False) -> str:
     return LIB_PATH
 
 
-def build_ref(reference_root: str = "/root/reference") -> str | None:
-    """Build the reference CPU engine harness when the reference is present."""
+def build_ref(reference_root: str | None = None) -> str | None:
+    """Build the reference CPU engine harness when the reference sources are
+    present (build_ref.sh finds them: its argument, else
+    $CGGRAPH_REFERENCE_ROOT, else its default location; it keeps any
+    prebuilt harness when they are absent)."""
     script = os.path.join(HERE, "build_ref.sh")
-    if os.path.isdir(os.path.join(reference_root, "CGgraph")):
-        subprocess.check_call(["bash", script, reference_root])
+    subprocess.check_call(["bash", script] + ([reference_root] if reference_root else []))
     return REF_BIN if os.path.exists(REF_BIN) else None
 
 
@@ -73,6 +75,8 @@ def lib():
         L.ora_pagerank_pull_omp.argtypes = [ctypes.c_uint32, _u32p, _u32p, _u32p, ctypes.c_uint32,
                                             ctypes.c_int, _f64p]
         L.ora_num_threads.restype = ctypes.c_int
+        L.ora_csc.argtypes = [ctypes.c_uint32, _u32p, _u32p, _u32p, _u32p]
+        L.ora_csc.restype = ctypes.c_int
         L.ora_rmat_edges.argtypes = [ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64,
                                      ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, _u32p, _u32p]
         L.ora_build_csr.argtypes = [ctypes.c_uint32, ctypes.c_uint64, _u32p, _u32p, ctypes.c_int, _u32p, _u32p]
@@ -144,12 +148,10 @@ def csc(off, dst):
     """In-edge CSC (in_off, in_src) with ascending sources, by counting sort."""
     off, dst = _u32(off), _u32(dst)
     V = off.size - 1
-    src = np.repeat(np.arange(V, dtype=np.uint32), np.diff(off.astype(np.int64)))
-    order = np.lexsort((src, dst))
-    in_src = src[order].astype(np.uint32)
-    in_off = np.zeros(V + 1, np.uint32)
-    np.cumsum(np.bincount(dst, minlength=V), out=in_off[1:])
-    return in_off, in_src
+    in_off = np.empty(V + 1, np.uint32)
+    in_src = np.empty(max(1, dst.size), np.uint32)
+    assert lib().ora_csc(V, _p(off), _p(dst), _p(in_off), _p(in_src)) == 0
+    return in_off, in_src[:dst.size].copy()
 
 
 def pagerank_pull_omp(off, in_off, in_src, iters=20, threads=0):
@@ -341,6 +343,9 @@ def build_csr(V, src, dst, symmetrise=False):
 
 
 def edge_weights(off, dst, seed, wmax=64, sym_key=False):
+    """Seeded weights in [1, wmax]; None when wmax is 0 (an unweighted graph)."""
+    if not wmax:
+        return None
     off, dst = _u32(off), _u32(dst)
     w = np.empty(dst.size, np.uint32)
     lib().ora_edge_weights(off.size - 1, _p(off), _p(dst), seed, wmax, int(sym_key), _p(w))

@@ -157,7 +157,7 @@ def make_sortnbr():
 
 def main():
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
-    ref_root = args[0] if args else "/root/reference"
+    ref_root = args[0] if args else os.environ.get("CGGRAPH_REFERENCE_ROOT", "/root/reference")
     O.build()
     if O.build_ref(ref_root) is None:
         raise SystemExit("reference oracle unavailable")
