@@ -564,26 +564,42 @@ def bench_shapes(args, cg, L, dev):
 
 def bench_serving(args, cg, L, dev):
     """Serving: BFS/SSSP queries (half each, seeded uniform non-isolated
-    roots) with Poisson arrivals at 1k, 5k and 20k req/s against a resident
-    RMAT graph (scale --serve-scale, weights [1,64]), and at 1k req/s against
-    the 4800 x 5000 grid (weights [1,1000]); latency = completion - arrival."""
+    roots) with Poisson arrivals against a resident RMAT graph (scale
+    --serve-scale, weights [1,64]) at 25, 50 and 100 req/s (below the
+    server's capacity, so latency is service time) and at 1k, 5k and 20k
+    req/s (above it: throughput), and at 2 and 1k req/s against the
+    4800 x 5000 grid (weights [1,1000]); latency = completion - arrival.
+    Each rate also reports the lone-run latency of its queries' median
+    (one cgb_run) for comparison."""
     out = {}
+    n_sub = max(32, args.serve_requests // 4)
     cases = [(f"rmat{args.serve_scale}", lambda: cg.Graph.rmat(args.serve_scale, 16, args.seed + 3, wmax=64,
-                                                                   device=dev), (1000, 5000, 20000),
-              args.serve_requests)]
+                                                                   device=dev),
+              ((25, n_sub), (50, n_sub), (100, n_sub), (1000, args.serve_requests), (5000, args.serve_requests),
+               (20000, args.serve_requests)))]
     if args.serve_scale >= 20:
-        cases.append(("grid4800x5000", lambda: cg.Graph.grid(4800, 5000, seed=1, device=dev), (1000,),
-                      max(64, args.serve_requests // 2)))
-    for name, make, rates, nreq in cases:
+        cases.append(("grid4800x5000", lambda: cg.Graph.grid(4800, 5000, seed=1, device=dev),
+                      ((2, 16), (1000, max(64, args.serve_requests // 2)))))
+    for name, make, rates in cases:
         g = make()
         off_h, _, _ = g.download(with_weight=False)
         deg = np.diff(off_h.astype(np.int64))
         nzv = np.nonzero(deg)[0]
-        res = {"vertices": g.vertexNum, "edges": g.edgeNum, "requests_per_rate": nreq}
+        res = {"vertices": g.vertexNum, "edges": g.edgeNum}
         with cg.Server(g) as srv:
             st = srv.stats()
             res["slots"] = {"bfs": st["bfs_slots"], "sssp": st["sssp_slots"]}
-        for rate in rates:
+        # lone runs: the service time a query has on an idle engine
+        lone = {}
+        rng0 = np.random.default_rng(args.seed + 99)
+        for a, an in ((BFS, "bfs"), (SSSP, "sssp")):
+            ms = []
+            for r in nzv[rng0.integers(0, nzv.size, 6)]:
+                g.run(a, int(r), to_host=False)
+                ms.append(g.stats().ms)
+            lone[an] = {"median_ms": float(np.median(ms)), "max_ms": float(np.max(ms))}
+        res["lone_run"] = lone
+        for rate, nreq in rates:
             rng = np.random.default_rng(args.seed * 1000 + rate)
             arrivals = np.cumsum(rng.exponential(1e6 / rate, nreq))
             algs_q = rng.integers(0, 2, nreq)
@@ -603,7 +619,8 @@ def bench_serving(args, cg, L, dev):
                 la = np.array([r["done_us"] - r["arrival_us"] for r in recs if r["algorithm"] == a]) / 1e3
                 if la.size:
                     per[an] = {"p50_ms": float(np.percentile(la, 50)), "p99_ms": float(np.percentile(la, 99))}
-            res[f"rate{rate}"] = {"completed": len(recs), "errors": sum(1 for r in recs if r["status"] != 0),
+            res[f"rate{rate}"] = {"requests": nreq, "completed": len(recs),
+                                  "errors": sum(1 for r in recs if r["status"] != 0),
                                   "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                                   "throughput_req_s": len(recs) / makespan, "gteps": edges / makespan / 1e9,
                                   "ticks": sst["ticks"], "per_algorithm": per}

@@ -35,8 +35,9 @@ EXPORTS = [
     "cgb_batch_info", "cgb_batch_stats", "cgb_server_create", "cgb_server_submit", "cgb_server_start",
     "cgb_server_wait", "cgb_server_poll", "cgb_server_stats", "cgb_server_destroy", "cgb_tuning_get",
     "cgb_tuning_set", "cgb_autotune", "cgb_memory_trim", "cgb_memory_info", "cgb_memory_reserve",
+    "cgb_check_barrier_timeout",
 ]
-POLICY_FEATURES, POLICY_OUTPUTS, POLICY_PARAMS = 24, 9, 6345
+POLICY_FEATURES, POLICY_OUTPUTS, POLICY_PARAMS = 24, 14, 6670
 
 
 class Options(ctypes.Structure):
@@ -120,14 +121,15 @@ class Tuning(ctypes.Structure):
         ("sssp_pull_alpha", ctypes.c_uint32),
         ("cluster_enter", ctypes.c_uint32),
         ("sssp_dense_alpha", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32 * 3),
+        ("push_block", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 2),
     ]
 
 
 TUNE_BATCH, TUNE_KEEP_DEFAULT, TUNE_CC_WEAK = 0x1, 0x2, 0x4
 TUNING_FIELDS = ("push_big_deg", "push_chunk", "push_ctas_per_sm", "persist_enter", "persist_deg", "ms_edges",
                  "pr_unroll", "pr_ctas_per_sm", "persist_ctas", "sssp_pull_alpha",
-                 "cluster_enter", "sssp_dense_alpha")
+                 "cluster_enter", "sssp_dense_alpha", "push_block")
 
 
 class ServerConfig(ctypes.Structure):
@@ -142,7 +144,7 @@ class ServerConfig(ctypes.Structure):
     ]
 
 
-SERVER_NO_BFS, SERVER_NO_SSSP = 0x1, 0x2
+SERVER_NO_BFS, SERVER_NO_SSSP, SERVER_HOST_TICKS = 0x1, 0x2, 0x4
 
 
 class RequestInfo(ctypes.Structure):

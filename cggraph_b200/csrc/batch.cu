@@ -87,10 +87,13 @@ __global__ void k_batch_roots(const uint32_t* roots, const uint32_t* base, uint3
     }
     st->qlen[0] = len;
     if (sx) {
+        sx->bucket_lo = 0;
         sx->thr[0] = delta;
         for (int k = 0; k < 3; k++) {
             sx->min_far[k] = kValueMax;
             sx->far_delta[k] = 0;
+            sx->kept[k] = 0;
+            sx->split[k] = 0;
         }
     }
 }
@@ -217,7 +220,7 @@ cgb_status cgb_batch_create(uint32_t n, const uint32_t* const* offsets, const ui
             CGB_CUDA_TRY(cudaMemcpy(b->d_base, b->base.data(), (n + 1) * 4ull, cudaMemcpyHostToDevice));
             CGB_CUDA_TRY(cudaMalloc((void**)&b->sx, sizeof(PersistSssp)));
             ensure_frontier(g);
-            if (!g->persist) g->persist = pool_alloc(sizeof(PersistState), g->stream);
+            if (!g->persist) g->persist = pool_alloc(sizeof(PersistBlock), g->stream);
             b->delta = sssp_default_delta(g);
         } catch (...) {
             if (b->g) graph_free(b->g);

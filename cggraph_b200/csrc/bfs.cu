@@ -37,6 +37,7 @@ struct BfsTdOp {
     uint32_t* qlen;
     uint32_t cap;
     DevCounters* ctr;
+    static constexpr int kBatch = 4;  // edge slots per lane visited together (push.cuh)
 
     __device__ __forceinline__ bool load(uint32_t v, uint32_t& s, uint32_t& d, uint32_t& m) const
     {
@@ -45,34 +46,55 @@ struct BfsTdOp {
         m = 0;
         return true;
     }
-    __device__ __forceinline__ void edge(bool valid, uint32_t e, uint32_t) const
+    template <int N>
+    __device__ __forceinline__ void edges(const bool (&valid)[N], const uint32_t (&e)[N], const uint32_t (&)[N]) const
     {
-        bool win = false;
-        uint32_t d = 0;
-        if (valid) {
-            d = __ldcs(dst + e);  // streamed once: evict first, keep the visited bitmap in L2
-            const uint32_t bit = 1u << (d & 31u);
-            uint32_t* wp = visited + (d >> 5);
-            if (!(*wp & bit)) {
-                const uint32_t old = atomicOr(wp, bit);
-                if (!(old & bit)) {
-                    win = true;
-                    level[d] = next_level;
-                }
-            }
+        uint32_t d[N], word[N], bit[N], lo[N], hi[N];
+        bool win[N], enq[N];
+#pragma unroll
+        for (int i = 0; i < N; i++) d[i] = valid[i] ? __ldcs(dst + e[i]) : 0u;  // streamed once: evict first
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+            bit[i] = 1u << (d[i] & 31u);
+            word[i] = valid[i] ? visited[d[i] >> 5] : ~0u;
         }
-        const bool enq = win && d < nz;
-        uint32_t deg = 0;
-        if (enq) deg = off[d + 1] - off[d];
-        warp_append(enq, d, qout, qlen, cap, &ctr->overflow);
-        if (__any_sync(0xffffffffu, enq)) {
-            const unsigned long long s = warp_sum((unsigned long long)deg);
-            const uint32_t mx = warp_max(deg);
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+            win[i] = false;
+            if (!(word[i] & bit[i])) win[i] = !(atomicOr(visited + (d[i] >> 5), bit[i]) & bit[i]);
+        }
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+            if (win[i]) level[d[i]] = next_level;
+            enq[i] = win[i] && d[i] < nz;
+            lo[i] = enq[i] ? off[d[i]] : 0u;
+            hi[i] = enq[i] ? off[d[i] + 1] : 0u;
+        }
+        warp_append_n<N>(enq, d, qout, qlen, cap, &ctr->overflow);
+        bool any = false;
+#pragma unroll
+        for (int i = 0; i < N; i++) any |= enq[i];
+        if (__any_sync(0xffffffffu, any)) {
+            unsigned long long sum = 0;
+            uint32_t mx = 0;
+#pragma unroll
+            for (int i = 0; i < N; i++) {
+                sum += hi[i] - lo[i];
+                mx = max(mx, hi[i] - lo[i]);
+            }
+            sum = warp_sum(sum);
+            mx = warp_max(mx);
             if (lane_id() == 0) {
-                atomicAdd(&s_td_medges, s);
+                atomicAdd(&s_td_medges, sum);
                 atomicMax(&s_td_maxdeg, mx);
             }
         }
+    }
+    __device__ __forceinline__ void edge(bool valid, uint32_t e, uint32_t m) const
+    {
+        const bool v[1] = {valid};
+        const uint32_t ee[1] = {e}, mm[1] = {m};
+        edges<1>(v, ee, mm);
     }
     __device__ __forceinline__ void block_begin() const
     {
@@ -114,7 +136,10 @@ __global__ void k_q2bm(const uint32_t* __restrict__ q, uint32_t n, uint32_t* bm)
 }
 
 // One bottom-up level.  Reads front (current frontier bitmap), writes
-// next (all words, so it needs no clearing) and the next queue.
+// next (all words, so it needs no clearing) and the next queue.  Each lane
+// scans its vertex's in-list four entries at a time: four source loads,
+// then their four frontier words, are in flight together, and the scan
+// stops after the group that holds a parent.
 __global__ void __launch_bounds__(kBlock) k_bfs_bu(uint32_t V, const uint32_t* __restrict__ in_off,
                                                    const uint32_t* __restrict__ in_src,
                                                    const uint32_t* __restrict__ off, uint32_t* level,
@@ -132,12 +157,14 @@ __global__ void __launch_bounds__(kBlock) k_bfs_bu(uint32_t V, const uint32_t* _
         bool found = false;
         if (v < V && !((vis >> lane_id()) & 1u)) {
             const uint32_t e1 = in_off[v + 1];
-            for (uint32_t e = in_off[v]; e < e1; e++) {
-                const uint32_t u = in_src[e];
-                if ((front[u >> 5] >> (u & 31u)) & 1u) {
-                    found = true;
-                    break;
-                }
+            for (uint32_t e = in_off[v]; e < e1 && !found; e += 4) {
+                uint32_t u[4], f[4];
+#pragma unroll
+                for (int k = 0; k < 4; k++) u[k] = e + k < e1 ? in_src[e + k] : in_src[e];
+#pragma unroll
+                for (int k = 0; k < 4; k++) f[k] = front[u[k] >> 5] >> (u[k] & 31u);
+#pragma unroll
+                for (int k = 0; k < 4; k++) found |= (f[k] & 1u) != 0;
             }
         }
         const uint32_t fm = __ballot_sync(0xffffffffu, found);
@@ -224,8 +251,9 @@ void run_bfs(cgb_graph* g, uint32_t root, const cgb_options& o)
     const uint64_t max_iters = o.max_iterations ? o.max_iterations : (uint64_t)V + 2;
 
     // Queues one level in the given direction (frontier in q[cur] and, when
-    // the last level was pulled, in `front`; next frontier to q[out] / next).
-    auto do_level = [&](bool pull, int out) {
+    // the last level was pulled, in `front`; next frontier to q[out] / next);
+    // a push level with the given expansion variant (PushExpand).
+    auto do_level = [&](bool pull, int out, int expand) {
         reset_level_counters(g, out);
         if (pull) {
             if (!bottom_up) {
@@ -246,7 +274,7 @@ void run_bfs(cgb_graph* g, uint32_t root, const cgb_options& o)
         } else {
             if (timing) ktimer_begin(g, CGB_K_PUSH);
             BfsTdOp op{g->off, g->dst, g->value, g->visited, level + 1, g->nz, g->q[out], &g->ctr->qlen[out], V, g->ctr};
-            launch_push(g, g->q[cur], (uint32_t)nf, op, false);
+            launch_push(g, g->q[cur], (uint32_t)nf, op, false, expand);
             if (timing) ktimer_end(g);
         }
     };
@@ -267,7 +295,9 @@ void run_bfs(cgb_graph* g, uint32_t root, const cgb_options& o)
         return in;
     };
 
-    const bool persist_ok = !tracing && o.schedule != CGB_SCHED_FIXED;
+    // device-resident levels for small frontiers (not while collecting
+    // samples, which time each level's variants on the host)
+    const bool persist_ok = !tracing && !collect && o.schedule != CGB_SCHED_FIXED;
     while (nf > 0) {
         CGB_REQUIRE(iters < max_iters, CGB_ETIMEOUT, "BFS iteration budget exhausted");
         // ----- direction decision
@@ -299,33 +329,45 @@ void run_bfs(cgb_graph* g, uint32_t root, const cgb_options& o)
             }
         }
         const int out = cur ^ 1;
+        // the heuristic's expansion of a push level: every list of 32 edges or
+        // more chunked for small frontiers, else the degree-binned tiers
+        const int heur_expand = nf <= kSmallFrontier ? kExpandChunked : kExpandBinned;
         bool go_pull;
+        int expand = heur_expand;
         if (force_pull) go_pull = true;
         else if (!want_pull) go_pull = false;
         else if (collect) {
-            // counterfactual: time both directions from the same state
+            // counterfactual: time the three level variants from the same state
             const size_t vbytes = (size_t)V * 4, wbytes = (size_t)words * 4;
             CGB_CUDA_TRY(cudaMemcpyAsync(collect->save_value, g->value, vbytes, cudaMemcpyDeviceToDevice, g->stream));
             CGB_CUDA_TRY(cudaMemcpyAsync(collect->save_bm0, g->visited, wbytes, cudaMemcpyDeviceToDevice, g->stream));
             float ms[kPolicyOutputs] = {};
             bool have[kPolicyOutputs] = {};
-            for (int d = 0; d < 2; d++) {
+            const int outs[3] = {kOutPush, kOutPull, kOutPushChunked};
+            for (int d = 0; d < 3; d++) {
                 CGB_CUDA_TRY(cudaEventRecord(g->ev_iter[0], g->stream));
-                do_level(d == 1, out);
+                do_level(d == 1, out, d == 2 ? kExpandChunked : kExpandBinned);
                 CGB_CUDA_TRY(cudaEventRecord(g->ev_iter[1], g->stream));
                 sync_counters(g);
-                CGB_CUDA_TRY(cudaEventElapsedTime(&ms[kOutPush + d], g->ev_iter[0], g->ev_iter[1]));
-                have[kOutPush + d] = true;
+                CGB_CUDA_TRY(cudaEventElapsedTime(&ms[outs[d]], g->ev_iter[0], g->ev_iter[1]));
+                have[outs[d]] = true;
                 CGB_CUDA_TRY(cudaMemcpyAsync(g->value, collect->save_value, vbytes, cudaMemcpyDeviceToDevice,
                                              g->stream));
                 CGB_CUDA_TRY(cudaMemcpyAsync(g->visited, collect->save_bm0, wbytes, cudaMemcpyDeviceToDevice,
                                              g->stream));
             }
             policy_log_sample(g, state_now(), ms, have);
-            go_pull = ms[kOutPull] < ms[kOutPush];
+            int best = 0;
+            for (int d = 1; d < 3; d++)
+                if (ms[outs[d]] < ms[outs[best]]) best = d;
+            go_pull = best == 1;
+            expand = best == 2 ? kExpandChunked : kExpandBinned;
         } else if (pol && have_policy_out) {
-            const int choice = policy_pick_direction(g->h_ctr->policy_out);
+            const int hc = heur ? 1 : (heur_expand == kExpandChunked ? 2 : 0);
+            const int choice = policy_pick_bfs_level(g->h_ctr->policy_out, hc);
             go_pull = choice < 0 ? heur : choice == 1;
+            if (choice == 0) expand = kExpandBinned;
+            if (choice == 2) expand = kExpandChunked;
         } else {
             go_pull = heur;
         }
@@ -333,7 +375,7 @@ void run_bfs(cgb_graph* g, uint32_t root, const cgb_options& o)
         float it_ms = 0.f;
         if (tracing) CGB_CUDA_TRY(cudaEventRecord(g->ev_iter[0], g->stream));
         const FeatIn before = state_now();
-        do_level(go_pull, out);
+        do_level(go_pull, out, expand);
         if (go_pull) {
             if (!bottom_up) {
                 awake = nf;
@@ -355,7 +397,7 @@ void run_bfs(cgb_graph* g, uint32_t root, const cgb_options& o)
         if (infer) {
             FeatIn in = before;
             in.unvisited_e = (double)std::max<int64_t>(edges_to_check - (int64_t)scout, 0);
-            policy_enqueue(pol, g, in, true, go_pull, out);
+            policy_enqueue(pol, g, in, 1, go_pull, out);
         }
         sync_counters(g);
         have_policy_out = infer;

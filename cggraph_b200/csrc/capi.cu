@@ -10,6 +10,7 @@
 #include "../../include/cgb200.h"
 #include "../../include/cgb200_gen.h"
 #include "engine.cuh"
+#include "persist.cuh"
 
 namespace cgb {
 cgb_graph* gen_rmat(uint32_t scale, uint32_t ef, uint64_t seed, double a, double b, double c, int scr, int sym,
@@ -60,6 +61,16 @@ static void copy_any(void* dst, const void* src, size_t bytes, cudaStream_t s)
 extern "C" {
 
 int cgb_abi_version(void) { return CGB_ABI_VERSION; }
+
+cgb_status cgb_check_barrier_timeout(int device, uint32_t spin_limit)
+{
+    return guarded([&] {
+        CGB_REQUIRE(spin_limit >= 1 && spin_limit <= (1u << 24), CGB_EINVAL, "spin_limit must be in [1, 2^24]");
+        CGB_CUDA_TRY(cudaSetDevice(device));
+        const cgb_status st = barrier_timeout_check(spin_limit);
+        if (st != CGB_OK) throw Error{st, "grid barrier gave up after spin_limit polls (the expected outcome)"};
+    });
+}
 
 const char* cgb_last_error_string(void) { return last_error().c_str(); }
 
@@ -471,6 +482,8 @@ cgb_status cgb_policy_collect(cgb_graph* g, int algorithm, uint32_t root, const 
         CGB_CUDA_TRY(cudaSetDevice(g->device));
         CGB_CUDA_TRY(cudaMalloc((void**)&ps.save_value, (size_t)g->V * 4));
         CGB_CUDA_TRY(cudaMalloc((void**)&ps.save_bm0, (size_t)g->words() * 4));
+        CGB_CUDA_TRY(cudaMalloc((void**)&ps.save_q, (size_t)g->V * 4));
+        CGB_CUDA_TRY(cudaMalloc((void**)&ps.save_ctr, sizeof(DevCounters)));
         g->collect = &ps;
         try {
             run_one(g, algorithm, root, o);
@@ -482,6 +495,8 @@ cgb_status cgb_policy_collect(cgb_graph* g, int algorithm, uint32_t root, const 
     });
     if (ps.save_value) cudaFree(ps.save_value);
     if (ps.save_bm0) cudaFree(ps.save_bm0);
+    if (ps.save_q) cudaFree(ps.save_q);
+    if (ps.save_ctr) cudaFree(ps.save_ctr);
     if (count) *count = ps.count;
     return st;
 }

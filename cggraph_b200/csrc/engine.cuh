@@ -38,6 +38,7 @@ struct PolicySamples {
     uint32_t* save_bm0 = nullptr;
     uint32_t* save_bm1 = nullptr;
     uint32_t* save_q = nullptr;
+    DevCounters* save_ctr = nullptr;
 };
 
 namespace cgb {
@@ -72,6 +73,7 @@ inline cgb_tuning default_tuning()
     t.sssp_pull_alpha = 0;
     t.cluster_enter = 8192;
     t.sssp_dense_alpha = 4;
+    t.push_block = 256;
     return t;
 }
 

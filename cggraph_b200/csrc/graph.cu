@@ -1074,8 +1074,9 @@ void ensure_frontier(cgb_graph* g)
     g->q[0] = dalloc<uint32_t>(V, g->stream);
     g->q[1] = dalloc<uint32_t>(V, g->stream);
     // any frontier (each vertex once): sum over lists >= big_deg of ceil(deg / chunk)
-    // <= E / chunk + E / big_deg, at the smallest sizes cgb_tuning_set allows
-    g->chunk_cap = (uint32_t)std::min<uint64_t>((uint64_t)g->E / kMinChunk + g->E / kMinBigDeg + 64, 0xFFFFFFF0ull);
+    // <= E / chunk + E / big_deg, at the smallest sizes launch_push uses (kMinChunk;
+    // big_deg 32 for small frontiers, else at least kMinBigDeg)
+    g->chunk_cap = (uint32_t)std::min<uint64_t>((uint64_t)g->E / kMinChunk + g->E / 32 + 64, 0xFFFFFFF0ull);
     g->chunk_q = dalloc<uint2>(g->chunk_cap, g->stream);
     g->visited = dalloc<uint32_t>(g->words(), g->stream);
     g->front_bm = dalloc<uint32_t>(2 * (size_t)g->words(), g->stream);

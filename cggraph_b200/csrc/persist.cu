@@ -32,22 +32,6 @@ __device__ __forceinline__ void expand_small(const uint32_t* __restrict__ qin, u
     }
 }
 
-__device__ __forceinline__ void append(bool pred, uint32_t item, uint32_t* q, uint32_t* ctr, uint32_t cap,
-                                       PersistState* st)
-{
-    const uint32_t want = __ballot_sync(0xffffffffu, pred);
-    if (!want) return;
-    const uint32_t leader = __ffs(want) - 1;
-    uint32_t base = 0;
-    if (lane_id() == leader) base = atomicAdd(ctr, (uint32_t)__popc(want));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    if (pred) {
-        const uint32_t idx = base + __popc(want & lanemask_lt());
-        if (idx < cap) q[idx] = item;
-        else atomicOr(&st->status, 2u);
-    }
-}
-
 __global__ void __launch_bounds__(kBlock) k_bfs_persistent(const uint32_t* __restrict__ off,
                                                            const uint32_t* __restrict__ dst, uint32_t* level,
                                                            uint32_t* visited, uint32_t* q0, uint32_t* q1, uint32_t cap,
@@ -188,107 +172,61 @@ __global__ void __launch_bounds__(kThreads, 1) k_bfs_cluster(const uint32_t* __r
     }
 }
 
-template <bool kHasW>
-__global__ void __launch_bounds__(kBlock) k_sssp_persistent(const uint32_t* __restrict__ off,
-                                                            const uint32_t* __restrict__ dst,
-                                                            const uint32_t* __restrict__ w, uint32_t* dist,
-                                                            uint32_t* near_bm3, uint32_t words, uint32_t* far_bm,
-                                                            uint32_t* q0, uint32_t* q1, uint32_t cap, uint32_t nz,
-                                                            uint32_t thr, uint32_t cur, uint32_t nf_exit,
-                                                            uint32_t max_rounds, DevCounters* ctr, PersistState* st)
-{
-    uint32_t it = 0;
-    const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x, gthreads = gridDim.x * blockDim.x;
-    for (; it < max_rounds; it++) {
-        const uint32_t s_cur = it % 3, s_next = (it + 1) % 3, s_zero = (it + 2) % 3;
-        const uint32_t nf = *(volatile uint32_t*)&st->qlen[s_cur];
-        if (nf == 0 || nf > nf_exit) break;
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
-            st->qlen[s_zero] = 0;
-            st->added += nf;
-        }
-        uint32_t* zero_bm = near_bm3 + (size_t)s_zero * words;
-        for (uint32_t i = gtid; i < words; i += gthreads) zero_bm[i] = 0;
-        uint32_t* nbm = near_bm3 + (size_t)s_next * words;
-        const uint32_t* qin = cur ? q1 : q0;
-        uint32_t* qout = cur ? q0 : q1;
-        auto load = [&](uint32_t v, uint32_t& s, uint32_t& d, uint32_t& m) {
-            s = off[v];
-            d = off[v + 1] - s;
-            m = dist[v];
-        };
-        auto visit = [&](bool valid, uint32_t e, uint32_t du) {
-            bool to_near = false, new_far = false;
-            uint32_t d = 0;
-            if (valid && du < kValueMax) {
-                d = dst[e];
-                const uint64_t cand = (uint64_t)du + (kHasW ? (uint64_t)w[e] : 1ull);
-                if (cand < kValueMax) {
-                    const uint32_t nd = (uint32_t)cand;
-                    if (nd < dist[d]) {
-                        const uint32_t old = atomicMin(dist + d, nd);
-                        if (nd < old && d < nz) {
-                            const uint32_t bit = 1u << (d & 31u);
-                            uint32_t* wp = (nd < thr ? nbm : far_bm) + (d >> 5);
-                            const bool fresh = !(*wp & bit) && !(atomicOr(wp, bit) & bit);
-                            to_near = fresh && nd < thr;
-                            new_far = fresh && nd >= thr;
-                        }
-                    }
-                }
-            }
-            append(to_near, d, qout, &st->qlen[s_next], cap, st);
-            const uint32_t nfar = __popc(__ballot_sync(0xffffffffu, new_far));
-            if (nfar && lane_id() == 0) atomicAdd(&ctr->far_len[0], nfar);  // the host loop's far count
-        };
-        expand_small(qin, nf, load, visit);
-        if (!grid_barrier(st)) break;
-        cur ^= 1;
-    }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        st->levels = it;
-        st->cur = cur;
-        st->nf = st->qlen[it % 3];
-    }
-}
-
-
-// Whole delta-stepping SSSP on the device (used for graph batches, whose
-// frontiers are small): each round either expands the near queue at the
-// current threshold or, when it is empty and far vertices remain, splits
-// the far bitmap at the next bucket [lo, hi) into a new near queue.  The
-// thresholds, the smallest far distance and the change of the far count
-// rotate over the same three slots as the queue lengths; every CTA keeps
-// the running far count itself by adding the previous round's change, so
-// all CTAs take the same decision each round.
+// Whole delta-stepping SSSP on the device (graph batches, whose frontiers
+// are small, and the tail of a single run once its frontiers are): each
+// round either expands the near queue at the current threshold or, when it
+// is empty and far vertices remain, splits the far bitmap at the next bucket
+// [lo, hi) into a new near queue.  The thresholds, the smallest far
+// distance, the change of the far count and the longest list of the next
+// frontier rotate over the same three slots as the queue lengths; every CTA
+// keeps the running far count itself by adding the previous round's change,
+// so all CTAs take the same decision each round.  The loop leaves before a
+// round whose frontier exceeds nf_exit vertices or holds a list of deg_exit
+// edges or more (the host loop's binned kernels take those), and sx
+// receives the far count and bucket bound the host continues from; the far
+// count is also written to *far_len_out (the host loop's counter) when it is
+// given.  Each split recounts the far bitmap's population rather than
+// subtracting what it cleared, so a count that was off (it only decides
+// when the run ends) is corrected at the next split.
 template <bool kHasW>
 __global__ void __launch_bounds__(kBlock) k_sssp_device(const uint32_t* __restrict__ off,
                                                         const uint32_t* __restrict__ dst,
                                                         const uint32_t* __restrict__ w, uint32_t* dist,
                                                         uint32_t* near_bm3, uint32_t words, uint32_t* far_bm,
                                                         uint32_t* q0, uint32_t* q1, uint32_t cap, uint32_t nz,
-                                                        uint32_t delta, uint32_t max_rounds, PersistState* st,
-                                                        PersistSssp* sx)
+                                                        uint32_t delta, uint32_t max_rounds, uint32_t nf_exit,
+                                                        uint32_t deg_exit, uint32_t cur, PersistState* st,
+                                                        PersistSssp* sx, uint32_t* far_len_out)
 {
-    uint32_t it = 0, cur = 0, far = 0;
+    uint32_t it = 0, far = 0, far_now = 0;
+    uint64_t bucket_lo = *(volatile unsigned long long*)&sx->bucket_lo;
     const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x, gthreads = gridDim.x * blockDim.x;
+    const uint32_t lane = lane_id();
     for (; it < max_rounds; it++) {
         const uint32_t s_cur = it % 3, s_next = (it + 1) % 3, s_zero = (it + 2) % 3;
         const uint32_t nf = *(volatile uint32_t*)&st->qlen[s_cur];
-        far += *(volatile uint32_t*)&sx->far_delta[s_cur];
+        far_now = *(volatile uint32_t*)&sx->split[s_cur] ? *(volatile uint32_t*)&sx->kept[s_cur]
+                                                          : far + *(volatile uint32_t*)&sx->far_delta[s_cur];
         const uint64_t thr = *(volatile unsigned long long*)&sx->thr[s_cur];
         const uint32_t min_far = *(volatile uint32_t*)&sx->min_far[s_cur];
-        if (nf == 0 && far == 0) break;
+        const uint32_t mdeg = *(volatile uint32_t*)&st->max_deg[s_cur];
+        if (nf == 0 && far_now == 0) break;
+        if (nf > nf_exit || mdeg >= deg_exit) break;
+        far = far_now;
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             st->qlen[s_zero] = 0;
+            st->max_deg[s_zero] = 0;
             sx->min_far[s_zero] = kValueMax;
             sx->far_delta[s_zero] = 0;
+            sx->kept[s_zero] = 0;
+            sx->split[s_zero] = 0;
             st->added += nf;
         }
         uint32_t* zero_bm = near_bm3 + (size_t)s_zero * words;
         for (uint32_t i = gtid; i < words; i += gthreads) zero_bm[i] = 0;
         const uint32_t* qin = cur ? q1 : q0;
         uint32_t* qout = cur ? q0 : q1;
+        uint32_t mx = 0;  // longest list this thread appended to the next frontier
         if (nf > 0) {
             // expansion round at threshold thr
             if (blockIdx.x == 0 && threadIdx.x == 0) sx->thr[s_next] = thr;
@@ -320,6 +258,7 @@ __global__ void __launch_bounds__(kBlock) k_sssp_device(const uint32_t* __restri
                     }
                 }
                 append(to_near, d, qout, &st->qlen[s_next], cap, st);
+                if (to_near) mx = max(mx, off[d + 1] - off[d]);
                 const uint32_t nfar = __popc(__ballot_sync(0xffffffffu, new_far));
                 if (nfar && lane_id() == 0) atomicAdd(&sx->far_delta[s_next], nfar);
             };
@@ -333,48 +272,71 @@ __global__ void __launch_bounds__(kBlock) k_sssp_device(const uint32_t* __restri
                 const uint64_t j = ((uint64_t)min_far / delta + 1) * (uint64_t)delta;
                 if (j > hi) hi = j;
             }
-            if (blockIdx.x == 0 && threadIdx.x == 0) sx->thr[s_next] = hi;
+            bucket_lo = lo;
+            if (blockIdx.x == 0 && threadIdx.x == 0) {
+                sx->thr[s_next] = hi;
+                sx->split[s_next] = 1;
+            }
             const uint32_t lo32 = (uint32_t)(lo < kValueMax ? lo : kValueMax);
             const uint32_t hi32 = (uint32_t)(hi < kValueMax ? hi : kValueMax);
-            uint32_t mn = kValueMax, cleared = 0;
-            const uint32_t words_round = (words + 31u) & ~31u;
-            for (uint32_t wi = gtid; wi < words_round; wi += gthreads) {
-                uint32_t word = wi < words ? far_bm[wi] : 0u;
-                uint32_t keep = word;
-                while (__any_sync(0xffffffffu, word != 0)) {
-                    bool to_near = false;
-                    uint32_t v = 0;
-                    if (word) {
-                        const uint32_t b = __ffs(word) - 1;
-                        word &= word - 1;
-                        v = wi * 32 + b;
-                        const uint32_t dv = dist[v];
-                        if (dv < hi32) {
-                            keep &= ~(1u << b);
-                            cleared++;
-                            to_near = dv >= lo32;
-                        } else {
-                            mn = min(mn, dv);
+            uint32_t mn = kValueMax, kept = 0;
+            // a warp takes 4 x 32 words with four coalesced loads in flight
+            // (the far bitmap is mostly empty on high-diameter graphs, so the
+            // scan itself is most of a split); lane b of word j reads the
+            // distance of vertex 32 j + b (coalesced); the warp owns its
+            // words, so it writes back what stays without atomics
+            const uint32_t gw = gtid / 32, nwarps = gthreads / 32;
+            for (uint32_t w4 = gw * 128; w4 < words; w4 += nwarps * 128) {
+                uint32_t mine[4];
+#pragma unroll
+                for (int k = 0; k < 4; k++) mine[k] = w4 + 32 * k + lane < words ? far_bm[w4 + 32 * k + lane] : 0u;
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const uint32_t w0 = w4 + 32 * k;
+                    uint32_t todo = __ballot_sync(0xffffffffu, mine[k] != 0);
+                    while (todo) {
+                        const uint32_t j = __ffs(todo) - 1;
+                        todo &= todo - 1;
+                        const uint32_t bits = __shfl_sync(0xffffffffu, mine[k], j);
+                        const uint32_t v = (w0 + j) * 32 + lane;
+                        const bool in = (bits >> lane) & 1u;
+                        const uint32_t dv = in ? dist[v] : 0u;
+                        const bool leave = in && dv < hi32;
+                        const bool to_near = leave && dv >= lo32;
+                        const bool keep = in && !leave;
+                        if (keep) mn = min(mn, dv);
+                        const uint32_t km = __ballot_sync(0xffffffffu, keep);
+                        if (lane == 0) {
+                            if (km != bits) far_bm[w0 + j] = km;
+                            kept += __popc(km);
                         }
+                        if (to_near) mx = max(mx, off[v + 1] - off[v]);
+                        append(to_near, v, qout, &st->qlen[s_next], cap, st);
                     }
-                    append(to_near, v, qout, &st->qlen[s_next], cap, st);
                 }
-                if (wi < words && keep != far_bm[wi]) far_bm[wi] = keep;
             }
             mn = __reduce_min_sync(0xffffffffu, mn);
-            cleared = warp_sum(cleared);
-            if (lane_id() == 0) {
+            kept = warp_sum(kept);
+            if (lane == 0) {
                 if (mn != kValueMax) atomicMin(&sx->min_far[s_next], mn);
-                if (cleared) atomicSub(&sx->far_delta[s_next], cleared);
+                if (kept) atomicAdd(&sx->kept[s_next], kept);
             }
         }
+        mx = warp_max(mx);
+        if (mx && lane == 0) atomicMax(&st->max_deg[s_next], mx);
         if (!grid_barrier(st)) break;
         cur ^= 1;  // both kinds of round wrote the other queue
     }
+    if (it == max_rounds)
+        far_now = *(volatile uint32_t*)&sx->split[it % 3] ? *(volatile uint32_t*)&sx->kept[it % 3]
+                                                           : far + *(volatile uint32_t*)&sx->far_delta[it % 3];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         st->levels = it;
         st->cur = cur;
         st->nf = st->qlen[it % 3];
+        sx->far_left = far_now;
+        sx->bucket_lo = bucket_lo;
+        if (far_len_out) *far_len_out = far_now;
     }
 }
 
@@ -392,31 +354,37 @@ void launch_bfs_unbounded(cgb_graph* g, PersistState* st)
 void launch_sssp_device(cgb_graph* g, uint32_t* far_bm, uint32_t delta, PersistState* st, PersistSssp* sx)
 {
     uint32_t cap = g->V, nz = g->nz, words = g->words(), rounds = 0xFFFFFFF0u;
+    uint32_t nf_exit = 0xFFFFFFFFu, deg_exit = 0xFFFFFFFFu, cur = 0;
     uint32_t* nbm = g->aux_bm;
+    uint32_t* far_len_out = nullptr;
     void* args[] = {&g->off, &g->dst, &g->w, &g->value, &nbm, &words, &far_bm, &g->q[0], &g->q[1], &cap, &nz, &delta,
-                    &rounds, &st, &sx};
+                    &rounds, &nf_exit, &deg_exit, &cur, &st, &sx, &far_len_out};
     if (g->w)
         CGB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_sssp_device<true>, num_sms(), kBlock, args, 0, g->stream));
     else
         CGB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_sssp_device<false>, num_sms(), kBlock, args, 0, g->stream));
 }
 
-static PersistState* persist_state(cgb_graph* g)
+static PersistBlock* persist_block(cgb_graph* g)
 {
-    if (!g->persist) g->persist = pool_alloc(sizeof(PersistState), g->stream);
-    return static_cast<PersistState*>(g->persist);
+    if (!g->persist) g->persist = pool_alloc(sizeof(PersistBlock), g->stream);
+    return static_cast<PersistBlock*>(g->persist);
 }
+
+static PersistState* persist_state(cgb_graph* g) { return &persist_block(g)->st; }
 
 // The graph's pinned host block for the state (pinned: a pageable copy waits
 // for other threads' pageable copies, see pinned_acquire).
-static PersistState* host_state(cgb_graph* g)
+static PersistBlock* host_block(cgb_graph* g)
 {
     if (!g->h_persist) {
-        g->h_persist = pinned_acquire(sizeof(PersistState));
-        g->h_persist_bytes = sizeof(PersistState);
+        g->h_persist = pinned_acquire(sizeof(PersistBlock));
+        g->h_persist_bytes = sizeof(PersistBlock);
     }
-    return static_cast<PersistState*>(g->h_persist);
+    return static_cast<PersistBlock*>(g->h_persist);
 }
+
+static PersistState* host_state(cgb_graph* g) { return &host_block(g)->st; }
 
 // Host copy of the state after a launch (synchronises the stream).
 static PersistState read_state(cgb_graph* g)
@@ -523,38 +491,86 @@ PersistResult bfs_persistent(cgb_graph* g, uint32_t cur, uint32_t nf, unsigned l
     return r;
 }
 
-PersistResult sssp_persistent(cgb_graph* g, uint32_t cur, uint32_t nf, uint32_t thr, uint32_t* far_bm,
-                              uint32_t nf_exit, uint32_t max_rounds)
+SsspTail sssp_device_tail(cgb_graph* g, uint32_t cur, uint32_t nf, uint32_t max_deg, uint64_t thr, uint32_t nfar,
+                          uint64_t bucket_lo, uint32_t* far_bm, uint32_t delta, uint32_t nf_exit, uint32_t deg_exit,
+                          uint32_t max_rounds)
 {
-    PersistState* st = persist_state(g);
-    init_state(g, nf, 0, 0);
+    PersistBlock* blk = persist_block(g);
+    PersistState* st = &blk->st;
+    PersistSssp* sx = &blk->sx;
+    // the pinned host block: its previous copy has completed, since every
+    // launch is followed by a synchronising read-back
+    PersistBlock& h = *host_block(g);
+    h = PersistBlock{};
+    h.st.qlen[0] = nf;
+    h.st.max_deg[0] = max_deg;
+    h.sx.thr[0] = thr;
+    for (int k = 0; k < 3; k++) h.sx.min_far[k] = kValueMax;
+    h.sx.far_delta[0] = nfar;
+    h.sx.bucket_lo = bucket_lo;
+    static_assert(sizeof(PersistBlock) % 4 == 0, "copied as words");
+    h2d_small(blk, &h, sizeof(PersistBlock), g->stream);
     const uint32_t words = g->words();
     // round 0 appends against near bitmap slot 1; slot 2 is zeroed by round 0
     CGB_CUDA_TRY(cudaMemsetAsync(g->aux_bm + (size_t)words, 0, (size_t)words * 4, g->stream));
     uint32_t cap = g->V, nz = g->nz;
+    uint32_t* nbm = g->aux_bm;
+    uint32_t* far_len_out = &g->ctr->far_len[0];  // the host loop's far count continues from the tail's
+    void* args[] = {&g->off, &g->dst, &g->w, &g->value, &nbm, (void*)&words, &far_bm, &g->q[0], &g->q[1], &cap, &nz,
+                    &delta, &max_rounds, &nf_exit, &deg_exit, &cur, &st, &sx, &far_len_out};
     ++g->stats.launches;
     if (g->w) {
         static uint32_t full = 0;
-        if (!full) full = cooperative_grid(k_sssp_persistent<true>);
+        if (!full) full = cooperative_grid(k_sssp_device<true>);
         const uint32_t grid = g->tune.persist_ctas ? std::min(g->tune.persist_ctas, full) : full;
-        void* args[] = {&g->off, &g->dst, &g->w, &g->value, &g->aux_bm, (void*)&words, &far_bm, &g->q[0], &g->q[1],
-                        &cap, &nz, &thr, &cur, &nf_exit, &max_rounds, &g->ctr, &st};
-        CGB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_sssp_persistent<true>, grid, kBlock, args, 0, g->stream));
+        CGB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_sssp_device<true>, grid, kBlock, args, 0, g->stream));
     } else {
         static uint32_t full = 0;
-        if (!full) full = cooperative_grid(k_sssp_persistent<false>);
+        if (!full) full = cooperative_grid(k_sssp_device<false>);
         const uint32_t grid = g->tune.persist_ctas ? std::min(g->tune.persist_ctas, full) : full;
-        void* args[] = {&g->off, &g->dst, &g->w, &g->value, &g->aux_bm, (void*)&words, &far_bm, &g->q[0], &g->q[1],
-                        &cap, &nz, &thr, &cur, &nf_exit, &max_rounds, &g->ctr, &st};
-        CGB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_sssp_persistent<false>, grid, kBlock, args, 0, g->stream));
+        CGB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_sssp_device<false>, grid, kBlock, args, 0, g->stream));
     }
-    const PersistState h = read_state(g);
-    PersistResult r;
-    r.levels = h.levels;
-    r.cur = h.cur;
-    r.nf = h.nf;
-    r.added = h.added;
-    return r;
+    CGB_CUDA_TRY(cudaMemcpyAsync(&h.sx, sx, sizeof(PersistSssp), cudaMemcpyDeviceToHost, g->stream));
+    const PersistState hs = read_state(g);  // synchronises
+    SsspTail t;
+    t.r.levels = hs.levels;
+    t.r.cur = hs.cur;
+    t.r.nf = hs.nf;
+    t.r.max_deg = hs.max_deg[hs.levels % 3];
+    t.r.added = hs.added;
+    t.thr = h.sx.thr[hs.levels % 3];
+    t.nfar = h.sx.far_left;
+    t.bucket_lo = h.sx.bucket_lo;
+    return t;
+}
+
+// CTA 0 leaves at once; the others wait at the barrier for a release that
+// never comes and give up after spin_limit polls.
+__global__ void k_barrier_timeout(PersistState* st, uint32_t spin_limit)
+{
+    if (blockIdx.x == 0) return;
+    grid_barrier(st, spin_limit);
+}
+
+cgb_status barrier_timeout_check(uint32_t spin_limit)
+{
+    PersistState* st = nullptr;
+    CGB_CUDA_TRY(cudaMalloc((void**)&st, sizeof(PersistState)));
+    cudaStream_t s = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    PersistState h{};
+    if (e == cudaSuccess) e = cudaMemsetAsync(st, 0, sizeof(PersistState), s);
+    if (e == cudaSuccess) {
+        const uint32_t grid = cooperative_grid(k_barrier_timeout);
+        void* args[] = {&st, &spin_limit};
+        e = cudaLaunchCooperativeKernel((void*)k_barrier_timeout, grid, kBlock, args, 0, s);
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, st, sizeof(PersistState), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (s) cudaStreamDestroy(s);
+    cudaFree(st);
+    CGB_CUDA_TRY(e);
+    return (h.status & 1u) ? CGB_ETIMEOUT : CGB_OK;
 }
 
 }  // namespace cgb

@@ -44,7 +44,20 @@ struct PersistState {
 struct PersistSssp {
     unsigned long long thr[3];  // threshold of the round
     uint32_t min_far[3];        // smallest far distance seen by a split
-    uint32_t far_delta[3];      // change of the far-bitmap population made by a round (mod 2^32)
+    uint32_t far_delta[3];      // change of the far-bitmap population made by an expansion round (mod 2^32)
+    uint32_t kept[3];           // far-bitmap population left by a split round (a recount)
+    uint32_t split[3];          // 1: the round was a split (kept holds the population)
+    // on exit: vertices left in the far bitmap, and the lower bound of the
+    // bucket of the last split (0 if none ran)
+    uint32_t far_left;
+    unsigned long long bucket_lo;
+};
+
+// A graph's device-resident loop state (g->persist): the loop counters,
+// then the whole-device SSSP's bucket state.
+struct PersistBlock {
+    PersistState st;
+    PersistSssp sx;
 };
 
 struct PersistResult {
@@ -69,13 +82,6 @@ PersistResult bfs_persistent(cgb_graph* g, uint32_t cur, uint32_t nf, unsigned l
                              uint32_t level, uint32_t nf_exit, unsigned long long scout_exit, uint32_t deg_exit,
                              uint32_t max_levels);
 
-// Runs SSSP near rounds at threshold thr on the device from q[cur][0, nf)
-// until the near queue empties, exceeds nf_exit, or max_rounds have run.
-// New far-bitmap entries are added to the counters' far_len[0].  For graphs
-// whose lists are all shorter than cgb_tuning.persist_deg.
-PersistResult sssp_persistent(cgb_graph* g, uint32_t cur, uint32_t nf, uint32_t thr, uint32_t* far_bm,
-                              uint32_t nf_exit, uint32_t max_rounds);
-
 // One cooperative launch of k_bfs_persistent with no exit threshold, from
 // the state's qlen[0] roots in q[0] (graph batches).
 void launch_bfs_unbounded(cgb_graph* g, PersistState* st);
@@ -84,9 +90,44 @@ void launch_bfs_unbounded(cgb_graph* g, PersistState* st);
 // and the roots in q[0] (qlen[0]).
 void launch_sssp_device(cgb_graph* g, uint32_t* far_bm, uint32_t delta, PersistState* st, PersistSssp* sx);
 
+// The rest of one SSSP run on the device, from the host loop's state: the
+// near queue q[cur][0, nf) (longest list max_deg) at threshold thr, nfar
+// vertices in far_bm, bucket width delta.  Near rounds and bucket splits
+// alternate in one cooperative launch until the run ends, a round's
+// frontier exceeds nf_exit vertices or holds a list of deg_exit edges or
+// more, or max_rounds rounds have run; the state the host loop continues
+// from is returned (thr: the threshold of the next round; nfar; bucket_lo).
+struct SsspTail {
+    PersistResult r;
+    uint64_t thr = 0, bucket_lo = 0;
+    uint32_t nfar = 0;
+};
+SsspTail sssp_device_tail(cgb_graph* g, uint32_t cur, uint32_t nf, uint32_t max_deg, uint64_t thr, uint32_t nfar,
+                          uint64_t bucket_lo, uint32_t* far_bm, uint32_t delta, uint32_t nf_exit, uint32_t deg_exit,
+                          uint32_t max_rounds);
+
+// Warp-aggregated append into a device-resident loop's queue (every lane
+// calls it); past `cap` the loop's status records an overflow.
+__device__ __forceinline__ void append(bool pred, uint32_t item, uint32_t* q, uint32_t* ctr, uint32_t cap,
+                                       PersistState* st)
+{
+    const uint32_t want = __ballot_sync(0xffffffffu, pred);
+    if (!want) return;
+    const uint32_t leader = __ffs(want) - 1;
+    uint32_t base = 0;
+    if (lane_id() == leader) base = atomicAdd(ctr, (uint32_t)__popc(want));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (pred) {
+        const uint32_t idx = base + __popc(want & lanemask_lt());
+        if (idx < cap) q[idx] = item;
+        else atomicOr(&st->status, 2u);
+    }
+}
+
 // Grid-wide barrier (every CTA of a cooperative launch must call it).
-// Returns false when the wait gave up (status set by the CTA that gave up).
-__device__ __forceinline__ bool grid_barrier(PersistState* st)
+// Returns false when the wait gave up after `spins` polls (status set by the
+// CTA that gave up).
+__device__ __forceinline__ bool grid_barrier(PersistState* st, uint32_t spins_max = kBarrierSpins)
 {
     __shared__ uint32_t s_ok;
     __syncthreads();
@@ -103,7 +144,7 @@ __device__ __forceinline__ bool grid_barrier(PersistState* st)
         } else {
             uint32_t spins = 0;
             while (*gen == g0) {
-                if (++spins > kBarrierSpins) {
+                if (++spins > spins_max) {
                     atomicOr(&st->status, 1u);
                     ok = 0;
                     break;
@@ -117,6 +158,12 @@ __device__ __forceinline__ bool grid_barrier(PersistState* st)
     __syncthreads();
     return s_ok;
 }
+
+// Self-check of the barrier's bounded wait: one cooperative launch (one CTA
+// per SM) in which CTA 0 never arrives, so every other CTA gives up after
+// spin_limit polls and sets the status; returns CGB_ETIMEOUT when they did.
+// No wait in it is unbounded.
+cgb_status barrier_timeout_check(uint32_t spin_limit);
 
 // Cooperative grid of `kernel` with kBlock threads: one CTA per SM (enough
 // threads for the frontiers these loops take, and the fewest arrivals per

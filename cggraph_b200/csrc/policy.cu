@@ -67,11 +67,20 @@ __device__ __forceinline__ void mlp_forward_cta(const float* __restrict__ P, con
 // level just run into the raw quantities, builds the features, runs the
 // network and leaves the outputs in the counters.
 __global__ void __launch_bounds__(kH) k_policy_step(const float* __restrict__ P, FeatIn in, DevCounters* ctr,
-                                                    int patch_bfs, int was_pull, int out_q)
+                                                    int patch, int was_pull, int out_q)
 {
     __shared__ float f[kF], h1[kH], h2[kH];
     if (threadIdx.x == 0) {
-        if (patch_bfs) {
+        if (patch == 2) {
+            // SSSP near round just queued: the next near queue and the far set
+            in.prev_nf = in.nf;
+            in.nf = ctr->qlen[out_q];
+            in.mf = (double)ctr->medges;
+            in.max_deg = ctr->max_deg;
+            in.far_count = ctr->far_len[0];
+            in.iteration += 1;
+        }
+        if (patch == 1) {
             const double n_next = ctr->qlen[out_q];
             in.prev_nf = in.nf;
             in.nf = n_next;
@@ -190,10 +199,10 @@ __global__ void k_adam(float* P, const float* __restrict__ G, float* m, float* v
 }
 
 // ------------------------------------------------------------ host side
-void policy_enqueue(Policy* p, cgb_graph* g, const FeatIn& in, bool patch_bfs, bool was_pull, int out_q)
+void policy_enqueue(Policy* p, cgb_graph* g, const FeatIn& in, int patch, bool was_pull, int out_q)
 {
     ++g->stats.launches;
-    k_policy_step<<<1, kH, 0, g->stream>>>(p->params, in, g->ctr, patch_bfs ? 1 : 0, was_pull ? 1 : 0, out_q);
+    k_policy_step<<<1, kH, 0, g->stream>>>(p->params, in, g->ctr, patch, was_pull ? 1 : 0, out_q);
 }
 
 void policy_log_sample(cgb_graph* g, const FeatIn& in, const float* ms, const bool* have)
@@ -212,12 +221,34 @@ void policy_log_sample(cgb_graph* g, const FeatIn& in, const float* ms, const bo
 // cost); otherwise the heuristic decides.
 constexpr float kMargin = 0.05f;
 
-int policy_pick_direction(const float* out)
+// The cheapest of n choices (outputs out[idx[i]]), or -1 when it does not
+// beat the heuristic's choice `heur` by the margin.
+static int pick_among(const float* out, const int* idx, int n, int heur)
 {
-    const float a = out[kOutPush], b = out[kOutPull];
-    if (!std::isfinite(a) || !std::isfinite(b)) return -1;
-    if (std::fabs(a - b) < kMargin) return -1;
-    return b < a ? 1 : 0;
+    int best = -1;
+    float bv = 0.f;
+    for (int i = 0; i < n; i++) {
+        const float v = out[idx[i]];
+        if (!std::isfinite(v)) return -1;
+        if (best < 0 || v < bv) {
+            best = i;
+            bv = v;
+        }
+    }
+    if (best == heur || out[idx[heur]] - bv < kMargin) return -1;
+    return best;
+}
+
+int policy_pick_bfs_level(const float* out, int heur)
+{
+    const int idx[3] = {kOutPush, kOutPull, kOutPushChunked};
+    return pick_among(out, idx, 3, heur);
+}
+
+int policy_pick_round(const float* out, int heur)
+{
+    const int idx[kNumRoundChoices] = {kOutRound0, kOutRound0 + 1, kOutRound0 + 2, kOutRound0 + 3};
+    return pick_among(out, idx, kNumRoundChoices, heur);
 }
 
 int policy_pick_delta(const float* out)

@@ -1,6 +1,7 @@
 // Per-iteration schedule policy: a small FP32 MLP (24 features -> 64 -> 64
-// -> 9 predicted log-costs) trained on the engine's own counterfactual
-// traces, with the Beamer / fixed-delta heuristic as fallback.
+// -> 14 predicted log-costs) trained on the engine's own counterfactual
+// traces, with the Beamer / fixed-delta / size-threshold heuristics as
+// fallback.
 #pragma once
 
 #include "engine.cuh"
@@ -9,16 +10,22 @@ namespace cgb {
 
 constexpr int kPolicyFeatures = CGB_POLICY_FEATURES;  // 24
 constexpr int kPolicyHidden = 64;
-constexpr int kPolicyOutputs = CGB_POLICY_OUTPUTS;    // 9
-// parameter layout: W1[24][64] b1[64] W2[64][64] b2[64] W3[64][9] b3[9]
+constexpr int kPolicyOutputs = CGB_POLICY_OUTPUTS;    // 14
+// parameter layout: W1[24][64] b1[64] W2[64][64] b2[64] W3[64][14] b3[14]
 constexpr int kPolicyParams = CGB_POLICY_PARAMS;
 static_assert(kPolicyParams == kPolicyFeatures * kPolicyHidden + kPolicyHidden + kPolicyHidden * kPolicyHidden +
                                    kPolicyHidden + kPolicyHidden * kPolicyOutputs + kPolicyOutputs,
               "parameter count");
 
 // Output heads: predicted log-cost of each choice (lower is better).
-constexpr int kOutPush = 0, kOutPull = 1;  // BFS direction of the next level
+constexpr int kOutPush = 0, kOutPull = 1;  // BFS next level: binned push / bottom-up pull
+constexpr int kOutPushChunked = 9;         // BFS next level: push, every list >= 32 edges chunked
 constexpr int kOutDelta0 = 2;              // SSSP delta x delta_scale(i) for the next bucket
+// SSSP next near round: sparse frontier (binned push), sparse frontier with
+// chunked lists, dense frontier, pull
+constexpr int kOutRound0 = 10;
+constexpr int kNumRoundChoices = 4;
+enum RoundVariant { kRoundPush = 0, kRoundPushChunked = 1, kRoundDense = 2, kRoundPull = 3 };
 constexpr int kNumDeltaChoices = 7;        // x {1/4, 1/2, 1, 2, 4, 8, 16}
 constexpr int kDeltaUnit = 2;              // index of x1 (the heuristic delta)
 __host__ __device__ inline float delta_scale(int i) { return 0.25f * (float)(1 << i); }
@@ -77,18 +84,22 @@ Policy* policy_get();
 const float* policy_params_device(Policy* p);
 
 // Queues the network on the graph's stream: features from `in` (with the
-// counters of the level just run patched in when `patch_bfs` is set: next
-// frontier size, its out-edges and max degree, vertices found), outputs
-// into the DevCounters' policy_out, read back by the next sync_counters.
-void policy_enqueue(Policy* p, cgb_graph* g, const FeatIn& in, bool patch_bfs, bool was_pull, int out_q);
+// counters of the level or round just run patched in when `patch` is 1 for
+// BFS -- next frontier size, its out-edges and max degree, vertices found --
+// or 2 for an SSSP near round -- next near queue, its out-edges and max
+// degree, far count), outputs into the DevCounters' policy_out, read back by
+// the next sync_counters.
+void policy_enqueue(Policy* p, cgb_graph* g, const FeatIn& in, int patch, bool was_pull, int out_q);
 
 // Appends one counterfactual sample (features of `in`, measured ms of the
 // choices flagged in `have`) to g->collect.
 void policy_log_sample(cgb_graph* g, const FeatIn& in, const float* ms, const bool* have);
 
 // Decisions from the outputs read back with the counters; -1 = no
-// confident choice (use the heuristic).
-int policy_pick_direction(const float* out);
+// confident choice (use the heuristic).  `heur` is the heuristic's own
+// choice, which another choice must beat by the margin.
+int policy_pick_bfs_level(const float* out, int heur);  // 0 push, 1 pull, 2 push chunked
 int policy_pick_delta(const float* out);
+int policy_pick_round(const float* out, int heur);  // a RoundVariant
 
 }  // namespace cgb

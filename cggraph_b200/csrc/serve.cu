@@ -34,6 +34,7 @@
 #include "engine.cuh"
 #include "msbfs.cuh"
 #include "mssp.cuh"
+#include "persist.cuh"
 #include "push.cuh"
 
 namespace cgb {
@@ -174,6 +175,343 @@ __global__ void k_srv_sp_extract_cols(const uint32_t* __restrict__ dist, uint32_
 
 __global__ void k_srv_copy_u32(const uint32_t* src, uint32_t* dst) { *dst = *src; }
 
+// ------------------------------------------------ device-resident BFS levels
+//
+// The BFS group's levels run on the device, many per launch: one
+// cooperative kernel (one CTA per SM) separates the phases of a level with
+// the bounded grid barrier of persist.cuh and keeps going until
+//   - a slot's traversal ended (its result can be copied out: the host
+//     retires it),
+//   - the host raised the pinned mailbox (a query waits for a free slot:
+//     the host admits it), checked after every level,
+//   - the time budget ran out, or
+//   - the frontier outgrew the loop (more than nf_exit vertices, or enough
+//     out-edges that a bottom-up level is cheaper: the host loop's kernels
+//     take those levels).
+// A level is the top-down multi-root step of msbfs.cu: every frontier
+// vertex v offers its roots front[v] & ~seen[u] to each out-neighbour u
+// (atomicOr into next[u]; the first setter lists u), lists of kLoopHub
+// edges or more are cut into kLoopChunk-edge chunks that every warp takes
+// part in, then the listed vertices keep their new roots, write their
+// levels (level - start[slot]) and form the next frontier.
+
+constexpr uint32_t kLoopHub = 2048;    // lists at least this long are chunked across the grid
+constexpr uint32_t kLoopChunk = 1024;
+
+struct SrvBfsLoopState {
+    PersistState ps;               // barrier, rotating qlen / medges
+    uint32_t touched_len[3];       // vertices listed in next[] this level
+    uint32_t chunk_len[3];         // hub chunks this level
+    unsigned long long alive[3];   // slots given next-frontier vertices
+    uint32_t stop[3];              // block 0's decision to leave before the level
+    // on exit
+    uint32_t ticks, cur, nf, reason;
+    unsigned long long alive_out, finished, medges_out;
+};
+
+struct SrvBfsLoopArgs {
+    const uint32_t* off;
+    const uint32_t* dst;
+    unsigned long long* seen;
+    unsigned long long* front[2];
+    unsigned long long* next;
+    uint32_t* q[2];
+    uint32_t* touched;
+    uint32_t* region;
+    const uint32_t* start;
+    uint2* chunk_q;
+    uint32_t chunk_cap;
+    uint32_t V, nz, cap;
+    uint64_t E;
+    uint32_t cur, tick0;
+    unsigned long long active;
+    uint32_t nf_exit, max_ticks;
+    unsigned long long budget_ns;
+    const uint32_t* mailbox;  // pinned host word: non-zero asks the loop to return
+    SrvBfsLoopState* st;
+};
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// One edge v -> u of a top-down level (warp-collective).
+__device__ __forceinline__ void srv_td_edge(const SrvBfsLoopArgs& a, const unsigned long long* fcur, bool valid,
+                                            uint32_t e, uint32_t v, uint32_t* tlen)
+{
+    bool first = false;
+    uint32_t u = 0;
+    if (valid) {
+        u = a.dst[e];
+        const unsigned long long add = fcur[v] & ~a.seen[u];
+        if (add && (a.next[u] & add) != add) first = atomicOr(a.next + u, add) == 0ull;
+    }
+    append(first, u, a.touched, tlen, a.V, &a.st->ps);
+}
+
+__global__ void __launch_bounds__(kBlock) k_srv_bfs_loop(SrvBfsLoopArgs a)
+{
+    SrvBfsLoopState* st = a.st;
+    PersistState* ps = &st->ps;
+    const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x, gthreads = gridDim.x * blockDim.x;
+    const uint32_t lane = lane_id(), gw = gtid / 32, nwarps = gthreads / 32;
+    const unsigned long long t0 = global_ns();
+    uint32_t cur = a.cur, it = 0;
+    for (; it < a.max_ticks; it++) {
+        const uint32_t s_cur = it % 3, s_next = (it + 1) % 3, s_zero = (it + 2) % 3;
+        const uint32_t nf = *(volatile uint32_t*)&ps->qlen[s_cur];
+        const unsigned long long mf = *(volatile unsigned long long*)&ps->medges[s_cur];
+        if (*(volatile uint32_t*)&st->stop[s_cur] || nf == 0 || nf > a.nf_exit || (double)mf * 15.0 > (double)a.E)
+            break;
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            ps->qlen[s_zero] = 0;
+            ps->medges[s_zero] = 0;
+            st->touched_len[s_zero] = 0;
+            st->chunk_len[s_zero] = 0;
+            st->alive[s_zero] = 0;
+            st->stop[s_zero] = 0;
+        }
+        const uint32_t* qin = a.q[cur];
+        uint32_t* qout = a.q[cur ^ 1];
+        const unsigned long long* fcur = a.front[cur];
+        unsigned long long* fnxt = a.front[cur ^ 1];
+        uint32_t* tlen = &st->touched_len[s_cur];
+        // expansion: short lists lane by lane, medium lists by one warp, hub lists as chunks
+        for (uint32_t base = gw * 32; base < nf; base += nwarps * 32) {
+            const uint32_t i = base + lane;
+            uint32_t v = 0, s0 = 0, d = 0;
+            if (i < nf) {
+                v = qin[i];
+                s0 = a.off[v];
+                d = a.off[v + 1] - s0;
+            }
+            uint32_t hub = __ballot_sync(0xffffffffu, d >= kLoopHub);
+            while (hub) {
+                const uint32_t l = __ffs(hub) - 1;
+                hub &= hub - 1;
+                const uint32_t hv = __shfl_sync(0xffffffffu, v, l), hd = __shfl_sync(0xffffffffu, d, l);
+                const uint32_t nch = (hd + kLoopChunk - 1) / kLoopChunk;
+                uint32_t slot = 0;
+                if (lane == 0) slot = atomicAdd(&st->chunk_len[s_cur], nch);
+                slot = __shfl_sync(0xffffffffu, slot, 0);
+                for (uint32_t c = lane; c < nch; c += 32) {
+                    if (slot + c < a.chunk_cap) a.chunk_q[slot + c] = make_uint2(hv, c);
+                    else atomicOr(&ps->status, 2u);
+                }
+                if (lane == l) d = 0;
+            }
+            uint32_t wm;
+            while ((wm = __ballot_sync(0xffffffffu, d >= 32)) != 0) {
+                const uint32_t l = __ffs(wm) - 1;
+                const uint32_t wv = __shfl_sync(0xffffffffu, v, l), ws = __shfl_sync(0xffffffffu, s0, l);
+                const uint32_t wd = __shfl_sync(0xffffffffu, d, l);
+                if (lane == l) d = 0;
+                for (uint32_t k = 0; k < wd; k += 32) srv_td_edge(a, fcur, k + lane < wd, ws + k + lane, wv, tlen);
+            }
+            for (uint32_t j = 0; __any_sync(0xffffffffu, j < d); j++) srv_td_edge(a, fcur, j < d, s0 + j, v, tlen);
+        }
+        if (!grid_barrier(ps)) break;
+        const uint32_t nch = min(*(volatile uint32_t*)&st->chunk_len[s_cur], a.chunk_cap);
+        for (uint32_t c = gw; c < nch; c += nwarps) {
+            const uint2 dsc = a.chunk_q[c];
+            const uint32_t s0 = a.off[dsc.x], e1 = a.off[dsc.x + 1];
+            const uint32_t cs = s0 + dsc.y * kLoopChunk, ce = min(e1, cs + kLoopChunk);
+            for (uint32_t k = cs; k < ce; k += 32) srv_td_edge(a, fcur, k + lane < ce, k + lane, dsc.x, tlen);
+        }
+        if (!grid_barrier(ps)) break;
+        // the listed vertices keep their new roots and form the next frontier
+        const uint32_t nt = *(volatile uint32_t*)tlen;
+        const uint32_t lvl = a.tick0 + it + 1;
+        unsigned long long live = 0, medges = 0;
+        for (uint32_t b = gw * 32; b < nt; b += nwarps * 32) {
+            const uint32_t i = b + lane;
+            bool act = false;
+            uint32_t u = 0;
+            if (i < nt) {
+                u = a.touched[i];
+                const unsigned long long x = a.next[u] & ~a.seen[u];
+                a.next[u] = 0;
+                if (x) {
+                    a.seen[u] |= x;
+                    for (unsigned long long m = x; m; m &= m - 1) {
+                        const uint32_t k = __ffsll(m) - 1;
+                        a.region[(size_t)k * a.V + u] = lvl - a.start[k];
+                    }
+                    act = u < a.nz;
+                    if (act) {
+                        fnxt[u] = x;
+                        live |= x;
+                        medges += a.off[u + 1] - a.off[u];
+                    }
+                }
+            }
+            append(act, u, qout, &ps->qlen[s_next], a.cap, ps);
+        }
+        for (uint32_t i = gtid; i < nf; i += gthreads) a.front[cur][qin[i]] = 0;
+        live = warp_or(live);
+        medges = warp_sum(medges);
+        if (lane == 0) {
+            if (live) atomicOr(&st->alive[s_next], live);
+            if (medges) atomicAdd(&ps->medges[s_next], medges);
+        }
+        if (!grid_barrier(ps)) break;
+        // block 0 decides whether the next level runs here
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            const unsigned long long alive = *(volatile unsigned long long*)&st->alive[s_next];
+            const bool fin = (a.active & ~alive) != 0ull;
+            const bool mail = *(volatile const uint32_t*)a.mailbox != 0u;
+            const bool late = global_ns() - t0 > a.budget_ns;
+            st->stop[s_next] = (fin || mail || late) ? 1u : 0u;
+            st->reason = fin ? 1u : mail ? 2u : late ? 3u : 0u;
+        }
+        if (!grid_barrier(ps)) break;
+        cur ^= 1;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st->ticks = it;
+        st->cur = cur;
+        st->nf = ps->qlen[it % 3];
+        st->medges_out = ps->medges[it % 3];
+        const unsigned long long alive = it > 0 ? st->alive[it % 3] : a.active;
+        st->alive_out = alive;
+        st->finished = it > 0 ? (a.active & ~alive) : 0ull;
+    }
+}
+
+// ----------------------------------------------- device-resident SSSP rounds
+//
+// The SSSP group's rounds on the device, many per launch: one cooperative
+// kernel runs the tick of the host loop (sp_issue) as grid phases separated
+// by the bounded grid barrier -- plan (per-slot bucket advances, by the
+// slots' near / far liveness of the previous round), split of the far list
+// for the advancing slots, descriptors, expansion -- using the bodies of the
+// multi-root kernels of mssp.cu, until a slot's query ended, the host
+// raised the pinned mailbox (a query waits for a free slot), or the time
+// budget ran out.  Per-slot thresholds, smallest far distances and
+// liveness live in the loop state between launches; the host loads them
+// before a launch and reads them back after it.
+
+struct SrvSpLoopState {
+    PersistState ps;                   // barrier and status
+    unsigned long long thr[kSrvSlots]; // per-slot threshold
+    uint32_t thr32[kSrvSlots];         // the same, clamped (expansion)
+    uint32_t lo[kSrvSlots], hi[kSrvSlots];  // bucket being split in (split)
+    uint32_t min_far[kSrvSlots];       // smallest far distance the slot's last split kept
+    uint32_t min_far_new[kSrvSlots];   // ... reported by this round's split
+    uint32_t last_empty[kSrvSlots];    // the slot's last split found no near pair
+    unsigned long long near_alive, far_alive, adv, active;
+    unsigned long long alive_round[2]; // this round: [0] near work, [1] far work
+    uint32_t cur, fcur, stop, reason;
+    uint32_t ticks;
+    unsigned long long finished;
+};
+
+struct SrvSpLoopArgs {
+    const uint32_t* off;
+    const uint32_t* dst;
+    const uint32_t* w;
+    uint32_t* dist;
+    unsigned long long* pend;
+    unsigned long long* farm;
+    unsigned long long* maskq;
+    uint32_t* far_list[2];
+    uint4* desc;
+    uint64_t desc_cap;
+    MsspCounters* c;
+    uint32_t* q[2];
+    uint32_t V, ms_edges, delta, max_ticks;
+    unsigned long long budget_ns;
+    const uint32_t* mailbox;
+    SrvSpLoopState* st;
+};
+
+template <bool kHasW>
+__global__ void __launch_bounds__(kBlock) k_srv_sssp_loop(SrvSpLoopArgs a)
+{
+    SrvSpLoopState* st = a.st;
+    PersistState* ps = &st->ps;
+    MsspCounters* c = a.c;
+    const unsigned long long t0 = global_ns();
+    uint32_t it = 0;
+    for (; it < a.max_ticks; it++) {
+        // plan (block 0): slots whose near work ran out but which keep far pairs advance a bucket
+        if (blockIdx.x == 0 && threadIdx.x < kSrvSlots) {
+            const uint32_t k = threadIdx.x;
+            const unsigned long long adv = st->active & ~st->near_alive & st->far_alive;
+            if ((adv >> k) & 1ull) {
+                const uint64_t t = st->thr[k];
+                uint64_t hi = t + a.delta;
+                if (st->last_empty[k] && st->min_far[k] != kValueMax)
+                    hi = std::max<uint64_t>(hi, ((uint64_t)st->min_far[k] / a.delta + 1) * (uint64_t)a.delta);
+                st->lo[k] = t < 0xFFFFFFFFull ? (uint32_t)t : 0xFFFFFFFFu;
+                st->hi[k] = hi < 0xFFFFFFFFull ? (uint32_t)hi : 0xFFFFFFFFu;
+                st->thr[k] = hi;
+                st->min_far_new[k] = kValueMax;
+            }
+            st->thr32[k] = st->thr[k] < 0xFFFFFFFFull ? (uint32_t)st->thr[k] : 0xFFFFFFFFu;
+            if (k == 0) {
+                st->adv = adv;
+                c->nfar_next = 0;
+                c->nq_out = 0;
+                c->ndesc = 0;
+                st->alive_round[0] = 0;
+                if (adv) st->alive_round[1] = 0;  // recomputed by the split
+            }
+        }
+        if (!grid_barrier(ps)) break;
+        const unsigned long long adv = *(volatile unsigned long long*)&st->adv;
+        const uint32_t cur = *(volatile uint32_t*)&st->cur;
+        uint32_t fcur = *(volatile uint32_t*)&st->fcur;
+        if (adv) {
+            mssp_split_body(a.far_list[fcur], &c->nfar_live, a.dist, a.pend, a.farm, a.q[cur], &c->nq_in,
+                            a.far_list[fcur ^ 1], &c->nfar_next, a.V, 0, 0, st->lo, st->hi, adv, st->min_far_new,
+                            &st->alive_round[1], c);
+            if (!grid_barrier(ps)) break;
+            if (blockIdx.x == 0 && threadIdx.x == 0) {
+                c->nfar_live = c->nfar_next;
+                st->fcur = fcur ^ 1;
+            }
+            fcur ^= 1;
+        }
+        mssp_desc_body(a.q[cur], &c->nq_in, a.off, a.pend, a.maskq, a.desc, a.desc_cap, c, a.ms_edges);
+        if (!grid_barrier(ps)) break;
+        mssp_expand_body<kHasW>(a.desc, c, a.maskq, a.dst, a.w, a.dist, a.pend, a.farm, a.q[cur ^ 1], &c->nq_out,
+                                a.far_list[fcur], &c->nfar_live, a.V, 0, st->thr32, st->alive_round, c);
+        if (!grid_barrier(ps)) break;
+        // round's end (block 0): liveness, the split slots' far minima, the decision to go on
+        if (blockIdx.x == 0 && threadIdx.x < kSrvSlots) {
+            const uint32_t k = threadIdx.x;
+            const unsigned long long near = st->alive_round[0], far = st->alive_round[1];
+            if ((st->adv >> k) & 1ull) {
+                st->min_far[k] = st->min_far_new[k];
+                st->last_empty[k] = ((near >> k) & 1ull) ? 0u : 1u;
+            }
+            __syncwarp(0xffffffffu);
+            if (k == 0) {
+                c->nq_in = c->nq_out;
+                st->cur = cur ^ 1;
+                st->near_alive = near;
+                st->far_alive = far;
+                const unsigned long long fin = st->active & ~(near | far);
+                const bool mail = *(volatile const uint32_t*)a.mailbox != 0u;
+                const bool late = global_ns() - t0 > a.budget_ns;
+                st->finished = fin;
+                st->stop = (fin || mail || late || c->overflow) ? 1u : 0u;
+                st->reason = fin ? 1u : mail ? 2u : late ? 3u : 0u;
+            }
+        }
+        if (!grid_barrier(ps)) break;
+        if (*(volatile uint32_t*)&st->stop) {
+            it++;
+            break;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->ticks = it;
+}
+
 // ------------------------------------------------------------------ state
 
 using Clock = std::chrono::steady_clock;
@@ -224,12 +562,19 @@ struct Group {
     uint32_t* out[kSrvSlots];  // where the slot's result goes (host / device / NULL)
     std::vector<uint32_t> admit;  // slots admitted this tick (root / out filled under the server lock)
     // BFS
+    SrvBfsLoopState* loop = nullptr;    // device-resident levels (null: host ticks only)
+    SrvBfsLoopState* h_loop = nullptr;  // pinned mirror
+    uint32_t* mailbox = nullptr;        // pinned word the loop polls: non-zero = return to the host
+    cudaEvent_t ev_loop = nullptr;
+    uint64_t loop_levels = 0, loop_launches = 0;
     MsBuffers* mb = nullptr;
     uint32_t* q[2] = {nullptr, nullptr};
     uint32_t* touched = nullptr;
     uint32_t nact = 0, cur = 0, tick = 0;
     unsigned long long medges = 0;
     // SSSP
+    SrvSpLoopState* sp_loop = nullptr;    // device-resident rounds (null: host ticks only)
+    SrvSpLoopState* h_sp_loop = nullptr;  // pinned mirror
     MsspBuffers* sp = nullptr;
     uint32_t delta = 1, fcur = 0;
     unsigned long long near_alive = 0, far_alive = 0, split_mask = 0;
@@ -244,6 +589,11 @@ using namespace cgb;
 
 struct cgb_server {
     cgb_graph* g = nullptr;
+    uint32_t flags = 0;  // cgb_server_config.flags
+    // The groups' device-resident loops are cooperative launches whose CTAs wait
+    // for each other at grid barriers; two of them resident at once could each
+    // hold SMs the other waits for, so one runs at a time.
+    std::mutex coop_mu;
     Group grp[2];  // [0] BFS, [1] SSSP
     std::vector<SrvReq> reqs;
     std::deque<int64_t> waiting[2];    // submitted, not admitted (arrival order of submission)
@@ -291,6 +641,13 @@ static void group_alloc(cgb_server* s, Group& G, int alg, uint32_t nslots)
     if (alg == CGB_BFS) {
         G.stream = g->stream;  // the binned push expansion runs on the graph's stream
         G.mb = ms_buffers_alloc(V, g->E);
+        if (!(s->flags & CGB_SERVER_HOST_TICKS)) {
+            CGB_CUDA_TRY(cudaMalloc((void**)&G.loop, sizeof(SrvBfsLoopState)));
+            CGB_CUDA_TRY(cudaMallocHost((void**)&G.h_loop, sizeof(SrvBfsLoopState)));
+            CGB_CUDA_TRY(cudaMallocHost((void**)&G.mailbox, sizeof(uint32_t)));
+            *G.mailbox = 0;
+            CGB_CUDA_TRY(cudaEventCreateWithFlags(&G.ev_loop, cudaEventDisableTiming));
+        }
         CGB_CUDA_TRY(cudaMemset(G.mb->seen, 0, (size_t)V * 8));
         CGB_CUDA_TRY(cudaMemset(G.mb->front[0], 0, (size_t)V * 8));
         CGB_CUDA_TRY(cudaMemset(G.mb->front[1], 0, (size_t)V * 8));
@@ -301,6 +658,13 @@ static void group_alloc(cgb_server* s, Group& G, int alg, uint32_t nslots)
     } else {
         CGB_CUDA_TRY(cudaStreamCreateWithFlags(&G.stream, cudaStreamNonBlocking));
         G.sp = mssp_buffers_alloc(V, g->E);
+        if (!(s->flags & CGB_SERVER_HOST_TICKS)) {
+            CGB_CUDA_TRY(cudaMalloc((void**)&G.sp_loop, sizeof(SrvSpLoopState)));
+            CGB_CUDA_TRY(cudaMallocHost((void**)&G.h_sp_loop, sizeof(SrvSpLoopState)));
+            CGB_CUDA_TRY(cudaMallocHost((void**)&G.mailbox, sizeof(uint32_t)));
+            *G.mailbox = 0;
+            CGB_CUDA_TRY(cudaEventCreateWithFlags(&G.ev_loop, cudaEventDisableTiming));
+        }
         CGB_CUDA_TRY(cudaMalloc((void**)&G.q[0], (size_t)V * 4));
         CGB_CUDA_TRY(cudaMalloc((void**)&G.q[1], (size_t)V * 4));
         CGB_CUDA_TRY(cudaMemset(G.sp->c, 0, sizeof(MsspCounters)));
@@ -319,6 +683,12 @@ static void group_free(cgb_server* s, Group& G)
     cudaFree(G.d_up);
     if (G.h_up) cudaFreeHost(G.h_up);
     ms_buffers_free(G.mb);
+    cudaFree(G.loop);
+    if (G.h_loop) cudaFreeHost(G.h_loop);
+    cudaFree(G.sp_loop);
+    if (G.h_sp_loop) cudaFreeHost(G.h_sp_loop);
+    if (G.mailbox) cudaFreeHost(G.mailbox);
+    if (G.ev_loop) cudaEventDestroy(G.ev_loop);
     cudaFree(G.q[0]);
     cudaFree(G.q[1]);
     cudaFree(G.touched);
@@ -327,13 +697,13 @@ static void group_free(cgb_server* s, Group& G)
     G = Group();
 }
 
-// ---- BFS group: issue one level for every active slot (no host sync)
-static void bfs_issue(cgb_server* s, Group& G)
+// ---- BFS group: this tick's admissions (no host sync)
+static void bfs_admit(cgb_server* s, Group& G)
 {
     cgb_graph* g = s->g;
     const uint32_t V = g->V;
     cudaStream_t st = G.stream;
-    const uint32_t cur = G.cur, nxt = cur ^ 1;
+    const uint32_t cur = G.cur;
     if (!G.admit.empty()) {
         unsigned long long reuse = 0;
         uint32_t n = 0, qpos = G.nact;
@@ -356,7 +726,18 @@ static void bfs_issue(cgb_server* s, Group& G)
         CGB_CUDA_TRY(cudaMemcpyAsync(G.d_up, G.h_up, sizeof(SlotUpload), cudaMemcpyHostToDevice, st));
         k_srv_bfs_admit<<<1, kSrvSlots, 0, st>>>(n, G.d_up->slots, G.d_up->roots, G.d_up->qidx, V, G.region,
                                                  G.mb->seen, G.mb->front[cur], G.q[cur]);
+        G.admit.clear();
     }
+}
+
+// ---- BFS group: issue one level for every active slot (no host sync)
+static void bfs_issue(cgb_server* s, Group& G)
+{
+    cgb_graph* g = s->g;
+    const uint32_t V = g->V;
+    cudaStream_t st = G.stream;
+    const uint32_t cur = G.cur, nxt = cur ^ 1;
+    bfs_admit(s, G);
     CGB_CUDA_TRY(cudaMemsetAsync(&G.d_stats->alive[0], 0, 8, st));
     CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->qlen[nxt], 0, 4, st));
     CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->medges, 0, 8, st));
@@ -384,21 +765,20 @@ static void bfs_issue(cgb_server* s, Group& G)
 }
 
 // ---- SSSP group: admissions, per-slot bucket splits, one near round
-static void sp_issue(cgb_server* s, Group& G)
+// ---- SSSP group: this tick's admissions (no host sync)
+static void sp_admit(cgb_server* s, Group& G)
 {
     cgb_graph* g = s->g;
     const uint32_t V = g->V;
     cudaStream_t st = G.stream;
     MsspBuffers& b = *G.sp;
-    const uint32_t cur = G.cur, nxt = cur ^ 1;
-    unsigned long long admitted = 0;
+    const uint32_t cur = G.cur;
     if (!G.admit.empty()) {
         unsigned long long reuse = 0;
         uint32_t n = 0;
         for (const uint32_t k : G.admit) {
             if (G.used[k]) reuse |= 1ull << k;
             G.used[k] = true;
-            admitted |= 1ull << k;
             G.h_up->slots[n] = k;
             G.h_up->roots[n] = G.root[k];
             G.thr[k] = G.delta;
@@ -411,9 +791,22 @@ static void sp_issue(cgb_server* s, Group& G)
         CGB_CUDA_TRY(cudaMemcpyAsync(G.d_up, G.h_up, sizeof(SlotUpload), cudaMemcpyHostToDevice, st));
         k_srv_sp_admit<<<1, kSrvSlots, 0, st>>>(n, G.d_up->slots, G.d_up->roots, b.dist, b.pend, G.q[cur],
                                                 &b.c->nq_in, V, b.c);
+        G.admit.clear();
     }
-    // slots whose near work ran out but which still have far pairs move to their next bucket
-    const unsigned long long adv = G.active & ~admitted & ~G.near_alive & G.far_alive;
+}
+
+// ---- SSSP group: per-slot bucket splits and one near round (no host sync)
+static void sp_issue(cgb_server* s, Group& G)
+{
+    cgb_graph* g = s->g;
+    const uint32_t V = g->V;
+    cudaStream_t st = G.stream;
+    MsspBuffers& b = *G.sp;
+    const uint32_t cur = G.cur, nxt = cur ^ 1;
+    sp_admit(s, G);
+    // slots whose near work ran out but which still have far pairs move to their
+    // next bucket (a slot admitted this tick, or free, has neither bit)
+    const unsigned long long adv = G.active & ~G.near_alive & G.far_alive;
     G.split_mask = adv;
     if (adv) {
         for (uint32_t k = 0; k < kSrvSlots; k++) {
@@ -452,6 +845,179 @@ static void sp_issue(cgb_server* s, Group& G)
     CGB_CUDA_TRY(cudaMemcpyAsync(G.h_stats->min_far, G.d_stats->min_far, sizeof(G.h_stats->min_far),
                                  cudaMemcpyDeviceToHost, st));
     CGB_CUDA_TRY(cudaMemcpyAsync(b.h, b.c, sizeof(MsspCounters), cudaMemcpyDeviceToHost, st));
+}
+
+// A query waits whose arrival time has passed, and a slot is free for it.
+static bool admission_due(cgb_server* s, const Group& G, int a)
+{
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->waiting[a].empty()) return false;
+    if (s->reqs[s->waiting[a].front()].info.arrival_us > us_since(s, Clock::now())) return false;
+    for (uint32_t k = 0; k < G.nslots; k++)
+        if (G.state[k] == SlotState::kFree) return true;
+    return false;
+}
+
+// Levels of the BFS group on the device (k_srv_bfs_loop) from its current
+// frontier; returns the slots whose traversal ended.  While the loop runs,
+// this thread raises the pinned mailbox as soon as a waiting query could be
+// admitted, and the loop returns after the level in progress.
+constexpr unsigned long long kLoopBudgetNs = 4000000;  // a launch returns after 4 ms at most
+static unsigned long long bfs_device_levels(cgb_server* s, Group& G, uint32_t nf_exit)
+{
+    cgb_graph* g = s->g;
+    SrvBfsLoopState& h = *G.h_loop;
+    h = SrvBfsLoopState{};
+    h.ps.qlen[0] = G.nact;
+    h.ps.medges[0] = G.medges;
+    static_assert(sizeof(SrvBfsLoopState) % 4 == 0, "copied as words");
+    h2d_small(G.loop, &h, sizeof(SrvBfsLoopState), G.stream);
+    *reinterpret_cast<volatile uint32_t*>(G.mailbox) = 0;
+    SrvBfsLoopArgs args{};
+    args.off = g->off;
+    args.dst = g->dst;
+    args.seen = G.mb->seen;
+    args.front[0] = G.mb->front[0];
+    args.front[1] = G.mb->front[1];
+    args.next = G.mb->next;
+    args.q[0] = G.q[0];
+    args.q[1] = G.q[1];
+    args.touched = G.touched;
+    args.region = G.region;
+    args.start = G.d_up->start;
+    args.chunk_q = g->chunk_q;
+    args.chunk_cap = g->chunk_cap;
+    args.V = g->V;
+    args.nz = g->nz;
+    args.cap = g->V;
+    args.E = g->E;
+    args.cur = G.cur;
+    args.tick0 = G.tick;
+    args.active = G.active;
+    args.nf_exit = nf_exit;
+    args.max_ticks = g->V + 2;
+    args.budget_ns = kLoopBudgetNs;
+    args.mailbox = G.mailbox;
+    args.st = G.loop;
+    static uint32_t grid = 0;
+    if (!grid) grid = cooperative_grid(k_srv_bfs_loop);
+    void* kargs[] = {&args};
+    std::lock_guard<std::mutex> coop(s->coop_mu);
+    CGB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_srv_bfs_loop, grid, kBlock, kargs, 0, G.stream));
+    CGB_CUDA_TRY(cudaMemcpyAsync(&h, G.loop, sizeof(SrvBfsLoopState), cudaMemcpyDeviceToHost, G.stream));
+    CGB_CUDA_TRY(cudaEventRecord(G.ev_loop, G.stream));
+    for (;;) {
+        const cudaError_t e = cudaEventQuery(G.ev_loop);
+        if (e == cudaSuccess) break;
+        if (e != cudaErrorNotReady) CGB_CUDA_TRY(e);
+        if (admission_due(s, G, 0)) *reinterpret_cast<volatile uint32_t*>(G.mailbox) = 1;
+        std::this_thread::sleep_for(std::chrono::microseconds(20));
+    }
+    CGB_REQUIRE(!(h.ps.status & 2u), CGB_EOVERFLOW, "server BFS loop: queue overflow");
+    CGB_REQUIRE(!(h.ps.status & 1u), CGB_ETIMEOUT, "server BFS loop: grid barrier gave up");
+    G.cur = h.cur;
+    G.nact = h.nf;
+    G.tick += h.ticks;
+    G.live = h.alive_out;
+    G.medges = h.medges_out;
+    G.loop_levels += h.ticks;
+    G.loop_launches++;
+    return h.finished;
+}
+
+// Cooperative grid of `kernel` with up to `per_sm` kBlock-thread CTAs per SM
+// (as many as are resident at once).
+template <typename K>
+static uint32_t cooperative_grid_n(K kernel, int per_sm)
+{
+    int dev = 0, occ = 0;
+    CGB_CUDA_TRY(cudaGetDevice(&dev));
+    CGB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, kBlock, 0));
+    CGB_REQUIRE(occ >= 1, CGB_EUNSUPPORTED, "device-resident loop does not fit on an SM");
+    return (uint32_t)num_sms() * (uint32_t)std::min(occ, per_sm);
+}
+
+// Rounds of the SSSP group on the device (k_srv_sssp_loop) from its current
+// state; returns the slots whose query ended.  The host raises the pinned
+// mailbox as for the BFS loop.
+static unsigned long long sp_device_ticks(cgb_server* s, Group& G)
+{
+    cgb_graph* g = s->g;
+    MsspBuffers& b = *G.sp;
+    SrvSpLoopState& h = *G.h_sp_loop;
+    h = SrvSpLoopState{};
+    for (uint32_t k = 0; k < kSrvSlots; k++) {
+        h.thr[k] = G.thr[k];
+        h.min_far[k] = G.min_far[k];
+        h.last_empty[k] = G.last_empty[k] ? 1u : 0u;
+    }
+    h.near_alive = G.near_alive;
+    h.far_alive = G.far_alive;
+    h.alive_round[1] = G.far_alive;
+    h.active = G.active;
+    h.cur = G.cur;
+    h.fcur = G.fcur;
+    static_assert(sizeof(SrvSpLoopState) % 4 == 0, "copied as words");
+    h2d_small(G.sp_loop, &h, sizeof(SrvSpLoopState), G.stream);
+    *reinterpret_cast<volatile uint32_t*>(G.mailbox) = 0;
+    SrvSpLoopArgs args{};
+    args.off = g->off;
+    args.dst = g->dst;
+    args.w = g->w;
+    args.dist = b.dist;
+    args.pend = b.pend;
+    args.farm = b.farm;
+    args.maskq = b.maskq;
+    args.far_list[0] = b.far_list[0];
+    args.far_list[1] = b.far_list[1];
+    args.desc = b.desc;
+    args.desc_cap = b.desc_cap;
+    args.c = b.c;
+    args.q[0] = G.q[0];
+    args.q[1] = G.q[1];
+    args.V = g->V;
+    args.ms_edges = g->tune_alg[CGB_SSSP].ms_edges;
+    args.delta = G.delta;
+    args.max_ticks = 4u * g->V + 64u;
+    args.budget_ns = kLoopBudgetNs;
+    args.mailbox = G.mailbox;
+    args.st = G.sp_loop;
+    void* kargs[] = {&args};
+    std::lock_guard<std::mutex> coop(s->coop_mu);
+    if (g->w) {
+        static uint32_t grid = 0;
+        if (!grid) grid = cooperative_grid_n(k_srv_sssp_loop<true>, 4);
+        CGB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_srv_sssp_loop<true>, grid, kBlock, kargs, 0, G.stream));
+    } else {
+        static uint32_t grid = 0;
+        if (!grid) grid = cooperative_grid_n(k_srv_sssp_loop<false>, 4);
+        CGB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_srv_sssp_loop<false>, grid, kBlock, kargs, 0, G.stream));
+    }
+    CGB_CUDA_TRY(cudaMemcpyAsync(&h, G.sp_loop, sizeof(SrvSpLoopState), cudaMemcpyDeviceToHost, G.stream));
+    CGB_CUDA_TRY(cudaMemcpyAsync(b.h, b.c, sizeof(MsspCounters), cudaMemcpyDeviceToHost, G.stream));
+    CGB_CUDA_TRY(cudaEventRecord(G.ev_loop, G.stream));
+    for (;;) {
+        const cudaError_t e = cudaEventQuery(G.ev_loop);
+        if (e == cudaSuccess) break;
+        if (e != cudaErrorNotReady) CGB_CUDA_TRY(e);
+        if (admission_due(s, G, 1)) *reinterpret_cast<volatile uint32_t*>(G.mailbox) = 1;
+        std::this_thread::sleep_for(std::chrono::microseconds(20));
+    }
+    CGB_REQUIRE(!b.h->overflow, CGB_EOVERFLOW, "server SSSP loop: queue overflow");
+    CGB_REQUIRE(!(h.ps.status & 1u), CGB_ETIMEOUT, "server SSSP loop: grid barrier gave up");
+    for (uint32_t k = 0; k < kSrvSlots; k++) {
+        G.thr[k] = h.thr[k];
+        G.min_far[k] = h.min_far[k];
+        G.last_empty[k] = h.last_empty[k] != 0;
+    }
+    G.near_alive = h.near_alive;
+    G.far_alive = h.far_alive;
+    G.cur = h.cur;
+    G.fcur = h.fcur;
+    G.tick += h.ticks;
+    G.loop_levels += h.ticks;
+    G.loop_launches++;
+    return h.ticks ? h.finished : 0ull;
 }
 
 // After the tick's kernels completed: slots whose traversal ended.
@@ -581,17 +1147,35 @@ static void group_loop(cgb_server* s, int a)
             if (a == 0) {
                 std::lock_guard<GraphMutex> glk(g->mu);
                 g->tune = g->tune_alg[CGB_BFS];
-                bfs_issue(s, G);
-                CGB_CUDA_TRY(cudaMemcpyAsync(G.h_stats->alive, G.d_stats->alive, sizeof(G.h_stats->alive),
-                                             cudaMemcpyDeviceToHost, G.stream));
-                CGB_CUDA_TRY(cudaMemcpyAsync(g->h_ctr, g->ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, G.stream));
-                CGB_CUDA_TRY(cudaStreamSynchronize(G.stream));
-                fin = group_finished(s, G);
+                bfs_admit(s, G);
+                // small frontiers whose levels push: on the device, many levels per launch
+                const uint32_t nf_exit = std::max<uint32_t>(g->tune.persist_enter, 1u);
+                const bool pull = (double)G.medges * 15.0 > (double)g->E;
+                uint64_t before = G.loop_levels;
+                fin = 0;
+                if (G.loop && G.nact > 0 && G.nact <= nf_exit && !pull) fin = bfs_device_levels(s, G, nf_exit);
+                if (G.loop_levels == before) {
+                    bfs_issue(s, G);
+                    CGB_CUDA_TRY(cudaMemcpyAsync(G.h_stats->alive, G.d_stats->alive, sizeof(G.h_stats->alive),
+                                                 cudaMemcpyDeviceToHost, G.stream));
+                    CGB_CUDA_TRY(cudaMemcpyAsync(g->h_ctr, g->ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost,
+                                                 G.stream));
+                    CGB_CUDA_TRY(cudaStreamSynchronize(G.stream));
+                    fin = group_finished(s, G);
+                }
                 group_retire(s, G, fin);
             } else {
-                sp_issue(s, G);
-                CGB_CUDA_TRY(cudaStreamSynchronize(G.stream));
-                fin = group_finished(s, G);
+                uint64_t before = G.loop_levels;
+                fin = 0;
+                if (G.sp_loop) {
+                    sp_admit(s, G);
+                    fin = sp_device_ticks(s, G);
+                }
+                if (G.loop_levels == before) {
+                    sp_issue(s, G);
+                    CGB_CUDA_TRY(cudaStreamSynchronize(G.stream));
+                    fin = group_finished(s, G);
+                }
                 group_retire(s, G, fin);
             }
             std::lock_guard<std::mutex> lk(s->mu);
@@ -679,6 +1263,7 @@ cgb_status cgb_server_create(cgb_graph* g, const cgb_server_config* cfg, cgb_ser
         if (ns && g->w && g->sum_w == 0) compute_weight_sum(g);
         cgb_server* s = new cgb_server();
         s->g = g;
+        s->flags = c.flags;
         try {
             group_alloc(s, s->grp[0], CGB_BFS, nb);
             group_alloc(s, s->grp[1], CGB_SSSP, ns);

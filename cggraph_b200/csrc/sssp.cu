@@ -28,7 +28,13 @@ namespace cgb {
 __shared__ uint32_t s_sssp_newfar;  // per-CTA count of vertices newly set in the far bitmap
 __shared__ unsigned long long s_sssp_medges;  // per-CTA out-degree sum of the next near queue
 __shared__ uint32_t s_sssp_touched;  // per-CTA count of vertices reached for the first time
+__shared__ uint32_t s_sssp_maxdeg;   // per-CTA longest list of the next near queue
 
+// Push round: each improvement is an atomicMin whose returned value tells the
+// one thread that lowered a distance; it claims the vertex in the near
+// bitmap (next near queue, distance below thr) or the far bitmap.  Edges are
+// visited kBatch slots per lane at a time (push.cuh): the slots' edge,
+// distance and bitmap loads are each issued together.
 template <bool kHasW>
 struct SsspOp {
     const uint32_t* __restrict__ off;
@@ -43,6 +49,7 @@ struct SsspOp {
     uint32_t cap;
     uint32_t* far_bm;
     DevCounters* ctr;
+    static constexpr int kBatch = 4;
 
     __device__ __forceinline__ bool load(uint32_t v, uint32_t& s, uint32_t& d, uint32_t& m) const
     {
@@ -51,43 +58,82 @@ struct SsspOp {
         m = dist[v];
         return m < kValueMax;
     }
-    __device__ __forceinline__ void edge(bool valid, uint32_t e, uint32_t du) const
+    template <int N>
+    __device__ __forceinline__ void edges(const bool (&valid)[N], const uint32_t (&e)[N],
+                                          const uint32_t (&du)[N]) const
     {
-        bool to_near = false, new_far = false, first = false;
-        uint32_t d = 0;
-        if (valid) {
+        uint32_t d[N], nd[N], cur[N], old[N], word[N], bit[N];
+        bool ok[N], near_c[N], far_c[N], first[N], to_near[N], new_far[N];
+#pragma unroll
+        for (int i = 0; i < N; i++) {
             // the edge arrays stream through once: evict first, so L2 keeps dist[] and the bitmaps
-            d = __ldcs(dst + e);
-            const uint64_t cand = (uint64_t)du + (kHasW ? (uint64_t)__ldcs(w + e) : 1ull);
-            if (cand < kValueMax) {
-                const uint32_t nd = (uint32_t)cand;
-                if (nd < dist[d]) {
-                    const uint32_t old = atomicMin(dist + d, nd);
-                    first = old == kValueMax;
-                    if (nd < old && d < nz) {
-                        if (nd < thr) {
-                            const uint32_t bit = 1u << (d & 31u);
-                            uint32_t* wp = near_bm + (d >> 5);
-                            to_near = !(*wp & bit) && !(atomicOr(wp, bit) & bit);
-                        } else {
-                            const uint32_t bit = 1u << (d & 31u);
-                            uint32_t* wp = far_bm + (d >> 5);
-                            new_far = !(*wp & bit) && !(atomicOr(wp, bit) & bit);
-                        }
-                    }
-                }
+            d[i] = valid[i] ? __ldcs(dst + e[i]) : 0u;
+            const uint64_t cand = (uint64_t)du[i] + (kHasW ? (valid[i] ? (uint64_t)__ldcs(w + e[i]) : 0ull) : 1ull);
+            ok[i] = valid[i] && cand < kValueMax;
+            nd[i] = ok[i] ? (uint32_t)cand : 0u;
+        }
+#pragma unroll
+        for (int i = 0; i < N; i++) cur[i] = ok[i] ? dist[d[i]] : 0u;
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+            ok[i] = ok[i] && nd[i] < cur[i];
+            old[i] = ok[i] ? atomicMin(dist + d[i], nd[i]) : 0u;
+        }
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+            first[i] = ok[i] && old[i] == kValueMax;
+            const bool q = ok[i] && nd[i] < old[i] && d[i] < nz;
+            near_c[i] = q && nd[i] < thr;
+            far_c[i] = q && !near_c[i];
+            bit[i] = 1u << (d[i] & 31u);
+            word[i] = q ? (near_c[i] ? near_bm : far_bm)[d[i] >> 5] : ~0u;
+        }
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+            bool fresh = false;
+            if (!(word[i] & bit[i])) fresh = !(atomicOr((near_c[i] ? near_bm : far_bm) + (d[i] >> 5), bit[i]) & bit[i]);
+            to_near[i] = fresh && near_c[i];
+            new_far[i] = fresh && far_c[i];
+        }
+        warp_append_n<N>(to_near, d, near_out, near_len, cap, &ctr->overflow);
+        uint32_t nf = 0, nt = 0;
+        bool any_near = false;
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+            nf += __popc(__ballot_sync(0xffffffffu, new_far[i]));
+            nt += __popc(__ballot_sync(0xffffffffu, first[i]));
+            any_near |= to_near[i];
+        }
+        if (nf && lane_id() == 0) atomicAdd(&s_sssp_newfar, nf);
+        if (nt && lane_id() == 0) atomicAdd(&s_sssp_touched, nt);
+        if (__any_sync(0xffffffffu, any_near)) {
+            // out-edges of the next near queue: the next round's push / pull choice
+            uint32_t lo[N], hi[N];
+#pragma unroll
+            for (int i = 0; i < N; i++) {
+                lo[i] = to_near[i] ? off[d[i]] : 0u;
+                hi[i] = to_near[i] ? off[d[i] + 1] : 0u;
+            }
+            unsigned long long dg = 0;
+            uint32_t mx = 0;
+#pragma unroll
+            for (int i = 0; i < N; i++) {
+                dg += hi[i] - lo[i];
+                mx = max(mx, hi[i] - lo[i]);
+            }
+            dg = warp_sum(dg);
+            mx = warp_max(mx);
+            if (dg && lane_id() == 0) {
+                atomicAdd(&s_sssp_medges, dg);
+                atomicMax(&s_sssp_maxdeg, mx);
             }
         }
-        warp_append(to_near, d, near_out, near_len, cap, &ctr->overflow);
-        const uint32_t nf = __popc(__ballot_sync(0xffffffffu, new_far));
-        if (nf && lane_id() == 0) atomicAdd(&s_sssp_newfar, nf);
-        const uint32_t nt = __popc(__ballot_sync(0xffffffffu, first));
-        if (nt && lane_id() == 0) atomicAdd(&s_sssp_touched, nt);
-        if (__any_sync(0xffffffffu, to_near)) {
-            // out-edges of the next near queue: the next round's push / pull choice
-            const unsigned long long dg = warp_sum((unsigned long long)(to_near ? off[d + 1] - off[d] : 0u));
-            if (dg && lane_id() == 0) atomicAdd(&s_sssp_medges, dg);
-        }
+    }
+    __device__ __forceinline__ void edge(bool valid, uint32_t e, uint32_t du) const
+    {
+        const bool v[1] = {valid};
+        const uint32_t ee[1] = {e}, m[1] = {du};
+        edges<1>(v, ee, m);
     }
     __device__ __forceinline__ void block_begin() const
     {
@@ -95,6 +141,7 @@ struct SsspOp {
             s_sssp_newfar = 0;
             s_sssp_medges = 0;
             s_sssp_touched = 0;
+            s_sssp_maxdeg = 0;
         }
     }
     __device__ __forceinline__ void block_end() const
@@ -102,6 +149,7 @@ struct SsspOp {
         if (threadIdx.x == 0 && s_sssp_newfar) atomicAdd(&ctr->far_len[0], s_sssp_newfar);
         if (threadIdx.x == 0 && s_sssp_medges) atomicAdd(&ctr->medges, s_sssp_medges);
         if (threadIdx.x == 0 && s_sssp_touched) atomicAdd(&ctr->touched, s_sssp_touched);
+        if (threadIdx.x == 0 && s_sssp_maxdeg) atomicMax(&ctr->max_deg, s_sssp_maxdeg);
     }
 };
 
@@ -109,12 +157,16 @@ struct SsspOp {
 // fire-and-forget atomicMin (the result is unused, so it issues as a
 // reduction) and enqueue nothing; k_sssp_dense_scan then finds the improved
 // vertices by comparing dist[] with its snapshot from before the round.
+// (Marking improved vertices in a bitmap instead costs more than the scan:
+// the bitmap's words are shared by 32 vertices, and their reductions queue
+// behind each other.)  Edges are visited kBatch slots per lane at a time.
 template <bool kHasW>
 struct SsspDenseOp {
     const uint32_t* __restrict__ off;
     const uint32_t* __restrict__ dst;
     const uint32_t* __restrict__ w;
     uint32_t* dist;
+    static constexpr int kBatch = 4;
 
     __device__ __forceinline__ bool load(uint32_t v, uint32_t& s, uint32_t& d, uint32_t& m) const
     {
@@ -123,57 +175,110 @@ struct SsspDenseOp {
         m = dist[v];
         return m < kValueMax;
     }
+    template <int N>
+    __device__ __forceinline__ void edges(const bool (&valid)[N], const uint32_t (&e)[N],
+                                          const uint32_t (&du)[N]) const
+    {
+        uint32_t d[N], nd[N], cur[N];
+        bool ok[N];
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+            d[i] = valid[i] ? __ldcs(dst + e[i]) : 0u;
+            const uint64_t cand = (uint64_t)du[i] + (kHasW ? (valid[i] ? (uint64_t)__ldcs(w + e[i]) : 0ull) : 1ull);
+            ok[i] = valid[i] && cand < kValueMax;
+            nd[i] = ok[i] ? (uint32_t)cand : 0u;
+        }
+#pragma unroll
+        for (int i = 0; i < N; i++) cur[i] = ok[i] ? dist[d[i]] : 0u;
+#pragma unroll
+        for (int i = 0; i < N; i++)
+            if (ok[i] && nd[i] < cur[i]) atomicMin(dist + d[i], nd[i]);
+    }
     __device__ __forceinline__ void edge(bool valid, uint32_t e, uint32_t du) const
     {
-        if (!valid) return;
-        const uint32_t d = __ldcs(dst + e);
-        const uint64_t cand = (uint64_t)du + (kHasW ? (uint64_t)__ldcs(w + e) : 1ull);
-        if (cand < kValueMax && (uint32_t)cand < dist[d]) atomicMin(dist + d, (uint32_t)cand);
+        const bool v[1] = {valid};
+        const uint32_t ee[1] = {e}, m[1] = {du};
+        edges<1>(v, ee, m);
     }
     __device__ __forceinline__ void block_begin() const {}
     __device__ __forceinline__ void block_end() const {}
 };
 
 // After a dense round: every vertex whose distance dropped below its snapshot
-// joins the next near queue (below thr) or the far bitmap.  A warp owns one
-// 32-vertex bitmap word, so far bits are set without atomics; the next
-// queue's out-edges and the new far bits are counted.
+// joins the next near queue (below thr) or the far bitmap; first touches
+// (the snapshot was infinite) are counted.  A lane takes four consecutive
+// vertices with one 16-byte load of each array, so a warp covers 128
+// vertices = 4 bitmap words per step; the 8 lanes of a word OR their far
+// bits together, and the first of them writes the word (no atomics: only
+// this warp touches it).  The next queue's out-edges and the new far bits
+// are counted.
 __global__ void __launch_bounds__(kBlock) k_sssp_dense_scan(uint32_t V, const uint32_t* __restrict__ dist,
                                                             const uint32_t* __restrict__ snap, uint32_t thr,
                                                             uint32_t nz, const uint32_t* __restrict__ off,
                                                             uint32_t* far_bm, uint32_t* near_out, uint32_t* near_len,
                                                             uint32_t cap, DevCounters* ctr)
 {
-    const uint32_t n_round = (V + 31u) & ~31u;
+    const uint32_t lane = lane_id();
+    const uint32_t gw = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    const uint32_t nwarps = gridDim.x * (blockDim.x / 32);
     unsigned long long deg_sum = 0;
-    uint32_t new_far = 0, touched = 0;
-    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n_round; v += gridDim.x * blockDim.x) {
-        bool to_near = false, to_far = false;
-        if (v < V) {
-            const uint32_t dv = dist[v], sv = snap[v];
-            touched += (sv == kValueMax && dv < kValueMax) ? 1u : 0u;
-            if (v < nz && dv < sv) {
-                to_near = dv < thr;
-                to_far = !to_near;
-                if (to_near) deg_sum += off[v + 1] - off[v];
+    uint32_t new_far = 0, touched = 0, max_deg = 0;
+    for (uint64_t b0 = (uint64_t)gw * 128; b0 < V; b0 += (uint64_t)nwarps * 128) {
+        const uint32_t v0 = (uint32_t)b0 + 4 * lane;
+        uint32_t dv[4], sv[4], v[4];
+        if (v0 + 3 < V) {
+            const uint4 a = *reinterpret_cast<const uint4*>(dist + v0);
+            const uint4 b = *reinterpret_cast<const uint4*>(snap + v0);
+            dv[0] = a.x, dv[1] = a.y, dv[2] = a.z, dv[3] = a.w;
+            sv[0] = b.x, sv[1] = b.y, sv[2] = b.z, sv[3] = b.w;
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                dv[k] = v0 + k < V ? dist[v0 + k] : kValueMax;
+                sv[k] = v0 + k < V ? snap[v0 + k] : kValueMax;
             }
         }
-        warp_append(to_near, v, near_out, near_len, cap, &ctr->overflow);
-        const uint32_t fm = __ballot_sync(0xffffffffu, to_far);
-        if (fm && lane_id() == 0) {
-            const uint32_t old = far_bm[v >> 5];
+        bool to_near[4];
+        uint32_t far4 = 0, lo[4], hi[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            v[k] = v0 + k;
+            touched += (sv[k] == kValueMax && dv[k] < kValueMax) ? 1u : 0u;
+            const bool imp = v[k] < nz && dv[k] < sv[k];
+            to_near[k] = imp && dv[k] < thr;
+            if (imp && !to_near[k]) far4 |= 1u << k;
+            lo[k] = to_near[k] ? off[v[k]] : 0u;
+            hi[k] = to_near[k] ? off[v[k] + 1] : 0u;
+        }
+        // lanes 8j .. 8j+7 hold the 32 vertices of bitmap word b0/32 + j
+        uint32_t fm = far4 << (4 * (lane & 7u));
+        fm |= __shfl_xor_sync(0xffffffffu, fm, 1);
+        fm |= __shfl_xor_sync(0xffffffffu, fm, 2);
+        fm |= __shfl_xor_sync(0xffffffffu, fm, 4);
+        if ((lane & 7u) == 0 && fm) {
+            const uint32_t wi = v0 >> 5;
+            const uint32_t old = far_bm[wi];
             if (fm & ~old) {
-                far_bm[v >> 5] = old | fm;
+                far_bm[wi] = old | fm;
                 new_far += __popc(fm & ~old);
             }
         }
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            deg_sum += hi[k] - lo[k];
+            max_deg = max(max_deg, hi[k] - lo[k]);
+        }
+        warp_append_n<4>(to_near, v, near_out, near_len, cap, &ctr->overflow);
     }
     deg_sum = warp_sum(deg_sum);
     touched = warp_sum(touched);
-    if (lane_id() == 0) {
+    new_far = warp_sum(new_far);
+    max_deg = warp_max(max_deg);
+    if (lane == 0) {
         if (deg_sum) atomicAdd(&ctr->medges, deg_sum);
         if (new_far) atomicAdd(&ctr->far_len[0], new_far);
         if (touched) atomicAdd(&ctr->touched, touched);
+        if (max_deg) atomicMax(&ctr->max_deg, max_deg);
     }
 }
 
@@ -186,6 +291,7 @@ __global__ void k_sssp_round_reset(DevCounters* ctr, int out, uint32_t* bm, uint
         ctr->qlen[out] = 0;
         ctr->chunk_len = 0;
         ctr->medges = 0;
+        ctr->max_deg = 0;
     }
     if (bm)
         for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < words; i += gridDim.x * blockDim.x) bm[i] = 0;
@@ -198,6 +304,7 @@ __global__ void k_sssp_split_reset(DevCounters* ctr, int out)
     ctr->far_len[0] = 0;
     ctr->min_far = 0xFFFFFFFFu;
     ctr->medges = 0;
+    ctr->max_deg = 0;
 }
 
 __global__ void k_sssp_init(uint32_t V, uint32_t* dist, uint32_t* far_bm, uint32_t words)
@@ -213,54 +320,79 @@ __global__ void k_sssp_root(uint32_t* dist, uint32_t root, uint32_t* q0)
     q0[0] = root;
 }
 
-// Splits the far bitmap at [lo, hi) (see file comment).  One lane per bitmap
-// word; far_len[0] receives the number of vertices left in the bitmap and
-// min_far the smallest distance among them.
+// Splits the far bitmap at [lo, hi) (see file comment).  A warp takes 32
+// consecutive words with one coalesced load and visits the non-zero ones
+// four at a time, lane b of word j reading the distance of vertex 32 * j + b
+// (coalesced, four words in flight); the warp owns its words, so it writes
+// back what stays without atomics.  far_len[0] receives the number of
+// vertices left in the bitmap and min_far the smallest distance among them.
 __global__ void __launch_bounds__(kBlock) k_sssp_split(uint32_t words, uint32_t* far_bm, const uint32_t* dist,
                                                        uint32_t lo, uint32_t hi, uint32_t* near_out,
                                                        uint32_t* near_len, uint32_t cap, DevCounters* ctr,
                                                        const uint32_t* __restrict__ off)
 {
-    uint32_t mn = kValueMax, left = 0;
+    constexpr int N = 4;
+    const uint32_t lane = lane_id();
+    const uint32_t gw = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    const uint32_t nwarps = gridDim.x * (blockDim.x / 32);
+    uint32_t mn = kValueMax, left = 0, max_deg = 0;
     unsigned long long dg = 0;
-    const uint32_t stride = gridDim.x * blockDim.x;
-    const uint32_t words_round = (words + 31u) & ~31u;
-    for (uint32_t wi = blockIdx.x * blockDim.x + threadIdx.x; wi < words_round; wi += stride) {
-        uint32_t word = wi < words ? far_bm[wi] : 0u;
-        uint32_t keep = word;
-        // at most 32 near candidates per lane: append them one bit position at a time
-        while (__any_sync(0xffffffffu, word != 0)) {
-            bool to_near = false;
-            uint32_t v = 0;
-            if (word) {
-                const uint32_t b = __ffs(word) - 1;
-                word &= word - 1;
-                v = wi * 32 + b;
-                const uint32_t dv = dist[v];
-                if (dv < hi) {
-                    keep &= ~(1u << b);
-                    to_near = dv >= lo;
-                    if (to_near) dg += off[v + 1] - off[v];
-                } else {
-                    mn = min(mn, dv);
-                }
+    for (uint32_t w0 = gw * 32; w0 < words; w0 += nwarps * 32) {
+        const uint32_t mine = w0 + lane < words ? far_bm[w0 + lane] : 0u;
+        uint32_t todo = __ballot_sync(0xffffffffu, mine != 0);
+        while (todo) {
+            uint32_t wi[N], bits[N], v[N], dv[N];
+            bool in[N];
+#pragma unroll
+            for (int k = 0; k < N; k++) {
+                const uint32_t j = todo ? __ffs(todo) - 1 : 32u;
+                todo &= todo ? todo - 1 : 0u;
+                bits[k] = j < 32 ? __shfl_sync(0xffffffffu, mine, j & 31u) : 0u;
+                wi[k] = w0 + (j & 31u);
+                v[k] = wi[k] * 32 + lane;
+                in[k] = (bits[k] >> lane) & 1u;
             }
-            warp_append(to_near, v, near_out, near_len, cap, &ctr->overflow);
-        }
-        if (wi < words) {
-            if (keep != far_bm[wi]) far_bm[wi] = keep;
-            left += __popc(keep);
+#pragma unroll
+            for (int k = 0; k < N; k++) dv[k] = in[k] ? dist[v[k]] : 0u;
+            bool to_near[N];
+            uint32_t a[N], b[N];
+#pragma unroll
+            for (int k = 0; k < N; k++) {
+                const bool leave = in[k] && dv[k] < hi;
+                to_near[k] = leave && dv[k] >= lo;
+                const bool keep = in[k] && !leave;
+                if (keep) mn = min(mn, dv[k]);
+                const uint32_t km = __ballot_sync(0xffffffffu, keep);
+                if (lane == 0 && bits[k]) {
+                    if (km != bits[k]) far_bm[wi[k]] = km;
+                    left += __popc(km);
+                }
+                a[k] = to_near[k] ? off[v[k]] : 0u;
+                b[k] = to_near[k] ? off[v[k] + 1] : 0u;
+            }
+#pragma unroll
+            for (int k = 0; k < N; k++) {
+                dg += b[k] - a[k];
+                max_deg = max(max_deg, b[k] - a[k]);
+            }
+            warp_append_n<N>(to_near, v, near_out, near_len, cap, &ctr->overflow);
         }
     }
     mn = __reduce_min_sync(0xffffffffu, mn);
-    left = warp_sum(left);
     dg = warp_sum(dg);
-    if (lane_id() == 0) {
+    max_deg = warp_max(max_deg);
+    if (lane == 0) {
         if (mn != kValueMax) atomicMin(&ctr->min_far, mn);
         if (left) atomicAdd(&ctr->far_len[0], left);
         if (dg) atomicAdd(&ctr->medges, dg);
+        if (max_deg) atomicMax(&ctr->max_deg, max_deg);
     }
 }
+
+// Near rounds smaller than this (and with fewer than E / 1024 out-edges)
+// are neither sampled for the learned scheduler nor preceded by its
+// inference: their variant hardly changes the run's time.
+constexpr uint64_t kCollectMinRound = 4096;
 
 template <bool kHasW>
 static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_options& o)
@@ -290,6 +422,7 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
     uint64_t thr = delta;
     uint64_t bucket_lo = 0;      // the current bucket is [bucket_lo, thr): every near vertex is in it
     uint64_t near_edges = 0;     // out-edges of the near queue (0 = unknown: push)
+    uint32_t near_maxdeg = ~0u;  // longest list of the near queue (unknown for the root: its round runs here)
     double touch_rate = 0.0;     // vertices reached for the first time per edge, last push or dense round
     uint64_t touched_seen = 0;   // ctr->touched after that round
     // pull rounds need the in-edges (and their weights in CSC order)
@@ -297,71 +430,170 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
     uint64_t iters = 0;
     uint64_t expanded = 0;
 
+    // The device-resident tail (persist.cuh): once the near queue holds at
+    // most persist_enter vertices whose lists are all shorter than
+    // persist_deg edges, near rounds and bucket splits run in one cooperative
+    // launch until the run ends or a frontier outgrows those bounds (then
+    // the host loop's binned kernels take over again).  It keeps the current
+    // delta for the buckets it splits.  Graphs with lists of persist_deg
+    // edges or more (power-law graphs) stay on the host loop: their tail
+    // rounds hold medium-degree lists that the tail's one-warp-per-list
+    // expansion walks slowly, and their frontiers outgrow the tail's bounds
+    // bucket after bucket (measured on RMAT-24: 6.9 against 5.2 ms a run).
+    // Under the learned schedule the tail waits for the first bucket
+    // boundary, so that the network picks the delta it keeps.
+    const bool tail_ok = !tracing && !collect && o.schedule != CGB_SCHED_FIXED && g->tune.persist_enter > 0 &&
+                         g->max_degree < g->tune.persist_deg;
+    bool tail_delta_chosen = pol == nullptr;
+    auto device_tail = [&]() -> bool {
+        if (timing) ktimer_begin(g, CGB_K_PUSH);
+        const SsspTail t = sssp_device_tail(g, cur, (uint32_t)nnear, near_maxdeg, thr, (uint32_t)nfar, bucket_lo,
+                                            far_bm, delta, g->tune.persist_enter, g->tune.persist_deg,
+                                            (uint32_t)std::min<uint64_t>(max_iters - iters, 1u << 30));
+        if (timing) ktimer_end(g);
+        iters += t.r.levels;
+        expanded += t.r.added;
+        nnear = t.r.nf;
+        near_maxdeg = t.r.max_deg;
+        nfar = t.nfar;
+        thr = t.thr;
+        bucket_lo = t.bucket_lo;
+        near_edges = 0;  // not counted by the device-resident rounds: push next
+        cur = (int)t.r.cur;
+        return t.r.levels > 0;
+    };
+    // Queues one near round of the given RoundVariant, next near queue to q[out].
+    auto run_round = [&](int variant, int out) {
+        const bool pull = variant == kRoundPull, dense = variant == kRoundDense;
+        if (pull) {
+            ensure_csc(g);
+            ensure_csc_weights(g);
+        }
+        ++g->stats.launches;
+        k_sssp_round_reset<<<(!pull && !dense) ? num_sms() * 2 : 1, kBlock, 0, g->stream>>>(
+            g->ctr, out, (!pull && !dense) ? near_bm : nullptr, words);
+        if (timing) ktimer_begin(g, pull ? CGB_K_PULL : CGB_K_PUSH);
+        if (pull) {
+            sssp_pull_round(g, g->q[cur], (uint32_t)nnear, (uint32_t)std::min<uint64_t>(bucket_lo, kValueMax),
+                            (uint32_t)std::min<uint64_t>(thr, kValueMax), g->q[out], &g->ctr->qlen[out], far_bm,
+                            g->aux_bm);
+        } else if (dense) {
+            CGB_CUDA_TRY(cudaMemcpyAsync(g->stamp, g->value, (size_t)V * 4, cudaMemcpyDeviceToDevice, g->stream));
+            SsspDenseOp<kHasW> op{g->off, g->dst, g->w, g->value};
+            launch_push(g, g->q[cur], (uint32_t)nnear, op, false);
+            ++g->stats.launches;
+            k_sssp_dense_scan<<<grid_for(div_up(V, 4), kBlock, num_sms() * 8), kBlock, 0, g->stream>>>(
+                V, g->value, g->stamp, (uint32_t)std::min<uint64_t>(thr, kValueMax), g->nz, g->off, far_bm,
+                g->q[out], &g->ctr->qlen[out], V, g->ctr);
+        } else {
+            SsspOp<kHasW> op{g->off, g->dst, g->w, g->value, near_bm,
+                             (uint32_t)std::min<uint64_t>(thr, kValueMax), g->nz, g->q[out], &g->ctr->qlen[out],
+                             V, far_bm, g->ctr};
+            launch_push(g, g->q[cur], (uint32_t)nnear, op, false,
+                        variant == kRoundPushChunked ? kExpandChunked : kExpandBinned);
+        }
+        if (timing) ktimer_end(g);
+    };
+    int last_variant = kRoundPush;
+    bool have_round_out = false;  // the policy's outputs for the next round were read back
+    // set while a bucket phase runs as one of the delta trials of a sample:
+    // its rounds are not sampled themselves (the trial's timing events must
+    // span the whole phase)
+    bool in_delta_trial = false;
+    auto round_state = [&]() {
+        FeatIn in{};
+        in.alg = CGB_SSSP;
+        in.iteration = (uint32_t)iters;
+        in.prev_dir = last_variant;
+        in.symmetric = g->symmetric == 1;
+        in.V = V;
+        in.E = g->E;
+        in.nf = (double)nnear;
+        in.mf = (double)near_edges;
+        in.max_deg = near_maxdeg == ~0u ? 0.0 : (double)near_maxdeg;
+        in.unvisited_v = (double)V - (double)g->h_ctr->touched;
+        in.unvisited_e = (double)near_edges * touch_rate;  // improvements the round is expected to make
+        in.delta = delta;
+        in.base_delta = base_delta;
+        in.far_count = (double)nfar;
+        in.settled = (double)std::min<uint64_t>(expanded, V);
+        return in;
+    };
     // Near rounds at threshold thr until the near queue is empty.
-    const bool persist_ok = !tracing && o.schedule != CGB_SCHED_FIXED && g->max_degree < g->tune.persist_deg;
     auto near_rounds = [&]() {
         while (nnear > 0) {
             CGB_REQUIRE(iters < max_iters, CGB_ETIMEOUT, "SSSP iteration budget exhausted");
-            if (persist_ok && nnear <= g->tune.persist_enter) {
-                // small near queue: run the rounds on the device
-                if (timing) ktimer_begin(g, CGB_K_PUSH);
-                const PersistResult r =
-                    sssp_persistent(g, cur, (uint32_t)nnear, (uint32_t)std::min<uint64_t>(thr, kValueMax), far_bm,
-                                    g->tune.persist_enter, (uint32_t)std::min<uint64_t>(max_iters - iters, 1u << 20));
-                if (timing) ktimer_end(g);
-                sync_counters(g);
-                iters += r.levels;
-                expanded += r.added;
-                nnear = r.nf;
-                nfar = g->h_ctr->far_len[0];
-                near_edges = 0;  // not counted by the device-resident rounds: push next
-                cur = r.cur;
-                if (r.levels > 0) continue;
+            if (tail_ok && tail_delta_chosen && nnear <= g->tune.persist_enter && near_maxdeg < g->tune.persist_deg) {
+                have_round_out = false;
+                if (device_tail()) continue;
             }
             const int out = cur ^ 1;
-            // direction: pull when the near set's out-edges times alpha exceed the graph's edges;
-            // else a dense frontier when they are many for what the round will change.  A push
-            // round pays an atomic with a returned value and a queue append per improvement, a
-            // dense round a reduction per edge plus one pass over V.  While the search reaches
-            // new territory nearly every edge improves its target, so the out-edges are weighted
-            // by the previous round's first touches per edge, floored at 1/8 for the rounds that
-            // mostly lower known distances
-            const bool pull = pull_ok && (double)near_edges * g->tune.sssp_pull_alpha > (double)g->E;
-            const bool dense = !pull && o.schedule != CGB_SCHED_FIXED && g->tune.sssp_dense_alpha > 0 &&
-                               (double)near_edges * g->tune.sssp_dense_alpha * std::max(touch_rate, 0.125) >
-                                   (double)V;
-            if (pull) {
+            // heuristic: pull when the near set's out-edges times alpha exceed the graph's
+            // edges; else a dense frontier when they are many for what the round will change.
+            // A push round pays an atomic with a returned value and a queue append per
+            // improvement, a dense round a reduction per edge plus one pass over V.  While the
+            // search reaches new territory nearly every edge improves its target, so the
+            // out-edges are weighted by the previous round's first touches per edge, floored at
+            // 1/8 for the rounds that mostly lower known distances.  A push round chunks every
+            // list of 32 edges or more when its queue is small.
+            const bool h_pull = pull_ok && (double)near_edges * g->tune.sssp_pull_alpha > (double)g->E;
+            const bool h_dense = !h_pull && o.schedule != CGB_SCHED_FIXED && g->tune.sssp_dense_alpha > 0 &&
+                                 (double)near_edges * g->tune.sssp_dense_alpha * std::max(touch_rate, 0.125) >
+                                     (double)V;
+            const int heur = h_pull ? kRoundPull
+                             : h_dense ? kRoundDense
+                                       : (nnear <= kSmallFrontier ? kRoundPushChunked : kRoundPush);
+            int variant = heur;
+            if (collect && !in_delta_trial && (nnear >= kCollectMinRound || near_edges >= g->E / 1024)) {
+                // counterfactual: the four round variants from the same state, timed
                 ensure_csc(g);
                 ensure_csc_weights(g);
+                const size_t vbytes = (size_t)V * 4, wbytes = (size_t)words * 4, qbytes = nnear * 4;
+                CGB_CUDA_TRY(cudaMemcpyAsync(collect->save_value, g->value, vbytes, cudaMemcpyDeviceToDevice,
+                                             g->stream));
+                CGB_CUDA_TRY(cudaMemcpyAsync(collect->save_bm0, far_bm, wbytes, cudaMemcpyDeviceToDevice, g->stream));
+                CGB_CUDA_TRY(cudaMemcpyAsync(collect->save_q, g->q[cur], qbytes, cudaMemcpyDeviceToDevice,
+                                             g->stream));
+                CGB_CUDA_TRY(cudaMemcpyAsync(collect->save_ctr, g->ctr, sizeof(DevCounters),
+                                             cudaMemcpyDeviceToDevice, g->stream));
+                float ms[kPolicyOutputs] = {};
+                bool have[kPolicyOutputs] = {};
+                int best = heur;
+                for (int v = 0; v < kNumRoundChoices; v++) {
+                    CGB_CUDA_TRY(cudaEventRecord(g->ev_iter[0], g->stream));
+                    run_round(v, out);
+                    CGB_CUDA_TRY(cudaEventRecord(g->ev_iter[1], g->stream));
+                    CGB_CUDA_TRY(cudaEventSynchronize(g->ev_iter[1]));
+                    CGB_CUDA_TRY(cudaEventElapsedTime(&ms[kOutRound0 + v], g->ev_iter[0], g->ev_iter[1]));
+                    have[kOutRound0 + v] = true;
+                    if (ms[kOutRound0 + v] < ms[kOutRound0 + best]) best = v;
+                    CGB_CUDA_TRY(cudaMemcpyAsync(g->value, collect->save_value, vbytes, cudaMemcpyDeviceToDevice,
+                                                 g->stream));
+                    CGB_CUDA_TRY(cudaMemcpyAsync(far_bm, collect->save_bm0, wbytes, cudaMemcpyDeviceToDevice,
+                                                 g->stream));
+                    CGB_CUDA_TRY(cudaMemcpyAsync(g->q[cur], collect->save_q, qbytes, cudaMemcpyDeviceToDevice,
+                                                 g->stream));
+                    CGB_CUDA_TRY(cudaMemcpyAsync(g->ctr, collect->save_ctr, sizeof(DevCounters),
+                                                 cudaMemcpyDeviceToDevice, g->stream));
+                }
+                policy_log_sample(g, round_state(), ms, have);
+                variant = best;
+            } else if (pol && have_round_out) {
+                const int c = policy_pick_round(g->h_ctr->policy_out, heur);
+                if (c >= 0) variant = c;
             }
-            ++g->stats.launches;
-            k_sssp_round_reset<<<(!pull && !dense) ? num_sms() * 2 : 1, kBlock, 0, g->stream>>>(
-                g->ctr, out, (!pull && !dense) ? near_bm : nullptr, words);
             if (tracing) CGB_CUDA_TRY(cudaEventRecord(g->ev_iter[0], g->stream));
-            if (timing) ktimer_begin(g, pull ? CGB_K_PULL : CGB_K_PUSH);
-            if (pull) {
-                sssp_pull_round(g, g->q[cur], (uint32_t)nnear, (uint32_t)std::min<uint64_t>(bucket_lo, kValueMax),
-                                (uint32_t)std::min<uint64_t>(thr, kValueMax), g->q[out], &g->ctr->qlen[out], far_bm,
-                                g->aux_bm);
-                g->stats.pulls_bu++;
-            } else if (dense) {
-                CGB_CUDA_TRY(cudaMemcpyAsync(g->stamp, g->value, (size_t)V * 4, cudaMemcpyDeviceToDevice, g->stream));
-                SsspDenseOp<kHasW> op{g->off, g->dst, g->w, g->value};
-                launch_push(g, g->q[cur], (uint32_t)nnear, op, false);
-                ++g->stats.launches;
-                k_sssp_dense_scan<<<grid_for(V, kBlock, num_sms() * 8), kBlock, 0, g->stream>>>(
-                    V, g->value, g->stamp, (uint32_t)std::min<uint64_t>(thr, kValueMax), g->nz, g->off, far_bm,
-                    g->q[out], &g->ctr->qlen[out], V, g->ctr);
-                g->stats.pushes_td++;
-            } else {
-                SsspOp<kHasW> op{g->off, g->dst, g->w, g->value, near_bm,
-                                 (uint32_t)std::min<uint64_t>(thr, kValueMax), g->nz, g->q[out], &g->ctr->qlen[out],
-                                 V, far_bm, g->ctr};
-                launch_push(g, g->q[cur], (uint32_t)nnear, op, false);
-                g->stats.pushes_td++;
-            }
-            if (timing) ktimer_end(g);
+            const FeatIn before = round_state();
+            run_round(variant, out);
+            if (variant == kRoundPull) g->stats.pulls_bu++;
+            else g->stats.pushes_td++;
             if (tracing) CGB_CUDA_TRY(cudaEventRecord(g->ev_iter[1], g->stream));
+            // inference for the next round, fused before the counter read-back; skipped
+            // after small rounds, whose successors' variant hardly matters
+            const bool infer = pol && !collect && (nnear >= kCollectMinRound || near_edges >= g->E / 1024);
+            if (infer) policy_enqueue(pol, g, before, 2, false, out);
+            have_round_out = infer;
+            last_variant = variant;
             sync_counters(g);
             CGB_REQUIRE(!g->h_ctr->overflow, CGB_EOVERFLOW, "SSSP queue overflow");
             if (tracing) {
@@ -372,20 +604,21 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
                 t.algorithm = CGB_SSSP;
                 t.frontier_vertices = nnear;
                 t.unvisited_vertices = g->h_ctr->far_len[0];
-                t.variant = pull ? CGB_VAR_PULL : dense ? CGB_VAR_DENSE : CGB_VAR_TWC;
+                t.variant = variant == kRoundPull ? CGB_VAR_PULL : variant == kRoundDense ? CGB_VAR_DENSE : CGB_VAR_TWC;
                 t.frontier_edges = near_edges;
                 t.delta = delta;
                 t.ms = ms;
                 g->trace.push_back(t);
             }
             expanded += nnear;
-            if (!pull && near_edges > 0) {
+            if (variant != kRoundPull && near_edges > 0) {
                 touch_rate = (double)(g->h_ctr->touched - touched_seen) / (double)near_edges;
                 touched_seen = g->h_ctr->touched;
             }
             nnear = g->h_ctr->qlen[out];
             nfar = g->h_ctr->far_len[0];
             near_edges = g->h_ctr->medges;
+            near_maxdeg = g->h_ctr->max_deg;
             cur = out;
             iters++;
         }
@@ -411,6 +644,7 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
             nnear = g->h_ctr->qlen[out];
             nfar = g->h_ctr->far_len[0];
             near_edges = g->h_ctr->medges;
+            near_maxdeg = g->h_ctr->max_deg;
             cur = out;
             iters++;
             bucket_lo = lo;
@@ -450,6 +684,7 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
             float ms[kPolicyOutputs] = {};
             bool have[kPolicyOutputs] = {};
             int best = kDeltaUnit;
+            in_delta_trial = true;
             for (int k = 0; k < kNumDeltaChoices; k++) {
                 const uint32_t dk = std::max<uint32_t>(1u, (uint32_t)(base_delta * delta_scale(k)));
                 CGB_CUDA_TRY(cudaEventRecord(g->ev_iter[0], g->stream));
@@ -473,15 +708,25 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
                 nnear = 0;
                 cur = s_cur;
             }
+            in_delta_trial = false;
             policy_log_sample(g, state_now(), ms, have);
             d = std::max<uint32_t>(1u, (uint32_t)(base_delta * delta_scale(best)));
         } else if (pol) {
-            policy_enqueue(pol, g, state_now(), false, false, 0);
+            policy_enqueue(pol, g, state_now(), 0, false, 0);
             sync_counters(g);
             const int k = policy_pick_delta(g->h_ctr->policy_out);
             if (k >= 0) d = std::max<uint32_t>(1u, (uint32_t)(base_delta * delta_scale(k)));
         }
         delta = d;
+        tail_delta_chosen = true;
+        if (tail_ok) {
+            // the next bucket's split, and what follows, on the device
+            near_maxdeg = 0;
+            if (device_tail()) {
+                near_rounds();
+                continue;
+            }
+        }
         advance(d);
         near_rounds();
     }

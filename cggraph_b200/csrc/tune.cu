@@ -5,9 +5,11 @@
 // (WarpDonate / CTA::schedule switch at 16 / 32 / 256 edges,
 // my_project/CGgraph/device_warpDonate.cuh:42-388, device_CTA.cuh:28-112).
 // Here they are per-graph parameters: the out-degree from which a list is
-// cut into chunks, the chunk length, the push grid (CTAs per SM), the
-// frontier size and list length below which the device-resident loops run,
-// and the multi-root SSSP descriptor length.  None of them changes a result.
+// cut into chunks, the chunk length, the push grid (CTAs per SM) and CTA
+// size (the reference's fixed BLOCKSIZE 256, Basic/Graph/basic_def.hpp:8),
+// the frontier size and list length below which the device-resident loops
+// run, and the multi-root SSSP descriptor length.  None of them changes a
+// result.
 //
 // Each algorithm has its own tuning (a run makes its algorithm's tuning the
 // active one).  The autotuner is coordinate descent: starting from the
@@ -33,7 +35,9 @@ bool valid(const cgb_tuning& t)
            t.push_chunk <= 65536 && pow2(t.push_chunk) && t.push_ctas_per_sm >= 1 && t.push_ctas_per_sm <= 32 &&
            t.persist_deg >= 64 && t.persist_deg <= 65536 && t.ms_edges >= kMinMsEdges && t.ms_edges <= 4096 &&
            (t.pr_unroll == 4 || t.pr_unroll == 8 || t.pr_unroll == 16) && t.pr_ctas_per_sm >= 1 &&
-           t.pr_ctas_per_sm <= 1024 && t.persist_ctas <= 4096 && t.sssp_pull_alpha <= 1024 && t.cluster_enter <= (1u << 24) && t.sssp_dense_alpha <= 1024;
+           t.pr_ctas_per_sm <= 1024 && t.persist_ctas <= 4096 && t.sssp_pull_alpha <= 1024 &&
+           t.cluster_enter <= (1u << 24) && t.sssp_dense_alpha <= 1024 &&
+           (t.push_block == 128 || t.push_block == 256 || t.push_block == 512);
 }
 
 struct Field {
@@ -48,6 +52,7 @@ std::vector<Field> fields()
         {&cgb_tuning::push_big_deg, {128, 256, 512, 1024, 2048, 4096}, true, true, true, false, true, false},
         {&cgb_tuning::push_chunk, {256, 512, 1024, 2048, 4096}, true, true, true, false, true, false},
         {&cgb_tuning::push_ctas_per_sm, {2, 4, 8, 16}, true, true, true, false, true, false},
+        {&cgb_tuning::push_block, {128, 256, 512}, true, true, true, false, true, false},
         {&cgb_tuning::persist_enter, {0, 4096, 16384, 32768, 131072}, true, true, false, false, false, false},
         {&cgb_tuning::persist_deg, {256, 1024, 2048, 8192}, true, true, false, false, false, false},
         {&cgb_tuning::persist_ctas, {0, 16, 32, 64}, true, true, false, false, false, false},
@@ -58,6 +63,40 @@ std::vector<Field> fields()
         {&cgb_tuning::pr_unroll, {4, 8, 16}, false, false, false, true, false, false},
         {&cgb_tuning::pr_ctas_per_sm, {16, 32, 64, 128, 256, 1024}, false, false, false, true, false, false},
     };
+}
+
+// The batching autotuner's tiler: the reference's two-level partition
+// (my_project/CGgraph/Two-level_partition.cuh:213-342, cgb_graph_partition)
+// cuts the vertices into 1024-vertex segments and sorts them into four
+// buckets by average out-degree (up to 16, 32, 256, above).  The bucket that
+// holds the median edge sets the multi-root SSSP work tile (descriptor
+// length, ms_edges): lists in segments of degree above 256 are walked in
+// 1024-edge tiles, 33..256 in 256, 17..32 in 128, up to 16 in 64.  The
+// search then starts from the better of that tile and the graph's current
+// one.
+uint32_t tile_from_partition(cgb_graph* g)
+{
+    cgb_partition_info info{};
+    const uint32_t nseg = (uint32_t)(((uint64_t)g->nz + 1023) / 1024);
+    if (nseg == 0) return 0;
+    std::vector<uint32_t> order(nseg), edges(nseg);
+    const uint64_t roomy = ~0ull >> 2;  // one device that holds everything: the deal is irrelevant here
+    {
+        std::lock_guard<GraphMutex> lock(g->mu);
+        CGB_CUDA_TRY(cudaSetDevice(g->device));
+        graph_partition(g, CGB_SSSP, 1, &roomy, order.data(), edges.data(), nullptr, nullptr, &info);
+    }
+    uint64_t per_bucket[4] = {0, 0, 0, 0}, total = 0;
+    for (int b = 0; b < 4; b++)
+        for (uint32_t j = info.bucket_start[b]; j < info.bucket_start[b + 1]; j++) per_bucket[b] += edges[order[j]];
+    for (int b = 0; b < 4; b++) total += per_bucket[b];
+    const uint32_t tiles[4] = {64, 128, 256, 1024};
+    uint64_t acc = 0;
+    for (int b = 0; b < 4; b++) {
+        acc += per_bucket[b];
+        if (2 * acc >= total) return tiles[b];
+    }
+    return tiles[3];
 }
 
 }  // namespace
@@ -84,6 +123,9 @@ cgb_status cgb_tuning_set(cgb_graph* g, int algorithm, const cgb_tuning* t)
         set_error("cgb_tuning.struct_size too small");
         return CGB_EINVAL;
     }
+    cgb_tuning tv = *t;
+    if (tv.push_block == 0) tv.push_block = 256;
+    t = &tv;
     if (!valid(*t)) {
         set_error("cgb_tuning value out of range");
         return CGB_EINVAL;
@@ -150,6 +192,38 @@ cgb_status cgb_autotune(cgb_graph* g, int algorithm, const uint32_t* roots, uint
     if (st != CGB_OK) return st;
     const double first_ms = cur_ms;
     cgb_tuning cur = start;
+    if (batch && algorithm == CGB_SSSP) {
+        // the partition's degree buckets propose the starting tile
+        uint32_t tile = 0;
+        try {
+            tile = tile_from_partition(g);
+        } catch (const Error& e) {
+            set_error(e.msg);
+            return e.code;
+        }
+        if (tile && tile != cur.ms_edges) {
+            cgb_tuning cand = cur;
+            cand.ms_edges = tile;
+            if (valid(cand)) {
+                {
+                    std::lock_guard<GraphMutex> lock(g->mu);
+                    slot = cand;
+                }
+                double ms = 0;
+                st = score(ms);
+                std::lock_guard<GraphMutex> lock(g->mu);
+                if (st != CGB_OK) {
+                    slot = start;
+                    return st;
+                }
+                if (ms < cur_ms) {
+                    cur_ms = ms;
+                    cur = cand;
+                }
+                slot = cur;
+            }
+        }
+    }
     for (int sweep = 0; sweep < 2; sweep++) {
         bool moved = false;
         for (const Field& f : fields()) {

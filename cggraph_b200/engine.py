@@ -164,7 +164,7 @@ def chunglu_weight_offset(vertices: int, draws: int, max_degree: int) -> int:
 DEFAULT_TUNING = {"push_big_deg": 512, "push_chunk": 1024, "push_ctas_per_sm": 8, "persist_enter": 1 << 15,
                   "persist_deg": 2048, "ms_edges": 256, "pr_unroll": 16, "pr_ctas_per_sm": 128, "persist_ctas": 0,
                   "sssp_pull_alpha": 0, "cluster_enter": 8192,
-                  "sssp_dense_alpha": 4}
+                  "sssp_dense_alpha": 4, "push_block": 256}
 
 
 def _count(a) -> int:

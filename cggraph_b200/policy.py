@@ -1,12 +1,14 @@
 """The learned per-iteration scheduler: trace collection, GPU training,
 loading.
 
-The network (24 features -> 64 -> 64 -> 9 log-cost predictions, FP32) lives
+The network (24 features -> 64 -> 64 -> 14 log-cost predictions, FP32) lives
 in the engine; this module drives its C entry points (cgb_policy_*):
 
 * ``collect(graph, alg, root)`` -- counterfactual samples of one run: at each
-  BFS level both directions, at each SSSP bucket boundary all seven delta
-  multipliers (x 1/4 .. x 16), timed from the same snapshot;
+  BFS level the three variants (binned push, chunked push, bottom-up pull),
+  at each SSSP bucket boundary all seven delta multipliers (x 1/4 .. x 16),
+  at each large SSSP near round the four round variants (sparse frontier
+  binned or chunked, dense frontier, pull), timed from the same snapshot;
 * ``train(X, T, M)`` -- masked-MSE training on the GPU by the engine's own
   forward / backward / Adam kernels;
 * ``load(params)`` -- makes a network the policy of CGB_SCHED_LEARNED runs;
@@ -91,9 +93,16 @@ def load_default() -> bool:
     return True
 
 
+# output heads (include/cgb200.h)
+BFS_LEVEL = [0, 1, 9]            # binned push, pull, chunked push
+SSSP_DELTA = list(range(2, 9))   # x 1/4 .. x 16
+SSSP_ROUND = [10, 11, 12, 13]    # sparse binned, sparse chunked, dense, pull
+
+
 def decisions(params, X) -> dict:
-    """What the policy would choose for each sample: BFS direction (0 push,
-    1 pull) and SSSP delta index (0..6: x 1/4 .. x 16), before the confidence
-    margin."""
+    """What the policy would choose for each sample, before the confidence
+    margin: BFS level variant (0 push, 1 pull, 2 chunked push), SSSP delta
+    index (0..6: x 1/4 .. x 16), SSSP round variant (0..3)."""
     Y = forward(params, X)
-    return {"direction": np.argmin(Y[:, 0:2], axis=1), "delta": np.argmin(Y[:, 2:9], axis=1)}
+    return {"bfs_level": np.argmin(Y[:, BFS_LEVEL], axis=1), "delta": np.argmin(Y[:, SSSP_DELTA], axis=1),
+            "round": np.argmin(Y[:, SSSP_ROUND], axis=1)}

@@ -334,7 +334,10 @@ typedef struct {
     uint32_t sssp_dense_alpha; /* SSSP rounds use a dense frontier when the near set's out-edges times
                                   this times max(first touches per edge in the previous round, 1/8)
                                   exceed V (0 = never, default 4) */
-    uint32_t reserved[3];
+    uint32_t push_block;       /* threads per CTA of the push expansion kernels: 128, 256 or 512
+                                  (0 = 256, the default); the reference fixes 256 (BLOCKSIZE,
+                                  Basic/Graph/basic_def.hpp:8) */
+    uint32_t reserved[2];
 } cgb_tuning;
 
 cgb_status cgb_tuning_get(const cgb_graph* g, int algorithm, cgb_tuning* out);
@@ -407,6 +410,8 @@ typedef struct {
 
 #define CGB_SERVER_NO_BFS 0x1u  /* no BFS slots (saves their masks) */
 #define CGB_SERVER_NO_SSSP 0x2u /* no SSSP slots (saves the 256 B per vertex of distances) */
+#define CGB_SERVER_HOST_TICKS 0x4u /* advance every level from the host thread (one synchronisation per
+                                      level) instead of the device-resident level loop */
 
 typedef struct {
     uint64_t id;
@@ -467,26 +472,33 @@ cgb_status cgb_bfs_noalloc(const uint32_t* offsets, const uint32_t* dest, uint32
 
 /* The per-iteration scheduler (CGB_SCHED_LEARNED) is an FP32 MLP
  * CGB_POLICY_FEATURES -> 64 -> 64 -> CGB_POLICY_OUTPUTS whose outputs predict
- * the log-cost of each choice: [0] BFS next level pushed, [1] pulled,
- * [2..8] SSSP next bucket with delta x {1/4, 1/2, 1, 2, 4, 8, 16} (the cost of
- * a bucket phase divided by its width).
+ * the log-cost of each choice:
+ *   [0] BFS next level pushed (degree-binned expansion), [1] pulled
+ *       (bottom-up over a dense frontier bitmap), [9] pushed with every list
+ *       of 32 edges or more cut into chunks dealt across the grid;
+ *   [2..8] SSSP next bucket with delta x {1/4, 1/2, 1, 2, 4, 8, 16} (the cost
+ *       of a bucket phase divided by its width);
+ *   [10..13] SSSP next near round as a sparse frontier (queue) with the
+ *       degree-binned expansion, a sparse frontier with every list of 32
+ *       edges or more chunked, a dense frontier (relax, then scan all
+ *       vertices), or a pull over the in-edges.
  * Parameters are CGB_POLICY_PARAMS floats: W1[24][64] b1[64] W2[64][64]
- * b2[64] W3[64][9] b3[9] (row-major, input index first).  The reference has
- * no scheduler; these entry points have no counterpart in it. */
+ * b2[64] W3[64][14] b3[14] (row-major, input index first).  The reference
+ * has no scheduler; these entry points have no counterpart in it. */
 #define CGB_POLICY_FEATURES 24
-#define CGB_POLICY_OUTPUTS 9
-#define CGB_POLICY_PARAMS 6345
+#define CGB_POLICY_OUTPUTS 14
+#define CGB_POLICY_PARAMS 6670
 
 /* Makes `params` the policy of the current device (NULL unloads it: the
  * heuristic decides). */
 cgb_status cgb_policy_load(const float* params);
 
 /* Per-iteration training samples of one run: at every decision point the
- * engine snapshots its state, runs each choice (BFS: both directions; SSSP:
- * all seven deltas), times it with CUDA events, restores, and continues with
- * the fastest.  features: max * 24 floats;
- * targets: max * 9 log-costs; mask: max * 9 (1 where measured).  The run's
- * result equals a plain cgb_run. */
+ * engine snapshots its state, runs each choice (BFS level: the three
+ * variants; SSSP bucket: all seven deltas; SSSP near round: the four round
+ * variants), times it with CUDA events, restores, and continues with the
+ * fastest.  features: max * 24 floats; targets: max * 14 log-costs; mask:
+ * max * 14 (1 where measured).  The run's result equals a plain cgb_run. */
 cgb_status cgb_policy_collect(cgb_graph* g, int algorithm, uint32_t root, const cgb_options* opt, float* features,
                               float* targets, uint8_t* mask, uint32_t max, uint32_t* count);
 
@@ -505,6 +517,15 @@ cgb_status cgb_policy_loss_grad(const float* params, const float* features, cons
                                 const uint8_t* mask, uint32_t n, float* loss, float* grad);
 
 /* ---------------------------------------------------------------- misc */
+
+/* Self-check of the engine's device-side timeout path (no counterpart in
+ * the reference).  The device-resident loops separate their levels with a
+ * grid barrier whose wait is bounded: a CTA that polls it more than a limit
+ * sets a status flag and leaves, and the run returns CGB_ETIMEOUT instead of
+ * hanging.  This launches one such loop on `device` in which one CTA never
+ * arrives, with the given limit (1 .. 2^24 polls), and returns CGB_ETIMEOUT
+ * when the others gave up as they should (the context stays usable). */
+cgb_status cgb_check_barrier_timeout(int device, uint32_t spin_limit);
 
 const char* cgb_last_error_string(void);
 const char* cgb_status_string(cgb_status s);

@@ -1,7 +1,7 @@
 """FP64 CPU restatement of the scheduler network (TEST INFRASTRUCTURE ONLY).
 
 Same layout as the engine (include/cgb200.h, CGB_POLICY_PARAMS):
-W1[24][64] b1[64] W2[64][64] b2[64] W3[64][9] b3[9], ReLU after the two
+W1[24][64] b1[64] W2[64][64] b2[64] W3[64][14] b3[14], ReLU after the two
 hidden layers, loss = sum(mask * (Y - T)^2) / sum(mask).  Used to check the
 GPU forward pass and the GPU gradient, and checked itself by central finite
 differences.
@@ -10,7 +10,7 @@ from __future__ import annotations
 
 import numpy as np
 
-F, H, O = 24, 64, 9
+F, H, O = 24, 64, 14
 SIZES = [("W1", (F, H)), ("b1", (H,)), ("W2", (H, H)), ("b2", (H,)), ("W3", (H, O)), ("b3", (O,))]
 NPARAMS = sum(int(np.prod(s)) for _, s in SIZES)
 

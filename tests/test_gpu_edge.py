@@ -483,3 +483,22 @@ def test_two_level_partition(oracle):
                         np.testing.assert_array_equal(got[k], exp[k], err_msg=f"{k} {alg} {mem}")
             got = g.partition(BFS, 1)  # the device's own memory: everything fits
             assert got["can_hold_all"] and np.all(got["seg_owner"] == 0)
+
+
+def test_device_barrier_gives_up_and_context_survives(oracle):
+    """The device-resident loops' grid barrier waits a bounded number of
+    polls.  cgb_check_barrier_timeout runs such a loop in which one CTA never
+    arrives: the others give up after the limit, the call reports
+    CGB_ETIMEOUT, and a normal run right after still works."""
+    import ctypes
+    lib = L.lib()
+    f = lib.cgb_check_barrier_timeout
+    f.argtypes = [ctypes.c_int, ctypes.c_uint32]
+    f.restype = ctypes.c_int
+    assert f(0, 1 << 12) == L.ETIMEOUT
+    assert f(0, 0) == L.EINVAL
+    off, dst, w = oracle.rmat_graph(10, 8, seed=3)
+    root = int(np.diff(off.astype(np.int64)).argmax())
+    with cg.Graph.from_csr(off, dst, w) as g:
+        np.testing.assert_array_equal(g.run(BFS, root)[0], oracle.bfs(off, dst, root))
+        np.testing.assert_array_equal(g.run(SSSP, root)[0], oracle.sssp(off, dst, w, root))

@@ -16,12 +16,15 @@ pytestmark = pytest.mark.gpu
 BFS, SSSP = 0, 1
 
 
+NO = L.POLICY_OUTPUTS
+
+
 def _batch(seed=0, n=300):
     rng = np.random.default_rng(seed)
     p = rng.normal(0, 0.15, MO.NPARAMS).astype(np.float32)
     X = rng.random((n, 24)).astype(np.float32)
-    T = rng.normal(0, 1, (n, 9)).astype(np.float32)
-    M = (rng.random((n, 9)) < 0.4).astype(np.uint8)
+    T = rng.normal(0, 1, (n, NO)).astype(np.float32)
+    M = (rng.random((n, NO)) < 0.4).astype(np.uint8)
     return p, X, T, M
 
 
@@ -48,10 +51,10 @@ def test_gpu_gradient_matches_cpu_oracle():
 def test_gpu_training_fits_a_known_function():
     rng = np.random.default_rng(3)
     X = rng.random((2000, 24)).astype(np.float32)
-    T = np.zeros((2000, 9), np.float32)
+    T = np.zeros((2000, NO), np.float32)
     T[:, 0] = X[:, 0] * 2 - X[:, 1]
     T[:, 1] = np.sin(3 * X[:, 2])
-    M = np.zeros((2000, 9), np.uint8)
+    M = np.zeros((2000, NO), np.uint8)
     M[:, :2] = 1
     p, loss = policy.train(X, T, M, epochs=200, batch=128, lr=3e-3, seed=1)
     assert loss < 0.01, loss
@@ -60,16 +63,25 @@ def test_gpu_training_fits_a_known_function():
 
 
 def test_collect_samples_and_unchanged_results(oracle):
-    off, dst, w = oracle.rmat_graph(14, 16, seed=9)
+    """BFS samples time the three level variants; SSSP samples are either a
+    bucket boundary (the seven deltas) or a large near round (the four round
+    variants); collecting leaves the results exact."""
+    off, dst, w = oracle.rmat_graph(16, 16, seed=9)
     root = int(np.diff(off.astype(np.int64)).argmax())
     with cg.Graph.from_csr(off, dst, w) as g:
         X, T, M = policy.collect(g, BFS, root)
-        assert len(X) >= 3 and np.all(M[:, 0:2] == 1) and np.all(M[:, 2:] == 0)
+        level = policy.BFS_LEVEL
+        assert len(X) >= 3 and np.all(M[:, level] == 1)
+        assert np.all(np.delete(M, level, axis=1) == 0)
         np.testing.assert_array_equal(g.run(BFS, root)[0], oracle.bfs(off, dst, root))
         X2, T2, M2 = policy.collect(g, SSSP, root)
-        assert len(X2) >= 1 and np.all(M2[:, 2:9] == 1)
+        bucket = np.all(M2[:, policy.SSSP_DELTA] == 1, axis=1)
+        rnd = np.all(M2[:, policy.SSSP_ROUND] == 1, axis=1)
+        assert bucket.any() and rnd.any()
+        assert np.all(bucket ^ rnd)
+        assert np.all(M2[:, level] == 0)
         np.testing.assert_array_equal(g.run(SSSP, root)[0], oracle.sssp(off, dst, w, root))
-        assert np.all(np.isfinite(X)) and np.all(np.isfinite(T))
+        assert np.all(np.isfinite(X)) and np.all(np.isfinite(T)) and np.all(np.isfinite(T2))
 
 
 def test_learned_schedule_gives_identical_results(oracle):

@@ -40,9 +40,12 @@ def _serve_and_check(g, queries, arrivals, **cfg):
     return recs, st
 
 
-def test_server_mix_equals_lone_runs(oracle):
+@pytest.mark.parametrize("flags", [0, L.SERVER_HOST_TICKS])
+def test_server_mix_equals_lone_runs(oracle, flags):
     """RMAT-14 (weights 1..64): 120 BFS/SSSP queries with Poisson arrivals,
-    8 slots per algorithm so that slots are reused while other queries run."""
+    8 slots per algorithm so that slots are reused while other queries run;
+    BFS levels in the device-resident loop (default) or one host tick per
+    level."""
     off, dst, w = oracle.rmat_graph(14, 16, seed=31)
     rng = np.random.default_rng(4)
     V = off.size - 1
@@ -52,15 +55,17 @@ def test_server_mix_equals_lone_runs(oracle):
     arrivals = _poisson_arrivals(len(queries), 20000, 9)
     with cg.Graph.from_csr(off, dst, w) as g:
         g._host_off = off
-        recs, st = _serve_and_check(g, queries, arrivals, bfs_slots=8, sssp_slots=8)
+        recs, st = _serve_and_check(g, queries, arrivals, bfs_slots=8, sssp_slots=8, flags=flags)
         assert st["bfs_slots"] == 8 and st["sssp_slots"] == 8
         # slots were reused: more queries than slots per algorithm
         assert max(r["slot"] for r in recs.values()) < 8
 
 
-def test_server_high_diameter_grid(oracle):
+@pytest.mark.parametrize("flags", [0, L.SERVER_HOST_TICKS])
+def test_server_high_diameter_grid(oracle, flags):
     """A grid keeps SSSP queries alive for hundreds of rounds while short
-    BFS queries come and go; per-slot buckets keep late arrivals exact."""
+    BFS queries come and go; per-slot buckets keep late arrivals exact; BFS
+    levels run many per launch in the device-resident loop (default)."""
     off, dst, w = oracle.grid_graph(40, 60, seed=5)
     rng = np.random.default_rng(2)
     V = off.size - 1
@@ -68,7 +73,7 @@ def test_server_high_diameter_grid(oracle):
     arrivals = _poisson_arrivals(len(queries), 5000, 3)
     with cg.Graph.from_csr(off, dst, w) as g:
         g._host_off = off
-        _serve_and_check(g, queries, arrivals, bfs_slots=4, sssp_slots=4, sssp_delta=300)
+        _serve_and_check(g, queries, arrivals, bfs_slots=4, sssp_slots=4, sssp_delta=300, flags=flags)
 
 
 def test_server_memory_budget_caps_slots(oracle):

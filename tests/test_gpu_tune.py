@@ -24,6 +24,8 @@ TUNINGS = [
     {"sssp_dense_alpha": 1000},
     {"sssp_dense_alpha": 0, "sssp_pull_alpha": 0},
     {"cluster_enter": 1 << 20},
+    {"push_block": 128},
+    {"push_block": 512, "push_ctas_per_sm": 2},
 ]
 
 
@@ -79,7 +81,8 @@ def test_autotune_and_range_checks(oracle):
         best_pr, pms, psms = g.autotune(PR, [5, 5])
         assert pms <= psms and g.get_tuning(PR) == best_pr
         for bad in ({"push_big_deg": 64}, {"push_chunk": 1000}, {"push_ctas_per_sm": 0}, {"ms_edges": 8192},
-                    {"persist_deg": 1}, {"pr_unroll": 6}, {"pr_ctas_per_sm": 1025}):
+                    {"persist_deg": 1}, {"pr_unroll": 6}, {"pr_ctas_per_sm": 1025}, {"push_block": 300},
+                    {"push_block": 1024}):
             with pytest.raises(cg.CgbError):
                 g.set_tuning(bad, SSSP)
         assert g.get_tuning(SSSP) == best
