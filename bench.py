@@ -65,9 +65,9 @@ def parse_args():
     p.add_argument("--no-batching", action="store_true", help="skip the multi-root and graph-batch section")
     p.add_argument("--no-serving", action="store_true", help="skip the request-server section")
     p.add_argument("--no-shapes", action="store_true",
-                   help="skip the skewed / high-diameter shapes (Chung-Lu 41.6 M / 1.47 B, 4800 x 5000 grid)")
+                   help="skip the skewed / high-diameter shapes (Chung-Lu 41.6 M vertices / 1.47 B edges, 4800 x 5000 grid)")
     p.add_argument("--shapes-scale", type=float, default=1.0,
-                   help="fraction of the Chung-Lu vertices and draws (1.0 = 41.6 M / 1.47 B)")
+                   help="fraction of the Chung-Lu vertices and edges (1.0 = 41.6 M / 1.47 B)")
     p.add_argument("--serve-scale", type=int, default=25, help="RMAT scale of the served graph")
     p.add_argument("--serve-requests", type=int, default=256, help="queries per arrival rate")
     p.add_argument("--algorithms", default="bfs,sssp,cc,pr",
@@ -436,6 +436,19 @@ def compare_schedules(args, cg, L, gd, roots, dev):
                 res[an] = {"heuristic_ms": t["heuristic"], "learned_ms": t["learned"],
                            "heuristic_gteps": edges / t["heuristic"] / 1e6, "learned_gteps": edges / t["learned"] / 1e6,
                            "learned_speedup": t["heuristic"] / t["learned"]}
+            # the best fixed delta: the heuristic schedule with the default delta
+            # scaled by 1/4 ... 16 (the learned schedule's own choices per bucket)
+            _, st0 = _best_of(g, SSSP, rts[0], cg.make_options(schedule=L.SCHED_HEURISTIC), reps=1)
+            base = st0.sssp_delta
+            sweep = {}
+            for sc in (0.25, 0.5, 1, 2, 4, 8, 16):
+                dk = max(1, int(base * sc))
+                sweep[str(sc)] = sum(_best_of(g, SSSP, r, cg.make_options(schedule=L.SCHED_HEURISTIC,
+                                                                            sssp_delta=dk))[0] for r in rts)
+            best = min(sweep, key=sweep.get)
+            res["sssp"].update({"default_delta": base, "fixed_delta_ms": sweep, "best_fixed_scale": float(best),
+                                "best_fixed_ms": sweep[best],
+                                "learned_vs_best_fixed": sweep[best] / t_sssp if (t_sssp := res["sssp"]["learned_ms"]) else None})
             out[name] = res
             if own:
                 g.close()
@@ -511,8 +524,9 @@ def bench_batching(args, cg, L, gd, roots, dev):
 def bench_shapes(args, cg, L, dev):
     """Skewed and high-diameter shapes, all four algorithms under the plain
     heuristic schedule: a Chung-Lu power-law directed graph of 41.6 M
-    vertices and 1.47 B edge draws (degree-distribution exponent 2, largest
-    expected degree about 3 M, weights [1,64]; its symmetrised copy for CC),
+    vertices and about 1.47 B distinct edges (about 1.96 B draws before
+    duplicates are removed; degree-distribution exponent 2, largest
+    out-degree about 3 M, weights [1,64]; its symmetrised copy for CC),
     and the 4800 x 5000 grid (weights [1,1000]).  One untimed run, then the
     best of two; GTEPS numerators as in the main line."""
     out = {}
@@ -526,8 +540,8 @@ def bench_shapes(args, cg, L, dev):
         return min(ms), g.stats().traversed_edges
 
     Vc = int(41_600_000 * args.shapes_scale)
-    draws = int(1_470_000_000 * args.shapes_scale)
-    i0 = cg.chunglu_weight_offset(Vc, draws, int(3_000_000 * args.shapes_scale) or 1)
+    draws, i0 = cg.chunglu_draws_for_edges(Vc, int(1_470_000_000 * args.shapes_scale),
+                                           int(3_000_000 * args.shapes_scale) or 1)
     t0 = time.perf_counter()
     g = cg.Graph.chunglu(Vc, draws, i0, seed=args.seed, wmax=64, device=dev)
     gen_s = time.perf_counter() - t0

@@ -18,6 +18,8 @@ from .engine import (  # noqa: F401
     Server,
     VertexValue_MAX,
     checkBinResult,
+    chunglu_draws_for_edges,
+    chunglu_expected_edges,
     chunglu_weight_offset,
     load_binFile,
     main_partition,

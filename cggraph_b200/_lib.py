@@ -144,7 +144,7 @@ class ServerConfig(ctypes.Structure):
     ]
 
 
-SERVER_NO_BFS, SERVER_NO_SSSP, SERVER_HOST_TICKS = 0x1, 0x2, 0x4
+SERVER_NO_BFS, SERVER_NO_SSSP, SERVER_HOST_TICKS, SERVER_BATCH_ONLY = 0x1, 0x2, 0x4, 0x8
 
 
 class RequestInfo(ctypes.Structure):

@@ -286,7 +286,11 @@ cgb_status cgb_graph_result_download(const cgb_graph* g, void* values)
     });
 }
 
-static void run_one(cgb_graph* g, int alg, uint32_t root_or_iters, const cgb_options& o)
+}  // extern "C"
+
+// One run of the single-root engine; the caller holds the graph's lock.
+namespace cgb {
+void run_one(cgb_graph* g, int alg, uint32_t root_or_iters, const cgb_options& o)
 {
     g->tune = g->tune_alg[alg];
     g->stats = cgb_run_stats{};
@@ -333,6 +337,9 @@ static void run_one(cgb_graph* g, int alg, uint32_t root_or_iters, const cgb_opt
     if (alg != CGB_PR) g->result = g->value;
     g->result_alg = alg;
 }
+}  // namespace cgb
+
+extern "C" {
 
 cgb_status cgb_run(cgb_graph* g, int algorithm, uint32_t root_or_iters, const cgb_options* opt, uint32_t* out_u32,
                    double* out_f64, double* out_ms)
@@ -484,6 +491,7 @@ cgb_status cgb_policy_collect(cgb_graph* g, int algorithm, uint32_t root, const 
         CGB_CUDA_TRY(cudaMalloc((void**)&ps.save_bm0, (size_t)g->words() * 4));
         CGB_CUDA_TRY(cudaMalloc((void**)&ps.save_q, (size_t)g->V * 4));
         CGB_CUDA_TRY(cudaMalloc((void**)&ps.save_ctr, sizeof(DevCounters)));
+        CGB_CUDA_TRY(cudaMalloc((void**)&ps.settled, sizeof(unsigned long long)));
         g->collect = &ps;
         try {
             run_one(g, algorithm, root, o);
@@ -497,6 +505,7 @@ cgb_status cgb_policy_collect(cgb_graph* g, int algorithm, uint32_t root, const 
     if (ps.save_bm0) cudaFree(ps.save_bm0);
     if (ps.save_q) cudaFree(ps.save_q);
     if (ps.save_ctr) cudaFree(ps.save_ctr);
+    if (ps.settled) cudaFree(ps.settled);
     if (count) *count = ps.count;
     return st;
 }

@@ -39,6 +39,9 @@
 
 namespace cgb {
 
+// One run of the single-root engine (capi.cu), with the graph's lock held.
+void run_one(cgb_graph* g, int alg, uint32_t root_or_iters, const cgb_options& o);
+
 constexpr uint32_t kSrvSlots = 64;
 
 // ---------------------------------------------------------------- kernels
@@ -606,6 +609,8 @@ struct cgb_server {
     Clock::time_point t0;
     uint64_t ticks[2] = {0, 0}, completed = 0;
     double busy_ms[2] = {0, 0};
+    double lone_est_us[2] = {0, 0};  // running mean of single-root run times (service estimate)
+    uint64_t lone_runs[2] = {0, 0};
     cgb_status error = CGB_OK;
     std::string error_msg;
 };
@@ -1048,20 +1053,22 @@ static unsigned long long group_finished(cgb_server* s, Group& G)
 }
 
 // Results of the finished slots: statistics, copy to the request's buffer.
-static void group_retire(cgb_server* s, Group& G, unsigned long long fin)
+// `lone`: slots whose result region already holds a single-root run's result.
+static void group_retire(cgb_server* s, Group& G, unsigned long long fin, unsigned long long lone = 0)
 {
     if (!fin) return;
     cgb_graph* g = s->g;
     const uint32_t V = g->V;
     cudaStream_t st = G.stream;
-    if (G.alg == CGB_SSSP) {
-        if (__builtin_popcountll(fin) <= 4) {
+    const unsigned long long ext = fin & ~lone;
+    if (G.alg == CGB_SSSP && ext) {
+        if (__builtin_popcountll(ext) <= 4) {
             uint32_t k[4] = {0, 0, 0, 0}, n = 0;
-            for (unsigned long long m = fin; m; m &= m - 1) k[n++] = __builtin_ctzll(m);
+            for (unsigned long long m = ext; m; m &= m - 1) k[n++] = __builtin_ctzll(m);
             k_srv_sp_extract_cols<<<num_sms() * 8, kBlock, 0, st>>>(G.sp->dist, V, make_uint4(k[0], k[1], k[2], k[3]), n,
                                                                   G.region);
         } else {
-            k_srv_sp_extract<<<num_sms() * 8, kBlock, 0, st>>>(G.sp->dist, V, fin, G.region);
+            k_srv_sp_extract<<<num_sms() * 8, kBlock, 0, st>>>(G.sp->dist, V, ext, G.region);
         }
     }
     CGB_CUDA_TRY(cudaMemsetAsync(G.d_stats, 0, offsetof(SlotStats, alive), st));
@@ -1091,6 +1098,36 @@ static void group_retire(cgb_server* s, Group& G, unsigned long long fin)
     }
     G.active &= ~fin;
     s->cv.notify_all();
+}
+
+// A query that finds its group idle runs on the single-root engine (the
+// latency of a lone cgb_run) when no other query of its algorithm is due
+// before that run would end, by the running mean of such runs; queries that
+// arrive meanwhile wait for it, then are batched.  Its result region gets the
+// engine's result, and the slot retires as a batched one does.
+static void lone_run(cgb_server* s, Group& G, int a, uint32_t k)
+{
+    cgb_graph* g = s->g;
+    const auto t0 = Clock::now();
+    {
+        std::lock_guard<GraphMutex> glk(g->mu);
+        // the engine's device-resident loops are cooperative launches, as the groups' are
+        std::lock_guard<std::mutex> coop(s->coop_mu);
+        cgb_options o;
+        memset(&o, 0, sizeof(o));
+        o.struct_size = sizeof(o);
+        run_one(g, G.alg, G.root[k], o);
+        CGB_CUDA_TRY(cudaMemcpyAsync(G.region + (size_t)k * g->V, g->value, (size_t)g->V * 4,
+                                     cudaMemcpyDeviceToDevice, g->stream));
+        CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    }
+    const double us = std::chrono::duration<double, std::micro>(Clock::now() - t0).count();
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        const uint64_t n = ++s->lone_runs[a];
+        s->lone_est_us[a] += (us - s->lone_est_us[a]) / (double)std::min<uint64_t>(n, 8);
+    }
+    group_retire(s, G, 1ull << k, 1ull << k);
 }
 
 // Pairs free slots with requests whose arrival time has passed.
@@ -1124,6 +1161,7 @@ static void group_loop(cgb_server* s, int a)
 {
     cgb_graph* g = s->g;
     Group& G = s->grp[a];
+    int lone_k = -1;  // slot admitted this tick for the single-root engine
     try {
         CGB_CUDA_TRY(cudaSetDevice(g->device));
         while (!s->stop.load()) {
@@ -1131,7 +1169,14 @@ static void group_loop(cgb_server* s, int a)
                 std::unique_lock<std::mutex> lk(s->mu);
                 if (s->error != CGB_OK) break;
                 const double now = us_since(s, Clock::now());
+                const bool idle = G.active == 0;
                 pick_admissions(s, G, s->waiting[a], now);
+                if (idle && G.admit.size() == 1 && !(s->flags & CGB_SERVER_BATCH_ONLY) &&
+                    (s->waiting[a].empty() ||
+                     s->reqs[s->waiting[a].front()].info.arrival_us > now + s->lone_est_us[a])) {
+                    lone_k = (int)G.admit[0];
+                    G.admit.clear();
+                }
                 if (!G.active) {
                     if (s->waiting[a].empty()) {
                         s->cv.wait_for(lk, std::chrono::milliseconds(5));
@@ -1144,7 +1189,10 @@ static void group_loop(cgb_server* s, int a)
             }
             const auto t_tick = Clock::now();
             unsigned long long fin;
-            if (a == 0) {
+            if (lone_k >= 0) {
+                lone_run(s, G, a, (uint32_t)lone_k);
+                lone_k = -1;
+            } else if (a == 0) {
                 std::lock_guard<GraphMutex> glk(g->mu);
                 g->tune = g->tune_alg[CGB_BFS];
                 bfs_admit(s, G);

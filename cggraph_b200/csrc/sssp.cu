@@ -297,6 +297,17 @@ __global__ void k_sssp_round_reset(DevCounters* ctr, int out, uint32_t* bm, uint
         for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < words; i += gridDim.x * blockDim.x) bm[i] = 0;
 }
 
+// Vertices whose distance is below thr (trace collection only).
+__global__ void k_sssp_count_below(uint32_t V, const uint32_t* __restrict__ value, uint32_t thr,
+                                   unsigned long long* out)
+{
+    uint32_t c = 0;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x)
+        c += value[v] < thr ? 1u : 0u;
+    c = warp_sum(c);
+    if (lane_id() == 0 && c) atomicAdd(out, (unsigned long long)c);
+}
+
 // The same before a bucket split: next queue, far count, smallest far distance.
 __global__ void k_sssp_split_reset(DevCounters* ctr, int out)
 {
@@ -671,6 +682,17 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
         return in;
     };
 
+    // vertices with a distance below t: after a bucket phase, the settled ones
+    auto settled_below = [&](uint64_t t) {
+        CGB_CUDA_TRY(cudaMemsetAsync(collect->settled, 0, sizeof(unsigned long long), g->stream));
+        k_sssp_count_below<<<num_sms() * 4, kBlock, 0, g->stream>>>(
+            V, g->value, (uint32_t)std::min<uint64_t>(t, kValueMax), collect->settled);
+        unsigned long long n = 0;
+        CGB_CUDA_TRY(cudaMemcpyAsync(&n, collect->settled, sizeof(n), cudaMemcpyDeviceToHost, g->stream));
+        CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        return (uint64_t)n;
+    };
+
     near_rounds();
     while (nfar > 0) {
         uint32_t d = delta;
@@ -684,6 +706,7 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
             float ms[kPolicyOutputs] = {};
             bool have[kPolicyOutputs] = {};
             int best = kDeltaUnit;
+            const uint64_t s_settled = settled_below(s_thr);
             in_delta_trial = true;
             for (int k = 0; k < kNumDeltaChoices; k++) {
                 const uint32_t dk = std::max<uint32_t>(1u, (uint32_t)(base_delta * delta_scale(k)));
@@ -694,8 +717,11 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
                 CGB_CUDA_TRY(cudaEventSynchronize(g->ev_iter[1]));
                 float t = 0.f;
                 CGB_CUDA_TRY(cudaEventElapsedTime(&t, g->ev_iter[0], g->ev_iter[1]));
-                // cost per unit of distance the phase covers (delta x scale)
-                ms[kOutDelta0 + k] = t / delta_scale(k);
+                // the phase's cost per vertex it settles, as the time to settle
+                // all V at that rate (wide buckets cover more distance, but on
+                // skewed graphs most of it holds few vertices)
+                const uint64_t gained = settled_below(thr) - s_settled;
+                ms[kOutDelta0 + k] = t * (float)((double)V / (double)std::max<uint64_t>(gained, 1));
                 have[kOutDelta0 + k] = true;
                 if (ms[kOutDelta0 + k] < ms[kOutDelta0 + best]) best = k;
                 CGB_CUDA_TRY(cudaMemcpyAsync(g->value, collect->save_value, vbytes, cudaMemcpyDeviceToDevice,

@@ -161,6 +161,44 @@ def chunglu_weight_offset(vertices: int, draws: int, max_degree: int) -> int:
     return lo if abs(distinct(lo) - max_degree) < abs(distinct(hi) - max_degree) else hi
 
 
+def chunglu_expected_edges(vertices: int, draws: int, weight_offset: int) -> float:
+    """Expected distinct edges of cgb_gen_chunglu.  Source and target ranks
+    are drawn independently with p_j proportional to 1 / (j + i0), so pair
+    (x, y) is present with probability 1 - exp(-draws * p_x * p_y); summed
+    over rank bins (the first 4096 ranks one by one, then 1000 geometric
+    bins).  Self-loops, which the builder drops, are a negligible share."""
+    lead = min(4096, vertices)
+    edges = np.unique(np.concatenate([np.arange(lead),
+                                      np.geomspace(max(lead, 1), vertices, 1000).astype(np.int64),
+                                      [vertices]]))
+    mid = (edges[:-1] + edges[1:] - 1) / 2.0
+    width = np.diff(edges).astype(np.float64)
+    p = 1.0 / (mid + weight_offset)
+    p /= float(np.sum(width * p))
+    s = 0.0
+    for k in range(0, len(p), 1024):
+        s += float(np.sum(width[k:k + 1024, None] * width[None, :]
+                          * -np.expm1(-float(draws) * p[k:k + 1024, None] * p[None, :])))
+    return s
+
+
+def chunglu_draws_for_edges(vertices: int, edges: int, max_degree: int) -> tuple:
+    """(draws, weight offset) of a Chung-Lu graph with about `edges`
+    distinct edges whose top vertex has about max_degree out-neighbours:
+    bisection on the draw count, the offset re-fitted at each step
+    (duplicates grow with the draws, so more draws than edges are needed)."""
+    lo, hi = int(edges), int(edges)
+    while chunglu_expected_edges(vertices, hi, chunglu_weight_offset(vertices, hi, max_degree)) < edges:
+        lo, hi = hi, hi * 2
+    while hi - lo > max(1, edges // 2000):
+        m = (lo + hi) // 2
+        if chunglu_expected_edges(vertices, m, chunglu_weight_offset(vertices, m, max_degree)) < edges:
+            lo = m
+        else:
+            hi = m
+    return hi, chunglu_weight_offset(vertices, hi, max_degree)
+
+
 DEFAULT_TUNING = {"push_big_deg": 512, "push_chunk": 1024, "push_ctas_per_sm": 8, "persist_enter": 1 << 15,
                   "persist_deg": 2048, "ms_edges": 256, "pr_unroll": 16, "pr_ctas_per_sm": 128, "persist_ctas": 0,
                   "sssp_pull_alpha": 0, "cluster_enter": 8192,

@@ -173,8 +173,8 @@ def test_grid4800x5000(oracle):
 
 
 def test_chunglu_tenth_of_bench_shape(oracle):
-    Vc, draws = 4_160_000, 147_000_000
-    i0 = cg.chunglu_weight_offset(Vc, draws, 300_000)
+    Vc = 4_160_000
+    draws, i0 = cg.chunglu_draws_for_edges(Vc, 147_000_000, 300_000)
     with cg.Graph.chunglu(Vc, draws, i0, seed=1) as g:
         off, dst, w = g.download()
         deg = np.diff(off.astype(np.int64))

@@ -40,12 +40,13 @@ def _serve_and_check(g, queries, arrivals, **cfg):
     return recs, st
 
 
-@pytest.mark.parametrize("flags", [0, L.SERVER_HOST_TICKS])
+@pytest.mark.parametrize("flags", [0, L.SERVER_HOST_TICKS, L.SERVER_BATCH_ONLY])
 def test_server_mix_equals_lone_runs(oracle, flags):
     """RMAT-14 (weights 1..64): 120 BFS/SSSP queries with Poisson arrivals,
     8 slots per algorithm so that slots are reused while other queries run;
     BFS levels in the device-resident loop (default) or one host tick per
-    level."""
+    level; queries that find their group idle on the single-root engine
+    (default) or batched like the rest."""
     off, dst, w = oracle.rmat_graph(14, 16, seed=31)
     rng = np.random.default_rng(4)
     V = off.size - 1
@@ -61,7 +62,7 @@ def test_server_mix_equals_lone_runs(oracle, flags):
         assert max(r["slot"] for r in recs.values()) < 8
 
 
-@pytest.mark.parametrize("flags", [0, L.SERVER_HOST_TICKS])
+@pytest.mark.parametrize("flags", [0, L.SERVER_HOST_TICKS, L.SERVER_BATCH_ONLY])
 def test_server_high_diameter_grid(oracle, flags):
     """A grid keeps SSSP queries alive for hundreds of rounds while short
     BFS queries come and go; per-slot buckets keep late arrivals exact; BFS
@@ -74,6 +75,24 @@ def test_server_high_diameter_grid(oracle, flags):
     with cg.Graph.from_csr(off, dst, w) as g:
         g._host_off = off
         _serve_and_check(g, queries, arrivals, bfs_slots=4, sssp_slots=4, sssp_delta=300, flags=flags)
+
+
+def test_server_sparse_arrivals_run_alone(oracle):
+    """Below capacity (20 req/s against queries of well under a
+    millisecond) each query finds its group idle and runs on the
+    single-root engine: results exact, and each query's latency close to
+    a lone run's (admitted on arrival, done within 50 ms)."""
+    off, dst, w = oracle.rmat_graph(14, 16, seed=7)
+    rng = np.random.default_rng(8)
+    V = off.size - 1
+    queries = [(int(rng.integers(0, 2)), int(rng.integers(0, V))) for _ in range(12)]
+    arrivals = 50000.0 * np.arange(1, len(queries) + 1)
+    with cg.Graph.from_csr(off, dst, w) as g:
+        g._host_off = off
+        recs, _ = _serve_and_check(g, queries, arrivals)
+        for r in recs.values():
+            assert r["admit_us"] - r["arrival_us"] < 10000
+            assert r["done_us"] - r["arrival_us"] < 50000
 
 
 def test_server_memory_budget_caps_slots(oracle):

@@ -68,6 +68,22 @@ def test_chunglu_weight_offset_matches_twin(oracle):
     assert cg.chunglu_weight_offset(V, n, 100) > cg.chunglu_weight_offset(V, n, 3000)
 
 
+def test_chunglu_draws_for_edges_matches_twin(oracle):
+    """The draw-count solver: the CPU twin, given the solved draws and
+    offset, keeps the requested number of distinct edges (to 1 %), and the
+    expected-edge estimate tracks the twin's count at another draw count."""
+    import numpy as np
+    import cggraph_b200 as cg
+    V, want = 200003, 3_000_000
+    draws, i0 = cg.chunglu_draws_for_edges(V, want, 20000)
+    assert draws > want
+    off, _, _ = oracle.chunglu_graph(V, draws, i0, seed=5)
+    assert abs(int(off[-1]) - want) < 0.01 * want
+    off, _, _ = oracle.chunglu_graph(V, want, 7, seed=6)
+    est = cg.chunglu_expected_edges(V, want, 7)
+    assert abs(int(off[-1]) - est) < 0.01 * est
+
+
 def test_reorder_engine_type_writes_the_reference_files(tmp_path, monkeypatch):
     """main_partition(Engine_type.REORDER) is the reference's preprocessing
     branch (main_partition.hpp:466-487): the IN_DEGREE_DEC relabelling, written
