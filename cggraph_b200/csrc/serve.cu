@@ -609,8 +609,9 @@ struct cgb_server {
     Clock::time_point t0;
     uint64_t ticks[2] = {0, 0}, completed = 0;
     double busy_ms[2] = {0, 0};
-    double lone_est_us[2] = {0, 0};  // running mean of single-root run times (service estimate)
-    uint64_t lone_runs[2] = {0, 0};
+    double lone_est_us[2] = {0, 0};   // running mean of single-root run times
+    double batch_est_us[2] = {0, 0};  // running mean of batched queries' admission-to-result times
+    uint64_t lone_runs[2] = {0, 0}, batch_runs[2] = {0, 0};
     cgb_status error = CGB_OK;
     std::string error_msg;
 };
@@ -1091,6 +1092,11 @@ static void group_retire(cgb_server* s, Group& G, unsigned long long fin, unsign
         R.info.depth = G.h_stats->depth[k];
         R.info.done_us = now;
         R.info.status = CGB_OK;
+        if (!((lone >> k) & 1ull)) {
+            const uint64_t n = ++s->batch_runs[G.alg == CGB_BFS ? 0 : 1];
+            double& e = s->batch_est_us[G.alg == CGB_BFS ? 0 : 1];
+            e += (now - R.info.admit_us - e) / (double)std::min<uint64_t>(n, 16);
+        }
         s->done.push_back(R.info);
         s->completed++;
         G.state[k] = SlotState::kFree;
@@ -1100,11 +1106,9 @@ static void group_retire(cgb_server* s, Group& G, unsigned long long fin, unsign
     s->cv.notify_all();
 }
 
-// A query that finds its group idle runs on the single-root engine (the
-// latency of a lone cgb_run) when no other query of its algorithm is due
-// before that run would end, by the running mean of such runs; queries that
-// arrive meanwhile wait for it, then are batched.  Its result region gets the
-// engine's result, and the slot retires as a batched one does.
+// A query served alone on the single-root engine (the latency of a lone
+// cgb_run).  Its result region gets the engine's result, and the slot
+// retires as a batched one does.
 static void lone_run(cgb_server* s, Group& G, int a, uint32_t k)
 {
     cgb_graph* g = s->g;
@@ -1131,11 +1135,11 @@ static void lone_run(cgb_server* s, Group& G, int a, uint32_t k)
 }
 
 // Pairs free slots with requests whose arrival time has passed.
-static void pick_admissions(cgb_server* s, Group& G, std::deque<int64_t>& waiting, double now_us)
+static void pick_admissions(cgb_server* s, Group& G, std::deque<int64_t>& waiting, double now_us, uint32_t max_n)
 {
     G.admit.clear();
     uint32_t k = 0;
-    while (!waiting.empty()) {
+    while (!waiting.empty() && G.admit.size() < max_n) {
         SrvReq& R = s->reqs[waiting.front()];
         if (R.info.arrival_us > now_us) break;
         while (k < G.nslots && G.state[k] != SlotState::kFree) k++;
@@ -1169,11 +1173,21 @@ static void group_loop(cgb_server* s, int a)
                 std::unique_lock<std::mutex> lk(s->mu);
                 if (s->error != CGB_OK) break;
                 const double now = us_since(s, Clock::now());
-                const bool idle = G.active == 0;
-                pick_admissions(s, G, s->waiting[a], now);
-                if (idle && G.admit.size() == 1 && !(s->flags & CGB_SERVER_BATCH_ONLY) &&
-                    (s->waiting[a].empty() ||
-                     s->reqs[s->waiting[a].front()].info.arrival_us > now + s->lone_est_us[a])) {
+                // an idle group serves its due queries one by one on the
+                // single-root engine while that ends them sooner than a batch
+                // would (running means of both services), else batches them
+                bool lone = false;
+                if (G.active == 0 && !(s->flags & CGB_SERVER_BATCH_ONLY)) {
+                    uint32_t due = 0;
+                    for (const int64_t r : s->waiting[a]) {
+                        if (s->reqs[r].info.arrival_us > now || due == kSrvSlots) break;
+                        due++;
+                    }
+                    lone = due > 0 &&
+                           (double)due * s->lone_est_us[a] <= std::max(s->batch_est_us[a], s->lone_est_us[a]);
+                }
+                pick_admissions(s, G, s->waiting[a], now, lone ? 1u : kSrvSlots);
+                if (lone && G.admit.size() == 1) {
                     lone_k = (int)G.admit[0];
                     G.admit.clear();
                 }

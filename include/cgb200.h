@@ -412,10 +412,10 @@ typedef struct {
 #define CGB_SERVER_NO_SSSP 0x2u /* no SSSP slots (saves the 256 B per vertex of distances) */
 #define CGB_SERVER_HOST_TICKS 0x4u /* advance every level from the host thread (one synchronisation per
                                       level) instead of the device-resident level loop */
-#define CGB_SERVER_BATCH_ONLY 0x8u /* every query joins its multi-root group; by default a query that
-                                      finds its group idle, with no other query of its algorithm due
-                                      before a single-root run would end (running mean of those runs),
-                                      runs on the single-root engine of cgb_run */
+#define CGB_SERVER_BATCH_ONLY 0x8u /* every query joins its multi-root group.  By default an idle group
+                                      serves its n due queries one at a time on the single-root engine
+                                      of cgb_run while n x (mean single-root time) <= (mean admission-to-
+                                      result time of batched queries), and batches them otherwise */
 
 typedef struct {
     uint64_t id;
