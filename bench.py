@@ -613,6 +613,20 @@ def bench_serving(args, cg, L, dev):
                 ms.append(g.stats().ms)
             lone[an] = {"median_ms": float(np.median(ms)), "max_ms": float(np.max(ms))}
         res["lone_run"] = lone
+        # the batch engines' rate for the same mix: 64 BFS and 64 SSSP roots as
+        # two cgb_run_batch passes (results left on the device)
+        import torch
+        buf = torch.empty((64, g.vertexNum), dtype=torch.int32, device=f"cuda:{dev}")
+        rngb = np.random.default_rng(args.seed + 98)
+        bt = {}
+        for a, an in ((BFS, "bfs"), (SSSP, "sssp")):
+            rb = [int(x) for x in nzv[rngb.integers(0, nzv.size, 64)]]
+            g.run_batch(a, rb, out=buf)
+            bt[an] = min(g.run_batch(a, rb, out=buf)[1] for _ in range(2))
+        del buf
+        torch.cuda.empty_cache()
+        batch_rate = 128.0 / (bt["bfs"] + bt["sssp"]) * 1e3
+        res["batch64"] = {"bfs_ms": bt["bfs"], "sssp_ms": bt["sssp"], "mix_rate_req_s": batch_rate}
         for rate, nreq in rates:
             rng = np.random.default_rng(args.seed * 1000 + rate)
             arrivals = np.cumsum(rng.exponential(1e6 / rate, nreq))
@@ -633,10 +647,13 @@ def bench_serving(args, cg, L, dev):
                 la = np.array([r["done_us"] - r["arrival_us"] for r in recs if r["algorithm"] == a]) / 1e3
                 if la.size:
                     per[an] = {"p50_ms": float(np.percentile(la, 50)), "p99_ms": float(np.percentile(la, 99))}
+            for an in per:
+                per[an]["p50_vs_lone"] = per[an]["p50_ms"] / lone[an]["median_ms"]
             res[f"rate{rate}"] = {"requests": nreq, "completed": len(recs),
                                   "errors": sum(1 for r in recs if r["status"] != 0),
                                   "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                                   "throughput_req_s": len(recs) / makespan, "gteps": edges / makespan / 1e9,
+                                  "served_vs_batch_rate": len(recs) / makespan / batch_rate,
                                   "ticks": sst["ticks"], "per_algorithm": per}
         g.close()
         out[name] = res
