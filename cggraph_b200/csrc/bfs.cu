@@ -139,7 +139,9 @@ __global__ void k_q2bm(const uint32_t* __restrict__ q, uint32_t n, uint32_t* bm)
 // next (all words, so it needs no clearing) and the next queue.  Each lane
 // scans its vertex's in-list four entries at a time: four source loads,
 // then their four frontier words, are in flight together, and the scan
-// stops after the group that holds a parent.
+// stops after the group that holds a parent.  A CTA takes kBlock / 32
+// consecutive bitmap words per step (one per warp) and appends the step's
+// found vertices with one atomic.
 __global__ void __launch_bounds__(kBlock) k_bfs_bu(uint32_t V, const uint32_t* __restrict__ in_off,
                                                    const uint32_t* __restrict__ in_src,
                                                    const uint32_t* __restrict__ off, uint32_t* level,
@@ -148,38 +150,44 @@ __global__ void __launch_bounds__(kBlock) k_bfs_bu(uint32_t V, const uint32_t* _
                                                    uint32_t* qlen, uint32_t cap, DevCounters* ctr)
 {
     const uint32_t words = (V + 31) / 32;
-    const uint32_t warps = gridDim.x * (blockDim.x / 32);
+    constexpr uint32_t kWarps = kBlock / 32;
     unsigned long long medges = 0;
     uint32_t found_cnt = 0, mx = 0;
-    for (uint32_t wi = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); wi < words; wi += warps) {
-        const uint32_t vis = visited[wi];
+    for (uint32_t base = blockIdx.x * kWarps; base < words; base += gridDim.x * kWarps) {
+        const uint32_t wi = base + (threadIdx.x >> 5);
         const uint32_t v = wi * 32 + lane_id();
-        bool found = false;
-        if (v < V && !((vis >> lane_id()) & 1u)) {
-            const uint32_t e1 = in_off[v + 1];
-            for (uint32_t e = in_off[v]; e < e1 && !found; e += 4) {
-                uint32_t u[4], f[4];
+        bool enq = false;
+        if (wi < words) {  // uniform across the warp
+            const uint32_t vis = visited[wi];
+            bool found = false;
+            if (v < V && !((vis >> lane_id()) & 1u)) {
+                const uint32_t e1 = in_off[v + 1];
+                for (uint32_t e = in_off[v]; e < e1 && !found; e += 4) {
+                    uint32_t u[4], f[4];
 #pragma unroll
-                for (int k = 0; k < 4; k++) u[k] = e + k < e1 ? in_src[e + k] : in_src[e];
+                    for (int k = 0; k < 4; k++) u[k] = e + k < e1 ? in_src[e + k] : in_src[e];
 #pragma unroll
-                for (int k = 0; k < 4; k++) f[k] = front[u[k] >> 5] >> (u[k] & 31u);
+                    for (int k = 0; k < 4; k++) f[k] = front[u[k] >> 5] >> (u[k] & 31u);
 #pragma unroll
-                for (int k = 0; k < 4; k++) found |= (f[k] & 1u) != 0;
+                    for (int k = 0; k < 4; k++) found |= (f[k] & 1u) != 0;
+                }
             }
+            const uint32_t fm = __ballot_sync(0xffffffffu, found);
+            if (found) level[v] = next_level;
+            if (lane_id() == 0) {
+                next[wi] = fm;
+                if (fm) visited[wi] = vis | fm;
+            }
+            enq = found && v < nz;
+            uint32_t deg = 0;
+            if (enq) deg = off[v + 1] - off[v];
+            medges += deg;
+            found_cnt += enq;
+            mx = max(mx, deg);
         }
-        const uint32_t fm = __ballot_sync(0xffffffffu, found);
-        if (found) level[v] = next_level;
-        if (lane_id() == 0) {
-            next[wi] = fm;
-            if (fm) visited[wi] = vis | fm;
-        }
-        const bool enq = found && v < nz;
-        uint32_t deg = 0;
-        if (enq) deg = off[v + 1] - off[v];
-        warp_append(enq, v, qout, qlen, cap, &ctr->overflow);
-        medges += deg;
-        found_cnt += enq;
-        mx = max(mx, deg);
+        const bool p[1] = {enq};
+        const uint32_t it[1] = {v};
+        block_append_n<1>(p, it, qout, qlen, cap, &ctr->overflow);
     }
     medges = warp_sum(medges);
     found_cnt = warp_sum(found_cnt);

@@ -123,6 +123,36 @@ __device__ __forceinline__ void warp_append_n(const bool (&pred)[N], const uint3
     }
 }
 
+// CTA-aggregated append of up to N items per thread: one atomic per CTA of
+// kBlock threads instead of one per warp (a queue counter that every warp of
+// a full-graph scan hits serialises at its L2 slice).  Every thread of the
+// CTA must call it: it synchronises the CTA.
+template <int N>
+__device__ __forceinline__ void block_append_n(const bool (&pred)[N], const uint32_t (&item)[N], uint32_t* q,
+                                               uint32_t* ctr, uint32_t cap, uint32_t* overflow)
+{
+    __shared__ uint32_t s_scan[kBlock / 32 + 1];
+    __shared__ uint32_t s_base;
+    uint32_t cnt = 0;
+#pragma unroll
+    for (int i = 0; i < N; i++) cnt += pred[i] ? 1u : 0u;
+    uint32_t total;
+    const uint32_t excl = block_excl_scan(cnt, total, s_scan);
+    if (total == 0) return;  // uniform across the CTA
+    if (threadIdx.x == 0) s_base = atomicAdd(ctr, total);
+    __syncthreads();
+    uint32_t idx = s_base + excl;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        if (pred[i]) {
+            if (idx < cap) q[idx] = item[i];
+            else atomicOr(overflow, 1u);
+            idx++;
+        }
+    }
+    __syncthreads();  // s_base is rewritten by the next call
+}
+
 // Fine-grained tier: a CTA-wide exclusive scan of the (small) remaining
 // degrees packs the lists into shared memory, one edge per thread per round.
 // Every thread of the CTA must call it.

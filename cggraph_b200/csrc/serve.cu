@@ -859,6 +859,9 @@ static bool admission_due(cgb_server* s, const Group& G, int a)
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->waiting[a].empty()) return false;
     if (s->reqs[s->waiting[a].front()].info.arrival_us > us_since(s, Clock::now())) return false;
+    if ((s->flags & CGB_SERVER_GENERATIONS) && G.active != 0 &&
+        2u * (uint32_t)__builtin_popcountll(G.active) > G.nslots)
+        return false;
     for (uint32_t k = 0; k < G.nslots; k++)
         if (G.state[k] == SlotState::kFree) return true;
     return false;
@@ -1186,7 +1189,13 @@ static void group_loop(cgb_server* s, int a)
                     lone = due > 0 &&
                            (double)due * s->lone_est_us[a] <= std::max(s->batch_est_us[a], s->lone_est_us[a]);
                 }
-                pick_admissions(s, G, s->waiting[a], now, lone ? 1u : kSrvSlots);
+                // CGB_SERVER_GENERATIONS: a running group takes new queries only
+                // while at least half of its slots are free, so admitted queries
+                // share more of their dense levels
+                const bool hold = (s->flags & CGB_SERVER_GENERATIONS) && G.active != 0 &&
+                                  2u * (uint32_t)__builtin_popcountll(G.active) > G.nslots;
+                if (!hold) pick_admissions(s, G, s->waiting[a], now, lone ? 1u : kSrvSlots);
+                else G.admit.clear();
                 if (lone && G.admit.size() == 1) {
                     lone_k = (int)G.admit[0];
                     G.admit.clear();

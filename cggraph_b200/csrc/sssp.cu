@@ -73,7 +73,7 @@ struct SsspOp {
             nd[i] = ok[i] ? (uint32_t)cand : 0u;
         }
 #pragma unroll
-        for (int i = 0; i < N; i++) cur[i] = ok[i] ? dist[d[i]] : 0u;
+        for (int i = 0; i < N; i++) cur[i] = ok[i] ? __ldcg(dist + d[i]) : 0u;  // L2 only: a gather rarely hits L1
 #pragma unroll
         for (int i = 0; i < N; i++) {
             ok[i] = ok[i] && nd[i] < cur[i];
@@ -189,7 +189,7 @@ struct SsspDenseOp {
             nd[i] = ok[i] ? (uint32_t)cand : 0u;
         }
 #pragma unroll
-        for (int i = 0; i < N; i++) cur[i] = ok[i] ? dist[d[i]] : 0u;
+        for (int i = 0; i < N; i++) cur[i] = ok[i] ? __ldcg(dist + d[i]) : 0u;  // L2 only: a gather rarely hits L1
 #pragma unroll
         for (int i = 0; i < N; i++)
             if (ok[i] && nd[i] < cur[i]) atomicMin(dist + d[i], nd[i]);
@@ -210,8 +210,9 @@ struct SsspDenseOp {
 // vertices with one 16-byte load of each array, so a warp covers 128
 // vertices = 4 bitmap words per step; the 8 lanes of a word OR their far
 // bits together, and the first of them writes the word (no atomics: only
-// this warp touches it).  The next queue's out-edges and the new far bits
-// are counted.
+// this warp touches it).  A CTA takes kBlock * 4 consecutive vertices per
+// step and appends the step's next-queue vertices with one atomic.  The next
+// queue's out-edges and the new far bits are counted.
 __global__ void __launch_bounds__(kBlock) k_sssp_dense_scan(uint32_t V, const uint32_t* __restrict__ dist,
                                                             const uint32_t* __restrict__ snap, uint32_t thr,
                                                             uint32_t nz, const uint32_t* __restrict__ off,
@@ -219,12 +220,10 @@ __global__ void __launch_bounds__(kBlock) k_sssp_dense_scan(uint32_t V, const ui
                                                             uint32_t cap, DevCounters* ctr)
 {
     const uint32_t lane = lane_id();
-    const uint32_t gw = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
-    const uint32_t nwarps = gridDim.x * (blockDim.x / 32);
     unsigned long long deg_sum = 0;
     uint32_t new_far = 0, touched = 0, max_deg = 0;
-    for (uint64_t b0 = (uint64_t)gw * 128; b0 < V; b0 += (uint64_t)nwarps * 128) {
-        const uint32_t v0 = (uint32_t)b0 + 4 * lane;
+    for (uint64_t b0 = (uint64_t)blockIdx.x * kBlock * 4; b0 < V; b0 += (uint64_t)gridDim.x * kBlock * 4) {
+        const uint32_t v0 = (uint32_t)b0 + 4 * threadIdx.x;
         uint32_t dv[4], sv[4], v[4];
         if (v0 + 3 < V) {
             const uint4 a = *reinterpret_cast<const uint4*>(dist + v0);
@@ -268,7 +267,7 @@ __global__ void __launch_bounds__(kBlock) k_sssp_dense_scan(uint32_t V, const ui
             deg_sum += hi[k] - lo[k];
             max_deg = max(max_deg, hi[k] - lo[k]);
         }
-        warp_append_n<4>(to_near, v, near_out, near_len, cap, &ctr->overflow);
+        block_append_n<4>(to_near, v, near_out, near_len, cap, &ctr->overflow);
     }
     deg_sum = warp_sum(deg_sum);
     touched = warp_sum(touched);

@@ -416,6 +416,9 @@ typedef struct {
                                       serves its n due queries one at a time on the single-root engine
                                       of cgb_run while n x (mean single-root time) <= (mean admission-to-
                                       result time of batched queries), and batches them otherwise */
+#define CGB_SERVER_GENERATIONS 0x10u /* a running group admits new queries only while at least half of
+                                        its slots are free (queries then share more of their dense
+                                        levels; a query may wait for a slot that is already free) */
 
 typedef struct {
     uint64_t id;
