@@ -144,7 +144,7 @@ class ServerConfig(ctypes.Structure):
     ]
 
 
-SERVER_NO_BFS, SERVER_NO_SSSP, SERVER_HOST_TICKS, SERVER_BATCH_ONLY, SERVER_GENERATIONS = 0x1, 0x2, 0x4, 0x8, 0x10
+SERVER_NO_BFS, SERVER_NO_SSSP, SERVER_HOST_TICKS, SERVER_BATCH_ONLY, SERVER_ADMIT_ANY_SLOT = 0x1, 0x2, 0x4, 0x8, 0x10
 
 
 class RequestInfo(ctypes.Structure):

@@ -221,7 +221,7 @@ cgb_status cgb_batch_create(uint32_t n, const uint32_t* const* offsets, const ui
             CGB_CUDA_TRY(cudaMalloc((void**)&b->sx, sizeof(PersistSssp)));
             ensure_frontier(g);
             if (!g->persist) g->persist = pool_alloc(sizeof(PersistBlock), g->stream);
-            b->delta = sssp_default_delta(g);
+            b->delta = sssp_delta_for(g, 8.0);
         } catch (...) {
             if (b->g) graph_free(b->g);
             if (b->d_base) cudaFree(b->d_base);

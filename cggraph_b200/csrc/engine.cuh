@@ -191,7 +191,8 @@ void graph_free(cgb_graph* g);
 void graph_set_weights(cgb_graph* g, const uint32_t* weight);
 void validate_and_sort(cgb_graph* g);
 void compute_weight_sum(cgb_graph* g);
-uint32_t sssp_default_delta(const cgb_graph* g);
+uint32_t sssp_default_delta(const cgb_graph* g);           // single-root runs
+uint32_t sssp_delta_for(const cgb_graph* g, double c);     // c x mean weight / mean out-degree
 
 // workspace management (graph.cu)
 void ensure_frontier(cgb_graph* g);

@@ -186,10 +186,9 @@ __global__ void k_mssp_set(uint32_t* a, uint32_t value) { *a = value; }
 uint32_t mssp_default_delta(cgb_graph* g)
 {
     if (g->w && g->sum_w == 0) compute_weight_sum(g);
-    // a round serves up to 64 roots: wider buckets than one root's (on
-    // RMAT-22/24 rounds stop shrinking beyond about 8x)
-    const uint64_t d = 8ull * sssp_default_delta(g);
-    return (uint32_t)std::min<uint64_t>(d, 100000000ull);
+    // a round serves up to 64 roots (on RMAT-22/24 its rounds stop shrinking
+    // beyond 64 x the unit); at least 8
+    return std::max<uint32_t>(8u, sssp_delta_for(g, 64.0));
 }
 
 void run_mssp(cgb_graph* g, const uint32_t* d_roots, uint32_t n, uint32_t* out, uint32_t delta)

@@ -859,7 +859,7 @@ static bool admission_due(cgb_server* s, const Group& G, int a)
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->waiting[a].empty()) return false;
     if (s->reqs[s->waiting[a].front()].info.arrival_us > us_since(s, Clock::now())) return false;
-    if ((s->flags & CGB_SERVER_GENERATIONS) && G.active != 0 &&
+    if (!(s->flags & CGB_SERVER_ADMIT_ANY_SLOT) && G.active != 0 &&
         2u * (uint32_t)__builtin_popcountll(G.active) > G.nslots)
         return false;
     for (uint32_t k = 0; k < G.nslots; k++)
@@ -1112,6 +1112,8 @@ static void group_retire(cgb_server* s, Group& G, unsigned long long fin, unsign
 // A query served alone on the single-root engine (the latency of a lone
 // cgb_run).  Its result region gets the engine's result, and the slot
 // retires as a batched one does.
+constexpr uint32_t kLoneMaxDue = 4;
+
 static void lone_run(cgb_server* s, Group& G, int a, uint32_t k)
 {
     cgb_graph* g = s->g;
@@ -1168,7 +1170,8 @@ static void group_loop(cgb_server* s, int a)
 {
     cgb_graph* g = s->g;
     Group& G = s->grp[a];
-    int lone_k = -1;  // slot admitted this tick for the single-root engine
+    int lone_k = -1;         // slot admitted this tick for the single-root engine
+    bool other_idle = true;  // the other group had no query at this tick's admission
     try {
         CGB_CUDA_TRY(cudaSetDevice(g->device));
         while (!s->stop.load()) {
@@ -1176,24 +1179,31 @@ static void group_loop(cgb_server* s, int a)
                 std::unique_lock<std::mutex> lk(s->mu);
                 if (s->error != CGB_OK) break;
                 const double now = us_since(s, Clock::now());
-                // an idle group serves its due queries one by one on the
-                // single-root engine while that ends them sooner than a batch
-                // would (running means of both services), else batches them
+                // an idle group serves up to kLoneMaxDue due queries one by one
+                // on the single-root engine while that ends them sooner than a
+                // batch would (running means of both services), else batches
+                // them.  The cap bounds how long single-root runs, which hold the
+                // graph, keep the other group's ticks waiting; and under load a
+                // batch serves many more queries per second.
                 bool lone = false;
                 if (G.active == 0 && !(s->flags & CGB_SERVER_BATCH_ONLY)) {
                     uint32_t due = 0;
                     for (const int64_t r : s->waiting[a]) {
-                        if (s->reqs[r].info.arrival_us > now || due == kSrvSlots) break;
+                        if (s->reqs[r].info.arrival_us > now || due > kLoneMaxDue) break;
                         due++;
                     }
-                    lone = due > 0 &&
+                    lone = due > 0 && due <= kLoneMaxDue &&
                            (double)due * s->lone_est_us[a] <= std::max(s->batch_est_us[a], s->lone_est_us[a]);
                 }
-                // CGB_SERVER_GENERATIONS: a running group takes new queries only
-                // while at least half of its slots are free, so admitted queries
-                // share more of their dense levels
-                const bool hold = (s->flags & CGB_SERVER_GENERATIONS) && G.active != 0 &&
+                // a running group takes new queries only while at least half of
+                // its slots are free (unless CGB_SERVER_ADMIT_ANY_SLOT), so that
+                // admitted queries share more of their dense levels
+                const bool hold = !(s->flags & CGB_SERVER_ADMIT_ANY_SLOT) && G.active != 0 &&
                                   2u * (uint32_t)__builtin_popcountll(G.active) > G.nslots;
+                // the device-resident loops run only while the other group is idle:
+                // they take turns on the cooperative-launch lock, whereas ticks of
+                // both groups overlap on their two streams
+                other_idle = s->grp[a ^ 1].active == 0;
                 if (!hold) pick_admissions(s, G, s->waiting[a], now, lone ? 1u : kSrvSlots);
                 else G.admit.clear();
                 if (lone && G.admit.size() == 1) {
@@ -1224,7 +1234,8 @@ static void group_loop(cgb_server* s, int a)
                 const bool pull = (double)G.medges * 15.0 > (double)g->E;
                 uint64_t before = G.loop_levels;
                 fin = 0;
-                if (G.loop && G.nact > 0 && G.nact <= nf_exit && !pull) fin = bfs_device_levels(s, G, nf_exit);
+                if (G.loop && other_idle && G.nact > 0 && G.nact <= nf_exit && !pull)
+                    fin = bfs_device_levels(s, G, nf_exit);
                 if (G.loop_levels == before) {
                     bfs_issue(s, G);
                     CGB_CUDA_TRY(cudaMemcpyAsync(G.h_stats->alive, G.d_stats->alive, sizeof(G.h_stats->alive),
@@ -1238,7 +1249,7 @@ static void group_loop(cgb_server* s, int a)
             } else {
                 uint64_t before = G.loop_levels;
                 fin = 0;
-                if (G.sp_loop) {
+                if (G.sp_loop && other_idle) {
                     sp_admit(s, G);
                     fin = sp_device_ticks(s, G);
                 }

@@ -70,7 +70,7 @@ typedef struct cgb_options {
     uint32_t struct_size;   /* sizeof(cgb_options); 0 = all defaults */
     int32_t schedule;       /* cgb_schedule */
     int32_t variant;        /* cgb_variant, for CGB_SCHED_FIXED */
-    uint32_t sssp_delta;    /* 0 = heuristic: 8 * mean weight / mean degree (x8 for multi-root passes) */
+    uint32_t sssp_delta;    /* 0 = heuristic: 128 * mean weight / mean degree (64 x for multi-root passes) */
     double bfs_alpha;       /* Beamer alpha, 0 = 15 */
     double bfs_beta;        /* Beamer beta, 0 = 18 */
     uint64_t max_iterations;/* 0 = unlimited (V + 1 levels bound BFS anyway) */
@@ -413,12 +413,13 @@ typedef struct {
 #define CGB_SERVER_HOST_TICKS 0x4u /* advance every level from the host thread (one synchronisation per
                                       level) instead of the device-resident level loop */
 #define CGB_SERVER_BATCH_ONLY 0x8u /* every query joins its multi-root group.  By default an idle group
-                                      serves its n due queries one at a time on the single-root engine
-                                      of cgb_run while n x (mean single-root time) <= (mean admission-to-
-                                      result time of batched queries), and batches them otherwise */
-#define CGB_SERVER_GENERATIONS 0x10u /* a running group admits new queries only while at least half of
-                                        its slots are free (queries then share more of their dense
-                                        levels; a query may wait for a slot that is already free) */
+                                      serves its n <= 4 due queries one at a time on the single-root
+                                      engine of cgb_run while n x (mean single-root time) <= (mean
+                                      admission-to-result time of batched queries), and batches them
+                                      otherwise */
+#define CGB_SERVER_ADMIT_ANY_SLOT 0x10u /* a running group admits a due query into any free slot; by
+                                           default only while at least half of its slots are free, so
+                                           that admitted queries share more of their dense levels */
 
 typedef struct {
     uint64_t id;

@@ -40,7 +40,7 @@ def _serve_and_check(g, queries, arrivals, **cfg):
     return recs, st
 
 
-@pytest.mark.parametrize("flags", [0, L.SERVER_HOST_TICKS, L.SERVER_BATCH_ONLY])
+@pytest.mark.parametrize("flags", [0, L.SERVER_HOST_TICKS, L.SERVER_BATCH_ONLY, L.SERVER_ADMIT_ANY_SLOT])
 def test_server_mix_equals_lone_runs(oracle, flags):
     """RMAT-14 (weights 1..64): 120 BFS/SSSP queries with Poisson arrivals,
     8 slots per algorithm so that slots are reused while other queries run;
