@@ -491,7 +491,6 @@ cgb_status cgb_policy_collect(cgb_graph* g, int algorithm, uint32_t root, const 
         CGB_CUDA_TRY(cudaMalloc((void**)&ps.save_bm0, (size_t)g->words() * 4));
         CGB_CUDA_TRY(cudaMalloc((void**)&ps.save_q, (size_t)g->V * 4));
         CGB_CUDA_TRY(cudaMalloc((void**)&ps.save_ctr, sizeof(DevCounters)));
-        CGB_CUDA_TRY(cudaMalloc((void**)&ps.settled, sizeof(unsigned long long)));
         g->collect = &ps;
         try {
             run_one(g, algorithm, root, o);
@@ -505,7 +504,6 @@ cgb_status cgb_policy_collect(cgb_graph* g, int algorithm, uint32_t root, const 
     if (ps.save_bm0) cudaFree(ps.save_bm0);
     if (ps.save_q) cudaFree(ps.save_q);
     if (ps.save_ctr) cudaFree(ps.save_ctr);
-    if (ps.settled) cudaFree(ps.settled);
     if (count) *count = ps.count;
     return st;
 }

@@ -228,6 +228,42 @@ __global__ void k_cc_sample(uint32_t V, uint32_t* comp, uint32_t* out, uint32_t 
     }
 }
 
+// Steps from n sampled vertices towards their roots in the init forest,
+// each walk cut at max_steps (read only).
+__global__ void k_cc_depth(uint32_t V, const uint32_t* __restrict__ comp, uint32_t n, uint64_t seed,
+                           uint32_t max_steps, unsigned long long* steps)
+{
+    unsigned long long t = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t v = (uint32_t)(mix64(seed ^ i) % V);
+        for (uint32_t k = 0; k < max_steps; k++) {
+            const uint32_t p = comp[v];
+            if (p == v) break;
+            v = p;
+            t++;
+        }
+    }
+    t = warp_sum(t);
+    if (lane_id() == 0 && t) atomicAdd(steps, t);
+}
+
+// One pointer-jumping pass, comp[v] = comp[comp[v]] (an ancestor replaces
+// the parent, so a concurrent update only shortens a walk); raises *changed
+// when some pointer moved.
+__global__ void k_cc_jump(uint32_t V, uint32_t* comp, uint32_t* changed)
+{
+    bool ch = false;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+        const uint32_t p = comp[v];
+        const uint32_t pp = comp[p];
+        if (pp != p) {
+            comp[v] = pp;
+            ch = true;
+        }
+    }
+    if (__any_sync(0xffffffffu, ch) && lane_id() == 0) *changed = 1u;
+}
+
 struct CcLinkOp {
     const uint32_t* __restrict__ off;
     const uint32_t* __restrict__ dst;
@@ -313,7 +349,37 @@ static void cc_afforest(cgb_graph* g, bool weak)
         k_cc_init_min_nbr<<<grid, kBlock, 0, g->stream>>>(V, g->off, g->dst, g->value);
     CGB_CUDA_TRY(cudaMemsetAsync(g->ctr, 0, sizeof(DevCounters), g->stream));
     if (timing) ktimer_end(g);
-    // no compress here: the link round's finds halve the init forest's paths
+    // The init forest is shallow on skewed graphs, and the link round's finds
+    // halve its paths.  On meshes it is deep: on a grid numbered row by row,
+    // each vertex's smallest neighbour is the one above it, so the trees are
+    // whole columns (4800 levels on the 4800 x 5000 grid) and every find of
+    // the link rounds walks one.  A probe measures the mean depth of 1024
+    // sampled vertices; above kDeepForest the forest is flattened by
+    // pointer jumping first (each pass halves every path).  The probe's
+    // walks stop after 4 x kDeepForest steps.
+    {
+        constexpr uint32_t kProbe = 1024;
+        constexpr double kDeepForest = 8.0;
+        if (timing) ktimer_begin(g, CGB_K_COMPRESS);
+        ++g->stats.launches;
+        k_cc_depth<<<4, kBlock, 0, g->stream>>>(V, g->value, kProbe, 0xDE9741ull, (uint32_t)(4 * kDeepForest),
+                                                &g->ctr->reached_edges);
+        sync_counters(g);
+        if ((double)g->h_ctr->reached_edges / kProbe > kDeepForest) {
+            const uint32_t jgrid = grid_for(V, kBlock, num_sms() * 8);
+            uint32_t pass = 0;
+            for (;; pass++) {
+                CGB_REQUIRE(pass < 40, CGB_ETIMEOUT, "CC pointer jumping did not converge");
+                CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->found, 0, sizeof(uint32_t), g->stream));
+                ++g->stats.launches;
+                k_cc_jump<<<jgrid, kBlock, 0, g->stream>>>(V, g->value, &g->ctr->found);
+                sync_counters(g);
+                if (!g->h_ctr->found) break;
+            }
+        }
+        CGB_CUDA_TRY(cudaMemsetAsync(g->ctr, 0, sizeof(DevCounters), g->stream));
+        if (timing) ktimer_end(g);
+    }
     for (uint32_t r = 1; r < kRounds; r++) {
         if (timing) ktimer_begin(g, CGB_K_HOOK);
         ++g->stats.launches;

@@ -39,7 +39,6 @@ struct PolicySamples {
     uint32_t* save_bm1 = nullptr;
     uint32_t* save_q = nullptr;
     DevCounters* save_ctr = nullptr;
-    unsigned long long* settled = nullptr;  // SSSP delta trials: vertices below the threshold
 };
 
 namespace cgb {

@@ -20,7 +20,7 @@ static_assert(kPolicyParams == kPolicyFeatures * kPolicyHidden + kPolicyHidden +
 // Output heads: predicted log-cost of each choice (lower is better).
 constexpr int kOutPush = 0, kOutPull = 1;  // BFS next level: binned push / bottom-up pull
 constexpr int kOutPushChunked = 9;         // BFS next level: push, every list >= 32 edges chunked
-constexpr int kOutDelta0 = 2;              // SSSP delta x delta_scale(i) for the next bucket
+constexpr int kOutDelta0 = 2;              // SSSP delta x delta_scale(i) for the rest of the run
 // SSSP next near round: sparse frontier (binned push), sparse frontier with
 // chunked lists, dense frontier, pull
 constexpr int kOutRound0 = 10;

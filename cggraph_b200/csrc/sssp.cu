@@ -296,17 +296,6 @@ __global__ void k_sssp_round_reset(DevCounters* ctr, int out, uint32_t* bm, uint
         for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < words; i += gridDim.x * blockDim.x) bm[i] = 0;
 }
 
-// Vertices whose distance is below thr (trace collection only).
-__global__ void k_sssp_count_below(uint32_t V, const uint32_t* __restrict__ value, uint32_t thr,
-                                   unsigned long long* out)
-{
-    uint32_t c = 0;
-    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x)
-        c += value[v] < thr ? 1u : 0u;
-    c = warp_sum(c);
-    if (lane_id() == 0 && c) atomicAdd(out, (unsigned long long)c);
-}
-
 // The same before a bucket split: next queue, far count, smallest far distance.
 __global__ void k_sssp_split_reset(DevCounters* ctr, int out)
 {
@@ -681,46 +670,37 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
         return in;
     };
 
-    // vertices with a distance below t: after a bucket phase, the settled ones
-    auto settled_below = [&](uint64_t t) {
-        CGB_CUDA_TRY(cudaMemsetAsync(collect->settled, 0, sizeof(unsigned long long), g->stream));
-        k_sssp_count_below<<<num_sms() * 4, kBlock, 0, g->stream>>>(
-            V, g->value, (uint32_t)std::min<uint64_t>(t, kValueMax), collect->settled);
-        unsigned long long n = 0;
-        CGB_CUDA_TRY(cudaMemcpyAsync(&n, collect->settled, sizeof(n), cudaMemcpyDeviceToHost, g->stream));
-        CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
-        return (uint64_t)n;
-    };
-
+    // The learned (or collected) delta is chosen once, at the first bucket
+    // boundary, for the rest of the run: a counterfactual trial runs the whole
+    // remainder of the run with each candidate, so the sample's costs include
+    // everything a narrower or wider bucket changes later (a trial of one
+    // bucket phase saw only that phase).
+    bool delta_decided = false;
     near_rounds();
     while (nfar > 0) {
         uint32_t d = delta;
-        if (collect) {
-            // counterfactual: one bucket phase per delta choice from the same state
+        if (collect && !delta_decided) {
             const size_t vbytes = (size_t)V * 4, wbytes = (size_t)words * 4;
             CGB_CUDA_TRY(cudaMemcpyAsync(collect->save_value, g->value, vbytes, cudaMemcpyDeviceToDevice, g->stream));
             CGB_CUDA_TRY(cudaMemcpyAsync(collect->save_bm0, far_bm, wbytes, cudaMemcpyDeviceToDevice, g->stream));
-            const uint64_t s_thr = thr, s_iters = iters, s_exp = expanded, s_far = nfar;
+            const uint64_t s_thr = thr, s_iters = iters, s_exp = expanded, s_far = nfar, s_lo = bucket_lo;
             const int s_cur = cur;
             float ms[kPolicyOutputs] = {};
             bool have[kPolicyOutputs] = {};
             int best = kDeltaUnit;
-            const uint64_t s_settled = settled_below(s_thr);
             in_delta_trial = true;
             for (int k = 0; k < kNumDeltaChoices; k++) {
                 const uint32_t dk = std::max<uint32_t>(1u, (uint32_t)(base_delta * delta_scale(k)));
                 CGB_CUDA_TRY(cudaEventRecord(g->ev_iter[0], g->stream));
-                advance(dk);
-                near_rounds();
+                do {
+                    advance(dk);
+                    near_rounds();
+                } while (nfar > 0);
                 CGB_CUDA_TRY(cudaEventRecord(g->ev_iter[1], g->stream));
                 CGB_CUDA_TRY(cudaEventSynchronize(g->ev_iter[1]));
                 float t = 0.f;
                 CGB_CUDA_TRY(cudaEventElapsedTime(&t, g->ev_iter[0], g->ev_iter[1]));
-                // the phase's cost per vertex it settles, as the time to settle
-                // all V at that rate (wide buckets cover more distance, but on
-                // skewed graphs most of it holds few vertices)
-                const uint64_t gained = settled_below(thr) - s_settled;
-                ms[kOutDelta0 + k] = t * (float)((double)V / (double)std::max<uint64_t>(gained, 1));
+                ms[kOutDelta0 + k] = t;  // the rest of the run
                 have[kOutDelta0 + k] = true;
                 if (ms[kOutDelta0 + k] < ms[kOutDelta0 + best]) best = k;
                 CGB_CUDA_TRY(cudaMemcpyAsync(g->value, collect->save_value, vbytes, cudaMemcpyDeviceToDevice,
@@ -730,17 +710,20 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
                 iters = s_iters;
                 expanded = s_exp;
                 nfar = s_far;
+                bucket_lo = s_lo;
                 nnear = 0;
                 cur = s_cur;
             }
             in_delta_trial = false;
             policy_log_sample(g, state_now(), ms, have);
             d = std::max<uint32_t>(1u, (uint32_t)(base_delta * delta_scale(best)));
-        } else if (pol) {
+            delta_decided = true;
+        } else if (pol && !delta_decided) {
             policy_enqueue(pol, g, state_now(), 0, false, 0);
             sync_counters(g);
             const int k = policy_pick_delta(g->h_ctr->policy_out);
             if (k >= 0) d = std::max<uint32_t>(1u, (uint32_t)(base_delta * delta_scale(k)));
+            delta_decided = true;
         }
         delta = d;
         tail_delta_chosen = true;

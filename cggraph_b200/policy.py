@@ -6,7 +6,8 @@ in the engine; this module drives its C entry points (cgb_policy_*):
 
 * ``collect(graph, alg, root)`` -- counterfactual samples of one run: at each
   BFS level the three variants (binned push, chunked push, bottom-up pull),
-  at each SSSP bucket boundary all seven delta multipliers (x 1/4 .. x 16),
+  at the first SSSP bucket boundary the rest of the run under each of the
+  seven delta multipliers (x 1/4 .. x 16),
   at each large SSSP near round the four round variants (sparse frontier
   binned or chunked, dense frontier, pull), timed from the same snapshot;
 * ``train(X, T, M)`` -- masked-MSE training on the GPU by the engine's own

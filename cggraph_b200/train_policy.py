@@ -2,13 +2,15 @@
 
 Training graphs (seeded, none of them a benchmark input):
   RMAT scales 18, 20, 22 and 24 (a=.57, b=.19, c=.19, edge factor 16,
-  weights U[1,64]; seeds 2..5, the benchmark uses seed 1), Chung-Lu power-law
-  graphs of 1 M and 4 M vertices (the benchmark's degree exponent, seeds 2
-  and 3) and 2-D grids 256x256 to 4096x4096 (weights U[1,1000]).
-For each graph and a few seeded roots the engine records counterfactual
-samples (cgb_policy_collect): every BFS level timed as a binned push, a
-chunked push and a pull; every SSSP bucket timed with delta x {1/4, 1/2, 1,
-2, 4, 8, 16}; every large SSSP near round timed as each of its four variants.
+  weights U[1,64]; seeds 2..5, the benchmark uses seed 1) and scales 20 and
+  22 with edge factors 4 and 8, Chung-Lu power-law graphs of 1, 2 and 4 M
+  vertices (the benchmark's degree exponent, seeds 2..4) and 2-D grids
+  256x256 to 4096x4096 and 1024x4096 (weights U[1,1000]).
+For each graph and a few seeded roots (3 for BFS, 8 for SSSP) the engine
+records counterfactual samples (cgb_policy_collect): every BFS level timed as
+a binned push, a chunked push and a pull; at the first SSSP bucket boundary
+the rest of the run timed with delta x {1/4, 1/2, 1, 2, 4, 8, 16}; every
+large SSSP near round timed as each of its four variants.
 The network is trained on the GPU by the engine's own kernels
 (cgb_policy_train).
 
@@ -41,15 +43,18 @@ def training_graphs(quick: bool):
         return
     for scale, seed in ((18, 2), (20, 3), (22, 4), (24, 5)):
         yield f"rmat{scale}_s{seed}", (lambda s=scale, d=seed: cg.Graph.rmat(s, 16, seed=d))
-    for vc, seed in ((1_000_000, 2), (4_000_000, 3)):
+    for scale, ef, seed in ((20, 4, 6), (20, 8, 7), (22, 4, 8), (22, 8, 9)):
+        yield f"rmat{scale}_ef{ef}_s{seed}", (lambda s=scale, e=ef, d=seed: cg.Graph.rmat(s, e, seed=d))
+    for vc, seed in ((1_000_000, 2), (2_000_000, 4), (4_000_000, 3)):
         draws = int(vc * 35.3)  # the benchmark's draws per vertex (1.47 B / 41.6 M)
         i0 = cg.chunglu_weight_offset(vc, draws, max(1, int(vc * 0.072)))
         yield f"chunglu{vc // 1_000_000}m_s{seed}", (lambda v=vc, n=draws, o=i0, d=seed: cg.Graph.chunglu(v, n, o, seed=d))
     for n, seed in ((256, 2), (512, 3), (1024, 4), (2048, 6), (4096, 7)):
         yield f"grid{n}_s{seed}", (lambda n=n, d=seed: cg.Graph.grid(n, n, seed=d))
+    yield "grid1024x4096_s8", lambda: cg.Graph.grid(1024, 4096, seed=8)
 
 
-def collect_all(quick: bool, roots_per_graph: int = 3, log=print):
+def collect_all(quick: bool, roots_per_graph: int = 3, sssp_roots: int = 8, log=print):
     Xs, Ts, Ms, info = [], [], [], []
     for name, make in training_graphs(quick):
         g = make()
@@ -57,9 +62,12 @@ def collect_all(quick: bool, roots_per_graph: int = 3, log=print):
         deg = np.diff(off.astype(np.int64))
         rng = np.random.default_rng(zlib.crc32(name.encode()))
         cand = np.nonzero(deg)[0]
-        roots = [int(deg.argmax())] + [int(x) for x in rng.choice(cand, roots_per_graph - 1, replace=False)]
-        for r in roots:
+        nr = max(roots_per_graph, sssp_roots)
+        roots = [int(deg.argmax())] + [int(x) for x in rng.choice(cand, nr - 1, replace=False)]
+        for i, r in enumerate(roots):
             for alg in (BFS, SSSP):
+                if i >= (roots_per_graph if alg == BFS else sssp_roots):
+                    continue
                 t0 = time.time()
                 X, T, M = policy.collect(g, alg, r)
                 Xs.append(X)

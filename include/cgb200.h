@@ -484,8 +484,8 @@ cgb_status cgb_bfs_noalloc(const uint32_t* offsets, const uint32_t* dest, uint32
  *   [0] BFS next level pushed (degree-binned expansion), [1] pulled
  *       (bottom-up over a dense frontier bitmap), [9] pushed with every list
  *       of 32 edges or more cut into chunks dealt across the grid;
- *   [2..8] SSSP next bucket with delta x {1/4, 1/2, 1, 2, 4, 8, 16} (the cost
- *       of a bucket phase divided by its width);
+ *   [2..8] SSSP delta x {1/4, 1/2, 1, 2, 4, 8, 16} for the rest of the run,
+ *       chosen once at the first bucket boundary (the cost of the remainder);
  *   [10..13] SSSP next near round as a sparse frontier (queue) with the
  *       degree-binned expansion, a sparse frontier with every list of 32
  *       edges or more chunked, a dense frontier (relax, then scan all

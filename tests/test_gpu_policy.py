@@ -74,7 +74,8 @@ def test_collect_samples_and_unchanged_results(oracle):
         assert len(X) >= 3 and np.all(M[:, level] == 1)
         assert np.all(np.delete(M, level, axis=1) == 0)
         np.testing.assert_array_equal(g.run(BFS, root)[0], oracle.bfs(off, dst, root))
-        X2, T2, M2 = policy.collect(g, SSSP, root)
+        # a narrow delta, so that this small graph has several bucket boundaries
+        X2, T2, M2 = policy.collect(g, SSSP, root, cg.make_options(sssp_delta=16))
         bucket = np.all(M2[:, policy.SSSP_DELTA] == 1, axis=1)
         rnd = np.all(M2[:, policy.SSSP_ROUND] == 1, axis=1)
         assert bucket.any() and rnd.any()
@@ -117,18 +118,20 @@ def test_learned_schedule_gives_identical_results(oracle):
 
 def test_learned_gain():
     """The shipped network against the heuristic on held-out graphs (RMAT
-    seed 1, the benchmark's; a 700x700 grid): results identical, time
-    reported.  On the grid's SSSP, where the network learned to widen the
-    buckets, it must gain at least 1.25x (measured about 1.7x); elsewhere it
-    must not lose more than 15 % (its inference runs before the levels near
-    the Beamer switch)."""
+    seed 1, the benchmark's; a 700x700 grid; a Chung-Lu graph of a seed not
+    trained on): results identical, speed-up printed.  The heuristic's
+    delta is already within a few percent of the best fixed delta on RMAT
+    and grids, so the network must not lose more than 10 % there; on
+    Chung-Lu, where a narrower delta is 20 % faster, it must gain."""
     if not policy.load_default():
         pytest.skip("no trained weights shipped (python -m cggraph_b200.train_policy)")
+    dr, i0 = cg.chunglu_draws_for_edges(2_000_000, 70_000_000, 150_000)
     try:
         res = {}
         for name, make, alg in (("rmat20", lambda: cg.Graph.rmat(20, 16, seed=1), BFS),
                                 ("rmat20", lambda: cg.Graph.rmat(20, 16, seed=1), SSSP),
-                                ("grid700", lambda: cg.Graph.grid(700, 700, seed=1), SSSP)):
+                                ("grid700", lambda: cg.Graph.grid(700, 700, seed=1), SSSP),
+                                ("chunglu2m", lambda: cg.Graph.chunglu(2_000_000, dr, i0, seed=1), SSSP)):
             with make() as g:
                 t = {}
                 out = {}
@@ -143,7 +146,7 @@ def test_learned_gain():
                 np.testing.assert_array_equal(out[L.SCHED_HEURISTIC], out[L.SCHED_LEARNED])
                 res[(name, alg)] = t[L.SCHED_HEURISTIC] / t[L.SCHED_LEARNED]
         print("learned / heuristic speed-up:", res)
-        assert res[("grid700", SSSP)] >= 1.25, res
-        assert all(v > 0.85 for v in res.values()), res
+        assert all(v > 0.9 for v in res.values()), res
+        assert res[("chunglu2m", SSSP)] > 1.0, res
     finally:
         policy.load(None)
