@@ -356,8 +356,11 @@ static void cc_afforest(cgb_graph* g, bool weak)
     // the link rounds walks one.  A probe measures the mean depth of 1024
     // sampled vertices; above kDeepForest the forest is flattened by
     // pointer jumping first (each pass halves every path).  The probe's
-    // walks stop after 4 x kDeepForest steps.
-    {
+    // walks stop after 4 x kDeepForest steps.  Graphs with a vertex of
+    // kProbeMaxDeg or more out-edges skip the probe (and its host
+    // synchronisation): their hubs give shallow init forests.
+    constexpr uint32_t kProbeMaxDeg = 64;
+    if (g->max_degree < kProbeMaxDeg) {
         constexpr uint32_t kProbe = 1024;
         constexpr double kDeepForest = 8.0;
         if (timing) ktimer_begin(g, CGB_K_COMPRESS);

@@ -30,8 +30,7 @@
 // Set-up: host code cannot use the array's name as a device address (in host
 // code it names a host-side stand-in), so the first call on each device,
 // with that device current, asks cudaGetSymbolAddress for the array's device
-// address and caches it; that first call should therefore come before any
-// stream capture.  The cached address belongs to the device's primary
+// address and caches it.  The cached address belongs to the device's primary
 // context: calling cudaDeviceReset while this library is loaded is not
 // supported.  Nothing here calls cudaMalloc, cudaFree, cudaMallocHost or any
 // other allocating routine.

@@ -245,10 +245,21 @@ int policy_pick_bfs_level(const float* out, int heur)
     return pick_among(out, idx, 3, heur);
 }
 
+// The network may move a round between the two sparse-frontier expansions,
+// or keep the heuristic's dense or pull round; it never starts a dense or
+// pull round itself.  Those are rarely the cheapest in the traces (a pull
+// round on RMAT-24 costs 3-6 ms against 0.05-4 ms pushed), and on graphs
+// beyond the training range the network chose them where they cost 5x.
 int policy_pick_round(const float* out, int heur)
 {
     const int idx[kNumRoundChoices] = {kOutRound0, kOutRound0 + 1, kOutRound0 + 2, kOutRound0 + 3};
-    return pick_among(out, idx, kNumRoundChoices, heur);
+    if (heur != kRoundPush && heur != kRoundPushChunked) {
+        const int pair[2] = {heur, kRoundPush};
+        const int k[2] = {idx[heur], idx[kRoundPush]};
+        const int c = pick_among(out, k, 2, 0);
+        return c < 0 ? -1 : pair[c];
+    }
+    return pick_among(out, idx, 2, heur);
 }
 
 int policy_pick_delta(const float* out)

@@ -5,7 +5,8 @@ Training graphs (seeded, none of them a benchmark input):
   weights U[1,64]; seeds 2..5, the benchmark uses seed 1) and scales 20 and
   22 with edge factors 4 and 8, Chung-Lu power-law graphs of 1, 2 and 4 M
   vertices (the benchmark's degree exponent, seeds 2..4) and 2-D grids
-  256x256 to 4096x4096 and 1024x4096 (weights U[1,1000]).
+  256x256 to 4096x4096, 1024x4096 and 4800x5000 (weights U[1,1000]; the
+  benchmark's grid is seed 1, this one seed 9).
 For each graph and a few seeded roots (3 for BFS, 8 for SSSP) the engine
 records counterfactual samples (cgb_policy_collect): every BFS level timed as
 a binned push, a chunked push and a pull; at the first SSSP bucket boundary
@@ -52,6 +53,8 @@ def training_graphs(quick: bool):
     for n, seed in ((256, 2), (512, 3), (1024, 4), (2048, 6), (4096, 7)):
         yield f"grid{n}_s{seed}", (lambda n=n, d=seed: cg.Graph.grid(n, n, seed=d))
     yield "grid1024x4096_s8", lambda: cg.Graph.grid(1024, 4096, seed=8)
+    # the benchmark's grid shape with another seed (2 BFS and 4 SSSP roots)
+    yield "grid4800x5000_s9", lambda: cg.Graph.grid(4800, 5000, seed=9)
 
 
 def collect_all(quick: bool, roots_per_graph: int = 3, sssp_roots: int = 8, log=print):
@@ -62,11 +65,12 @@ def collect_all(quick: bool, roots_per_graph: int = 3, sssp_roots: int = 8, log=
         deg = np.diff(off.astype(np.int64))
         rng = np.random.default_rng(zlib.crc32(name.encode()))
         cand = np.nonzero(deg)[0]
-        nr = max(roots_per_graph, sssp_roots)
+        nb, ns = (2, 4) if name.startswith("grid4800") else (roots_per_graph, sssp_roots)
+        nr = max(nb, ns)
         roots = [int(deg.argmax())] + [int(x) for x in rng.choice(cand, nr - 1, replace=False)]
         for i, r in enumerate(roots):
             for alg in (BFS, SSSP):
-                if i >= (roots_per_graph if alg == BFS else sssp_roots):
+                if i >= (nb if alg == BFS else ns):
                     continue
                 t0 = time.time()
                 X, T, M = policy.collect(g, alg, r)

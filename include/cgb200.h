@@ -469,10 +469,10 @@ cgb_status cgb_server_destroy(cgb_server* s);
  * Scratch (frontier queues, visited bitmap, counters) lives in one static
  * device array of about 12.7 MB that every GPU loading the library keeps
  * until exit; V > CGB_NOALLOC_MAX_VERTICES is rejected with CGB_EINVAL.
- * The first call on a device looks up the array's device address (make it
- * before any stream capture).  All calls share the array: calls that overlap
- * on the GPU race and must be serialised by the caller.  Allocates nothing:
- * no cudaMalloc, cudaFree or allocating library routine. */
+ * The first call on a device looks up the array's device address.  All
+ * calls share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller.  Allocates nothing: no cudaMalloc, cudaFree or
+ * allocating library routine. */
 cgb_status cgb_bfs_noalloc(const uint32_t* offsets, const uint32_t* dest, uint32_t V, uint32_t E, uint32_t root,
                            uint32_t* levels, void* stream);
 
