@@ -369,13 +369,16 @@ static void cc_afforest(cgb_graph* g, bool weak)
                                                 &g->ctr->reached_edges);
         sync_counters(g);
         if ((double)g->h_ctr->reached_edges / kProbe > kDeepForest) {
+            // four passes per read-back; only the last pass of each group raises
+            // the flag, so a clear flag means that pass moved nothing
             const uint32_t jgrid = grid_for(V, kBlock, num_sms() * 8);
-            uint32_t pass = 0;
-            for (;; pass++) {
-                CGB_REQUIRE(pass < 40, CGB_ETIMEOUT, "CC pointer jumping did not converge");
-                CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->found, 0, sizeof(uint32_t), g->stream));
-                ++g->stats.launches;
-                k_cc_jump<<<jgrid, kBlock, 0, g->stream>>>(V, g->value, &g->ctr->found);
+            for (uint32_t group = 0;; group++) {
+                CGB_REQUIRE(group < 12, CGB_ETIMEOUT, "CC pointer jumping did not converge");
+                for (int k = 0; k < 4; k++) {
+                    if (k == 3) CGB_CUDA_TRY(cudaMemsetAsync(&g->ctr->found, 0, sizeof(uint32_t), g->stream));
+                    ++g->stats.launches;
+                    k_cc_jump<<<jgrid, kBlock, 0, g->stream>>>(V, g->value, &g->ctr->found);
+                }
                 sync_counters(g);
                 if (!g->h_ctr->found) break;
             }

@@ -219,7 +219,9 @@ void policy_log_sample(cgb_graph* g, const FeatIn& in, const float* ms, const bo
 
 // A choice is taken only when the network predicts a clear gain (5 % in
 // cost); otherwise the heuristic decides.
-constexpr float kMargin = 0.05f;
+// An override needs a predicted gain of 10 % (log-cost 0.1): about twice the
+// network's RMS error on its training samples.
+constexpr float kMargin = 0.10f;
 
 // The cheapest of n choices (outputs out[idx[i]]), or -1 when it does not
 // beat the heuristic's choice `heur` by the margin.

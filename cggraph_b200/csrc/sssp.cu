@@ -441,8 +441,9 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
     // bucket after bucket (measured on RMAT-24: 6.9 against 5.2 ms a run).
     // Under the learned schedule the tail waits for the first bucket
     // boundary, so that the network picks the delta it keeps.
-    const bool tail_ok = !tracing && !collect && o.schedule != CGB_SCHED_FIXED && g->tune.persist_enter > 0 &&
-                         g->max_degree < g->tune.persist_deg;
+    const bool tail_fits = !tracing && o.schedule != CGB_SCHED_FIXED && g->tune.persist_enter > 0 &&
+                           g->max_degree < g->tune.persist_deg;
+    const bool tail_ok = tail_fits && !collect;
     bool tail_delta_chosen = pol == nullptr;
     auto device_tail = [&]() -> bool {
         if (timing) ktimer_begin(g, CGB_K_PUSH);
@@ -692,7 +693,17 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
             for (int k = 0; k < kNumDeltaChoices; k++) {
                 const uint32_t dk = std::max<uint32_t>(1u, (uint32_t)(base_delta * delta_scale(k)));
                 CGB_CUDA_TRY(cudaEventRecord(g->ev_iter[0], g->stream));
+                // the rest of the run as a run with this delta would go, the
+                // device-resident tail included (it changes what a round costs)
+                delta = dk;
                 do {
+                    if (tail_fits) {
+                        near_maxdeg = 0;
+                        if (device_tail()) {
+                            near_rounds();
+                            continue;
+                        }
+                    }
                     advance(dk);
                     near_rounds();
                 } while (nfar > 0);
@@ -713,6 +724,7 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
                 bucket_lo = s_lo;
                 nnear = 0;
                 cur = s_cur;
+                delta = base_delta;
             }
             in_delta_trial = false;
             policy_log_sample(g, state_now(), ms, have);
