@@ -1194,14 +1194,6 @@ static void group_loop(cgb_server* s, int a)
                     }
                     lone = due > 0 && due <= kLoneMaxDue &&
                            (double)due * s->lone_est_us[a] <= std::max(s->batch_est_us[a], s->lone_est_us[a]);
-                    // a single-root run holds the graph, which the other group's
-                    // single-root runs and BFS ticks need: the group with the
-                    // longer runs takes it only while the other one is quiet
-                    const int b = a ^ 1;
-                    const bool other_quiet =
-                        s->grp[b].active == 0 &&
-                        (s->waiting[b].empty() || s->reqs[s->waiting[b].front()].info.arrival_us > now);
-                    if (lone && !other_quiet && s->lone_est_us[a] > s->lone_est_us[b]) lone = false;
                 }
                 // a running group takes new queries only while at least half of
                 // its slots are free (unless CGB_SERVER_ADMIT_ANY_SLOT), so that
