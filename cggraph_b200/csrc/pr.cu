@@ -43,6 +43,21 @@ __global__ void k_pr_init(uint32_t V, const uint32_t* __restrict__ outdeg, doubl
     }
 }
 
+// Gathers of the hottest contributions carry an L2 evict-last policy and the
+// rest evict-first.  The layout puts vertices in descending out-degree
+// buckets, so contributions [0, kPrHot) are the most gathered ones; 6.5 M
+// doubles (52 MB) stay in L2 beside the streamed column indices while the
+// long tail passes through (Chung-Lu, 330 MB of contributions: 7.3 -> 6.8 ms
+// per iteration; RMAT-24: 0.847 -> 0.817 ms; same results).
+constexpr uint32_t kPrHot = 6500000;
+
+__device__ __forceinline__ double ld_f64_l2hint(const double* p, uint64_t policy)
+{
+    double v;
+    asm volatile("ld.global.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(policy));
+    return v;
+}
+
 // One warp per 32-row slice of the sliced ELL: in step j every lane loads
 // its row's j-th source (one coalesced 128-byte load per warp) and gathers
 // that contribution; kU steps (cgb_tuning.pr_unroll) are issued before they
@@ -62,6 +77,9 @@ __global__ void __launch_bounds__(kBlock) k_pr_pull(uint32_t V, const uint64_t* 
     const uint32_t lane = lane_id();
     const uint32_t nslices = (V + 31) / 32;
     const uint32_t nwarps = gridDim.x * (kBlock / 32);
+    uint64_t pol_hot, pol_cold;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol_hot));
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol_cold));
     for (uint32_t s = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5); s < nslices; s += nwarps) {
         const uint32_t len = slice_len[s];
         const uint32_t* c = col + slice_ptr[s] + lane;
@@ -75,7 +93,7 @@ __global__ void __launch_bounds__(kBlock) k_pr_pull(uint32_t V, const uint64_t* 
             for (int t = 0; t < kU; t++) u[t] = j + t < len ? __ldcs(c + 32u * (j + t)) : V;  // read once
             double x[kU];
 #pragma unroll
-            for (int t = 0; t < kU; t++) x[t] = contrib[u[t]];
+            for (int t = 0; t < kU; t++) x[t] = ld_f64_l2hint(contrib + u[t], u[t] < kPrHot ? pol_hot : pol_cold);
 #pragma unroll
             for (int t = 0; t < kU; t++) acc += x[t];
         }
