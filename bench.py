@@ -145,7 +145,7 @@ def pick_roots(offsets: np.ndarray, seed: int, n: int) -> list:
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_pr_pull
 # launch, from a one-pass ncu capture of this bench with --algorithms pr on the
 # same graph, keyed by (scale, edge factor, seed).
-PR_PULL_DRAM_BYTES = {(24, 16, 1): 1.16e9 + 250.26e6, (22, 16, 1): 250.19e6 + 23.33e6}
+PR_PULL_DRAM_BYTES = {(24, 16, 1): 1166656256 + 225822208, (22, 16, 1): 250001920 + 20899072}
 
 
 def load_peaks() -> dict:

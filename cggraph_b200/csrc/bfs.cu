@@ -228,7 +228,7 @@ void run_bfs(cgb_graph* g, uint32_t root, const cgb_options& o)
     const bool timing = g->flags & CGB_FLAG_KERNEL_TIMING;
     const bool tracing = g->flags & CGB_FLAG_TRACE;
     PolicySamples* collect = want_pull && !force_pull ? g->collect : nullptr;
-    Policy* pol = (o.schedule == CGB_SCHED_LEARNED && want_pull && !force_pull) ? policy_get() : nullptr;
+    Policy* pol = (o.schedule == CGB_SCHED_LEARNED && want_pull && !force_pull) ? policy_for(g) : nullptr;
 
     PinnedArray<uint32_t> host_root_deg(2);  // pinned: see pinned_acquire
     CGB_CUDA_TRY(cudaMemcpyAsync(host_root_deg.data(), g->off + root, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost,

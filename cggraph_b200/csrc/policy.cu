@@ -38,6 +38,11 @@ Policy* policy_get()
 
 const float* policy_params_device(Policy* p) { return p ? p->params : nullptr; }
 
+Policy* policy_for(const cgb_graph* g)
+{
+    return g->E >= kPolicyMinEdges ? policy_get() : nullptr;
+}
+
 // ------------------------------------------------------------ kernels
 // One sample through the network with the CTA's 64 threads.  f: 24 features
 // in shared memory; h1, h2: 64 floats each in shared memory.

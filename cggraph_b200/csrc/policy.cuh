@@ -81,6 +81,13 @@ struct Policy;
 
 // The policy loaded on the current device, or nullptr (heuristic fallback).
 Policy* policy_get();
+
+// The policy for a learned run on g: none below kPolicyMinEdges edges.  Each
+// decision costs about 10 us of inference and a read-back; on such graphs a
+// whole BFS takes about half a millisecond, and the measured choices were
+// worth less (RMAT-20 BFS ran 0.86-0.91x under the network).
+constexpr uint64_t kPolicyMinEdges = 1ull << 26;
+Policy* policy_for(const cgb_graph* g);
 const float* policy_params_device(Policy* p);
 
 // Queues the network on the graph's stream: features from `in` (with the

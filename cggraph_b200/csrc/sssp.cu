@@ -403,7 +403,7 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
     uint32_t* far_bm = g->front_bm;  // the BFS bitmaps are free during SSSP
     uint32_t* near_bm = g->visited;
     const uint64_t max_iters = o.max_iterations ? o.max_iterations : ~0ull;
-    Policy* pol = (o.schedule == CGB_SCHED_LEARNED) ? policy_get() : nullptr;
+    Policy* pol = (o.schedule == CGB_SCHED_LEARNED) ? policy_for(g) : nullptr;
     PolicySamples* collect = g->collect;
     const uint32_t base_delta = delta;
 
