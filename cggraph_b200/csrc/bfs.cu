@@ -352,6 +352,11 @@ void run_bfs(cgb_graph* g, uint32_t root, const cgb_options& o)
             float ms[kPolicyOutputs] = {};
             bool have[kPolicyOutputs] = {};
             const int outs[3] = {kOutPush, kOutPull, kOutPushChunked};
+            // every trial starts right after a restore, the first one too: after
+            // the snapshot copy alone the levels array is colder in L2, and the
+            // first variant timed slower than it runs (a bias toward the others)
+            CGB_CUDA_TRY(cudaMemcpyAsync(g->value, collect->save_value, vbytes, cudaMemcpyDeviceToDevice, g->stream));
+            CGB_CUDA_TRY(cudaMemcpyAsync(g->visited, collect->save_bm0, wbytes, cudaMemcpyDeviceToDevice, g->stream));
             for (int d = 0; d < 3; d++) {
                 CGB_CUDA_TRY(cudaEventRecord(g->ev_iter[0], g->stream));
                 do_level(d == 1, out, d == 2 ? kExpandChunked : kExpandBinned);

@@ -559,6 +559,11 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
                 float ms[kPolicyOutputs] = {};
                 bool have[kPolicyOutputs] = {};
                 int best = heur;
+                // every trial starts right after a restore, the first one too (the
+                // snapshot copy alone leaves dist[] colder in L2 for the first)
+                CGB_CUDA_TRY(cudaMemcpyAsync(g->value, collect->save_value, vbytes, cudaMemcpyDeviceToDevice,
+                                             g->stream));
+                CGB_CUDA_TRY(cudaMemcpyAsync(far_bm, collect->save_bm0, wbytes, cudaMemcpyDeviceToDevice, g->stream));
                 for (int v = 0; v < kNumRoundChoices; v++) {
                     CGB_CUDA_TRY(cudaEventRecord(g->ev_iter[0], g->stream));
                     run_round(v, out);
@@ -690,6 +695,8 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
             bool have[kPolicyOutputs] = {};
             int best = kDeltaUnit;
             in_delta_trial = true;
+            CGB_CUDA_TRY(cudaMemcpyAsync(g->value, collect->save_value, vbytes, cudaMemcpyDeviceToDevice, g->stream));
+            CGB_CUDA_TRY(cudaMemcpyAsync(far_bm, collect->save_bm0, wbytes, cudaMemcpyDeviceToDevice, g->stream));
             for (int k = 0; k < kNumDeltaChoices; k++) {
                 const uint32_t dk = std::max<uint32_t>(1u, (uint32_t)(base_delta * delta_scale(k)));
                 CGB_CUDA_TRY(cudaEventRecord(g->ev_iter[0], g->stream));
