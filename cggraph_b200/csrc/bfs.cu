@@ -406,7 +406,7 @@ void run_bfs(cgb_graph* g, uint32_t root, const cgb_options& o)
         const double r_alpha = (double)scout * alpha / (double)std::max<int64_t>(edges_to_check, 1);
         const double r_beta = (double)nf * beta / (double)V;
         const bool near_boundary = (r_alpha > 1.0 / 64 && r_alpha < 64.0) || (r_beta > 1.0 / 64 && r_beta < 64.0);
-        const bool infer = pol && near_boundary;
+        const bool infer = kPolicyLevels && pol && near_boundary;
         if (infer) {
             FeatIn in = before;
             in.unvisited_e = (double)std::max<int64_t>(edges_to_check - (int64_t)scout, 0);

@@ -87,6 +87,17 @@ Policy* policy_get();
 // whole BFS takes about half a millisecond, and the measured choices were
 // worth less (RMAT-20 BFS ran 0.86-0.91x under the network).
 constexpr uint64_t kPolicyMinEdges = 1ull << 26;
+
+// Which of the network's decisions a learned run applies.  The delta is
+// trained on the cost of the whole rest of the run.  A BFS level's or an
+// SSSP round's variant is trained on that step alone, and a step's choice
+// also shapes the next one (a dense round hands the next round a queue in
+// vertex order, a pushed one in discovery order): the step costs predicted
+// the trials faithfully, yet following them made RMAT-23/24 SSSP 0.82-0.89x
+// and BFS 0.91-0.97x of the heuristic.  Those heads are trained and
+// evaluated (cgb_policy_collect, cgb_policy_forward) but not applied.
+constexpr bool kPolicyLevels = false;  // BFS push / pull and expansion variant
+constexpr bool kPolicyRounds = false;  // SSSP round variant
 Policy* policy_for(const cgb_graph* g);
 const float* policy_params_device(Policy* p);
 

@@ -595,7 +595,8 @@ static void sssp_loop(cgb_graph* g, uint32_t root, uint32_t delta, const cgb_opt
             if (tracing) CGB_CUDA_TRY(cudaEventRecord(g->ev_iter[1], g->stream));
             // inference for the next round, fused before the counter read-back; skipped
             // after small rounds, whose successors' variant hardly matters
-            const bool infer = pol && !collect && (nnear >= kCollectMinRound || near_edges >= g->E / 1024);
+            const bool infer =
+                kPolicyRounds && pol && !collect && (nnear >= kCollectMinRound || near_edges >= g->E / 1024);
             if (infer) policy_enqueue(pol, g, before, 2, false, out);
             have_round_out = infer;
             last_variant = variant;
