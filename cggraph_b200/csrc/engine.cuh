@@ -191,6 +191,7 @@ void graph_set_weights(cgb_graph* g, const uint32_t* weight);
 void validate_and_sort(cgb_graph* g);
 void compute_weight_sum(cgb_graph* g);
 uint32_t sssp_default_delta(const cgb_graph* g);           // single-root runs
+void ensure_max_degree(cgb_graph* g);                      // g->max_degree, computed once
 uint32_t sssp_delta_for(const cgb_graph* g, double c);     // c x mean weight / mean out-degree
 
 // workspace management (graph.cu)

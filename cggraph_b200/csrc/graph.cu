@@ -1083,9 +1083,15 @@ void ensure_frontier(cgb_graph* g)
     g->stamp = dalloc<uint32_t>(V, g->stream);
     g->sample = dalloc<uint32_t>(1024, g->stream);
     g->aux_bm = dalloc<uint32_t>(3 * (size_t)g->words(), g->stream);
+    ensure_max_degree(g);
+}
+
+void ensure_max_degree(cgb_graph* g)
+{
+    if (g->max_degree || g->E == 0) return;
     uint32_t* d = dalloc<uint32_t>(1, g->stream);
     CGB_CUDA_TRY(cudaMemsetAsync(d, 0, 4, g->stream));
-    k_max_degree<<<grid_for(V, kBlock, num_sms() * 8), kBlock, 0, g->stream>>>(V, g->off, d);
+    k_max_degree<<<grid_for(g->V, kBlock, num_sms() * 8), kBlock, 0, g->stream>>>(g->V, g->off, d);
     PinnedArray<uint32_t> md(1);
     CGB_CUDA_TRY(cudaMemcpyAsync(md.data(), d, 4, cudaMemcpyDeviceToHost, g->stream));
     CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));

@@ -43,13 +43,17 @@ __global__ void k_pr_init(uint32_t V, const uint32_t* __restrict__ outdeg, doubl
     }
 }
 
-// Gathers of the hottest contributions carry an L2 evict-last policy and the
-// rest evict-first.  The layout puts vertices in descending out-degree
-// buckets, so contributions [0, kPrHot) are the most gathered ones; 6.5 M
-// doubles (52 MB) stay in L2 beside the streamed column indices while the
-// long tail passes through (Chung-Lu, 330 MB of contributions: 7.3 -> 6.8 ms
-// per iteration; RMAT-24: 0.847 -> 0.817 ms; same results).
+// On skewed graphs (kHint) the gathers of the hottest contributions carry an
+// L2 evict-last policy and the rest evict-first.  The layout puts vertices in
+// descending out-degree buckets, so contributions [0, kPrHot) are the most
+// gathered ones; 6.5 M doubles (52 MB) stay in L2 beside the streamed column
+// indices while the long tail passes through (Chung-Lu, 330 MB of
+// contributions: 7.3 -> 6.8 ms per iteration; RMAT-24: 0.847 -> 0.817 ms;
+// same results).  Graphs without hubs (meshes) keep plain loads: their
+// contributions are reused by nearby rows, which evict-first cut short (the
+// 4800 x 5000 grid: 6.5 -> 7.5 ms per run with the hints).
 constexpr uint32_t kPrHot = 6500000;
+constexpr uint32_t kPrHintMinDeg = 64;  // largest out-degree from which a graph counts as skewed
 
 __device__ __forceinline__ double ld_f64_l2hint(const double* p, uint64_t policy)
 {
@@ -65,7 +69,7 @@ __device__ __forceinline__ double ld_f64_l2hint(const double* p, uint64_t policy
 // vertex V, whose contribution is 0.  Hub rows (bit set in hub_bm) are
 // finished by k_pr_hub_finish.  The slice stream and the outputs use
 // evict-first accesses so that L2 keeps the gathered contributions.
-template <int kU>
+template <int kU, bool kHint>
 __global__ void __launch_bounds__(kBlock) k_pr_pull(uint32_t V, const uint64_t* __restrict__ slice_ptr,
                                                     const uint32_t* __restrict__ slice_len,
                                                     const uint32_t* __restrict__ col,
@@ -93,7 +97,8 @@ __global__ void __launch_bounds__(kBlock) k_pr_pull(uint32_t V, const uint64_t* 
             for (int t = 0; t < kU; t++) u[t] = j + t < len ? __ldcs(c + 32u * (j + t)) : V;  // read once
             double x[kU];
 #pragma unroll
-            for (int t = 0; t < kU; t++) x[t] = ld_f64_l2hint(contrib + u[t], u[t] < kPrHot ? pol_hot : pol_cold);
+            for (int t = 0; t < kU; t++)
+                x[t] = kHint ? ld_f64_l2hint(contrib + u[t], u[t] < kPrHot ? pol_hot : pol_cold) : contrib[u[t]];
 #pragma unroll
             for (int t = 0; t < kU; t++) acc += x[t];
         }
@@ -169,6 +174,7 @@ void run_pr(cgb_graph* g, uint32_t iters, const cgb_options& o)
 {
     (void)o;
     ensure_pr(g);
+    ensure_max_degree(g);
     const bool timing = g->flags & CGB_FLAG_KERNEL_TIMING;
     const uint32_t V = g->V;
     const double base = 0.15 / (double)V;
@@ -203,7 +209,10 @@ void run_pr(cgb_graph* g, uint32_t iters, const cgb_options& o)
             CGB_CUDA_TRY(cudaEventRecord(g->ev_join, g->aux_stream));
         }
         ++g->stats.launches;
-        auto pull = unroll == 4 ? k_pr_pull<4> : unroll == 16 ? k_pr_pull<16> : k_pr_pull<8>;
+        const bool hint = g->max_degree >= kPrHintMinDeg;
+        auto pull = unroll == 4 ? (hint ? k_pr_pull<4, true> : k_pr_pull<4, false>)
+                    : unroll == 16 ? (hint ? k_pr_pull<16, true> : k_pr_pull<16, false>)
+                                   : (hint ? k_pr_pull<8, true> : k_pr_pull<8, false>);
         pull<<<grid, kBlock, 0, g->stream>>>(V, g->pr_slice_ptr, g->pr_slice_len, g->pr_col, g->pr_hub_bm,
                                              g->pr_outdeg, g->contrib[cur], g->pr[out], g->contrib[out], base, damp);
         if (fork) CGB_CUDA_TRY(cudaStreamWaitEvent(g->stream, g->ev_join, 0));
