@@ -609,7 +609,6 @@ struct cgb_server {
     Clock::time_point t0;
     uint64_t ticks[2] = {0, 0}, completed = 0;
     double busy_ms[2] = {0, 0};
-    std::atomic<int> graph_waiters{0};  // group threads waiting for the graph's lock
     double lone_est_us[2] = {0, 0};   // running mean of single-root run times
     double batch_est_us[2] = {0, 0};  // running mean of batched queries' admission-to-result times
     uint64_t lone_runs[2] = {0, 0}, batch_runs[2] = {0, 0};
@@ -1120,9 +1119,7 @@ static void lone_run(cgb_server* s, Group& G, int a, uint32_t k)
     cgb_graph* g = s->g;
     const auto t0 = Clock::now();
     {
-        s->graph_waiters++;
         std::lock_guard<GraphMutex> glk(g->mu);
-        s->graph_waiters--;
         // the engine's device-resident loops are cooperative launches, as the groups' are
         std::lock_guard<std::mutex> coop(s->coop_mu);
         cgb_options o;
@@ -1197,13 +1194,6 @@ static void group_loop(cgb_server* s, int a)
                     }
                     lone = due > 0 && due <= kLoneMaxDue &&
                            (double)due * s->lone_est_us[a] <= std::max(s->batch_est_us[a], s->lone_est_us[a]);
-                    // the other group waits for the graph (a BFS tick, or its own
-                    // single-root run): let it have the graph first, then decide
-                    // again, instead of taking it for one more run
-                    if (lone && s->graph_waiters.load() > 0) {
-                        s->cv.wait_for(lk, std::chrono::microseconds(50));
-                        continue;
-                    }
                 }
                 // a running group takes new queries only while at least half of
                 // its slots are free (unless CGB_SERVER_ADMIT_ANY_SLOT), so that
@@ -1236,9 +1226,7 @@ static void group_loop(cgb_server* s, int a)
                 lone_run(s, G, a, (uint32_t)lone_k);
                 lone_k = -1;
             } else if (a == 0) {
-                s->graph_waiters++;
                 std::lock_guard<GraphMutex> glk(g->mu);
-                s->graph_waiters--;
                 g->tune = g->tune_alg[CGB_BFS];
                 bfs_admit(s, G);
                 // small frontiers whose levels push: on the device, many levels per launch
