@@ -1117,11 +1117,12 @@ constexpr uint32_t kLoneMaxDue = 4;
 static void lone_run(cgb_server* s, Group& G, int a, uint32_t k)
 {
     cgb_graph* g = s->g;
-    const auto t0 = Clock::now();
+    Clock::time_point t0;
     {
         std::lock_guard<GraphMutex> glk(g->mu);
         // the engine's device-resident loops are cooperative launches, as the groups' are
         std::lock_guard<std::mutex> coop(s->coop_mu);
+        t0 = Clock::now();  // the run's own time, not the wait for the graph
         cgb_options o;
         memset(&o, 0, sizeof(o));
         o.struct_size = sizeof(o);
