@@ -1025,6 +1025,15 @@ static unsigned long long sp_device_ticks(cgb_server* s, Group& G)
     G.fcur = h.fcur;
     G.tick += h.ticks;
     G.loop_levels += h.ticks;
+    if (h.ticks) {
+        // the host ticks' expansions read the thresholds from d_up: they moved on
+        // the device, so the next host tick must not classify with the old ones
+        // (a vertex improved into [old, new) would go to the far list and be
+        // dropped by the next split, which starts at the new threshold)
+        for (uint32_t k = 0; k < kSrvSlots; k++)
+            G.h_up->thr[k] = (uint32_t)std::min<uint64_t>(G.thr[k], 0xFFFFFFFFu);
+        CGB_CUDA_TRY(cudaMemcpyAsync(G.d_up->thr, G.h_up->thr, sizeof(G.h_up->thr), cudaMemcpyHostToDevice, G.stream));
+    }
     G.loop_launches++;
     return h.ticks ? h.finished : 0ull;
 }

@@ -77,6 +77,23 @@ def test_server_high_diameter_grid(oracle, flags):
         _serve_and_check(g, queries, arrivals, bfs_slots=4, sssp_slots=4, sssp_delta=300, flags=flags)
 
 
+@pytest.mark.parametrize("seed", [11, 12, 13, 14])
+def test_server_loop_and_tick_switches(oracle, seed):
+    """Default flags on the grid with both algorithms in the mix: the SSSP
+    group runs its device-resident loop while the BFS group is idle and host
+    ticks while it is not, so one traversal switches between the two many
+    times; thresholds advanced on the device must reach the host ticks (a
+    stale threshold once dropped vertices from a late query's far list)."""
+    off, dst, w = oracle.grid_graph(40, 60, seed=5)
+    rng = np.random.default_rng(seed)
+    V = off.size - 1
+    queries = [(int(rng.integers(0, 2)), int(rng.integers(0, V))) for _ in range(48)]
+    arrivals = _poisson_arrivals(len(queries), 2000 * (seed - 10), seed)
+    with cg.Graph.from_csr(off, dst, w) as g:
+        g._host_off = off
+        _serve_and_check(g, queries, arrivals, bfs_slots=4, sssp_slots=4, sssp_delta=300)
+
+
 def test_server_sparse_arrivals_run_alone(oracle):
     """Below capacity (20 req/s against queries of well under a
     millisecond) each query finds its group idle and runs on the
