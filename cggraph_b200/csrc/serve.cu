@@ -597,6 +597,7 @@ struct cgb_server {
     // for each other at grid barriers; two of them resident at once could each
     // hold SMs the other waits for, so one runs at a time.
     std::mutex coop_mu;
+    std::atomic<int> coop_waiters{0};  // threads waiting for coop_mu: a running loop returns for them
     Group grp[2];  // [0] BFS, [1] SSSP
     std::vector<SrvReq> reqs;
     std::deque<int64_t> waiting[2];    // submitted, not admitted (arrival order of submission)
@@ -911,7 +912,9 @@ static unsigned long long bfs_device_levels(cgb_server* s, Group& G, uint32_t nf
     static uint32_t grid = 0;
     if (!grid) grid = cooperative_grid(k_srv_bfs_loop);
     void* kargs[] = {&args};
+    s->coop_waiters++;
     std::lock_guard<std::mutex> coop(s->coop_mu);
+    s->coop_waiters--;
     CGB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_srv_bfs_loop, grid, kBlock, kargs, 0, G.stream));
     CGB_CUDA_TRY(cudaMemcpyAsync(&h, G.loop, sizeof(SrvBfsLoopState), cudaMemcpyDeviceToHost, G.stream));
     CGB_CUDA_TRY(cudaEventRecord(G.ev_loop, G.stream));
@@ -919,7 +922,8 @@ static unsigned long long bfs_device_levels(cgb_server* s, Group& G, uint32_t nf
         const cudaError_t e = cudaEventQuery(G.ev_loop);
         if (e == cudaSuccess) break;
         if (e != cudaErrorNotReady) CGB_CUDA_TRY(e);
-        if (admission_due(s, G, 0)) *reinterpret_cast<volatile uint32_t*>(G.mailbox) = 1;
+        if (admission_due(s, G, 0) || s->coop_waiters.load() > 0)
+            *reinterpret_cast<volatile uint32_t*>(G.mailbox) = 1;
         std::this_thread::sleep_for(std::chrono::microseconds(20));
     }
     CGB_REQUIRE(!(h.ps.status & 2u), CGB_EOVERFLOW, "server BFS loop: queue overflow");
@@ -992,7 +996,9 @@ static unsigned long long sp_device_ticks(cgb_server* s, Group& G)
     args.mailbox = G.mailbox;
     args.st = G.sp_loop;
     void* kargs[] = {&args};
+    s->coop_waiters++;
     std::lock_guard<std::mutex> coop(s->coop_mu);
+    s->coop_waiters--;
     if (g->w) {
         static uint32_t grid = 0;
         if (!grid) grid = cooperative_grid_n(k_srv_sssp_loop<true>, 4);
@@ -1009,7 +1015,8 @@ static unsigned long long sp_device_ticks(cgb_server* s, Group& G)
         const cudaError_t e = cudaEventQuery(G.ev_loop);
         if (e == cudaSuccess) break;
         if (e != cudaErrorNotReady) CGB_CUDA_TRY(e);
-        if (admission_due(s, G, 1)) *reinterpret_cast<volatile uint32_t*>(G.mailbox) = 1;
+        if (admission_due(s, G, 1) || s->coop_waiters.load() > 0)
+            *reinterpret_cast<volatile uint32_t*>(G.mailbox) = 1;
         std::this_thread::sleep_for(std::chrono::microseconds(20));
     }
     CGB_REQUIRE(!b.h->overflow, CGB_EOVERFLOW, "server SSSP loop: queue overflow");
@@ -1130,7 +1137,9 @@ static void lone_run(cgb_server* s, Group& G, int a, uint32_t k)
     {
         std::lock_guard<GraphMutex> glk(g->mu);
         // the engine's device-resident loops are cooperative launches, as the groups' are
+        s->coop_waiters++;
         std::lock_guard<std::mutex> coop(s->coop_mu);
+        s->coop_waiters--;
         t0 = Clock::now();  // the run's own time, not the wait for the graph
         cgb_options o;
         memset(&o, 0, sizeof(o));
