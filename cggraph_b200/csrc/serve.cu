@@ -1198,14 +1198,17 @@ static void group_loop(cgb_server* s, int a)
                 std::unique_lock<std::mutex> lk(s->mu);
                 if (s->error != CGB_OK) break;
                 const double now = us_since(s, Clock::now());
-                // an idle group serves up to kLoneMaxDue due queries one by one
-                // on the single-root engine while that ends them sooner than a
-                // batch would (running means of both services), else batches
-                // them.  The cap bounds how long single-root runs, which hold the
+                // up to kLoneMaxDue due queries are served one by one on the
+                // single-root engine while that ends them sooner than a batch
+                // would (running means of both services), else they are batched.
+                // This holds while the group's batch runs too (a single-root run
+                // then comes between two of its ticks): otherwise one batched query
+                // at moderate load made every later arrival join a slow batch of a
+                // few.  The cap bounds how long single-root runs, which hold the
                 // graph, keep the other group's ticks waiting; and under load a
                 // batch serves many more queries per second.
                 bool lone = false;
-                if (G.active == 0 && !(s->flags & CGB_SERVER_BATCH_ONLY)) {
+                if (!(s->flags & CGB_SERVER_BATCH_ONLY)) {
                     uint32_t due = 0;
                     for (const int64_t r : s->waiting[a]) {
                         if (s->reqs[r].info.arrival_us > now || due > kLoneMaxDue) break;
@@ -1223,7 +1226,8 @@ static void group_loop(cgb_server* s, int a)
                 // they take turns on the cooperative-launch lock, whereas ticks of
                 // both groups overlap on their two streams
                 other_idle = s->grp[a ^ 1].active == 0;
-                if (!hold) pick_admissions(s, G, s->waiting[a], now, lone ? 1u : kSrvSlots);
+                if (lone) pick_admissions(s, G, s->waiting[a], now, 1u);  // needs a free slot, not a batch
+                else if (!hold) pick_admissions(s, G, s->waiting[a], now, kSrvSlots);
                 else G.admit.clear();
                 if (lone && G.admit.size() == 1) {
                     lone_k = (int)G.admit[0];
