@@ -611,7 +611,11 @@ struct cgb_server {
     uint64_t ticks[2] = {0, 0}, completed = 0;
     double busy_ms[2] = {0, 0};
     double lone_est_us[2] = {0, 0};   // running mean of single-root run times
-    double batch_est_us[2] = {0, 0};  // running mean of batched queries' admission-to-result times
+    // running mean of batched queries' admission-to-result times; until a batched
+    // query has finished, unknown (infinite): due queries go the single-root way
+    // (at most kLoneMaxDue at a time), since a zero start let the first two queries
+    // due together start a batch that later arrivals joined
+    double batch_est_us[2] = {1e300, 1e300};
     uint64_t lone_runs[2] = {0, 0}, batch_runs[2] = {0, 0};
     cgb_status error = CGB_OK;
     std::string error_msg;
