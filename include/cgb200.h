@@ -412,10 +412,11 @@ typedef struct {
 #define CGB_SERVER_NO_SSSP 0x2u /* no SSSP slots (saves the 256 B per vertex of distances) */
 #define CGB_SERVER_HOST_TICKS 0x4u /* advance every level from the host thread (one synchronisation per
                                       level) instead of the device-resident level loop */
-#define CGB_SERVER_BATCH_ONLY 0x8u /* every query joins its multi-root group.  By default an idle group
+#define CGB_SERVER_BATCH_ONLY 0x8u /* every query joins its multi-root group.  By default a group
                                       serves its n <= 4 due queries one at a time on the single-root
-                                      engine of cgb_run while n x (mean single-root time) <= (mean
-                                      admission-to-result time of batched queries), and batches them
+                                      engine of cgb_run (between two ticks of its batch, if one runs)
+                                      while n x (mean single-root time) <= (mean admission-to-result
+                                      time of batched queries; unknown = infinite), and batches them
                                       otherwise */
 #define CGB_SERVER_ADMIT_ANY_SLOT 0x10u /* a running group admits a due query into any free slot; by
                                            default only while at least half of its slots are free, so
