@@ -221,7 +221,10 @@ cgb_status cgb_graph_partition(cgb_graph* g, int algorithm, uint32_t num_devices
 
 cgb_status cgb_graph_destroy(cgb_graph* g)
 {
-    return guarded([&] { graph_free(g); });
+    return guarded([&] {
+        CGB_REQUIRE(!g || g->servers.load() == 0, CGB_EINVAL, "a request server is attached to the graph");
+        graph_free(g);
+    });
 }
 
 cgb_status cgb_graph_set_stream(cgb_graph* g, void* stream)

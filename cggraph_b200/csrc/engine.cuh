@@ -2,6 +2,7 @@
 #pragma once
 
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 #include <vector>
 
@@ -171,6 +172,11 @@ struct cgb_graph {
     PolicySamples* collect = nullptr;   // set while cgb_policy_collect runs
     uint32_t flags = 0;
 
+    // request servers attached (cgb_server_create): their SSSP groups and
+    // second engine context read w without the graph's lock, so the weights
+    // cannot be replaced meanwhile
+    std::atomic<int> servers{0};
+
     uint32_t words() const { return V / 32 + 1; }
     cgb_graph() { mu.owner = this; }
 };
@@ -192,6 +198,11 @@ void validate_and_sort(cgb_graph* g);
 void compute_weight_sum(cgb_graph* g);
 uint32_t sssp_default_delta(const cgb_graph* g);           // single-root runs
 void ensure_max_degree(cgb_graph* g);                      // g->max_degree, computed once
+// A second single-root engine context over g's CSR (borrowed, not copied):
+// own stream, counters, distances and frontier scratch.  Freed with
+// graph_shadow_free, which leaves g's arrays alone.
+cgb_graph* graph_shadow(cgb_graph* g);
+void graph_shadow_free(cgb_graph* sh);
 uint32_t sssp_delta_for(const cgb_graph* g, double c);     // c x mean weight / mean out-degree
 
 // workspace management (graph.cu)

@@ -703,6 +703,7 @@ void graph_set_weights(cgb_graph* g, const uint32_t* weight)
 {
     CGB_REQUIRE(!g->lists_resorted, CGB_EINVAL,
                 "weights must be given to cgb_graph_create when it had to sort the neighbour lists");
+    CGB_REQUIRE(g->servers.load() == 0, CGB_EINVAL, "weights cannot change while a server is attached to the graph");
     const uint32_t E = g->E;
     if (E == 0) return;
     CGB_CUDA_TRY(cudaSetDevice(g->device));
@@ -1443,6 +1444,57 @@ cgb_graph* graph_alloc(uint32_t V, uint32_t E, uint32_t nz, int device, bool wit
         throw;
     }
     return g;
+}
+
+cgb_graph* graph_shadow(cgb_graph* g)
+{
+    CGB_CUDA_TRY(cudaSetDevice(g->device));
+    cgb_graph* sh = new cgb_graph();
+    sh->device = g->device;
+    sh->V = g->V;
+    sh->E = g->E;
+    sh->nz = g->nz;
+    sh->off = g->off;
+    sh->dst = g->dst;
+    sh->w = g->w;
+    sh->sum_w = g->sum_w;
+    sh->max_degree = g->max_degree;
+    sh->symmetric = g->symmetric;
+    sh->lists_resorted = g->lists_resorted;
+    // the in-edges too, when the graph has built them (borrowed as well)
+    sh->in_off = g->in_off;
+    sh->in_src = g->in_src;
+    sh->csc_owned = false;
+    sh->in_w = g->in_w;
+    sh->in_w_owned = false;
+    for (int a = 0; a < 4; a++) sh->tune_alg[a] = g->tune_alg[a];
+    try {
+        CGB_CUDA_TRY(cudaStreamCreateWithFlags(&sh->own_stream, cudaStreamNonBlocking));
+        sh->stream = sh->own_stream;
+        CGB_CUDA_TRY(cudaEventCreate(&sh->ev_start));
+        CGB_CUDA_TRY(cudaEventCreate(&sh->ev_stop));
+        CGB_CUDA_TRY(cudaEventCreate(&sh->ev_iter[0]));
+        CGB_CUDA_TRY(cudaEventCreate(&sh->ev_iter[1]));
+        sh->ctr = dalloc<DevCounters>(1, sh->stream);
+        sh->h_ctr = static_cast<DevCounters*>(pinned_small_alloc(sizeof(DevCounters)));
+        CGB_CUDA_TRY(cudaMemsetAsync(sh->ctr, 0, sizeof(DevCounters), sh->stream));
+        sh->value = dalloc<uint32_t>(sh->V, sh->stream);
+        CGB_CUDA_TRY(cudaStreamSynchronize(sh->stream));
+    } catch (...) {
+        graph_shadow_free(sh);
+        throw;
+    }
+    return sh;
+}
+
+void graph_shadow_free(cgb_graph* sh)
+{
+    if (!sh) return;
+    // borrowed from the graph it shadows (a CSC it built itself stays owned)
+    if (!sh->csc_owned) sh->in_off = sh->in_src = nullptr;
+    if (!sh->in_w_owned) sh->in_w = nullptr;
+    sh->off = sh->dst = sh->w = nullptr;
+    graph_free(sh);
 }
 
 void graph_free(cgb_graph* g)

@@ -592,6 +592,10 @@ using namespace cgb;
 
 struct cgb_server {
     cgb_graph* g = nullptr;
+    // a second single-root engine context over g's CSR for the SSSP group's
+    // single-root runs, so that they do not hold g, which BFS ticks and BFS
+    // single-root runs need
+    cgb_graph* shadow = nullptr;
     uint32_t flags = 0;  // cgb_server_config.flags
     // The groups' device-resident loops are cooperative launches whose CTAs wait
     // for each other at grid barriers; two of them resident at once could each
@@ -1136,7 +1140,7 @@ constexpr uint32_t kLoneMaxDue = 4;
 
 static void lone_run(cgb_server* s, Group& G, int a, uint32_t k)
 {
-    cgb_graph* g = s->g;
+    cgb_graph* g = (a == 1 && s->shadow) ? s->shadow : s->g;
     Clock::time_point t0;
     {
         std::lock_guard<GraphMutex> glk(g->mu);
@@ -1377,13 +1381,16 @@ cgb_status cgb_server_create(cgb_graph* g, const cgb_server_config* cfg, cgb_ser
             group_alloc(s, s->grp[0], CGB_BFS, nb);
             group_alloc(s, s->grp[1], CGB_SSSP, ns);
             s->grp[1].delta = c.sssp_delta ? c.sssp_delta : mssp_default_delta(g);
+            if (ns && !(c.flags & CGB_SERVER_BATCH_ONLY)) s->shadow = graph_shadow(g);
             CGB_CUDA_TRY(cudaDeviceSynchronize());
         } catch (...) {
             group_free(s, s->grp[0]);
             group_free(s, s->grp[1]);
+            graph_shadow_free(s->shadow);
             delete s;
             throw;
         }
+        g->servers++;
         *out = s;
     });
 }
@@ -1481,6 +1488,8 @@ cgb_status cgb_server_destroy(cgb_server* s)
         cudaSetDevice(s->g->device);
         group_free(s, s->grp[0]);
         group_free(s, s->grp[1]);
+        graph_shadow_free(s->shadow);
+        s->g->servers--;
         delete s;
     });
 }

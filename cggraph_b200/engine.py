@@ -343,7 +343,8 @@ class Graph:
     def set_weights(self, weight) -> None:
         """Attach (or replace) the edge weights, E values in CSR order
         (cgb_graph_set_weights); safe to call from another thread while a
-        BFS, CC or PageRank run uses the graph."""
+        BFS, CC or PageRank run uses the graph; refused while a Server is
+        attached to it."""
         weight = _u32(weight)
         check(L.lib().cgb_graph_set_weights(self._h, _ptr(weight)))
 

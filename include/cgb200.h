@@ -231,6 +231,8 @@ cgb_status cgb_graph_partition(cgb_graph* g, int algorithm, uint32_t num_devices
                                uint32_t* seg_order, uint32_t* seg_edges, int32_t* seg_owner,
                                uint32_t* device_segments, cgb_partition_info* info);
 
+/* CGB_EINVAL while a request server is attached to the graph (destroy the
+ * server first). */
 cgb_status cgb_graph_destroy(cgb_graph* g);
 
 /* Runs all later work of this graph on `stream` (a cudaStream_t of the
@@ -245,8 +247,8 @@ cgb_status cgb_graph_set_stream(cgb_graph* g, void* stream);
  * run on the same graph from another thread: the upload does not wait for
  * the graph. When it returns, the weights are in effect for every later
  * call on the graph (a run already in progress finishes with the old ones;
- * SSSP without weights uses unit weights). Not while a request server runs
- * on the graph. CGB_EINVAL when cgb_graph_create had to sort the neighbour
+ * SSSP without weights uses unit weights). CGB_EINVAL while a request
+ * server is attached to the graph, and when cgb_graph_create had to sort the neighbour
  * lists (give the weights to create then). Engine-specific (no reference
  * counterpart). */
 cgb_status cgb_graph_set_weights(cgb_graph* g, const uint32_t* weight);

@@ -112,6 +112,22 @@ def test_server_sparse_arrivals_run_alone(oracle):
             assert r["done_us"] - r["arrival_us"] < 50000
 
 
+def test_weights_fixed_while_a_server_is_attached(oracle):
+    """The SSSP group and its second engine context read the weights without
+    the graph's lock, so replacing them is refused while a server exists,
+    and allowed again once it is gone."""
+    off, dst, w = oracle.rmat_graph(12, 8, seed=3)
+    with cg.Graph.from_csr(off, dst, w) as g:
+        srv = cg.Server(g)
+        with pytest.raises(cg.CgbError):
+            g.set_weights(w)
+        srv.close()
+        g.set_weights(w[::-1].copy())
+        lone, _ = g.run(SSSP, 1)
+        g.set_weights(w)
+        np.testing.assert_array_equal(g.run(SSSP, 1)[0], oracle.sssp(off, dst, w, 1))
+
+
 def test_server_memory_budget_caps_slots(oracle):
     off, dst, w = oracle.rmat_graph(12, 8, seed=2)
     V = off.size - 1
