@@ -1141,13 +1141,23 @@ constexpr uint32_t kLoneMaxDue = 4;
 static void lone_run(cgb_server* s, Group& G, int a, uint32_t k)
 {
     cgb_graph* g = (a == 1 && s->shadow) ? s->shadow : s->g;
+    // the engine's device-resident loops are cooperative launches, as the
+    // groups' are, so a run that may start one takes the cooperative-launch
+    // lock: any BFS run (its small-frontier levels), and an SSSP run only
+    // where its device-resident tail can run (no list of persist_deg edges or
+    // more; on power-law graphs it never does, and SSSP runs then overlap
+    // BFS runs and ticks)
+    const cgb_tuning& t = g->tune_alg[CGB_SSSP];
+    const bool coop_needed = a == 0 || (t.persist_enter > 0 && g->max_degree < t.persist_deg);
     Clock::time_point t0;
     {
         std::lock_guard<GraphMutex> glk(g->mu);
-        // the engine's device-resident loops are cooperative launches, as the groups' are
-        s->coop_waiters++;
-        std::lock_guard<std::mutex> coop(s->coop_mu);
-        s->coop_waiters--;
+        std::unique_lock<std::mutex> coop(s->coop_mu, std::defer_lock);
+        if (coop_needed) {
+            s->coop_waiters++;
+            coop.lock();
+            s->coop_waiters--;
+        }
         t0 = Clock::now();  // the run's own time, not the wait for the graph
         cgb_options o;
         memset(&o, 0, sizeof(o));
