@@ -213,3 +213,19 @@ def test_struct_layouts_match_header(tmp_path):
         assert int(got[cname]) == ctypes.sizeof(py), cname
         for f, _ in py._fields_:
             assert int(got[f"{cname}.{f}"]) == getattr(py, f).offset, f"{cname}.{f}"
+
+
+def test_flag_constants_match_header():
+    """Every CGB_ flag and limit #define of the header that the Python
+    mirror names has the header's value (server, run, tuning flags...)."""
+    import re
+    from cggraph_b200 import _lib
+    text = open(os.path.join(ROOT, "include", "cgb200.h")).read()
+    defs = re.findall(r"#define CGB_(\w+)\s+(0x[0-9a-fA-F]+|\d+)u?\b", text)
+    named = [(n, int(v, 0)) for n, v in defs if hasattr(_lib, n)]
+    assert len(named) >= 20
+    for n, v in named:
+        assert getattr(_lib, n) == v, n
+    for n in ("SERVER_NO_BFS", "SERVER_NO_SSSP", "SERVER_HOST_TICKS", "SERVER_BATCH_ONLY", "SERVER_ADMIT_ANY_SLOT",
+              "FLAG_CC_WEAK", "TUNE_CC_WEAK"):
+        assert any(m == n for m, _ in named), n
