@@ -596,12 +596,6 @@ struct cgb_server {
     // single-root runs, so that they do not hold g, which BFS ticks and BFS
     // single-root runs need
     cgb_graph* shadow = nullptr;
-    // the graph's stream while the server is attached: created with the
-    // device's greatest priority, so BFS work (ticks and single-root runs,
-    // short) is scheduled ahead of SSSP work running beside it; the stream
-    // the graph had is restored when the server goes
-    cudaStream_t hi_stream = nullptr;
-    cudaStream_t prev_stream = nullptr;
     uint32_t flags = 0;  // cgb_server_config.flags
     // The groups' device-resident loops are cooperative launches whose CTAs wait
     // for each other at grid barriers; two of them resident at once could each
@@ -1394,12 +1388,6 @@ cgb_status cgb_server_create(cgb_graph* g, const cgb_server_config* cfg, cgb_ser
         s->g = g;
         s->flags = c.flags;
         try {
-            int least = 0, greatest = 0;
-            CGB_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
-            CGB_CUDA_TRY(cudaStreamCreateWithPriority(&s->hi_stream, cudaStreamNonBlocking, greatest));
-            CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
-            s->prev_stream = g->stream;
-            g->stream = s->hi_stream;
             group_alloc(s, s->grp[0], CGB_BFS, nb);
             group_alloc(s, s->grp[1], CGB_SSSP, ns);
             s->grp[1].delta = c.sssp_delta ? c.sssp_delta : mssp_default_delta(g);
@@ -1409,11 +1397,6 @@ cgb_status cgb_server_create(cgb_graph* g, const cgb_server_config* cfg, cgb_ser
             group_free(s, s->grp[0]);
             group_free(s, s->grp[1]);
             graph_shadow_free(s->shadow);
-            if (s->prev_stream) g->stream = s->prev_stream;
-            if (s->hi_stream) {
-                cudaStreamSynchronize(s->hi_stream);
-                cudaStreamDestroy(s->hi_stream);
-            }
             delete s;
             throw;
         }
@@ -1516,12 +1499,6 @@ cgb_status cgb_server_destroy(cgb_server* s)
         group_free(s, s->grp[0]);
         group_free(s, s->grp[1]);
         graph_shadow_free(s->shadow);
-        {
-            std::lock_guard<GraphMutex> lock(s->g->mu);
-            cudaStreamSynchronize(s->hi_stream);
-            s->g->stream = s->prev_stream;
-            cudaStreamDestroy(s->hi_stream);
-        }
         s->g->servers--;
         delete s;
     });
