@@ -231,6 +231,7 @@ cgb_status cgb_graph_set_stream(cgb_graph* g, void* stream)
 {
     return guarded([&] {
         CGB_REQUIRE(g != nullptr, CGB_EINVAL, "graph is NULL");
+        CGB_REQUIRE(g->servers.load() == 0, CGB_EINVAL, "a request server is attached to the graph");
         std::lock_guard<GraphMutex> lock(g->mu);
         CGB_CUDA_TRY(cudaSetDevice(g->device));
         CGB_CUDA_TRY(cudaStreamSynchronize(g->stream));

@@ -239,6 +239,8 @@ cgb_status cgb_graph_destroy(cgb_graph* g);
  * graph's device; NULL restores the graph's own stream).  Lets a caller
  * order the engine's kernels with its own work and time them with events on
  * its stream. */
+/* CGB_EINVAL while a request server is attached to the graph (its BFS group
+ * runs on the graph's stream). */
 cgb_status cgb_graph_set_stream(cgb_graph* g, void* stream);
 
 /* Attaches edge weights to a graph created without them, or replaces its
