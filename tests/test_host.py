@@ -150,3 +150,17 @@ def test_compute_indegree_engine_type():
     r = cg.main_partition(csr, cg.Algorithm_type.BFS, engine_type=cg.Engine_type.COMPUTE_INDEGREE)
     assert r["inDegree"].tolist() == [1, 1, 0, 3] and r["outDegree"].tolist() == [2, 1, 2, 0]
     assert r["top"] == [(3, 3), (0, 1), (1, 1), (2, 0)]
+
+
+def test_bench_refuses_gpus_without_one_process_per_gpu():
+    """bench.py --gpus N without torchrun's WORLD_SIZE=N stops with a message
+    naming the launch it needs, before any device work."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = {k: v for k, v in os.environ.items() if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK")}
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--gpus", "2", "--steps", "1"],
+                       capture_output=True, text=True, env=env, timeout=300)
+    assert r.returncode != 0
+    assert "torch.distributed.run --nproc-per-node 2" in r.stderr + r.stdout
